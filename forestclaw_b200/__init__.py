@@ -1,0 +1,308 @@
+"""forestclaw_b200 -- B200-native (sm_100a) clawpack 4.6 patch update, ghost fill and
+conservative time sync for ForestClaw-style forests of patches.
+
+The product is ``libfc2d_b200.so`` (C ABI in ``include/fc2d_b200.h``).  This module
+is a thin ctypes mirror of that ABI with the names and option keys of the
+reference's ``fc2d_clawpack46`` / ``fclaw`` options, so Python callers (and the
+tests) drive the same entry points a ForestClaw C shim would.  There is no CPU
+fallback: if the library or a GPU is missing, constructing a :class:`Solver`
+raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfc2d_b200.so")
+
+RP_ADVECTION, RP_SW_ROE, RP_SW_FWAVE = 0, 1, 2
+APP_NONE, APP_SWIRL, APP_RADIALDAM, APP_TSUNAMI = 0, 1, 2, 3
+PREC_FP64, PREC_FP32WAVE = 0, 1
+
+
+class B200Error(RuntimeError):
+    """A failed fc2d_b200_* call (status code and library message)."""
+
+    def __init__(self, fn: str, code: int, msg: str):
+        super().__init__(f"{fn} failed ({code}): {msg}")
+        self.code = code
+
+
+class _Options(ctypes.Structure):
+    _fields_ = [
+        ("mx", ctypes.c_int), ("my", ctypes.c_int), ("mbc", ctypes.c_int), ("meqn", ctypes.c_int),
+        ("maux", ctypes.c_int), ("mwaves", ctypes.c_int), ("order", ctypes.c_int * 2),
+        ("mthlim", ctypes.c_int * 8), ("mthbc", ctypes.c_int * 4), ("mcapa", ctypes.c_int),
+        ("use_fwaves", ctypes.c_int), ("rp", ctypes.c_int), ("minlevel", ctypes.c_int),
+        ("maxlevel", ctypes.c_int), ("subcycle", ctypes.c_int), ("time_sync", ctypes.c_int),
+        ("flux_correction", ctypes.c_int), ("fluctuation_correction", ctypes.c_int),
+        ("refine_threshold", ctypes.c_double), ("coarsen_threshold", ctypes.c_double),
+        ("ax", ctypes.c_double), ("bx", ctypes.c_double), ("ay", ctypes.c_double), ("by", ctypes.c_double),
+        ("mi", ctypes.c_int), ("mj", ctypes.c_int), ("app", ctypes.c_int), ("grav", ctypes.c_double),
+        ("tperiod", ctypes.c_double), ("r0", ctypes.c_double), ("hin", ctypes.c_double),
+        ("hout", ctypes.c_double), ("x0", ctypes.c_double), ("y0", ctypes.c_double),
+        ("pdata", ctypes.c_double * 32), ("precision", ctypes.c_int), ("device", ctypes.c_int),
+    ]
+
+
+@dataclass
+class Options:
+    """fc2d_b200_options_t with the reference's option names and defaults."""
+    mx: int = 16
+    my: int = 16
+    mbc: int = 2
+    meqn: int = 1
+    maux: int = 0
+    mwaves: int = 1
+    order: Sequence[int] = (2, 2)
+    mthlim: Sequence[int] = (4,)
+    mthbc: Sequence[int] = (1, 1, 1, 1)
+    mcapa: int = 0
+    use_fwaves: int = 0
+    rp: int = RP_ADVECTION
+    minlevel: int = 0
+    maxlevel: int = 0
+    subcycle: int = 0
+    time_sync: int = 0
+    flux_correction: int = 1
+    fluctuation_correction: int = 1
+    refine_threshold: float = 0.5
+    coarsen_threshold: float = 0.1
+    ax: float = 0.0
+    bx: float = 1.0
+    ay: float = 0.0
+    by: float = 1.0
+    mi: int = 1
+    mj: int = 1
+    app: int = APP_NONE
+    grav: float = 1.0
+    tperiod: float = 0.0
+    r0: float = 0.3
+    hin: float = 2.0
+    hout: float = 1.0
+    x0: float = 0.0
+    y0: float = 0.0
+    pdata: Sequence[float] = field(default_factory=tuple)
+    precision: int = PREC_FP64
+    device: int = 0
+
+    def to_c(self) -> _Options:
+        o = _Options()
+        for k in ("mx", "my", "mbc", "meqn", "maux", "mwaves", "mcapa", "use_fwaves", "rp", "minlevel",
+                  "maxlevel", "subcycle", "time_sync", "flux_correction", "fluctuation_correction",
+                  "refine_threshold", "coarsen_threshold", "ax", "bx", "ay", "by", "mi", "mj", "app", "grav",
+                  "tperiod", "r0", "hin", "hout", "x0", "y0", "precision", "device"):
+            setattr(o, k, getattr(self, k))
+        for i, v in enumerate(self.order):
+            o.order[i] = v
+        for i, v in enumerate(self.mthlim):
+            o.mthlim[i] = v
+        for i, v in enumerate(self.mthbc):
+            o.mthbc[i] = v
+        for i, v in enumerate(self.pdata):
+            o.pdata[i] = v
+        return o
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load the CUDA library (built in-tree by forestclaw_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: run `python -m forestclaw_b200.build` first")
+    L = ctypes.CDLL(path)
+    P, I, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    dp, ip = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    sig = {
+        "fc2d_b200_create": [ctypes.POINTER(_Options), ctypes.POINTER(P)],
+        "fc2d_b200_destroy": [P],
+        "fc2d_b200_set_riemann": [P, I],
+        "fc2d_b200_initialize": [P],
+        "fc2d_b200_set_forest": [P, I, ip, ip, ip],
+        "fc2d_b200_num_patches": [P, ip],
+        "fc2d_b200_patch_info": [P, ip, ip, ip, ip],
+        "fc2d_b200_get_q": [P, dp],
+        "fc2d_b200_set_q": [P, dp],
+        "fc2d_b200_get_aux": [P, dp],
+        "fc2d_b200_set_aux": [P, dp],
+        "fc2d_b200_registers_size": [P, ip],
+        "fc2d_b200_get_registers": [P, dp],
+        "fc2d_b200_level_update": [P, I, D, D, dp],
+        "fc2d_b200_single_step_update": [P, I, I, I, D, D, dp],
+        "fc2d_b200_ghost_update": [P, I, I, D, I],
+        "fc2d_b200_timeinterp": [P, I, D],
+        "fc2d_b200_time_sync": [P, I, I],
+        "fc2d_b200_advance": [P, D, D, dp],
+        "fc2d_b200_regrid": [P, ip],
+        "fc2d_b200_mass": [P, dp],
+        "fc2d_b200_cell_updates": [P, dp],
+        "fc2d_b200_synchronize": [P],
+        "fc2d_b200_last_update_stats": [P, dp, dp, ip, ip],
+        "fc2d_b200_set_timing": [P, I],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int
+    L.fc2d_b200_last_error.restype = ctypes.c_char_p
+    L.fc2d_b200_last_error.argtypes = []
+    _lib = L
+    return L
+
+
+def exported_symbols() -> list[str]:
+    """Names of the C ABI entry points declared in include/fc2d_b200.h."""
+    hdr = os.path.join(os.path.dirname(_HERE), "include", "fc2d_b200.h")
+    import re
+    with open(hdr) as f:
+        txt = f.read()
+    return sorted(set(re.findall(r"\b(fc2d_b200_[a-z_0-9]+)\s*\(", txt)))
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+class Solver:
+    """A device-resident forest of patches advanced by the sm_100a kernels."""
+
+    def __init__(self, opts: Options):
+        self.lib = load_library()
+        self.opts = opts
+        self._c = opts.to_c()
+        h = ctypes.c_void_p()
+        self._check("fc2d_b200_create", self.lib.fc2d_b200_create(ctypes.byref(self._c), ctypes.byref(h)))
+        self.h = h
+        self.nx = opts.mx + 2 * opts.mbc
+        self.ny = opts.my + 2 * opts.mbc
+
+    def _check(self, fn: str, rc: int) -> None:
+        if rc != 0:
+            raise B200Error(fn, rc, (self.lib.fc2d_b200_last_error() or b"").decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.fc2d_b200_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- setup -------------------------------------------------------------
+    def initialize(self) -> int:
+        self._check("fc2d_b200_initialize", self.lib.fc2d_b200_initialize(self.h))
+        return self.num_patches
+
+    def set_forest(self, level, gx, gy) -> None:
+        lv = np.ascontiguousarray(level, np.int32)
+        x = np.ascontiguousarray(gx, np.int32)
+        y = np.ascontiguousarray(gy, np.int32)
+        self._check("fc2d_b200_set_forest", self.lib.fc2d_b200_set_forest(self.h, len(lv), _ip(lv), _ip(x), _ip(y)))
+
+    @property
+    def num_patches(self) -> int:
+        n = ctypes.c_int()
+        self._check("fc2d_b200_num_patches", self.lib.fc2d_b200_num_patches(self.h, ctypes.byref(n)))
+        return n.value
+
+    def patch_info(self) -> np.ndarray:
+        n = self.num_patches
+        a = [np.zeros(n, np.int32) for _ in range(4)]
+        self._check("fc2d_b200_patch_info", self.lib.fc2d_b200_patch_info(self.h, *[_ip(x) for x in a]))
+        return np.stack(a, axis=1)
+
+    # -- data ---------------------------------------------------------------
+    def get_q(self) -> np.ndarray:
+        out = np.zeros((self.num_patches, self.opts.meqn, self.ny, self.nx), np.float64)
+        self._check("fc2d_b200_get_q", self.lib.fc2d_b200_get_q(self.h, _dp(out)))
+        return out
+
+    def set_q(self, q: np.ndarray) -> None:
+        q = np.ascontiguousarray(q, np.float64)
+        self._check("fc2d_b200_set_q", self.lib.fc2d_b200_set_q(self.h, _dp(q)))
+
+    def get_aux(self) -> np.ndarray:
+        out = np.zeros((self.num_patches, self.opts.maux, self.ny, self.nx), np.float64)
+        self._check("fc2d_b200_get_aux", self.lib.fc2d_b200_get_aux(self.h, _dp(out)))
+        return out
+
+    def set_aux(self, aux: np.ndarray) -> None:
+        aux = np.ascontiguousarray(aux, np.float64)
+        self._check("fc2d_b200_set_aux", self.lib.fc2d_b200_set_aux(self.h, _dp(aux)))
+
+    def get_registers(self) -> np.ndarray:
+        n = ctypes.c_int()
+        self._check("fc2d_b200_registers_size", self.lib.fc2d_b200_registers_size(self.h, ctypes.byref(n)))
+        out = np.zeros((self.num_patches, n.value), np.float64)
+        self._check("fc2d_b200_get_registers", self.lib.fc2d_b200_get_registers(self.h, _dp(out)))
+        return out
+
+    # -- stepping -------------------------------------------------------------
+    def advance(self, t: float, dt: float) -> float:
+        cfl = ctypes.c_double()
+        self._check("fc2d_b200_advance", self.lib.fc2d_b200_advance(self.h, t, dt, ctypes.byref(cfl)))
+        return cfl.value
+
+    def level_update(self, level: int, t: float, dt: float) -> float:
+        cfl = ctypes.c_double()
+        self._check("fc2d_b200_level_update", self.lib.fc2d_b200_level_update(self.h, level, t, dt, ctypes.byref(cfl)))
+        return cfl.value
+
+    def single_step_update(self, level: int, it: int, total: int, t: float, dt: float) -> float:
+        cfl = ctypes.c_double()
+        self._check("fc2d_b200_single_step_update",
+                    self.lib.fc2d_b200_single_step_update(self.h, level, it, total, t, dt, ctypes.byref(cfl)))
+        return cfl.value
+
+    def ghost_update(self, minlevel: int, maxlevel: int, t: float, time_interp: int = 0) -> None:
+        self._check("fc2d_b200_ghost_update", self.lib.fc2d_b200_ghost_update(self.h, minlevel, maxlevel, t, time_interp))
+
+    def time_sync(self, minlevel: int, maxlevel: int) -> None:
+        self._check("fc2d_b200_time_sync", self.lib.fc2d_b200_time_sync(self.h, minlevel, maxlevel))
+
+    def regrid(self) -> int:
+        c = ctypes.c_int()
+        self._check("fc2d_b200_regrid", self.lib.fc2d_b200_regrid(self.h, ctypes.byref(c)))
+        return c.value
+
+    def mass(self) -> np.ndarray:
+        out = np.zeros(self.opts.meqn, np.float64)
+        self._check("fc2d_b200_mass", self.lib.fc2d_b200_mass(self.h, _dp(out)))
+        return out
+
+    @property
+    def cell_updates(self) -> float:
+        v = ctypes.c_double()
+        self._check("fc2d_b200_cell_updates", self.lib.fc2d_b200_cell_updates(self.h, ctypes.byref(v)))
+        return v.value
+
+    def synchronize(self) -> None:
+        self._check("fc2d_b200_synchronize", self.lib.fc2d_b200_synchronize(self.h))
+
+    def set_timing(self, on: bool) -> None:
+        self._check("fc2d_b200_set_timing", self.lib.fc2d_b200_set_timing(self.h, int(on)))
+
+    def last_update_stats(self) -> dict:
+        ms, by = ctypes.c_double(), ctypes.c_double()
+        ul, tl = ctypes.c_int(), ctypes.c_int()
+        self._check("fc2d_b200_last_update_stats",
+                    self.lib.fc2d_b200_last_update_stats(self.h, ctypes.byref(ms), ctypes.byref(by),
+                                                         ctypes.byref(ul), ctypes.byref(tl)))
+        return {"update_ms": ms.value, "update_bytes": by.value, "update_launches": ul.value,
+                "total_launches": tl.value}

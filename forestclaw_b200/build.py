@@ -1,0 +1,90 @@
+"""Build recipe of libfc2d_b200.so (sm_100a), in-tree.
+
+    python -m forestclaw_b200.build [--force]
+
+Device code is compiled for sm_100a only.  The FP64 translation units
+(k_step2_f64.cu, k_amr.cu) are compiled with -fmad=false so no FMA contraction
+changes the rounding of the FP64 path; the FP32-wave unit keeps FMA.  Host C++
+is compiled with -ffp-contract=off for the same reason (patch geometry, app
+initial data).  The CUDA runtime is linked statically so the library loads on
+any machine with a driver.
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+INC = os.path.join(os.path.dirname(HERE), "include")
+OUT = os.path.join(HERE, "libfc2d_b200.so")
+BUILD = os.path.join(HERE, "_build")
+CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+NVCC = os.path.join(CUDA, "bin", "nvcc")
+GXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+CU_UNITS = {
+    "k_step2_f64.cu": ["-fmad=false"],
+    "k_amr.cu": ["-fmad=false"],
+    "k_step2_f32w.cu": [],
+}
+CPP_UNITS = ["host_forest.cpp", "host_api.cpp", "apps.cpp"]
+
+
+def _sources_digest() -> str:
+    h = hashlib.sha256()
+    for name in sorted(os.listdir(CSRC)):
+        with open(os.path.join(CSRC, name), "rb") as f:
+            h.update(name.encode())
+            h.update(f.read())
+    with open(os.path.join(INC, "fc2d_b200.h"), "rb") as f:
+        h.update(f.read())
+    with open(__file__, "rb") as f:
+        h.update(f.read())
+    return h.hexdigest()
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        raise RuntimeError("build step failed: " + os.path.basename(cmd[-1]))
+    return r
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    stamp = os.path.join(BUILD, "stamp")
+    digest = _sources_digest()
+    if not force and os.path.exists(OUT) and os.path.exists(stamp):
+        with open(stamp) as f:
+            if f.read().strip() == digest:
+                return OUT
+    objs = []
+    common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", CSRC, "-I", INC, "-lineinfo"]
+    for cu, extra in CU_UNITS.items():
+        obj = os.path.join(BUILD, cu + ".o")
+        cmd = [NVCC, *ARCH, *common, *extra, "-Xptxas", "-v" if verbose else "-O3", "-c",
+               os.path.join(CSRC, cu), "-o", obj]
+        r = _run(cmd)
+        if verbose:
+            sys.stderr.write(r.stderr)
+        objs.append(obj)
+    for cpp in CPP_UNITS:
+        obj = os.path.join(BUILD, cpp + ".o")
+        cmd = [GXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
+               "-I", CSRC, "-I", INC, "-I", os.path.join(CUDA, "include"), "-c", os.path.join(CSRC, cpp), "-o", obj]
+        _run(cmd)
+        objs.append(obj)
+    _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-Xcompiler", "-fPIC", "-o", OUT, *objs])
+    with open(stamp, "w") as f:
+        f.write(digest)
+    return OUT
+
+
+if __name__ == "__main__":
+    p = build(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    print(p)

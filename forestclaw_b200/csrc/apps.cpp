@@ -1,0 +1,118 @@
+// apps.cpp -- host-side app callbacks of the built-in problems.
+//
+//   swirl:      applications/clawpack/advection/2d/swirl/user_4.6/qinit.f, b4step2.f:25-36, psi.f:9.
+//               The time-independent part of b4step2, psi(x,y+dy)-psi(x,y) and
+//               psi(x+dx,y)-psi(x,y), is stored as aux; the fused update kernel
+//               scales it by cos(2 pi (t+dt/2)/T)/dy and -cos(...)/dx each step.
+//   radial dam: applications/clawpack/shallow/2d/radialdam/user_4.6/qinit.f with the
+//               disc test at the cell centre.
+//   tsunami:    bathymetry b = -1 + 0.5 exp(-50|x-c|^2) in aux(:,:,1), surface eta = sum of bumps.
+//   tagging:    fort_4.6/fclaw2d_clawpatch46_tag4refinement.f / _tag4coarsening.f with the
+//               gradient criterion (fort_user/fclaw2d_clawpatch_gradient_exceeds_th.f90) times dx.
+#include "apps.hpp"
+#include <cmath>
+
+namespace fcb {
+
+static inline size_t qi(const Dims& d, int i, int j, int m)
+{
+    return (size_t)(i + d.mbc - 1) + (size_t)(j + d.mbc - 1) * d.nx() + (size_t)(m - 1) * d.nxy();
+}
+
+static double swirl_psi(double x, double y, double pi)
+{
+    const double sx = std::sin(pi * x), sy = std::sin(pi * y);
+    return ((sx * sx) * (sy * sy)) / pi;
+}
+
+void app_setaux(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, double* aux)
+{
+    const int mx = d.mx, my = d.my, mbc = d.mbc;
+    if (o.app == FC2D_B200_APP_SWIRL) {
+        const double pi = 4.0 * std::atan(1.0);
+        for (int j = 1 - mbc; j <= my + mbc; j++) {
+            const double yll = P.ylower + (j - 1) * P.dy;
+            for (int i = 1 - mbc; i <= mx + mbc; i++) {
+                const double xll = P.xlower + (i - 1) * P.dx;
+                const double pij = swirl_psi(xll, yll, pi);
+                aux[qi(d, i, j, 1)] = swirl_psi(xll, yll + P.dy, pi) - pij;
+                aux[qi(d, i, j, 2)] = swirl_psi(xll + P.dx, yll, pi) - pij;
+            }
+        }
+    } else if (o.app == FC2D_B200_APP_TSUNAMI) {
+        const double cx = o.pdata[0], cy = o.pdata[1];
+        for (int j = 1 - mbc; j <= my + mbc; j++)
+            for (int i = 1 - mbc; i <= mx + mbc; i++) {
+                const double xc = P.xlower + (i - 0.5) * P.dx, yc = P.ylower + (j - 0.5) * P.dy;
+                const double r2 = (xc - cx) * (xc - cx) + (yc - cy) * (yc - cy);
+                aux[qi(d, i, j, 1)] = -1.0 + 0.5 * std::exp(-50.0 * r2);
+            }
+    }
+}
+
+void app_qinit(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, const double* aux, double* q)
+{
+    const int mx = d.mx, my = d.my, mbc = d.mbc, meqn = d.meqn;
+    if (o.app == FC2D_B200_APP_SWIRL) {
+        for (int m = 1; m <= meqn; m++)
+            for (int i = 1 - mbc; i <= mx + mbc; i++) {
+                const double xc = P.xlower + (i - 0.5) * P.dx;
+                for (int j = 1 - mbc; j <= my + mbc; j++) q[qi(d, i, j, m)] = (xc < 0.5) ? 1.0 : 0.0;
+            }
+    } else if (o.app == FC2D_B200_APP_RADIALDAM) {
+        for (int i = 1 - mbc; i <= mx + mbc; i++) {
+            const double xc = P.xlower + (i - 0.5) * P.dx;
+            for (int j = 1 - mbc; j <= my + mbc; j++) {
+                const double yc = P.ylower + (j - 0.5) * P.dy;
+                const double r2 = (xc - o.x0) * (xc - o.x0) + (yc - o.y0) * (yc - o.y0);
+                const double win = (r2 - o.r0 * o.r0 < 0.0) ? 1.0 : 0.0;
+                q[qi(d, i, j, 1)] = o.hin * win + o.hout * (1.0 - win);
+                q[qi(d, i, j, 2)] = 0.0;
+                q[qi(d, i, j, 3)] = 0.0;
+            }
+        }
+    } else if (o.app == FC2D_B200_APP_TSUNAMI) {
+        const int nb = (int)o.pdata[2];
+        for (int j = 1 - mbc; j <= my + mbc; j++)
+            for (int i = 1 - mbc; i <= mx + mbc; i++) {
+                const double xc = P.xlower + (i - 0.5) * P.dx, yc = P.ylower + (j - 0.5) * P.dy;
+                double eta = 0.0;
+                for (int k = 0; k < nb; k++) {
+                    const double A = o.pdata[3 + 4 * k], w = o.pdata[4 + 4 * k];
+                    const double bx = o.pdata[5 + 4 * k], by = o.pdata[6 + 4 * k];
+                    const double r2 = (xc - bx) * (xc - bx) + (yc - by) * (yc - by);
+                    eta = eta + A * std::exp(-r2 / (w * w));
+                }
+                q[qi(d, i, j, 1)] = eta - aux[qi(d, i, j, 1)];
+                q[qi(d, i, j, 2)] = 0.0;
+                q[qi(d, i, j, 3)] = 0.0;
+            }
+    }
+}
+
+static bool grad_exceeds(const Dims& d, const PatchInfo& P, const double* q, int i, int j, double thr)
+{
+    const double dx2 = 2 * P.dx, dy2 = 2 * P.dy;
+    const double dqx = (q[qi(d, i + 1, j, 1)] - q[qi(d, i - 1, j, 1)]) / dx2;
+    const double dqy = (q[qi(d, i, j + 1, 1)] - q[qi(d, i, j - 1, 1)]) / dy2;
+    const double ds = std::sqrt(dqx * dqx + dqy * dqy + 0.0 * 0.0);
+    return ds * P.dx > thr;
+}
+
+int app_tag_refine(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, const double* q)
+{
+    for (int j = 1; j <= d.my; j++)
+        for (int i = 1; i <= d.mx; i++)
+            if (grad_exceeds(d, P, q, i, j, o.refine_threshold)) return 1;
+    return 0;
+}
+
+int app_coarsen_ok(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, const double* q)
+{
+    for (int i = 1; i <= d.mx; i++)
+        for (int j = 1; j <= d.my; j++)
+            if (grad_exceeds(d, P, q, i, j, o.coarsen_threshold)) return 0;
+    return 1;
+}
+
+}  // namespace fcb

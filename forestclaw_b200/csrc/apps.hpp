@@ -1,0 +1,18 @@
+// apps.hpp -- host-side application callbacks of the built-in problems
+// (the qinit / setaux / tagging a ForestClaw app installs in its vtables).
+#pragma once
+#include "fc2d_b200.h"
+#include "host_forest.hpp"
+
+namespace fcb {
+
+// setaux for one patch into aux (maux*nxy doubles, Fortran layout).
+void app_setaux(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, double* aux);
+// qinit for one patch into q (meqn*nxy doubles, ghosts included).
+void app_qinit(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, const double* aux, double* q);
+// Refinement test of one patch (tag4refinement with the dx-scaled gradient criterion).
+int app_tag_refine(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, const double* q);
+// True when no interior cell exceeds the coarsening threshold (one member of tag4coarsening).
+int app_coarsen_ok(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, const double* q);
+
+}  // namespace fcb

@@ -1,0 +1,35 @@
+// fcb_common.h -- plain structs shared by the host driver and the device kernels.
+#pragma once
+#include <stdint.h>
+
+namespace fcb {
+
+// One leaf patch as seen by the device: physical lower-left corner, mesh widths,
+// refinement level and a bit mask of faces on the physical boundary
+// (bit f set <=> face f intersects the boundary, fclaw2d_physical_get_bc).
+struct PatchDesc {
+    double xlower, ylower, dx, dy;
+    int level;
+    int phys_mask;
+    int face_type;      // 2 bits per face: 0 boundary, 1 half (finer nbr), 2 same, 3 double (coarser nbr)
+    int pad;
+};
+
+// Parameters of one level update launch (clawpack46 method flags and the
+// per-step scalars the reference passes through common blocks).
+struct StepParams {
+    int order1, order2;     // method(2), method(3)
+    int mthlim[8];
+    int mcapa;
+    int store_flux;         // time_sync && flux_correction   (clawpack46_time_sync_store_flux)
+    int accumulate_waves;   // time_sync && fluctuation_correction (clawpack46_time_sync_accumulate_waves)
+    int save_last;          // fclaw2d_clawpatch_save_current_step (q -> qlast)
+    int app;                // b4step2 hook
+    double dt;
+    double t;
+    double grav;
+    double dry_tolerance;
+    double vt;              // swirl: cos(2 pi (t + dt/2) / T), computed on the host
+};
+
+}  // namespace fcb

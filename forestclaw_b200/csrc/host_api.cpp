@@ -1,0 +1,846 @@
+// host_api.cpp -- the C ABI of the B200 package and the level-stepping driver.
+//
+// The driver restates, with device launches instead of per-patch callbacks:
+//   fclaw2d_advance_all_levels / advance_level   src/fclaw2d_advance.c:54-357
+//   fclaw2d_update_single_step                   src/fclaw2d_update_single_step.c:73-103
+//   fclaw2d_ghost_update (one process)           src/fclaw2d_ghost_fill.c:611-830
+//   fclaw2d_time_sync / correct_coarse_cells     src/fclaw2d_time_sync.c:66-202
+//   fclaw2d_timeinterp                           src/fclaw2d_timeinterp.c:29-57
+//   fclaw2d_regrid / fclaw2d_initialize          src/fclaw2d_regrid.c:44-335, src/fclaw2d_initialize.c:75-250
+// All patch data stays in device memory; the host touches it only to install
+// initial data and at regrid (one flag per patch down, repopulation ops up).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+#include "apps.hpp"
+#include "fc2d_b200.h"
+#include "host_forest.hpp"
+#include "kernels.h"
+
+namespace fcb {
+cudaError_t launch_step2_f64(int rp, const Dims& d, double* q, double* qlast, const double* aux, double* regs,
+                             const PatchDesc* desc, int p0, int npatch, const StepParams& sp,
+                             unsigned long long* cfl_bits, cudaStream_t st);
+bool step2_f64_supported(int rp, int mx, int my, int mbc);
+cudaError_t launch_step2_f32w(int rp, const Dims& d, double* q, double* qlast, const double* aux, double* regs,
+                              const PatchDesc* desc, int p0, int npatch, const StepParams& sp,
+                              unsigned long long* cfl_bits, cudaStream_t st);
+bool step2_f32w_supported(int rp, int mx, int my, int mbc);
+}  // namespace fcb
+
+using namespace fcb;
+
+static thread_local std::string g_err;
+static int fail(int code, const std::string& msg) { g_err = msg; return code; }
+#define CK(call)                                                                                           \
+    do {                                                                                                   \
+        cudaError_t e_ = (call);                                                                           \
+        if (e_ != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class T>
+struct DevVec {
+    T* p = nullptr;
+    size_t n = 0, cap = 0;
+    ~DevVec() { if (p) cudaFree(p); }
+    cudaError_t assign(const std::vector<T>& v, cudaStream_t st)
+    {
+        if (v.size() > cap) {
+            if (p) cudaFree(p);
+            p = nullptr;
+            cap = v.size() + v.size() / 4 + 16;
+            cudaError_t e = cudaMalloc(&p, cap * sizeof(T));
+            if (e != cudaSuccess) { cap = 0; return e; }
+        }
+        n = v.size();
+        if (n) return cudaMemcpyAsync(p, v.data(), n * sizeof(T), cudaMemcpyHostToDevice, st);
+        return cudaSuccess;
+    }
+};
+
+struct LevelRanges {
+    int copy_off = 0, copy_n = 0, avg_off = 0, avg_n = 0, interp_off = 0, interp_n = 0, phys_off = 0, phys_n = 0;
+    int ti_off = 0, ti_n = 0, ss_off = 0, ss_start_off = 0, ss_np = 0, f2c_off = 0, f2c_start_off = 0, f2c_np = 0;
+};
+
+struct fc2d_b200_solver {
+    fc2d_b200_options_t o;
+    Dims d;
+    Forest forest;
+    cudaStream_t st = nullptr;
+    double *q = nullptr, *qlast = nullptr, *qinterp = nullptr, *aux = nullptr, *regs = nullptr;
+    PatchDesc* desc = nullptr;
+    int cap = 0;                                   // patch capacity of the slabs
+    std::vector<double> aux_host;                  // static aux mirror (level-major)
+    DevVec<CopyEnt> t_copy, t_avg;
+    DevVec<InterpEnt> t_interp;
+    DevVec<PhysEnt> t_phys;
+    DevVec<int> t_ti, t_ss_start, t_f2c_start;
+    DevVec<SyncOp> t_ss, t_f2c;
+    LevelRanges lr[33];
+    unsigned long long* cfl_dev = nullptr;
+    unsigned long long* cfl_host = nullptr;
+    double* mass_dev = nullptr;
+    int mass_cap = 0;
+    double cell_updates = 0;
+    double t_curr = 0;
+    bool initialized = false;
+    // single_step_update protocol
+    int ss_level = -1, ss_count = 0;
+    // timing
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;
+    int ev_used = 0;
+    std::vector<std::pair<int, double>> upd_launch_bytes;   // (event index, algorithmic bytes)
+    double upd_ms = 0, upd_bytes = 0;
+    int upd_launches = 0, total_launches = 0;
+};
+
+const char* fc2d_b200_last_error(void) { return g_err.c_str(); }
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+static int alloc_slabs(fc2d_b200_solver* s, int np)
+{
+    const Dims& d = s->d;
+    if (np <= s->cap && s->q) return 0;
+    int cap = np + np / 4 + 16;
+    double *q, *ql, *qi = nullptr, *aux = nullptr, *regs;
+    PatchDesc* desc;
+    CK(cudaMalloc(&q, (size_t)cap * d.nq() * sizeof(double)));
+    CK(cudaMalloc(&ql, (size_t)cap * d.nq() * sizeof(double)));
+    if (s->o.subcycle) CK(cudaMalloc(&qi, (size_t)cap * d.nq() * sizeof(double)));
+    if (d.maux > 0) CK(cudaMalloc(&aux, (size_t)cap * d.naux() * sizeof(double)));
+    CK(cudaMalloc(&regs, (size_t)cap * d.nreg() * sizeof(double)));
+    CK(cudaMalloc(&desc, (size_t)cap * sizeof(PatchDesc)));
+    CK(cudaMemsetAsync(q, 0, (size_t)cap * d.nq() * sizeof(double), s->st));
+    CK(cudaMemsetAsync(ql, 0, (size_t)cap * d.nq() * sizeof(double), s->st));
+    if (qi) CK(cudaMemsetAsync(qi, 0, (size_t)cap * d.nq() * sizeof(double), s->st));
+    CK(cudaMemsetAsync(regs, 0, (size_t)cap * d.nreg() * sizeof(double), s->st));
+    if (s->q) {
+        // caller copies what it needs before freeing; here the old slabs are released
+        cudaFree(s->q); cudaFree(s->qlast); if (s->qinterp) cudaFree(s->qinterp);
+        if (s->aux) cudaFree(s->aux); cudaFree(s->regs); cudaFree(s->desc);
+    }
+    s->q = q; s->qlast = ql; s->qinterp = qi; s->aux = aux; s->regs = regs; s->desc = desc; s->cap = cap;
+    return 0;
+}
+
+static int upload_desc_and_tables(fc2d_b200_solver* s)
+{
+    const Forest& f = s->forest;
+    std::vector<PatchDesc> hd(f.np());
+    for (int i = 0; i < f.np(); i++) {
+        const PatchInfo& P = f.p[i];
+        PatchDesc pd{};
+        pd.xlower = P.xlower; pd.ylower = P.ylower; pd.dx = P.dx; pd.dy = P.dy;
+        pd.level = P.level;
+        pd.phys_mask = (P.phys[0] ? 1 : 0) | (P.phys[1] ? 2 : 0) | (P.phys[2] ? 4 : 0) | (P.phys[3] ? 8 : 0);
+        int ft = 0;
+        for (int k = 0; k < 4; k++) ft |= (P.face_type[k] & 3) << (2 * k);
+        pd.face_type = ft;
+        hd[i] = pd;
+    }
+    if (!hd.empty()) CK(cudaMemcpyAsync(s->desc, hd.data(), hd.size() * sizeof(PatchDesc), cudaMemcpyHostToDevice, s->st));
+    std::vector<LevelTables> T;
+    build_tables(f, s->o.mthbc, T);
+    std::vector<CopyEnt> copy, avg;
+    std::vector<InterpEnt> interp;
+    std::vector<PhysEnt> phys;
+    std::vector<int> ti, ss_start, f2c_start;
+    std::vector<SyncOp> ss, f2c;
+    for (int l = 0; l < 33; l++) {
+        LevelRanges& r = s->lr[l];
+        r = LevelRanges();
+        const LevelTables& L = T[l];
+        r.copy_off = (int)copy.size(); r.copy_n = (int)L.copy.size(); copy.insert(copy.end(), L.copy.begin(), L.copy.end());
+        r.avg_off = (int)avg.size(); r.avg_n = (int)L.avg.size(); avg.insert(avg.end(), L.avg.begin(), L.avg.end());
+        r.interp_off = (int)interp.size(); r.interp_n = (int)L.interp.size();
+        interp.insert(interp.end(), L.interp.begin(), L.interp.end());
+        r.phys_off = (int)phys.size(); r.phys_n = (int)L.phys.size(); phys.insert(phys.end(), L.phys.begin(), L.phys.end());
+        r.ti_off = (int)ti.size(); r.ti_n = (int)L.ti.size(); ti.insert(ti.end(), L.ti.begin(), L.ti.end());
+        r.ss_off = (int)ss.size(); r.ss_start_off = (int)ss_start.size(); r.ss_np = (int)L.ss_start.size() - 1;
+        ss.insert(ss.end(), L.ss.begin(), L.ss.end());
+        ss_start.insert(ss_start.end(), L.ss_start.begin(), L.ss_start.end());
+        r.f2c_off = (int)f2c.size(); r.f2c_start_off = (int)f2c_start.size(); r.f2c_np = (int)L.f2c_start.size() - 1;
+        f2c.insert(f2c.end(), L.f2c.begin(), L.f2c.end());
+        f2c_start.insert(f2c_start.end(), L.f2c_start.begin(), L.f2c_start.end());
+    }
+    CK(s->t_copy.assign(copy, s->st));
+    CK(s->t_avg.assign(avg, s->st));
+    CK(s->t_interp.assign(interp, s->st));
+    CK(s->t_phys.assign(phys, s->st));
+    CK(s->t_ti.assign(ti, s->st));
+    CK(s->t_ss.assign(ss, s->st));
+    CK(s->t_ss_start.assign(ss_start, s->st));
+    CK(s->t_f2c.assign(f2c, s->st));
+    CK(s->t_f2c_start.assign(f2c_start, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+static cudaEvent_t next_event(fc2d_b200_solver* s)
+{
+    if (s->ev_used >= (int)s->ev_pool.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        s->ev_pool.push_back(e);
+    }
+    return s->ev_pool[s->ev_used++];
+}
+
+// ---------------------------------------------------------------------------
+// level operations
+// ---------------------------------------------------------------------------
+static int update_level(fc2d_b200_solver* s, int level, double t, double dt)
+{
+    const Forest& f = s->forest;
+    if (level < 0 || level > 32) return 0;
+    const int p0 = f.lev_off[level], np = f.lev_off[level + 1] - p0;
+    if (np <= 0) return 0;
+    StepParams sp{};
+    sp.order1 = s->o.order[0]; sp.order2 = s->o.order[1];
+    for (int k = 0; k < 8; k++) sp.mthlim[k] = s->o.mthlim[k];
+    sp.mcapa = s->o.mcapa;
+    sp.store_flux = s->o.time_sync && s->o.flux_correction;
+    sp.accumulate_waves = s->o.time_sync && s->o.fluctuation_correction;
+    sp.save_last = 1;
+    sp.app = s->o.app;
+    sp.dt = dt; sp.t = t; sp.grav = s->o.grav;
+    sp.dry_tolerance = s->o.pdata[31] > 0 ? s->o.pdata[31] : 1e-3;
+    sp.vt = 0.0;
+    if (s->o.app == FC2D_B200_APP_SWIRL && s->o.tperiod != 0.0) {
+        const double pi = 4.0 * std::atan(1.0), pi2 = 2.0 * pi;
+        sp.vt = std::cos(pi2 * (t + dt / 2.0) / s->o.tperiod);
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (s->timing) { e0 = next_event(s); e1 = next_event(s); CK(cudaEventRecord(e0, s->st)); }
+    cudaError_t e;
+    if (s->o.precision == FC2D_B200_PREC_FP32WAVE)
+        e = launch_step2_f32w(s->o.rp, s->d, s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, sp, s->cfl_dev, s->st);
+    else
+        e = launch_step2_f64(s->o.rp, s->d, s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, sp, s->cfl_dev, s->st);
+    if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("step2 launch: ") + cudaGetErrorString(e));
+    if (s->timing) {
+        CK(cudaEventRecord(e1, s->st));
+        const double cells = (double)np * s->d.mx * s->d.my;
+        const double bytes = cells * 8.0 * (2.0 * s->d.meqn + s->d.maux);
+        s->upd_launch_bytes.push_back({s->ev_used - 2, bytes});
+    }
+    s->upd_launches++;
+    s->total_launches++;
+    s->cell_updates += (double)np * s->d.mx * s->d.my;
+    return 0;
+}
+
+static double* tsdata(fc2d_b200_solver* s, int ti) { return ti ? s->qinterp : s->q; }
+
+static void copy2ghost(fc2d_b200_solver* s, int l, int ti)
+{
+    if (l < 0 || l > 32 || !s->lr[l].copy_n) return;
+    launch_copy(s->d, tsdata(s, ti), tsdata(s, ti), s->t_copy.p + s->lr[l].copy_off, s->lr[l].copy_n, s->st);
+    s->total_launches++;
+}
+static void average2ghost(fc2d_b200_solver* s, int l, int ti)
+{
+    if (l < 0 || l > 32 || !s->lr[l].avg_n) return;
+    launch_average(s->d, tsdata(s, ti), s->q, s->t_avg.p + s->lr[l].avg_off, s->lr[l].avg_n, s->st);
+    s->total_launches++;
+}
+static void interpolate2ghost(fc2d_b200_solver* s, int l, int ti)
+{
+    if (l < 0 || l > 32 || !s->lr[l].interp_n) return;
+    launch_interp(s->d, s->q, tsdata(s, ti), s->t_interp.p + s->lr[l].interp_off, s->lr[l].interp_n, s->st);
+    s->total_launches++;
+}
+static void setphysical(fc2d_b200_solver* s, int l, int ti)
+{
+    if (l < 0 || l > 32 || !s->lr[l].phys_n) return;
+    launch_phys(s->d, tsdata(s, ti), s->t_phys.p + s->lr[l].phys_off, s->lr[l].phys_n, s->st);
+    s->total_launches++;
+}
+
+static void ghost_update(fc2d_b200_solver* s, int minlevel, int maxlevel, int time_interp)
+{
+    const int mincoarse = minlevel, maxcoarse = maxlevel - 1;
+    for (int l = maxcoarse; l >= mincoarse; l--) average2ghost(s, l, 0);
+    if (time_interp) average2ghost(s, mincoarse - 1, 1);
+    for (int l = maxlevel; l >= minlevel; l--) copy2ghost(s, l, 0);
+    if (time_interp) copy2ghost(s, minlevel - 1, 1);
+    for (int l = maxcoarse; l >= mincoarse; l--) setphysical(s, l, 0);
+    if (time_interp) setphysical(s, mincoarse - 1, 1);
+    for (int l = maxcoarse; l >= mincoarse; l--) interpolate2ghost(s, l, 0);
+    if (time_interp) interpolate2ghost(s, mincoarse - 1, 1);
+    const int minfine = mincoarse + 1, maxfine = maxlevel;
+    for (int l = maxfine; l >= minfine; l--) setphysical(s, l, 0);
+    if (time_interp) setphysical(s, minfine - 1, 1);
+    for (int l = maxlevel; l >= minlevel; l--) setphysical(s, l, 0);
+    if (time_interp) setphysical(s, minlevel - 1, 1);
+}
+
+static void reset_level(fc2d_b200_solver* s, int coarse_level, int mode)
+{
+    const Forest& f = s->forest;
+    if (coarse_level < 0 || coarse_level > 32) return;
+    const int p0 = f.lev_off[coarse_level];
+    const int hi = (mode == 1) ? std::min(coarse_level + 2, 33) : coarse_level + 1;
+    const int np = f.lev_off[hi] - p0;
+    if (np <= 0) return;
+    launch_reset(s->d, s->regs, s->desc, p0, np, coarse_level, mode, s->st);
+    s->total_launches++;
+}
+
+static void time_sync(fc2d_b200_solver* s, int minlevel, int maxlevel)
+{
+    (void)maxlevel;
+    const int maxl = s->o.maxlevel;
+    for (int level = maxl; level >= minlevel; level--) {
+        if (level < 0 || level > 32) continue;
+        const LevelRanges& r = s->lr[level];
+        if (r.ss_np > 0) {
+            launch_samesize(s->d, s->q, s->regs, s->desc, s->t_ss.p + r.ss_off, s->t_ss_start.p + r.ss_start_off,
+                            r.ss_np, s->st);
+            s->total_launches++;
+        }
+        reset_level(s, level, 2);
+        if (level < maxl) {
+            if (r.f2c_np > 0) {
+                launch_f2c(s->d, s->q, s->regs, s->desc, s->t_f2c.p + r.f2c_off, s->t_f2c_start.p + r.f2c_start_off,
+                           r.f2c_np, s->st);
+                s->total_launches++;
+            }
+            reset_level(s, level, 1);
+        }
+    }
+    for (int level = maxl; level >= minlevel; level--) reset_level(s, level, 3);
+}
+
+static void timeinterp(fc2d_b200_solver* s, int level, double alpha)
+{
+    if (level < 0 || level > 32 || !s->lr[level].ti_n) return;
+    launch_timeinterp(s->d, s->q, s->qlast, s->qinterp, s->t_ti.p + s->lr[level].ti_off, s->lr[level].ti_n, alpha, s->st);
+    s->total_launches++;
+}
+
+struct Tsc { int last_step, step_inc, total_steps; double current_time, dt_step; };
+
+static int advance_level(fc2d_b200_solver* s, Tsc* ts, int level, int curr_fine_step)
+{
+    int rc = update_level(s, level, ts[level].current_time, ts[level].dt_step);
+    if (rc) return rc;
+    ts[level].last_step += ts[level].step_inc;
+    ts[level].current_time += ts[level].dt_step;
+    if (level > s->forest.minlevel_present) {
+        const int last_coarse_step = ts[level - 1].last_step;
+        if (last_coarse_step == curr_fine_step) {
+            rc = advance_level(s, ts, level - 1, last_coarse_step);
+            if (rc) return rc;
+            if (s->o.subcycle) {
+                const int coarse_inc = ts[level - 1].step_inc;
+                const int new_curr_step = ts[level].last_step;
+                const double alpha = ((double)(new_curr_step % coarse_inc)) / coarse_inc;
+                timeinterp(s, level - 1, alpha);
+            }
+        }
+    }
+    return 0;
+}
+
+static double bits_to_double(unsigned long long b)
+{
+    double v;
+    std::memcpy(&v, &b, sizeof(v));
+    return v;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver_t** out)
+{
+    if (!opt || !out) return fail(FC2D_B200_EINVAL, "null argument");
+    const fc2d_b200_options_t& o = *opt;
+    if (o.mx <= 0 || o.my <= 0 || o.mbc < 2 || o.meqn <= 0 || o.meqn > 8 || o.maux < 0 || o.mwaves <= 0)
+        return fail(FC2D_B200_EINVAL, "bad patch dimensions (need mx,my>0, mbc>=2, 0<meqn<=8)");
+    if ((o.mx % 2) || (o.my % 2)) return fail(FC2D_B200_EINVAL, "mx and my must be even");
+    if (o.time_sync && o.rp == FC2D_B200_RP_ADVECTION)
+        return fail(FC2D_B200_EINVAL, "time sync needs a shallow-water flux function (rpn2_cons)");
+    if (o.minlevel < 0 || o.maxlevel < o.minlevel || o.maxlevel > 20)
+        return fail(FC2D_B200_EINVAL, "bad minlevel/maxlevel");
+    const bool sup = (o.precision == FC2D_B200_PREC_FP32WAVE) ? step2_f32w_supported(o.rp, o.mx, o.my, o.mbc)
+                                                              : step2_f64_supported(o.rp, o.mx, o.my, o.mbc);
+    if (!sup) return fail(FC2D_B200_EINVAL, "no compiled update kernel for this (rp, mx, my, mbc, precision)");
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev));
+    if (ndev <= 0) return fail(FC2D_B200_ECUDA, "no CUDA device");
+    CK(cudaSetDevice(o.device));
+    auto s = std::make_unique<fc2d_b200_solver>();
+    s->o = o;
+    if (s->o.mi <= 0) s->o.mi = 1;
+    if (s->o.mj <= 0) s->o.mj = 1;
+    s->d = Dims{o.mx, o.my, o.mbc, o.meqn, o.maux};
+    s->forest.g = Geometry{s->d, s->o.mi, s->o.mj, o.ax, o.bx, o.ay, o.by};
+    CK(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+    CK(cudaMalloc(&s->cfl_dev, sizeof(unsigned long long)));
+    CK(cudaMallocHost(&s->cfl_host, sizeof(unsigned long long)));
+    *out = s.release();
+    return 0;
+}
+
+extern "C" int fc2d_b200_destroy(fc2d_b200_solver_t* s)
+{
+    if (!s) return 0;
+    cudaStreamSynchronize(s->st);
+    for (auto e : s->ev_pool) cudaEventDestroy(e);
+    cudaFree(s->q); cudaFree(s->qlast); if (s->qinterp) cudaFree(s->qinterp);
+    if (s->aux) cudaFree(s->aux); cudaFree(s->regs); cudaFree(s->desc);
+    cudaFree(s->cfl_dev); cudaFreeHost(s->cfl_host);
+    if (s->mass_dev) cudaFree(s->mass_dev);
+    cudaStreamDestroy(s->st);
+    delete s;
+    return 0;
+}
+
+extern "C" int fc2d_b200_set_riemann(fc2d_b200_solver_t* s, int rp_id)
+{
+    if (!s) return fail(FC2D_B200_EINVAL, "null solver");
+    const bool sup = (s->o.precision == FC2D_B200_PREC_FP32WAVE) ? step2_f32w_supported(rp_id, s->o.mx, s->o.my, s->o.mbc)
+                                                                 : step2_f64_supported(rp_id, s->o.mx, s->o.my, s->o.mbc);
+    if (!sup) return fail(FC2D_B200_EINVAL, "Riemann solver id not compiled for these patch dimensions");
+    s->o.rp = rp_id;
+    return 0;
+}
+
+// Install a new forest: slabs sized, descriptors and tables uploaded; data zero.
+static int install_forest(fc2d_b200_solver* s, const std::vector<Leaf>& leaves)
+{
+    std::string err;
+    Forest nf;
+    nf.g = s->forest.g;
+    if (!nf.build(leaves, err)) return fail(FC2D_B200_EFOREST, err);
+    s->forest = std::move(nf);
+    int rc = alloc_slabs(s, s->forest.np());
+    if (rc) return rc;
+    return upload_desc_and_tables(s);
+}
+
+extern "C" int fc2d_b200_set_forest(fc2d_b200_solver_t* s, int np, const int* level, const int* gx, const int* gy)
+{
+    if (!s || np <= 0 || !level || !gx || !gy) return fail(FC2D_B200_EINVAL, "bad forest arguments");
+    std::vector<Leaf> L(np);
+    for (int i = 0; i < np; i++) L[i] = {level[i], gx[i], gy[i]};
+    int rc = install_forest(s, L);
+    if (rc) return rc;
+    if (s->d.maux > 0) s->aux_host.assign((size_t)np * s->d.naux(), 0.0);
+    s->initialized = true;
+    return 0;
+}
+
+extern "C" int fc2d_b200_initialize(fc2d_b200_solver_t* s)
+{
+    if (!s) return fail(FC2D_B200_EINVAL, "null solver");
+    if (s->o.app == FC2D_B200_APP_NONE) return fail(FC2D_B200_EINVAL, "initialize needs a built-in app");
+    const Dims& d = s->d;
+    const int l0 = s->o.minlevel;
+    std::vector<Leaf> leaves;
+    for (int y = 0; y < (s->o.mj << l0); y++)
+        for (int x = 0; x < (s->o.mi << l0); x++) leaves.push_back({l0, x, y});
+    std::string err;
+    Forest f;
+    f.g = s->forest.g;
+    if (!f.build(leaves, err)) return fail(FC2D_B200_EFOREST, err);
+    std::vector<double> q((size_t)f.np() * d.nq(), 0.0), aux((size_t)f.np() * d.naux(), 0.0);
+    for (int i = 0; i < f.np(); i++) {
+        if (d.maux > 0) app_setaux(s->o, d, f.p[i], &aux[(size_t)i * d.naux()]);
+        app_qinit(s->o, d, f.p[i], d.maux > 0 ? &aux[(size_t)i * d.naux()] : nullptr, &q[(size_t)i * d.nq()]);
+    }
+    // initial refinement (fclaw2d_initialize.c:150-230): tag with init_flag, new patches get qinit
+    if (s->o.minlevel < s->o.maxlevel) {
+        for (int lev = s->o.minlevel; lev <= s->o.maxlevel; lev++) {
+            std::vector<int> mark(f.np(), 0);
+            for (int i = 0; i < f.np(); i++)
+                if (f.p[i].level < s->o.maxlevel && app_tag_refine(s->o, d, f.p[i], &q[(size_t)i * d.nq()])) mark[i] = 1;
+            int changed = 0;
+            std::vector<Leaf> L = adapt_leaves(f, mark, changed, err);
+            if (!changed) break;
+            Forest nf;
+            nf.g = f.g;
+            if (!nf.build(L, err)) return fail(FC2D_B200_EFOREST, err);
+            std::vector<double> nq((size_t)nf.np() * d.nq(), 0.0), naux((size_t)nf.np() * d.naux(), 0.0);
+            for (int i = 0; i < nf.np(); i++) {
+                const PatchInfo& P = nf.p[i];
+                const int old = f.lookup(P.level, P.gx, P.gy);
+                if (old >= 0) {
+                    std::memcpy(&nq[(size_t)i * d.nq()], &q[(size_t)old * d.nq()], sizeof(double) * d.nq());
+                    if (d.maux > 0) std::memcpy(&naux[(size_t)i * d.naux()], &aux[(size_t)old * d.naux()], sizeof(double) * d.naux());
+                } else {
+                    if (d.maux > 0) app_setaux(s->o, d, P, &naux[(size_t)i * d.naux()]);
+                    app_qinit(s->o, d, P, d.maux > 0 ? &naux[(size_t)i * d.naux()] : nullptr, &nq[(size_t)i * d.nq()]);
+                }
+            }
+            f = std::move(nf);
+            q.swap(nq); aux.swap(naux);
+        }
+    }
+    std::vector<Leaf> L;
+    for (const auto& P : f.p) L.push_back({P.level, P.gx, P.gy});
+    int rc = install_forest(s, L);
+    if (rc) return rc;
+    // install_forest sorted identically (same keys) -> same slot order as f
+    CK(cudaMemcpyAsync(s->q, q.data(), q.size() * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    if (d.maux > 0) CK(cudaMemcpyAsync(s->aux, aux.data(), aux.size() * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    s->aux_host.swap(aux);
+    s->t_curr = 0;
+    s->initialized = true;
+    return 0;
+}
+
+extern "C" int fc2d_b200_num_patches(const fc2d_b200_solver_t* s, int* np)
+{
+    if (!s || !np) return fail(FC2D_B200_EINVAL, "null argument");
+    *np = s->forest.np();
+    return 0;
+}
+
+extern "C" int fc2d_b200_patch_info(const fc2d_b200_solver_t* s, int* level, int* block, int* gx, int* gy)
+{
+    if (!s) return fail(FC2D_B200_EINVAL, "null solver");
+    for (int i = 0; i < s->forest.np(); i++) {
+        const PatchInfo& P = s->forest.p[i];
+        if (level) level[i] = P.level;
+        if (block) block[i] = P.block;
+        if (gx) gx[i] = P.gx;
+        if (gy) gy[i] = P.gy;
+    }
+    return 0;
+}
+
+extern "C" int fc2d_b200_get_q(fc2d_b200_solver_t* s, double* q)
+{
+    if (!s || !q) return fail(FC2D_B200_EINVAL, "null argument");
+    CK(cudaMemcpyAsync(q, s->q, (size_t)s->forest.np() * s->d.nq() * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+extern "C" int fc2d_b200_set_q(fc2d_b200_solver_t* s, const double* q)
+{
+    if (!s || !q) return fail(FC2D_B200_EINVAL, "null argument");
+    CK(cudaMemcpyAsync(s->q, q, (size_t)s->forest.np() * s->d.nq() * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+extern "C" int fc2d_b200_get_aux(fc2d_b200_solver_t* s, double* aux)
+{
+    if (!s || !aux) return fail(FC2D_B200_EINVAL, "null argument");
+    if (s->d.maux == 0) return 0;
+    CK(cudaMemcpyAsync(aux, s->aux, (size_t)s->forest.np() * s->d.naux() * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+extern "C" int fc2d_b200_set_aux(fc2d_b200_solver_t* s, const double* aux)
+{
+    if (!s || !aux) return fail(FC2D_B200_EINVAL, "null argument");
+    if (s->d.maux == 0) return 0;
+    const size_t n = (size_t)s->forest.np() * s->d.naux();
+    s->aux_host.assign(aux, aux + n);
+    CK(cudaMemcpyAsync(s->aux, aux, n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+extern "C" int fc2d_b200_registers_size(const fc2d_b200_solver_t* s, int* n)
+{
+    if (!s || !n) return fail(FC2D_B200_EINVAL, "null argument");
+    *n = s->d.nreg();
+    return 0;
+}
+
+extern "C" int fc2d_b200_get_registers(fc2d_b200_solver_t* s, double* r)
+{
+    if (!s || !r) return fail(FC2D_B200_EINVAL, "null argument");
+    CK(cudaMemcpyAsync(r, s->regs, (size_t)s->forest.np() * s->d.nreg() * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+static int begin_cfl(fc2d_b200_solver* s)
+{
+    CK(cudaMemsetAsync(s->cfl_dev, 0, sizeof(unsigned long long), s->st));
+    return 0;
+}
+
+static int end_cfl(fc2d_b200_solver* s, double* cfl)
+{
+    CK(cudaMemcpyAsync(s->cfl_host, s->cfl_dev, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    const double v = bits_to_double(*s->cfl_host);
+    if (cfl) *cfl = v;
+    if (!(v == v)) return fail(FC2D_B200_EDEVICE, "non-finite CFL (negative depth or NaN in the update)");
+    return 0;
+}
+
+extern "C" int fc2d_b200_level_update(fc2d_b200_solver_t* s, int level, double t, double dt, double* cfl)
+{
+    if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
+    int rc = begin_cfl(s);
+    if (rc) return rc;
+    rc = update_level(s, level, t, dt);
+    if (rc) return rc;
+    return end_cfl(s, cfl);
+}
+
+extern "C" int fc2d_b200_single_step_update(fc2d_b200_solver_t* s, int level, int iter, int total_count, double t,
+                                            double dt, double* cfl)
+{
+    if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
+    if (iter == 0) { s->ss_level = level; s->ss_count = 0; }
+    if (level != s->ss_level || iter != s->ss_count) return fail(FC2D_B200_ESTATE, "single_step_update calls out of order");
+    s->ss_count++;
+    if (cfl) *cfl = 0.0;
+    if (iter + 1 < total_count) return 0;
+    const int np = s->forest.lev_off[level + 1] - s->forest.lev_off[level];
+    if (total_count != np) return fail(FC2D_B200_ESTATE, "total_count differs from the patch count of the level");
+    s->ss_level = -1;
+    return fc2d_b200_level_update(s, level, t, dt, cfl);
+}
+
+extern "C" int fc2d_b200_ghost_update(fc2d_b200_solver_t* s, int minlevel, int maxlevel, double sync_time, int time_interp)
+{
+    (void)sync_time;
+    if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
+    if (time_interp && !s->qinterp) return fail(FC2D_B200_EINVAL, "time interpolation needs subcycle");
+    ghost_update(s, minlevel, maxlevel, time_interp);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+extern "C" int fc2d_b200_timeinterp(fc2d_b200_solver_t* s, int level, double alpha)
+{
+    if (!s || !s->initialized || !s->qinterp) return fail(FC2D_B200_ESTATE, "time interpolation needs subcycle");
+    timeinterp(s, level, alpha);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+extern "C" int fc2d_b200_time_sync(fc2d_b200_solver_t* s, int minlevel, int maxlevel)
+{
+    if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
+    time_sync(s, minlevel, maxlevel);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+extern "C" int fc2d_b200_advance(fc2d_b200_solver_t* s, double t, double dt, double* maxcfl)
+{
+    if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
+    const fc2d_b200_options_t& o = s->o;
+    Tsc ts[34];
+    std::memset(ts, 0, sizeof(ts));
+    const int minlevel = s->forest.minlevel_present, maxlevel = s->forest.maxlevel_present;
+    for (int l = o.minlevel; l <= o.maxlevel; l++) { ts[l].last_step = 0; ts[l].current_time = t; }
+    if (o.subcycle) {
+        double dt_level = dt;
+        int steps_inc = 1 << (maxlevel - o.minlevel);
+        int total = 1;
+        for (int l = o.minlevel; l <= o.maxlevel; l++) {
+            ts[l].dt_step = dt_level; ts[l].total_steps = total; ts[l].step_inc = steps_inc;
+            dt_level /= 2; steps_inc /= 2; total *= 2;
+        }
+    } else {
+        const int rf = 1 << (o.maxlevel - o.minlevel);
+        for (int l = o.minlevel; l <= o.maxlevel; l++) { ts[l].step_inc = 1; ts[l].dt_step = dt / rf; ts[l].total_steps = rf; }
+    }
+    s->ev_used = 0;
+    s->upd_launch_bytes.clear();
+    s->upd_launches = 0;
+    s->total_launches = 0;
+    int rc = begin_cfl(s);
+    if (rc) return rc;
+    const int nfine = ts[maxlevel].total_steps;
+    for (int nf = 0; nf < nfine; nf++) {
+        rc = advance_level(s, ts, maxlevel, nf);
+        if (rc) return rc;
+        if (ts[maxlevel].last_step < ts[maxlevel].total_steps) {
+            if (o.subcycle) {
+                int ti = maxlevel - 1;
+                while (ts[maxlevel].last_step % ts[ti].step_inc == 0) ti--;
+                ghost_update(s, ti + 1, maxlevel, 1);
+                if (o.time_sync) time_sync(s, ti + 1, maxlevel);
+            } else {
+                ghost_update(s, minlevel, maxlevel, 0);
+                if (o.time_sync) time_sync(s, minlevel, maxlevel);
+            }
+        }
+    }
+    ghost_update(s, minlevel, maxlevel, 0);
+    if (o.time_sync) time_sync(s, minlevel, maxlevel);
+    CK(cudaGetLastError());
+    rc = end_cfl(s, maxcfl);
+    if (s->timing) {
+        double ms = 0, bytes = 0;
+        for (auto& pr : s->upd_launch_bytes) {
+            float m = 0;
+            CK(cudaEventElapsedTime(&m, s->ev_pool[pr.first], s->ev_pool[pr.first + 1]));
+            ms += m;
+            bytes += pr.second;
+        }
+        s->upd_ms = ms;
+        s->upd_bytes = bytes;
+    }
+    s->t_curr = t + dt;
+    return rc;
+}
+
+extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
+{
+    if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
+    const Dims& d = s->d;
+    const Forest& f = s->forest;
+    const int np = f.np();
+    int* flags_dev;
+    CK(cudaMalloc(&flags_dev, sizeof(int) * (size_t)np));
+    launch_tag(d, s->q, s->desc, np, s->o.refine_threshold, s->o.coarsen_threshold, flags_dev, s->st);
+    std::vector<int> flags(np);
+    CK(cudaMemcpyAsync(flags.data(), flags_dev, sizeof(int) * (size_t)np, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    cudaFree(flags_dev);
+    // cb_regrid_tag4coarsening (families) then cb_fclaw2d_regrid_tag4refinement
+    std::vector<int> mark(np, 0);
+    for (int i = 0; i < np; i++) {
+        const PatchInfo& P = f.p[i];
+        if (P.level <= s->o.minlevel || (P.gx & 1) || (P.gy & 1)) continue;
+        int sib[4]; bool ok = true;
+        for (int k = 0; k < 4; k++) {
+            sib[k] = f.lookup(P.level, P.gx + (k & 1), P.gy + (k >> 1));
+            if (sib[k] < 0) { ok = false; break; }
+        }
+        if (!ok) continue;
+        bool coarsen = true;
+        for (int k = 0; k < 4; k++) if (!(flags[sib[k]] & 2)) coarsen = false;
+        if (coarsen) for (int k = 0; k < 4; k++) mark[sib[k]] = -1;
+    }
+    for (int i = 0; i < np; i++)
+        if (f.p[i].level < s->o.maxlevel && (flags[i] & 1)) mark[i] = 1;
+    int changed = 0;
+    std::string err;
+    std::vector<Leaf> L = adapt_leaves(f, mark, changed, err);
+    if (changed_out) *changed_out = changed;
+    if (!changed) return 0;
+    Forest nf;
+    nf.g = f.g;
+    if (!nf.build(L, err)) return fail(FC2D_B200_EFOREST, err);
+    // repopulation ops (cb_fclaw2d_regrid_repopulate)
+    std::vector<RepopOp> ops(nf.np());
+    std::vector<double> naux((size_t)nf.np() * d.naux(), 0.0);
+    for (int i = 0; i < nf.np(); i++) {
+        const PatchInfo& P = nf.p[i];
+        RepopOp op{};
+        op.dst = i;
+        const int old = f.lookup(P.level, P.gx, P.gy);
+        if (old >= 0) {
+            op.kind = 0; op.src = old;
+            if (d.maux > 0) std::memcpy(&naux[(size_t)i * d.naux()], &s->aux_host[(size_t)old * d.naux()], sizeof(double) * d.naux());
+        } else {
+            const int parent = f.lookup(P.level - 1, P.gx >> 1, P.gy >> 1);
+            if (parent >= 0) { op.kind = 1; op.src = parent; op.igrid = (P.gx & 1) + 2 * (P.gy & 1); }
+            else {
+                op.kind = 2;
+                for (int c = 0; c < 4; c++) {
+                    op.child[c] = f.lookup(P.level + 1, 2 * P.gx + (c & 1), 2 * P.gy + (c >> 1));
+                    if (op.child[c] < 0) return fail(FC2D_B200_EFOREST, "adapt jumped more than one level");
+                }
+            }
+            if (d.maux > 0) app_setaux(s->o, d, P, &naux[(size_t)i * d.naux()]);
+        }
+        ops[i] = op;
+    }
+    // new slabs; the old ones are read by the repopulation kernel, then freed
+    double *oq = s->q, *oql = s->qlast, *oqi = s->qinterp, *oaux = s->aux, *oregs = s->regs;
+    PatchDesc* odesc = s->desc;
+    s->q = nullptr; s->cap = 0;
+    s->qlast = nullptr; s->qinterp = nullptr; s->aux = nullptr; s->regs = nullptr; s->desc = nullptr;
+    int rc = alloc_slabs(s, nf.np());
+    if (rc) return rc;
+    RepopOp* ops_dev;
+    CK(cudaMalloc(&ops_dev, sizeof(RepopOp) * ops.size()));
+    CK(cudaMemcpyAsync(ops_dev, ops.data(), sizeof(RepopOp) * ops.size(), cudaMemcpyHostToDevice, s->st));
+    launch_repop(d, ops_dev, (int)ops.size(), oq, s->q, oql, s->qlast, oqi, s->qinterp, oregs, s->regs, s->st);
+    if (d.maux > 0) CK(cudaMemcpyAsync(s->aux, naux.data(), naux.size() * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    cudaFree(ops_dev);
+    cudaFree(oq); cudaFree(oql); if (oqi) cudaFree(oqi); if (oaux) cudaFree(oaux); cudaFree(oregs); cudaFree(odesc);
+    s->aux_host.swap(naux);
+    s->forest = std::move(nf);
+    rc = upload_desc_and_tables(s);
+    if (rc) return rc;
+    ghost_update(s, s->forest.minlevel_present, s->forest.maxlevel_present, 0);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+extern "C" int fc2d_b200_mass(fc2d_b200_solver_t* s, double* out)
+{
+    if (!s || !out || !s->initialized) return fail(FC2D_B200_EINVAL, "bad arguments");
+    const int np = s->forest.np(), meqn = s->d.meqn;
+    if (np * meqn > s->mass_cap) {
+        if (s->mass_dev) cudaFree(s->mass_dev);
+        s->mass_cap = np * meqn + 1024;
+        CK(cudaMalloc(&s->mass_dev, sizeof(double) * (size_t)s->mass_cap));
+    }
+    launch_patch_mass(s->d, s->q, s->desc, np, s->mass_dev, s->st);
+    std::vector<double> pm((size_t)np * meqn);
+    CK(cudaMemcpyAsync(pm.data(), s->mass_dev, sizeof(double) * pm.size(), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    for (int m = 0; m < meqn; m++) {
+        double sum = 0.0, comp = 0.0;
+        for (int p = 0; p < np; p++) {
+            const double y = pm[(size_t)p * meqn + m] - comp;
+            const double t = sum + y;
+            comp = (t - sum) - y;
+            sum = t;
+        }
+        out[m] = sum;
+    }
+    return 0;
+}
+
+extern "C" int fc2d_b200_cell_updates(const fc2d_b200_solver_t* s, double* out)
+{
+    if (!s || !out) return fail(FC2D_B200_EINVAL, "null argument");
+    *out = s->cell_updates;
+    return 0;
+}
+
+extern "C" int fc2d_b200_synchronize(fc2d_b200_solver_t* s)
+{
+    if (!s) return fail(FC2D_B200_EINVAL, "null solver");
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+extern "C" int fc2d_b200_last_update_stats(const fc2d_b200_solver_t* s, double* update_ms, double* update_bytes,
+                                           int* update_launches, int* total_launches)
+{
+    if (!s) return fail(FC2D_B200_EINVAL, "null solver");
+    if (update_ms) *update_ms = s->upd_ms;
+    if (update_bytes) *update_bytes = s->upd_bytes;
+    if (update_launches) *update_launches = s->upd_launches;
+    if (total_launches) *total_launches = s->total_launches;
+    return 0;
+}
+
+extern "C" int fc2d_b200_set_timing(fc2d_b200_solver_t* s, int enable)
+{
+    if (!s) return fail(FC2D_B200_EINVAL, "null solver");
+    s->timing = enable != 0;
+    return 0;
+}

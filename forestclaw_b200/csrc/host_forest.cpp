@@ -1,0 +1,477 @@
+// host_forest.cpp -- forest, neighbour relations, adaptation and gather tables.
+//
+// Neighbour semantics restate p4est's on a 2:1 face+corner balanced forest as
+// ForestClaw consumes them (src/fclaw2d_regrid.c:337-400, src/fclaw2d_patch.c:980-1034,
+// src/fclaw2d_corner_neighbors.c:80-300).  The gather tables replay, index by
+// index, the reference's ghost-fill callbacks
+//   copy2ghost / average2ghost / interpolate2ghost / setphysical  (src/fclaw2d_ghost_fill.c:140-295)
+//   cb_face_fill / cb_corner_fill                                  (src/fclaw2d_face_neighbors.c:195-450,
+//                                                                   src/fclaw2d_corner_neighbors.c:301-535)
+//   fort_4.6 copy / average / interpolate, clawpack46_bc2_default.f
+// with the same-orientation transforms of src/forestclaw2d.c:609-1360 (a shift
+// in brick-global cell indices, canonical child order).
+#include "host_forest.hpp"
+#include <algorithm>
+#include <cstdio>
+#include <map>
+
+namespace fcb {
+
+static uint64_t interleave(uint32_t x, uint32_t y)
+{
+    uint64_t r = 0;
+    for (int b = 0; b < 32; b++) {
+        r |= (uint64_t)((x >> b) & 1u) << (2 * b);
+        r |= (uint64_t)((y >> b) & 1u) << (2 * b + 1);
+    }
+    return r;
+}
+
+// p4est brick tree numbering: rank of the block position in Morton order.
+static int brick_block(int mi, int mj, int bx, int by)
+{
+    uint64_t k = interleave((uint32_t)bx, (uint32_t)by);
+    int r = 0;
+    for (int j = 0; j < mj; j++)
+        for (int i = 0; i < mi; i++)
+            if (interleave((uint32_t)i, (uint32_t)j) < k) r++;
+    return r;
+}
+
+// clawpatch_define geometry (fclaw2d_clawpatch.cpp:232-301, non-manifold, brick map
+// fclaw2d_map_brick.c:68-77).
+void Forest::geometry(PatchInfo& q) const
+{
+    const int l = q.level;
+    const int bx = q.gx >> l, by = q.gy >> l;
+    const int ix = q.gx - (bx << l), iy = q.gy - (by << l);
+    const double w = 1.0 / (double)(1 << l);
+    const double xl = ix * w, yl = iy * w, xu = (ix + 1) * w, yu = (iy + 1) * w;
+    double xlo, ylo, xup, yup;
+    if (g.mi == 1 && g.mj == 1) { xlo = xl; ylo = yl; xup = xu; yup = yu; }
+    else {
+        xlo = (double)(bx + xl) / g.mi; xup = (double)(bx + xu) / g.mi;
+        ylo = (double)(by + yl) / g.mj; yup = (double)(by + yu) / g.mj;
+    }
+    q.block = brick_block(g.mi, g.mj, bx, by);
+    q.xlower = g.ax + (g.bx - g.ax) * xlo;
+    const double xupper = g.ax + (g.bx - g.ax) * xup;
+    q.ylower = g.ay + (g.by - g.ay) * ylo;
+    const double yupper = g.ay + (g.by - g.ay) * yup;
+    q.dx = (xupper - q.xlower) / g.d.mx;
+    q.dy = (yupper - q.ylower) / g.d.my;
+    const unsigned sh = (unsigned)(24 - l);
+    q.morton = interleave((uint32_t)ix << sh, (uint32_t)iy << sh);
+}
+
+int Forest::lookup(int l, int x, int y) const
+{
+    if (l < 0 || !in_domain(l, x, y)) return -1;
+    auto it = index_.find(key(l, x, y));
+    return it == index_.end() ? -1 : it->second;
+}
+
+bool Forest::build(const std::vector<Leaf>& leaves, std::string& err)
+{
+    p.clear();
+    p.reserve(leaves.size());
+    for (const Leaf& lf : leaves) {
+        PatchInfo q{};
+        q.level = lf.level; q.gx = lf.gx; q.gy = lf.gy;
+        geometry(q);
+        p.push_back(q);
+    }
+    std::sort(p.begin(), p.end(), [](const PatchInfo& a, const PatchInfo& b) {
+        if (a.level != b.level) return a.level < b.level;
+        if (a.block != b.block) return a.block < b.block;
+        return a.morton < b.morton;
+    });
+    index_.clear();
+    index_.reserve(p.size() * 2);
+    for (int i = 0; i < np(); i++) index_[key(p[i].level, p[i].gx, p[i].gy)] = i;
+    for (int l = 0; l < 34; l++) lev_off[l] = 0;
+    minlevel_present = 99; maxlevel_present = -1;
+    {
+        int k = 0;
+        for (int l = 0; l < 33; l++) {
+            lev_off[l] = k;
+            while (k < np() && p[k].level == l) k++;
+            if (lev_off[l] != k) { minlevel_present = std::min(minlevel_present, l); maxlevel_present = l; }
+        }
+        lev_off[33] = k;
+    }
+    static const int FDX[4] = {-1, 1, 0, 0}, FDY[4] = {0, 0, -1, 1};
+    for (int ip = 0; ip < np(); ip++) {
+        PatchInfo& P = p[ip];
+        const int l = P.level;
+        P.has_fine_nbr = 0; P.on_cf = 0;
+        for (int f = 0; f < 4; f++) {
+            const int nx = P.gx + FDX[f], ny = P.gy + FDY[f];
+            P.face_nbr[f][0] = P.face_nbr[f][1] = -1;
+            P.phys[f] = !in_domain(l, nx, ny);
+            if (P.phys[f]) { P.face_type[f] = NB_BOUNDARY; continue; }
+            int k = lookup(l, nx, ny);
+            if (k >= 0) { P.face_type[f] = NB_SAME; P.face_nbr[f][0] = k; continue; }
+            k = lookup(l - 1, nx >> 1, ny >> 1);
+            if (k >= 0) { P.face_type[f] = NB_DOUBLE; P.face_nbr[f][0] = k; P.on_cf = 1; continue; }
+            int c0x, c0y, c1x, c1y;
+            if (f == 0) { c0x = 2 * nx + 1; c0y = 2 * ny; c1x = c0x; c1y = 2 * ny + 1; }
+            else if (f == 1) { c0x = 2 * nx; c0y = 2 * ny; c1x = c0x; c1y = 2 * ny + 1; }
+            else if (f == 2) { c0x = 2 * nx; c0y = 2 * ny + 1; c1x = 2 * nx + 1; c1y = c0y; }
+            else { c0x = 2 * nx; c0y = 2 * ny; c1x = 2 * nx + 1; c1y = c0y; }
+            const int a = lookup(l + 1, c0x, c0y), b = lookup(l + 1, c1x, c1y);
+            if (a < 0 || b < 0) { err = "forest is not 2:1 face balanced"; return false; }
+            P.face_type[f] = NB_HALF; P.face_nbr[f][0] = a; P.face_nbr[f][1] = b;
+            P.has_fine_nbr = 1; P.on_cf = 1;
+        }
+        for (int c = 0; c < 4; c++) {
+            const int f0 = (c & 1) ? 1 : 0, f1 = (c & 2) ? 3 : 2;
+            P.has_corner[c] = 0; P.corner_nbr[c] = -1; P.corner_type[c] = NB_BOUNDARY;
+            if (P.phys[f0] || P.phys[f1]) continue;            // not an interior corner
+            const int ddx = (c & 1) ? 1 : -1, ddy = (c & 2) ? 1 : -1;
+            const int nx = P.gx + ddx, ny = P.gy + ddy;
+            int k = lookup(l, nx, ny);
+            if (k >= 0) { P.has_corner[c] = 1; P.corner_type[c] = NB_SAME; P.corner_nbr[c] = k; continue; }
+            k = lookup(l + 1, 2 * nx + (ddx < 0), 2 * ny + (ddy < 0));
+            if (k >= 0) {
+                P.has_corner[c] = 1; P.corner_type[c] = NB_HALF; P.corner_nbr[c] = k;
+                P.has_fine_nbr = 1; P.on_cf = 1; continue;
+            }
+            k = lookup(l - 1, nx >> 1, ny >> 1);
+            const int cx = P.gx + (c & 1), cy = P.gy + (c >> 1);
+            if (k >= 0 && (cx % 2) == 0 && (cy % 2) == 0) {   // corner point is a corner of the big leaf
+                P.has_corner[c] = 1; P.corner_type[c] = NB_DOUBLE; P.corner_nbr[c] = k; P.on_cf = 1;
+            }
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// adaptation
+// ---------------------------------------------------------------------------
+std::vector<Leaf> adapt_leaves(const Forest& f, const std::vector<int>& mark, int& changed, std::string& err)
+{
+    const int np = f.np();
+    std::vector<Leaf> L;
+    L.reserve(np * 2 + 8);
+    std::vector<char> done(np, 0);
+    changed = 0;
+    for (int i = 0; i < np; i++) {
+        if (done[i]) continue;
+        const PatchInfo& P = f.p[i];
+        if (mark[i] > 0) {
+            for (int c = 0; c < 4; c++) L.push_back({P.level + 1, 2 * P.gx + (c & 1), 2 * P.gy + (c >> 1)});
+            changed = 1; done[i] = 1;
+        } else if (mark[i] < 0) {
+            const int px = P.gx >> 1, py = P.gy >> 1, l = P.level;
+            int sib[4]; bool ok = true;
+            for (int c = 0; c < 4; c++) {
+                sib[c] = f.lookup(l, 2 * px + (c & 1), 2 * py + (c >> 1));
+                if (sib[c] < 0 || mark[sib[c]] >= 0) ok = false;
+            }
+            if (ok) {
+                L.push_back({l - 1, px, py});
+                for (int c = 0; c < 4; c++) done[sib[c]] = 1;
+                changed = 1;
+            } else {
+                L.push_back({l, P.gx, P.gy}); done[i] = 1;
+            }
+        } else {
+            L.push_back({P.level, P.gx, P.gy}); done[i] = 1;
+        }
+    }
+    // 2:1 face+corner balance by refining the coarser side
+    for (;;) {
+        std::unordered_map<uint64_t, int> idx;
+        idx.reserve(L.size() * 2);
+        auto key = [](int l, int x, int y) { return ((uint64_t)l << 56) | ((uint64_t)x << 28) | (uint64_t)y; };
+        for (int i = 0; i < (int)L.size(); i++) idx[key(L[i].level, L[i].gx, L[i].gy)] = i;
+        std::vector<char> ref(L.size(), 0);
+        bool any = false;
+        for (int i = 0; i < (int)L.size(); i++) {
+            const int l = L[i].level;
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    if (!dx && !dy) continue;
+                    const int x = L[i].gx + dx, y = L[i].gy + dy;
+                    if (!f.in_domain(l, x, y)) continue;
+                    for (int k = l - 2; k >= 0; k--) {
+                        auto it = idx.find(key(k, x >> (l - k), y >> (l - k)));
+                        if (it != idx.end()) {
+                            if (!ref[it->second]) { ref[it->second] = 1; any = true; }
+                            break;
+                        }
+                    }
+                }
+        }
+        if (!any) break;
+        std::vector<Leaf> M;
+        M.reserve(L.size() + 64);
+        for (int i = 0; i < (int)L.size(); i++) {
+            if (!ref[i]) { M.push_back(L[i]); continue; }
+            for (int c = 0; c < 4; c++) M.push_back({L[i].level + 1, 2 * L[i].gx + (c & 1), 2 * L[i].gy + (c >> 1)});
+        }
+        L.swap(M);
+    }
+    if (!changed) {
+        bool same = ((int)L.size() == np);
+        for (size_t i = 0; same && i < L.size(); i++)
+            if (f.lookup(L[i].level, L[i].gx, L[i].gy) < 0) same = false;
+        if (!same) changed = 1;
+    }
+    (void)err;
+    return L;
+}
+
+// ---------------------------------------------------------------------------
+// gather tables
+// ---------------------------------------------------------------------------
+namespace {
+
+struct TableCtx {
+    const Forest& f;
+    int mx, my, mbc, nx, nq;
+    TableCtx(const Forest& ff) : f(ff)
+    {
+        mx = ff.g.d.mx; my = ff.g.d.my; mbc = ff.g.d.mbc; nx = mx + 2 * mbc; nq = ff.g.d.nq();
+    }
+    // absolute offset of Fortran cell (i,j), field 0, of slot p
+    int cell(int p, int i, int j) const { return p * nq + (j + mbc - 1) * nx + (i + mbc - 1); }
+    // transform_face2 / transform_corner2, same orientation: first child of coarse (i,j)
+    void half_first(const PatchInfo& C, const PatchInfo& F, int i, int j, int& di, int& dj) const
+    {
+        di = 1 + (2 * C.gx - F.gx) * mx + 2 * (i - 1);
+        dj = 1 + (2 * C.gy - F.gy) * my + 2 * (j - 1);
+    }
+};
+
+// Keeps the last entry written to each destination, in first-write order.
+template <class E>
+struct LastWriter {
+    std::vector<E> v;
+    std::unordered_map<int, int> at;
+    void put(const E& e)
+    {
+        auto it = at.find(e.dst);
+        if (it == at.end()) { at[e.dst] = (int)v.size(); v.push_back(e); }
+        else v[it->second] = e;
+    }
+};
+
+}  // namespace
+
+void build_tables(const Forest& f, const int mthbc[4], std::vector<LevelTables>& out)
+{
+    TableCtx T(f);
+    const int mx = T.mx, my = T.my, mbc = T.mbc;
+    out.assign(33, LevelTables());
+    for (int l = 0; l < 33; l++) {
+        LevelTables& LT = out[l];
+        const int p0 = f.lev_off[l], p1 = f.lev_off[l + 1];
+        if (p0 == p1) { LT.ss_start.assign(1, 0); LT.f2c_start.assign(1, 0); continue; }
+        // ---- copy2ghost: face pass then corner pass (fclaw2d_clawpatch46_copy.f) ----
+        {
+            LastWriter<CopyEnt> W;
+            for (int ip = p0; ip < p1; ip++) {
+                const PatchInfo& P = f.p[ip];
+                for (int fc = 0; fc < 4; fc++) {
+                    if (P.face_type[fc] != NB_SAME) continue;
+                    const int n = P.face_nbr[fc][0];
+                    const PatchInfo& N = f.p[n];
+                    const int si = (P.gx - N.gx) * mx, sj = (P.gy - N.gy) * my;
+                    int ilo, ihi, jlo, jhi;
+                    if (fc == 0) { ilo = 1 - mbc; ihi = 0; jlo = 1; jhi = my; }
+                    else if (fc == 1) { ilo = mx + 1; ihi = mx + mbc; jlo = 1; jhi = my; }
+                    else if (fc == 2) { ilo = 1; ihi = mx; jlo = 1 - mbc; jhi = 0; }
+                    else { ilo = 1; ihi = mx; jlo = my + 1; jhi = my + mbc; }
+                    for (int j = jlo; j <= jhi; j++)
+                        for (int i = ilo; i <= ihi; i++) W.put({T.cell(ip, i, j), T.cell(n, i + si, j + sj)});
+                }
+            }
+            for (int ip = p0; ip < p1; ip++) {
+                const PatchInfo& P = f.p[ip];
+                for (int c = 0; c < 4; c++) {
+                    if (!P.has_corner[c] || P.corner_type[c] != NB_SAME) continue;
+                    const int n = P.corner_nbr[c];
+                    const PatchInfo& N = f.p[n];
+                    const int si = (P.gx - N.gx) * mx, sj = (P.gy - N.gy) * my;
+                    for (int ibc = 1; ibc <= mbc; ibc++)
+                        for (int jbc = 1; jbc <= mbc; jbc++) {
+                            const int i1 = (c & 1) ? mx + ibc : 1 - ibc, j1 = (c & 2) ? my + jbc : 1 - jbc;
+                            W.put({T.cell(ip, i1, j1), T.cell(n, i1 + si, j1 + sj)});
+                        }
+                }
+            }
+            LT.copy = std::move(W.v);
+        }
+        // ---- average2ghost (coarse = this level) ----
+        {
+            LastWriter<CopyEnt> W;
+            for (int ip = p0; ip < p1; ip++) {
+                const PatchInfo& C = f.p[ip];
+                if (!C.on_cf) continue;
+                for (int fc = 0; fc < 4; fc++) {
+                    if (C.face_type[fc] != NB_HALF) continue;
+                    for (int ig = 0; ig < 2; ig++) {
+                        const int fi = C.face_nbr[fc][ig];
+                        const PatchInfo& F = f.p[fi];
+                        auto valid = [&](int i, int j) { return 1 <= i && i <= mx && 1 <= j && j <= my; };
+                        if (fc < 2) {
+                            for (int jc = 1; jc <= my; jc++)
+                                for (int ibc = 1; ibc <= mbc; ibc++) {
+                                    const int ic = (fc == 0) ? 1 - ibc : mx + ibc;
+                                    int di, dj; T.half_first(C, F, ic, jc, di, dj);
+                                    if (!valid(di, dj) || !valid(di + 1, dj + 1)) continue;
+                                    W.put({T.cell(ip, ic, jc), T.cell(fi, di, dj)});
+                                }
+                        } else {
+                            for (int jbc = 1; jbc <= mbc; jbc++)
+                                for (int ic = 1; ic <= mx; ic++) {
+                                    const int jc = (fc == 2) ? 1 - jbc : my + jbc;
+                                    int di, dj; T.half_first(C, F, ic, jc, di, dj);
+                                    if (!valid(di, dj) || !valid(di + 1, dj + 1)) continue;
+                                    W.put({T.cell(ip, ic, jc), T.cell(fi, di, dj)});
+                                }
+                        }
+                    }
+                }
+            }
+            for (int ip = p0; ip < p1; ip++) {
+                const PatchInfo& C = f.p[ip];
+                if (!C.on_cf) continue;
+                for (int c = 0; c < 4; c++) {
+                    if (!C.has_corner[c] || C.corner_type[c] != NB_HALF) continue;
+                    const int fi = C.corner_nbr[c];
+                    const PatchInfo& F = f.p[fi];
+                    for (int ibc = 1; ibc <= mbc; ibc++)
+                        for (int jbc = 1; jbc <= mbc; jbc++) {
+                            const int i1 = (c & 1) ? mx + ibc : 1 - ibc, j1 = (c & 2) ? my + jbc : 1 - jbc;
+                            int di, dj; T.half_first(C, F, i1, j1, di, dj);
+                            W.put({T.cell(ip, i1, j1), T.cell(fi, di, dj)});
+                        }
+                }
+            }
+            LT.avg = std::move(W.v);
+        }
+        // ---- interpolate2ghost (coarse = this level) ----
+        {
+            LastWriter<InterpEnt> W;
+            auto validi = [&](int i, int j) { return 1 - mbc <= i && i <= mx + mbc && 1 - mbc <= j && j <= my + mbc; };
+            auto emit = [&](int cp, int ic, int jc, int fp, int di, int dj) {
+                for (int m = 0; m < 4; m++) {
+                    const int ii = m & 1, jj = m >> 1;
+                    W.put({T.cell(fp, di + ii, dj + jj), T.cell(cp, ic, jc), m, 0});
+                }
+            };
+            for (int ip = p0; ip < p1; ip++) {
+                const PatchInfo& C = f.p[ip];
+                if (!C.on_cf) continue;
+                for (int fc = 0; fc < 4; fc++) {
+                    if (C.face_type[fc] != NB_HALF) continue;
+                    for (int ig = 0; ig < 2; ig++) {
+                        const int fi = C.face_nbr[fc][ig];
+                        const PatchInfo& F = f.p[fi];
+                        if (fc < 2) {
+                            for (int ibc = 1; ibc <= mbc / 2; ibc++) {
+                                const int ic = (fc == 0) ? ibc : mx - ibc + 1;
+                                for (int jc = 1; jc <= mx; jc++) {
+                                    int di, dj; T.half_first(C, F, ic, jc, di, dj);
+                                    if (!validi(di, dj) || !validi(di + 1, dj + 1)) continue;
+                                    emit(ip, ic, jc, fi, di, dj);
+                                }
+                            }
+                        } else {
+                            for (int jbc = 1; jbc <= mbc / 2; jbc++) {
+                                const int jc = (fc == 2) ? jbc : my - jbc + 1;
+                                for (int ic = 1; ic <= mx; ic++) {
+                                    int di, dj; T.half_first(C, F, ic, jc, di, dj);
+                                    if (!validi(di, dj) || !validi(di + 1, dj + 1)) continue;
+                                    emit(ip, ic, jc, fi, di, dj);
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            for (int ip = p0; ip < p1; ip++) {
+                const PatchInfo& C = f.p[ip];
+                if (!C.on_cf) continue;
+                for (int c = 0; c < 4; c++) {
+                    if (!C.has_corner[c] || C.corner_type[c] != NB_HALF) continue;
+                    const int fi = C.corner_nbr[c];
+                    const PatchInfo& F = f.p[fi];
+                    for (int ibc = 1; ibc <= mbc / 2; ibc++)
+                        for (int jbc = 1; jbc <= mbc / 2; jbc++) {
+                            const int ic = (c & 1) ? mx - ibc + 1 : ibc, jc = (c & 2) ? my - jbc + 1 : jbc;
+                            int di, dj; T.half_first(C, F, ic, jc, di, dj);
+                            emit(ip, ic, jc, fi, di, dj);
+                        }
+                }
+            }
+            LT.interp = std::move(W.v);
+        }
+        // ---- setphysical: clawpack46_bc2_default with chains resolved per patch ----
+        {
+            for (int ip = p0; ip < p1; ip++) {
+                const PatchInfo& P = f.p[ip];
+                if (!(P.phys[0] || P.phys[1] || P.phys[2] || P.phys[3])) continue;
+                // written cell -> (source cell, negate mask), within this bc2 call
+                std::map<int, std::pair<int, int>> wr;
+                std::vector<int> order;
+                auto put = [&](int di, int dj, int si, int sj, int neg) {
+                    const int dst = T.cell(ip, di, dj);
+                    int src = T.cell(ip, si, sj);
+                    auto it = wr.find(src);
+                    if (it != wr.end()) { neg ^= it->second.second; src = it->second.first; }
+                    if (wr.find(dst) == wr.end()) order.push_back(dst);
+                    wr[dst] = {src, neg};
+                };
+                const int NEG2 = 1 << 1, NEG3 = 1 << 2;   // field 2 (x momentum) / field 3 (y momentum)
+                int bc[4];
+                for (int k = 0; k < 4; k++) bc[k] = P.phys[k] ? mthbc[k] : -1;
+                if (bc[0] == 1) for (int ibc = 1; ibc <= mbc; ibc++) for (int j = 1 - mbc; j <= my + mbc; j++) put(1 - ibc, j, 1, j, 0);
+                if (bc[0] == 3) for (int ibc = 1; ibc <= mbc; ibc++) for (int j = 1 - mbc; j <= my + mbc; j++) put(1 - ibc, j, ibc, j, NEG2);
+                if (bc[1] == 1) for (int ibc = 1; ibc <= mbc; ibc++) for (int j = 1 - mbc; j <= my + mbc; j++) put(mx + ibc, j, mx, j, 0);
+                if (bc[1] == 3) for (int ibc = 1; ibc <= mbc; ibc++) for (int j = 1 - mbc; j <= my + mbc; j++) put(mx + ibc, j, mx + 1 - ibc, j, NEG2);
+                if (bc[2] == 1) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, 1 - jbc, i, 1, 0);
+                if (bc[2] == 3) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, 1 - jbc, i, jbc, NEG3);
+                if (bc[3] == 1) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, my + jbc, i, my, 0);
+                if (bc[3] == 3) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, my + jbc, i, my + 1 - jbc, NEG3);
+                for (int dst : order) {
+                    const auto& s = wr[dst];
+                    LT.phys.push_back({dst, s.first, s.second, 0});
+                }
+            }
+        }
+        // ---- time interpolation patches ----
+        for (int ip = p0; ip < p1; ip++) if (f.p[ip].has_fine_nbr) LT.ti.push_back(ip);
+        // ---- time sync ops ----
+        LT.ss_start.push_back(0);
+        for (int ip = p0; ip < p1; ip++) {
+            const PatchInfo& P = f.p[ip];
+            int nops = 0;
+            for (int fc = 0; fc < 4; fc++)
+                if (P.face_type[fc] == NB_SAME) { LT.ss.push_back({ip, P.face_nbr[fc][0], fc, 0, 0, {0, 0, 0}}); nops++; }
+            if (nops) LT.ss_start.push_back((int)LT.ss.size());
+        }
+        LT.f2c_start.push_back(0);
+        for (int ip = p0; ip < p1; ip++) {
+            const PatchInfo& C = f.p[ip];
+            int nops = 0;
+            for (int fc = 0; fc < 4; fc++) {
+                if (C.face_type[fc] != NB_HALF) continue;
+                for (int ig = 0; ig < 2; ig++) {
+                    const int fi = C.face_nbr[fc][ig];
+                    const PatchInfo& F = f.p[fi];
+                    const int noff = (fc < 2) ? (2 * C.gy - F.gy) * my : (2 * C.gx - F.gx) * mx;
+                    LT.f2c.push_back({ip, fi, fc, ig, noff, {0, 0, 0}});
+                    nops++;
+                }
+            }
+            if (nops) LT.f2c_start.push_back((int)LT.f2c.size());
+        }
+    }
+}
+
+}  // namespace fcb

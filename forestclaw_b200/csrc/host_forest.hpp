@@ -1,0 +1,75 @@
+// host_forest.hpp -- host-side forest of patches and the device gather tables.
+//
+// The forest plays p4est's role for the B200 package: leaves of a quadtree over
+// a brick of equally oriented blocks, face/corner neighbour relations, 2:1
+// face+corner balance and adaptation.  From it the host builds, once per
+// regrid, the per-level gather tables that turn the reference's per-patch
+// ghost-fill and time-sync callbacks into single device launches.
+#pragma once
+#include <stdint.h>
+#include <string>
+#include <unordered_map>
+#include <vector>
+#include "kernels.h"
+
+namespace fcb {
+
+enum { NB_BOUNDARY = 0, NB_HALF = 1, NB_SAME = 2, NB_DOUBLE = 3 };
+
+struct Leaf { int level, gx, gy; };
+
+struct PatchInfo {
+    int level, gx, gy, block;
+    uint64_t morton;
+    double xlower, ylower, dx, dy;
+    int face_type[4];
+    int face_nbr[4][2];
+    int phys[4];
+    int has_corner[4], corner_type[4], corner_nbr[4];
+    int has_fine_nbr, on_cf;
+};
+
+struct Geometry {
+    Dims d;
+    int mi, mj;
+    double ax, bx, ay, by;
+};
+
+class Forest {
+public:
+    Geometry g;
+    std::vector<PatchInfo> p;        // slot order: level-major, then block, then Morton
+    int lev_off[34];                 // patches of level l: [lev_off[l], lev_off[l+1])
+    int minlevel_present = 0, maxlevel_present = -1;
+
+    // Install leaves (any order).  Returns false (and sets err) if not 2:1 balanced.
+    bool build(const std::vector<Leaf>& leaves, std::string& err);
+    int lookup(int l, int x, int y) const;
+    int np() const { return (int)p.size(); }
+    bool in_domain(int l, int x, int y) const { return x >= 0 && y >= 0 && x < (g.mi << l) && y < (g.mj << l); }
+    void geometry(PatchInfo& q) const;
+
+private:
+    std::unordered_map<uint64_t, int> index_;
+    static uint64_t key(int l, int x, int y) { return ((uint64_t)l << 56) | ((uint64_t)x << 28) | (uint64_t)y; }
+};
+
+// Refine marked leaves, coarsen fully marked families, then 2:1 balance
+// (p4est_wrap adapt semantics).  mark: +1 refine, -1 coarsen, 0 keep.
+// Returns the new leaf list; changed = 0 if identical to the old forest.
+std::vector<Leaf> adapt_leaves(const Forest& f, const std::vector<int>& mark, int& changed, std::string& err);
+
+// Gather tables of one level.
+struct LevelTables {
+    std::vector<CopyEnt> copy;       // copy2ghost(level)
+    std::vector<CopyEnt> avg;        // average2ghost(level): level is the coarse level
+    std::vector<InterpEnt> interp;   // interpolate2ghost(level): level is the coarse level
+    std::vector<PhysEnt> phys;       // setphysical(level)
+    std::vector<int> ti;             // patches with fine-grid neighbours (fclaw2d_timeinterp)
+    std::vector<SyncOp> ss; std::vector<int> ss_start;   // time_sync_samesize ops grouped per patch
+    std::vector<SyncOp> f2c; std::vector<int> f2c_start; // time_sync_f2c ops grouped per coarse patch
+};
+
+void build_tables(const Forest& f, const int mthbc[4], std::vector<LevelTables>& out);
+
+}  // namespace fcb

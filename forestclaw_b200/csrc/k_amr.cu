@@ -1,0 +1,436 @@
+// k_amr.cu -- ghost-fill, time-sync, diagnostics and regrid kernels.
+//
+// Ghost fill runs from gather tables built on the host at regrid time: every
+// ghost cell the reference's copy / average / interpolate / physical-BC
+// callbacks would write in one stage becomes one table entry (last writer of the
+// reference's callback order wins), so each stage is one launch with one thread
+// per ghost cell and disjoint destinations.  Arithmetic follows the clawpatch
+// 4.6 Fortran in evaluation order; this file is compiled without FMA
+// contraction so the FP64 results match the FP64 CPU path bit for bit.
+//   average face/corner   fort_4.6/fclaw2d_clawpatch46_average.f:16-272
+//   interpolate           fort_4.6/fclaw2d_clawpatch46_interpolate.f:30-392, utils.f:45-63
+//   physical BC           clawpack46_bc2_default.f:1-213
+//   timeinterp            fort_4.6/fclaw2d_clawpatch46_timeinterp.f:11-78
+//   time sync             clawpack46_time_sync.f:254-704, clawpatch_conservation.c:207-280
+//   mass                  fort_4.6/fclaw2d_clawpatch46_diagnostics.f:13-55
+//   tagging               fort_4.6/fclaw2d_clawpatch46_tag4refinement.f / _tag4coarsening.f
+#include "kernels.h"
+
+namespace fcb {
+
+static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
+
+__global__ void k_copy(double* __restrict__ dst, const double* __restrict__ src, const CopyEnt* __restrict__ e,
+                       int n, int nxy, int meqn)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    CopyEnt c = e[t];
+    for (int m = 0; m < meqn; m++) dst[c.dst + m * nxy] = src[c.src + m * nxy];
+}
+
+__global__ void k_average(double* __restrict__ dst, const double* __restrict__ src, const CopyEnt* __restrict__ e,
+                          int n, int nx, int nxy, int meqn)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    CopyEnt c = e[t];
+    for (int m = 0; m < meqn; m++) {
+        const double* f = src + c.src + m * nxy;
+        double sum = 0.0;
+        sum = sum + f[0];
+        sum = sum + f[1];
+        sum = sum + f[nx];
+        sum = sum + f[nx + 1];
+        dst[c.dst + m * nxy] = sum / 4.0;
+    }
+}
+
+// AMRClaw limited slopes (fclaw2d_clawpatch_utils.f:52-55, mth = 5)
+__device__ __forceinline__ double compute_slopes(double sl, double sr)
+{
+    double sc = (sl + sr) / 2.0;
+    double a = fabs(sl) * 2.0, b = fabs(sr) * 2.0, c = fabs(sc);
+    double mn = a < b ? a : b;
+    mn = mn < c ? mn : c;
+    double s = copysign(1.0, sl * sr);
+    return mn * (s > 0.0 ? s : 0.0) * copysign(1.0, sc);
+}
+
+__global__ void k_interp(double* __restrict__ dst, const double* __restrict__ src, const InterpEnt* __restrict__ e,
+                         int n, int nx, int nxy, int meqn)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    InterpEnt c = e[t];
+    const double shx = (c.sub & 1) ? 0.25 : -0.25;
+    const double shy = (c.sub & 2) ? 0.25 : -0.25;
+    for (int m = 0; m < meqn; m++) {
+        const double* qc = src + c.src + m * nxy;
+        double q0 = qc[0];
+        double sl = (q0 - qc[-1]);
+        double sr = (qc[1] - q0);
+        double gradx = compute_slopes(sl, sr);
+        sl = (q0 - qc[-nx]);
+        sr = (qc[nx] - q0);
+        double grady = compute_slopes(sl, sr);
+        dst[c.dst + m * nxy] = q0 + gradx * shx + grady * shy;
+    }
+}
+
+__global__ void k_phys(double* __restrict__ q, const PhysEnt* __restrict__ e, int n, int nxy, int meqn)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    PhysEnt c = e[t];
+    for (int m = 0; m < meqn; m++) {
+        double v = q[c.src + m * nxy];
+        q[c.dst + m * nxy] = ((c.neg >> m) & 1) ? -v : v;
+    }
+}
+
+// Band of width mbc inside the patch, in the four loops of timeinterp.f:33-70.
+__global__ void k_timeinterp(const double* __restrict__ q, const double* __restrict__ ql, double* __restrict__ qi,
+                             const int* __restrict__ patches, int mx, int my, int mbc, int meqn, double alpha)
+{
+    const int p = patches[blockIdx.x];
+    const int nx = mx + 2 * mbc, ny = my + 2 * mbc, nxy = nx * ny;
+    const size_t base = (size_t)p * nxy * meqn;
+    for (int c = threadIdx.x; c < nxy; c += blockDim.x) {
+        const int ic = c % nx, jc = c / nx;
+        const int i = ic - mbc + 1, j = jc - mbc + 1;     // Fortran indices
+        if (i < 1 || i > mx || j < 1 || j > my) continue;
+        const bool band = (i <= mbc) || (i > mx - mbc) || (j <= mbc) || (j > my - mbc);
+        if (!band) continue;
+        for (int m = 0; m < meqn; m++) {
+            const size_t k = base + (size_t)m * nxy + c;
+            qi[k] = ql[k] + alpha * (q[k] - ql[k]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Time sync
+// ---------------------------------------------------------------------------
+struct RegOff {
+    int fp0, fp1, fm0, fm1, gp0, gp1, gm0, gm1, ef0, ef1, ef2, ef3;
+    __device__ RegOff(int mx, int my, int meqn)
+    {
+        fp0 = 0; fp1 = my * meqn; fm0 = 2 * my * meqn; fm1 = 3 * my * meqn;
+        gp0 = 4 * my * meqn; gp1 = gp0 + mx * meqn; gm0 = gp0 + 2 * mx * meqn; gm1 = gp0 + 3 * mx * meqn;
+        ef0 = gp0 + 4 * mx * meqn; ef1 = ef0 + 2 * my * meqn; ef2 = ef1 + 2 * my * meqn; ef3 = ef2 + 2 * mx * meqn;
+    }
+};
+
+// clawpack46_fort_time_sync_samesize (same orientation, sc = 1): one CTA per
+// patch, faces in order 0..3 so corner cells see both corrections in order.
+__global__ void k_samesize(double* __restrict__ q, const double* __restrict__ regs, const PatchDesc* __restrict__ desc,
+                           const SyncOp* __restrict__ ops, const int* __restrict__ op_start,
+                           int mx, int my, int mbc, int meqn, int nreg)
+{
+    const int o0 = op_start[blockIdx.x], o1 = op_start[blockIdx.x + 1];
+    const int nx = mx + 2 * mbc, ny = my + 2 * mbc, nxy = nx * ny;
+    RegOff R(mx, my, meqn);
+    for (int o = o0; o < o1; o++) {
+        const SyncOp op = ops[o];
+        const double* rt = regs + (size_t)op.p * nreg;
+        const double* rn = regs + (size_t)op.n * nreg;
+        const PatchDesc pd = desc[op.p];
+        const double area = pd.dx * pd.dy;
+        double* qp = q + (size_t)op.p * nxy * meqn;
+        const int nt = (op.face < 2) ? my : mx;
+        for (int t = threadIdx.x; t < nt * meqn; t += blockDim.x) {
+            const int j = t % nt, m = t / nt;                      // j: 0-based tangential index
+            double delta;
+            int ic, jc;
+            if (op.face == 0) {
+                double fp = rn[R.fp1 + j + m * my];
+                double ef = 1 * rn[R.ef1 + j + m * my + my * meqn];
+                delta = (ef - rt[R.ef0 + j + m * my]) - (fp - rt[R.fp0 + j + m * my]);
+                ic = mbc; jc = mbc + j;
+            } else if (op.face == 1) {
+                double fm = rn[R.fm0 + j + m * my];
+                double ef = 1 * rn[R.ef0 + j + m * my + my * meqn];
+                delta = (rt[R.ef1 + j + m * my] - ef) - (fm - rt[R.fm1 + j + m * my]);
+                ic = mx + mbc - 1; jc = mbc + j;
+            } else if (op.face == 2) {
+                double gp = rn[R.gp1 + j + m * mx];
+                double ef = 1 * rn[R.ef3 + j + m * mx + mx * meqn];
+                delta = (ef - rt[R.ef2 + j + m * mx]) - (gp - rt[R.gp0 + j + m * mx]);
+                ic = mbc + j; jc = mbc;
+            } else {
+                double gm = rn[R.gm0 + j + m * mx];
+                double ef = 1 * rn[R.ef2 + j + m * mx + mx * meqn];
+                delta = (rt[R.ef3 + j + m * mx] - ef) - (gm - rt[R.gm1 + j + m * mx]);
+                ic = mbc + j; jc = my + mbc - 1;
+            }
+            double* qq = qp + (size_t)m * nxy + jc * nx + ic;
+            *qq = *qq + 0.5 * delta / area;
+        }
+        __syncthreads();
+    }
+}
+
+// clawpack46_fort_time_sync_f2c (same orientation, sc = 1): one CTA per coarse
+// patch; ops ordered (face, igrid) as in cb_face_fill.  n_off = first fine index
+// offset (2*Cg - Fg)*n along the face.
+__global__ void k_f2c(double* __restrict__ q, const double* __restrict__ regs, const PatchDesc* __restrict__ desc,
+                      const SyncOp* __restrict__ ops, const int* __restrict__ op_start,
+                      int mx, int my, int mbc, int meqn, int nreg)
+{
+    const int o0 = op_start[blockIdx.x], o1 = op_start[blockIdx.x + 1];
+    const int nx = mx + 2 * mbc, ny = my + 2 * mbc, nxy = nx * ny;
+    RegOff R(mx, my, meqn);
+    for (int o = o0; o < o1; o++) {
+        const SyncOp op = ops[o];
+        const double* rc = regs + (size_t)op.p * nreg;
+        const double* rf = regs + (size_t)op.n * nreg;
+        const PatchDesc pd = desc[op.p];
+        const double areac = pd.dx * pd.dy;
+        double* qp = q + (size_t)op.p * nxy * meqn;
+        const int nt = (op.face < 2) ? my : mx;
+        for (int t = threadIdx.x; t < nt * meqn; t += blockDim.x) {
+            const int jcn = t % nt, m = t / nt;                 // 0-based coarse tangential index
+            const int d = 1 + op.n_off + 2 * jcn;               // first fine child (Fortran index)
+            if (d < 1 || d + 1 > nt) continue;                  // fc46_skip_this_grid
+            const int f0 = d - 1, f1 = d;                       // 0-based fine pair
+            double deltac;
+            int ic, jc;
+            if (op.face == 0) {
+                double fp = rf[R.fp1 + f0 + m * my] + rf[R.fp1 + f1 + m * my];
+                double ef = 1 * (rf[R.ef1 + f0 + m * my + my * meqn] + rf[R.ef1 + f1 + m * my + my * meqn]);
+                deltac = (ef - rc[R.ef0 + jcn + m * my]) - (fp - rc[R.fp0 + jcn + m * my]);
+                ic = mbc; jc = mbc + jcn;
+            } else if (op.face == 1) {
+                double fm = rf[R.fm0 + f0 + m * my] + rf[R.fm0 + f1 + m * my];
+                double ef = 1 * (rf[R.ef0 + f0 + m * my + my * meqn] + rf[R.ef0 + f1 + m * my + my * meqn]);
+                deltac = (rc[R.ef1 + jcn + m * my] - ef) - (fm - rc[R.fm1 + jcn + m * my]);
+                ic = mx + mbc - 1; jc = mbc + jcn;
+            } else if (op.face == 2) {
+                double gp = rf[R.gp1 + f0 + m * mx] + rf[R.gp1 + f1 + m * mx];
+                double ef = 1 * (rf[R.ef3 + f0 + m * mx + mx * meqn] + rf[R.ef3 + f1 + m * mx + mx * meqn]);
+                deltac = (ef - rc[R.ef2 + jcn + m * mx]) - (gp - rc[R.gp0 + jcn + m * mx]);
+                ic = mbc + jcn; jc = mbc;
+            } else {
+                double gm = rf[R.gm0 + f0 + m * mx] + rf[R.gm0 + f1 + m * mx];
+                double ef = 1 * (rf[R.ef2 + f0 + m * mx + mx * meqn] + rf[R.ef2 + f1 + m * mx + mx * meqn]);
+                deltac = (rc[R.ef3 + jcn + m * mx] - ef) - (gm - rc[R.gm1 + jcn + m * mx]);
+                ic = mbc + jcn; jc = my + mbc - 1;
+            }
+            double* qq = qp + (size_t)m * nxy + jc * nx + ic;
+            *qq = *qq + deltac / areac;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_reset(double* __restrict__ regs, const PatchDesc* __restrict__ desc, int p0, int mx, int my,
+                        int meqn, int nreg, int coarse_level, int mode)
+{
+    const int p = p0 + blockIdx.x;
+    const PatchDesc pd = desc[p];
+    double* r = regs + (size_t)p * nreg;
+    RegOff R(mx, my, meqn);
+    for (int k = 0; k < 4; k++) {
+        const int ft = (pd.face_type >> (2 * k)) & 3;        // 0 bnd, 1 half, 2 same, 3 double
+        bool reset;
+        if (mode == 1) reset = (ft == 1 && pd.level == coarse_level) || (ft == 3 && pd.level == coarse_level + 1);
+        else if (mode == 2) reset = (ft == 2 && pd.level == coarse_level);
+        else reset = (ft == 0);
+        if (!reset) continue;
+        if (k < 2) {
+            for (int t = threadIdx.x; t < meqn * my; t += blockDim.x) {
+                r[(k == 0 ? R.fm0 : R.fm1) + t] = 0.0;
+                r[(k == 0 ? R.fp0 : R.fp1) + t] = 0.0;
+                const int ef = (k == 0) ? R.ef0 : R.ef1;
+                r[ef + t] = 0.0;
+                r[ef + t + meqn * my] = 0.0;
+            }
+        } else {
+            for (int t = threadIdx.x; t < meqn * mx; t += blockDim.x) {
+                r[(k == 2 ? R.gm0 : R.gm1) + t] = 0.0;
+                r[(k == 2 ? R.gp0 : R.gp1) + t] = 0.0;
+                const int ef = (k == 2) ? R.ef2 : R.ef3;
+                r[ef + t] = 0.0;
+                r[ef + t + meqn * mx] = 0.0;
+            }
+        }
+    }
+}
+
+// Per-patch, per-field Kahan sums of q*dx*dy over interior cells in (j, i) order.
+__global__ void k_patch_mass(const double* __restrict__ q, const PatchDesc* __restrict__ desc, int mx, int my,
+                             int mbc, int meqn, double* __restrict__ out)
+{
+    const int p = blockIdx.x, m = threadIdx.x;
+    if (m >= meqn) return;
+    const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
+    const PatchDesc pd = desc[p];
+    const double area = pd.dx * pd.dy;
+    const double* qp = q + ((size_t)p * meqn + m) * nx * ny;
+    double sum = 0.0, comp = 0.0;
+    for (int j = 0; j < my; j++)
+        for (int i = 0; i < mx; i++) {
+            double y = qp[(j + mbc) * nx + i + mbc] * area - comp;
+            double t = sum + y;
+            comp = (t - sum) - y;
+            sum = t;
+        }
+    out[(size_t)p * meqn + m] = sum;
+}
+
+// Gradient criterion scaled by dx on field 1 (gradient_exceeds_th.f90, unmapped branch).
+__global__ void k_tag(const double* __restrict__ q, const PatchDesc* __restrict__ desc, int mx, int my, int mbc,
+                      int meqn, double rthr, double cthr, int* __restrict__ flags)
+{
+    const int p = blockIdx.x;
+    const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
+    const PatchDesc pd = desc[p];
+    const double* qp = q + (size_t)p * meqn * nx * ny;
+    const double dx2 = 2 * pd.dx, dy2 = 2 * pd.dy;
+    int refine = 0, exceed_c = 0;
+    for (int c = threadIdx.x; c < mx * my; c += blockDim.x) {
+        const int i = c % mx + mbc, j = c / mx + mbc;
+        double dqx = (qp[j * nx + i + 1] - qp[j * nx + i - 1]) / dx2;
+        double dqy = (qp[(j + 1) * nx + i] - qp[(j - 1) * nx + i]) / dy2;
+        double ds = sqrt(dqx * dqx + dqy * dqy + 0.0 * 0.0);
+        double v = ds * pd.dx;
+        refine |= (v > rthr);
+        exceed_c |= (v > cthr);
+    }
+    refine = __syncthreads_or(refine);
+    exceed_c = __syncthreads_or(exceed_c);
+    if (threadIdx.x == 0) flags[p] = (refine ? 1 : 0) | (exceed_c ? 0 : 2);
+}
+
+// Regrid repopulation (cb_fclaw2d_regrid_repopulate, fclaw2d_regrid.c:93-205).
+__global__ void k_repop(const RepopOp* __restrict__ ops, int mx, int my, int mbc, int meqn, int nreg,
+                        const double* __restrict__ oq, double* __restrict__ nq,
+                        const double* __restrict__ oql, double* __restrict__ nql,
+                        const double* __restrict__ oqi, double* __restrict__ nqi,
+                        const double* __restrict__ oregs, double* __restrict__ nregs)
+{
+    const RepopOp op = ops[blockIdx.x];
+    const int nx = mx + 2 * mbc, ny = my + 2 * mbc, nxy = nx * ny, nqp = nxy * meqn;
+    double* d = nq + (size_t)op.dst * nqp;
+    if (op.kind == 0) {
+        const size_t so = (size_t)op.src * nqp;
+        for (int k = threadIdx.x; k < nqp; k += blockDim.x) {
+            d[k] = oq[so + k];
+            nql[(size_t)op.dst * nqp + k] = oql[so + k];
+            if (nqi) nqi[(size_t)op.dst * nqp + k] = oqi[so + k];
+        }
+        for (int k = threadIdx.x; k < nreg; k += blockDim.x)
+            nregs[(size_t)op.dst * nreg + k] = oregs[(size_t)op.src * nreg + k];
+        return;
+    }
+    // new patch: zero everything first
+    for (int k = threadIdx.x; k < nqp; k += blockDim.x) {
+        d[k] = 0.0;
+        nql[(size_t)op.dst * nqp + k] = 0.0;
+        if (nqi) nqi[(size_t)op.dst * nqp + k] = 0.0;
+    }
+    for (int k = threadIdx.x; k < nreg; k += blockDim.x) nregs[(size_t)op.dst * nreg + k] = 0.0;
+    __syncthreads();
+    if (op.kind == 1) {
+        // interpolate2fine (interpolate.f:324-392)
+        const double* qc = oq + (size_t)op.src * nqp;
+        const int ig = op.igrid % 2, jg = op.igrid / 2;
+        const int i1 = 1 - ig, i2 = mx / 2 + (1 - ig), j1 = 1 - jg, j2 = my / 2 + (1 - jg);
+        const int icadd = ig * mx / 2, jcadd = jg * my / 2;
+        const int ni = i2 - i1 + 1, nj = j2 - j1 + 1;
+        for (int t = threadIdx.x; t < ni * nj * meqn; t += blockDim.x) {
+            const int i = i1 + t % ni, j = j1 + (t / ni) % nj, m = t / (ni * nj);
+            const int ic = i + icadd, jc = j + jcadd;
+            const double* c0 = qc + (size_t)m * nxy + (jc + mbc - 1) * nx + (ic + mbc - 1);
+            double q0 = c0[0];
+            double sl = (q0 - c0[-1]);
+            double sr = (c0[1] - q0);
+            double gradx = compute_slopes(sl, sr);
+            sl = (q0 - c0[-nx]);
+            sr = (c0[nx] - q0);
+            double grady = compute_slopes(sl, sr);
+            for (int ii = 1; ii <= 2; ii++)
+                for (int jj = 1; jj <= 2; jj++) {
+                    const double shx = (ii - 2 / 2.0 - 0.5) / 2, shy = (jj - 2 / 2.0 - 0.5) / 2;
+                    const int fi = (i - 1) * 2 + ii, fj = (j - 1) * 2 + jj;
+                    d[(size_t)m * nxy + (fj + mbc - 1) * nx + (fi + mbc - 1)] = q0 + shx * gradx + shy * grady;
+                }
+        }
+    } else {
+        // average2coarse (average.f:282-364): child c fills quarter (ig, jg)
+        for (int c = 0; c < 4; c++) {
+            const double* qf = oq + (size_t)op.child[c] * nqp;
+            const int ig = c % 2, jg = c / 2;
+            const int icadd = ig * mx / 2, jcadd = jg * mx / 2;
+            for (int t = threadIdx.x; t < (mx / 2) * (my / 2) * meqn; t += blockDim.x) {
+                const int i = 1 + t % (mx / 2), j = 1 + (t / (mx / 2)) % (my / 2), m = t / ((mx / 2) * (my / 2));
+                double sum = 0.0;
+                for (int jj = 1; jj <= 2; jj++)
+                    for (int ii = 1; ii <= 2; ii++) {
+                        const int fi = (i - 1) * 2 + ii, fj = (j - 1) * 2 + jj;
+                        sum = sum + qf[(size_t)m * nxy + (fj + mbc - 1) * nx + (fi + mbc - 1)];
+                    }
+                d[(size_t)m * nxy + (j + jcadd + mbc - 1) * nx + (i + icadd + mbc - 1)] = sum / 4;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launch wrappers
+// ---------------------------------------------------------------------------
+void launch_copy(const Dims& d, double* dst, const double* src, const CopyEnt* e, int n, cudaStream_t st)
+{
+    if (n > 0) k_copy<<<nblk(n, 256), 256, 0, st>>>(dst, src, e, n, d.nxy(), d.meqn);
+}
+void launch_average(const Dims& d, double* dst, const double* src, const CopyEnt* e, int n, cudaStream_t st)
+{
+    if (n > 0) k_average<<<nblk(n, 256), 256, 0, st>>>(dst, src, e, n, d.nx(), d.nxy(), d.meqn);
+}
+void launch_interp(const Dims& d, double* dst, const double* src, const InterpEnt* e, int n, cudaStream_t st)
+{
+    if (n > 0) k_interp<<<nblk(n, 256), 256, 0, st>>>(dst, src, e, n, d.nx(), d.nxy(), d.meqn);
+}
+void launch_phys(const Dims& d, double* q, const PhysEnt* e, int n, cudaStream_t st)
+{
+    if (n > 0) k_phys<<<nblk(n, 256), 256, 0, st>>>(q, e, n, d.nxy(), d.meqn);
+}
+void launch_timeinterp(const Dims& d, const double* q, const double* qlast, double* qinterp, const int* patches,
+                       int npatch, double alpha, cudaStream_t st)
+{
+    if (npatch > 0) k_timeinterp<<<npatch, 256, 0, st>>>(q, qlast, qinterp, patches, d.mx, d.my, d.mbc, d.meqn, alpha);
+}
+void launch_samesize(const Dims& d, double* q, const double* regs, const PatchDesc* desc, const SyncOp* ops,
+                     const int* op_start, int npatch, cudaStream_t st)
+{
+    if (npatch > 0) k_samesize<<<npatch, 64, 0, st>>>(q, regs, desc, ops, op_start, d.mx, d.my, d.mbc, d.meqn, d.nreg());
+}
+void launch_f2c(const Dims& d, double* q, const double* regs, const PatchDesc* desc, const SyncOp* ops,
+                const int* op_start, int npatch, cudaStream_t st)
+{
+    if (npatch > 0) k_f2c<<<npatch, 64, 0, st>>>(q, regs, desc, ops, op_start, d.mx, d.my, d.mbc, d.meqn, d.nreg());
+}
+void launch_reset(const Dims& d, double* regs, const PatchDesc* desc, int p0, int np, int coarse_level, int mode,
+                  cudaStream_t st)
+{
+    if (np > 0) k_reset<<<np, 64, 0, st>>>(regs, desc, p0, d.mx, d.my, d.meqn, d.nreg(), coarse_level, mode);
+}
+void launch_patch_mass(const Dims& d, const double* q, const PatchDesc* desc, int np, double* out, cudaStream_t st)
+{
+    if (np > 0) k_patch_mass<<<np, 32, 0, st>>>(q, desc, d.mx, d.my, d.mbc, d.meqn, out);
+}
+void launch_tag(const Dims& d, const double* q, const PatchDesc* desc, int np, double rthr, double cthr, int* flags,
+                cudaStream_t st)
+{
+    if (np > 0) k_tag<<<np, 128, 0, st>>>(q, desc, d.mx, d.my, d.mbc, d.meqn, rthr, cthr, flags);
+}
+void launch_repop(const Dims& d, const RepopOp* ops, int nops, const double* oq, double* nq, const double* oqlast,
+                  double* nqlast, const double* oqi, double* nqi, const double* oregs, double* nregs, cudaStream_t st)
+{
+    if (nops > 0)
+        k_repop<<<nops, 256, 0, st>>>(ops, d.mx, d.my, d.mbc, d.meqn, d.nreg(), oq, nq, oqlast, nqlast, oqi, nqi,
+                                      oregs, nregs);
+}
+
+}  // namespace fcb

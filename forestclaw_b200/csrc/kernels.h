@@ -1,0 +1,68 @@
+// kernels.h -- host-callable launch wrappers of the device kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "fcb_common.h"
+
+namespace fcb {
+
+struct Dims {
+    int mx, my, mbc, meqn, maux;
+    int nx() const { return mx + 2 * mbc; }
+    int ny() const { return my + 2 * mbc; }
+    int nxy() const { return nx() * ny(); }
+    int nq() const { return nxy() * meqn; }
+    int naux() const { return nxy() * maux; }
+    // conservation registers per patch (fclaw2d_clawpatch_conservation.h:56-77)
+    int nreg() const { return 4 * my * meqn + 4 * mx * meqn + 4 * my * meqn + 4 * mx * meqn; }
+};
+
+// ---- fused update (k_step2_f64.cu) ------------------------------------------
+// Returns cudaErrorInvalidValue when no specialisation exists for (rp, mx, my, mbc).
+cudaError_t launch_step2(int rp, int precision, const Dims& d, double* q, double* qlast, const double* aux,
+                         double* regs, const PatchDesc* desc, int p0, int npatch, const StepParams& sp,
+                         unsigned long long* cfl_bits, cudaStream_t st);
+bool step2_supported(int rp, int precision, int mx, int my, int mbc);
+
+// ---- ghost fill (k_amr.cu) ----------------------------------------------------
+// Gather tables: offsets are absolute indices of field 0 in the q slab; fields
+// follow at +m*nxy.
+struct CopyEnt { int dst, src; };                  // copy / average (src = first child)
+struct InterpEnt { int dst, src, sub, pad; };      // sub = child position 0..3 (ii + 2 jj)
+struct PhysEnt { int dst, src, neg, pad; };        // neg: bit m set => negate field m
+
+void launch_copy(const Dims& d, double* dst, const double* src, const CopyEnt* e, int n, cudaStream_t st);
+void launch_average(const Dims& d, double* dst, const double* src, const CopyEnt* e, int n, cudaStream_t st);
+void launch_interp(const Dims& d, double* dst, const double* src, const InterpEnt* e, int n, cudaStream_t st);
+void launch_phys(const Dims& d, double* q, const PhysEnt* e, int n, cudaStream_t st);
+void launch_timeinterp(const Dims& d, const double* q, const double* qlast, double* qinterp,
+                       const int* patches, int npatch, double alpha, cudaStream_t st);
+
+// ---- time sync (k_amr.cu) -------------------------------------------------------
+// One op = (coarse/this patch, fine/neighbour patch, face, igrid).  Ops of one
+// patch are contiguous and in the reference order; op_start[i]..op_start[i+1]
+// are the ops of the i-th patch of the launch.
+struct SyncOp { int p, n, face, igrid; int n_off; int pad[3]; };
+void launch_samesize(const Dims& d, double* q, const double* regs, const PatchDesc* desc,
+                     const SyncOp* ops, const int* op_start, int npatch, cudaStream_t st);
+void launch_f2c(const Dims& d, double* q, const double* regs, const PatchDesc* desc,
+                const SyncOp* ops, const int* op_start, int npatch, cudaStream_t st);
+// mode 1 = F2C, 2 = SAMESIZE, 3 = PHYS (fclaw2d_clawpatch_time_sync_reset)
+void launch_reset(const Dims& d, double* regs, const PatchDesc* desc, int p0, int np, int coarse_level,
+                  int mode, cudaStream_t st);
+
+// ---- diagnostics / regrid (k_amr.cu) -------------------------------------------
+void launch_patch_mass(const Dims& d, const double* q, const PatchDesc* desc, int np, double* out,
+                       cudaStream_t st);
+// flags[p] bit0: some interior cell exceeds refine threshold, bit1: no cell exceeds coarsen threshold
+void launch_tag(const Dims& d, const double* q, const PatchDesc* desc, int np, double refine_thr,
+                double coarsen_thr, int* flags, cudaStream_t st);
+// Repopulation after adapt: op kind 0 copy old slot, 1 interpolate2fine from old parent (igrid),
+// 2 average2coarse from 4 old children (src = first child slot; children consecutive by igrid
+// via child_slots).
+struct RepopOp { int kind, dst, src, igrid; int child[4]; };
+void launch_repop(const Dims& d, const RepopOp* ops, int nops, const double* oq, double* nq,
+                  const double* oqlast, double* nqlast, const double* oqi, double* nqi,
+                  const double* oregs, double* nregs, cudaStream_t st);
+
+}  // namespace fcb

@@ -1,0 +1,158 @@
+/*
+ * fc2d_b200.h -- C ABI of the B200 (sm_100a) clawpack 4.6 patch-update package.
+ *
+ * A drop-in for ForestClaw's per-patch wave-propagation update, the ghost fill
+ * around it and the conservative fine/coarse correction.  All leaf patches of a
+ * forest live in device memory in level-major slabs; the entry points below are
+ * the batched equivalents of the reference's patch / clawpatch / clawpack46
+ * vtable calls.  Every function returns 0 on success and a negative
+ * FC2D_B200_E* code on failure; fc2d_b200_last_error() describes the failure.
+ *
+ * Host arrays of patch data use the reference's FArrayBox layout per patch
+ * (fclaw2d_clawpatch.hpp:46-81; Fortran order q(1-mbc:mx+mbc, 1-mbc:my+mbc, meqn)),
+ * patches concatenated in level-major order (level, then block, then Morton
+ * order within the block).
+ */
+#ifndef FC2D_B200_H
+#define FC2D_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FC2D_B200_OK          0
+#define FC2D_B200_EINVAL     -1   /* bad argument or option combination */
+#define FC2D_B200_ECUDA      -2   /* CUDA runtime error */
+#define FC2D_B200_ESTATE     -3   /* call made in the wrong state */
+#define FC2D_B200_EDEVICE    -4   /* device status word reported a kernel-side failure */
+#define FC2D_B200_EFOREST    -5   /* forest is not 2:1 balanced / adapt failed */
+
+/* Riemann solvers compiled into the package as __device__ functions.  They are
+ * registered by id, the way cudaclaw apps register __device__ function pointers
+ * (fc2d_cudaclaw.h:156-162, fc2d_cudaclaw_cuda.h:52-73); the ids select a
+ * compile-time specialisation of the fused update so the solver inlines. */
+#define FC2D_B200_RP_ADVECTION   0   /* clawpack46_rpn2adv.f / clawpack46_rpt2adv.f */
+#define FC2D_B200_RP_SW_ROE      1   /* shallow/2d/rp/clawpack46_rpn2.f / clawpack46_rpt2.f (Roe + HH fix) */
+#define FC2D_B200_RP_SW_FWAVE    2   /* shallow/2d/rp/rpn2_tsunami.f90 / rpt2_tsunami.f90 (f-waves, bathymetry) */
+
+/* Built-in application callbacks (qinit / setaux / b4step2 / tagging). */
+#define FC2D_B200_APP_NONE       0   /* q and aux supplied by the caller */
+#define FC2D_B200_APP_SWIRL      1   /* advection/2d/swirl */
+#define FC2D_B200_APP_RADIALDAM  2   /* shallow/2d/radialdam (cell-centre disc) */
+#define FC2D_B200_APP_TSUNAMI    3   /* bathymetry + Gaussian bumps */
+
+/* Arithmetic of the update kernel. */
+#define FC2D_B200_PREC_FP64      0   /* FP64 throughout, no FMA contraction (bitwise with the FP64 CPU path) */
+#define FC2D_B200_PREC_FP32WAVE  1   /* FP32 waves/limiter/transverse, FP64 q accumulation */
+
+typedef struct fc2d_b200_options {
+    /* clawpatch options (fclaw2d_clawpatch_options.c) */
+    int mx, my, mbc, meqn, maux;
+    /* clawpack46 options (fc2d_clawpack46_options.c:37-99) */
+    int mwaves;
+    int order[2];          /* method(2), method(3) */
+    int mthlim[8];
+    int mthbc[4];
+    int mcapa;
+    int use_fwaves;
+    int rp;                /* FC2D_B200_RP_* */
+    /* forest / time stepping options (fclaw_options.c:93-220) */
+    int minlevel, maxlevel;
+    int subcycle;
+    int time_sync, flux_correction, fluctuation_correction;
+    double refine_threshold, coarsen_threshold;
+    double ax, bx, ay, by;
+    int mi, mj;            /* brick of mi x mj equally oriented blocks */
+    /* application */
+    int app;               /* FC2D_B200_APP_* */
+    double grav, tperiod;
+    double r0, hin, hout, x0, y0;
+    double pdata[32];
+    /* B200 specifics */
+    int precision;         /* FC2D_B200_PREC_* */
+    int device;            /* CUDA device ordinal */
+} fc2d_b200_options_t;
+
+typedef struct fc2d_b200_solver fc2d_b200_solver_t;
+
+/* Last error message of the calling thread. */
+const char* fc2d_b200_last_error(void);
+
+/* Solver package lifetime.  Replaces fc2d_clawpack46_solver_initialize
+ * (fc2d_clawpack46.cpp:483-538) + clawpatch allocation (fclaw2d_clawpatch.cpp:192-471). */
+int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver_t** out);
+int fc2d_b200_destroy(fc2d_b200_solver_t* s);
+
+/* Select the registered __device__ Riemann pair (vt->fort_rpn2 / fort_rpt2,
+ * fc2d_clawpack46.h:161-188; cudaclaw's cuda_rpn2 / cuda_rpt2). */
+int fc2d_b200_set_riemann(fc2d_b200_solver_t* s, int rp_id);
+
+/* fclaw2d_initialize (src/fclaw2d_initialize.c:75-250): uniform forest at minlevel,
+ * setaux + qinit, then the initial-refinement loop.  Needs app != NONE. */
+int fc2d_b200_initialize(fc2d_b200_solver_t* s);
+
+/* Install an externally built forest (e.g. p4est leaves): level and
+ * brick-global integer coordinates of each leaf, any order.  Patch data is zero
+ * until fc2d_b200_set_q / fc2d_b200_set_aux. */
+int fc2d_b200_set_forest(fc2d_b200_solver_t* s, int npatches, const int* level, const int* gx, const int* gy);
+
+int fc2d_b200_num_patches(const fc2d_b200_solver_t* s, int* npatches);
+/* level, block, brick-global gx, gy of each patch in level-major order. */
+int fc2d_b200_patch_info(const fc2d_b200_solver_t* s, int* level, int* block, int* gx, int* gy);
+
+/* Host <-> device copies of all patches (level-major FArrayBox layout). */
+int fc2d_b200_get_q(fc2d_b200_solver_t* s, double* q);
+int fc2d_b200_set_q(fc2d_b200_solver_t* s, const double* q);
+int fc2d_b200_get_aux(fc2d_b200_solver_t* s, double* aux);
+int fc2d_b200_set_aux(fc2d_b200_solver_t* s, const double* aux);
+/* Conservation registers per patch: fp0 fp1 fm0 fm1 (my*meqn each), gp0 gp1
+ * gm0 gm1 (mx*meqn each), edge fluxes 0..3 (2*{my,my,mx,mx}*meqn)
+ * (fclaw2d_clawpatch_conservation.h:56-77). */
+int fc2d_b200_registers_size(const fc2d_b200_solver_t* s, int* ndoubles_per_patch);
+int fc2d_b200_get_registers(fc2d_b200_solver_t* s, double* regs);
+
+/* Batched patch_vt->single_step_update for every patch of `level`
+ * (fclaw2d_patch_single_step_update_t, src/fclaw2d_patch.h:937-943, called from
+ * src/fclaw2d_update_single_step.c:44-70; clawpack46_update,
+ * fc2d_clawpack46.cpp:402-444).  Includes b4step2, save_current_step,
+ * time-sync flux/wave accumulation and the q update.  *cfl = level max CFL. */
+int fc2d_b200_level_update(fc2d_b200_solver_t* s, int level, double t, double dt, double* cfl);
+
+/* The cudaclaw buffering protocol (fc2d_cudaclaw.cpp:309-349) with plain types:
+ * call once per patch of `level` with iter = 0..total_count-1; the launch
+ * happens on the last call, which returns the level CFL in *cfl (0 before). */
+int fc2d_b200_single_step_update(fc2d_b200_solver_t* s, int level, int iter, int total_count,
+                                 double t, double dt, double* cfl);
+
+/* fclaw2d_ghost_update (src/fclaw2d_ghost_fill.c:838-856). */
+int fc2d_b200_ghost_update(fc2d_b200_solver_t* s, int minlevel, int maxlevel, double sync_time, int time_interp);
+/* fclaw2d_timeinterp (src/fclaw2d_timeinterp.c:49-57). */
+int fc2d_b200_timeinterp(fc2d_b200_solver_t* s, int level, double alpha);
+/* fclaw2d_time_sync (src/fclaw2d_time_sync.c:157-202). */
+int fc2d_b200_time_sync(fc2d_b200_solver_t* s, int minlevel, int maxlevel);
+/* fclaw2d_advance_all_levels (src/fclaw2d_advance.c:247-357). */
+int fc2d_b200_advance(fc2d_b200_solver_t* s, double t, double dt, double* maxcfl);
+/* fclaw2d_regrid (src/fclaw2d_regrid.c:230-335): device tagging, host tree edit,
+ * device repopulation, ghost update.  *changed = 1 if the forest changed. */
+int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed);
+
+/* Kahan-summed mass per field over interior cells, FP64
+ * (fclaw2d_clawpatch46_diagnostics.f:13-55). */
+int fc2d_b200_mass(fc2d_b200_solver_t* s, double* out);
+/* Interior cell updates performed so far (sum over levels of patches*mx*my per step). */
+int fc2d_b200_cell_updates(const fc2d_b200_solver_t* s, double* out);
+/* Wait for all device work of the solver's stream. */
+int fc2d_b200_synchronize(fc2d_b200_solver_t* s);
+
+/* Device kernel timing of the most recent fc2d_b200_advance: milliseconds spent
+ * in the update kernels and the bytes they moved algorithmically (interior
+ * cells, q read + write + aux read). */
+int fc2d_b200_last_update_stats(const fc2d_b200_solver_t* s, double* update_ms, double* update_bytes,
+                                int* update_launches, int* total_launches);
+/* Enable/disable CUDA-event timing of the update kernels (off by default). */
+int fc2d_b200_set_timing(fc2d_b200_solver_t* s, int enable);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

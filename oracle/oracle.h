@@ -1,0 +1,115 @@
+/*
+ * oracle.h -- CPU FP64 oracle for the ForestClaw clawpack 4.6 patch-update hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is a plain-C restatement of the
+ * reference's Fortran/C algorithms (clawpack46 step2/flux2/limiter, the
+ * clawpatch 4.6 ghost-fill kernels, time-sync, the level/ghost-fill/time-sync
+ * orchestration).  It is the checker the CUDA product is compared against and
+ * the timed CPU baseline; the product never links, loads or calls it.
+ *
+ * Parity status: the reference's hot path is Fortran and cannot be compiled in
+ * this environment (no Fortran compiler; p4est/libsc are empty submodules), and
+ * the reference's own tests pin no field values.  Parity of this oracle against
+ * the reference is therefore "parity unpinned": it rests on line-by-line review
+ * against the cited Fortran plus mathematical known-answer tests (constant-state
+ * preservation, exact translation at CFL 1, conservation, symmetry).
+ *
+ * Floating-point semantics: every expression is evaluated left to right in the
+ * Fortran order of the cited line, without FMA contraction
+ * (-ffp-contract=off), so that a no-contraction FP64 GPU kernel can match it
+ * bit for bit.
+ */
+#ifndef FCB_ORACLE_H
+#define FCB_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Riemann solver identifiers (mirrors the user solvers of the reference apps). */
+enum {
+    ORC_RP_ADVECTION = 0,     /* applications/clawpack/advection/2d/all/clawpack46_rpn2adv.f, rpt2adv.f */
+    ORC_RP_SW_ROE = 1,        /* applications/clawpack/shallow/2d/rp/clawpack46_rpn2.f, clawpack46_rpt2.f */
+    ORC_RP_SW_FWAVE = 2,      /* applications/clawpack/shallow/2d/rp/rpn2_tsunami.f90, rpt2_tsunami.f90 */
+    ORC_RP_EULER_EXACT = 3    /* build-originated exact Euler solver (no reference counterpart) */
+};
+
+/* Problem (app) identifiers: qinit/b4step2/setprob of the reference apps. */
+enum {
+    ORC_PROB_SWIRL = 0,       /* applications/clawpack/advection/2d/swirl */
+    ORC_PROB_RADIALDAM = 1,   /* applications/clawpack/shallow/2d/radialdam */
+    ORC_PROB_UNIFORM_SW = 2,  /* radial dam initial data on a uniform grid (same app) */
+    ORC_PROB_TSUNAMI = 3      /* batched bathymetry problem (rpn2_tsunami) */
+};
+
+typedef struct orc_config {
+    /* clawpatch options (fclaw2d_clawpatch_options.c) */
+    int mx, my, mbc, meqn, maux;
+    /* clawpack46 options (fc2d_clawpack46_options.c:37-99) */
+    int mwaves;
+    int order[2];          /* method(2), method(3) */
+    int mthlim[8];
+    int mthbc[4];
+    int mcapa;
+    int use_fwaves;
+    int rp;                /* ORC_RP_* */
+    /* fclaw options (fclaw_options.c) */
+    int minlevel, maxlevel;
+    int subcycle;
+    int time_sync, flux_correction, fluctuation_correction;
+    int regrid_interval;
+    double refine_threshold, coarsen_threshold;
+    double ax, bx, ay, by;
+    int mi, mj;            /* brick blocks; 1x1 = single block */
+    /* problem */
+    int problem;           /* ORC_PROB_* */
+    double grav;
+    double tperiod;        /* swirl time period T */
+    double r0, hin, hout, x0, y0;   /* radial dam */
+    int qinit_sharp;       /* 1: cell-centre test instead of cellave2 quadrature */
+    double pdata[32];      /* extra problem parameters (tsunami bumps etc.) */
+    int nthreads;          /* OpenMP threads for the patch loops (0 = default) */
+} orc_config;
+
+typedef struct orc_sim orc_sim;
+
+orc_sim* orc_create(const orc_config* cfg);
+void     orc_destroy(orc_sim* s);
+
+/* Uniform forest at minlevel + qinit (+ init-regrid when maxlevel > minlevel). */
+int    orc_initialize(orc_sim* s);
+/* fclaw2d_advance_all_levels (src/fclaw2d_advance.c:247-357); returns max CFL. */
+double orc_advance(orc_sim* s, double t, double dt);
+/* fclaw2d_regrid (src/fclaw2d_regrid.c). Returns 1 if the forest changed. */
+int    orc_regrid(orc_sim* s);
+/* Ghost update over all levels at sync time t (time_interp = 0). */
+void   orc_ghost_update_all(orc_sim* s, double t);
+
+int    orc_num_patches(const orc_sim* s);
+/* Patches in level-major order: level, block, ix, iy (integer coordinates at the patch level). */
+void   orc_patch_info(const orc_sim* s, int* level, int* block, int* ix, int* iy);
+/* Copy q (Fortran layout, ghosts included) of all patches in level-major order. */
+void   orc_get_q(const orc_sim* s, double* out);
+void   orc_set_q(orc_sim* s, const double* in);
+void   orc_get_aux(const orc_sim* s, double* out);
+/* Kahan-summed mass per field (fclaw2d_clawpatch46_diagnostics.f:13-55). */
+void   orc_mass(const orc_sim* s, double* out);
+/* Number of interior cell updates performed so far. */
+double orc_cell_updates(const orc_sim* s);
+/* Registers of all patches (for tests): per patch 4*? doubles, see orc_registers_size. */
+int    orc_registers_size(const orc_sim* s);
+void   orc_get_registers(const orc_sim* s, double* out);
+
+/* ---- single-patch numerics, exposed for unit tests ---------------------- */
+/* clawpack46_step2_wrap on one patch: q updated in place, returns cfl.
+ * fm/fp/gm/gp (size (mx+2mbc)(my+2mbc)meqn each) receive the flux arrays. */
+double orc_patch_step2(const orc_config* cfg, double* q, const double* aux,
+                       double dx, double dy, double dt,
+                       double* fm, double* fp, double* gm, double* gp);
+/* clawpack46_inlinelimiter phi(r) for one r (tests of the limiter table). */
+double orc_limiter_phi(int mthlim, double r);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

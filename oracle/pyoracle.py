@@ -1,0 +1,202 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+The oracle is the checker the CUDA product is compared against and the timed
+CPU baseline.  Only tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg
+of ``bench.py`` import this module; the product package never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liborc.so")
+
+RP_ADVECTION, RP_SW_ROE, RP_SW_FWAVE, RP_EULER_EXACT = 0, 1, 2, 3
+PROB_SWIRL, PROB_RADIALDAM, PROB_UNIFORM_SW, PROB_TSUNAMI = 0, 1, 2, 3
+
+
+class OrcConfig(ctypes.Structure):
+    _fields_ = [
+        ("mx", ctypes.c_int), ("my", ctypes.c_int), ("mbc", ctypes.c_int),
+        ("meqn", ctypes.c_int), ("maux", ctypes.c_int),
+        ("mwaves", ctypes.c_int), ("order", ctypes.c_int * 2), ("mthlim", ctypes.c_int * 8),
+        ("mthbc", ctypes.c_int * 4), ("mcapa", ctypes.c_int), ("use_fwaves", ctypes.c_int),
+        ("rp", ctypes.c_int),
+        ("minlevel", ctypes.c_int), ("maxlevel", ctypes.c_int), ("subcycle", ctypes.c_int),
+        ("time_sync", ctypes.c_int), ("flux_correction", ctypes.c_int),
+        ("fluctuation_correction", ctypes.c_int), ("regrid_interval", ctypes.c_int),
+        ("refine_threshold", ctypes.c_double), ("coarsen_threshold", ctypes.c_double),
+        ("ax", ctypes.c_double), ("bx", ctypes.c_double), ("ay", ctypes.c_double), ("by", ctypes.c_double),
+        ("mi", ctypes.c_int), ("mj", ctypes.c_int),
+        ("problem", ctypes.c_int), ("grav", ctypes.c_double), ("tperiod", ctypes.c_double),
+        ("r0", ctypes.c_double), ("hin", ctypes.c_double), ("hout", ctypes.c_double),
+        ("x0", ctypes.c_double), ("y0", ctypes.c_double), ("qinit_sharp", ctypes.c_int),
+        ("pdata", ctypes.c_double * 32), ("nthreads", ctypes.c_int),
+    ]
+
+
+def build(force: bool = False) -> str:
+    """Compile liborc.so from the sources beside this file (make)."""
+    if force or not os.path.exists(_LIB):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB)
+        P = ctypes.c_void_p
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.orc_create.restype = P
+        L.orc_create.argtypes = [ctypes.POINTER(OrcConfig)]
+        L.orc_destroy.argtypes = [P]
+        L.orc_initialize.argtypes = [P]
+        L.orc_advance.restype = ctypes.c_double
+        L.orc_advance.argtypes = [P, ctypes.c_double, ctypes.c_double]
+        L.orc_regrid.argtypes = [P]
+        L.orc_ghost_update_all.argtypes = [P, ctypes.c_double]
+        L.orc_num_patches.argtypes = [P]
+        L.orc_patch_info.argtypes = [P, ip, ip, ip, ip]
+        L.orc_get_q.argtypes = [P, dp]
+        L.orc_set_q.argtypes = [P, dp]
+        L.orc_get_aux.argtypes = [P, dp]
+        L.orc_mass.argtypes = [P, dp]
+        L.orc_cell_updates.restype = ctypes.c_double
+        L.orc_cell_updates.argtypes = [P]
+        L.orc_registers_size.argtypes = [P]
+        L.orc_get_registers.argtypes = [P, dp]
+        L.orc_patch_step2.restype = ctypes.c_double
+        L.orc_patch_step2.argtypes = [ctypes.POINTER(OrcConfig), dp, dp, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, dp, dp, dp, dp]
+        L.orc_limiter_phi.restype = ctypes.c_double
+        L.orc_limiter_phi.argtypes = [ctypes.c_int, ctypes.c_double]
+        _lib = L
+    return _lib
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def make_config(**kw) -> OrcConfig:
+    c = OrcConfig()
+    defaults = dict(mx=16, my=16, mbc=2, meqn=1, maux=0, mwaves=1, mcapa=0, use_fwaves=0, rp=0,
+                    minlevel=0, maxlevel=0, subcycle=0, time_sync=0, flux_correction=1,
+                    fluctuation_correction=1, regrid_interval=0, refine_threshold=0.5,
+                    coarsen_threshold=0.1, ax=0.0, bx=1.0, ay=0.0, by=1.0, mi=1, mj=1,
+                    problem=0, grav=1.0, tperiod=0.0, r0=0.3, hin=2.0, hout=1.0, x0=0.0, y0=0.0,
+                    qinit_sharp=1, nthreads=0)
+    defaults.update(kw)
+    order = defaults.pop("order", (2, 2))
+    mthlim = defaults.pop("mthlim", (4,) * 8)
+    mthbc = defaults.pop("mthbc", (1, 1, 1, 1))
+    pdata = defaults.pop("pdata", ())
+    for k, v in defaults.items():
+        setattr(c, k, v)
+    for i, v in enumerate(order):
+        c.order[i] = v
+    for i, v in enumerate(mthlim):
+        c.mthlim[i] = v
+    for i, v in enumerate(mthbc):
+        c.mthbc[i] = v
+    for i, v in enumerate(pdata):
+        c.pdata[i] = v
+    return c
+
+
+class OracleSim:
+    """One oracle simulation: a forest of patches advanced on the host cores."""
+
+    def __init__(self, cfg: OrcConfig):
+        self.cfg = cfg
+        self._cfg_ref = ctypes.byref(cfg)
+        self.h = lib().orc_create(self._cfg_ref)
+        self.nx = cfg.mx + 2 * cfg.mbc
+        self.ny = cfg.my + 2 * cfg.mbc
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    def initialize(self) -> int:
+        return lib().orc_initialize(self.h)
+
+    def advance(self, t: float, dt: float) -> float:
+        return lib().orc_advance(self.h, t, dt)
+
+    def regrid(self) -> int:
+        return lib().orc_regrid(self.h)
+
+    def ghost_update(self, t: float) -> None:
+        lib().orc_ghost_update_all(self.h, t)
+
+    @property
+    def num_patches(self) -> int:
+        return lib().orc_num_patches(self.h)
+
+    def patch_info(self) -> np.ndarray:
+        n = self.num_patches
+        arrs = [np.zeros(n, np.int32) for _ in range(4)]
+        lib().orc_patch_info(self.h, *[_iptr(a) for a in arrs])
+        return np.stack(arrs, axis=1)   # level, block, gx, gy
+
+    def get_q(self) -> np.ndarray:
+        n = self.num_patches
+        out = np.zeros((n, self.cfg.meqn, self.ny, self.nx), np.float64)
+        lib().orc_get_q(self.h, _dptr(out))
+        return out
+
+    def set_q(self, q: np.ndarray) -> None:
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        lib().orc_set_q(self.h, _dptr(q))
+
+    def get_aux(self) -> np.ndarray:
+        n = self.num_patches
+        out = np.zeros((n, max(self.cfg.maux, 0), self.ny, self.nx), np.float64)
+        lib().orc_get_aux(self.h, _dptr(out))
+        return out
+
+    def get_registers(self) -> np.ndarray:
+        n = self.num_patches
+        sz = lib().orc_registers_size(self.h)
+        out = np.zeros((n, sz), np.float64)
+        lib().orc_get_registers(self.h, _dptr(out))
+        return out
+
+    def mass(self) -> np.ndarray:
+        out = np.zeros(self.cfg.meqn, np.float64)
+        lib().orc_mass(self.h, _dptr(out))
+        return out
+
+    @property
+    def cell_updates(self) -> float:
+        return lib().orc_cell_updates(self.h)
+
+
+def patch_step2(cfg: OrcConfig, q: np.ndarray, aux, dx: float, dy: float, dt: float):
+    """clawpack46_step2_wrap on one patch (q updated in place); returns cfl, fm, fp, gm, gp."""
+    n = q.size
+    fm, fp, gm, gp = (np.zeros(n) for _ in range(4))
+    a = aux if aux is not None else np.zeros(1)
+    cfl = lib().orc_patch_step2(ctypes.byref(cfg), _dptr(q), _dptr(a), dx, dy, dt,
+                                _dptr(fm), _dptr(fp), _dptr(gm), _dptr(gp))
+    return cfl, fm, fp, gm, gp
+
+
+def limiter_phi(mthlim: int, r: float) -> float:
+    return lib().orc_limiter_phi(mthlim, r)
