@@ -148,6 +148,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_synchronize": [P],
         "fc2d_b200_last_update_stats": [P, dp, dp, ip, ip],
         "fc2d_b200_set_timing": [P, I],
+        "fc2d_b200_event_record": [P, I],
+        "fc2d_b200_event_elapsed": [P, I, I, dp],
+        "fc2d_b200_get_stream": [P, ctypes.POINTER(P)],
+        "fc2d_b200_set_graphs": [P, I],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -295,8 +299,31 @@ class Solver:
     def synchronize(self) -> None:
         self._check("fc2d_b200_synchronize", self.lib.fc2d_b200_synchronize(self.h))
 
+    def set_graphs(self, on: bool) -> None:
+        self._check("fc2d_b200_set_graphs", self.lib.fc2d_b200_set_graphs(self.h, int(on)))
+
     def set_timing(self, on: bool) -> None:
         self._check("fc2d_b200_set_timing", self.lib.fc2d_b200_set_timing(self.h, int(on)))
+
+    def event_record(self, slot: int) -> None:
+        self._check("fc2d_b200_event_record", self.lib.fc2d_b200_event_record(self.h, slot))
+
+    def event_elapsed(self, a: int, b: int) -> float:
+        ms = ctypes.c_double()
+        self._check("fc2d_b200_event_elapsed", self.lib.fc2d_b200_event_elapsed(self.h, a, b, ctypes.byref(ms)))
+        return ms.value
+
+    def stream_handle(self) -> int:
+        p = ctypes.c_void_p()
+        self._check("fc2d_b200_get_stream", self.lib.fc2d_b200_get_stream(self.h, ctypes.byref(p)))
+        return p.value or 0
+
+    def set_q_ptr(self, ptr: int) -> None:
+        """set_q from a raw host pointer (e.g. pinned memory)."""
+        self._check("fc2d_b200_set_q", self.lib.fc2d_b200_set_q(self.h, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double))))
+
+    def get_q_ptr(self, ptr: int) -> None:
+        self._check("fc2d_b200_get_q", self.lib.fc2d_b200_get_q(self.h, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double))))
 
     def last_update_stats(self) -> dict:
         ms, by = ctypes.c_double(), ctypes.c_double()

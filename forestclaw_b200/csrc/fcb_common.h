@@ -12,8 +12,10 @@ struct PatchDesc {
     int level;
     int phys_mask;
     int face_type;      // 2 bits per face: 0 boundary, 1 half (finer nbr), 2 same, 3 double (coarser nbr)
-    int pad;
+    int flags;          // PATCH_* bits
 };
+
+enum { PATCH_HAS_FINE_NBR = 1 };   // a face or corner neighbour is finer (fclaw2d_patch.c:980-1034)
 
 // Parameters of one level update launch (clawpack46 method flags and the
 // per-step scalars the reference passes through common blocks).

@@ -22,11 +22,11 @@
 
 namespace fcb {
 cudaError_t launch_step2_f64(int rp, const Dims& d, double* q, double* qlast, const double* aux, double* regs,
-                             const PatchDesc* desc, int p0, int npatch, const StepParams& sp,
+                             const PatchDesc* desc, int p0, int npatch, const StepParams* sp,
                              unsigned long long* cfl_bits, cudaStream_t st);
 bool step2_f64_supported(int rp, int mx, int my, int mbc);
 cudaError_t launch_step2_f32w(int rp, const Dims& d, double* q, double* qlast, const double* aux, double* regs,
-                              const PatchDesc* desc, int p0, int npatch, const StepParams& sp,
+                              const PatchDesc* desc, int p0, int npatch, const StepParams* sp,
                               unsigned long long* cfl_bits, cudaStream_t st);
 bool step2_f32w_supported(int rp, int mx, int my, int mbc);
 }  // namespace fcb
@@ -97,7 +97,26 @@ struct fc2d_b200_solver {
     std::vector<std::pair<int, double>> upd_launch_bytes;   // (event index, algorithmic bytes)
     double upd_ms = 0, upd_bytes = 0;
     int upd_launches = 0, total_launches = 0;
+    std::vector<cudaEvent_t> user_ev;
+    // per-launch update parameters in device memory (filled each advance)
+    static constexpr int PCAP = 1 << 14;
+    StepParams* params_dev = nullptr;
+    StepParams* params_host = nullptr;
+    int n_upd = 0;
+    bool emit = true;                              // false: host traversal only (fill parameters)
+    bool fill = true;                              // fill params_host / count statistics
+    // CUDA graph of one fclaw2d_advance_all_levels for the current forest
+    bool use_graphs = true;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_nupd = -1;
 };
+
+static void invalidate_graph(fc2d_b200_solver* s)
+{
+    if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+    s->graph_exec = nullptr;
+    s->graph_nupd = -1;
+}
 
 const char* fc2d_b200_last_error(void) { return g_err.c_str(); }
 
@@ -143,6 +162,7 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
         int ft = 0;
         for (int k = 0; k < 4; k++) ft |= (P.face_type[k] & 3) << (2 * k);
         pd.face_type = ft;
+        pd.flags = P.has_fine_nbr ? PATCH_HAS_FINE_NBR : 0;
         hd[i] = pd;
     }
     if (!hd.empty()) CK(cudaMemcpyAsync(s->desc, hd.data(), hd.size() * sizeof(PatchDesc), cudaMemcpyHostToDevice, s->st));
@@ -165,10 +185,10 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
         r.ti_off = (int)ti.size(); r.ti_n = (int)L.ti.size(); ti.insert(ti.end(), L.ti.begin(), L.ti.end());
         r.ss_off = (int)ss.size(); r.ss_start_off = (int)ss_start.size(); r.ss_np = (int)L.ss_start.size() - 1;
         ss.insert(ss.end(), L.ss.begin(), L.ss.end());
-        ss_start.insert(ss_start.end(), L.ss_start.begin(), L.ss_start.end());
+        for (int v : L.ss_start) ss_start.push_back(v + r.ss_off);
         r.f2c_off = (int)f2c.size(); r.f2c_start_off = (int)f2c_start.size(); r.f2c_np = (int)L.f2c_start.size() - 1;
         f2c.insert(f2c.end(), L.f2c.begin(), L.f2c.end());
-        f2c_start.insert(f2c_start.end(), L.f2c_start.begin(), L.f2c_start.end());
+        for (int v : L.f2c_start) f2c_start.push_back(v + r.f2c_off);
     }
     CK(s->t_copy.assign(copy, s->st));
     CK(s->t_avg.assign(avg, s->st));
@@ -202,13 +222,19 @@ static int update_level(fc2d_b200_solver* s, int level, double t, double dt)
     if (level < 0 || level > 32) return 0;
     const int p0 = f.lev_off[level], np = f.lev_off[level + 1] - p0;
     if (np <= 0) return 0;
-    StepParams sp{};
+    if (s->n_upd >= fc2d_b200_solver::PCAP) return fail(FC2D_B200_EINVAL, "too many level updates in one advance");
+    const StepParams* spd = s->params_dev + s->n_upd;
+    StepParams& sp = s->params_host[s->n_upd];
+    s->n_upd++;
+    if (!s->fill) goto launch;
+    sp = StepParams{};
     sp.order1 = s->o.order[0]; sp.order2 = s->o.order[1];
     for (int k = 0; k < 8; k++) sp.mthlim[k] = s->o.mthlim[k];
     sp.mcapa = s->o.mcapa;
     sp.store_flux = s->o.time_sync && s->o.flux_correction;
     sp.accumulate_waves = s->o.time_sync && s->o.fluctuation_correction;
-    sp.save_last = 1;
+    // save_current_step is only read by time interpolation of the coarser levels
+    sp.save_last = (s->o.subcycle && level < f.maxlevel_present) ? 1 : 0;
     sp.app = s->o.app;
     sp.dt = dt; sp.t = t; sp.grav = s->o.grav;
     sp.dry_tolerance = s->o.pdata[31] > 0 ? s->o.pdata[31] : 1e-3;
@@ -217,13 +243,19 @@ static int update_level(fc2d_b200_solver* s, int level, double t, double dt)
         const double pi = 4.0 * std::atan(1.0), pi2 = 2.0 * pi;
         sp.vt = std::cos(pi2 * (t + dt / 2.0) / s->o.tperiod);
     }
+    s->cell_updates += (double)np * s->d.mx * s->d.my;
+    s->upd_launches++;
+    s->total_launches++;
+    if (s->emit) CK(cudaMemcpyAsync((void*)spd, &sp, sizeof(StepParams), cudaMemcpyHostToDevice, s->st));
+launch:
+    if (!s->emit) return 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (s->timing) { e0 = next_event(s); e1 = next_event(s); CK(cudaEventRecord(e0, s->st)); }
     cudaError_t e;
     if (s->o.precision == FC2D_B200_PREC_FP32WAVE)
-        e = launch_step2_f32w(s->o.rp, s->d, s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, sp, s->cfl_dev, s->st);
+        e = launch_step2_f32w(s->o.rp, s->d, s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, spd, s->cfl_dev, s->st);
     else
-        e = launch_step2_f64(s->o.rp, s->d, s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, sp, s->cfl_dev, s->st);
+        e = launch_step2_f64(s->o.rp, s->d, s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, spd, s->cfl_dev, s->st);
     if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("step2 launch: ") + cudaGetErrorString(e));
     if (s->timing) {
         CK(cudaEventRecord(e1, s->st));
@@ -231,99 +263,114 @@ static int update_level(fc2d_b200_solver* s, int level, double t, double dt)
         const double bytes = cells * 8.0 * (2.0 * s->d.meqn + s->d.maux);
         s->upd_launch_bytes.push_back({s->ev_used - 2, bytes});
     }
-    s->upd_launches++;
-    s->total_launches++;
-    s->cell_updates += (double)np * s->d.mx * s->d.my;
     return 0;
 }
 
 static double* tsdata(fc2d_b200_solver* s, int ti) { return ti ? s->qinterp : s->q; }
 
-static void copy2ghost(fc2d_b200_solver* s, int l, int ti)
+// Stage launches over a range of levels [a, b]: the per-level tables are laid
+// out level after level, so a range is one contiguous slice.  Copy, average and
+// physical-BC stages of different levels touch disjoint cells and read no cell
+// the same stage writes, so a range is one launch; interpolation stays one
+// launch per level (coarser levels overwrite ghost cells the finer level's
+// interpolation reads first, as in the reference's max-to-min level loop).
+static bool lrange(int& a, int& b)
 {
-    if (l < 0 || l > 32 || !s->lr[l].copy_n) return;
-    launch_copy(s->d, tsdata(s, ti), tsdata(s, ti), s->t_copy.p + s->lr[l].copy_off, s->lr[l].copy_n, s->st);
-    s->total_launches++;
+    if (a < 0) a = 0;
+    if (b > 32) b = 32;
+    return a <= b;
 }
-static void average2ghost(fc2d_b200_solver* s, int l, int ti)
+static void copy_range(fc2d_b200_solver* s, int a, int b, int ti)
 {
-    if (l < 0 || l > 32 || !s->lr[l].avg_n) return;
-    launch_average(s->d, tsdata(s, ti), s->q, s->t_avg.p + s->lr[l].avg_off, s->lr[l].avg_n, s->st);
-    s->total_launches++;
+    if (!lrange(a, b)) return;
+    const int off = s->lr[a].copy_off, n = s->lr[b].copy_off + s->lr[b].copy_n - off;
+    if (n <= 0) return;
+    if (s->fill) s->total_launches++;
+    if (s->emit) launch_copy(s->d, tsdata(s, ti), tsdata(s, ti), s->t_copy.p + off, n, s->st);
+}
+static void average_range(fc2d_b200_solver* s, int a, int b, int ti)
+{
+    if (!lrange(a, b)) return;
+    const int off = s->lr[a].avg_off, n = s->lr[b].avg_off + s->lr[b].avg_n - off;
+    if (n <= 0) return;
+    if (s->fill) s->total_launches++;
+    if (s->emit) launch_average(s->d, tsdata(s, ti), s->q, s->t_avg.p + off, n, s->st);
+}
+static void phys_range(fc2d_b200_solver* s, int a, int b, int ti)
+{
+    if (!lrange(a, b)) return;
+    const int off = s->lr[a].phys_off, n = s->lr[b].phys_off + s->lr[b].phys_n - off;
+    if (n <= 0) return;
+    if (s->fill) s->total_launches++;
+    if (s->emit) launch_phys(s->d, tsdata(s, ti), s->t_phys.p + off, n, s->st);
 }
 static void interpolate2ghost(fc2d_b200_solver* s, int l, int ti)
 {
     if (l < 0 || l > 32 || !s->lr[l].interp_n) return;
-    launch_interp(s->d, s->q, tsdata(s, ti), s->t_interp.p + s->lr[l].interp_off, s->lr[l].interp_n, s->st);
-    s->total_launches++;
-}
-static void setphysical(fc2d_b200_solver* s, int l, int ti)
-{
-    if (l < 0 || l > 32 || !s->lr[l].phys_n) return;
-    launch_phys(s->d, tsdata(s, ti), s->t_phys.p + s->lr[l].phys_off, s->lr[l].phys_n, s->st);
-    s->total_launches++;
+    if (s->fill) s->total_launches++;
+    if (s->emit)
+        launch_interp(s->d, s->q, tsdata(s, ti), s->t_interp.p + s->lr[l].interp_off, s->lr[l].interp_n, s->st);
 }
 
 static void ghost_update(fc2d_b200_solver* s, int minlevel, int maxlevel, int time_interp)
 {
     const int mincoarse = minlevel, maxcoarse = maxlevel - 1;
-    for (int l = maxcoarse; l >= mincoarse; l--) average2ghost(s, l, 0);
-    if (time_interp) average2ghost(s, mincoarse - 1, 1);
-    for (int l = maxlevel; l >= minlevel; l--) copy2ghost(s, l, 0);
-    if (time_interp) copy2ghost(s, minlevel - 1, 1);
-    for (int l = maxcoarse; l >= mincoarse; l--) setphysical(s, l, 0);
-    if (time_interp) setphysical(s, mincoarse - 1, 1);
+    average_range(s, mincoarse, maxcoarse, 0);
+    if (time_interp) average_range(s, mincoarse - 1, mincoarse - 1, 1);
+    copy_range(s, minlevel, maxlevel, 0);
+    if (time_interp) copy_range(s, minlevel - 1, minlevel - 1, 1);
+    phys_range(s, mincoarse, maxcoarse, 0);
+    if (time_interp) phys_range(s, mincoarse - 1, mincoarse - 1, 1);
     for (int l = maxcoarse; l >= mincoarse; l--) interpolate2ghost(s, l, 0);
     if (time_interp) interpolate2ghost(s, mincoarse - 1, 1);
     const int minfine = mincoarse + 1, maxfine = maxlevel;
-    for (int l = maxfine; l >= minfine; l--) setphysical(s, l, 0);
-    if (time_interp) setphysical(s, minfine - 1, 1);
-    for (int l = maxlevel; l >= minlevel; l--) setphysical(s, l, 0);
-    if (time_interp) setphysical(s, minlevel - 1, 1);
+    phys_range(s, minfine, maxfine, 0);
+    if (time_interp) phys_range(s, minfine - 1, minfine - 1, 1);
+    phys_range(s, minlevel, maxlevel, 0);
+    if (time_interp) phys_range(s, minlevel - 1, minlevel - 1, 1);
 }
 
-static void reset_level(fc2d_b200_solver* s, int coarse_level, int mode)
-{
-    const Forest& f = s->forest;
-    if (coarse_level < 0 || coarse_level > 32) return;
-    const int p0 = f.lev_off[coarse_level];
-    const int hi = (mode == 1) ? std::min(coarse_level + 2, 33) : coarse_level + 1;
-    const int np = f.lev_off[hi] - p0;
-    if (np <= 0) return;
-    launch_reset(s->d, s->regs, s->desc, p0, np, coarse_level, mode, s->st);
-    s->total_launches++;
-}
-
+// fclaw2d_time_sync(minlevel, maxlevel) as three launches: the same-size
+// corrections of every synced level, the fine-to-coarse corrections of every
+// synced coarse level, then every register reset.  Per level the reference runs
+// samesize, reset, f2c, reset; the corrections of different levels touch
+// disjoint cells and read only registers no earlier reset of the sync touches
+// (f2c reads half-size faces of the coarse level and double-size faces of the
+// fine level), so the merged order gives the same values.
 static void time_sync(fc2d_b200_solver* s, int minlevel, int maxlevel)
 {
     (void)maxlevel;
-    const int maxl = s->o.maxlevel;
-    for (int level = maxl; level >= minlevel; level--) {
-        if (level < 0 || level > 32) continue;
-        const LevelRanges& r = s->lr[level];
-        if (r.ss_np > 0) {
-            launch_samesize(s->d, s->q, s->regs, s->desc, s->t_ss.p + r.ss_off, s->t_ss_start.p + r.ss_start_off,
-                            r.ss_np, s->st);
-            s->total_launches++;
-        }
-        reset_level(s, level, 2);
-        if (level < maxl) {
-            if (r.f2c_np > 0) {
-                launch_f2c(s->d, s->q, s->regs, s->desc, s->t_f2c.p + r.f2c_off, s->t_f2c_start.p + r.f2c_start_off,
-                           r.f2c_np, s->st);
-                s->total_launches++;
-            }
-            reset_level(s, level, 1);
+    const int maxl = std::min(s->o.maxlevel, 32);
+    int a = std::max(minlevel, 0);
+    if (a > maxl) return;
+    {   // samesize, levels [a, maxl]
+        const int g0 = s->lr[a].ss_start_off, g1 = s->lr[maxl].ss_start_off + s->lr[maxl].ss_np;
+        if (g1 > g0) {
+            if (s->fill) s->total_launches++;
+            if (s->emit) launch_samesize(s->d, s->q, s->regs, s->desc, s->t_ss.p, s->t_ss_start.p + g0, g1 - g0, s->st);
         }
     }
-    for (int level = maxl; level >= minlevel; level--) reset_level(s, level, 3);
+    if (a <= maxl - 1) {   // f2c, coarse levels [a, maxl-1]
+        const int g0 = s->lr[a].f2c_start_off, g1 = s->lr[maxl - 1].f2c_start_off + s->lr[maxl - 1].f2c_np;
+        if (g1 > g0) {
+            if (s->fill) s->total_launches++;
+            if (s->emit) launch_f2c(s->d, s->q, s->regs, s->desc, s->t_f2c.p, s->t_f2c_start.p + g0, g1 - g0, s->st);
+        }
+    }
+    const int p0 = s->forest.lev_off[a], p1 = s->forest.lev_off[maxl + 1];
+    if (p1 > p0) {
+        if (s->fill) s->total_launches++;
+        if (s->emit) launch_reset_sync(s->d, s->regs, s->desc, p0, p1 - p0, a, maxl, s->st);
+    }
 }
 
 static void timeinterp(fc2d_b200_solver* s, int level, double alpha)
 {
     if (level < 0 || level > 32 || !s->lr[level].ti_n) return;
-    launch_timeinterp(s->d, s->q, s->qlast, s->qinterp, s->t_ti.p + s->lr[level].ti_off, s->lr[level].ti_n, alpha, s->st);
-    s->total_launches++;
+    if (s->fill) s->total_launches++;
+    if (s->emit)
+        launch_timeinterp(s->d, s->q, s->qlast, s->qinterp, s->t_ti.p + s->lr[level].ti_off, s->lr[level].ti_n, alpha,
+                          s->st);
 }
 
 struct Tsc { int last_step, step_inc, total_steps; double current_time, dt_step; };
@@ -387,6 +434,14 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
     CK(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
     CK(cudaMalloc(&s->cfl_dev, sizeof(unsigned long long)));
     CK(cudaMallocHost(&s->cfl_host, sizeof(unsigned long long)));
+    CK(cudaMalloc(&s->params_dev, sizeof(StepParams) * fc2d_b200_solver::PCAP));
+    CK(cudaMallocHost(&s->params_host, sizeof(StepParams) * fc2d_b200_solver::PCAP));
+    {   // set the kernel's shared-memory attribute outside any stream capture
+        cudaError_t e = (o.precision == FC2D_B200_PREC_FP32WAVE)
+            ? launch_step2_f32w(o.rp, s->d, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st)
+            : launch_step2_f64(o.rp, s->d, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st);
+        if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
+    }
     *out = s.release();
     return 0;
 }
@@ -396,9 +451,12 @@ extern "C" int fc2d_b200_destroy(fc2d_b200_solver_t* s)
     if (!s) return 0;
     cudaStreamSynchronize(s->st);
     for (auto e : s->ev_pool) cudaEventDestroy(e);
+    for (auto e : s->user_ev) cudaEventDestroy(e);
     cudaFree(s->q); cudaFree(s->qlast); if (s->qinterp) cudaFree(s->qinterp);
     if (s->aux) cudaFree(s->aux); cudaFree(s->regs); cudaFree(s->desc);
     cudaFree(s->cfl_dev); cudaFreeHost(s->cfl_host);
+    invalidate_graph(s);
+    cudaFree(s->params_dev); cudaFreeHost(s->params_host);
     if (s->mass_dev) cudaFree(s->mass_dev);
     cudaStreamDestroy(s->st);
     delete s;
@@ -412,12 +470,18 @@ extern "C" int fc2d_b200_set_riemann(fc2d_b200_solver_t* s, int rp_id)
                                                                  : step2_f64_supported(rp_id, s->o.mx, s->o.my, s->o.mbc);
     if (!sup) return fail(FC2D_B200_EINVAL, "Riemann solver id not compiled for these patch dimensions");
     s->o.rp = rp_id;
+    invalidate_graph(s);
+    cudaError_t e = (s->o.precision == FC2D_B200_PREC_FP32WAVE)
+        ? launch_step2_f32w(rp_id, s->d, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st)
+        : launch_step2_f64(rp_id, s->d, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st);
+    if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
     return 0;
 }
 
 // Install a new forest: slabs sized, descriptors and tables uploaded; data zero.
 static int install_forest(fc2d_b200_solver* s, const std::vector<Leaf>& leaves)
 {
+    invalidate_graph(s);
     std::string err;
     Forest nf;
     nf.g = s->forest.g;
@@ -592,6 +656,8 @@ extern "C" int fc2d_b200_level_update(fc2d_b200_solver_t* s, int level, double t
     if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
     int rc = begin_cfl(s);
     if (rc) return rc;
+    s->n_upd = 0;
+    s->emit = true; s->fill = true;
     rc = update_level(s, level, t, dt);
     if (rc) return rc;
     return end_cfl(s, cfl);
@@ -638,9 +704,9 @@ extern "C" int fc2d_b200_time_sync(fc2d_b200_solver_t* s, int minlevel, int maxl
     return 0;
 }
 
-extern "C" int fc2d_b200_advance(fc2d_b200_solver_t* s, double t, double dt, double* maxcfl)
+// One pass of fclaw2d_advance_all_levels over the current forest.
+static int traverse_advance(fc2d_b200_solver* s, double t, double dt)
 {
-    if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
     const fc2d_b200_options_t& o = s->o;
     Tsc ts[34];
     std::memset(ts, 0, sizeof(ts));
@@ -658,15 +724,10 @@ extern "C" int fc2d_b200_advance(fc2d_b200_solver_t* s, double t, double dt, dou
         const int rf = 1 << (o.maxlevel - o.minlevel);
         for (int l = o.minlevel; l <= o.maxlevel; l++) { ts[l].step_inc = 1; ts[l].dt_step = dt / rf; ts[l].total_steps = rf; }
     }
-    s->ev_used = 0;
-    s->upd_launch_bytes.clear();
-    s->upd_launches = 0;
-    s->total_launches = 0;
-    int rc = begin_cfl(s);
-    if (rc) return rc;
+    s->n_upd = 0;
     const int nfine = ts[maxlevel].total_steps;
     for (int nf = 0; nf < nfine; nf++) {
-        rc = advance_level(s, ts, maxlevel, nf);
+        int rc = advance_level(s, ts, maxlevel, nf);
         if (rc) return rc;
         if (ts[maxlevel].last_step < ts[maxlevel].total_steps) {
             if (o.subcycle) {
@@ -682,6 +743,46 @@ extern "C" int fc2d_b200_advance(fc2d_b200_solver_t* s, double t, double dt, dou
     }
     ghost_update(s, minlevel, maxlevel, 0);
     if (o.time_sync) time_sync(s, minlevel, maxlevel);
+    return 0;
+}
+
+extern "C" int fc2d_b200_advance(fc2d_b200_solver_t* s, double t, double dt, double* maxcfl)
+{
+    if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
+    s->ev_used = 0;
+    s->upd_launch_bytes.clear();
+    s->upd_launches = 0;
+    s->total_launches = 0;
+    // pass 1: host traversal filling the per-launch parameters and statistics
+    s->emit = false; s->fill = true;
+    int rc = traverse_advance(s, t, dt);
+    if (rc) { s->emit = true; return rc; }
+    const int nupd = s->n_upd;
+    rc = begin_cfl(s);
+    if (rc) return rc;
+    if (nupd) CK(cudaMemcpyAsync(s->params_dev, s->params_host, sizeof(StepParams) * nupd, cudaMemcpyHostToDevice, s->st));
+    // pass 2: the launches, captured once per forest into a CUDA graph and replayed
+    s->emit = true; s->fill = false;
+    if (s->use_graphs && !s->timing) {
+        if (!s->graph_exec || s->graph_nupd != nupd) {
+            invalidate_graph(s);
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+            rc = traverse_advance(s, t, dt);
+            cudaError_t ec = cudaStreamEndCapture(s->st, &g);
+            if (rc) { if (g) cudaGraphDestroy(g); s->fill = true; return rc; }
+            if (ec != cudaSuccess) { s->fill = true; return fail(FC2D_B200_ECUDA, std::string("graph capture: ") + cudaGetErrorString(ec)); }
+            ec = cudaGraphInstantiate(&s->graph_exec, g, 0);
+            cudaGraphDestroy(g);
+            if (ec != cudaSuccess) { s->graph_exec = nullptr; s->fill = true; return fail(FC2D_B200_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(ec)); }
+            s->graph_nupd = nupd;
+        }
+        CK(cudaGraphLaunch(s->graph_exec, s->st));
+    } else {
+        rc = traverse_advance(s, t, dt);
+    }
+    s->fill = true;
+    if (rc) return rc;
     CK(cudaGetLastError());
     rc = end_cfl(s, maxcfl);
     if (s->timing) {
@@ -779,6 +880,7 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     cudaFree(oq); cudaFree(oql); if (oqi) cudaFree(oqi); if (oaux) cudaFree(oaux); cudaFree(oregs); cudaFree(odesc);
     s->aux_host.swap(naux);
     s->forest = std::move(nf);
+    invalidate_graph(s);
     rc = upload_desc_and_tables(s);
     if (rc) return rc;
     ghost_update(s, s->forest.minlevel_present, s->forest.maxlevel_present, 0);
@@ -842,5 +944,42 @@ extern "C" int fc2d_b200_set_timing(fc2d_b200_solver_t* s, int enable)
 {
     if (!s) return fail(FC2D_B200_EINVAL, "null solver");
     s->timing = enable != 0;
+    return 0;
+}
+
+extern "C" int fc2d_b200_event_record(fc2d_b200_solver_t* s, int slot)
+{
+    if (!s || slot < 0 || slot >= 64) return fail(FC2D_B200_EINVAL, "bad event slot");
+    if (s->user_ev.empty()) {
+        s->user_ev.resize(64);
+        for (auto& e : s->user_ev) CK(cudaEventCreate(&e));
+    }
+    CK(cudaEventRecord(s->user_ev[slot], s->st));
+    return 0;
+}
+
+extern "C" int fc2d_b200_event_elapsed(fc2d_b200_solver_t* s, int a, int b, double* ms)
+{
+    if (!s || !ms || a < 0 || b < 0 || a >= (int)s->user_ev.size() || b >= (int)s->user_ev.size())
+        return fail(FC2D_B200_EINVAL, "bad event slots");
+    CK(cudaEventSynchronize(s->user_ev[b]));
+    float m = 0;
+    CK(cudaEventElapsedTime(&m, s->user_ev[a], s->user_ev[b]));
+    *ms = m;
+    return 0;
+}
+
+extern "C" int fc2d_b200_get_stream(const fc2d_b200_solver_t* s, void** stream)
+{
+    if (!s || !stream) return fail(FC2D_B200_EINVAL, "null argument");
+    *stream = (void*)s->st;
+    return 0;
+}
+
+extern "C" int fc2d_b200_set_graphs(fc2d_b200_solver_t* s, int enable)
+{
+    if (!s) return fail(FC2D_B200_EINVAL, "null solver");
+    s->use_graphs = enable != 0;
+    invalidate_graph(s);
     return 0;
 }

@@ -258,6 +258,46 @@ __global__ void k_reset(double* __restrict__ regs, const PatchDesc* __restrict__
     }
 }
 
+// fclaw2d_time_sync's resets for levels [minlevel, maxl] (src/fclaw2d_time_sync.c:118-154):
+// same-size faces of every synced level, coarse/fine faces of each synced pair
+// (half-size faces of levels < maxl, double-size faces of levels > minlevel) and
+// physical faces.
+__global__ void k_reset_sync(double* __restrict__ regs, const PatchDesc* __restrict__ desc, int p0, int mx, int my,
+                             int meqn, int nreg, int minlevel, int maxl)
+{
+    const int p = p0 + blockIdx.x;
+    const PatchDesc pd = desc[p];
+    const int L = pd.level;
+    double* r = regs + (size_t)p * nreg;
+    RegOff R(mx, my, meqn);
+    for (int k = 0; k < 4; k++) {
+        const int ft = (pd.face_type >> (2 * k)) & 3;        // 0 bnd, 1 half, 2 same, 3 double
+        bool reset;
+        if (ft == 2) reset = true;
+        else if (ft == 1) reset = L < maxl;
+        else if (ft == 3) reset = L - 1 >= minlevel && L - 1 < maxl;
+        else reset = true;
+        if (!reset) continue;
+        if (k < 2) {
+            for (int t = threadIdx.x; t < meqn * my; t += blockDim.x) {
+                r[(k == 0 ? R.fm0 : R.fm1) + t] = 0.0;
+                r[(k == 0 ? R.fp0 : R.fp1) + t] = 0.0;
+                const int ef = (k == 0) ? R.ef0 : R.ef1;
+                r[ef + t] = 0.0;
+                r[ef + t + meqn * my] = 0.0;
+            }
+        } else {
+            for (int t = threadIdx.x; t < meqn * mx; t += blockDim.x) {
+                r[(k == 2 ? R.gm0 : R.gm1) + t] = 0.0;
+                r[(k == 2 ? R.gp0 : R.gp1) + t] = 0.0;
+                const int ef = (k == 2) ? R.ef2 : R.ef3;
+                r[ef + t] = 0.0;
+                r[ef + t + meqn * mx] = 0.0;
+            }
+        }
+    }
+}
+
 // Per-patch, per-field Kahan sums of q*dx*dy over interior cells in (j, i) order.
 __global__ void k_patch_mass(const double* __restrict__ q, const PatchDesc* __restrict__ desc, int mx, int my,
                              int mbc, int meqn, double* __restrict__ out)
@@ -415,6 +455,11 @@ void launch_reset(const Dims& d, double* regs, const PatchDesc* desc, int p0, in
                   cudaStream_t st)
 {
     if (np > 0) k_reset<<<np, 64, 0, st>>>(regs, desc, p0, d.mx, d.my, d.meqn, d.nreg(), coarse_level, mode);
+}
+void launch_reset_sync(const Dims& d, double* regs, const PatchDesc* desc, int p0, int np, int minlevel, int maxl,
+                       cudaStream_t st)
+{
+    if (np > 0) k_reset_sync<<<np, 64, 0, st>>>(regs, desc, p0, d.mx, d.my, d.meqn, d.nreg(), minlevel, maxl);
 }
 void launch_patch_mass(const Dims& d, const double* q, const PatchDesc* desc, int np, double* out, cudaStream_t st)
 {

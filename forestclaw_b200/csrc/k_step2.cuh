@@ -13,10 +13,20 @@
 //   the conservative q update over i,j = 1-mbc..mx+mbc-1 (clawpack46_step2_wrap.f:107-125)
 //   and the warp-shuffle CFL maximum.
 //
+// TW is the arithmetic type of the waves, speeds, limiter, second-order
+// correction and transverse splitting.  TW = double is the FP64 path (built
+// without FMA contraction: bitwise equal to the FP64 CPU path).  TW = float is
+// the FP32-wave path: the flux arrays fm/fp/gm/gp, the q update, the time-sync
+// registers and the CFL reduction stay FP64, and the Godunov split is taken as
+// an FP64 remainder, amdq = [f(q_i) - f(q_{i-1})](FP64) - apdq, so that
+// amdq + apdq telescopes to FP64 round-off and mass stays conserved to
+// FP64 accuracy although the waves are FP32.
+//
 // Index conventions: padded 0-based cell (ic, jc), ic = i + mbc - 1 for the
 // Fortran index i.  Interface ic sits between cells ic-1 and ic.
 #pragma once
 #include <cuda_runtime.h>
+#include <type_traits>
 #include "fcb_common.h"
 #include "riemann.cuh"
 
@@ -24,22 +34,31 @@ namespace fcb {
 
 enum { APP_NONE = 0, APP_SWIRL = 1, APP_RADIALDAM = 2, APP_TSUNAMI = 3 };
 
-template <class RP, int MX, int MY, int MBC, bool FWAVE>
+template <class RP, int MX, int MY, int MBC, typename TW, int NT = 0>
 struct Step2Geom {
+    static constexpr bool F32 = std::is_same<TW, float>::value;
     static constexpr int NX = MX + 2 * MBC, NY = MY + 2 * MBC, NXY = NX * NY;
     static constexpr int MEQN = RP::MEQN, MWAVES = RP::MWAVES, MAUX = RP::MAUX, NEXTRA = RP::NEXTRA;
     static constexpr int NIX = (NY - 2) * (NX - 1);          // x-sweep interfaces
     static constexpr int NIY = (NX - 2) * (NY - 1);          // y-sweep interfaces
     static constexpr int NI = NIX > NIY ? NIX : NIY;
+    // REG: every interface of a sweep has its own thread, so the normal solve
+    // (speeds, fluctuations, Roe averages) stays in registers across the
+    // barrier and only the waves, which the limiter reads from the neighbours,
+    // go through shared memory.
+    static constexpr bool REG = NT >= NI;
     // per-interface record of the normal solve: waves, speeds, amdq, apdq, solver extra
     static constexpr int W_WAVE = 0, W_S = MWAVES * MEQN, W_AM = W_S + MWAVES, W_AP = W_AM + MEQN,
-                         W_EX = W_AP + MEQN, WSZ = W_EX + NEXTRA;
-    // per-interface transverse terms: A1, A2 (from amdq), B1, B2 (from apdq), flags
+                         W_EX = W_AP + MEQN, WSZ_FULL = W_EX + NEXTRA;
+    static constexpr int WSZ = REG ? MWAVES * MEQN : WSZ_FULL;
+    // per-interface transverse terms: A1, A2 (from amdq), B1, B2 (from apdq)
     static constexpr int TSZ = 4 * MEQN;
     static constexpr int AUXS = MAUX > 0 ? MAUX : 0;
-    static constexpr size_t SMEM_DOUBLES = (size_t)MEQN * NXY * 5 + (size_t)AUXS * NXY + (size_t)WSZ * NI +
-                                           (size_t)TSZ * NI + 64;
-    static constexpr size_t SMEM_BYTES = SMEM_DOUBLES * sizeof(double) + (size_t)NI * 4;
+    static constexpr bool USE_FLX = F32 && RP::CONS_FLUX;     // per-cell FP64 fluxes for the remainder
+    static constexpr size_t DOUBLES = (size_t)MEQN * NXY * 5 + (size_t)AUXS * NXY +
+                                      (USE_FLX ? (size_t)MEQN * NXY : 0) + 64;
+    static constexpr size_t TWS = (size_t)WSZ * NI + (size_t)TSZ * NI + (F32 ? (size_t)MEQN * NXY : 0);
+    static constexpr size_t SMEM_BYTES = DOUBLES * 8 + TWS * sizeof(TW) + NI;
     // conservation registers (fclaw2d_clawpatch_conservation.h:56-77), per patch
     static constexpr int R_FP0 = 0, R_FP1 = MY * MEQN, R_FM0 = 2 * MY * MEQN, R_FM1 = 3 * MY * MEQN;
     static constexpr int R_GP0 = 4 * MY * MEQN, R_GP1 = R_GP0 + MX * MEQN, R_GM0 = R_GP0 + 2 * MX * MEQN,
@@ -47,7 +66,6 @@ struct Step2Geom {
     static constexpr int R_EF0 = R_GP0 + 4 * MX * MEQN, R_EF1 = R_EF0 + 2 * MY * MEQN,
                          R_EF2 = R_EF1 + 2 * MY * MEQN, R_EF3 = R_EF2 + 2 * MX * MEQN,
                          NREG = R_EF3 + 2 * MX * MEQN;
-    // interface ranges of flux2 (FWAVE=false) / flux2fw (FWAVE=true) in padded indices
 };
 
 // Shallow-water flux function used by the time-sync flux store
@@ -63,16 +81,19 @@ __device__ __forceinline__ void rpn2_cons_sw(int idir, const T* q, T grav, T* fl
     flux[mv] = un * hut;
 }
 
-template <class RP, int MX, int MY, int MBC, bool FWAVE, int NT>
-__global__ void __launch_bounds__(NT)
-step2_f64_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* __restrict__ aux,
-                 double* __restrict__ regs, const PatchDesc* __restrict__ desc, int p0, StepParams sp,
-                 unsigned long long* __restrict__ cfl_bits)
+template <class RP, int MX, int MY, int MBC, bool FWAVE, int NT, typename TW>
+__global__ void __launch_bounds__(NT, 2)
+step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* __restrict__ aux,
+             double* __restrict__ regs, const PatchDesc* __restrict__ desc, int p0,
+             const StepParams* __restrict__ spp, unsigned long long* __restrict__ cfl_bits)
 {
-    using G = Step2Geom<RP, MX, MY, MBC, FWAVE>;
+    using G = Step2Geom<RP, MX, MY, MBC, TW, NT>;
+    const StepParams sp = *spp;     // per-launch parameters live in device memory (graph replay)
+    constexpr bool F32 = G::F32, REG = G::REG;
     constexpr int NX = G::NX, NY = G::NY, NXY = G::NXY, MEQN = G::MEQN, MWAVES = G::MWAVES;
     constexpr int MAUX = G::MAUX, NEXTRA = G::NEXTRA, NI = G::NI, WSZ = G::WSZ;
-    // flux2 / flux2fw interface ranges (padded): Godunov, cqxx, amdq+=cqxx, transverse, CFL
+    constexpr int MA = MAUX > 0 ? MAUX : 1;
+    // flux2 / flux2fw interface ranges (padded): Godunov, cqxx, amdq+=cqxx, transverse
     constexpr int GOD_LO = FWAVE ? MBC : 1, GOD_HI = FWAVE ? MX + MBC : NX - 2;
     constexpr int CQ_LO = FWAVE ? MBC : 1, CQ_HI = FWAVE ? MX + MBC : NX - 1;
     constexpr int AC_LO = FWAVE ? MBC : 1, AC_HI = FWAVE ? MX + MBC : NX - 2;
@@ -89,10 +110,12 @@ step2_f64_kernel(double* __restrict__ q, double* __restrict__ qlast, const doubl
     double* GMs = FPs + MEQN * NXY;
     double* GPs = GMs + MEQN * NXY;
     double* As = GPs + MEQN * NXY;                  // [MAUX][NY][NX]
-    double* W = As + G::AUXS * NXY;                 // [WSZ][NI]  (SoA)
-    double* Tt = W + (size_t)WSZ * NI;              // [TSZ][NI]
-    double* red = Tt + (size_t)G::TSZ * NI;         // 64 doubles for reductions
-    unsigned char* tflag = (unsigned char*)(red + 64);   // [NI] presence bits of A/B terms
+    double* FLX = As + G::AUXS * NXY;               // [MEQN][NY][NX] cell fluxes (FP32-wave path)
+    double* red = FLX + (G::USE_FLX ? MEQN * NXY : 0);   // 64 doubles for reductions
+    TW* W = reinterpret_cast<TW*>(red + 64);        // [WSZ][NI]  (SoA)
+    TW* Tt = W + (size_t)WSZ * NI;                  // [TSZ][NI]
+    TW* Qf = Tt + (size_t)G::TSZ * NI;              // [MEQN][NY][NX] q in TW (FP32-wave path)
+    unsigned char* tflag = reinterpret_cast<unsigned char*>(Qf + (F32 ? MEQN * NXY : 0));
 
     const int tid = threadIdx.x;
     const int p = p0 + blockIdx.x;
@@ -101,12 +124,16 @@ step2_f64_kernel(double* __restrict__ q, double* __restrict__ qlast, const doubl
     const double dt = sp.dt;
     const double dtdx = dt / dx, dtdy = dt / dy;
     double* qg = q + (size_t)p * MEQN * NXY;
+    // save_current_step: only the data time interpolation will read (coarser
+    // levels of a subcycled step, patches with fine-grid neighbours)
+    const bool save = sp.save_last && (pd.flags & PATCH_HAS_FINE_NBR);
 
     // ---- stage q (and aux) in shared memory --------------------------------
     for (int k = tid; k < MEQN * NXY; k += NT) {
         double v = qg[k];
         Qs[k] = v;
-        if (sp.save_last) qlast[(size_t)p * MEQN * NXY + k] = v;
+        if (F32) Qf[k] = (TW)v;
+        if (save) qlast[(size_t)p * MEQN * NXY + k] = v;
         FMs[k] = 0.0; FPs[k] = 0.0; GMs[k] = 0.0; GPs[k] = 0.0;
     }
     if (MAUX > 0) {
@@ -126,14 +153,19 @@ step2_f64_kernel(double* __restrict__ q, double* __restrict__ qlast, const doubl
     __syncthreads();
 
     const int mcapa = sp.mcapa;
-    auto dtdx1d_x = [&](int ic, int jc) -> double {
-        return mcapa > 0 ? dtdx / As[(mcapa - 1) * NXY + jc * NX + ic] : dtdx;
+    auto dtdx1d_x = [&](int ic, int jc) -> TW {
+        return mcapa > 0 ? (TW)(dtdx / As[(mcapa - 1) * NXY + jc * NX + ic]) : (TW)dtdx;
     };
-    auto dtdy1d_y = [&](int ic, int jc) -> double {
-        return mcapa > 0 ? dtdy / As[(mcapa - 1) * NXY + jc * NX + ic] : dtdy;
+    auto dtdy1d_y = [&](int ic, int jc) -> TW {
+        return mcapa > 0 ? (TW)(dtdy / As[(mcapa - 1) * NXY + jc * NX + ic]) : (TW)dtdy;
     };
+    auto qload = [&](int m, int c) -> TW {
+        if constexpr (F32) return Qf[m * NXY + c];
+        else return (TW)Qs[m * NXY + c];
+    };
+    const TW gravw = (TW)sp.grav, drytolw = (TW)sp.dry_tolerance;
 
-    // ---- time-sync flux store (before the update) ----------------------------
+    // ---- time-sync flux store (before the update), FP64 ----------------------
     double* rg = regs + (size_t)p * G::NREG;
     if (MEQN >= 3 && sp.store_flux) {
         // faces 0,1: j = 1..my, k = 0,1 ; faces 2,3: i = 1..mx, k = 0,1
@@ -160,283 +192,268 @@ step2_f64_kernel(double* __restrict__ q, double* __restrict__ qlast, const doubl
     }
 
     double cflmax = 0.0;
+    TW cflw = TW(0);
 
-    // =================== x-sweeps (clawpack46_step2.f:113-167) ===================
-    // X1: normal Riemann problems
-    for (int k = tid; k < G::NIX; k += NT) {
-        const int jc = 1 + k / (NX - 1), ic = 1 + k % (NX - 1);
-        double qL[MEQN], qR[MEQN], aL[MAUX > 0 ? MAUX : 1], aR[MAUX > 0 ? MAUX : 1];
-        for (int m = 0; m < MEQN; m++) { qL[m] = Qs[m * NXY + jc * NX + ic - 1]; qR[m] = Qs[m * NXY + jc * NX + ic]; }
-        for (int a = 0; a < MAUX; a++) { aL[a] = As[a * NXY + jc * NX + ic - 1]; aR[a] = As[a * NXY + jc * NX + ic]; }
-        double wave[MWAVES][MEQN], s[MWAVES], am[MEQN], ap[MEQN], ex[NEXTRA];
-        RP::template rpn2<double>(1, qL, qR, aL, aR, wave, s, am, ap, ex, sp.grav);
+    struct State { TW wave[MWAVES][MEQN]; TW s[MWAVES]; TW am[MEQN]; TW ap[MEQN]; TW ex[NEXTRA]; };
+
+    // Normal solve of one interface (qL = cell cL, qR = cell cR).
+    auto normal_solve = [&](int ixy, int cL, int cR, int k, bool cfl_range, TW d1, TW d0, State& st) {
+        TW qL[MEQN], qR[MEQN], aL[MA], aR[MA];
+        for (int m = 0; m < MEQN; m++) { qL[m] = qload(m, cL); qR[m] = qload(m, cR); }
+        for (int a = 0; a < MAUX; a++) { aL[a] = (TW)As[a * NXY + cL]; aR[a] = (TW)As[a * NXY + cR]; }
+        RP::template rpn2<TW>(ixy, qL, qR, aL, aR, st.wave, st.s, st.am, st.ap, st.ex, gravw);
+        for (int mw = 0; mw < MWAVES; mw++)
+            for (int m = 0; m < MEQN; m++) W[(G::W_WAVE + mw * MEQN + m) * NI + k] = st.wave[mw][m];
+        if (!REG) {
+            for (int mw = 0; mw < MWAVES; mw++) W[(G::W_S + mw) * NI + k] = st.s[mw];
+            for (int m = 0; m < MEQN; m++) { W[(G::W_AM + m) * NI + k] = st.am[m]; W[(G::W_AP + m) * NI + k] = st.ap[m]; }
+            for (int e = 0; e < NEXTRA; e++) W[(G::W_EX + e) * NI + k] = st.ex[e];
+        }
+        if (cfl_range) {
+            if (F32) {
+                for (int mw = 0; mw < MWAVES; mw++) cflw = dmax1(dmax1(cflw, d1 * st.s[mw]), -(d0 * st.s[mw]));
+            } else {
+                for (int mw = 0; mw < MWAVES; mw++)
+                    cflmax = dmax1(dmax1(cflmax, (double)(d1 * st.s[mw])), (double)(-(d0 * st.s[mw])));
+            }
+        }
+    };
+    auto restore = [&](int k, State& st) {
+        if (REG) return;
         for (int mw = 0; mw < MWAVES; mw++) {
-            for (int m = 0; m < MEQN; m++) W[(G::W_WAVE + mw * MEQN + m) * NI + k] = wave[mw][m];
-            W[(G::W_S + mw) * NI + k] = s[mw];
+            for (int m = 0; m < MEQN; m++) st.wave[mw][m] = W[(G::W_WAVE + mw * MEQN + m) * NI + k];
+            st.s[mw] = W[(G::W_S + mw) * NI + k];
         }
-        for (int m = 0; m < MEQN; m++) { W[(G::W_AM + m) * NI + k] = am[m]; W[(G::W_AP + m) * NI + k] = ap[m]; }
-        for (int e = 0; e < NEXTRA; e++) W[(G::W_EX + e) * NI + k] = ex[e];
-        if (ic >= MBC && ic <= MX + MBC) {
-            const double d1 = dtdx1d_x(ic, jc), d0 = dtdx1d_x(ic - 1, jc);
-            for (int mw = 0; mw < MWAVES; mw++)
-                cflmax = dmax1(dmax1(cflmax, d1 * s[mw]), -(d0 * s[mw]));
+        for (int m = 0; m < MEQN; m++) { st.am[m] = W[(G::W_AM + m) * NI + k]; st.ap[m] = W[(G::W_AP + m) * NI + k]; }
+        for (int e = 0; e < NEXTRA; e++) st.ex[e] = W[(G::W_EX + e) * NI + k];
+    };
+
+    // Limiter, second-order correction, fadd and transverse split of one interface.
+    // Returns faddm/faddp (FP64) and writes the transverse terms into Tt.
+    auto interface_update = [&](int ixy, int k, int cL, int cR, int pos, int lim_lo, int lim_hi,
+                                bool god, bool cqr, bool acr, bool trr, TW dlo, TW dhi, TW dave,
+                                const int* a1c, const int* a2c, const int* a3c, State& st,
+                                double* faddm, double* faddp) {
+        TW cq[MEQN];
+        for (int m = 0; m < MEQN; m++) { cq[m] = TW(0); faddm[m] = 0.0; faddp[m] = 0.0; }
+        if (god) {
+            if constexpr (F32) {
+                double am64[MEQN], ap64[MEQN];
+                double qL[MEQN], qR[MEQN], aL[MA], aR[MA], fL[MEQN], fR[MEQN];
+                for (int m = 0; m < MEQN; m++) {
+                    qL[m] = Qs[m * NXY + cL]; qR[m] = Qs[m * NXY + cR];
+                    if (G::USE_FLX) { fL[m] = FLX[m * NXY + cL]; fR[m] = FLX[m * NXY + cR]; }
+                    else { fL[m] = 0.0; fR[m] = 0.0; }
+                }
+                for (int a = 0; a < MAUX; a++) { aL[a] = As[a * NXY + cL]; aR[a] = As[a * NXY + cR]; }
+                RP::godunov64(ixy, qL, qR, aL, aR, fL, fR, st.ap, am64, ap64, sp.grav);
+                for (int m = 0; m < MEQN; m++) { faddp[m] = faddp[m] - ap64[m]; faddm[m] = faddm[m] + am64[m]; }
+            } else {
+                for (int m = 0; m < MEQN; m++) { faddp[m] = faddp[m] - (double)st.ap[m]; faddm[m] = faddm[m] + (double)st.am[m]; }
+            }
         }
-    }
-    __syncthreads();
-    // X2: limiter, second-order correction, fadd, transverse splitting
-    for (int k = tid; k < G::NIX; k += NT) {
-        const int jc = 1 + k / (NX - 1), ic = 1 + k % (NX - 1);
-        double wave[MWAVES][MEQN], s[MWAVES], am[MEQN], ap[MEQN], ex[NEXTRA], cq[MEQN];
-        for (int mw = 0; mw < MWAVES; mw++) {
-            for (int m = 0; m < MEQN; m++) wave[mw][m] = W[(G::W_WAVE + mw * MEQN + m) * NI + k];
-            s[mw] = W[(G::W_S + mw) * NI + k];
-        }
-        for (int m = 0; m < MEQN; m++) { am[m] = W[(G::W_AM + m) * NI + k]; ap[m] = W[(G::W_AP + m) * NI + k]; }
-        for (int e = 0; e < NEXTRA; e++) ex[e] = W[(G::W_EX + e) * NI + k];
-        double faddm[MEQN], faddp[MEQN];
-        for (int m = 0; m < MEQN; m++) { faddm[m] = 0.0; faddp[m] = 0.0; }
-        if (ic >= GOD_LO && ic <= GOD_HI)
-            for (int m = 0; m < MEQN; m++) { faddp[m] = faddp[m] - ap[m]; faddm[m] = faddm[m] + am[m]; }
         const bool second = FWAVE ? (sp.order1 != 1) : (sp.order1 == 2);
         if (second) {
-            if (ic >= MBC && ic <= MX + MBC) {
+            if (pos >= lim_lo && pos <= lim_hi) {
                 // inline limiter (clawpack46_inlinelimiter.f:267-343) with unlimited neighbours
                 for (int mw = 0; mw < MWAVES; mw++) {
                     const int ml = sp.mthlim[mw];
                     if (ml == 0) continue;
-                    double wnorm2 = 0.0, dotl = 0.0, dotr = 0.0;
+                    TW wnorm2 = TW(0), dotl = TW(0), dotr = TW(0);
                     for (int m = 0; m < MEQN; m++) {
-                        const double w = wave[mw][m];
-                        const double wl = W[(G::W_WAVE + mw * MEQN + m) * NI + k - 1];
-                        const double wr = W[(G::W_WAVE + mw * MEQN + m) * NI + k + 1];
+                        const TW w = st.wave[mw][m];
+                        const TW wl = W[(G::W_WAVE + mw * MEQN + m) * NI + k - 1];
+                        const TW wr = W[(G::W_WAVE + mw * MEQN + m) * NI + k + 1];
                         wnorm2 = wnorm2 + w * w;
                         dotl = dotl + wl * w;
                         dotr = dotr + w * wr;
                     }
-                    if (wnorm2 == 0.0) continue;
-                    const double r = (s[mw] > 0.0) ? dotl / wnorm2 : dotr / wnorm2;
-                    const double wlim = limiter_phi<double>(ml, r);
-                    for (int m = 0; m < MEQN; m++) wave[mw][m] = wlim * wave[mw][m];
+                    if (wnorm2 == TW(0)) continue;
+                    const TW r = (st.s[mw] > TW(0)) ? dotl / wnorm2 : dotr / wnorm2;
+                    const TW wlim = limiter_phi<TW>(ml, r);
+                    for (int m = 0; m < MEQN; m++) st.wave[mw][m] = wlim * st.wave[mw][m];
                 }
             }
-            if (ic >= CQ_LO && ic <= CQ_HI) {
-                const double dtdxave = 0.5 * (dtdx1d_x(ic - 1, jc) + dtdx1d_x(ic, jc));
+            if (cqr) {
                 for (int m = 0; m < MEQN; m++) {
-                    double c = 0.0;
+                    TW c = TW(0);
                     for (int mw = 0; mw < MWAVES; mw++) {
-                        if (FWAVE) c = c + sgn1(s[mw]) * (1.0 - fabs(s[mw]) * dtdxave) * wave[mw][m];
-                        else { const double sa = fabs(s[mw]); c = c + sa * (1.0 - sa * dtdxave) * wave[mw][m]; }
+                        if (FWAVE) c = c + sgn1(st.s[mw]) * (TW(1) - fabs(st.s[mw]) * dave) * st.wave[mw][m];
+                        else { const TW sa = fabs(st.s[mw]); c = c + sa * (TW(1) - sa * dave) * st.wave[mw][m]; }
                     }
                     cq[m] = c;
-                    faddm[m] = faddm[m] + 0.5 * c;
-                    faddp[m] = faddp[m] + 0.5 * c;
+                    if (F32) {
+                        const double h = 0.5 * (double)c;
+                        faddm[m] = faddm[m] + h;
+                        faddp[m] = faddp[m] + h;
+                    } else {
+                        faddm[m] = faddm[m] + (double)(TW(0.5) * c);
+                        faddp[m] = faddp[m] + (double)(TW(0.5) * c);
+                    }
                 }
             }
         }
-        for (int m = 0; m < MEQN; m++) {
-            FMs[m * NXY + jc * NX + ic] = 0.0 + faddm[m];
-            FPs[m * NXY + jc * NX + ic] = 0.0 + faddp[m];
-        }
         unsigned char fl = 0;
-        if (sp.order2 > 0 && ic >= TR_LO && ic <= TR_HI) {
-            if (sp.order1 > 1 && sp.order2 == 2 && ic >= AC_LO && ic <= AC_HI)
+        if (sp.order2 > 0 && trr) {
+            TW am[MEQN], ap[MEQN];
+            for (int m = 0; m < MEQN; m++) { am[m] = st.am[m]; ap[m] = st.ap[m]; }
+            if (sp.order1 > 1 && sp.order2 == 2 && acr)
                 for (int m = 0; m < MEQN; m++) { am[m] = am[m] + cq[m]; ap[m] = ap[m] - cq[m]; }
-            double qL[MEQN], qR[MEQN];
-            for (int m = 0; m < MEQN; m++) { qL[m] = Qs[m * NXY + jc * NX + ic - 1]; qR[m] = Qs[m * NXY + jc * NX + ic]; }
-            double a1[MAUX > 0 ? MAUX : 1], a2[MAUX > 0 ? MAUX : 1], a3[MAUX > 0 ? MAUX : 1];
-            double bm[MEQN], bp[MEQN];
-            // amdq: aux of cell i1 = ic-1 on rows jc-1, jc, jc+1
-            for (int a = 0; a < MAUX; a++) {
-                a1[a] = As[a * NXY + (jc - 1) * NX + ic - 1];
-                a2[a] = As[a * NXY + jc * NX + ic - 1];
-                a3[a] = As[a * NXY + (jc + 1) * NX + ic - 1];
-            }
-            RP::template rpt2<double>(1, 1, qL, qR, a1, a2, a3, ex, am, bm, bp, sp.grav, sp.dry_tolerance);
-            const double dlo = dtdx1d_x(ic - 1, jc);
+            TW qL[MEQN], qR[MEQN];
+            for (int m = 0; m < MEQN; m++) { qL[m] = qload(m, cL); qR[m] = qload(m, cR); }
+            TW a1[MA], a2[MA], a3[MA], bm[MEQN], bp[MEQN];
+            for (int a = 0; a < MAUX; a++) { a1[a] = (TW)As[a * NXY + a1c[0]]; a2[a] = (TW)As[a * NXY + a2c[0]]; a3[a] = (TW)As[a * NXY + a3c[0]]; }
+            RP::template rpt2<TW>(ixy, 1, qL, qR, a1, a2, a3, st.ex, am, bm, bp, gravw, drytolw);
             for (int m = 0; m < MEQN; m++) {
-                Tt[(0 * MEQN + m) * NI + k] = 0.5 * dlo * bm[m];
-                Tt[(1 * MEQN + m) * NI + k] = 0.5 * dlo * bp[m];
+                Tt[(0 * MEQN + m) * NI + k] = TW(0.5) * dlo * bm[m];
+                Tt[(1 * MEQN + m) * NI + k] = TW(0.5) * dlo * bp[m];
             }
-            for (int a = 0; a < MAUX; a++) {
-                a1[a] = As[a * NXY + (jc - 1) * NX + ic];
-                a2[a] = As[a * NXY + jc * NX + ic];
-                a3[a] = As[a * NXY + (jc + 1) * NX + ic];
-            }
-            RP::template rpt2<double>(1, 2, qL, qR, a1, a2, a3, ex, ap, bm, bp, sp.grav, sp.dry_tolerance);
-            const double dhi = FWAVE ? dlo : dtdx1d_x(ic, jc);
+            for (int a = 0; a < MAUX; a++) { a1[a] = (TW)As[a * NXY + a1c[1]]; a2[a] = (TW)As[a * NXY + a2c[1]]; a3[a] = (TW)As[a * NXY + a3c[1]]; }
+            RP::template rpt2<TW>(ixy, 2, qL, qR, a1, a2, a3, st.ex, ap, bm, bp, gravw, drytolw);
             for (int m = 0; m < MEQN; m++) {
-                Tt[(2 * MEQN + m) * NI + k] = 0.5 * dhi * bm[m];
-                Tt[(3 * MEQN + m) * NI + k] = 0.5 * dhi * bp[m];
+                Tt[(2 * MEQN + m) * NI + k] = TW(0.5) * dhi * bm[m];
+                Tt[(3 * MEQN + m) * NI + k] = TW(0.5) * dhi * bp[m];
             }
             fl = 1;
         }
         tflag[k] = fl;
-    }
-    __syncthreads();
+    };
+
+    // cell fluxes for the FP64 remainder of the Godunov split
+    auto cell_fluxes = [&](int ixy) {
+        if constexpr (G::USE_FLX) {
+            for (int c = tid; c < NXY; c += NT) {
+                double qv[MEQN], fv[MEQN];
+                for (int m = 0; m < MEQN; m++) qv[m] = Qs[m * NXY + c];
+                RP::flux64(ixy, qv, sp.grav, fv);
+                for (int m = 0; m < MEQN; m++) FLX[m * NXY + c] = fv[m];
+            }
+        }
+    };
+
+    // x-sweep interface k -> row jc = 1 + k / (NX-1), interface ic = 1 + k % (NX-1)
+    auto x1 = [&](int k, State& st) {
+        const int jc = 1 + k / (NX - 1), ic = 1 + k % (NX - 1);
+        const bool cr = (ic >= MBC && ic <= MX + MBC);
+        normal_solve(1, jc * NX + ic - 1, jc * NX + ic, k, cr, cr ? dtdx1d_x(ic, jc) : TW(0),
+                     cr ? dtdx1d_x(ic - 1, jc) : TW(0), st);
+    };
+    auto x2 = [&](int k, State& st) {
+        const int jc = 1 + k / (NX - 1), ic = 1 + k % (NX - 1);
+        const TW dlo = dtdx1d_x(ic - 1, jc);
+        const TW dhi = FWAVE ? dlo : dtdx1d_x(ic, jc);
+        const TW dave = TW(0.5) * (dtdx1d_x(ic - 1, jc) + dtdx1d_x(ic, jc));
+        // aux of cell i1 = ic-1 (amdq) / ic (apdq) on rows jc-1, jc, jc+1
+        const int a1c[2] = {(jc - 1) * NX + ic - 1, (jc - 1) * NX + ic};
+        const int a2c[2] = {jc * NX + ic - 1, jc * NX + ic};
+        const int a3c[2] = {(jc + 1) * NX + ic - 1, (jc + 1) * NX + ic};
+        double faddm[MEQN], faddp[MEQN];
+        interface_update(1, k, jc * NX + ic - 1, jc * NX + ic, ic, MBC, MX + MBC,
+                         ic >= GOD_LO && ic <= GOD_HI, ic >= CQ_LO && ic <= CQ_HI, ic >= AC_LO && ic <= AC_HI,
+                         ic >= TR_LO && ic <= TR_HI, dlo, dhi, dave, a1c, a2c, a3c, st, faddm, faddp);
+        for (int m = 0; m < MEQN; m++) {
+            FMs[m * NXY + jc * NX + ic] = 0.0 + faddm[m];
+            FPs[m * NXY + jc * NX + ic] = 0.0 + faddp[m];
+        }
+    };
+    // y-sweep interface k -> column ic = 1 + k / (NY-1), interface jc = 1 + k % (NY-1)
+    auto y1 = [&](int k, State& st) {
+        const int ic = 1 + k / (NY - 1), jc = 1 + k % (NY - 1);
+        const bool cr = (jc >= MBC && jc <= MY + MBC);
+        normal_solve(2, (jc - 1) * NX + ic, jc * NX + ic, k, cr, cr ? dtdy1d_y(ic, jc) : TW(0),
+                     cr ? dtdy1d_y(ic, jc - 1) : TW(0), st);
+    };
+    auto y2 = [&](int k, State& st) {
+        const int ic = 1 + k / (NY - 1), jc = 1 + k % (NY - 1);
+        const TW dlo = dtdy1d_y(ic, jc - 1);
+        const TW dhi = FWAVE ? dlo : dtdy1d_y(ic, jc);
+        const TW dave = TW(0.5) * (dtdy1d_y(ic, jc - 1) + dtdy1d_y(ic, jc));
+        // aux of sweep cell i1 = jc-1 (amdq) / jc (apdq) on columns ic-1, ic, ic+1
+        const int a1c[2] = {(jc - 1) * NX + ic - 1, jc * NX + ic - 1};
+        const int a2c[2] = {(jc - 1) * NX + ic, jc * NX + ic};
+        const int a3c[2] = {(jc - 1) * NX + ic + 1, jc * NX + ic + 1};
+        double faddm[MEQN], faddp[MEQN];
+        interface_update(2, k, (jc - 1) * NX + ic, jc * NX + ic, jc, MBC, MY + MBC,
+                         jc >= GOD_LOY && jc <= GOD_HIY, jc >= CQ_LOY && jc <= CQ_HIY,
+                         jc >= AC_LOY && jc <= AC_HIY, jc >= TR_LOY && jc <= TR_HIY, dlo, dhi, dave,
+                         a1c, a2c, a3c, st, faddm, faddp);
+        for (int m = 0; m < MEQN; m++) {
+            GMs[m * NXY + jc * NX + ic] = GMs[m * NXY + jc * NX + ic] + faddm[m];
+            GPs[m * NXY + jc * NX + ic] = GPs[m * NXY + jc * NX + ic] + faddp[m];
+        }
+    };
     // X3: gadd -> gm/gp.  gm(ic,jc) = ((0 + G2(row jc-1)) + G1(row jc)), gp identical.
-    for (int c = tid; c < NXY; c += NT) {
+    auto x3 = [&](int c) {
         const int jc = c / NX, ic = c % NX;
-        if (ic < 1 || jc < 1) continue;                  // accumulation range ic >= 1, rows >= 1
+        if (ic < 1 || jc < 1) return;                    // accumulation range ic >= 1, rows >= 1
         for (int m = 0; m < MEQN; m++) {
             double g = 0.0;
-            // row jc-1 (its gadd(:,2)) contributes to gm(ic,jc)
-            if (jc - 1 >= 1 && jc - 1 <= NY - 2) {
+            if (jc - 1 >= 1 && jc - 1 <= NY - 2) {       // row jc-1, its gadd(:,2)
                 const int r = jc - 1;
                 double v = 0.0;
-                if (ic + 1 <= NX - 1) { const int kk = (r - 1) * (NX - 1) + ic; if (tflag[kk]) v = v - Tt[(1 * MEQN + m) * NI + kk]; }
-                { const int kk = (r - 1) * (NX - 1) + ic - 1; if (tflag[kk]) v = v - Tt[(3 * MEQN + m) * NI + kk]; }
+                if (ic + 1 <= NX - 1) { const int kk = (r - 1) * (NX - 1) + ic; if (tflag[kk]) v = v - (double)Tt[(1 * MEQN + m) * NI + kk]; }
+                { const int kk = (r - 1) * (NX - 1) + ic - 1; if (tflag[kk]) v = v - (double)Tt[(3 * MEQN + m) * NI + kk]; }
                 g = g + v;
             }
-            if (jc <= NY - 2) {
+            if (jc <= NY - 2) {                          // row jc, its gadd(:,1)
                 const int r = jc;
                 double v = 0.0;
-                if (ic + 1 <= NX - 1) { const int kk = (r - 1) * (NX - 1) + ic; if (tflag[kk]) v = v - Tt[(0 * MEQN + m) * NI + kk]; }
-                { const int kk = (r - 1) * (NX - 1) + ic - 1; if (tflag[kk]) v = v - Tt[(2 * MEQN + m) * NI + kk]; }
+                if (ic + 1 <= NX - 1) { const int kk = (r - 1) * (NX - 1) + ic; if (tflag[kk]) v = v - (double)Tt[(0 * MEQN + m) * NI + kk]; }
+                { const int kk = (r - 1) * (NX - 1) + ic - 1; if (tflag[kk]) v = v - (double)Tt[(2 * MEQN + m) * NI + kk]; }
                 g = g + v;
             }
             GMs[m * NXY + c] = g;
             GPs[m * NXY + c] = g;
         }
-    }
-    __syncthreads();
-
-    // =================== y-sweeps (clawpack46_step2.f:182-236) ===================
-    // interface k -> column ic = 1 + k / (NY-1), interface jc = 1 + k % (NY-1)
-    for (int k = tid; k < G::NIY; k += NT) {
-        const int ic = 1 + k / (NY - 1), jc = 1 + k % (NY - 1);
-        double qL[MEQN], qR[MEQN], aL[MAUX > 0 ? MAUX : 1], aR[MAUX > 0 ? MAUX : 1];
-        for (int m = 0; m < MEQN; m++) { qL[m] = Qs[m * NXY + (jc - 1) * NX + ic]; qR[m] = Qs[m * NXY + jc * NX + ic]; }
-        for (int a = 0; a < MAUX; a++) { aL[a] = As[a * NXY + (jc - 1) * NX + ic]; aR[a] = As[a * NXY + jc * NX + ic]; }
-        double wave[MWAVES][MEQN], s[MWAVES], am[MEQN], ap[MEQN], ex[NEXTRA];
-        RP::template rpn2<double>(2, qL, qR, aL, aR, wave, s, am, ap, ex, sp.grav);
-        for (int mw = 0; mw < MWAVES; mw++) {
-            for (int m = 0; m < MEQN; m++) W[(G::W_WAVE + mw * MEQN + m) * NI + k] = wave[mw][m];
-            W[(G::W_S + mw) * NI + k] = s[mw];
-        }
-        for (int m = 0; m < MEQN; m++) { W[(G::W_AM + m) * NI + k] = am[m]; W[(G::W_AP + m) * NI + k] = ap[m]; }
-        for (int e = 0; e < NEXTRA; e++) W[(G::W_EX + e) * NI + k] = ex[e];
-        if (jc >= MBC && jc <= MY + MBC) {
-            const double d1 = dtdy1d_y(ic, jc), d0 = dtdy1d_y(ic, jc - 1);
-            for (int mw = 0; mw < MWAVES; mw++)
-                cflmax = dmax1(dmax1(cflmax, d1 * s[mw]), -(d0 * s[mw]));
-        }
-    }
-    __syncthreads();
-    for (int k = tid; k < G::NIY; k += NT) {
-        const int ic = 1 + k / (NY - 1), jc = 1 + k % (NY - 1);
-        double wave[MWAVES][MEQN], s[MWAVES], am[MEQN], ap[MEQN], ex[NEXTRA], cq[MEQN];
-        for (int mw = 0; mw < MWAVES; mw++) {
-            for (int m = 0; m < MEQN; m++) wave[mw][m] = W[(G::W_WAVE + mw * MEQN + m) * NI + k];
-            s[mw] = W[(G::W_S + mw) * NI + k];
-        }
-        for (int m = 0; m < MEQN; m++) { am[m] = W[(G::W_AM + m) * NI + k]; ap[m] = W[(G::W_AP + m) * NI + k]; }
-        for (int e = 0; e < NEXTRA; e++) ex[e] = W[(G::W_EX + e) * NI + k];
-        double faddm[MEQN], faddp[MEQN];
-        for (int m = 0; m < MEQN; m++) { faddm[m] = 0.0; faddp[m] = 0.0; }
-        if (jc >= GOD_LOY && jc <= GOD_HIY)
-            for (int m = 0; m < MEQN; m++) { faddp[m] = faddp[m] - ap[m]; faddm[m] = faddm[m] + am[m]; }
-        const bool second = FWAVE ? (sp.order1 != 1) : (sp.order1 == 2);
-        if (second) {
-            if (jc >= MBC && jc <= MY + MBC) {
-                for (int mw = 0; mw < MWAVES; mw++) {
-                    const int ml = sp.mthlim[mw];
-                    if (ml == 0) continue;
-                    double wnorm2 = 0.0, dotl = 0.0, dotr = 0.0;
-                    for (int m = 0; m < MEQN; m++) {
-                        const double w = wave[mw][m];
-                        const double wl = W[(G::W_WAVE + mw * MEQN + m) * NI + k - 1];
-                        const double wr = W[(G::W_WAVE + mw * MEQN + m) * NI + k + 1];
-                        wnorm2 = wnorm2 + w * w;
-                        dotl = dotl + wl * w;
-                        dotr = dotr + w * wr;
-                    }
-                    if (wnorm2 == 0.0) continue;
-                    const double r = (s[mw] > 0.0) ? dotl / wnorm2 : dotr / wnorm2;
-                    const double wlim = limiter_phi<double>(ml, r);
-                    for (int m = 0; m < MEQN; m++) wave[mw][m] = wlim * wave[mw][m];
-                }
-            }
-            if (jc >= CQ_LOY && jc <= CQ_HIY) {
-                const double dtdxave = 0.5 * (dtdy1d_y(ic, jc - 1) + dtdy1d_y(ic, jc));
-                for (int m = 0; m < MEQN; m++) {
-                    double c = 0.0;
-                    for (int mw = 0; mw < MWAVES; mw++) {
-                        if (FWAVE) c = c + sgn1(s[mw]) * (1.0 - fabs(s[mw]) * dtdxave) * wave[mw][m];
-                        else { const double sa = fabs(s[mw]); c = c + sa * (1.0 - sa * dtdxave) * wave[mw][m]; }
-                    }
-                    cq[m] = c;
-                    faddm[m] = faddm[m] + 0.5 * c;
-                    faddp[m] = faddp[m] + 0.5 * c;
-                }
-            }
-        }
-        for (int m = 0; m < MEQN; m++) {
-            GMs[m * NXY + jc * NX + ic] = GMs[m * NXY + jc * NX + ic] + faddm[m];
-            GPs[m * NXY + jc * NX + ic] = GPs[m * NXY + jc * NX + ic] + faddp[m];
-        }
-        unsigned char fl = 0;
-        if (sp.order2 > 0 && jc >= TR_LOY && jc <= TR_HIY) {
-            if (sp.order1 > 1 && sp.order2 == 2 && jc >= AC_LOY && jc <= AC_HIY)
-                for (int m = 0; m < MEQN; m++) { am[m] = am[m] + cq[m]; ap[m] = ap[m] - cq[m]; }
-            double qL[MEQN], qR[MEQN];
-            for (int m = 0; m < MEQN; m++) { qL[m] = Qs[m * NXY + (jc - 1) * NX + ic]; qR[m] = Qs[m * NXY + jc * NX + ic]; }
-            double a1[MAUX > 0 ? MAUX : 1], a2[MAUX > 0 ? MAUX : 1], a3[MAUX > 0 ? MAUX : 1];
-            double bm[MEQN], bp[MEQN];
-            // amdq: aux of sweep cell i1 = jc-1 on columns ic-1, ic, ic+1
-            for (int a = 0; a < MAUX; a++) {
-                a1[a] = As[a * NXY + (jc - 1) * NX + ic - 1];
-                a2[a] = As[a * NXY + (jc - 1) * NX + ic];
-                a3[a] = As[a * NXY + (jc - 1) * NX + ic + 1];
-            }
-            RP::template rpt2<double>(2, 1, qL, qR, a1, a2, a3, ex, am, bm, bp, sp.grav, sp.dry_tolerance);
-            const double dlo = dtdy1d_y(ic, jc - 1);
-            for (int m = 0; m < MEQN; m++) {
-                Tt[(0 * MEQN + m) * NI + k] = 0.5 * dlo * bm[m];
-                Tt[(1 * MEQN + m) * NI + k] = 0.5 * dlo * bp[m];
-            }
-            for (int a = 0; a < MAUX; a++) {
-                a1[a] = As[a * NXY + jc * NX + ic - 1];
-                a2[a] = As[a * NXY + jc * NX + ic];
-                a3[a] = As[a * NXY + jc * NX + ic + 1];
-            }
-            RP::template rpt2<double>(2, 2, qL, qR, a1, a2, a3, ex, ap, bm, bp, sp.grav, sp.dry_tolerance);
-            const double dhi = FWAVE ? dlo : dtdy1d_y(ic, jc);
-            for (int m = 0; m < MEQN; m++) {
-                Tt[(2 * MEQN + m) * NI + k] = 0.5 * dhi * bm[m];
-                Tt[(3 * MEQN + m) * NI + k] = 0.5 * dhi * bp[m];
-            }
-            fl = 1;
-        }
-        tflag[k] = fl;
-    }
-    __syncthreads();
+    };
     // Y3: gadd -> fm/fp.  fm(ic,jc) = (fm + G2(col ic-1)) + G1(col ic)
-    for (int c = tid; c < NXY; c += NT) {
+    auto y3 = [&](int c) {
         const int jc = c / NX, ic = c % NX;
-        if (jc < 1) continue;
+        if (jc < 1) return;
         for (int m = 0; m < MEQN; m++) {
             double fm = FMs[m * NXY + c], fp = FPs[m * NXY + c];
             if (ic - 1 >= 1 && ic - 1 <= NX - 2) {
                 const int col = ic - 1;
                 double v = 0.0;
-                if (jc + 1 <= NY - 1) { const int kk = (col - 1) * (NY - 1) + jc; if (tflag[kk]) v = v - Tt[(1 * MEQN + m) * NI + kk]; }
-                { const int kk = (col - 1) * (NY - 1) + jc - 1; if (tflag[kk]) v = v - Tt[(3 * MEQN + m) * NI + kk]; }
+                if (jc + 1 <= NY - 1) { const int kk = (col - 1) * (NY - 1) + jc; if (tflag[kk]) v = v - (double)Tt[(1 * MEQN + m) * NI + kk]; }
+                { const int kk = (col - 1) * (NY - 1) + jc - 1; if (tflag[kk]) v = v - (double)Tt[(3 * MEQN + m) * NI + kk]; }
                 fm = fm + v; fp = fp + v;
             }
             if (ic >= 1 && ic <= NX - 2) {
                 const int col = ic;
                 double v = 0.0;
-                if (jc + 1 <= NY - 1) { const int kk = (col - 1) * (NY - 1) + jc; if (tflag[kk]) v = v - Tt[(0 * MEQN + m) * NI + kk]; }
-                { const int kk = (col - 1) * (NY - 1) + jc - 1; if (tflag[kk]) v = v - Tt[(2 * MEQN + m) * NI + kk]; }
+                if (jc + 1 <= NY - 1) { const int kk = (col - 1) * (NY - 1) + jc; if (tflag[kk]) v = v - (double)Tt[(0 * MEQN + m) * NI + kk]; }
+                { const int kk = (col - 1) * (NY - 1) + jc - 1; if (tflag[kk]) v = v - (double)Tt[(2 * MEQN + m) * NI + kk]; }
                 fm = fm + v; fp = fp + v;
             }
             FMs[m * NXY + c] = fm;
             FPs[m * NXY + c] = fp;
         }
-    }
+    };
+
+    // =================== x-sweeps (clawpack46_step2.f:113-167) ===================
+    State st;
+    cell_fluxes(1);
+    if (REG) { if (tid < G::NIX) x1(tid, st); }
+    else for (int k = tid; k < G::NIX; k += NT) x1(k, st);
+    __syncthreads();
+    if (REG) { if (tid < G::NIX) x2(tid, st); }
+    else for (int k = tid; k < G::NIX; k += NT) { restore(k, st); x2(k, st); }
+    __syncthreads();
+    // X3 and the y-sweep normal solves touch disjoint data: one phase
+    for (int c = tid; c < NXY; c += NT) x3(c);
+    cell_fluxes(2);
+    // =================== y-sweeps (clawpack46_step2.f:182-236) ===================
+    if (REG) { if (tid < G::NIY) y1(tid, st); }
+    else for (int k = tid; k < G::NIY; k += NT) y1(k, st);
+    __syncthreads();
+    if (REG) { if (tid < G::NIY) y2(tid, st); }
+    else for (int k = tid; k < G::NIY; k += NT) { restore(k, st); y2(k, st); }
+    __syncthreads();
+    for (int c = tid; c < NXY; c += NT) y3(c);
     __syncthreads();
 
-    // ---- time-sync wave accumulation (clawpack46_time_sync.f:163-226) --------
+    // ---- time-sync wave accumulation (clawpack46_time_sync.f:163-226), FP64 ----
     if (sp.accumulate_waves) {
         const double dtdyv = dt * dy, dtdxv = dt * dx;
         for (int it = tid; it < (MY + MX) * MEQN; it += NT) {
@@ -467,19 +484,20 @@ step2_f64_kernel(double* __restrict__ q, double* __restrict__ qlast, const doubl
     for (int k = tid; k < MEQN * NXY; k += NT) {
         const int m = k / NXY, c = k % NXY;
         const int jc = c / NX, ic = c % NX;
-        double v = Qs[k];
         if (ic <= NX - 2 && jc <= NY - 2) {
             const int b = m * NXY;
+            double v = Qs[k];
             if (mcapa == 0)
                 v = v - dtdx * (FMs[b + c + 1] - FPs[b + c]) - dtdy * (GMs[b + c + NX] - GPs[b + c]);
             else
                 v = v - (dtdx * (FMs[b + c + 1] - FPs[b + c]) + dtdy * (GMs[b + c + NX] - GPs[b + c])) /
                             As[(mcapa - 1) * NXY + c];
+            qg[k] = v;
         }
-        qg[k] = v;
     }
 
     // ---- CFL maximum: warp shuffles, then one atomic per CTA -----------------
+    if (F32) cflmax = (double)cflw;
     for (int off = 16; off > 0; off >>= 1) cflmax = dmax1(cflmax, __shfl_xor_sync(0xffffffffu, cflmax, off));
     if ((tid & 31) == 0) red[tid >> 5] = cflmax;
     __syncthreads();

@@ -9,12 +9,12 @@ namespace fcb {
 
 template <class RP, int MX, int MY, int MBC, bool FW, int NT>
 static cudaError_t run_step2(const Dims& d, double* q, double* qlast, const double* aux, double* regs,
-                             const PatchDesc* desc, int p0, int npatch, const StepParams& sp,
+                             const PatchDesc* desc, int p0, int npatch, const StepParams* sp,
                              unsigned long long* cfl_bits, cudaStream_t st)
 {
-    using G = Step2Geom<RP, MX, MY, MBC, FW>;
+    using G = Step2Geom<RP, MX, MY, MBC, double, NT>;
     static bool attr_set = false;
-    auto kern = step2_f64_kernel<RP, MX, MY, MBC, FW, NT>;
+    auto kern = step2_kernel<RP, MX, MY, MBC, FW, NT, double>;
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM_BYTES);
         if (e != cudaSuccess) return e;
@@ -31,16 +31,16 @@ static cudaError_t run_step2(const Dims& d, double* q, double* qlast, const doub
         return run_step2<RPT, MXV, MYV, MBCV, FW, NT>(d, q, qlast, aux, regs, desc, p0, npatch, sp, cfl_bits, st);
 
 cudaError_t launch_step2_f64(int rp, const Dims& d, double* q, double* qlast, const double* aux, double* regs,
-                             const PatchDesc* desc, int p0, int npatch, const StepParams& sp,
+                             const PatchDesc* desc, int p0, int npatch, const StepParams* sp,
                              unsigned long long* cfl_bits, cudaStream_t st)
 {
     FCB_CASE(FC2D_B200_RP_ADVECTION, RPAdvection, 32, 32, 2, false, 512)
-    FCB_CASE(FC2D_B200_RP_ADVECTION, RPAdvection, 16, 16, 2, false, 352)
-    FCB_CASE(FC2D_B200_RP_ADVECTION, RPAdvection, 8, 8, 2, false, 128)
+    FCB_CASE(FC2D_B200_RP_ADVECTION, RPAdvection, 16, 16, 2, false, 416)
+    FCB_CASE(FC2D_B200_RP_ADVECTION, RPAdvection, 8, 8, 2, false, 160)
     FCB_CASE(FC2D_B200_RP_SW_ROE, RPShallowRoe, 16, 16, 2, false, 352)
-    FCB_CASE(FC2D_B200_RP_SW_ROE, RPShallowRoe, 8, 8, 2, false, 128)
+    FCB_CASE(FC2D_B200_RP_SW_ROE, RPShallowRoe, 8, 8, 2, false, 160)
     FCB_CASE(FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 16, 16, 2, true, 352)
-    FCB_CASE(FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 8, 8, 2, true, 128)
+    FCB_CASE(FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 8, 8, 2, true, 160)
     return cudaErrorInvalidValue;
 }
 

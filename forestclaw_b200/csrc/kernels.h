@@ -19,10 +19,6 @@ struct Dims {
 
 // ---- fused update (k_step2_f64.cu) ------------------------------------------
 // Returns cudaErrorInvalidValue when no specialisation exists for (rp, mx, my, mbc).
-cudaError_t launch_step2(int rp, int precision, const Dims& d, double* q, double* qlast, const double* aux,
-                         double* regs, const PatchDesc* desc, int p0, int npatch, const StepParams& sp,
-                         unsigned long long* cfl_bits, cudaStream_t st);
-bool step2_supported(int rp, int precision, int mx, int my, int mbc);
 
 // ---- ghost fill (k_amr.cu) ----------------------------------------------------
 // Gather tables: offsets are absolute indices of field 0 in the q slab; fields
@@ -50,6 +46,10 @@ void launch_f2c(const Dims& d, double* q, const double* regs, const PatchDesc* d
 // mode 1 = F2C, 2 = SAMESIZE, 3 = PHYS (fclaw2d_clawpatch_time_sync_reset)
 void launch_reset(const Dims& d, double* regs, const PatchDesc* desc, int p0, int np, int coarse_level,
                   int mode, cudaStream_t st);
+// All register resets of one fclaw2d_time_sync(minlevel, maxl) call in one launch
+// over the patches of levels [minlevel, maxl].
+void launch_reset_sync(const Dims& d, double* regs, const PatchDesc* desc, int p0, int np, int minlevel, int maxl,
+                       cudaStream_t st);
 
 // ---- diagnostics / regrid (k_amr.cu) -------------------------------------------
 void launch_patch_mass(const Dims& d, const double* q, const PatchDesc* desc, int np, double* out,

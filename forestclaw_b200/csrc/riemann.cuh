@@ -27,6 +27,18 @@ template <typename T> __device__ __forceinline__ T sgn1(T x) { return copysign(T
 // ---------------------------------------------------------------------------
 struct RPAdvection {
     static constexpr int MEQN = 1, MWAVES = 1, MAUX = 2, NEXTRA = 1;
+    static constexpr bool CONS_FLUX = false;
+    __device__ static void flux64(int ixy, const double* q, double grav, double* f) { (void)ixy; (void)grav; f[0] = q[0]; }
+    // FP64 Godunov split for the FP32-wave path
+    __device__ static void godunov64(int ixy, const double* qL, const double* qR, const double* aL, const double* aR,
+                                     const double* fL, const double* fR, const float* ap32, double* am, double* ap,
+                                     double grav)
+    {
+        (void)aL; (void)fL; (void)fR; (void)ap32; (void)grav;
+        const double s = aR[ixy - 1], d = qR[0] - qL[0];
+        am[0] = 0.0 + dmin1(s, 0.0) * d;
+        ap[0] = 0.0 + dmax1(s, 0.0) * d;
+    }
     template <typename T>
     __device__ static void rpn2(int ixy, const T* qL, const T* qR, const T* auxL, const T* auxR,
                                 T wave[MWAVES][MEQN], T s[MWAVES], T amdq[MEQN], T apdq[MEQN],
@@ -57,6 +69,24 @@ struct RPAdvection {
 // ---------------------------------------------------------------------------
 struct RPShallowRoe {
     static constexpr int MEQN = 3, MWAVES = 3, MAUX = 0, NEXTRA = 3;
+    static constexpr bool CONS_FLUX = true;
+    // normal flux in direction ixy, FP64 (one division per cell)
+    __device__ static void flux64(int ixy, const double* q, double grav, double* f)
+    {
+        const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+        const double h = q[0], inv = 1.0 / h;
+        f[0] = q[mu];
+        f[mu] = q[mu] * q[mu] * inv + 0.5 * grav * h * h;
+        f[mv] = q[mu] * q[mv] * inv;
+    }
+    // amdq as the FP64 remainder of the flux difference: amdq + apdq = f(qR) - f(qL)
+    __device__ static void godunov64(int ixy, const double* qL, const double* qR, const double* aL, const double* aR,
+                                     const double* fL, const double* fR, const float* ap32, double* am, double* ap,
+                                     double grav)
+    {
+        (void)ixy; (void)qL; (void)qR; (void)aL; (void)aR; (void)grav;
+        for (int m = 0; m < 3; m++) { ap[m] = (double)ap32[m]; am[m] = (fR[m] - fL[m]) - ap[m]; }
+    }
     template <typename T>
     __device__ static void rpn2(int ixy, const T* qL, const T* qR, const T* auxL, const T* auxR,
                                 T wave[MWAVES][MEQN], T s[MWAVES], T amdq[MEQN], T apdq[MEQN],
@@ -152,6 +182,29 @@ struct RPShallowRoe {
 // ---------------------------------------------------------------------------
 struct RPShallowFWave {
     static constexpr int MEQN = 3, MWAVES = 3, MAUX = 1, NEXTRA = 1;
+    static constexpr bool CONS_FLUX = true;
+    // normal flux in direction ixy, FP64 (one division per cell)
+    __device__ static void flux64(int ixy, const double* q, double grav, double* f)
+    {
+        const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+        const double h = q[0], inv = 1.0 / h;
+        f[0] = q[mu];
+        f[mu] = q[mu] * q[mu] * inv + 0.5 * grav * h * h;
+        f[mv] = q[mu] * q[mv] * inv;
+    }
+    // f-waves sum to the flux difference plus the bathymetry source g*hbar*(bR-bL)
+    __device__ static void godunov64(int ixy, const double* qL, const double* qR, const double* aL, const double* aR,
+                                     const double* fL, const double* fR, const float* ap32, double* am, double* ap,
+                                     double grav)
+    {
+        const int mu = (ixy == 1) ? 1 : 2;
+        for (int m = 0; m < 3; m++) {
+            double fd = fR[m] - fL[m];
+            if (m == mu) fd = fd + grav * (0.5 * (qR[0] + qL[0])) * (aR[0] - aL[0]);
+            ap[m] = (double)ap32[m];
+            am[m] = fd - ap[m];
+        }
+    }
     template <typename T>
     __device__ static void rpn2(int ixy, const T* qL, const T* qR, const T* auxL, const T* auxR,
                                 T fwave[MWAVES][MEQN], T s[MWAVES], T amdq[MEQN], T apdq[MEQN],

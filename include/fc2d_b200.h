@@ -149,8 +149,19 @@ int fc2d_b200_synchronize(fc2d_b200_solver_t* s);
  * cells, q read + write + aux read). */
 int fc2d_b200_last_update_stats(const fc2d_b200_solver_t* s, double* update_ms, double* update_bytes,
                                 int* update_launches, int* total_launches);
+/* Replay each fclaw2d_advance_all_levels as a CUDA graph captured once per
+ * forest (on by default; disabled while update timing is on). */
+int fc2d_b200_set_graphs(fc2d_b200_solver_t* s, int enable);
 /* Enable/disable CUDA-event timing of the update kernels (off by default). */
 int fc2d_b200_set_timing(fc2d_b200_solver_t* s, int enable);
+
+/* CUDA events on the solver's stream, for callers that time device work:
+ * record into one of 64 slots, then read the elapsed milliseconds between two
+ * recorded slots (waits for the later event). */
+int fc2d_b200_event_record(fc2d_b200_solver_t* s, int slot);
+int fc2d_b200_event_elapsed(fc2d_b200_solver_t* s, int slot_a, int slot_b, double* ms);
+/* The cudaStream_t the solver launches on (returned as void*). */
+int fc2d_b200_get_stream(const fc2d_b200_solver_t* s, void** stream);
 
 #ifdef __cplusplus
 }

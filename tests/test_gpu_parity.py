@@ -130,3 +130,89 @@ def test_single_step_protocol_matches_level_update():
         cb = b.single_step_update(3, it, np_, 0.0, 0.004)
     assert ca == cb
     assert np.array_equal(a.get_q(), b.get_q())
+
+
+# ---------------------------------------------------------------------------
+# FP32-wave path: tolerance against the FP64 oracle, FP64 conservation
+# ---------------------------------------------------------------------------
+FP32_L1_TOL = 2e-5      # relative L1 error of every field vs the FP64 oracle
+
+
+def _l1_rel(a, b, field):
+    num = np.abs(a[:, field, 2:-2, 2:-2] - b[:, field, 2:-2, 2:-2]).sum()
+    den = np.abs(b[:, field, 2:-2, 2:-2]).sum()
+    return num / max(den, 1e-300)
+
+
+def _run_fp32(problem, nsteps, dt, cfl_target=None, **kw):
+    from oracle import pyoracle as po
+    import forestclaw_b200 as fb
+    oc, gc = make(problem, **kw)
+    gc.precision = fb.PREC_FP32WAVE
+    o, g = po.OracleSim(oc), fb.Solver(gc)
+    o.initialize(); g.initialize()
+    _same_forest(o, g)
+    m0 = g.mass()
+    t = 0.0
+    for _ in range(nsteps):
+        co = o.advance(t, dt)
+        cg = g.advance(t, dt)
+        assert abs(cg - co) <= 1e-4 * co
+        t += dt
+        if cfl_target:
+            dt *= cfl_target / co
+    return o, g, m0
+
+
+def test_fp32wave_dam_uniform_error_and_mass():
+    o, g, m0 = _run_fp32(DAM, 20, 0.004, mx=16, my=16, minlevel=4, maxlevel=4)
+    qo, qg = o.get_q(), g.get_q()
+    h_err = _l1_rel(qg, qo, 0)
+    assert h_err < FP32_L1_TOL, h_err
+    for f in (1, 2):
+        assert np.abs(qg[:, f, 2:-2, 2:-2] - qo[:, f, 2:-2, 2:-2]).sum() <= FP32_L1_TOL * np.abs(qo[:, 0, 2:-2, 2:-2]).sum()
+    m1 = g.mass()
+    assert abs(m1[0] - m0[0]) <= 1e-12 * abs(m0[0])
+
+
+def test_fp32wave_dam_amr_timesync_mass():
+    o, g, m0 = _run_fp32(DAM, 8, 0.01, cfl_target=0.9, mx=16, my=16, minlevel=2, maxlevel=4, subcycle=1,
+                         time_sync=1)
+    qo, qg = o.get_q(), g.get_q()
+    assert _l1_rel(qg, qo, 0) < FP32_L1_TOL
+    m1 = g.mass()
+    assert abs(m1[0] - m0[0]) <= 1e-12 * abs(m0[0])
+
+
+def test_fp32wave_swirl_error():
+    o, g, m0 = _run_fp32(SWIRL, 12, swirl_dt(32, 2), mx=32, my=32, minlevel=2, maxlevel=2)
+    assert _l1_rel(g.get_q(), o.get_q(), 0) < FP32_L1_TOL
+
+
+def test_fp32wave_fwave_error():
+    o, g, m0 = _run_fp32(TSUNAMI, 6, 0.01, cfl_target=0.9, mx=8, my=8, minlevel=2, maxlevel=4, subcycle=1,
+                         time_sync=1)
+    qo, qg = o.get_q(), g.get_q()
+    assert _l1_rel(qg, qo, 0) < FP32_L1_TOL
+
+
+def test_graph_replay_matches_eager():
+    """advance() replayed from the captured graph equals the eager launches, across a regrid."""
+    import forestclaw_b200 as fb
+    _, gc = make(DAM, mx=16, my=16, minlevel=2, maxlevel=4, subcycle=1, time_sync=1)
+    outs = []
+    for graphs in (True, False):
+        g = fb.Solver(gc)
+        g.set_graphs(graphs)
+        g.initialize()
+        t, dt = 0.0, 0.01
+        for n in range(6):
+            c = g.advance(t, dt)
+            t += dt
+            dt *= 0.9 / c
+            if n == 2:
+                g.regrid()
+        outs.append((g.get_q(), g.get_registers()))
+        g.close()
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
