@@ -63,14 +63,22 @@ def _peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def _traffic_from_profiles(kernel_key: str):
-    """dram bytes per update launch from a committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "traffic.json")
-    if not os.path.exists(p):
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per interior
+# cell-update of the fused update kernel, from one ncu --set full capture of a
+# 16384-patch launch (radial dam, uniform level 7, 16x16 patches, mbc 2); the
+# summaries are profiles/step2_sw_roe_16x16_<precision>.md.  A launch of n
+# patches moves n * 256 times this.
+DRAM_BYTES_PER_CELL = {
+    ("sw_roe_16x16", "fp32wave"): (158.340352e6 + 89.620224e6) / (16384 * 256),
+    ("sw_roe_16x16", "fp64"): (159.835648e6 + 243.607808e6) / (16384 * 256),
+}
+
+
+def _traffic_per_launch(wl: dict, precision: str, cells_per_launch: float):
+    if wl["name"].startswith("swirl") or wl["mx"] != 16:
         return None
-    with open(p) as f:
-        d = json.load(f)
-    return d.get(kernel_key)
+    b = DRAM_BYTES_PER_CELL.get(("sw_roe_16x16", precision))
+    return None if b is None else b * cells_per_launch
 
 
 class ClockSampler:
@@ -292,7 +300,7 @@ def run_ours(args, wl, rank, world, local_rank):
     peaks = _peaks()
     achieved = upd_bytes / (upd_ms * 1e-3) / 1e9 if upd_ms > 0 else None
     per_launch_bytes = upd_bytes / max(upd_launches, 1)
-    traffic = _traffic_from_profiles(f"{wl['name']}:{args.precision}")
+    traffic = _traffic_per_launch(wl, args.precision, per_launch_bytes / (8 * (2 * gc.meqn + gc.maux)))
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": (achieved / peaks["hbm_gbs"]) if achieved else None, "traffic": traffic,
                 "peak_source": peaks["source"], "kernel": "step2 fused update",
