@@ -152,6 +152,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_event_elapsed": [P, I, I, dp],
         "fc2d_b200_get_stream": [P, ctypes.POINTER(P)],
         "fc2d_b200_set_graphs": [P, I],
+        "fc2d_b200_mass_noalloc": [P, ctypes.POINTER(ctypes.c_double)],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -288,6 +289,12 @@ class Solver:
     def mass(self) -> np.ndarray:
         out = np.zeros(self.opts.meqn, np.float64)
         self._check("fc2d_b200_mass", self.lib.fc2d_b200_mass(self.h, _dp(out)))
+        return out
+
+    def mass_noalloc(self) -> np.ndarray:
+        """mass() through the allocation-free entry point (static device scratch)."""
+        out = np.zeros(self.opts.meqn, np.float64)
+        self._check("fc2d_b200_mass_noalloc", self.lib.fc2d_b200_mass_noalloc(self.h, _dp(out)))
         return out
 
     @property

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 #include "apps.hpp"
@@ -981,5 +982,50 @@ extern "C" int fc2d_b200_set_graphs(fc2d_b200_solver_t* s, int enable)
     if (!s) return fail(FC2D_B200_EINVAL, "null solver");
     s->use_graphs = enable != 0;
     invalidate_graph(s);
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Mass without device allocation: the scratch is the file-scope device array of
+// k_mass_noalloc.cu, whose address is resolved once per device (with that
+// device current) and cached.
+// ---------------------------------------------------------------------------
+static std::mutex g_scratch_mu;
+static double* g_scratch_addr[128];
+
+static int scratch_for_device(int dev, double** out)
+{
+    if (dev < 0 || dev >= 128) return fail(FC2D_B200_EINVAL, "device ordinal out of range for the mass scratch");
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    if (!g_scratch_addr[dev]) {
+        int cur = -1;
+        CK(cudaGetDevice(&cur));
+        if (cur != dev) CK(cudaSetDevice(dev));
+        double* p = nullptr;
+        cudaError_t e = mass_scratch_address(&p);
+        if (cur != dev) cudaSetDevice(cur);
+        if (e != cudaSuccess || !p)
+            return fail(FC2D_B200_ECUDA, std::string("cudaGetSymbolAddress(mass scratch): ") + cudaGetErrorString(e));
+        g_scratch_addr[dev] = p;
+    }
+    *out = g_scratch_addr[dev];
+    return 0;
+}
+
+extern "C" int fc2d_b200_mass_noalloc(fc2d_b200_solver_t* s, double* out)
+{
+    if (!s || !out || !s->initialized) return fail(FC2D_B200_EINVAL, "bad arguments");
+    const long long np = s->forest.np(), meqn = s->d.meqn;
+    if (np * meqn + meqn > (long long)MASS_SCRATCH_DOUBLES)
+        return fail(FC2D_B200_EINVAL, "fc2d_b200_mass_noalloc: npatches*meqn + meqn = " + std::to_string(np * meqn + meqn) +
+                                          " exceeds the static scratch of " + std::to_string((int)MASS_SCRATCH_DOUBLES) +
+                                          " doubles; use fc2d_b200_mass");
+    double* scratch = nullptr;
+    int rc = scratch_for_device(s->o.device, &scratch);
+    if (rc) return rc;
+    launch_mass_noalloc(s->d, s->q, s->desc, (int)np, scratch, s->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, scratch + np * meqn, sizeof(double) * (size_t)meqn, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
     return 0;
 }

@@ -60,6 +60,16 @@ void launch_tag(const Dims& d, const double* q, const PatchDesc* desc, int np, d
 // Repopulation after adapt: op kind 0 copy old slot, 1 interpolate2fine from old parent (igrid),
 // 2 average2coarse from 4 old children (src = first child slot; children consecutive by igrid
 // via child_slots).
+// ---- allocation-free mass (k_mass_noalloc.cu) ------------------------------------
+// Capacity of the file-scope device scratch: patch partials (npatches*meqn) plus
+// the meqn results must fit.  1 MiB.
+enum { MASS_SCRATCH_DOUBLES = 131072 };
+// Device address of the scratch on the current device.
+cudaError_t mass_scratch_address(double** ptr);
+// Partials, then per-field sums at scratch[np*meqn + m]; the stream orders the two launches.
+void launch_mass_noalloc(const Dims& d, const double* q, const PatchDesc* desc, int np, double* scratch,
+                         cudaStream_t st);
+
 struct RepopOp { int kind, dst, src, igrid; int child[4]; };
 void launch_repop(const Dims& d, const RepopOp* ops, int nops, const double* oq, double* nq,
                   const double* oqlast, double* nqlast, const double* oqi, double* nqi,

@@ -139,6 +139,16 @@ int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed);
 /* Kahan-summed mass per field over interior cells, FP64
  * (fclaw2d_clawpatch46_diagnostics.f:13-55). */
 int fc2d_b200_mass(fc2d_b200_solver_t* s, double* out);
+/* fc2d_b200_mass computed without allocating memory (no counterpart in the
+ * reference): the patch partials and the per-field sums go to one static device
+ * array of FC2D_B200_MASS_SCRATCH_DOUBLES doubles per device, so
+ * npatches*meqn + meqn must not exceed it (else FC2D_B200_EINVAL, nothing runs).
+ * Same result as fc2d_b200_mass, bit for bit.  No part of the scratch has to
+ * start at zero.  The first call on a device resolves the scratch address; make
+ * it before any stream capture begins on that device.  Calls that overlap in
+ * time on one device (several host threads) share the scratch and race. */
+#define FC2D_B200_MASS_SCRATCH_DOUBLES 131072
+int fc2d_b200_mass_noalloc(fc2d_b200_solver_t* s, double* out);
 /* Interior cell updates performed so far (sum over levels of patches*mx*my per step). */
 int fc2d_b200_cell_updates(const fc2d_b200_solver_t* s, double* out);
 /* Wait for all device work of the solver's stream. */
