@@ -75,6 +75,12 @@ struct fc2d_b200_solver {
     double *q = nullptr, *qlast = nullptr, *qinterp = nullptr, *aux = nullptr, *regs = nullptr;
     PatchDesc* desc = nullptr;
     int cap = 0;                                   // patch capacity of the slabs
+    // second set of slabs: regrid repopulates into it and swaps, so a regrid
+    // allocates only when the forest outgrows the spare's capacity
+    struct Spare { double *q = nullptr, *qlast = nullptr, *qinterp = nullptr, *aux = nullptr, *regs = nullptr;
+                   PatchDesc* desc = nullptr; int cap = 0; } spare;
+    DevVec<int> flags_dev;                         // regrid tag flags
+    DevVec<RepopOp> repop_dev;                     // regrid repopulation ops
     std::vector<double> aux_host;                  // static aux mirror (level-major)
     DevVec<CopyEnt> t_copy, t_avg;
     DevVec<InterpEnt> t_interp;
@@ -147,6 +153,37 @@ static int alloc_slabs(fc2d_b200_solver* s, int np)
         if (s->aux) cudaFree(s->aux); cudaFree(s->regs); cudaFree(s->desc);
     }
     s->q = q; s->qlast = ql; s->qinterp = qi; s->aux = aux; s->regs = regs; s->desc = desc; s->cap = cap;
+    return 0;
+}
+
+static void free_spare(fc2d_b200_solver* s)
+{
+    auto& sp = s->spare;
+    if (sp.q) cudaFree(sp.q);
+    if (sp.qlast) cudaFree(sp.qlast);
+    if (sp.qinterp) cudaFree(sp.qinterp);
+    if (sp.aux) cudaFree(sp.aux);
+    if (sp.regs) cudaFree(sp.regs);
+    if (sp.desc) cudaFree(sp.desc);
+    sp = fc2d_b200_solver::Spare{};
+}
+
+// Make the spare slabs hold np patches.  Contents are undefined: regrid's
+// repopulation writes every array of every new patch.
+static int ensure_spare(fc2d_b200_solver* s, int np)
+{
+    auto& sp = s->spare;
+    if (sp.q && np <= sp.cap) return 0;
+    free_spare(s);
+    const Dims& d = s->d;
+    const int cap = np + np / 4 + 16;
+    CK(cudaMalloc(&sp.q, (size_t)cap * d.nq() * sizeof(double)));
+    CK(cudaMalloc(&sp.qlast, (size_t)cap * d.nq() * sizeof(double)));
+    if (s->o.subcycle) CK(cudaMalloc(&sp.qinterp, (size_t)cap * d.nq() * sizeof(double)));
+    if (d.maux > 0) CK(cudaMalloc(&sp.aux, (size_t)cap * d.naux() * sizeof(double)));
+    CK(cudaMalloc(&sp.regs, (size_t)cap * d.nreg() * sizeof(double)));
+    CK(cudaMalloc(&sp.desc, (size_t)cap * sizeof(PatchDesc)));
+    sp.cap = cap;
     return 0;
 }
 
@@ -455,6 +492,7 @@ extern "C" int fc2d_b200_destroy(fc2d_b200_solver_t* s)
     for (auto e : s->user_ev) cudaEventDestroy(e);
     cudaFree(s->q); cudaFree(s->qlast); if (s->qinterp) cudaFree(s->qinterp);
     if (s->aux) cudaFree(s->aux); cudaFree(s->regs); cudaFree(s->desc);
+    free_spare(s);
     cudaFree(s->cfl_dev); cudaFreeHost(s->cfl_host);
     invalidate_graph(s);
     cudaFree(s->params_dev); cudaFreeHost(s->params_host);
@@ -807,13 +845,11 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     const Dims& d = s->d;
     const Forest& f = s->forest;
     const int np = f.np();
-    int* flags_dev;
-    CK(cudaMalloc(&flags_dev, sizeof(int) * (size_t)np));
-    launch_tag(d, s->q, s->desc, np, s->o.refine_threshold, s->o.coarsen_threshold, flags_dev, s->st);
     std::vector<int> flags(np);
-    CK(cudaMemcpyAsync(flags.data(), flags_dev, sizeof(int) * (size_t)np, cudaMemcpyDeviceToHost, s->st));
+    CK(s->flags_dev.assign(flags, s->st));
+    launch_tag(d, s->q, s->desc, np, s->o.refine_threshold, s->o.coarsen_threshold, s->flags_dev.p, s->st);
+    CK(cudaMemcpyAsync(flags.data(), s->flags_dev.p, sizeof(int) * (size_t)np, cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
-    cudaFree(flags_dev);
     // cb_regrid_tag4coarsening (families) then cb_fclaw2d_regrid_tag4refinement
     std::vector<int> mark(np, 0);
     for (int i = 0; i < np; i++) {
@@ -864,21 +900,18 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
         }
         ops[i] = op;
     }
-    // new slabs; the old ones are read by the repopulation kernel, then freed
-    double *oq = s->q, *oql = s->qlast, *oqi = s->qinterp, *oaux = s->aux, *oregs = s->regs;
-    PatchDesc* odesc = s->desc;
-    s->q = nullptr; s->cap = 0;
-    s->qlast = nullptr; s->qinterp = nullptr; s->aux = nullptr; s->regs = nullptr; s->desc = nullptr;
-    int rc = alloc_slabs(s, nf.np());
+    // repopulate into the spare slabs, then swap them with the current ones
+    int rc = ensure_spare(s, nf.np());
     if (rc) return rc;
-    RepopOp* ops_dev;
-    CK(cudaMalloc(&ops_dev, sizeof(RepopOp) * ops.size()));
-    CK(cudaMemcpyAsync(ops_dev, ops.data(), sizeof(RepopOp) * ops.size(), cudaMemcpyHostToDevice, s->st));
-    launch_repop(d, ops_dev, (int)ops.size(), oq, s->q, oql, s->qlast, oqi, s->qinterp, oregs, s->regs, s->st);
-    if (d.maux > 0) CK(cudaMemcpyAsync(s->aux, naux.data(), naux.size() * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    auto& sp = s->spare;
+    CK(s->repop_dev.assign(ops, s->st));
+    launch_repop(d, s->repop_dev.p, (int)ops.size(), s->q, sp.q, s->qlast, sp.qlast, s->qinterp, sp.qinterp, s->regs,
+                 sp.regs, s->st);
+    if (d.maux > 0) CK(cudaMemcpyAsync(sp.aux, naux.data(), naux.size() * sizeof(double), cudaMemcpyHostToDevice, s->st));
     CK(cudaStreamSynchronize(s->st));
-    cudaFree(ops_dev);
-    cudaFree(oq); cudaFree(oql); if (oqi) cudaFree(oqi); if (oaux) cudaFree(oaux); cudaFree(oregs); cudaFree(odesc);
+    std::swap(s->q, sp.q); std::swap(s->qlast, sp.qlast); std::swap(s->qinterp, sp.qinterp);
+    std::swap(s->aux, sp.aux); std::swap(s->regs, sp.regs); std::swap(s->desc, sp.desc);
+    std::swap(s->cap, sp.cap);
     s->aux_host.swap(naux);
     s->forest = std::move(nf);
     invalidate_graph(s);

@@ -246,16 +246,23 @@ struct TableCtx {
     }
 };
 
-// Keeps the last entry written to each destination, in first-write order.
+// Keeps the last entry written to each destination, in first-write order.  The
+// destination cell (slot p, plane-0 offset c) indexes a dense slot map shared by
+// all tables of a build; the touched slots are cleared again on destruction.
 template <class E>
 struct LastWriter {
     std::vector<E> v;
-    std::unordered_map<int, int> at;
+    std::vector<int>& at;
+    int nq, nxy;
+    std::vector<int> touched;
+    LastWriter(std::vector<int>& slots, int nq_, int nxy_) : at(slots), nq(nq_), nxy(nxy_) {}
+    ~LastWriter() { for (int k : touched) at[k] = -1; }
     void put(const E& e)
     {
-        auto it = at.find(e.dst);
-        if (it == at.end()) { at[e.dst] = (int)v.size(); v.push_back(e); }
-        else v[it->second] = e;
+        const int k = (e.dst / nq) * nxy + e.dst % nq;
+        int& a = at[k];
+        if (a < 0) { a = (int)v.size(); touched.push_back(k); v.push_back(e); }
+        else v[a] = e;
     }
 };
 
@@ -265,6 +272,8 @@ void build_tables(const Forest& f, const int mthbc[4], std::vector<LevelTables>&
 {
     TableCtx T(f);
     const int mx = T.mx, my = T.my, mbc = T.mbc;
+    const int nxy = T.nx * (my + 2 * mbc);
+    std::vector<int> slots((size_t)f.np() * nxy, -1);
     out.assign(33, LevelTables());
     for (int l = 0; l < 33; l++) {
         LevelTables& LT = out[l];
@@ -272,7 +281,7 @@ void build_tables(const Forest& f, const int mthbc[4], std::vector<LevelTables>&
         if (p0 == p1) { LT.ss_start.assign(1, 0); LT.f2c_start.assign(1, 0); continue; }
         // ---- copy2ghost: face pass then corner pass (fclaw2d_clawpatch46_copy.f) ----
         {
-            LastWriter<CopyEnt> W;
+            LastWriter<CopyEnt> W(slots, T.nq, nxy);
             for (int ip = p0; ip < p1; ip++) {
                 const PatchInfo& P = f.p[ip];
                 for (int fc = 0; fc < 4; fc++) {
@@ -307,7 +316,7 @@ void build_tables(const Forest& f, const int mthbc[4], std::vector<LevelTables>&
         }
         // ---- average2ghost (coarse = this level) ----
         {
-            LastWriter<CopyEnt> W;
+            LastWriter<CopyEnt> W(slots, T.nq, nxy);
             for (int ip = p0; ip < p1; ip++) {
                 const PatchInfo& C = f.p[ip];
                 if (!C.on_cf) continue;
@@ -356,7 +365,7 @@ void build_tables(const Forest& f, const int mthbc[4], std::vector<LevelTables>&
         }
         // ---- interpolate2ghost (coarse = this level) ----
         {
-            LastWriter<InterpEnt> W;
+            LastWriter<InterpEnt> W(slots, T.nq, nxy);
             auto validi = [&](int i, int j) { return 1 - mbc <= i && i <= mx + mbc && 1 - mbc <= j && j <= my + mbc; };
             auto emit = [&](int cp, int ic, int jc, int fp, int di, int dj) {
                 for (int m = 0; m < 4; m++) {
@@ -413,19 +422,22 @@ void build_tables(const Forest& f, const int mthbc[4], std::vector<LevelTables>&
         }
         // ---- setphysical: clawpack46_bc2_default with chains resolved per patch ----
         {
+            std::vector<int> wsrc(nxy, -1), wneg(nxy, 0);
             for (int ip = p0; ip < p1; ip++) {
                 const PatchInfo& P = f.p[ip];
                 if (!(P.phys[0] || P.phys[1] || P.phys[2] || P.phys[3])) continue;
-                // written cell -> (source cell, negate mask), within this bc2 call
-                std::map<int, std::pair<int, int>> wr;
+                // written cell -> (source cell, negate mask), within this bc2 call;
+                // indexed by the plane-0 offset of the cell inside the patch
+                const int base = T.cell(ip, 1 - mbc, 1 - mbc);
+                std::fill(wsrc.begin(), wsrc.end(), -1);
                 std::vector<int> order;
                 auto put = [&](int di, int dj, int si, int sj, int neg) {
                     const int dst = T.cell(ip, di, dj);
                     int src = T.cell(ip, si, sj);
-                    auto it = wr.find(src);
-                    if (it != wr.end()) { neg ^= it->second.second; src = it->second.first; }
-                    if (wr.find(dst) == wr.end()) order.push_back(dst);
-                    wr[dst] = {src, neg};
+                    if (wsrc[src - base] >= 0) { neg ^= wneg[src - base]; src = wsrc[src - base]; }
+                    if (wsrc[dst - base] < 0) order.push_back(dst);
+                    wsrc[dst - base] = src;
+                    wneg[dst - base] = neg;
                 };
                 const int NEG2 = 1 << 1, NEG3 = 1 << 2;   // field 2 (x momentum) / field 3 (y momentum)
                 int bc[4];
@@ -438,10 +450,7 @@ void build_tables(const Forest& f, const int mthbc[4], std::vector<LevelTables>&
                 if (bc[2] == 3) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, 1 - jbc, i, jbc, NEG3);
                 if (bc[3] == 1) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, my + jbc, i, my, 0);
                 if (bc[3] == 3) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, my + jbc, i, my + 1 - jbc, NEG3);
-                for (int dst : order) {
-                    const auto& s = wr[dst];
-                    LT.phys.push_back({dst, s.first, s.second, 0});
-                }
+                for (int dst : order) LT.phys.push_back({dst, wsrc[dst - base], wneg[dst - base], 0});
             }
         }
         // ---- time interpolation patches ----
