@@ -39,7 +39,8 @@ enum {
     ORC_PROB_SWIRL = 0,       /* applications/clawpack/advection/2d/swirl */
     ORC_PROB_RADIALDAM = 1,   /* applications/clawpack/shallow/2d/radialdam */
     ORC_PROB_UNIFORM_SW = 2,  /* radial dam initial data on a uniform grid (same app) */
-    ORC_PROB_TSUNAMI = 3      /* batched bathymetry problem (rpn2_tsunami) */
+    ORC_PROB_TSUNAMI = 3,     /* batched bathymetry problem (rpn2_tsunami) */
+    ORC_PROB_SHOCKBUBBLE = 4  /* applications/clawpack/euler/2d/shockbubble (Mach-M shock, light bubble) */
 };
 
 typedef struct orc_config {
@@ -68,6 +69,9 @@ typedef struct orc_config {
     double r0, hin, hout, x0, y0;   /* radial dam */
     int qinit_sharp;       /* 1: cell-centre test instead of cellave2 quadrature */
     double pdata[32];      /* extra problem parameters (tsunami bumps etc.) */
+    /* Euler (shock-bubble): gas constant, shock Mach number, bubble density,
+     * Newton tolerance on p* (relative change); bubble centre/radius in x0, y0, r0 */
+    double gamma, mach, rhob, newton_tol;
     int nthreads;          /* OpenMP threads for the patch loops (0 = default) */
 } orc_config;
 
@@ -108,6 +112,20 @@ double orc_patch_step2(const orc_config* cfg, double* q, const double* aux,
                        double* fm, double* fp, double* gm, double* gp);
 /* clawpack46_inlinelimiter phi(r) for one r (tests of the limiter table). */
 double orc_limiter_phi(int mthlim, double r);
+
+/* ---- exact Euler Riemann solver (orc_euler.c), exposed for unit tests ----- */
+double orc_log(double x);
+double orc_exp(double y);
+double orc_pow(double x, double a);
+/* primitive (rho, u, p) states; seed <= 0 selects the PVRS start.  out[6] =
+ * p*, u*, rho*L, rho*R, a*L, a*R.  Returns the Newton iterations. */
+int  orc_euler_star(double gam, const double* wl, const double* wr, double seed, double tol, double* out);
+/* conserved (rho, m_n, m_t, E) states -> waves[3][4], speeds[3], amdq, apdq */
+int  orc_euler_interface(double gam, double tol, const double* ql, const double* qr, double seed,
+                         double wave[3][4], double s[3], double* amdq, double* apdq);
+void orc_euler_postshock(double gam, double mach, double* out);
+/* Newton-iteration histogram of all exact solves so far (32 bins; reset if asked). */
+void orc_newton_hist(long* out, int reset);
 
 #ifdef __cplusplus
 }

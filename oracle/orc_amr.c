@@ -319,7 +319,8 @@ static void setphysical(orc_sim* s, int level, int time_interp)
         int mthbc[4], any = 0;
         for (int f = 0; f < 4; f++) { mthbc[f] = P->phys[f] ? s->cfg.mthbc[f] : -1; any |= P->phys[f]; }
         if (!any) continue;
-        orc_bc2(s->cfg.mx, s->cfg.my, s->cfg.mbc, s->cfg.meqn, tsdata(P, time_interp), mthbc);
+        orc_bc2(s->cfg.mx, s->cfg.my, s->cfg.mbc, s->cfg.meqn, tsdata(P, time_interp), mthbc,
+                s->cfg.problem == ORC_PROB_SHOCKBUBBLE ? s->inflow : NULL);
     }
 }
 
@@ -733,6 +734,11 @@ orc_sim* orc_create(const orc_config* cfg)
     s->nq = (size_t)s->nx * s->ny * cfg->meqn;
     s->naux = (size_t)s->nx * s->ny * (cfg->maux > 0 ? cfg->maux : 0);
     s->dummy = (double*)calloc((size_t)(cfg->mx + 4 * cfg->mbc) * (cfg->my + 4 * cfg->mbc) * cfg->meqn, sizeof(double));
+    if (cfg->problem == ORC_PROB_SHOCKBUBBLE) {
+        double ps[3];
+        orc_euler_postshock(cfg->gamma, cfg->mach, ps);
+        s->inflow[0] = ps[0]; s->inflow[1] = ps[0] * ps[1]; s->inflow[2] = 0.0; s->inflow[3] = ps[2];
+    }
 #ifdef _OPENMP
     s->nthreads = cfg->nthreads > 0 ? cfg->nthreads : omp_get_max_threads();
 #else

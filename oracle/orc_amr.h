@@ -56,6 +56,7 @@ struct orc_sim {
     double cell_updates;
     int nthreads;
     double t_curr;
+    double inflow[8];                 /* shock-bubble inflow state (mthbc = 0 side) */
 };
 
 void orc_copy_face(const orc_sim* s, double* qthis, const double* qnbr, const orc_patch* P, const orc_patch* N, int iface);

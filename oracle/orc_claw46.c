@@ -250,6 +250,7 @@ void orc_rp_select(int rp, orc_rpn2_t* rpn2, orc_rpt2_t* rpt2)
     case ORC_RP_ADVECTION: *rpn2 = rpn2_adv; *rpt2 = rpt2_adv; break;
     case ORC_RP_SW_ROE:    *rpn2 = rpn2_sw_roe; *rpt2 = rpt2_sw_roe; break;
     case ORC_RP_SW_FWAVE:  *rpn2 = orc_rpn2_fwave; *rpt2 = orc_rpt2_fwave; break;
+    case ORC_RP_EULER_EXACT: *rpn2 = orc_rpn2_euler; *rpt2 = orc_rpt2_euler; break;
     default: *rpn2 = NULL; *rpt2 = NULL; break;
     }
 }
@@ -468,7 +469,7 @@ size_t orc_ws_size(int mx, int my, int mbc, int meqn, int maux, int mwaves)
     n += L * (maux > 0 ? maux : 1) * 3;/* aux1..3 */
     n += L * meqn * mwaves + L * mwaves; /* wave, s */
     n += L * meqn * 5;                 /* amdq apdq cqxx bmasdq bpasdq */
-    n += L * 4;                        /* comroe */
+    n += L * 5;                        /* comroe */
     return n;
 }
 
@@ -508,6 +509,9 @@ double orc_step2(const orc_config* cfg, orc_rpn2_t rpn2, orc_rpt2_t rpt2, double
     ctx.v = ctx.u + L;
     ctx.a = ctx.v + L;
     ctx.h = ctx.a + L;
+    ctx.e = ctx.h + L;
+    ctx.gamma = cfg->gamma;
+    ctx.newton_tol = cfg->newton_tol;
     ctx.cfg = cfg;
 
     double cflgrid = 0.0;
@@ -611,12 +615,19 @@ double orc_patch_step2(const orc_config* cfg, double* q, const double* aux,
 }
 
 /* ------------------------------------------------------------------------- */
-/* bc2 default: clawpack46_bc2_default.f:1-213 (mthbc<0 means "not a physical side") */
+/* bc2 default: clawpack46_bc2_default.f:1-213 (mthbc<0 means "not a physical side").
+ * mthbc = 0 (user) with an inflow state: the shock-bubble inflow of
+ * applications/clawpack/euler/2d/shockbubble/user_4.6/bc2.f:53-60 on that side. */
 /* ------------------------------------------------------------------------- */
-void orc_bc2(int mx, int my, int mbc, int meqn, double* q, const int* mthbc)
+void orc_bc2(int mx, int my, int mbc, int meqn, double* q, const int* mthbc, const double* inflow)
 {
     const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
 #define Q(i, j, m) q[QIDX(i, j, m, mbc, nx, ny)]
+    if (mthbc[0] == 0 && inflow) {
+        for (int ibc = 1; ibc <= mbc; ibc++)
+            for (int j = 1 - mbc; j <= my + mbc; j++)
+                for (int m = 1; m <= meqn; m++) Q(1 - ibc, j, m) = inflow[m - 1];
+    }
     if (mthbc[0] == 1) {
         for (int m = 1; m <= meqn; m++) for (int ibc = 1; ibc <= mbc; ibc++)
             for (int j = 1 - mbc; j <= my + mbc; j++) Q(1 - ibc, j, m) = Q(1, j, m);

@@ -17,6 +17,8 @@ typedef struct orc_rpctx {
     double grav;
     double dry_tolerance;
     double* u; double* v; double* a; double* h;   /* common /comroe/ */
+    double* e;                                    /* Euler: gamma1/a^2 (g1a2 of comroe) */
+    double gamma, newton_tol;
     const orc_config* cfg;
 } orc_rpctx;
 
@@ -33,10 +35,17 @@ void orc_rpn2_fwave(orc_rpctx*, int, int, int, int, int, int, int, const double*
 void orc_rpt2_fwave(orc_rpctx*, int, int, int, int, int, int, int, const double*, const double*,
                     const double*, const double*, const double*, int, const double*, double*, double*);
 
+void orc_rpn2_euler(orc_rpctx*, int, int, int, int, int, int, int, const double*, const double*,
+                    const double*, const double*, double*, double*, double*, double*);
+void orc_rpt2_euler(orc_rpctx*, int, int, int, int, int, int, int, const double*, const double*,
+                    const double*, const double*, const double*, int, const double*, double*, double*);
+void orc_euler_cons_flux(double gam, int idir, const double* q, double* flux);
+
 size_t orc_ws_size(int mx, int my, int mbc, int meqn, int maux, int mwaves);
 double orc_step2(const orc_config* cfg, orc_rpn2_t rpn2, orc_rpt2_t rpt2, double* work,
                  double* qold, const double* aux, double dx, double dy, double dt,
                  double* fm, double* fp, double* gm, double* gp, const int* block_corner_count);
-void orc_bc2(int mx, int my, int mbc, int meqn, double* q, const int* mthbc);
+/* inflow: state written by mthbc = 0 (user) sides, NULL for none */
+void orc_bc2(int mx, int my, int mbc, int meqn, double* q, const int* mthbc, const double* inflow);
 
 #endif

@@ -465,6 +465,12 @@ static void rpn2_cons_sw(int meqn, int idir, const double* q, double grav, doubl
     flux[mv - 1] = un * hut;
 }
 
+static void rpn2_cons(const orc_config* c, int idir, const double* q, double* flux)
+{
+    if (c->rp == ORC_RP_EULER_EXACT) orc_euler_cons_flux(c->gamma, idir, q, flux);
+    else rpn2_cons_sw(c->meqn, idir, q, c->grav, flux);
+}
+
 void orc_store_flux(const orc_sim* s, orc_patch* P, double dt)
 {
     const orc_config* c = &s->cfg;
@@ -474,13 +480,13 @@ void orc_store_flux(const orc_sim* s, orc_patch* P, double dt)
     for (int j = 1; j <= my; j++) {
         for (int k = 0; k <= 1; k++) {
             for (int m = 1; m <= meqn; m++) qv[m - 1] = P->q[QIDX(1 - k, j, m, mbc, nx, ny)];
-            rpn2_cons_sw(meqn, 0, qv, c->grav, fl);
+            rpn2_cons(c, 0, qv, fl);
             for (int m = 1; m <= meqn; m++)
                 r->ef[0][RJK(j, m, k, my, meqn)] = r->ef[0][RJK(j, m, k, my, meqn)] + dt * r->el[0][j - 1] * fl[m - 1];
         }
         for (int k = 0; k <= 1; k++) {
             for (int m = 1; m <= meqn; m++) qv[m - 1] = P->q[QIDX(mx + k, j, m, mbc, nx, ny)];
-            rpn2_cons_sw(meqn, 0, qv, c->grav, fl);
+            rpn2_cons(c, 0, qv, fl);
             for (int m = 1; m <= meqn; m++)
                 r->ef[1][RJK(j, m, k, my, meqn)] = r->ef[1][RJK(j, m, k, my, meqn)] + dt * r->el[1][j - 1] * fl[m - 1];
         }
@@ -488,13 +494,13 @@ void orc_store_flux(const orc_sim* s, orc_patch* P, double dt)
     for (int i = 1; i <= mx; i++) {
         for (int k = 0; k <= 1; k++) {
             for (int m = 1; m <= meqn; m++) qv[m - 1] = P->q[QIDX(i, 1 - k, m, mbc, nx, ny)];
-            rpn2_cons_sw(meqn, 1, qv, c->grav, fl);
+            rpn2_cons(c, 1, qv, fl);
             for (int m = 1; m <= meqn; m++)
                 r->ef[2][RJK(i, m, k, mx, meqn)] = r->ef[2][RJK(i, m, k, mx, meqn)] + dt * r->el[2][i - 1] * fl[m - 1];
         }
         for (int k = 0; k <= 1; k++) {
             for (int m = 1; m <= meqn; m++) qv[m - 1] = P->q[QIDX(i, my + k, m, mbc, nx, ny)];
-            rpn2_cons_sw(meqn, 1, qv, c->grav, fl);
+            rpn2_cons(c, 1, qv, fl);
             for (int m = 1; m <= meqn; m++)
                 r->ef[3][RJK(i, m, k, mx, meqn)] = r->ef[3][RJK(i, m, k, mx, meqn)] + dt * r->el[3][i - 1] * fl[m - 1];
         }

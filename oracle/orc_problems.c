@@ -58,6 +58,27 @@ void orc_qinit(const orc_sim* s, orc_patch* P)
                 P->q[QIDX(i, j, 3, mbc, nx, ny)] = 0.0;
             }
         }
+    } else if (c->problem == ORC_PROB_SHOCKBUBBLE) {
+        /* shockbubble/user_4.6/qinit.f:24-62: bubble (by cell centre) of density rhob
+         * at pressure 1, ambient (1, 0, 0, 1/(gamma-1)), post-shock state where the
+         * cell's lower edge is left of x = 0.2 */
+        const double gamma1 = c->gamma - 1.0;
+        for (int i = 1 - mbc; i <= mx + mbc; i++) {
+            const double xclow = P->xlower + (i - 1) * P->dx;
+            const double xc = P->xlower + (i - 0.5) * P->dx;
+            for (int j = 1 - mbc; j <= my + mbc; j++) {
+                const double yc = P->ylower + (j - 0.5) * P->dy;
+                const double r2 = (xc - c->x0) * (xc - c->x0) + (yc - c->y0) * (yc - c->y0);
+                const double win = (r2 - c->r0 * c->r0 < 0.0) ? 1.0 : 0.0;
+                double q[4];
+                q[0] = win * c->rhob + (1.0 - win) * 1.0;
+                q[1] = 0.0;
+                q[2] = 0.0;
+                q[3] = 1.0 / gamma1;
+                if (xclow < 0.2) { q[0] = s->inflow[0]; q[1] = s->inflow[1]; q[2] = 0.0; q[3] = s->inflow[3]; }
+                for (int m = 1; m <= meqn; m++) P->q[QIDX(i, j, m, mbc, nx, ny)] = q[m - 1];
+            }
+        }
     } else if (c->problem == ORC_PROB_TSUNAMI) {
         int nb = (int)c->pdata[2];
         for (int j = 1 - mbc; j <= my + mbc; j++)

@@ -16,7 +16,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "liborc.so")
 
 RP_ADVECTION, RP_SW_ROE, RP_SW_FWAVE, RP_EULER_EXACT = 0, 1, 2, 3
-PROB_SWIRL, PROB_RADIALDAM, PROB_UNIFORM_SW, PROB_TSUNAMI = 0, 1, 2, 3
+PROB_SWIRL, PROB_RADIALDAM, PROB_UNIFORM_SW, PROB_TSUNAMI, PROB_SHOCKBUBBLE = 0, 1, 2, 3, 4
 
 
 class OrcConfig(ctypes.Structure):
@@ -35,14 +35,21 @@ class OrcConfig(ctypes.Structure):
         ("problem", ctypes.c_int), ("grav", ctypes.c_double), ("tperiod", ctypes.c_double),
         ("r0", ctypes.c_double), ("hin", ctypes.c_double), ("hout", ctypes.c_double),
         ("x0", ctypes.c_double), ("y0", ctypes.c_double), ("qinit_sharp", ctypes.c_int),
-        ("pdata", ctypes.c_double * 32), ("nthreads", ctypes.c_int),
+        ("pdata", ctypes.c_double * 32),
+        ("gamma", ctypes.c_double), ("mach", ctypes.c_double), ("rhob", ctypes.c_double),
+        ("newton_tol", ctypes.c_double),
+        ("nthreads", ctypes.c_int),
     ]
 
 
 def build(force: bool = False) -> str:
-    """Compile liborc.so from the sources beside this file (make)."""
-    if force or not os.path.exists(_LIB):
-        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    """Compile liborc.so from the sources beside this file (make; a no-op when up to date)."""
+    cmd = ["make", "-s", "-C", _HERE] + (["-B"] if force else [])
+    try:
+        subprocess.run(cmd, check=True)
+    except (OSError, subprocess.CalledProcessError):
+        if force or not os.path.exists(_LIB):
+            raise
     return _LIB
 
 
@@ -80,6 +87,17 @@ def lib():
                                       ctypes.c_double, dp, dp, dp, dp]
         L.orc_limiter_phi.restype = ctypes.c_double
         L.orc_limiter_phi.argtypes = [ctypes.c_int, ctypes.c_double]
+        for fn in ("orc_log", "orc_exp"):
+            getattr(L, fn).restype = ctypes.c_double
+            getattr(L, fn).argtypes = [ctypes.c_double]
+        L.orc_pow.restype = ctypes.c_double
+        L.orc_pow.argtypes = [ctypes.c_double, ctypes.c_double]
+        L.orc_euler_star.restype = ctypes.c_int
+        L.orc_euler_star.argtypes = [ctypes.c_double, dp, dp, ctypes.c_double, ctypes.c_double, dp]
+        L.orc_euler_interface.restype = ctypes.c_int
+        L.orc_euler_interface.argtypes = [ctypes.c_double, ctypes.c_double, dp, dp, ctypes.c_double, dp, dp, dp, dp]
+        L.orc_euler_postshock.argtypes = [ctypes.c_double, ctypes.c_double, dp]
+        L.orc_newton_hist.argtypes = [ctypes.POINTER(ctypes.c_long), ctypes.c_int]
         _lib = L
     return _lib
 
@@ -99,7 +117,7 @@ def make_config(**kw) -> OrcConfig:
                     fluctuation_correction=1, regrid_interval=0, refine_threshold=0.5,
                     coarsen_threshold=0.1, ax=0.0, bx=1.0, ay=0.0, by=1.0, mi=1, mj=1,
                     problem=0, grav=1.0, tperiod=0.0, r0=0.3, hin=2.0, hout=1.0, x0=0.0, y0=0.0,
-                    qinit_sharp=1, nthreads=0)
+                    qinit_sharp=1, gamma=1.4, mach=1.22, rhob=0.138, newton_tol=1e-10, nthreads=0)
     defaults.update(kw)
     order = defaults.pop("order", (2, 2))
     mthlim = defaults.pop("mthlim", (4,) * 8)
@@ -200,3 +218,32 @@ def patch_step2(cfg: OrcConfig, q: np.ndarray, aux, dx: float, dy: float, dt: fl
 
 def limiter_phi(mthlim: int, r: float) -> float:
     return lib().orc_limiter_phi(mthlim, r)
+
+
+# ---- exact Euler solver (unit tests) -------------------------------------------
+def euler_star(gam, wl, wr, seed=0.0, tol=1e-10):
+    """(p*, u*, rho*L, rho*R, a*L, a*R), Newton iterations for primitive states (rho, u, p)."""
+    a, b = np.asarray(wl, np.float64), np.asarray(wr, np.float64)
+    out = np.zeros(6)
+    it = lib().orc_euler_star(gam, _dptr(a), _dptr(b), seed, tol, _dptr(out))
+    return out, it
+
+
+def euler_interface(gam, ql, qr, seed=0.0, tol=1e-10):
+    """waves (3, 4), speeds (3,), amdq, apdq, iterations for conserved states (rho, m_n, m_t, E)."""
+    a, b = np.ascontiguousarray(ql, np.float64), np.ascontiguousarray(qr, np.float64)
+    w, s, am, ap = np.zeros((3, 4)), np.zeros(3), np.zeros(4), np.zeros(4)
+    it = lib().orc_euler_interface(gam, tol, _dptr(a), _dptr(b), seed, _dptr(w), _dptr(s), _dptr(am), _dptr(ap))
+    return w, s, am, ap, it
+
+
+def euler_postshock(gam, mach):
+    out = np.zeros(3)
+    lib().orc_euler_postshock(gam, mach, _dptr(out))
+    return out
+
+
+def newton_hist(reset=False) -> np.ndarray:
+    out = (ctypes.c_long * 32)()
+    lib().orc_newton_hist(out, int(reset))
+    return np.array(out[:], np.int64)
