@@ -20,8 +20,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libfc2d_b200.so")
 
-RP_ADVECTION, RP_SW_ROE, RP_SW_FWAVE = 0, 1, 2
-APP_NONE, APP_SWIRL, APP_RADIALDAM, APP_TSUNAMI = 0, 1, 2, 3
+RP_ADVECTION, RP_SW_ROE, RP_SW_FWAVE, RP_EULER_EXACT = 0, 1, 2, 3
+APP_NONE, APP_SWIRL, APP_RADIALDAM, APP_TSUNAMI, APP_SHOCKBUBBLE = 0, 1, 2, 3, 4
 PREC_FP64, PREC_FP32WAVE = 0, 1
 
 
@@ -46,7 +46,10 @@ class _Options(ctypes.Structure):
         ("mi", ctypes.c_int), ("mj", ctypes.c_int), ("app", ctypes.c_int), ("grav", ctypes.c_double),
         ("tperiod", ctypes.c_double), ("r0", ctypes.c_double), ("hin", ctypes.c_double),
         ("hout", ctypes.c_double), ("x0", ctypes.c_double), ("y0", ctypes.c_double),
-        ("pdata", ctypes.c_double * 32), ("precision", ctypes.c_int), ("device", ctypes.c_int),
+        ("pdata", ctypes.c_double * 32),
+        ("gamma", ctypes.c_double), ("mach", ctypes.c_double), ("rhob", ctypes.c_double),
+        ("newton_tol", ctypes.c_double),
+        ("precision", ctypes.c_int), ("device", ctypes.c_int),
     ]
 
 
@@ -88,6 +91,10 @@ class Options:
     x0: float = 0.0
     y0: float = 0.0
     pdata: Sequence[float] = field(default_factory=tuple)
+    gamma: float = 1.4
+    mach: float = 1.22
+    rhob: float = 0.138
+    newton_tol: float = 1e-10
     precision: int = PREC_FP64
     device: int = 0
 
@@ -96,7 +103,8 @@ class Options:
         for k in ("mx", "my", "mbc", "meqn", "maux", "mwaves", "mcapa", "use_fwaves", "rp", "minlevel",
                   "maxlevel", "subcycle", "time_sync", "flux_correction", "fluctuation_correction",
                   "refine_threshold", "coarsen_threshold", "ax", "bx", "ay", "by", "mi", "mj", "app", "grav",
-                  "tperiod", "r0", "hin", "hout", "x0", "y0", "precision", "device"):
+                  "tperiod", "r0", "hin", "hout", "x0", "y0", "gamma", "mach", "rhob", "newton_tol",
+                  "precision", "device"):
             setattr(o, k, getattr(self, k))
         for i, v in enumerate(self.order):
             o.order[i] = v
@@ -153,6 +161,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_get_stream": [P, ctypes.POINTER(P)],
         "fc2d_b200_set_graphs": [P, I],
         "fc2d_b200_mass_noalloc": [P, ctypes.POINTER(ctypes.c_double)],
+        "fc2d_b200_newton_histogram": [P, ctypes.POINTER(ctypes.c_ulonglong), I],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -290,6 +299,12 @@ class Solver:
         out = np.zeros(self.opts.meqn, np.float64)
         self._check("fc2d_b200_mass", self.lib.fc2d_b200_mass(self.h, _dp(out)))
         return out
+
+    def newton_histogram(self, reset: bool = False) -> np.ndarray:
+        """Interfaces solved in k Newton iterations (k = 0..31) by the exact Euler solver."""
+        out = (ctypes.c_ulonglong * 32)()
+        self._check("fc2d_b200_newton_histogram", self.lib.fc2d_b200_newton_histogram(self.h, out, int(reset)))
+        return np.array(out[:], np.int64)
 
     def mass_noalloc(self) -> np.ndarray:
         """mass() through the allocation-free entry point (static device scratch)."""

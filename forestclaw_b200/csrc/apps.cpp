@@ -7,6 +7,10 @@
 //   radial dam: applications/clawpack/shallow/2d/radialdam/user_4.6/qinit.f with the
 //               disc test at the cell centre.
 //   tsunami:    bathymetry b = -1 + 0.5 exp(-50|x-c|^2) in aux(:,:,1), surface eta = sum of bumps.
+//   shock-bubble: applications/clawpack/euler/2d/shockbubble/user_4.6/qinit.f:24-62 (bubble by
+//               cell centre), inflow of user_4.6/bc2.f:53-60, post-shock state from the
+//               Rankine-Hugoniot relations of setprob.f:59-62 for the pressure ratio of a
+//               Mach-M shock, 1 + 2 gamma (M^2 - 1) / (gamma + 1).
 //   tagging:    fort_4.6/fclaw2d_clawpatch46_tag4refinement.f / _tag4coarsening.f with the
 //               gradient criterion (fort_user/fclaw2d_clawpatch_gradient_exceeds_th.f90) times dx.
 #include "apps.hpp"
@@ -71,6 +75,26 @@ void app_qinit(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, 
                 q[qi(d, i, j, 3)] = 0.0;
             }
         }
+    } else if (o.app == FC2D_B200_APP_SHOCKBUBBLE) {
+        double qinf[4];
+        app_inflow_state(o, qinf);
+        const double gamma1 = o.gamma - 1.0;
+        for (int i = 1 - mbc; i <= mx + mbc; i++) {
+            const double xclow = P.xlower + (i - 1) * P.dx;
+            const double xc = P.xlower + (i - 0.5) * P.dx;
+            for (int j = 1 - mbc; j <= my + mbc; j++) {
+                const double yc = P.ylower + (j - 0.5) * P.dy;
+                const double r2 = (xc - o.x0) * (xc - o.x0) + (yc - o.y0) * (yc - o.y0);
+                const double win = (r2 - o.r0 * o.r0 < 0.0) ? 1.0 : 0.0;
+                double v[4];
+                v[0] = win * o.rhob + (1.0 - win) * 1.0;
+                v[1] = 0.0;
+                v[2] = 0.0;
+                v[3] = 1.0 / gamma1;
+                if (xclow < 0.2) { v[0] = qinf[0]; v[1] = qinf[1]; v[2] = 0.0; v[3] = qinf[3]; }
+                for (int m = 1; m <= meqn; m++) q[qi(d, i, j, m)] = v[m - 1];
+            }
+        }
     } else if (o.app == FC2D_B200_APP_TSUNAMI) {
         const int nb = (int)o.pdata[2];
         for (int j = 1 - mbc; j <= my + mbc; j++)
@@ -88,6 +112,18 @@ void app_qinit(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, 
                 q[qi(d, i, j, 3)] = 0.0;
             }
     }
+}
+
+bool app_inflow_state(const fc2d_b200_options_t& o, double* q)
+{
+    if (o.app != FC2D_B200_APP_SHOCKBUBBLE) return false;
+    const double gam = o.gamma, gamma1 = gam - 1.0, mach = o.mach;
+    const double pinf = 1.0 + 2.0 * gam * (mach * mach - 1.0) / (gam + 1.0);
+    const double rinf = (gamma1 + (gam + 1.0) * pinf) / ((gam + 1.0) + gamma1 * pinf);
+    const double vinf = (1.0 / std::sqrt(gam)) * (pinf - 1.0) / std::sqrt(0.5 * ((gam + 1.0) / gam) * pinf + 0.5 * gamma1 / gam);
+    const double einf = 0.5 * rinf * vinf * vinf + pinf / gamma1;
+    q[0] = rinf; q[1] = rinf * vinf; q[2] = 0.0; q[3] = einf;
+    return true;
 }
 
 static bool grad_exceeds(const Dims& d, const PatchInfo& P, const double* q, int i, int j, double thr)

@@ -32,6 +32,9 @@ struct StepParams {
     double grav;
     double dry_tolerance;
     double vt;              // swirl: cos(2 pi (t + dt/2) / T), computed on the host
+    double gamma;           // Euler: ratio of specific heats
+    double newton_tol;      // Euler: Newton tolerance on the relative change of p*
+    unsigned long long* newton_hist;   // Euler: 32-bin histogram of Newton iterations (or null)
 };
 
 }  // namespace fcb

@@ -80,6 +80,9 @@ struct fc2d_b200_solver {
     struct Spare { double *q = nullptr, *qlast = nullptr, *qinterp = nullptr, *aux = nullptr, *regs = nullptr;
                    PatchDesc* desc = nullptr; int cap = 0; } spare;
     DevVec<int> flags_dev;                         // regrid tag flags
+    bool has_inflow = false;                       // mthbc = 0 sides take bc_dev (app inflow state)
+    double* bc_dev = nullptr;                      // 8 doubles
+    unsigned long long* newton_hist = nullptr;     // 32 bins, exact Euler solver
     DevVec<RepopOp> repop_dev;                     // regrid repopulation ops
     std::vector<double> aux_host;                  // static aux mirror (level-major)
     DevVec<CopyEnt> t_copy, t_avg;
@@ -205,7 +208,7 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
     }
     if (!hd.empty()) CK(cudaMemcpyAsync(s->desc, hd.data(), hd.size() * sizeof(PatchDesc), cudaMemcpyHostToDevice, s->st));
     std::vector<LevelTables> T;
-    build_tables(f, s->o.mthbc, T);
+    build_tables(f, s->o.mthbc, s->has_inflow, T);
     std::vector<CopyEnt> copy, avg;
     std::vector<InterpEnt> interp;
     std::vector<PhysEnt> phys;
@@ -277,6 +280,9 @@ static int update_level(fc2d_b200_solver* s, int level, double t, double dt)
     sp.dt = dt; sp.t = t; sp.grav = s->o.grav;
     sp.dry_tolerance = s->o.pdata[31] > 0 ? s->o.pdata[31] : 1e-3;
     sp.vt = 0.0;
+    sp.gamma = s->o.gamma;
+    sp.newton_tol = s->o.newton_tol;
+    sp.newton_hist = s->newton_hist;
     if (s->o.app == FC2D_B200_APP_SWIRL && s->o.tperiod != 0.0) {
         const double pi = 4.0 * std::atan(1.0), pi2 = 2.0 * pi;
         sp.vt = std::cos(pi2 * (t + dt / 2.0) / s->o.tperiod);
@@ -340,7 +346,7 @@ static void phys_range(fc2d_b200_solver* s, int a, int b, int ti)
     const int off = s->lr[a].phys_off, n = s->lr[b].phys_off + s->lr[b].phys_n - off;
     if (n <= 0) return;
     if (s->fill) s->total_launches++;
-    if (s->emit) launch_phys(s->d, tsdata(s, ti), s->t_phys.p + off, n, s->st);
+    if (s->emit) launch_phys(s->d, tsdata(s, ti), s->t_phys.p + off, n, s->bc_dev, s->st);
 }
 static void interpolate2ghost(fc2d_b200_solver* s, int l, int ti)
 {
@@ -453,7 +459,9 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
         return fail(FC2D_B200_EINVAL, "bad patch dimensions (need mx,my>0, mbc>=2, 0<meqn<=8)");
     if ((o.mx % 2) || (o.my % 2)) return fail(FC2D_B200_EINVAL, "mx and my must be even");
     if (o.time_sync && o.rp == FC2D_B200_RP_ADVECTION)
-        return fail(FC2D_B200_EINVAL, "time sync needs a shallow-water flux function (rpn2_cons)");
+        return fail(FC2D_B200_EINVAL, "time sync needs a flux function (rpn2_cons): shallow water or Euler");
+    if (o.rp == FC2D_B200_RP_EULER_EXACT && (o.meqn != 4 || o.mwaves != 3 || !(o.gamma > 1.0) || !(o.newton_tol > 0.0)))
+        return fail(FC2D_B200_EINVAL, "exact Euler solver needs meqn 4, mwaves 3, gamma > 1, newton_tol > 0");
     if (o.minlevel < 0 || o.maxlevel < o.minlevel || o.maxlevel > 20)
         return fail(FC2D_B200_EINVAL, "bad minlevel/maxlevel");
     const bool sup = (o.precision == FC2D_B200_PREC_FP32WAVE) ? step2_f32w_supported(o.rp, o.mx, o.my, o.mbc)
@@ -473,6 +481,14 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
     CK(cudaMalloc(&s->cfl_dev, sizeof(unsigned long long)));
     CK(cudaMallocHost(&s->cfl_host, sizeof(unsigned long long)));
     CK(cudaMalloc(&s->params_dev, sizeof(StepParams) * fc2d_b200_solver::PCAP));
+    {
+        double bc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        s->has_inflow = app_inflow_state(s->o, bc);
+        CK(cudaMalloc(&s->bc_dev, sizeof(bc)));
+        CK(cudaMemcpy(s->bc_dev, bc, sizeof(bc), cudaMemcpyHostToDevice));
+        CK(cudaMalloc(&s->newton_hist, 32 * sizeof(unsigned long long)));
+        CK(cudaMemset(s->newton_hist, 0, 32 * sizeof(unsigned long long)));
+    }
     CK(cudaMallocHost(&s->params_host, sizeof(StepParams) * fc2d_b200_solver::PCAP));
     {   // set the kernel's shared-memory attribute outside any stream capture
         cudaError_t e = (o.precision == FC2D_B200_PREC_FP32WAVE)
@@ -497,6 +513,7 @@ extern "C" int fc2d_b200_destroy(fc2d_b200_solver_t* s)
     invalidate_graph(s);
     cudaFree(s->params_dev); cudaFreeHost(s->params_host);
     if (s->mass_dev) cudaFree(s->mass_dev);
+    cudaFree(s->bc_dev); cudaFree(s->newton_hist);
     cudaStreamDestroy(s->st);
     delete s;
     return 0;
@@ -1060,5 +1077,17 @@ extern "C" int fc2d_b200_mass_noalloc(fc2d_b200_solver_t* s, double* out)
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, scratch + np * meqn, sizeof(double) * (size_t)meqn, cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+extern "C" int fc2d_b200_newton_histogram(fc2d_b200_solver_t* s, unsigned long long* out, int reset)
+{
+    if (!s || !out) return fail(FC2D_B200_EINVAL, "null argument");
+    CK(cudaMemcpyAsync(out, s->newton_hist, 32 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    if (reset) {
+        CK(cudaMemsetAsync(s->newton_hist, 0, 32 * sizeof(unsigned long long), s->st));
+        CK(cudaStreamSynchronize(s->st));
+    }
     return 0;
 }

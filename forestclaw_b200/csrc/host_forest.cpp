@@ -268,7 +268,7 @@ struct LastWriter {
 
 }  // namespace
 
-void build_tables(const Forest& f, const int mthbc[4], std::vector<LevelTables>& out)
+void build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<LevelTables>& out)
 {
     TableCtx T(f);
     const int mx = T.mx, my = T.my, mbc = T.mbc;
@@ -422,7 +422,7 @@ void build_tables(const Forest& f, const int mthbc[4], std::vector<LevelTables>&
         }
         // ---- setphysical: clawpack46_bc2_default with chains resolved per patch ----
         {
-            std::vector<int> wsrc(nxy, -1), wneg(nxy, 0);
+            std::vector<int> wsrc(nxy, -1), wneg(nxy, 0), wconst(nxy, 0);
             for (int ip = p0; ip < p1; ip++) {
                 const PatchInfo& P = f.p[ip];
                 if (!(P.phys[0] || P.phys[1] || P.phys[2] || P.phys[3])) continue;
@@ -433,15 +433,24 @@ void build_tables(const Forest& f, const int mthbc[4], std::vector<LevelTables>&
                 std::vector<int> order;
                 auto put = [&](int di, int dj, int si, int sj, int neg) {
                     const int dst = T.cell(ip, di, dj);
-                    int src = T.cell(ip, si, sj);
-                    if (wsrc[src - base] >= 0) { neg ^= wneg[src - base]; src = wsrc[src - base]; }
+                    int src = T.cell(ip, si, sj), cst = 0;
+                    if (wsrc[src - base] >= 0) { neg ^= wneg[src - base]; cst = wconst[src - base]; src = wsrc[src - base]; }
                     if (wsrc[dst - base] < 0) order.push_back(dst);
                     wsrc[dst - base] = src;
                     wneg[dst - base] = neg;
+                    wconst[dst - base] = cst;
+                };
+                auto put_const = [&](int di, int dj) {
+                    const int dst = T.cell(ip, di, dj);
+                    if (wsrc[dst - base] < 0) order.push_back(dst);
+                    wsrc[dst - base] = dst;
+                    wneg[dst - base] = 0;
+                    wconst[dst - base] = 1;
                 };
                 const int NEG2 = 1 << 1, NEG3 = 1 << 2;   // field 2 (x momentum) / field 3 (y momentum)
                 int bc[4];
                 for (int k = 0; k < 4; k++) bc[k] = P.phys[k] ? mthbc[k] : -1;
+                if (bc[0] == 0 && inflow) for (int ibc = 1; ibc <= mbc; ibc++) for (int j = 1 - mbc; j <= my + mbc; j++) put_const(1 - ibc, j);
                 if (bc[0] == 1) for (int ibc = 1; ibc <= mbc; ibc++) for (int j = 1 - mbc; j <= my + mbc; j++) put(1 - ibc, j, 1, j, 0);
                 if (bc[0] == 3) for (int ibc = 1; ibc <= mbc; ibc++) for (int j = 1 - mbc; j <= my + mbc; j++) put(1 - ibc, j, ibc, j, NEG2);
                 if (bc[1] == 1) for (int ibc = 1; ibc <= mbc; ibc++) for (int j = 1 - mbc; j <= my + mbc; j++) put(mx + ibc, j, mx, j, 0);
@@ -450,7 +459,7 @@ void build_tables(const Forest& f, const int mthbc[4], std::vector<LevelTables>&
                 if (bc[2] == 3) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, 1 - jbc, i, jbc, NEG3);
                 if (bc[3] == 1) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, my + jbc, i, my, 0);
                 if (bc[3] == 3) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, my + jbc, i, my + 1 - jbc, NEG3);
-                for (int dst : order) LT.phys.push_back({dst, wsrc[dst - base], wneg[dst - base], 0});
+                for (int dst : order) LT.phys.push_back({dst, wsrc[dst - base], wneg[dst - base], wconst[dst - base]});
             }
         }
         // ---- time interpolation patches ----

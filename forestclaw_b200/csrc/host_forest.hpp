@@ -70,6 +70,7 @@ struct LevelTables {
     std::vector<SyncOp> f2c; std::vector<int> f2c_start; // time_sync_f2c ops grouped per coarse patch
 };
 
-void build_tables(const Forest& f, const int mthbc[4], std::vector<LevelTables>& out);
+// inflow: mthbc = 0 sides are set to a constant state (PhysEnt.pad = 1, src unused).
+void build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<LevelTables>& out);
 
 }  // namespace fcb

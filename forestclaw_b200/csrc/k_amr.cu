@@ -78,13 +78,14 @@ __global__ void k_interp(double* __restrict__ dst, const double* __restrict__ sr
     }
 }
 
-__global__ void k_phys(double* __restrict__ q, const PhysEnt* __restrict__ e, int n, int nxy, int meqn)
+__global__ void k_phys(double* __restrict__ q, const PhysEnt* __restrict__ e, int n, int nxy, int meqn,
+                       const double* __restrict__ bcstate)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     PhysEnt c = e[t];
     for (int m = 0; m < meqn; m++) {
-        double v = q[c.src + m * nxy];
+        double v = c.cst ? bcstate[m] : q[c.src + m * nxy];
         q[c.dst + m * nxy] = ((c.neg >> m) & 1) ? -v : v;
     }
 }
@@ -432,9 +433,9 @@ void launch_interp(const Dims& d, double* dst, const double* src, const InterpEn
 {
     if (n > 0) k_interp<<<nblk(n, 256), 256, 0, st>>>(dst, src, e, n, d.nx(), d.nxy(), d.meqn);
 }
-void launch_phys(const Dims& d, double* q, const PhysEnt* e, int n, cudaStream_t st)
+void launch_phys(const Dims& d, double* q, const PhysEnt* e, int n, const double* bcstate, cudaStream_t st)
 {
-    if (n > 0) k_phys<<<nblk(n, 256), 256, 0, st>>>(q, e, n, d.nxy(), d.meqn);
+    if (n > 0) k_phys<<<nblk(n, 256), 256, 0, st>>>(q, e, n, d.nxy(), d.meqn, bcstate);
 }
 void launch_timeinterp(const Dims& d, const double* q, const double* qlast, double* qinterp, const int* patches,
                        int npatch, double alpha, cudaStream_t st)

@@ -32,7 +32,7 @@
 
 namespace fcb {
 
-enum { APP_NONE = 0, APP_SWIRL = 1, APP_RADIALDAM = 2, APP_TSUNAMI = 3 };
+enum { APP_NONE = 0, APP_SWIRL = 1, APP_RADIALDAM = 2, APP_TSUNAMI = 3, APP_SHOCKBUBBLE = 4 };
 
 template <class RP, int MX, int MY, int MBC, typename TW, int NT = 0>
 struct Step2Geom {
@@ -54,7 +54,7 @@ struct Step2Geom {
     // per-interface transverse terms: A1, A2 (from amdq), B1, B2 (from apdq)
     static constexpr int TSZ = 4 * MEQN;
     static constexpr int AUXS = MAUX > 0 ? MAUX : 0;
-    static constexpr bool USE_FLX = F32 && RP::CONS_FLUX;     // per-cell FP64 fluxes for the remainder
+    static constexpr bool USE_FLX = F32 && RP::CONS_FLUX && !RP::EXACT64;   // per-cell FP64 fluxes for the remainder
     static constexpr size_t DOUBLES = (size_t)MEQN * NXY * 5 + (size_t)AUXS * NXY +
                                       (USE_FLX ? (size_t)MEQN * NXY : 0) + 64;
     static constexpr size_t TWS = (size_t)WSZ * NI + (size_t)TSZ * NI + (F32 ? (size_t)MEQN * NXY : 0);
@@ -81,8 +81,8 @@ __device__ __forceinline__ void rpn2_cons_sw(int idir, const T* q, T grav, T* fl
     flux[mv] = un * hut;
 }
 
-template <class RP, int MX, int MY, int MBC, bool FWAVE, int NT, typename TW>
-__global__ void __launch_bounds__(NT, 2)
+template <class RP, int MX, int MY, int MBC, bool FWAVE, int NT, typename TW, int MINB = 2>
+__global__ void __launch_bounds__(NT, MINB)
 step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* __restrict__ aux,
              double* __restrict__ regs, const PatchDesc* __restrict__ desc, int p0,
              const StepParams* __restrict__ spp, unsigned long long* __restrict__ cfl_bits)
@@ -90,6 +90,7 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
     using G = Step2Geom<RP, MX, MY, MBC, TW, NT>;
     const StepParams sp = *spp;     // per-launch parameters live in device memory (graph replay)
     constexpr bool F32 = G::F32, REG = G::REG;
+    static_assert(!RP::EXACT64 || G::REG, "exact solvers keep their FP64 fluctuations in registers");
     constexpr int NX = G::NX, NY = G::NY, NXY = G::NXY, MEQN = G::MEQN, MWAVES = G::MWAVES;
     constexpr int MAUX = G::MAUX, NEXTRA = G::NEXTRA, NI = G::NI, WSZ = G::WSZ;
     constexpr int MA = MAUX > 0 ? MAUX : 1;
@@ -119,6 +120,8 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
 
     const int tid = threadIdx.x;
     const int p = p0 + blockIdx.x;
+    __shared__ unsigned int nhist[RP::EXACT64 ? 32 : 1];   // Newton iterations of this patch
+    if (RP::EXACT64 && tid < 32) nhist[tid] = 0u;
     const PatchDesc pd = desc[p];
     const double dx = pd.dx, dy = pd.dy;
     const double dt = sp.dt;
@@ -180,7 +183,8 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
             else { ic = MBC + j; jc = MY + MBC - 1 + k; }
             double qv[MEQN >= 3 ? MEQN : 3], fl[MEQN >= 3 ? MEQN : 3];
             for (int m = 0; m < MEQN; m++) qv[m] = Qs[m * NXY + jc * NX + ic];
-            rpn2_cons_sw<double>(face / 2, qv, sp.grav, fl);
+            if constexpr (RP::EXACT64) RP::cons_flux(face / 2, qv, sp.gamma, fl);
+            else rpn2_cons_sw<double>(face / 2, qv, sp.grav, fl);
             const int n = (face < 2) ? MY : MX;
             const double el = (face < 2) ? dy : dx;
             const int base = (face == 0) ? G::R_EF0 : (face == 1) ? G::R_EF1 : (face == 2) ? G::R_EF2 : G::R_EF3;
@@ -194,14 +198,33 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
     double cflmax = 0.0;
     TW cflw = TW(0);
 
-    struct State { TW wave[MWAVES][MEQN]; TW s[MWAVES]; TW am[MEQN]; TW ap[MEQN]; TW ex[NEXTRA]; };
+    // g64: FP64 amdq, apdq of exact solvers (kept for the Godunov update)
+    struct State { TW wave[MWAVES][MEQN]; TW s[MWAVES]; TW am[MEQN]; TW ap[MEQN]; TW ex[NEXTRA];
+                   double g64[RP::EXACT64 ? 2 * MEQN : 1]; };
 
     // Normal solve of one interface (qL = cell cL, qR = cell cR).
-    auto normal_solve = [&](int ixy, int cL, int cR, int k, bool cfl_range, TW d1, TW d0, State& st) {
-        TW qL[MEQN], qR[MEQN], aL[MA], aR[MA];
-        for (int m = 0; m < MEQN; m++) { qL[m] = qload(m, cL); qR[m] = qload(m, cR); }
-        for (int a = 0; a < MAUX; a++) { aL[a] = (TW)As[a * NXY + cL]; aR[a] = (TW)As[a * NXY + cR]; }
-        RP::template rpn2<TW>(ixy, qL, qR, aL, aR, st.wave, st.s, st.am, st.ap, st.ex, gravw);
+    auto normal_solve = [&](int ixy, int cL, int cR, int k, bool cfl_range, TW d1, TW d0, State& st, double seed) {
+        if constexpr (RP::EXACT64) {
+            double qL64[MEQN], qR64[MEQN], w64[MWAVES][MEQN], s64[MWAVES], am64[MEQN], ap64[MEQN], ex64[NEXTRA];
+            for (int m = 0; m < MEQN; m++) { qL64[m] = Qs[m * NXY + cL]; qR64[m] = Qs[m * NXY + cR]; }
+            const EulerParams ep{sp.gamma, sp.newton_tol, seed};
+            const int it = RP::solve64(ixy, qL64, qR64, ep, w64, s64, am64, ap64, ex64);
+            atomicAdd(&nhist[it < 31 ? it : 31], 1u);
+            for (int mw = 0; mw < MWAVES; mw++) {
+                st.s[mw] = (TW)s64[mw];
+                for (int m = 0; m < MEQN; m++) st.wave[mw][m] = (TW)w64[mw][m];
+            }
+            for (int m = 0; m < MEQN; m++) {
+                st.am[m] = (TW)am64[m]; st.ap[m] = (TW)ap64[m];
+                st.g64[m] = am64[m]; st.g64[MEQN + m] = ap64[m];
+            }
+            for (int e = 0; e < NEXTRA; e++) st.ex[e] = (TW)ex64[e];
+        } else {
+            TW qL[MEQN], qR[MEQN], aL[MA], aR[MA];
+            for (int m = 0; m < MEQN; m++) { qL[m] = qload(m, cL); qR[m] = qload(m, cR); }
+            for (int a = 0; a < MAUX; a++) { aL[a] = (TW)As[a * NXY + cL]; aR[a] = (TW)As[a * NXY + cR]; }
+            RP::template rpn2<TW>(ixy, qL, qR, aL, aR, st.wave, st.s, st.am, st.ap, st.ex, gravw);
+        }
         for (int mw = 0; mw < MWAVES; mw++)
             for (int m = 0; m < MEQN; m++) W[(G::W_WAVE + mw * MEQN + m) * NI + k] = st.wave[mw][m];
         if (!REG) {
@@ -237,7 +260,9 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
         TW cq[MEQN];
         for (int m = 0; m < MEQN; m++) { cq[m] = TW(0); faddm[m] = 0.0; faddp[m] = 0.0; }
         if (god) {
-            if constexpr (F32) {
+            if constexpr (RP::EXACT64) {
+                for (int m = 0; m < MEQN; m++) { faddp[m] = faddp[m] - st.g64[MEQN + m]; faddm[m] = faddm[m] + st.g64[m]; }
+            } else if constexpr (F32) {
                 double am64[MEQN], ap64[MEQN];
                 double qL[MEQN], qR[MEQN], aL[MA], aR[MA], fL[MEQN], fR[MEQN];
                 for (int m = 0; m < MEQN; m++) {
@@ -336,7 +361,7 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
         const int jc = 1 + k / (NX - 1), ic = 1 + k % (NX - 1);
         const bool cr = (ic >= MBC && ic <= MX + MBC);
         normal_solve(1, jc * NX + ic - 1, jc * NX + ic, k, cr, cr ? dtdx1d_x(ic, jc) : TW(0),
-                     cr ? dtdx1d_x(ic - 1, jc) : TW(0), st);
+                     cr ? dtdx1d_x(ic - 1, jc) : TW(0), st, 0.0);
     };
     auto x2 = [&](int k, State& st) {
         const int jc = 1 + k / (NX - 1), ic = 1 + k % (NX - 1);
@@ -361,7 +386,7 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
         const int ic = 1 + k / (NY - 1), jc = 1 + k % (NY - 1);
         const bool cr = (jc >= MBC && jc <= MY + MBC);
         normal_solve(2, (jc - 1) * NX + ic, jc * NX + ic, k, cr, cr ? dtdy1d_y(ic, jc) : TW(0),
-                     cr ? dtdy1d_y(ic, jc - 1) : TW(0), st);
+                     cr ? dtdy1d_y(ic, jc - 1) : TW(0), st, 0.0);
     };
     auto y2 = [&](int k, State& st) {
         const int ic = 1 + k / (NY - 1), jc = 1 + k % (NY - 1);
@@ -509,6 +534,9 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
             if (v != v) bits = 0x7ff8000000000000ull;   // NaN (e.g. negative depth) wins the max
             atomicMax(cfl_bits, bits);
         }
+    }
+    if constexpr (RP::EXACT64) {
+        if (tid < 32 && sp.newton_hist && nhist[tid]) atomicAdd(&sp.newton_hist[tid], (unsigned long long)nhist[tid]);
     }
 }
 

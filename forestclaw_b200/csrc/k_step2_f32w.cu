@@ -8,14 +8,14 @@
 
 namespace fcb {
 
-template <class RP, int MX, int MY, int MBC, bool FW, int NT>
+template <class RP, int MX, int MY, int MBC, bool FW, int NT, int MINB = 2>
 static cudaError_t run_step2_f32(const Dims& d, double* q, double* qlast, const double* aux, double* regs,
                                  const PatchDesc* desc, int p0, int npatch, const StepParams* sp,
                                  unsigned long long* cfl_bits, cudaStream_t st)
 {
     using G = Step2Geom<RP, MX, MY, MBC, float, NT>;
     static bool attr_set = false;
-    auto kern = step2_kernel<RP, MX, MY, MBC, FW, NT, float>;
+    auto kern = step2_kernel<RP, MX, MY, MBC, FW, NT, float, MINB>;
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM_BYTES);
         if (e != cudaSuccess) return e;
@@ -41,6 +41,8 @@ cudaError_t launch_step2_f32w(int rp, const Dims& d, double* q, double* qlast, c
     FCB_CASE32(FC2D_B200_RP_SW_ROE, RPShallowRoe, 8, 8, 2, false, 160)
     FCB_CASE32(FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 16, 16, 2, true, 416)
     FCB_CASE32(FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 8, 8, 2, true, 160)
+    FCB_CASE32(FC2D_B200_RP_EULER_EXACT, RPEulerExact, 16, 16, 2, false, 352)
+    FCB_CASE32(FC2D_B200_RP_EULER_EXACT, RPEulerExact, 8, 8, 2, false, 128)
     return cudaErrorInvalidValue;
 }
 
@@ -48,7 +50,8 @@ bool step2_f32w_supported(int rp, int mx, int my, int mbc)
 {
     if (mbc != 2 || mx != my) return false;
     if (rp == FC2D_B200_RP_ADVECTION) return mx == 32 || mx == 16;
-    if (rp == FC2D_B200_RP_SW_ROE || rp == FC2D_B200_RP_SW_FWAVE) return mx == 16 || mx == 8;
+    if (rp == FC2D_B200_RP_SW_ROE || rp == FC2D_B200_RP_SW_FWAVE || rp == FC2D_B200_RP_EULER_EXACT)
+        return mx == 16 || mx == 8;
     return false;
 }
 

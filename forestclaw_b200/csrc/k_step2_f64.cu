@@ -7,14 +7,14 @@
 
 namespace fcb {
 
-template <class RP, int MX, int MY, int MBC, bool FW, int NT>
+template <class RP, int MX, int MY, int MBC, bool FW, int NT, int MINB = 2>
 static cudaError_t run_step2(const Dims& d, double* q, double* qlast, const double* aux, double* regs,
                              const PatchDesc* desc, int p0, int npatch, const StepParams* sp,
                              unsigned long long* cfl_bits, cudaStream_t st)
 {
     using G = Step2Geom<RP, MX, MY, MBC, double, NT>;
     static bool attr_set = false;
-    auto kern = step2_kernel<RP, MX, MY, MBC, FW, NT, double>;
+    auto kern = step2_kernel<RP, MX, MY, MBC, FW, NT, double, MINB>;
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM_BYTES);
         if (e != cudaSuccess) return e;
@@ -41,6 +41,9 @@ cudaError_t launch_step2_f64(int rp, const Dims& d, double* q, double* qlast, co
     FCB_CASE(FC2D_B200_RP_SW_ROE, RPShallowRoe, 8, 8, 2, false, 160)
     FCB_CASE(FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 16, 16, 2, true, 352)
     FCB_CASE(FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 8, 8, 2, true, 160)
+    if (rp == FC2D_B200_RP_EULER_EXACT && d.mx == 16 && d.my == 16 && d.mbc == 2)
+        return run_step2<RPEulerExact, 16, 16, 2, false, 352, 1>(d, q, qlast, aux, regs, desc, p0, npatch, sp, cfl_bits, st);
+    FCB_CASE(FC2D_B200_RP_EULER_EXACT, RPEulerExact, 8, 8, 2, false, 128)
     return cudaErrorInvalidValue;
 }
 
@@ -48,7 +51,8 @@ bool step2_f64_supported(int rp, int mx, int my, int mbc)
 {
     if (mbc != 2 || mx != my) return false;
     if (rp == FC2D_B200_RP_ADVECTION) return mx == 32 || mx == 16 || mx == 8;
-    if (rp == FC2D_B200_RP_SW_ROE || rp == FC2D_B200_RP_SW_FWAVE) return mx == 16 || mx == 8;
+    if (rp == FC2D_B200_RP_SW_ROE || rp == FC2D_B200_RP_SW_FWAVE || rp == FC2D_B200_RP_EULER_EXACT)
+        return mx == 16 || mx == 8;
     return false;
 }
 

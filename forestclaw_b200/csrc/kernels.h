@@ -25,12 +25,12 @@ struct Dims {
 // follow at +m*nxy.
 struct CopyEnt { int dst, src; };                  // copy / average (src = first child)
 struct InterpEnt { int dst, src, sub, pad; };      // sub = child position 0..3 (ii + 2 jj)
-struct PhysEnt { int dst, src, neg, pad; };        // neg: bit m set => negate field m
+struct PhysEnt { int dst, src, neg, cst; };        // neg: bit m set => negate field m; cst: constant state
 
 void launch_copy(const Dims& d, double* dst, const double* src, const CopyEnt* e, int n, cudaStream_t st);
 void launch_average(const Dims& d, double* dst, const double* src, const CopyEnt* e, int n, cudaStream_t st);
 void launch_interp(const Dims& d, double* dst, const double* src, const InterpEnt* e, int n, cudaStream_t st);
-void launch_phys(const Dims& d, double* q, const PhysEnt* e, int n, cudaStream_t st);
+void launch_phys(const Dims& d, double* q, const PhysEnt* e, int n, const double* bcstate, cudaStream_t st);
 void launch_timeinterp(const Dims& d, const double* q, const double* qlast, double* qinterp,
                        const int* patches, int npatch, double alpha, cudaStream_t st);
 

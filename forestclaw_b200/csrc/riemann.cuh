@@ -14,6 +14,7 @@
 //       aux1/2/3 = aux of cell i1 = i-2+imp on the lines below / on / above the sweep line.
 #pragma once
 #include <cuda_runtime.h>
+#include "fcb_math.cuh"
 
 namespace fcb {
 
@@ -27,7 +28,7 @@ template <typename T> __device__ __forceinline__ T sgn1(T x) { return copysign(T
 // ---------------------------------------------------------------------------
 struct RPAdvection {
     static constexpr int MEQN = 1, MWAVES = 1, MAUX = 2, NEXTRA = 1;
-    static constexpr bool CONS_FLUX = false;
+    static constexpr bool CONS_FLUX = false, EXACT64 = false;
     __device__ static void flux64(int ixy, const double* q, double grav, double* f) { (void)ixy; (void)grav; f[0] = q[0]; }
     // FP64 Godunov split for the FP32-wave path
     __device__ static void godunov64(int ixy, const double* qL, const double* qR, const double* aL, const double* aR,
@@ -69,7 +70,7 @@ struct RPAdvection {
 // ---------------------------------------------------------------------------
 struct RPShallowRoe {
     static constexpr int MEQN = 3, MWAVES = 3, MAUX = 0, NEXTRA = 3;
-    static constexpr bool CONS_FLUX = true;
+    static constexpr bool CONS_FLUX = true, EXACT64 = false;
     // normal flux in direction ixy, FP64 (one division per cell)
     __device__ static void flux64(int ixy, const double* q, double grav, double* f)
     {
@@ -182,7 +183,7 @@ struct RPShallowRoe {
 // ---------------------------------------------------------------------------
 struct RPShallowFWave {
     static constexpr int MEQN = 3, MWAVES = 3, MAUX = 1, NEXTRA = 1;
-    static constexpr bool CONS_FLUX = true;
+    static constexpr bool CONS_FLUX = true, EXACT64 = false;
     // normal flux in direction ixy, FP64 (one division per cell)
     __device__ static void flux64(int ixy, const double* q, double grav, double* f)
     {
@@ -315,6 +316,220 @@ struct RPShallowFWave {
             bm[m] = b1; bp[m] = b2;
         }
     }
+};
+
+
+// ---------------------------------------------------------------------------
+// 2D Euler, exact Riemann solver (no counterpart in the reference).
+// Newton iteration on p* (Toro, Riemann Solvers and Numerical Methods for
+// Fluid Dynamics, ch. 4: pressure functions 4.6-4.7, PVRS start 4.47, sampling
+// 4.5), always in FP64:
+//   amdq = F(q0) - F(qL), apdq = F(qR) - F(q0), q0 the Godunov state at x/t = 0,
+//   waves w1 = q*L - qL, w2 = q*R - q*L, w3 = qR - q*R,
+//   speeds s1 = left shock speed or rarefaction head uL - aL, s2 = u*,
+//          s3 = right shock speed or rarefaction head uR + aR.
+// The Roe averages of clawpack46_rpn2_euler4.f:83-100 are returned in extra for
+// the transverse solver clawpack46_rpt2_euler4.f:56-94.
+// EXACT64: the kernel calls solve64 with FP64 states and keeps amdq/apdq in FP64
+// in every precision; only the waves, speeds and transverse split use TW.
+// ---------------------------------------------------------------------------
+struct EulerParams { double gam, tol, seed; };
+
+struct RPEulerExact {
+    static constexpr int MEQN = 4, MWAVES = 3, MAUX = 0, NEXTRA = 5;
+    static constexpr bool CONS_FLUX = true, EXACT64 = true;
+
+    __device__ static void prefun(double g1, double g4, double g5, double g6, double p, double rk, double pk,
+                                  double ak, double& f, double& fd)
+    {
+        if (p <= pk) {
+            const double prat = p / pk;
+            const double z = fcb_exp(g1 * fcb_log(prat));
+            f = g4 * ak * (z - 1.0);
+            fd = (z / prat) / (rk * ak);
+        } else {
+            const double bk = g6 * pk;
+            const double qrt = sqrt((g5 / rk) / (bk + p));
+            f = (p - pk) * qrt;
+            fd = (1.0 - 0.5 * (p - pk) / (bk + p)) * qrt;
+        }
+    }
+    __device__ static void eflux(double r, double u, double v, double p, double en, double* f)
+    {
+        f[0] = r * u;
+        f[1] = r * u * u + p;
+        f[2] = r * u * v;
+        f[3] = u * (en + p);
+    }
+    // Euler flux of one cell in direction idir (0: x, 1: y), the time-sync rpn2_cons
+    __device__ static void cons_flux(int idir, const double* q, double gam, double* flux)
+    {
+        const int mu = (idir == 0) ? 1 : 2, mv = (idir == 0) ? 2 : 1;
+        const double r = q[0], un = q[mu] / r;
+        const double p = (gam - 1.0) * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) / r);
+        flux[0] = q[mu];
+        flux[mu] = q[mu] * un + p;
+        flux[mv] = q[mv] * un;
+        flux[3] = un * (q[3] + p);
+    }
+    // Primitive states of one interface (normal/tangential by ixy) and the PVRS start.
+    struct Prim { double rl, ul, vl, pl, al, rr, ur, vr, pr, ar; };
+    __device__ static Prim prim(int ixy, const double* qL, const double* qR, double gam)
+    {
+        const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+        const double gm1 = gam - 1.0;
+        Prim w;
+        w.rl = qL[0]; w.ul = qL[mu] / w.rl; w.vl = qL[mv] / w.rl;
+        w.pl = gm1 * (qL[3] - 0.5 * (qL[mu] * qL[mu] + qL[mv] * qL[mv]) / w.rl);
+        w.rr = qR[0]; w.ur = qR[mu] / w.rr; w.vr = qR[mv] / w.rr;
+        w.pr = gm1 * (qR[3] - 0.5 * (qR[mu] * qR[mu] + qR[mv] * qR[mv]) / w.rr);
+        w.al = sqrt(gam * w.pl / w.rl);
+        w.ar = sqrt(gam * w.pr / w.rr);
+        return w;
+    }
+    // One interface, FP64.  w[mw][m], am/ap in natural component order.
+    // Returns the Newton iteration count.
+    __device__ static int solve64(int ixy, const double* qL, const double* qR, const EulerParams& ep,
+                                  double w[3][4], double s[3], double* am, double* ap, double* ex)
+    {
+        const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+        const double gam = ep.gam, gamma1 = gam - 1.0;
+        // Roe averages (clawpack46_rpn2_euler4.f:84-99)
+        {
+            const double rhsqrtl = sqrt(qL[0]);
+            const double rhsqrtr = sqrt(qR[0]);
+            const double pl = gamma1 * (qL[3] - 0.5 * (qL[1] * qL[1] + qL[2] * qL[2]) / qL[0]);
+            const double pr = gamma1 * (qR[3] - 0.5 * (qR[1] * qR[1] + qR[2] * qR[2]) / qR[0]);
+            const double rhsq2 = rhsqrtl + rhsqrtr;
+            const double u = (qL[mu] / rhsqrtl + qR[mu] / rhsqrtr) / rhsq2;
+            const double v = (qL[mv] / rhsqrtl + qR[mv] / rhsqrtr) / rhsq2;
+            const double enth = ((qL[3] + pl) / rhsqrtl + (qR[3] + pr) / rhsqrtr) / rhsq2;
+            const double u2v2 = u * u + v * v;
+            const double a2 = gamma1 * (enth - 0.5 * u2v2);
+            ex[0] = u; ex[1] = v; ex[2] = enth; ex[3] = sqrt(a2); ex[4] = gamma1 / a2;
+        }
+        const double g1 = (gam - 1.0) / (2.0 * gam), g2 = (gam + 1.0) / (2.0 * gam);
+        const double g3 = 2.0 * gam / (gam - 1.0), g4 = 2.0 / (gam - 1.0), g5 = 2.0 / (gam + 1.0);
+        const double g6 = (gam - 1.0) / (gam + 1.0), g7 = (gam - 1.0) / 2.0;
+        const Prim P = prim(ixy, qL, qR, gam);
+        const double du = P.ur - P.ul;
+        const double tolpre = 1.0e-6;
+        double p;
+        if (ep.seed > 0.0 && isfinite(ep.seed)) p = ep.seed;
+        else {
+            const double ppv = 0.5 * (P.pl + P.pr) - 0.125 * du * (P.rl + P.rr) * (P.al + P.ar);
+            p = ppv > tolpre ? ppv : tolpre;
+        }
+        double fl = 0.0, fr = 0.0, fdl, fdr;
+        int it;
+        for (it = 1; it <= 64; it++) {
+            prefun(g1, g4, g5, g6, p, P.rl, P.pl, P.al, fl, fdl);
+            prefun(g1, g4, g5, g6, p, P.rr, P.pr, P.ar, fr, fdr);
+            double pn = p - (fl + fr + du) / (fdl + fdr);
+            if (pn < 0.0) pn = tolpre;
+            const double change = 2.0 * fabs(pn - p) / (pn + p);
+            p = pn;
+            if (change <= ep.tol) break;
+        }
+        if (it > 64) it = 64;
+        const double ps = p;
+        const double us = 0.5 * (P.ul + P.ur) + 0.5 * (fr - fl);
+        double rsl, rsr, asl, asr;
+        if (ps > P.pl) { const double q = ps / P.pl; rsl = P.rl * ((q + g6) / (g6 * q + 1.0)); asl = sqrt(gam * ps / rsl); }
+        else { const double lq = fcb_log(ps / P.pl); rsl = P.rl * fcb_exp(lq / gam); asl = P.al * fcb_exp(g1 * lq); }
+        if (ps > P.pr) { const double q = ps / P.pr; rsr = P.rr * ((q + g6) / (g6 * q + 1.0)); asr = sqrt(gam * ps / rsr); }
+        else { const double lq = fcb_log(ps / P.pr); rsr = P.rr * fcb_exp(lq / gam); asr = P.ar * fcb_exp(g1 * lq); }
+        const double shl = P.ul - P.al, shr = P.ur + P.ar;
+        double sl, sr;
+        if (ps > P.pl) sl = P.ul - P.al * sqrt(g2 * (ps / P.pl) + g1); else sl = shl;
+        if (ps > P.pr) sr = P.ur + P.ar * sqrt(g2 * (ps / P.pr) + g1); else sr = shr;
+        s[0] = sl; s[1] = us; s[2] = sr;
+        const double esl = ps / gamma1 + 0.5 * rsl * (us * us + P.vl * P.vl);
+        const double esr = ps / gamma1 + 0.5 * rsr * (us * us + P.vr * P.vr);
+        // waves in (rho, m_n, m_t, E) order, stored at the natural components
+        const double qln[4] = {qL[0], qL[mu], qL[mv], qL[3]}, qrn[4] = {qR[0], qR[mu], qR[mv], qR[3]};
+        const double qsl[4] = {rsl, rsl * us, rsl * P.vl, esl};
+        const double qsr[4] = {rsr, rsr * us, rsr * P.vr, esr};
+        const int comp[4] = {0, mu, mv, 3};
+        for (int k = 0; k < 4; k++) {
+            w[0][comp[k]] = qsl[k] - qln[k];
+            w[1][comp[k]] = qsr[k] - qsl[k];
+            w[2][comp[k]] = qrn[k] - qsr[k];
+        }
+        // Godunov state at x/t = 0
+        double r0, u0, v0, p0, e0;
+        int which;
+        if (0.0 <= us) {
+            v0 = P.vl;
+            if (ps > P.pl) which = (0.0 <= sl) ? 0 : 1;
+            else if (0.0 <= shl) which = 0;
+            else which = (0.0 > us - asl) ? 1 : 2;
+        } else {
+            v0 = P.vr;
+            if (ps > P.pr) which = (0.0 >= sr) ? 4 : 3;
+            else if (0.0 >= shr) which = 4;
+            else which = (0.0 < us + asr) ? 3 : 5;
+        }
+        if (which == 0) { r0 = P.rl; u0 = P.ul; p0 = P.pl; e0 = qL[3]; }
+        else if (which == 4) { r0 = P.rr; u0 = P.ur; p0 = P.pr; e0 = qR[3]; }
+        else if (which == 1) { r0 = rsl; u0 = us; p0 = ps; e0 = esl; }
+        else if (which == 3) { r0 = rsr; u0 = us; p0 = ps; e0 = esr; }
+        else if (which == 2) {
+            const double c = g5 + (g6 / P.al) * P.ul;
+            const double lc = fcb_log(c);
+            r0 = P.rl * fcb_exp(g4 * lc);
+            u0 = g5 * (P.al + g7 * P.ul);
+            p0 = P.pl * fcb_exp(g3 * lc);
+            e0 = p0 / gamma1 + 0.5 * r0 * (u0 * u0 + v0 * v0);
+        } else {
+            const double c = g5 - (g6 / P.ar) * P.ur;
+            const double lc = fcb_log(c);
+            r0 = P.rr * fcb_exp(g4 * lc);
+            u0 = g5 * (-P.ar + g7 * P.ur);
+            p0 = P.pr * fcb_exp(g3 * lc);
+            e0 = p0 / gamma1 + 0.5 * r0 * (u0 * u0 + v0 * v0);
+        }
+        double f0[4], flv[4], frv[4];
+        eflux(r0, u0, v0, p0, e0, f0);
+        eflux(P.rl, P.ul, P.vl, P.pl, qL[3], flv);
+        eflux(P.rr, P.ur, P.vr, P.pr, qR[3], frv);
+        for (int k = 0; k < 4; k++) { am[comp[k]] = f0[k] - flv[k]; ap[comp[k]] = frv[k] - f0[k]; }
+        return it;
+    }
+    // clawpack46_rpt2_euler4.f:56-94 with the Roe averages of the interface
+    template <typename T>
+    __device__ static void rpt2(int ixy, int imp, const T* qL, const T* qR, const T* aux1, const T* aux2,
+                                const T* aux3, const T extra[NEXTRA], const T* asdq, T* bm, T* bp, T grav, T drytol)
+    {
+        (void)imp; (void)qL; (void)qR; (void)aux1; (void)aux2; (void)aux3; (void)grav; (void)drytol;
+        const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+        const T u = extra[0], v = extra[1], enth = extra[2], a = extra[3], g1a2 = extra[4];
+        const T u2v2 = u * u + v * v;
+        const T euv = enth - u2v2;
+        const T a3 = g1a2 * (euv * asdq[0] + u * asdq[mu] + v * asdq[mv] - asdq[3]);
+        const T a2 = asdq[mu] - u * asdq[0];
+        const T a4 = (asdq[mv] + (a - v) * asdq[0] - a * a3) / (T(2) * a);
+        const T a1 = asdq[0] - a3 - a4;
+        T wb[4][3], sb[3];
+        wb[0][0] = a1; wb[mu][0] = a1 * u; wb[mv][0] = a1 * (v - a); wb[3][0] = a1 * (enth - v * a); sb[0] = v - a;
+        wb[0][1] = a3; wb[mu][1] = a3 * u + a2; wb[mv][1] = a3 * v; wb[3][1] = a3 * T(0.5) * u2v2 + a2 * u; sb[1] = v;
+        wb[0][2] = a4; wb[mu][2] = a4 * u; wb[mv][2] = a4 * (v + a); wb[3][2] = a4 * (enth + v * a); sb[2] = v + a;
+        for (int m = 0; m < 4; m++) {
+            T b1 = T(0), b2 = T(0);
+            for (int mw = 0; mw < 3; mw++) {
+                b1 = b1 + (sb[mw] < T(0) ? sb[mw] : T(0)) * wb[m][mw];
+                b2 = b2 + (sb[mw] > T(0) ? sb[mw] : T(0)) * wb[m][mw];
+            }
+            bm[m] = b1; bp[m] = b2;
+        }
+    }
+    // The generic normal-solver entry is not used for EXACT64 solvers.
+    __device__ static void flux64(int, const double*, double, double*) {}
+    __device__ static void godunov64(int, const double*, const double*, const double*, const double*, const double*,
+                                     const double*, const float*, double*, double*, double) {}
+    template <typename T>
+    __device__ static void rpn2(int, const T*, const T*, const T*, const T*, T[MWAVES][MEQN], T[MWAVES], T[MEQN],
+                                T[MEQN], T[NEXTRA], T) {}
 };
 
 // clawpack46_inlinelimiter.f:59-104

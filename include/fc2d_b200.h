@@ -34,12 +34,14 @@ extern "C" {
 #define FC2D_B200_RP_ADVECTION   0   /* clawpack46_rpn2adv.f / clawpack46_rpt2adv.f */
 #define FC2D_B200_RP_SW_ROE      1   /* shallow/2d/rp/clawpack46_rpn2.f / clawpack46_rpt2.f (Roe + HH fix) */
 #define FC2D_B200_RP_SW_FWAVE    2   /* shallow/2d/rp/rpn2_tsunami.f90 / rpt2_tsunami.f90 (f-waves, bathymetry) */
+#define FC2D_B200_RP_EULER_EXACT 3   /* Euler, exact Riemann solver (Newton on p*) + clawpack46_rpt2_euler4.f transverse */
 
 /* Built-in application callbacks (qinit / setaux / b4step2 / tagging). */
 #define FC2D_B200_APP_NONE       0   /* q and aux supplied by the caller */
 #define FC2D_B200_APP_SWIRL      1   /* advection/2d/swirl */
 #define FC2D_B200_APP_RADIALDAM  2   /* shallow/2d/radialdam (cell-centre disc) */
 #define FC2D_B200_APP_TSUNAMI    3   /* bathymetry + Gaussian bumps */
+#define FC2D_B200_APP_SHOCKBUBBLE 4  /* euler/2d/shockbubble: Mach-M shock, light bubble, inflow on the left */
 
 /* Arithmetic of the update kernel. */
 #define FC2D_B200_PREC_FP64      0   /* FP64 throughout, no FMA contraction (bitwise with the FP64 CPU path) */
@@ -68,6 +70,9 @@ typedef struct fc2d_b200_options {
     double grav, tperiod;
     double r0, hin, hout, x0, y0;
     double pdata[32];
+    /* Euler: gas constant, shock Mach number, bubble density (bubble centre and
+     * radius in x0, y0, r0), Newton tolerance on the relative change of p* */
+    double gamma, mach, rhob, newton_tol;
     /* B200 specifics */
     int precision;         /* FC2D_B200_PREC_* */
     int device;            /* CUDA device ordinal */
@@ -149,6 +154,9 @@ int fc2d_b200_mass(fc2d_b200_solver_t* s, double* out);
  * time on one device (several host threads) share the scratch and race. */
 #define FC2D_B200_MASS_SCRATCH_DOUBLES 131072
 int fc2d_b200_mass_noalloc(fc2d_b200_solver_t* s, double* out);
+/* Newton iterations of the exact Euler solver: out[k] = interfaces solved in k
+ * iterations since creation or the last reset (k = 31: 31 or more). */
+int fc2d_b200_newton_histogram(fc2d_b200_solver_t* s, unsigned long long* out, int reset);
 /* Interior cell updates performed so far (sum over levels of patches*mx*my per step). */
 int fc2d_b200_cell_updates(const fc2d_b200_solver_t* s, double* out);
 /* Wait for all device work of the solver's stream. */

@@ -5,15 +5,18 @@ from __future__ import annotations
 from oracle import pyoracle as po
 import forestclaw_b200 as fb
 from forestclaw_b200.problems import DAM as _DAM, SWIRL as _SWIRL, TSUNAMI as _TSUNAMI, swirl_dt  # noqa: F401
+from forestclaw_b200.problems import SHOCKBUBBLE as _SHOCKBUBBLE
 
 SWIRL = dict(_SWIRL, problem=po.PROB_SWIRL)
 DAM = dict(_DAM, problem=po.PROB_RADIALDAM)
 TSUNAMI = dict(_TSUNAMI, problem=po.PROB_TSUNAMI)
+SHOCKBUBBLE = dict(_SHOCKBUBBLE, problem=po.PROB_SHOCKBUBBLE)
 
 _ORC_KEYS = {"mx", "my", "mbc", "meqn", "maux", "mwaves", "order", "mthlim", "mthbc", "mcapa", "use_fwaves",
              "rp", "minlevel", "maxlevel", "subcycle", "time_sync", "flux_correction", "fluctuation_correction",
              "refine_threshold", "coarsen_threshold", "ax", "bx", "ay", "by", "mi", "mj", "problem", "grav",
-             "tperiod", "r0", "hin", "hout", "x0", "y0", "pdata", "nthreads"}
+             "tperiod", "r0", "hin", "hout", "x0", "y0", "pdata", "nthreads", "gamma", "mach", "rhob",
+             "newton_tol"}
 
 
 def make(problem: dict, **kw):
