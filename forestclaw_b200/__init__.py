@@ -130,6 +130,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L = ctypes.CDLL(path)
     P, I, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
     dp, ip = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    fp = ctypes.POINTER(ctypes.c_float)
     sig = {
         "fc2d_b200_create": [ctypes.POINTER(_Options), ctypes.POINTER(P)],
         "fc2d_b200_destroy": [P],
@@ -162,6 +163,18 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_set_graphs": [P, I],
         "fc2d_b200_mass_noalloc": [P, ctypes.POINTER(ctypes.c_double)],
         "fc2d_b200_newton_histogram": [P, ctypes.POINTER(ctypes.c_ulonglong), I],
+        "fc2d_b200_mlp_create": [I, ctypes.c_ulonglong, ctypes.POINTER(P)],
+        "fc2d_b200_mlp_destroy": [P],
+        "fc2d_b200_mlp_set_params": [P, fp],
+        "fc2d_b200_mlp_get_params": [P, fp],
+        "fc2d_b200_mlp_set_data": [P, dp, I, D, D],
+        "fc2d_b200_mlp_get_data": [P, fp, fp],
+        "fc2d_b200_mlp_train": [P, I, I, ctypes.c_float, ctypes.c_ulonglong, dp],
+        "fc2d_b200_mlp_gradient": [P, fp, fp, I, fp, dp],
+        "fc2d_b200_mlp_predict": [P, fp, I, fp],
+        "fc2d_b200_mlp_newton_histogram": [P, I, ctypes.POINTER(ctypes.c_longlong)],
+        "fc2d_b200_sample_interfaces": [P, I, ctypes.c_ulonglong, dp],
+        "fc2d_b200_set_pstar_seed": [P, P],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -188,6 +201,87 @@ def _dp(a: np.ndarray):
 
 def _ip(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+MLP_NPARAM = 4673
+
+
+class PStarMLP:
+    """The p*-seed network of the exact Euler solver and its GPU trainer
+    (fc2d_b200_mlp_*): parameters W1[64][6] b1 W2[64][64] b2 w3[64] b3."""
+
+    def __init__(self, device: int = 0, seed: int = 0):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        self._check("fc2d_b200_mlp_create", self.lib.fc2d_b200_mlp_create(device, seed, ctypes.byref(h)))
+        self.h = h
+        self.n = 0
+
+    def _check(self, fn: str, rc: int) -> None:
+        if rc != 0:
+            raise B200Error(fn, rc, (self.lib.fc2d_b200_last_error() or b"").decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.fc2d_b200_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def params(self) -> np.ndarray:
+        out = np.zeros(MLP_NPARAM, np.float32)
+        self._check("fc2d_b200_mlp_get_params", self.lib.fc2d_b200_mlp_get_params(self.h, _fp(out)))
+        return out
+
+    @params.setter
+    def params(self, p) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == MLP_NPARAM
+        self._check("fc2d_b200_mlp_set_params", self.lib.fc2d_b200_mlp_set_params(self.h, _fp(p)))
+
+    def set_data(self, prim, gamma: float = 1.4, tol: float = 1e-12) -> None:
+        prim = np.ascontiguousarray(prim, np.float64).reshape(-1, 6)
+        self._check("fc2d_b200_mlp_set_data", self.lib.fc2d_b200_mlp_set_data(self.h, _dp(prim), len(prim), gamma, tol))
+        self.n = len(prim)
+
+    def data(self):
+        X = np.zeros((self.n, 6), np.float32)
+        Y = np.zeros(self.n, np.float32)
+        self._check("fc2d_b200_mlp_get_data", self.lib.fc2d_b200_mlp_get_data(self.h, _fp(X), _fp(Y)))
+        return X, Y
+
+    def train(self, epochs: int, batch: int = 4096, lr: float = 2e-3, seed: int = 0) -> float:
+        loss = ctypes.c_double()
+        self._check("fc2d_b200_mlp_train", self.lib.fc2d_b200_mlp_train(self.h, epochs, batch, lr, seed, ctypes.byref(loss)))
+        return loss.value
+
+    def gradient(self, X, Y):
+        X = np.ascontiguousarray(X, np.float32).reshape(-1, 6)
+        Y = np.ascontiguousarray(Y, np.float32).reshape(-1)
+        g = np.zeros(MLP_NPARAM, np.float32)
+        loss = ctypes.c_double()
+        self._check("fc2d_b200_mlp_gradient", self.lib.fc2d_b200_mlp_gradient(self.h, _fp(X), _fp(Y), len(Y), _fp(g), ctypes.byref(loss)))
+        return g, loss.value
+
+    def predict(self, X) -> np.ndarray:
+        X = np.ascontiguousarray(X, np.float32).reshape(-1, 6)
+        Y = np.zeros(len(X), np.float32)
+        self._check("fc2d_b200_mlp_predict", self.lib.fc2d_b200_mlp_predict(self.h, _fp(X), len(X), _fp(Y)))
+        return Y
+
+    def newton_histogram(self, use_mlp: bool) -> np.ndarray:
+        h = (ctypes.c_longlong * 32)()
+        self._check("fc2d_b200_mlp_newton_histogram", self.lib.fc2d_b200_mlp_newton_histogram(self.h, int(use_mlp), h))
+        return np.array(h[:], np.int64)
 
 
 class Solver:
@@ -299,6 +393,17 @@ class Solver:
         out = np.zeros(self.opts.meqn, np.float64)
         self._check("fc2d_b200_mass", self.lib.fc2d_b200_mass(self.h, _dp(out)))
         return out
+
+    def sample_interfaces(self, n: int, seed: int = 0) -> np.ndarray:
+        """n normal-direction interface states (rhoL, uL, pL, rhoR, uR, pR), uniform over the forest."""
+        out = np.zeros((n, 6), np.float64)
+        self._check("fc2d_b200_sample_interfaces", self.lib.fc2d_b200_sample_interfaces(self.h, n, seed, _dp(out)))
+        return out
+
+    def set_pstar_seed(self, mlp) -> None:
+        """Start the exact solver's Newton iterations from the network (None: PVRS)."""
+        self._check("fc2d_b200_set_pstar_seed",
+                    self.lib.fc2d_b200_set_pstar_seed(self.h, mlp.h if mlp is not None else None))
 
     def newton_histogram(self, reset: bool = False) -> np.ndarray:
         """Interfaces solved in k Newton iterations (k = 0..31) by the exact Euler solver."""

@@ -30,6 +30,7 @@ CU_UNITS = {
     "k_step2_f64.cu": ["-fmad=false"],
     "k_amr.cu": ["-fmad=false"],
     "k_mass_noalloc.cu": ["-fmad=false"],
+    "k_mlp.cu": [],
     "k_step2_f32w.cu": ["--use_fast_math"],
 }
 CPP_UNITS = ["host_forest.cpp", "host_api.cpp", "apps.cpp"]

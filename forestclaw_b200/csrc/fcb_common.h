@@ -15,7 +15,17 @@ struct PatchDesc {
     int flags;          // PATCH_* bits
 };
 
-enum { PATCH_HAS_FINE_NBR = 1 };   // a face or corner neighbour is finer (fclaw2d_patch.c:980-1034)
+enum { PATCH_HAS_FINE_NBR = 1 };
+
+// p*-seed network sizes and layouts (k_mlp.cuh).  The network seeds Newton only
+// where the interface carries a wave of strength |dp|/pbar + |du|/cbar above
+// MLP_GATE; weaker jumps keep the PVRS start, whose error (below ~1e-2 there) a
+// BF16 network does not improve on.
+#define MLP_GATE 0.2
+enum { MLP_IN = 6, MLP_H = 64, MLP_NPARAM = 64 * 6 + 64 + 64 * 64 + 64 + 64 + 1 };
+enum { MLP_OFF_W1 = 0, MLP_OFF_B1 = 384, MLP_OFF_W2 = 448, MLP_OFF_B2 = 4544, MLP_OFF_W3 = 4608, MLP_OFF_B3 = 4672 };
+enum { MLP_BLOB_F_B1 = 0, MLP_BLOB_F_B2 = 64, MLP_BLOB_F_W3 = 128, MLP_BLOB_F_B3 = 192,
+       MLP_BLOB_W1_BYTE = 1024, MLP_BLOB_W2_BYTE = 1024 + 64 * 16 * 2, MLP_BLOB_BYTES = 1024 + 64 * 16 * 2 + 64 * 64 * 2 };   // a face or corner neighbour is finer (fclaw2d_patch.c:980-1034)
 
 // Parameters of one level update launch (clawpack46 method flags and the
 // per-step scalars the reference passes through common blocks).
@@ -35,6 +45,7 @@ struct StepParams {
     double gamma;           // Euler: ratio of specific heats
     double newton_tol;      // Euler: Newton tolerance on the relative change of p*
     unsigned long long* newton_hist;   // Euler: 32-bin histogram of Newton iterations (or null)
+    const void* mlp;        // Euler: p*-seed network blob (null: PVRS start)
 };
 
 }  // namespace fcb

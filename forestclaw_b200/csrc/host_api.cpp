@@ -14,6 +14,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <algorithm>
 #include <string>
 #include <vector>
 #include "apps.hpp"
@@ -83,6 +84,8 @@ struct fc2d_b200_solver {
     bool has_inflow = false;                       // mthbc = 0 sides take bc_dev (app inflow state)
     double* bc_dev = nullptr;                      // 8 doubles
     unsigned long long* newton_hist = nullptr;     // 32 bins, exact Euler solver
+    void* mlp_blob = nullptr;                      // p*-seed network (null: PVRS start)
+    bool use_mlp = false;
     DevVec<RepopOp> repop_dev;                     // regrid repopulation ops
     std::vector<double> aux_host;                  // static aux mirror (level-major)
     DevVec<CopyEnt> t_copy, t_avg;
@@ -283,6 +286,7 @@ static int update_level(fc2d_b200_solver* s, int level, double t, double dt)
     sp.gamma = s->o.gamma;
     sp.newton_tol = s->o.newton_tol;
     sp.newton_hist = s->newton_hist;
+    sp.mlp = s->use_mlp ? s->mlp_blob : nullptr;
     if (s->o.app == FC2D_B200_APP_SWIRL && s->o.tperiod != 0.0) {
         const double pi = 4.0 * std::atan(1.0), pi2 = 2.0 * pi;
         sp.vt = std::cos(pi2 * (t + dt / 2.0) / s->o.tperiod);
@@ -514,6 +518,7 @@ extern "C" int fc2d_b200_destroy(fc2d_b200_solver_t* s)
     cudaFree(s->params_dev); cudaFreeHost(s->params_host);
     if (s->mass_dev) cudaFree(s->mass_dev);
     cudaFree(s->bc_dev); cudaFree(s->newton_hist);
+    if (s->mlp_blob) cudaFree(s->mlp_blob);
     cudaStreamDestroy(s->st);
     delete s;
     return 0;
@@ -1089,5 +1094,272 @@ extern "C" int fc2d_b200_newton_histogram(fc2d_b200_solver_t* s, unsigned long l
         CK(cudaMemsetAsync(s->newton_hist, 0, 32 * sizeof(unsigned long long), s->st));
         CK(cudaStreamSynchronize(s->st));
     }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// p*-seed network: sampling, training, deployment
+// ---------------------------------------------------------------------------
+struct fc2d_b200_mlp {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    float *prm = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr;
+    void* blob = nullptr;
+    float *partial = nullptr, *loss_partial = nullptr, *loss_dev = nullptr;
+    int partial_blocks = 0;
+    double* prim = nullptr;
+    float *X = nullptr, *Y = nullptr, *Yp = nullptr;
+    int *idx = nullptr, *iters = nullptr;
+    int n = 0, cap = 0;
+    int step = 0;
+    double gamma = 1.4, tol = 1e-12;
+};
+
+static unsigned long long host_splitmix(unsigned long long& s)
+{
+    unsigned long long z = (s += 0x9e3779b97f4a7c15ULL);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+static double host_uniform(unsigned long long& s) { return (double)(host_splitmix(s) >> 11) * (1.0 / 9007199254740992.0); }
+
+static int mlp_partials(fc2d_b200_mlp* m, int nb)
+{
+    const int nblk = mlp_fwdbwd_blocks(nb);
+    if (nblk <= m->partial_blocks) return 0;
+    if (m->partial) cudaFree(m->partial);
+    if (m->loss_partial) cudaFree(m->loss_partial);
+    m->partial = nullptr; m->loss_partial = nullptr;
+    CK(cudaMalloc(&m->partial, sizeof(float) * (size_t)nblk * MLP_NPARAM));
+    CK(cudaMalloc(&m->loss_partial, sizeof(float) * (size_t)nblk));
+    m->partial_blocks = nblk;
+    return 0;
+}
+
+extern "C" int fc2d_b200_mlp_create(int device, unsigned long long seed, fc2d_b200_mlp_t** out)
+{
+    if (!out) return fail(FC2D_B200_EINVAL, "null argument");
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(FC2D_B200_EDEVICE, "no such CUDA device");
+    CK(cudaSetDevice(device));
+    auto m = std::make_unique<fc2d_b200_mlp>();
+    m->device = device;
+    CK(cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking));
+    CK(mlp_setup());
+    CK(cudaMalloc(&m->prm, sizeof(float) * MLP_NPARAM));
+    CK(cudaMalloc(&m->grad, sizeof(float) * MLP_NPARAM));
+    CK(cudaMalloc(&m->m, sizeof(float) * MLP_NPARAM));
+    CK(cudaMalloc(&m->v, sizeof(float) * MLP_NPARAM));
+    CK(cudaMalloc(&m->blob, MLP_BLOB_BYTES));
+    CK(cudaMalloc(&m->loss_dev, sizeof(float)));
+    CK(cudaMemset(m->m, 0, sizeof(float) * MLP_NPARAM));
+    CK(cudaMemset(m->v, 0, sizeof(float) * MLP_NPARAM));
+    // Glorot-uniform weights, zero biases, from a splitmix64 stream of `seed`
+    std::vector<float> p(MLP_NPARAM, 0.0f);
+    unsigned long long s = seed;
+    auto fill = [&](int off, int n, int fan_in, int fan_out) {
+        const double a = std::sqrt(6.0 / (fan_in + fan_out));
+        for (int k = 0; k < n; k++) p[off + k] = (float)((2.0 * host_uniform(s) - 1.0) * a);
+    };
+    fill(MLP_OFF_W1, 64 * 6, 6, 64);
+    fill(MLP_OFF_W2, 64 * 64, 64, 64);
+    fill(MLP_OFF_W3, 64, 64, 1);
+    CK(cudaMemcpy(m->prm, p.data(), sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice));
+    launch_mlp_blob(m->prm, m->blob, m->st);
+    CK(cudaStreamSynchronize(m->st));
+    *out = m.release();
+    return 0;
+}
+
+extern "C" int fc2d_b200_mlp_destroy(fc2d_b200_mlp_t* m)
+{
+    if (!m) return 0;
+    cudaSetDevice(m->device);
+    cudaStreamSynchronize(m->st);
+    for (void* p : {(void*)m->prm, (void*)m->grad, (void*)m->m, (void*)m->v, m->blob, (void*)m->partial,
+                    (void*)m->loss_partial, (void*)m->loss_dev, (void*)m->prim, (void*)m->X, (void*)m->Y,
+                    (void*)m->Yp, (void*)m->idx, (void*)m->iters})
+        if (p) cudaFree(p);
+    cudaStreamDestroy(m->st);
+    delete m;
+    return 0;
+}
+
+extern "C" int fc2d_b200_mlp_set_params(fc2d_b200_mlp_t* m, const float* params)
+{
+    if (!m || !params) return fail(FC2D_B200_EINVAL, "null argument");
+    CK(cudaSetDevice(m->device));
+    CK(cudaMemcpyAsync(m->prm, params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice, m->st));
+    launch_mlp_blob(m->prm, m->blob, m->st);
+    CK(cudaStreamSynchronize(m->st));
+    return 0;
+}
+
+extern "C" int fc2d_b200_mlp_get_params(fc2d_b200_mlp_t* m, float* params)
+{
+    if (!m || !params) return fail(FC2D_B200_EINVAL, "null argument");
+    CK(cudaSetDevice(m->device));
+    CK(cudaMemcpyAsync(params, m->prm, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    return 0;
+}
+
+static int mlp_reserve(fc2d_b200_mlp* m, int n)
+{
+    if (n <= m->cap) return 0;
+    for (void* p : {(void*)m->prim, (void*)m->X, (void*)m->Y, (void*)m->Yp, (void*)m->idx, (void*)m->iters})
+        if (p) cudaFree(p);
+    m->prim = nullptr; m->X = m->Y = m->Yp = nullptr; m->idx = m->iters = nullptr;
+    CK(cudaMalloc(&m->prim, sizeof(double) * 6 * (size_t)n));
+    CK(cudaMalloc(&m->X, sizeof(float) * MLP_IN * (size_t)n));
+    CK(cudaMalloc(&m->Y, sizeof(float) * (size_t)n));
+    CK(cudaMalloc(&m->Yp, sizeof(float) * (size_t)n));
+    CK(cudaMalloc(&m->idx, sizeof(int) * (size_t)n));
+    CK(cudaMalloc(&m->iters, sizeof(int) * (size_t)n));
+    m->cap = n;
+    return 0;
+}
+
+extern "C" int fc2d_b200_mlp_set_data(fc2d_b200_mlp_t* m, const double* prim, int n, double gamma, double tol)
+{
+    if (!m || !prim || n <= 0 || !(gamma > 1.0) || !(tol > 0.0)) return fail(FC2D_B200_EINVAL, "bad arguments");
+    CK(cudaSetDevice(m->device));
+    int rc = mlp_reserve(m, n);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(m->prim, prim, sizeof(double) * 6 * (size_t)n, cudaMemcpyHostToDevice, m->st));
+    launch_mlp_targets(m->prim, n, gamma, tol, m->X, m->Y, m->iters, m->st);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(m->st));
+    m->n = n; m->gamma = gamma; m->tol = tol;
+    return 0;
+}
+
+extern "C" int fc2d_b200_mlp_get_data(fc2d_b200_mlp_t* m, float* X, float* Y)
+{
+    if (!m || m->n <= 0) return fail(FC2D_B200_ESTATE, "no training data");
+    CK(cudaSetDevice(m->device));
+    if (X) CK(cudaMemcpyAsync(X, m->X, sizeof(float) * MLP_IN * (size_t)m->n, cudaMemcpyDeviceToHost, m->st));
+    if (Y) CK(cudaMemcpyAsync(Y, m->Y, sizeof(float) * (size_t)m->n, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    return 0;
+}
+
+extern "C" int fc2d_b200_mlp_train(fc2d_b200_mlp_t* m, int epochs, int batch, float lr, unsigned long long seed,
+                                   double* loss_out)
+{
+    if (!m || m->n <= 0) return fail(FC2D_B200_ESTATE, "no training data");
+    if (epochs <= 0 || batch <= 0 || !(lr > 0.0f)) return fail(FC2D_B200_EINVAL, "bad training arguments");
+    CK(cudaSetDevice(m->device));
+    const int n = m->n, nsteps = (n + batch - 1) / batch;
+    int rc = mlp_partials(m, batch);
+    if (rc) return rc;
+    std::vector<int> perm(n);
+    for (int i = 0; i < n; i++) perm[i] = i;
+    unsigned long long s = seed;
+    float* losses = nullptr;
+    CK(cudaMalloc(&losses, sizeof(float) * (size_t)nsteps));
+    double last = 0.0;
+    for (int e = 0; e < epochs; e++) {
+        for (int i = n - 1; i > 0; i--) {   // Fisher-Yates
+            const int j = (int)(host_splitmix(s) % (unsigned long long)(i + 1));
+            std::swap(perm[i], perm[j]);
+        }
+        CK(cudaMemcpyAsync(m->idx, perm.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, m->st));
+        for (int b = 0; b < nsteps; b++) {
+            const int nb = std::min(batch, n - b * batch);
+            m->step++;
+            launch_mlp_step(m->X, m->Y, m->idx + (size_t)b * batch, nb, m->blob, m->prm, m->grad, m->m, m->v,
+                            m->partial, m->loss_partial, losses + b, lr, m->step, true, m->st);
+        }
+        CK(cudaGetLastError());
+        std::vector<float> l(nsteps);
+        CK(cudaMemcpyAsync(l.data(), losses, sizeof(float) * nsteps, cudaMemcpyDeviceToHost, m->st));
+        CK(cudaStreamSynchronize(m->st));
+        double sum = 0.0;
+        for (int b = 0; b < nsteps; b++) sum += l[b] * std::min(batch, n - b * batch);
+        last = sum / n;
+    }
+    cudaFree(losses);
+    if (loss_out) *loss_out = last;
+    return 0;
+}
+
+extern "C" int fc2d_b200_mlp_gradient(fc2d_b200_mlp_t* m, const float* X, const float* Y, int n, float* grad,
+                                      double* loss)
+{
+    if (!m || !X || !Y || !grad || n <= 0) return fail(FC2D_B200_EINVAL, "bad arguments");
+    CK(cudaSetDevice(m->device));
+    int rc = mlp_partials(m, n);
+    if (rc) return rc;
+    float *Xd, *Yd;
+    CK(cudaMalloc(&Xd, sizeof(float) * MLP_IN * (size_t)n));
+    CK(cudaMalloc(&Yd, sizeof(float) * (size_t)n));
+    CK(cudaMemcpyAsync(Xd, X, sizeof(float) * MLP_IN * (size_t)n, cudaMemcpyHostToDevice, m->st));
+    CK(cudaMemcpyAsync(Yd, Y, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, m->st));
+    launch_mlp_step(Xd, Yd, nullptr, n, m->blob, m->prm, m->grad, m->m, m->v, m->partial, m->loss_partial,
+                    m->loss_dev, 0.0f, 1, false, m->st);
+    float l = 0.0f;
+    CK(cudaMemcpyAsync(grad, m->grad, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaMemcpyAsync(&l, m->loss_dev, sizeof(float), cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    cudaFree(Xd); cudaFree(Yd);
+    if (loss) *loss = l;
+    return 0;
+}
+
+extern "C" int fc2d_b200_mlp_predict(fc2d_b200_mlp_t* m, const float* X, int n, float* Y)
+{
+    if (!m || !X || !Y || n <= 0) return fail(FC2D_B200_EINVAL, "bad arguments");
+    CK(cudaSetDevice(m->device));
+    float *Xd, *Yd;
+    CK(cudaMalloc(&Xd, sizeof(float) * MLP_IN * (size_t)n));
+    CK(cudaMalloc(&Yd, sizeof(float) * (size_t)n));
+    CK(cudaMemcpyAsync(Xd, X, sizeof(float) * MLP_IN * (size_t)n, cudaMemcpyHostToDevice, m->st));
+    launch_mlp_predict(Xd, n, m->blob, Yd, m->st);
+    CK(cudaMemcpyAsync(Y, Yd, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    cudaFree(Xd); cudaFree(Yd);
+    return 0;
+}
+
+extern "C" int fc2d_b200_mlp_newton_histogram(fc2d_b200_mlp_t* m, int use_mlp, long long* hist)
+{
+    if (!m || !hist || m->n <= 0) return fail(FC2D_B200_ESTATE, "no data");
+    CK(cudaSetDevice(m->device));
+    if (use_mlp) launch_mlp_predict(m->X, m->n, m->blob, m->Yp, m->st);
+    launch_mlp_newton_iters(m->prim, m->X, use_mlp ? m->Yp : nullptr, m->n, m->gamma, m->tol, m->iters, m->st);
+    std::vector<int> it(m->n);
+    CK(cudaMemcpyAsync(it.data(), m->iters, sizeof(int) * (size_t)m->n, cudaMemcpyDeviceToHost, m->st));
+    CK(cudaStreamSynchronize(m->st));
+    for (int k = 0; k < 32; k++) hist[k] = 0;
+    for (int v : it) hist[v < 31 ? v : 31]++;
+    return 0;
+}
+
+extern "C" int fc2d_b200_sample_interfaces(fc2d_b200_solver_t* s, int n, unsigned long long seed, double* prim)
+{
+    if (!s || !s->initialized || !prim || n <= 0) return fail(FC2D_B200_EINVAL, "bad arguments");
+    if (s->o.rp != FC2D_B200_RP_EULER_EXACT) return fail(FC2D_B200_EINVAL, "interface sampling needs the Euler solver");
+    double* d = nullptr;
+    CK(cudaMalloc(&d, sizeof(double) * 6 * (size_t)n));
+    launch_sample_interfaces(s->d, s->q, s->forest.np(), s->o.gamma, seed, n, d, s->st);
+    cudaError_t e = cudaMemcpyAsync(prim, d, sizeof(double) * 6 * (size_t)n, cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("sample_interfaces: ") + cudaGetErrorString(e));
+    return 0;
+}
+
+extern "C" int fc2d_b200_set_pstar_seed(fc2d_b200_solver_t* s, const fc2d_b200_mlp_t* m)
+{
+    if (!s) return fail(FC2D_B200_EINVAL, "null solver");
+    if (!m) { s->use_mlp = false; return 0; }
+    if (s->o.rp != FC2D_B200_RP_EULER_EXACT) return fail(FC2D_B200_EINVAL, "the p* seed applies to the Euler solver");
+    if (!s->mlp_blob) CK(cudaMalloc(&s->mlp_blob, MLP_BLOB_BYTES));
+    CK(cudaMemcpyAsync(s->mlp_blob, m->blob, MLP_BLOB_BYTES, cudaMemcpyDeviceToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    s->use_mlp = true;
     return 0;
 }

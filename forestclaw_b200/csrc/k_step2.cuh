@@ -29,6 +29,7 @@
 #include <type_traits>
 #include "fcb_common.h"
 #include "riemann.cuh"
+#include "k_mlp.cuh"
 
 namespace fcb {
 
@@ -356,12 +357,43 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
         }
     };
 
+    // p*-seed of the exact solver for interface k of sweep ixy (all lanes of the
+    // warp take part; k < 0 marks a lane without an interface)
+    auto mlp_seed = [&](int ixy, int k) -> double {
+        if constexpr (RP::EXACT64) {
+            int cL = 0, cR = 1;
+            if (k >= 0) {
+                if (ixy == 1) { const int jc = 1 + k / (NX - 1), ic = 1 + k % (NX - 1); cL = jc * NX + ic - 1; cR = cL + 1; }
+                else { const int ic = 1 + k / (NY - 1), jc = 1 + k % (NY - 1); cL = (jc - 1) * NX + ic; cR = cL + NX; }
+            }
+            double qL[MEQN], qR[MEQN];
+            for (int m = 0; m < MEQN; m++) { qL[m] = Qs[m * NXY + cL]; qR[m] = Qs[m * NXY + cR]; }
+            const typename RP::Prim P = RP::prim(ixy, qL, qR, sp.gamma);
+            float x[MLP_IN];
+            double pbase;
+            mlp_features(P.rl, P.ul, P.pl, P.rr, P.ur, P.pr, sp.gamma, x, pbase);
+            if (k < 0 || !(x[0] == x[0] && x[1] == x[1] && x[2] == x[2] && x[3] == x[3] && x[4] == x[4] && x[5] == x[5])) {
+                x[0] = 1.0f; x[1] = 0.0f; x[2] = 1.0f; x[3] = 1.0f; x[4] = 0.0f; x[5] = 1.0f;
+                k = -1;
+            }
+            const bool use = k >= 0 && mlp_gate(x);
+            const MlpView W(sp.mlp);
+            MlpFrag h1, h2;
+            mlp_warp_hidden<true>(W, x, h1, h2);
+            const float y = mlp_warp_output(W, h2);
+            return use ? pbase * fcb_exp((double)y) : 0.0;
+        } else {
+            (void)ixy; (void)k;
+            return 0.0;
+        }
+    };
+
     // x-sweep interface k -> row jc = 1 + k / (NX-1), interface ic = 1 + k % (NX-1)
-    auto x1 = [&](int k, State& st) {
+    auto x1 = [&](int k, State& st, double seed) {
         const int jc = 1 + k / (NX - 1), ic = 1 + k % (NX - 1);
         const bool cr = (ic >= MBC && ic <= MX + MBC);
         normal_solve(1, jc * NX + ic - 1, jc * NX + ic, k, cr, cr ? dtdx1d_x(ic, jc) : TW(0),
-                     cr ? dtdx1d_x(ic - 1, jc) : TW(0), st, 0.0);
+                     cr ? dtdx1d_x(ic - 1, jc) : TW(0), st, seed);
     };
     auto x2 = [&](int k, State& st) {
         const int jc = 1 + k / (NX - 1), ic = 1 + k % (NX - 1);
@@ -382,11 +414,11 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
         }
     };
     // y-sweep interface k -> column ic = 1 + k / (NY-1), interface jc = 1 + k % (NY-1)
-    auto y1 = [&](int k, State& st) {
+    auto y1 = [&](int k, State& st, double seed) {
         const int ic = 1 + k / (NY - 1), jc = 1 + k % (NY - 1);
         const bool cr = (jc >= MBC && jc <= MY + MBC);
         normal_solve(2, (jc - 1) * NX + ic, jc * NX + ic, k, cr, cr ? dtdy1d_y(ic, jc) : TW(0),
-                     cr ? dtdy1d_y(ic, jc - 1) : TW(0), st, 0.0);
+                     cr ? dtdy1d_y(ic, jc - 1) : TW(0), st, seed);
     };
     auto y2 = [&](int k, State& st) {
         const int ic = 1 + k / (NY - 1), jc = 1 + k % (NY - 1);
@@ -459,8 +491,11 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
     // =================== x-sweeps (clawpack46_step2.f:113-167) ===================
     State st;
     cell_fluxes(1);
-    if (REG) { if (tid < G::NIX) x1(tid, st); }
-    else for (int k = tid; k < G::NIX; k += NT) x1(k, st);
+    {
+        const double seed = (RP::EXACT64 && sp.mlp) ? mlp_seed(1, tid < G::NIX ? tid : -1) : 0.0;
+        if (REG) { if (tid < G::NIX) x1(tid, st, seed); }
+        else for (int k = tid; k < G::NIX; k += NT) x1(k, st, 0.0);
+    }
     __syncthreads();
     if (REG) { if (tid < G::NIX) x2(tid, st); }
     else for (int k = tid; k < G::NIX; k += NT) { restore(k, st); x2(k, st); }
@@ -469,8 +504,11 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
     for (int c = tid; c < NXY; c += NT) x3(c);
     cell_fluxes(2);
     // =================== y-sweeps (clawpack46_step2.f:182-236) ===================
-    if (REG) { if (tid < G::NIY) y1(tid, st); }
-    else for (int k = tid; k < G::NIY; k += NT) y1(k, st);
+    {
+        const double seed = (RP::EXACT64 && sp.mlp) ? mlp_seed(2, tid < G::NIY ? tid : -1) : 0.0;
+        if (REG) { if (tid < G::NIY) y1(tid, st, seed); }
+        else for (int k = tid; k < G::NIY; k += NT) y1(k, st, 0.0);
+    }
     __syncthreads();
     if (REG) { if (tid < G::NIY) y2(tid, st); }
     else for (int k = tid; k < G::NIY; k += NT) { restore(k, st); y2(k, st); }

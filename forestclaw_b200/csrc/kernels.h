@@ -70,6 +70,21 @@ cudaError_t mass_scratch_address(double** ptr);
 void launch_mass_noalloc(const Dims& d, const double* q, const PatchDesc* desc, int np, double* scratch,
                          cudaStream_t st);
 
+// ---- p*-seed network (k_mlp.cu) ----------------------------------------------------
+cudaError_t mlp_setup();
+void launch_mlp_blob(const float* prm, void* blob, cudaStream_t st);
+void launch_mlp_targets(const double* prim, int n, double gam, double tol, float* X, float* Y, int* iters,
+                        cudaStream_t st);
+int mlp_fwdbwd_blocks(int nb);
+void launch_mlp_step(const float* X, const float* Y, const int* idx, int nb, void* blob, float* prm, float* grad,
+                     float* m, float* v, float* partial, float* loss_partial, float* loss, float lr, int step,
+                     bool update, cudaStream_t st);
+void launch_mlp_predict(const float* X, int n, const void* blob, float* Y, cudaStream_t st);
+void launch_mlp_newton_iters(const double* prim, const float* X, const float* Yseed, int n, double gam, double tol,
+                             int* iters, cudaStream_t st);
+void launch_sample_interfaces(const Dims& d, const double* q, int np, double gam, unsigned long long seed, int n,
+                              double* prim, cudaStream_t st);
+
 struct RepopOp { int kind, dst, src, igrid; int child[4]; };
 void launch_repop(const Dims& d, const RepopOp* ops, int nops, const double* oq, double* nq,
                   const double* oqlast, double* nqlast, const double* oqi, double* nqi,

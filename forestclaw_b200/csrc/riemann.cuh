@@ -387,6 +387,34 @@ struct RPEulerExact {
         w.ar = sqrt(gam * w.pr / w.rr);
         return w;
     }
+    // Star pressure of primitive states (Newton from seed, or PVRS if seed <= 0).
+    __device__ static double pstar(double rl, double ul, double pl, double rr, double ur, double pr, double gam,
+                                   double tol, double seed, int& iters)
+    {
+        const double g1 = (gam - 1.0) / (2.0 * gam), g4 = 2.0 / (gam - 1.0), g5 = 2.0 / (gam + 1.0);
+        const double g6 = (gam - 1.0) / (gam + 1.0);
+        const double al = sqrt(gam * pl / rl), ar = sqrt(gam * pr / rr);
+        const double du = ur - ul, tolpre = 1.0e-6;
+        double p;
+        if (seed > 0.0 && isfinite(seed)) p = seed;
+        else {
+            const double ppv = 0.5 * (pl + pr) - 0.125 * du * (rl + rr) * (al + ar);
+            p = ppv > tolpre ? ppv : tolpre;
+        }
+        int it;
+        for (it = 1; it <= 64; it++) {
+            double fl, fdl, fr, fdr;
+            prefun(g1, g4, g5, g6, p, rl, pl, al, fl, fdl);
+            prefun(g1, g4, g5, g6, p, rr, pr, ar, fr, fdr);
+            double pn = p - (fl + fr + du) / (fdl + fdr);
+            if (pn < 0.0) pn = tolpre;
+            const double change = 2.0 * fabs(pn - p) / (pn + p);
+            p = pn;
+            if (change <= tol) break;
+        }
+        iters = it > 64 ? 64 : it;
+        return p;
+    }
     // One interface, FP64.  w[mw][m], am/ap in natural component order.
     // Returns the Newton iteration count.
     __device__ static int solve64(int ixy, const double* qL, const double* qR, const EulerParams& ep,

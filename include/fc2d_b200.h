@@ -181,6 +181,38 @@ int fc2d_b200_event_elapsed(fc2d_b200_solver_t* s, int slot_a, int slot_b, doubl
 /* The cudaStream_t the solver launches on (returned as void*). */
 int fc2d_b200_get_stream(const fc2d_b200_solver_t* s, void** stream);
 
+/* ---- learned p* start of the exact Euler solver (no counterpart in the reference) ----
+ * A 6 -> 64 -> 64 -> 1 tanh network predicts the correction log(pstar/p_pvrs) of
+ * the PVRS estimate from the normalised primitive interface states; where the
+ * jump |dp|/pbar + |du|/cbar exceeds 0.2 Newton starts from p_pvrs exp(y)
+ * instead of p_pvrs and still iterates to newton_tol, so converged fluxes are
+ * unchanged to tolerance.  Parameters (FC2D_B200_MLP_NPARAM floats):
+ * W1[64][6] b1[64] W2[64][64] b2[64] w3[64] b3.  Training runs on the GPU:
+ * tensor-core forward (BF16 inputs, FP32 accumulation), FP32 backward, Adam. */
+#define FC2D_B200_MLP_NPARAM 4673
+typedef struct fc2d_b200_mlp fc2d_b200_mlp_t;
+int fc2d_b200_mlp_create(int device, unsigned long long seed, fc2d_b200_mlp_t** out);
+int fc2d_b200_mlp_destroy(fc2d_b200_mlp_t* m);
+int fc2d_b200_mlp_set_params(fc2d_b200_mlp_t* m, const float* params);
+int fc2d_b200_mlp_get_params(fc2d_b200_mlp_t* m, float* params);
+/* Training set: n primitive states (rhoL, uL, pL, rhoR, uR, pR) in the normal
+ * frame; targets are computed on the device by Newton (PVRS start) to `tol`. */
+int fc2d_b200_mlp_set_data(fc2d_b200_mlp_t* m, const double* prim, int n, double gamma, double tol);
+/* Features X[n][6] and targets Y[n] of the training set. */
+int fc2d_b200_mlp_get_data(fc2d_b200_mlp_t* m, float* X, float* Y);
+/* Minibatch Adam over shuffled epochs; *loss = mean squared error of the last epoch. */
+int fc2d_b200_mlp_train(fc2d_b200_mlp_t* m, int epochs, int batch, float lr, unsigned long long seed, double* loss);
+/* Gradient of the mean squared error over (X, Y) without an update. */
+int fc2d_b200_mlp_gradient(fc2d_b200_mlp_t* m, const float* X, const float* Y, int n, float* grad, double* loss);
+/* The deployed forward (approximate tanh, as inside the solver). */
+int fc2d_b200_mlp_predict(fc2d_b200_mlp_t* m, const float* X, int n, float* Y);
+/* Newton-iteration histogram over the training set from the PVRS (0) or network (1) start. */
+int fc2d_b200_mlp_newton_histogram(fc2d_b200_mlp_t* m, int use_mlp, long long* hist32);
+/* Uniform sample of n normal-direction interfaces of the solver's forest (Euler). */
+int fc2d_b200_sample_interfaces(fc2d_b200_solver_t* s, int n, unsigned long long seed, double* prim);
+/* Seed the solver's Newton iterations with the network (m = NULL: back to PVRS). */
+int fc2d_b200_set_pstar_seed(fc2d_b200_solver_t* s, const fc2d_b200_mlp_t* m);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,127 @@
+"""The learned p* start of the exact Euler solver on the B200.
+
+* forward and gradient kernels against the NumPy restatement (oracle/mlp_ref.py),
+* training on interface states sampled from an FP64 shock-bubble run lowers the
+  loss and the Newton iterations of the gated (strong-wave) interfaces,
+* the solver seeded by the trained network gives the PVRS-seeded solution to
+  the Newton tolerance with fewer Newton iterations.
+The gain needs waves that the PVRS start resolves poorly: the tests use a Mach-3
+shock (at Mach 1.22 PVRS already converges in at most 3 iterations and 95 % of
+the interfaces take 1).
+"""
+import numpy as np
+import pytest
+
+from oracle import mlp_ref
+from tests.cases import SHOCKBUBBLE, make
+
+pytestmark = pytest.mark.gpu
+
+def _gated(prim):
+    X, _ = mlp_ref.features(prim)
+    return mlp_ref.gated(X)
+
+
+def _random_states(rng, n):
+    rl, rr = rng.uniform(0.1, 3, n), rng.uniform(0.1, 3, n)
+    ul, ur = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    pl, pr = rng.uniform(0.2, 5, n), rng.uniform(0.2, 5, n)
+    return np.stack([rl, ul, pl, rr, ur, pr], axis=1)
+
+
+def test_forward_matches_oracle():
+    import forestclaw_b200 as fb
+    m = fb.PStarMLP(seed=1)
+    p = m.params.astype(np.float64)
+    X, _ = mlp_ref.features(_random_states(np.random.default_rng(0), 1000))
+    X = X.astype(np.float32)
+    y = m.predict(X)
+    yr, _ = mlp_ref.forward(p, X, bf=True)
+    # tensor-core BF16 layers as in the oracle; tanh.approx.f32 in the deployed forward
+    assert np.abs(y - yr).max() <= 5e-3 * (1 + np.abs(yr).max())
+    m.close()
+
+
+def test_gradient_matches_oracle():
+    import forestclaw_b200 as fb
+    m = fb.PStarMLP(seed=2)
+    p = m.params.astype(np.float64)
+    rng = np.random.default_rng(1)
+    X, pb = mlp_ref.features(_random_states(rng, 3000))
+    X = X.astype(np.float32)
+    Y = rng.normal(0, 0.3, len(X)).astype(np.float32)
+    g, loss = m.gradient(X, Y)
+    lr, gr = mlp_ref.loss_and_grad(p, X, Y, bf=True)
+    assert abs(loss - lr) <= 1e-4 * lr
+    blocks = [(0, 384), (384, 448), (448, 4544), (4544, 4608), (4608, 4672), (4672, 4673)]
+    for a, b in blocks:
+        err = np.abs(g[a:b] - gr[a:b]).max()
+        assert err <= 1e-3 * np.abs(gr[a:b]).max() + 1e-7, (a, b, err, np.abs(gr[a:b]).max())
+    m.close()
+
+
+MACH = 3.0
+
+
+def _shockbubble_samples(nper, snaps, seed=0):
+    import forestclaw_b200 as fb
+    _, gc = make(SHOCKBUBBLE, mx=16, my=16, minlevel=3, maxlevel=5, subcycle=1, time_sync=1, mach=MACH)
+    g = fb.Solver(gc)
+    g.initialize()
+    t, dt, out = 0.0, 0.0005, []
+    for n in range(snaps * 3):
+        c = g.advance(t, dt)
+        t += dt
+        dt *= 0.8 / c
+        if n % 3 == 2:
+            out.append(g.sample_interfaces(nper, seed + n))
+        if n % 4 == 3:
+            g.regrid()
+    g.close()
+    return np.concatenate(out)
+
+
+def test_training_lowers_loss_and_newton_iterations():
+    import forestclaw_b200 as fb
+    prim = _shockbubble_samples(200000, 6)
+    strong = prim[_gated(prim)]
+    assert len(strong) > 2000, len(strong)
+    m = fb.PStarMLP(seed=0)
+    m.set_data(strong, gamma=1.4, tol=1e-10)
+    X, Y = m.data()
+    l0 = mlp_ref.loss_and_grad(m.params.astype(np.float64), X[:4096], Y[:4096], bf=True)[0]
+    h_pvrs = m.newton_histogram(False)
+    loss = m.train(epochs=60, batch=1024, lr=3e-3, seed=1)
+    h_mlp = m.newton_histogram(True)
+    mean = lambda h: float((np.arange(32) * h).sum() / h.sum())
+    print("gated interfaces", len(strong), "PVRS", h_pvrs[:8], "network", h_mlp[:8], "loss", l0, "->", loss)
+    assert loss < 0.05 * l0, (loss, l0)
+    assert mean(h_mlp) < mean(h_pvrs), (mean(h_mlp), mean(h_pvrs))
+    m.close()
+
+
+def test_solver_seeded_by_network_matches_pvrs():
+    import forestclaw_b200 as fb
+    prim = _shockbubble_samples(200000, 6)
+    m = fb.PStarMLP(seed=0)
+    m.set_data(prim[_gated(prim)], gamma=1.4, tol=1e-10)
+    m.train(epochs=40, batch=1024, lr=3e-3, seed=2)
+    _, gc = make(SHOCKBUBBLE, mx=16, my=16, minlevel=3, maxlevel=5, subcycle=1, time_sync=1, mach=MACH)
+    a, b = fb.Solver(gc), fb.Solver(gc)
+    a.initialize(); b.initialize()
+    b.set_pstar_seed(m)
+    a.newton_histogram(reset=True); b.newton_histogram(reset=True)
+    t, dt = 0.0, 0.0005
+    for _ in range(6):
+        ca, cb = a.advance(t, dt), b.advance(t, dt)
+        assert abs(ca - cb) <= 1e-9 * ca
+        t += dt
+        dt *= 0.8 / ca
+    qa, qb = a.get_q(), b.get_q()
+    num = np.abs(qa[:, :, 2:-2, 2:-2] - qb[:, :, 2:-2, 2:-2]).sum()
+    assert num <= 1e-9 * np.abs(qa[:, :, 2:-2, 2:-2]).sum()
+    ha, hb = a.newton_histogram(), b.newton_histogram()
+    tot = lambda h: int((np.arange(32) * h).sum())
+    assert ha.sum() == hb.sum()
+    assert tot(hb) < tot(ha), (tot(hb), tot(ha))
+    m.close()
