@@ -1,7 +1,8 @@
 """Benchmark of the B200 patch-update path (cell-updates/s), one JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload dam|swirl|dam-uniform] [--precision fp64|fp32wave]
+                    [--workload dam|dam-uniform|swirl|shockbubble] [--precision fp64|fp32wave]
+                    [--pstar pvrs|mlp]
 
 Default workload (the configuration the metric is quoted on): 2D shallow water,
 radial dam break on [-1,1]^2, adaptive quadtree levels 3-7, 16x16 patches, mbc=2,
@@ -53,6 +54,8 @@ WORKLOADS = {
                         time_sync=0, regrid_interval=0, spinup=2),
     "swirl": dict(name="swirl_advection_uniform_l4_32x32", mx=32, my=32, minlevel=4, maxlevel=4, subcycle=0,
                   time_sync=0, regrid_interval=0, spinup=0),
+    "shockbubble": dict(name="euler_shockbubble_amr_l4-8_16x16", mx=16, my=16, minlevel=4, maxlevel=8, subcycle=1,
+                        time_sync=1, regrid_interval=4, spinup=8),
 }
 
 
@@ -133,7 +136,11 @@ class ClockSampler:
 
 def _preset(wl: dict):
     from forestclaw_b200 import problems
-    return problems.SWIRL if wl["name"].startswith("swirl") else problems.DAM
+    if wl["name"].startswith("swirl"):
+        return problems.SWIRL
+    if wl["name"].startswith("euler"):
+        return problems.SHOCKBUBBLE
+    return problems.DAM
 
 
 def _options(wl: dict, precision: str):
@@ -146,9 +153,12 @@ def _options(wl: dict, precision: str):
 
 
 def _initial_dt(wl: dict, prob) -> float:
-    from forestclaw_b200.problems import SWIRL, swirl_dt
+    from forestclaw_b200.problems import SHOCKBUBBLE, SWIRL, swirl_dt
     if prob is SWIRL:
         return swirl_dt(wl["mx"], wl["minlevel"])
+    if prob is SHOCKBUBBLE:
+        # CFL ~0.8 for the post-shock speed u + c (about 1.7) on the coarsest level
+        return 0.8 * (1.0 / (wl["mx"] << wl["minlevel"])) / 1.7
     # coarse-level dt for CFL ~0.9 at the initial state (max speed sqrt(g*2))
     dx = 2.0 / (wl["mx"] << wl["minlevel"])
     return 0.9 * dx / (2.0 ** 0.5 * 1.5)
@@ -157,10 +167,11 @@ def _initial_dt(wl: dict, prob) -> float:
 def cpu_sample(wl: dict, precision: str, max_seconds: float = 20.0, threads: int = 0):
     """Time the FP64 CPU oracle on the workload's initial forest for a bounded number of steps."""
     from oracle import pyoracle as po
-    from tests.cases import DAM, SWIRL, make
+    from tests.cases import DAM, SHOCKBUBBLE, SWIRL, make
     prob = _preset(wl)
     kw = {k: wl[k] for k in ("mx", "my", "minlevel", "maxlevel", "subcycle", "time_sync")}
-    oc, _ = make(SWIRL if wl["name"].startswith("swirl") else DAM, nthreads=threads, **kw)
+    case = SWIRL if wl["name"].startswith("swirl") else SHOCKBUBBLE if wl["name"].startswith("euler") else DAM
+    oc, _ = make(case, nthreads=threads, **kw)
     s = po.OracleSim(oc)
     s.initialize()
     dt = _initial_dt(wl, prob)
@@ -199,14 +210,86 @@ def run_reference(args, wl, rank, world):
     return 0
 
 
+def train_pstar_mlp(wl, prob, device, nsamples, epochs):
+    """Sample interface states uniformly from the FP64 run of the workload over
+    its spin-up steps (seed 0), train the p*-seed network on the GPU on the
+    states its gate selects, and return it with a summary (not timed)."""
+    import forestclaw_b200 as fb
+    from forestclaw_b200 import problems
+    kw = {k: wl[k] for k in ("mx", "my", "minlevel", "maxlevel", "subcycle", "time_sync")}
+    g = fb.Solver(problems.options(prob, device=device, **kw))
+    g.initialize()
+    t0 = time.perf_counter()
+    t, dt = 0.0, _initial_dt(wl, prob)
+    snaps = max(wl["spinup"], 1)
+    per = max(nsamples // snaps, 1)
+    parts = []
+    for n in range(snaps):
+        parts.append(g.sample_interfaces(per, seed=n))
+        cfl = g.advance(t, dt)
+        t += dt
+        dt *= 0.9 / cfl
+        if wl["regrid_interval"] and (n + 1) % wl["regrid_interval"] == 0:
+            g.regrid()
+    g.close()
+    prim = np.concatenate(parts)
+    rl, ul, pl, rr, ur, pr = prim.T
+    pb, rb = 0.5 * (pl + pr), 0.5 * (rl + rr)
+    strength = np.abs(pr - pl) / pb + np.abs(ur - ul) / np.sqrt(pb / rb)
+    strong = prim[strength > 0.2]
+    m = fb.PStarMLP(device=device, seed=0)
+    info = {"samples": int(len(prim)), "gated_samples": int(len(strong)), "epochs": epochs}
+    if len(strong) >= 256:
+        m.set_data(strong, gamma=1.4, tol=1e-10)
+        h0 = m.newton_histogram(False)
+        info["loss"] = m.train(epochs=epochs, batch=4096, lr=2e-3, seed=0)
+        h1 = m.newton_histogram(True)
+        mean = lambda h: float((np.arange(32) * h).sum() / max(h.sum(), 1))
+        info["gated_newton_mean_pvrs"] = mean(h0)
+        info["gated_newton_mean_mlp"] = mean(h1)
+    info["train_s"] = time.perf_counter() - t0
+    return m, info
+
+
+def error_vs_fp64(wl, prob, device, mlp, steps=8):
+    """Relative L1 error per field of the FP32-wave run against the FP64 run
+    (bitwise equal to the CPU oracle) from the same initial forest, no regrid."""
+    import forestclaw_b200 as fb
+    from forestclaw_b200 import problems
+    kw = {k: wl[k] for k in ("mx", "my", "minlevel", "maxlevel", "subcycle", "time_sync")}
+    a = fb.Solver(problems.options(prob, device=device, **kw))
+    b = fb.Solver(problems.options(prob, device=device, precision=fb.PREC_FP32WAVE, **kw))
+    a.initialize(); b.initialize()
+    if mlp is not None:
+        b.set_pstar_seed(mlp)
+    t, dt = 0.0, _initial_dt(wl, prob)
+    for _ in range(steps):
+        ca = a.advance(t, dt)
+        b.advance(t, dt)
+        t += dt
+        dt *= 0.9 / ca
+    qa, qb = a.get_q()[:, :, 2:-2, 2:-2], b.get_q()[:, :, 2:-2, 2:-2]
+    a.close(); b.close()
+    out = []
+    for m in range(qa.shape[1]):
+        den = np.abs(qa[:, m]).sum() if np.abs(qa[:, m]).sum() > 0 else np.abs(qa[:, 0]).sum()
+        out.append(float(np.abs(qa[:, m] - qb[:, m]).sum() / den))
+    return {"steps": steps, "l1_rel_per_field": out}
+
+
 def run_ours(args, wl, rank, world, local_rank):
     import torch
     import forestclaw_b200 as fb
     torch.cuda.set_device(local_rank)
     prob, gc = _options(wl, args.precision)
     gc.device = local_rank
+    mlp, mlp_info = None, None
+    if args.pstar == "mlp":
+        mlp, mlp_info = train_pstar_mlp(wl, prob, local_rank, args.mlp_samples, args.mlp_epochs)
     g = fb.Solver(gc)
     g.initialize()
+    if mlp is not None:
+        g.set_pstar_seed(mlp)
     dt = _initial_dt(wl, prob)
     t = 0.0
     # spin-up with regrid so the timed forest is representative (not timed)
@@ -320,6 +403,12 @@ def run_ours(args, wl, rank, world, local_rank):
                 "bytes_per_cell_update": 8 * (2 * gc.meqn + gc.maux),
                 "avg_launch_ms": upd_ms / max(upd_launches, 1)}
     cpu = cpu_sample(wl, args.precision, max_seconds=args.cpu_seconds) if args.cpu_seconds > 0 else None
+    err = error_vs_fp64(wl, prob, local_rank, mlp) if args.precision == "fp32wave" else None
+    newton = None
+    if wl["name"].startswith("euler"):
+        h = g.newton_histogram()
+        newton = {"mean_iterations": float((np.arange(32) * h).sum() / max(h.sum(), 1)),
+                  "histogram": [int(v) for v in h[:12]], "pstar_start": args.pstar, "mlp": mlp_info}
     line = {
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
@@ -335,6 +424,7 @@ def run_ours(args, wl, rank, world, local_rank):
                    "regrids_in_timed_loop": len(timed_regrid_ms),
                    "regrid_ms_median": float(np.median(regrid_ms + timed_regrid_ms)) if regrid_ms else None},
         "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+        "error_vs_fp64": err, "newton": newton,
         "gpu_launches": launches, "update_launches": upd_launches,
     }
     print(json.dumps(line), flush=True)
@@ -351,6 +441,10 @@ def main():
     ap.add_argument("--workload", default="dam", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32wave"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--pstar", default="pvrs", choices=["pvrs", "mlp"],
+                    help="Euler: Newton start of the exact solver (mlp: trained on the FP64 run first)")
+    ap.add_argument("--mlp-samples", type=int, default=1_000_000)
+    ap.add_argument("--mlp-epochs", type=int, default=20)
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -401,6 +401,7 @@ struct RPEulerExact {
             const double ppv = 0.5 * (pl + pr) - 0.125 * du * (rl + rr) * (al + ar);
             p = ppv > tolpre ? ppv : tolpre;
         }
+        if (pl == pr && ul == ur) { iters = 0; return pl; }
         int it;
         for (it = 1; it <= 64; it++) {
             double fl, fdl, fr, fdr;
@@ -449,23 +450,32 @@ struct RPEulerExact {
             p = ppv > tolpre ? ppv : tolpre;
         }
         double fl = 0.0, fr = 0.0, fdl, fdr;
-        int it;
-        for (it = 1; it <= 64; it++) {
-            prefun(g1, g4, g5, g6, p, P.rl, P.pl, P.al, fl, fdl);
-            prefun(g1, g4, g5, g6, p, P.rr, P.pr, P.ar, fr, fdr);
-            double pn = p - (fl + fr + du) / (fdl + fdr);
-            if (pn < 0.0) pn = tolpre;
-            const double change = 2.0 * fabs(pn - p) / (pn + p);
-            p = pn;
-            if (change <= ep.tol) break;
+        int it = 0;
+        if (P.pl == P.pr && P.ul == P.ur) {
+            // no pressure or normal-velocity jump: p* = p, u* = u exactly (the first
+            // Newton step's values, bit for bit), no iteration
+            p = P.pl;
+        } else {
+            for (it = 1; it <= 64; it++) {
+                prefun(g1, g4, g5, g6, p, P.rl, P.pl, P.al, fl, fdl);
+                prefun(g1, g4, g5, g6, p, P.rr, P.pr, P.ar, fr, fdr);
+                double pn = p - (fl + fr + du) / (fdl + fdr);
+                if (pn < 0.0) pn = tolpre;
+                const double change = 2.0 * fabs(pn - p) / (pn + p);
+                p = pn;
+                if (change <= ep.tol) break;
+            }
+            if (it > 64) it = 64;
         }
-        if (it > 64) it = 64;
         const double ps = p;
         const double us = 0.5 * (P.ul + P.ur) + 0.5 * (fr - fl);
+        // star densities and sound speeds (p* = pK: rhoK, aK exactly, as log 1 = 0, exp 0 = 1)
         double rsl, rsr, asl, asr;
         if (ps > P.pl) { const double q = ps / P.pl; rsl = P.rl * ((q + g6) / (g6 * q + 1.0)); asl = sqrt(gam * ps / rsl); }
+        else if (ps == P.pl) { rsl = P.rl; asl = P.al; }
         else { const double lq = fcb_log(ps / P.pl); rsl = P.rl * fcb_exp(lq / gam); asl = P.al * fcb_exp(g1 * lq); }
         if (ps > P.pr) { const double q = ps / P.pr; rsr = P.rr * ((q + g6) / (g6 * q + 1.0)); asr = sqrt(gam * ps / rsr); }
+        else if (ps == P.pr) { rsr = P.rr; asr = P.ar; }
         else { const double lq = fcb_log(ps / P.pr); rsr = P.rr * fcb_exp(lq / gam); asr = P.ar * fcb_exp(g1 * lq); }
         const double shl = P.ul - P.al, shr = P.ur + P.ar;
         double sl, sr;

@@ -9,6 +9,8 @@
  *   waves  w1 = q*L - qL, w2 = q*R - q*L, w3 = qR - q*R;
  *   speeds s1 = left shock speed (or rarefaction head uL - aL), s2 = u*,
  *          s3 = right shock speed (or rarefaction head uR + aR).
+ * Interfaces without a pressure or normal-velocity jump take p* = p, u* = u
+ * without iterating (0 Newton iterations; the values equal the first Newton step's).
  * The Roe averages of applications/clawpack/euler/2d/rp/clawpack46_rpn2_euler4.f:83-100
  * are formed as well, for the transverse solver clawpack46_rpt2_euler4.f:56-94
  * (restated below).
@@ -146,23 +148,32 @@ int orc_euler_star(double gam, const double* wl, const double* wr, double seed, 
     }
     double fl = 0.0, fr = 0.0, fdl, fdr;
     int it = 0;
-    for (it = 1; it <= 64; it++) {
-        prefun(&E, p, rl, pl, al, &fl, &fdl);
-        prefun(&E, p, rr, pr, ar, &fr, &fdr);
-        double pn = p - (fl + fr + du) / (fdl + fdr);
-        if (pn < 0.0) pn = tolpre;
-        const double change = 2.0 * fabs(pn - p) / (pn + p);
-        p = pn;
-        if (change <= tol) break;
+    if (pl == pr && ul == ur) {
+        /* no pressure or normal-velocity jump: p* = p, u* = u exactly (what the
+         * first Newton step returns bit for bit); no iteration is needed */
+        p = pl;
+    } else {
+        for (it = 1; it <= 64; it++) {
+            prefun(&E, p, rl, pl, al, &fl, &fdl);
+            prefun(&E, p, rr, pr, ar, &fr, &fdr);
+            double pn = p - (fl + fr + du) / (fdl + fdr);
+            if (pn < 0.0) pn = tolpre;
+            const double change = 2.0 * fabs(pn - p) / (pn + p);
+            p = pn;
+            if (change <= tol) break;
+        }
+        if (it > 64) it = 64;
     }
-    if (it > 64) it = 64;
     const double us = 0.5 * (ul + ur) + 0.5 * (fr - fl);
     out[0] = p;
     out[1] = us;
-    /* star densities and sound speeds */
+    /* star densities and sound speeds (p* = pK: the rarefaction formulas give
+     * rhoK, aK exactly, since log 1 = 0 and exp 0 = 1 in orc_log / orc_exp) */
     if (p > pl) { const double q = p / pl; out[2] = rl * ((q + E.g6) / (E.g6 * q + 1.0)); out[4] = sqrt(gam * p / out[2]); }
+    else if (p == pl) { out[2] = rl; out[4] = al; }
     else { const double lq = orc_log(p / pl); out[2] = rl * orc_exp(lq / gam); out[4] = al * orc_exp(E.g1 * lq); }
     if (p > pr) { const double q = p / pr; out[3] = rr * ((q + E.g6) / (E.g6 * q + 1.0)); out[5] = sqrt(gam * p / out[3]); }
+    else if (p == pr) { out[3] = rr; out[5] = ar; }
     else { const double lq = orc_log(p / pr); out[3] = rr * orc_exp(lq / gam); out[5] = ar * orc_exp(E.g1 * lq); }
     return it;
 }

@@ -163,4 +163,5 @@ def test_shockbubble_symmetry_and_conservation():
     m1 = s.mass()
     assert m1[0] > m0[0]
     hist = po.newton_hist(reset=True)
-    assert hist.sum() > 0 and hist[0] == 0
+    # bin 0: interfaces without a pressure / normal-velocity jump (no Newton step)
+    assert hist[0] > 0 and hist[1:].sum() > 0
