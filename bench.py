@@ -157,8 +157,9 @@ def _initial_dt(wl: dict, prob) -> float:
     if prob is SWIRL:
         return swirl_dt(wl["mx"], wl["minlevel"])
     if prob is SHOCKBUBBLE:
-        # CFL ~0.8 for the post-shock speed u + c (about 1.7) on the coarsest level
-        return 0.8 * (1.0 / (wl["mx"] << wl["minlevel"])) / 1.7
+        # CFL ~0.8 for the fastest initial wave, the sound speed sqrt(1.4/0.138) = 3.19
+        # inside the bubble, on the coarsest level
+        return 0.8 * (1.0 / (wl["mx"] << wl["minlevel"])) / 3.2
     # coarse-level dt for CFL ~0.9 at the initial state (max speed sqrt(g*2))
     dx = 2.0 / (wl["mx"] << wl["minlevel"])
     return 0.9 * dx / (2.0 ** 0.5 * 1.5)

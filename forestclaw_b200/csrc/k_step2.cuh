@@ -55,7 +55,7 @@ struct Step2Geom {
     // per-interface transverse terms: A1, A2 (from amdq), B1, B2 (from apdq)
     static constexpr int TSZ = 4 * MEQN;
     static constexpr int AUXS = MAUX > 0 ? MAUX : 0;
-    static constexpr bool USE_FLX = F32 && RP::CONS_FLUX && !RP::EXACT64;   // per-cell FP64 fluxes for the remainder
+    static constexpr bool USE_FLX = F32 && RP::CONS_FLUX;   // per-cell FP64 fluxes (remainder / Godunov split)
     static constexpr size_t DOUBLES = (size_t)MEQN * NXY * 5 + (size_t)AUXS * NXY +
                                       (USE_FLX ? (size_t)MEQN * NXY : 0) + 64;
     static constexpr size_t TWS = (size_t)WSZ * NI + (size_t)TSZ * NI + (F32 ? (size_t)MEQN * NXY : 0);
@@ -81,6 +81,17 @@ __device__ __forceinline__ void rpn2_cons_sw(int idir, const T* q, T grav, T* fl
     flux[mu] = (hun * hun) / h + T(0.5) * grav * (h * h);
     flux[mv] = un * hut;
 }
+
+// Correctly rounded, uncontracted multiply / add.  The FP32-wave unit is built with
+// FMA contraction; the second-order correction must not be contracted, or the
+// exactly opposite terms of the waves at a reflecting wall leave the rounding
+// error of one product as a flux through the wall.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
 
 template <class RP, int MX, int MY, int MBC, bool FWAVE, int NT, typename TW, int MINB = 2>
 __global__ void __launch_bounds__(NT, MINB)
@@ -205,7 +216,27 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
 
     // Normal solve of one interface (qL = cell cL, qR = cell cR).
     auto normal_solve = [&](int ixy, int cL, int cR, int k, bool cfl_range, TW d1, TW d0, State& st, double seed) {
-        if constexpr (RP::EXACT64) {
+        if constexpr (RP::EXACT64 && F32) {
+            float qL[MEQN], qR[MEQN], w32[MWAVES][MEQN], s32[MWAVES], ex32[NEXTRA];
+            double qL64[MEQN], qR64[MEQN], fL[MEQN], fR[MEQN], am64[MEQN], ap64[MEQN];
+            for (int m = 0; m < MEQN; m++) {
+                qL[m] = Qf[m * NXY + cL]; qR[m] = Qf[m * NXY + cR];
+                qL64[m] = Qs[m * NXY + cL]; qR64[m] = Qs[m * NXY + cR];
+                fL[m] = FLX[m * NXY + cL]; fR[m] = FLX[m * NXY + cR];
+            }
+            const EulerParams ep{sp.gamma, sp.newton_tol, seed};
+            const int it = RP::solve_mixed(ixy, qL, qR, qL64, qR64, fL, fR, ep, w32, s32, am64, ap64, ex32);
+            atomicAdd(&nhist[it < 31 ? it : 31], 1u);
+            for (int mw = 0; mw < MWAVES; mw++) {
+                st.s[mw] = (TW)s32[mw];
+                for (int m = 0; m < MEQN; m++) st.wave[mw][m] = (TW)w32[mw][m];
+            }
+            for (int m = 0; m < MEQN; m++) {
+                st.am[m] = (TW)am64[m]; st.ap[m] = (TW)ap64[m];
+                st.g64[m] = am64[m]; st.g64[MEQN + m] = ap64[m];
+            }
+            for (int e = 0; e < NEXTRA; e++) st.ex[e] = (TW)ex32[e];
+        } else if constexpr (RP::EXACT64) {
             double qL64[MEQN], qR64[MEQN], w64[MWAVES][MEQN], s64[MWAVES], am64[MEQN], ap64[MEQN], ex64[NEXTRA];
             for (int m = 0; m < MEQN; m++) { qL64[m] = Qs[m * NXY + cL]; qR64[m] = Qs[m * NXY + cR]; }
             const EulerParams ep{sp.gamma, sp.newton_tol, seed};
@@ -304,8 +335,13 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
                 for (int m = 0; m < MEQN; m++) {
                     TW c = TW(0);
                     for (int mw = 0; mw < MWAVES; mw++) {
-                        if (FWAVE) c = c + sgn1(st.s[mw]) * (TW(1) - fabs(st.s[mw]) * dave) * st.wave[mw][m];
-                        else { const TW sa = fabs(st.s[mw]); c = c + sa * (TW(1) - sa * dave) * st.wave[mw][m]; }
+                        if (FWAVE)
+                            c = add_rn(c, mul_rn(mul_rn(sgn1(st.s[mw]), sub_rn(TW(1), mul_rn(fabs(st.s[mw]), dave))),
+                                                 st.wave[mw][m]));
+                        else {
+                            const TW sa = fabs(st.s[mw]);
+                            c = add_rn(c, mul_rn(mul_rn(sa, sub_rn(TW(1), mul_rn(sa, dave))), st.wave[mw][m]));
+                        }
                     }
                     cq[m] = c;
                     if (F32) {
@@ -351,7 +387,7 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
             for (int c = tid; c < NXY; c += NT) {
                 double qv[MEQN], fv[MEQN];
                 for (int m = 0; m < MEQN; m++) qv[m] = Qs[m * NXY + c];
-                RP::flux64(ixy, qv, sp.grav, fv);
+                RP::flux64(ixy, qv, RP::EXACT64 ? sp.gamma : sp.grav, fv);
                 for (int m = 0; m < MEQN; m++) FLX[m * NXY + c] = fv[m];
             }
         }
@@ -491,6 +527,7 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
     // =================== x-sweeps (clawpack46_step2.f:113-167) ===================
     State st;
     cell_fluxes(1);
+    if constexpr (RP::EXACT64 && F32) __syncthreads();   // the exact solver reads the cell fluxes
     {
         const double seed = (RP::EXACT64 && sp.mlp) ? mlp_seed(1, tid < G::NIX ? tid : -1) : 0.0;
         if (REG) { if (tid < G::NIX) x1(tid, st, seed); }
@@ -503,6 +540,7 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
     // X3 and the y-sweep normal solves touch disjoint data: one phase
     for (int c = tid; c < NXY; c += NT) x3(c);
     cell_fluxes(2);
+    if constexpr (RP::EXACT64 && F32) __syncthreads();
     // =================== y-sweeps (clawpack46_step2.f:182-236) ===================
     {
         const double seed = (RP::EXACT64 && sp.mlp) ? mlp_seed(2, tid < G::NIY ? tid : -1) : 0.0;

@@ -41,7 +41,9 @@ cudaError_t launch_step2_f32w(int rp, const Dims& d, double* q, double* qlast, c
     FCB_CASE32(FC2D_B200_RP_SW_ROE, RPShallowRoe, 8, 8, 2, false, 160)
     FCB_CASE32(FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 16, 16, 2, true, 416)
     FCB_CASE32(FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 8, 8, 2, true, 160)
-    FCB_CASE32(FC2D_B200_RP_EULER_EXACT, RPEulerExact, 16, 16, 2, false, 352)
+    if (rp == FC2D_B200_RP_EULER_EXACT && d.mx == 16 && d.my == 16 && d.mbc == 2)
+        return run_step2_f32<RPEulerExact, 16, 16, 2, false, 352, 1>(d, q, qlast, aux, regs, desc, p0, npatch, sp,
+                                                                     cfl_bits, st);
     FCB_CASE32(FC2D_B200_RP_EULER_EXACT, RPEulerExact, 8, 8, 2, false, 128)
     return cudaErrorInvalidValue;
 }

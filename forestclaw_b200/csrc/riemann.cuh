@@ -534,6 +534,144 @@ struct RPEulerExact {
         for (int k = 0; k < 4; k++) { am[comp[k]] = f0[k] - flv[k]; ap[comp[k]] = frv[k] - f0[k]; }
         return it;
     }
+    // FP32-wave form of solve64.  Primitive states, Roe averages, star states,
+    // the Godunov state and the waves in FP32; the Newton iteration in FP64 (from
+    // the FP64 states, only where p or u jumps).  The Godunov flux f0 is one FP32
+    // value per interface, so amdq = f0 - F(qL) and apdq = F(qR) - f0 with the FP64
+    // cell fluxes of flxL/flxR keep the update conservative in FP64.
+    __device__ static int solve_mixed(int ixy, const float* qL, const float* qR, const double* qL64,
+                                      const double* qR64, const double* flxL, const double* flxR,
+                                      const EulerParams& ep, float w[3][4], float s[3], double* am, double* ap,
+                                      float* ex)
+    {
+        const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+        const float gam = (float)ep.gam, gamma1 = gam - 1.0f;
+        const float g1 = (gam - 1.0f) / (2.0f * gam), g2 = (gam + 1.0f) / (2.0f * gam);
+        const float g3 = 2.0f * gam / (gam - 1.0f), g4 = 2.0f / (gam - 1.0f), g5 = 2.0f / (gam + 1.0f);
+        const float g6 = (gam - 1.0f) / (gam + 1.0f), g7 = (gam - 1.0f) / 2.0f;
+        {   // Roe averages for rpt2
+            const float rhsqrtl = sqrtf(qL[0]), rhsqrtr = sqrtf(qR[0]);
+            const float pl = gamma1 * (qL[3] - 0.5f * (qL[1] * qL[1] + qL[2] * qL[2]) / qL[0]);
+            const float pr = gamma1 * (qR[3] - 0.5f * (qR[1] * qR[1] + qR[2] * qR[2]) / qR[0]);
+            const float rhsq2 = rhsqrtl + rhsqrtr;
+            const float u = (qL[mu] / rhsqrtl + qR[mu] / rhsqrtr) / rhsq2;
+            const float v = (qL[mv] / rhsqrtl + qR[mv] / rhsqrtr) / rhsq2;
+            const float enth = ((qL[3] + pl) / rhsqrtl + (qR[3] + pr) / rhsqrtr) / rhsq2;
+            const float a2 = gamma1 * (enth - 0.5f * (u * u + v * v));
+            ex[0] = u; ex[1] = v; ex[2] = enth; ex[3] = sqrtf(a2); ex[4] = gamma1 / a2;
+        }
+        // primitive states with correctly rounded, uncontracted operations, so the
+        // two sides of an interface between equal states compute the same values
+        auto pres = [&](const float* q) {
+            const float ke = __fdiv_rn(__fmul_rn(0.5f, __fadd_rn(__fmul_rn(q[mu], q[mu]), __fmul_rn(q[mv], q[mv]))), q[0]);
+            return __fmul_rn(gamma1, __fsub_rn(q[3], ke));
+        };
+        const float rl = qL[0], ul = __fdiv_rn(qL[mu], rl), vl = __fdiv_rn(qL[mv], rl), pl = pres(qL);
+        const float rr = qR[0], ur = __fdiv_rn(qR[mu], rr), vr = __fdiv_rn(qR[mv], rr), pr = pres(qR);
+        const float al = sqrtf(gam * pl / rl), ar = sqrtf(gam * pr / rr);
+        int it = 0;
+        float ps, us;
+        const bool nojump = (pl == pr && ul == ur);
+        if (nojump) {
+            ps = pl; us = ul;
+        } else {
+            const Prim P = prim(ixy, qL64, qR64, ep.gam);
+            const double gd = ep.gam;
+            const double d1 = (gd - 1.0) / (2.0 * gd), d4 = 2.0 / (gd - 1.0), d5 = 2.0 / (gd + 1.0);
+            const double d6 = (gd - 1.0) / (gd + 1.0);
+            const double du = P.ur - P.ul, tolpre = 1.0e-6;
+            double p;
+            if (ep.seed > 0.0 && isfinite(ep.seed)) p = ep.seed;
+            else {
+                const double ppv = 0.5 * (P.pl + P.pr) - 0.125 * du * (P.rl + P.rr) * (P.al + P.ar);
+                p = ppv > tolpre ? ppv : tolpre;
+            }
+            double fl = 0.0, fr = 0.0, fdl, fdr;
+            for (it = 1; it <= 64; it++) {
+                prefun(d1, d4, d5, d6, p, P.rl, P.pl, P.al, fl, fdl);
+                prefun(d1, d4, d5, d6, p, P.rr, P.pr, P.ar, fr, fdr);
+                double pn = p - (fl + fr + du) / (fdl + fdr);
+                if (pn < 0.0) pn = tolpre;
+                const double change = 2.0 * fabs(pn - p) / (pn + p);
+                p = pn;
+                if (change <= ep.tol) break;
+            }
+            if (it > 64) it = 64;
+            ps = (float)p;
+            us = (float)(0.5 * (P.ul + P.ur) + 0.5 * (fr - fl));
+        }
+        float rsl, rsr, asl, asr;
+        if (ps > pl) { const float q = ps / pl; rsl = rl * ((q + g6) / (g6 * q + 1.0f)); asl = sqrtf(gam * ps / rsl); }
+        else if (ps == pl) { rsl = rl; asl = al; }
+        else { const float lq = __logf(ps / pl); rsl = rl * __expf(lq / gam); asl = al * __expf(g1 * lq); }
+        if (ps > pr) { const float q = ps / pr; rsr = rr * ((q + g6) / (g6 * q + 1.0f)); asr = sqrtf(gam * ps / rsr); }
+        else if (ps == pr) { rsr = rr; asr = ar; }
+        else { const float lq = __logf(ps / pr); rsr = rr * __expf(lq / gam); asr = ar * __expf(g1 * lq); }
+        const float shl = ul - al, shr = ur + ar;
+        const float sl = (ps > pl) ? ul - al * sqrtf(g2 * (ps / pl) + g1) : shl;
+        const float sr = (ps > pr) ? ur + ar * sqrtf(g2 * (ps / pr) + g1) : shr;
+        s[0] = sl; s[1] = us; s[2] = sr;
+        const float esl = ps / gamma1 + 0.5f * rsl * (us * us + vl * vl);
+        const float esr = ps / gamma1 + 0.5f * rsr * (us * us + vr * vr);
+        const float qln[4] = {qL[0], qL[mu], qL[mv], qL[3]}, qrn[4] = {qR[0], qR[mu], qR[mv], qR[3]};
+        const float qsl[4] = {rsl, rsl * us, rsl * vl, esl};
+        const float qsr[4] = {rsr, rsr * us, rsr * vr, esr};
+        const int comp[4] = {0, mu, mv, 3};
+        for (int k = 0; k < 4; k++) {
+            if (nojump) {   // the star states are the outer states: only the contact/shear wave
+                w[0][comp[k]] = 0.0f;
+                w[1][comp[k]] = qrn[k] - qln[k];
+                w[2][comp[k]] = 0.0f;
+            } else {
+                w[0][comp[k]] = qsl[k] - qln[k];
+                w[1][comp[k]] = qsr[k] - qsl[k];
+                w[2][comp[k]] = qrn[k] - qsr[k];
+            }
+        }
+        float r0, u0, v0, p0, e0;
+        int which;
+        if (0.0f <= us) {
+            v0 = vl;
+            if (ps > pl) which = (0.0f <= sl) ? 0 : 1;
+            else if (0.0f <= shl) which = 0;
+            else which = (0.0f > us - asl) ? 1 : 2;
+        } else {
+            v0 = vr;
+            if (ps > pr) which = (0.0f >= sr) ? 4 : 3;
+            else if (0.0f >= shr) which = 4;
+            else which = (0.0f < us + asr) ? 3 : 5;
+        }
+        if (which == 0) { r0 = rl; u0 = ul; p0 = pl; e0 = qL[3]; }
+        else if (which == 4) { r0 = rr; u0 = ur; p0 = pr; e0 = qR[3]; }
+        else if (which == 1) { r0 = rsl; u0 = us; p0 = ps; e0 = esl; }
+        else if (which == 3) { r0 = rsr; u0 = us; p0 = ps; e0 = esr; }
+        else if (which == 2) {
+            const float c = g5 + (g6 / al) * ul, lc = __logf(c);
+            r0 = rl * __expf(g4 * lc); u0 = g5 * (al + g7 * ul); p0 = pl * __expf(g3 * lc);
+            e0 = p0 / gamma1 + 0.5f * r0 * (u0 * u0 + v0 * v0);
+        } else {
+            const float c = g5 - (g6 / ar) * ur, lc = __logf(c);
+            r0 = rr * __expf(g4 * lc); u0 = g5 * (-ar + g7 * ur); p0 = pr * __expf(g3 * lc);
+            e0 = p0 / gamma1 + 0.5f * r0 * (u0 * u0 + v0 * v0);
+        }
+        if (nojump) {
+            // without a pressure / normal-velocity jump the Godunov state on the
+            // sampled side of the contact is that side's own state: its FP64 flux
+            const bool left = which <= 2;
+            for (int m = 0; m < 4; m++) {
+                am[m] = left ? 0.0 : flxR[m] - flxL[m];
+                ap[m] = left ? flxR[m] - flxL[m] : 0.0;
+            }
+            return it;
+        }
+        const float f0[4] = {r0 * u0, r0 * u0 * u0 + p0, r0 * u0 * v0, u0 * (e0 + p0)};
+        for (int k = 0; k < 4; k++) {
+            const double f = (double)f0[k];
+            am[comp[k]] = f - flxL[comp[k]];
+            ap[comp[k]] = flxR[comp[k]] - f;
+        }
+        return it;
+    }
     // clawpack46_rpt2_euler4.f:56-94 with the Roe averages of the interface
     template <typename T>
     __device__ static void rpt2(int ixy, int imp, const T* qL, const T* qR, const T* aux1, const T* aux2,
@@ -561,8 +699,8 @@ struct RPEulerExact {
             bm[m] = b1; bp[m] = b2;
         }
     }
-    // The generic normal-solver entry is not used for EXACT64 solvers.
-    __device__ static void flux64(int, const double*, double, double*) {}
+    // FP64 normal flux of a cell for the FP32-wave form (gamma passed in place of grav)
+    __device__ static void flux64(int ixy, const double* q, double gam, double* f) { cons_flux(ixy - 1, q, gam, f); }
     __device__ static void godunov64(int, const double*, const double*, const double*, const double*, const double*,
                                      const double*, const float*, double*, double*, double) {}
     template <typename T>
