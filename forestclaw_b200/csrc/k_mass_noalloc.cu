@@ -1,4 +1,7 @@
-// k_mass_noalloc.cu -- mass diagnostic that allocates no device memory.
+// k_mass_noalloc.cu -- mass diagnostic that allocates no device memory, for
+// callers that may not allocate between steps (all device memory handed out by
+// their own pool, or other streams that the synchronisation of cudaFree would
+// stall).
 //
 // Same arithmetic as k_patch_mass + the host Kahan loop of fc2d_b200_mass
 // (fclaw2d_clawpatch46_diagnostics.f:13-55): per patch and field a Kahan sum of

@@ -145,9 +145,14 @@ int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed);
  * (fclaw2d_clawpatch46_diagnostics.f:13-55). */
 int fc2d_b200_mass(fc2d_b200_solver_t* s, double* out);
 /* fc2d_b200_mass computed without allocating memory (no counterpart in the
- * reference): the patch partials and the per-field sums go to one static device
- * array of FC2D_B200_MASS_SCRATCH_DOUBLES doubles per device, so
- * npatches*meqn + meqn must not exceed it (else FC2D_B200_EINVAL, nothing runs).
+ * reference).  It is for callers that must not allocate device memory between
+ * steps: an application whose device memory is all handed out by its own pool,
+ * or one that takes diagnostics while its other streams keep running, where the
+ * device-wide synchronisation of cudaFree would stall them.  The patch partials
+ * and the per-field sums go to one static device array of
+ * FC2D_B200_MASS_SCRATCH_DOUBLES doubles (1 MiB, held by every GPU that loads
+ * the library until the process exits), so npatches*meqn + meqn must not exceed
+ * it (else FC2D_B200_EINVAL, nothing runs).
  * Same result as fc2d_b200_mass, bit for bit.  No part of the scratch has to
  * start at zero.  The first call on a device resolves the scratch address; make
  * it before any stream capture begins on that device.  Calls that overlap in

@@ -1,7 +1,10 @@
-"""fc2d_b200_mass_noalloc: the mass diagnostic with its scratch in a static
-device array instead of allocated memory.  It must give the same bits as
-fc2d_b200_mass, on repeated calls and on a second solver of the same process,
-and refuse forests that do not fit the scratch."""
+"""fc2d_b200_mass_noalloc: the mass diagnostic for callers that may not
+allocate device memory between steps (an application that hands out all device
+memory from its own pool, or one whose other streams must not be stalled by the
+synchronisation of cudaFree).  Its scratch is a static device array instead of
+allocated memory.  It must give the same bits as fc2d_b200_mass, on two calls
+in a row and on a second solver of the same process, and refuse forests that do
+not fit the scratch.  This file is collected last on purpose."""
 import numpy as np
 import pytest
 
