@@ -53,6 +53,17 @@ class _Options(ctypes.Structure):
     ]
 
 
+class _Instance(ctypes.Structure):
+    _fields_ = [
+        ("minlevel", ctypes.c_int), ("maxlevel", ctypes.c_int),
+        ("ax", ctypes.c_double), ("bx", ctypes.c_double), ("ay", ctypes.c_double), ("by", ctypes.c_double),
+        ("mi", ctypes.c_int), ("mj", ctypes.c_int), ("pdata", ctypes.c_double * 32),
+    ]
+
+
+MAX_INSTANCES = 256
+
+
 @dataclass
 class Options:
     """fc2d_b200_options_t with the reference's option names and defaults."""
@@ -175,6 +186,11 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_mlp_newton_histogram": [P, I, ctypes.POINTER(ctypes.c_longlong)],
         "fc2d_b200_sample_interfaces": [P, I, ctypes.c_ulonglong, dp],
         "fc2d_b200_set_pstar_seed": [P, P],
+        "fc2d_b200_set_instances": [P, I, ctypes.POINTER(_Instance)],
+        "fc2d_b200_num_instances": [P, ip],
+        "fc2d_b200_patch_instance": [P, ip],
+        "fc2d_b200_advance_instances": [P, dp, dp],
+        "fc2d_b200_mass_instances": [P, dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -410,6 +426,38 @@ class Solver:
         out = (ctypes.c_ulonglong * 32)()
         self._check("fc2d_b200_newton_histogram", self.lib.fc2d_b200_newton_histogram(self.h, out, int(reset)))
         return np.array(out[:], np.int64)
+
+    # -- batches of independent forests ---------------------------------------
+    def set_instances(self, instances) -> None:
+        """Hold len(instances) independent forests; each is a dict with minlevel, maxlevel,
+        ax, bx, ay, by, mi, mj and pdata (up to 32 app parameters).  Before initialize()."""
+        n = len(instances)
+        arr = (_Instance * n)()
+        for i, d in enumerate(instances):
+            for k in ("minlevel", "maxlevel", "ax", "bx", "ay", "by", "mi", "mj"):
+                setattr(arr[i], k, d.get(k, getattr(self.opts, k)))
+            pd = d.get("pdata", self.opts.pdata)
+            for k, v in enumerate(pd):
+                arr[i].pdata[k] = v
+        self._check("fc2d_b200_set_instances", self.lib.fc2d_b200_set_instances(self.h, n, arr))
+        self.ninst = n
+
+    def patch_instance(self) -> np.ndarray:
+        out = np.zeros(self.num_patches, np.int32)
+        self._check("fc2d_b200_patch_instance", self.lib.fc2d_b200_patch_instance(self.h, _ip(out)))
+        return out
+
+    def advance_instances(self, dt) -> np.ndarray:
+        """One coarse step of every instance with its own dt; returns the CFL of each."""
+        dt = np.ascontiguousarray(dt, np.float64)
+        cfl = np.zeros(self.ninst, np.float64)
+        self._check("fc2d_b200_advance_instances", self.lib.fc2d_b200_advance_instances(self.h, _dp(dt), _dp(cfl)))
+        return cfl
+
+    def mass_instances(self) -> np.ndarray:
+        out = np.zeros((self.ninst, self.opts.meqn), np.float64)
+        self._check("fc2d_b200_mass_instances", self.lib.fc2d_b200_mass_instances(self.h, _dp(out)))
+        return out
 
     def mass_noalloc(self) -> np.ndarray:
         """mass() through the allocation-free entry point (static device scratch)."""

@@ -13,6 +13,8 @@ struct PatchDesc {
     int phys_mask;
     int face_type;      // 2 bits per face: 0 boundary, 1 half (finer nbr), 2 same, 3 double (coarser nbr)
     int flags;          // PATCH_* bits
+    int inst;           // instance of a batch of independent forests (0 otherwise)
+    int pad_;
 };
 
 enum { PATCH_HAS_FINE_NBR = 1 };
@@ -37,6 +39,7 @@ struct StepParams {
     int accumulate_waves;   // time_sync && fluctuation_correction (clawpack46_time_sync_accumulate_waves)
     int save_last;          // fclaw2d_clawpatch_save_current_step (q -> qlast)
     int app;                // b4step2 hook
+    int wall_faces;         // bit f: mthbc(f) == 3 (reflecting wall)
     double dt;
     double t;
     double grav;
@@ -46,6 +49,7 @@ struct StepParams {
     double newton_tol;      // Euler: Newton tolerance on the relative change of p*
     unsigned long long* newton_hist;   // Euler: 32-bin histogram of Newton iterations (or null)
     const void* mlp;        // Euler: p*-seed network blob (null: PVRS start)
+    const double* inst_dt;  // batch: coarse time step of each instance, dt = this[inst] * (level factor in dt)
 };
 
 }  // namespace fcb

@@ -86,7 +86,18 @@ struct fc2d_b200_solver {
     unsigned long long* newton_hist = nullptr;     // 32 bins, exact Euler solver
     void* mlp_blob = nullptr;                      // p*-seed network (null: PVRS start)
     bool use_mlp = false;
+    // batch of independent forests (instances); empty: one forest of the options
+    std::vector<fc2d_b200_instance_t> insts;
+    double* inst_dt_dev = nullptr;                 // coarse dt of each instance (device)
+    int ncfl = 1;                                  // CFL maxima kept (one per instance)
+    // phys_ok[l]: the ghost cells of level l on physical faces hold physical-BC
+    // values (set by a ghost update).  False after initialization: the reference
+    // fills no ghost cells there by default (init_ghostcell = 0,
+    // src/fclaw2d_initialize.c:140), so the first step sees qinit's ghost values.
+    unsigned char phys_ok[64] = {};
     DevVec<RepopOp> repop_dev;                     // regrid repopulation ops
+    DevVec<double> snap;                           // batch regrid: q of instances whose forest is unchanged
+    DevVec<int> keep_dev;
     std::vector<double> aux_host;                  // static aux mirror (level-major)
     DevVec<CopyEnt> t_copy, t_avg;
     DevVec<InterpEnt> t_interp;
@@ -207,6 +218,7 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
         for (int k = 0; k < 4; k++) ft |= (P.face_type[k] & 3) << (2 * k);
         pd.face_type = ft;
         pd.flags = P.has_fine_nbr ? PATCH_HAS_FINE_NBR : 0;
+        pd.inst = P.inst;
         hd[i] = pd;
     }
     if (!hd.empty()) CK(cudaMemcpyAsync(s->desc, hd.data(), hd.size() * sizeof(PatchDesc), cudaMemcpyHostToDevice, s->st));
@@ -280,6 +292,11 @@ static int update_level(fc2d_b200_solver* s, int level, double t, double dt)
     // save_current_step is only read by time interpolation of the coarser levels
     sp.save_last = (s->o.subcycle && level < f.maxlevel_present) ? 1 : 0;
     sp.app = s->o.app;
+    // reflecting walls whose ghost cells mirror the interior (FP32-wave mass rule)
+    sp.wall_faces = 0;
+    if (level >= 0 && level < 64 && s->phys_ok[level])
+        for (int f = 0; f < 4; f++)
+            if (s->o.mthbc[f] == 3) sp.wall_faces |= 1 << f;
     sp.dt = dt; sp.t = t; sp.grav = s->o.grav;
     sp.dry_tolerance = s->o.pdata[31] > 0 ? s->o.pdata[31] : 1e-3;
     sp.vt = 0.0;
@@ -287,6 +304,7 @@ static int update_level(fc2d_b200_solver* s, int level, double t, double dt)
     sp.newton_tol = s->o.newton_tol;
     sp.newton_hist = s->newton_hist;
     sp.mlp = s->use_mlp ? s->mlp_blob : nullptr;
+    sp.inst_dt = s->insts.empty() ? nullptr : s->inst_dt_dev;
     if (s->o.app == FC2D_B200_APP_SWIRL && s->o.tperiod != 0.0) {
         const double pi = 4.0 * std::atan(1.0), pi2 = 2.0 * pi;
         sp.vt = std::cos(pi2 * (t + dt / 2.0) / s->o.tperiod);
@@ -362,6 +380,8 @@ static void interpolate2ghost(fc2d_b200_solver* s, int l, int ti)
 
 static void ghost_update(fc2d_b200_solver* s, int minlevel, int maxlevel, int time_interp)
 {
+    if (s->fill)
+        for (int l = std::max(minlevel, 0); l <= std::min(maxlevel, 63); l++) s->phys_ok[l] = 1;
     const int mincoarse = minlevel, maxcoarse = maxlevel - 1;
     average_range(s, mincoarse, maxcoarse, 0);
     if (time_interp) average_range(s, mincoarse - 1, mincoarse - 1, 1);
@@ -482,8 +502,9 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
     s->d = Dims{o.mx, o.my, o.mbc, o.meqn, o.maux};
     s->forest.g = Geometry{s->d, s->o.mi, s->o.mj, o.ax, o.bx, o.ay, o.by};
     CK(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
-    CK(cudaMalloc(&s->cfl_dev, sizeof(unsigned long long)));
-    CK(cudaMallocHost(&s->cfl_host, sizeof(unsigned long long)));
+    CK(cudaMalloc(&s->cfl_dev, sizeof(unsigned long long) * FC2D_B200_MAX_INSTANCES));
+    CK(cudaMallocHost(&s->cfl_host, sizeof(unsigned long long) * FC2D_B200_MAX_INSTANCES));
+    CK(cudaMalloc(&s->inst_dt_dev, sizeof(double) * FC2D_B200_MAX_INSTANCES));
     CK(cudaMalloc(&s->params_dev, sizeof(StepParams) * fc2d_b200_solver::PCAP));
     {
         double bc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -513,7 +534,7 @@ extern "C" int fc2d_b200_destroy(fc2d_b200_solver_t* s)
     cudaFree(s->q); cudaFree(s->qlast); if (s->qinterp) cudaFree(s->qinterp);
     if (s->aux) cudaFree(s->aux); cudaFree(s->regs); cudaFree(s->desc);
     free_spare(s);
-    cudaFree(s->cfl_dev); cudaFreeHost(s->cfl_host);
+    cudaFree(s->cfl_dev); cudaFreeHost(s->cfl_host); cudaFree(s->inst_dt_dev);
     invalidate_graph(s);
     cudaFree(s->params_dev); cudaFreeHost(s->params_host);
     if (s->mass_dev) cudaFree(s->mass_dev);
@@ -546,8 +567,10 @@ static int install_forest(fc2d_b200_solver* s, const std::vector<Leaf>& leaves)
     std::string err;
     Forest nf;
     nf.g = s->forest.g;
+    nf.inst = s->forest.inst;
     if (!nf.build(leaves, err)) return fail(FC2D_B200_EFOREST, err);
     s->forest = std::move(nf);
+    std::memset(s->phys_ok, 0, sizeof(s->phys_ok));
     int rc = alloc_slabs(s, s->forest.np());
     if (rc) return rc;
     return upload_desc_and_tables(s);
@@ -565,54 +588,83 @@ extern "C" int fc2d_b200_set_forest(fc2d_b200_solver_t* s, int np, const int* le
     return 0;
 }
 
+// Options of instance i (a batch) or the solver's own.
+static fc2d_b200_options_t inst_options(const fc2d_b200_solver* s, int i)
+{
+    fc2d_b200_options_t o = s->o;
+    if (s->insts.empty()) return o;
+    const fc2d_b200_instance_t& I = s->insts[i];
+    o.minlevel = I.minlevel; o.maxlevel = I.maxlevel;
+    o.ax = I.ax; o.bx = I.bx; o.ay = I.ay; o.by = I.by; o.mi = I.mi; o.mj = I.mj;
+    for (int k = 0; k < 32; k++) o.pdata[k] = I.pdata[k];
+    return o;
+}
+// Forest-level bounds of an instance (levels are relative to the instance's minlevel in a batch).
+static int inst_minlev(const fc2d_b200_solver* s, int i) { (void)i; return s->insts.empty() ? s->o.minlevel : 0; }
+static int inst_maxlev(const fc2d_b200_solver* s, int i)
+{
+    return s->insts.empty() ? s->o.maxlevel : s->insts[i].maxlevel - s->insts[i].minlevel;
+}
+
 extern "C" int fc2d_b200_initialize(fc2d_b200_solver_t* s)
 {
     if (!s) return fail(FC2D_B200_EINVAL, "null solver");
     if (s->o.app == FC2D_B200_APP_NONE) return fail(FC2D_B200_EINVAL, "initialize needs a built-in app");
     const Dims& d = s->d;
-    const int l0 = s->o.minlevel;
+    const int ni = s->forest.ninst();
+    std::vector<fc2d_b200_options_t> io(ni);
+    for (int i = 0; i < ni; i++) io[i] = inst_options(s, i);
     std::vector<Leaf> leaves;
-    for (int y = 0; y < (s->o.mj << l0); y++)
-        for (int x = 0; x < (s->o.mi << l0); x++) leaves.push_back({l0, x, y});
+    for (int i = 0; i < ni; i++) {
+        const int l0 = inst_minlev(s, i), la = l0 + s->forest.gi(i).lbase;
+        for (int y = 0; y < (io[i].mj << la); y++)
+            for (int x = 0; x < (io[i].mi << la); x++) leaves.push_back({l0, x, y, i});
+    }
     std::string err;
     Forest f;
     f.g = s->forest.g;
+    f.inst = s->forest.inst;
     if (!f.build(leaves, err)) return fail(FC2D_B200_EFOREST, err);
     std::vector<double> q((size_t)f.np() * d.nq(), 0.0), aux((size_t)f.np() * d.naux(), 0.0);
     for (int i = 0; i < f.np(); i++) {
-        if (d.maux > 0) app_setaux(s->o, d, f.p[i], &aux[(size_t)i * d.naux()]);
-        app_qinit(s->o, d, f.p[i], d.maux > 0 ? &aux[(size_t)i * d.naux()] : nullptr, &q[(size_t)i * d.nq()]);
+        const fc2d_b200_options_t& oi = io[f.p[i].inst];
+        if (d.maux > 0) app_setaux(oi, d, f.p[i], &aux[(size_t)i * d.naux()]);
+        app_qinit(oi, d, f.p[i], d.maux > 0 ? &aux[(size_t)i * d.naux()] : nullptr, &q[(size_t)i * d.nq()]);
     }
     // initial refinement (fclaw2d_initialize.c:150-230): tag with init_flag, new patches get qinit
-    if (s->o.minlevel < s->o.maxlevel) {
-        for (int lev = s->o.minlevel; lev <= s->o.maxlevel; lev++) {
-            std::vector<int> mark(f.np(), 0);
-            for (int i = 0; i < f.np(); i++)
-                if (f.p[i].level < s->o.maxlevel && app_tag_refine(s->o, d, f.p[i], &q[(size_t)i * d.nq()])) mark[i] = 1;
-            int changed = 0;
-            std::vector<Leaf> L = adapt_leaves(f, mark, changed, err);
-            if (!changed) break;
-            Forest nf;
-            nf.g = f.g;
-            if (!nf.build(L, err)) return fail(FC2D_B200_EFOREST, err);
-            std::vector<double> nq((size_t)nf.np() * d.nq(), 0.0), naux((size_t)nf.np() * d.naux(), 0.0);
-            for (int i = 0; i < nf.np(); i++) {
-                const PatchInfo& P = nf.p[i];
-                const int old = f.lookup(P.level, P.gx, P.gy);
-                if (old >= 0) {
-                    std::memcpy(&nq[(size_t)i * d.nq()], &q[(size_t)old * d.nq()], sizeof(double) * d.nq());
-                    if (d.maux > 0) std::memcpy(&naux[(size_t)i * d.naux()], &aux[(size_t)old * d.naux()], sizeof(double) * d.naux());
-                } else {
-                    if (d.maux > 0) app_setaux(s->o, d, P, &naux[(size_t)i * d.naux()]);
-                    app_qinit(s->o, d, P, d.maux > 0 ? &naux[(size_t)i * d.naux()] : nullptr, &nq[(size_t)i * d.nq()]);
-                }
-            }
-            f = std::move(nf);
-            q.swap(nq); aux.swap(naux);
+    int maxspan = 0;
+    for (int i = 0; i < ni; i++) maxspan = std::max(maxspan, inst_maxlev(s, i) - inst_minlev(s, i));
+    for (int pass = 0; pass <= maxspan; pass++) {
+        std::vector<int> mark(f.np(), 0);
+        for (int i = 0; i < f.np(); i++) {
+            const PatchInfo& P = f.p[i];
+            if (P.level < inst_maxlev(s, P.inst) && app_tag_refine(io[P.inst], d, P, &q[(size_t)i * d.nq()])) mark[i] = 1;
         }
+        int changed = 0;
+        std::vector<Leaf> L = adapt_leaves(f, mark, changed, err);
+        if (!changed) break;
+        Forest nf;
+        nf.g = f.g;
+        nf.inst = f.inst;
+        if (!nf.build(L, err)) return fail(FC2D_B200_EFOREST, err);
+        std::vector<double> nq((size_t)nf.np() * d.nq(), 0.0), naux((size_t)nf.np() * d.naux(), 0.0);
+        for (int i = 0; i < nf.np(); i++) {
+            const PatchInfo& P = nf.p[i];
+            const int old = f.lookup(P.inst, P.level, P.gx, P.gy);
+            if (old >= 0) {
+                std::memcpy(&nq[(size_t)i * d.nq()], &q[(size_t)old * d.nq()], sizeof(double) * d.nq());
+                if (d.maux > 0) std::memcpy(&naux[(size_t)i * d.naux()], &aux[(size_t)old * d.naux()], sizeof(double) * d.naux());
+            } else {
+                const fc2d_b200_options_t& oi = io[P.inst];
+                if (d.maux > 0) app_setaux(oi, d, P, &naux[(size_t)i * d.naux()]);
+                app_qinit(oi, d, P, d.maux > 0 ? &naux[(size_t)i * d.naux()] : nullptr, &nq[(size_t)i * d.nq()]);
+            }
+        }
+        f = std::move(nf);
+        q.swap(nq); aux.swap(naux);
     }
     std::vector<Leaf> L;
-    for (const auto& P : f.p) L.push_back({P.level, P.gx, P.gy});
+    for (const auto& P : f.p) L.push_back({P.level, P.gx, P.gy, P.inst});
     int rc = install_forest(s, L);
     if (rc) return rc;
     // install_forest sorted identically (same keys) -> same slot order as f
@@ -637,7 +689,7 @@ extern "C" int fc2d_b200_patch_info(const fc2d_b200_solver_t* s, int* level, int
     if (!s) return fail(FC2D_B200_EINVAL, "null solver");
     for (int i = 0; i < s->forest.np(); i++) {
         const PatchInfo& P = s->forest.p[i];
-        if (level) level[i] = P.level;
+        if (level) level[i] = P.level + s->forest.gi(P.inst).lbase;
         if (block) block[i] = P.block;
         if (gx) gx[i] = P.gx;
         if (gy) gy[i] = P.gy;
@@ -658,6 +710,7 @@ extern "C" int fc2d_b200_set_q(fc2d_b200_solver_t* s, const double* q)
     if (!s || !q) return fail(FC2D_B200_EINVAL, "null argument");
     CK(cudaMemcpyAsync(s->q, q, (size_t)s->forest.np() * s->d.nq() * sizeof(double), cudaMemcpyHostToDevice, s->st));
     CK(cudaStreamSynchronize(s->st));
+    std::memset(s->phys_ok, 0, sizeof(s->phys_ok));   // ghost cells are the caller's values
     return 0;
 }
 
@@ -698,17 +751,25 @@ extern "C" int fc2d_b200_get_registers(fc2d_b200_solver_t* s, double* r)
 
 static int begin_cfl(fc2d_b200_solver* s)
 {
-    CK(cudaMemsetAsync(s->cfl_dev, 0, sizeof(unsigned long long), s->st));
+    CK(cudaMemsetAsync(s->cfl_dev, 0, sizeof(unsigned long long) * s->ncfl, s->st));
     return 0;
 }
 
-static int end_cfl(fc2d_b200_solver* s, double* cfl)
+// Level CFL maximum (over all instances); per instance into cfl_inst if given.
+static int end_cfl(fc2d_b200_solver* s, double* cfl, double* cfl_inst = nullptr)
 {
-    CK(cudaMemcpyAsync(s->cfl_host, s->cfl_dev, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(s->cfl_host, s->cfl_dev, sizeof(unsigned long long) * s->ncfl, cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
-    const double v = bits_to_double(*s->cfl_host);
-    if (cfl) *cfl = v;
-    if (!(v == v)) return fail(FC2D_B200_EDEVICE, "non-finite CFL (negative depth or NaN in the update)");
+    double v = 0.0;
+    bool bad = false;
+    for (int i = 0; i < s->ncfl; i++) {
+        const double c = bits_to_double(s->cfl_host[i]);
+        if (!(c == c)) bad = true;
+        if (c > v) v = c;
+        if (cfl_inst) cfl_inst[i] = c;
+    }
+    if (cfl) *cfl = bad ? bits_to_double(0x7ff8000000000000ull) : v;
+    if (bad) return fail(FC2D_B200_EDEVICE, "non-finite CFL (negative depth or NaN in the update)");
     return 0;
 }
 
@@ -876,10 +937,10 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     std::vector<int> mark(np, 0);
     for (int i = 0; i < np; i++) {
         const PatchInfo& P = f.p[i];
-        if (P.level <= s->o.minlevel || (P.gx & 1) || (P.gy & 1)) continue;
+        if (P.level <= inst_minlev(s, P.inst) || (P.gx & 1) || (P.gy & 1)) continue;
         int sib[4]; bool ok = true;
         for (int k = 0; k < 4; k++) {
-            sib[k] = f.lookup(P.level, P.gx + (k & 1), P.gy + (k >> 1));
+            sib[k] = f.lookup(P.inst, P.level, P.gx + (k & 1), P.gy + (k >> 1));
             if (sib[k] < 0) { ok = false; break; }
         }
         if (!ok) continue;
@@ -888,7 +949,7 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
         if (coarsen) for (int k = 0; k < 4; k++) mark[sib[k]] = -1;
     }
     for (int i = 0; i < np; i++)
-        if (f.p[i].level < s->o.maxlevel && (flags[i] & 1)) mark[i] = 1;
+        if (f.p[i].level < inst_maxlev(s, f.p[i].inst) && (flags[i] & 1)) mark[i] = 1;
     int changed = 0;
     std::string err;
     std::vector<Leaf> L = adapt_leaves(f, mark, changed, err);
@@ -896,7 +957,29 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     if (!changed) return 0;
     Forest nf;
     nf.g = f.g;
+    nf.inst = f.inst;
     if (!nf.build(L, err)) return fail(FC2D_B200_EFOREST, err);
+    // batch: an instance without an applied refinement or family coarsening
+    // keeps its ghost cells, as it would alone (fclaw2d_regrid does no ghost
+    // update then); a coarsening that balance refines again still counts as a change
+    std::vector<int> keep;
+    if (!s->insts.empty()) {
+        std::vector<int> adapted(nf.ninst(), 0);
+        for (int i = 0; i < np; i++) {
+            const PatchInfo& P = f.p[i];
+            if (mark[i] > 0) adapted[P.inst] = 1;
+            if (mark[i] < 0) {
+                bool all = true;
+                for (int k = 0; k < 4; k++) {
+                    const int j = f.lookup(P.inst, P.level, 2 * (P.gx >> 1) + (k & 1), 2 * (P.gy >> 1) + (k >> 1));
+                    if (j < 0 || mark[j] >= 0) all = false;
+                }
+                if (all) adapted[P.inst] = 1;
+            }
+        }
+        for (int i = 0; i < nf.np(); i++)
+            if (!adapted[nf.p[i].inst]) keep.push_back(i);
+    }
     // repopulation ops (cb_fclaw2d_regrid_repopulate)
     std::vector<RepopOp> ops(nf.np());
     std::vector<double> naux((size_t)nf.np() * d.naux(), 0.0);
@@ -904,21 +987,21 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
         const PatchInfo& P = nf.p[i];
         RepopOp op{};
         op.dst = i;
-        const int old = f.lookup(P.level, P.gx, P.gy);
+        const int old = f.lookup(P.inst, P.level, P.gx, P.gy);
         if (old >= 0) {
             op.kind = 0; op.src = old;
             if (d.maux > 0) std::memcpy(&naux[(size_t)i * d.naux()], &s->aux_host[(size_t)old * d.naux()], sizeof(double) * d.naux());
         } else {
-            const int parent = f.lookup(P.level - 1, P.gx >> 1, P.gy >> 1);
+            const int parent = f.lookup(P.inst, P.level - 1, P.gx >> 1, P.gy >> 1);
             if (parent >= 0) { op.kind = 1; op.src = parent; op.igrid = (P.gx & 1) + 2 * (P.gy & 1); }
             else {
                 op.kind = 2;
                 for (int c = 0; c < 4; c++) {
-                    op.child[c] = f.lookup(P.level + 1, 2 * P.gx + (c & 1), 2 * P.gy + (c >> 1));
+                    op.child[c] = f.lookup(P.inst, P.level + 1, 2 * P.gx + (c & 1), 2 * P.gy + (c >> 1));
                     if (op.child[c] < 0) return fail(FC2D_B200_EFOREST, "adapt jumped more than one level");
                 }
             }
-            if (d.maux > 0) app_setaux(s->o, d, P, &naux[(size_t)i * d.naux()]);
+            if (d.maux > 0) app_setaux(inst_options(s, P.inst), d, P, &naux[(size_t)i * d.naux()]);
         }
         ops[i] = op;
     }
@@ -939,7 +1022,26 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     invalidate_graph(s);
     rc = upload_desc_and_tables(s);
     if (rc) return rc;
+    if (!keep.empty()) {
+        const size_t nq_all = (size_t)s->forest.np() * d.nq();
+        if (s->snap.cap < nq_all) {
+            std::vector<double> sz(nq_all);
+            CK(s->snap.assign(sz, s->st));
+        }
+        CK(cudaMemcpyAsync(s->snap.p, s->q, sizeof(double) * nq_all, cudaMemcpyDeviceToDevice, s->st));
+        CK(s->keep_dev.assign(keep, s->st));
+    }
+    unsigned char phys_before[64];
+    std::memcpy(phys_before, s->phys_ok, sizeof(phys_before));
     ghost_update(s, s->forest.minlevel_present, s->forest.maxlevel_present, 0);
+    if (!keep.empty()) {
+        launch_restore_patches(d, s->q, s->snap.p, s->keep_dev.p, (int)keep.size(), s->st);
+        // kept instances have their old ghost cells back
+        for (int k : keep) {
+            const int l = s->forest.p[k].level;
+            if (l >= 0 && l < 64) s->phys_ok[l] = s->phys_ok[l] && phys_before[l];
+        }
+    }
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s->st));
     return 0;
@@ -1361,5 +1463,93 @@ extern "C" int fc2d_b200_set_pstar_seed(fc2d_b200_solver_t* s, const fc2d_b200_m
     CK(cudaMemcpyAsync(s->mlp_blob, m->blob, MLP_BLOB_BYTES, cudaMemcpyDeviceToDevice, s->st));
     CK(cudaStreamSynchronize(s->st));
     s->use_mlp = true;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// batches of independent forests
+// ---------------------------------------------------------------------------
+extern "C" int fc2d_b200_set_instances(fc2d_b200_solver_t* s, int n, const fc2d_b200_instance_t* inst)
+{
+    if (!s || n <= 0 || !inst) return fail(FC2D_B200_EINVAL, "bad arguments");
+    if (n > FC2D_B200_MAX_INSTANCES) return fail(FC2D_B200_EINVAL, "too many instances");
+    if (s->initialized) return fail(FC2D_B200_ESTATE, "instances are set before initialize");
+    if (s->o.app == FC2D_B200_APP_SWIRL)
+        return fail(FC2D_B200_EINVAL, "batched instances need a time-independent app (the swirl velocity depends on t)");
+    int span = 0;
+    std::vector<Geometry> G(n);
+    for (int i = 0; i < n; i++) {
+        const fc2d_b200_instance_t& I = inst[i];
+        if (I.minlevel < 0 || I.maxlevel < I.minlevel || I.maxlevel > 20 || I.mi <= 0 || I.mj <= 0)
+            return fail(FC2D_B200_EINVAL, "bad instance levels or brick");
+        span = std::max(span, I.maxlevel - I.minlevel);
+        G[i] = Geometry{s->d, I.mi, I.mj, I.ax, I.bx, I.ay, I.by, I.minlevel};
+    }
+    s->insts.assign(inst, inst + n);
+    s->forest.inst = G;
+    s->forest.g = G[0];
+    s->o.minlevel = 0;
+    s->o.maxlevel = span;
+    s->ncfl = n;
+    invalidate_graph(s);
+    return 0;
+}
+
+extern "C" int fc2d_b200_num_instances(const fc2d_b200_solver_t* s, int* n)
+{
+    if (!s || !n) return fail(FC2D_B200_EINVAL, "null argument");
+    *n = s->forest.ninst();
+    return 0;
+}
+
+extern "C" int fc2d_b200_patch_instance(const fc2d_b200_solver_t* s, int* inst)
+{
+    if (!s || !inst) return fail(FC2D_B200_EINVAL, "null argument");
+    for (int i = 0; i < s->forest.np(); i++) inst[i] = s->forest.p[i].inst;
+    return 0;
+}
+
+extern "C" int fc2d_b200_advance_instances(fc2d_b200_solver_t* s, const double* dt, double* cfl)
+{
+    if (!s || !s->initialized || !dt) return fail(FC2D_B200_EINVAL, "bad arguments");
+    if (s->insts.empty()) return fail(FC2D_B200_ESTATE, "no instances set");
+    const int n = (int)s->insts.size();
+    for (int i = 0; i < n; i++)
+        if (!(dt[i] > 0.0)) return fail(FC2D_B200_EINVAL, "instance time steps must be positive");
+    CK(cudaMemcpyAsync(s->inst_dt_dev, dt, sizeof(double) * n, cudaMemcpyHostToDevice, s->st));
+    // the level time steps 2^-l of a unit coarse step scale each instance's own dt
+    double dummy = 0.0;
+    int rc = fc2d_b200_advance(s, 0.0, 1.0, &dummy);
+    if (rc) return rc;
+    if (cfl) rc = end_cfl(s, nullptr, cfl);
+    return rc;
+}
+
+extern "C" int fc2d_b200_mass_instances(fc2d_b200_solver_t* s, double* out)
+{
+    if (!s || !out || !s->initialized) return fail(FC2D_B200_EINVAL, "bad arguments");
+    const int np = s->forest.np(), meqn = s->d.meqn, ni = s->forest.ninst();
+    if (np * meqn > s->mass_cap) {
+        if (s->mass_dev) cudaFree(s->mass_dev);
+        s->mass_cap = np * meqn + 1024;
+        CK(cudaMalloc(&s->mass_dev, sizeof(double) * (size_t)s->mass_cap));
+    }
+    launch_patch_mass(s->d, s->q, s->desc, np, s->mass_dev, s->st);
+    std::vector<double> pm((size_t)np * meqn);
+    CK(cudaMemcpyAsync(pm.data(), s->mass_dev, sizeof(double) * pm.size(), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    std::vector<double> sum((size_t)ni * meqn, 0.0), comp((size_t)ni * meqn, 0.0);
+    for (int p = 0; p < np; p++) {
+        const int i = s->forest.p[p].inst;
+        for (int m = 0; m < meqn; m++) {
+            double& S = sum[(size_t)i * meqn + m];
+            double& C = comp[(size_t)i * meqn + m];
+            const double y = pm[(size_t)p * meqn + m] - C;
+            const double t = S + y;
+            C = (t - S) - y;
+            S = t;
+        }
+    }
+    for (size_t k = 0; k < sum.size(); k++) out[k] = sum[k];
     return 0;
 }

@@ -42,7 +42,8 @@ static int brick_block(int mi, int mj, int bx, int by)
 // fclaw2d_map_brick.c:68-77).
 void Forest::geometry(PatchInfo& q) const
 {
-    const int l = q.level;
+    const Geometry& g = gi(q.inst);
+    const int l = q.level + g.lbase;
     const int bx = q.gx >> l, by = q.gy >> l;
     const int ix = q.gx - (bx << l), iy = q.gy - (by << l);
     const double w = 1.0 / (double)(1 << l);
@@ -64,10 +65,10 @@ void Forest::geometry(PatchInfo& q) const
     q.morton = interleave((uint32_t)ix << sh, (uint32_t)iy << sh);
 }
 
-int Forest::lookup(int l, int x, int y) const
+int Forest::lookup(int i, int l, int x, int y) const
 {
-    if (l < 0 || !in_domain(l, x, y)) return -1;
-    auto it = index_.find(key(l, x, y));
+    if (l < 0 || !in_domain(i, l, x, y)) return -1;
+    auto it = index_.find(key(i, l, x, y));
     return it == index_.end() ? -1 : it->second;
 }
 
@@ -77,18 +78,20 @@ bool Forest::build(const std::vector<Leaf>& leaves, std::string& err)
     p.reserve(leaves.size());
     for (const Leaf& lf : leaves) {
         PatchInfo q{};
-        q.level = lf.level; q.gx = lf.gx; q.gy = lf.gy;
+        q.level = lf.level; q.gx = lf.gx; q.gy = lf.gy; q.inst = lf.inst;
+        if (q.inst < 0 || q.inst >= ninst()) { err = "leaf of an unknown instance"; return false; }
         geometry(q);
         p.push_back(q);
     }
     std::sort(p.begin(), p.end(), [](const PatchInfo& a, const PatchInfo& b) {
         if (a.level != b.level) return a.level < b.level;
+        if (a.inst != b.inst) return a.inst < b.inst;
         if (a.block != b.block) return a.block < b.block;
         return a.morton < b.morton;
     });
     index_.clear();
     index_.reserve(p.size() * 2);
-    for (int i = 0; i < np(); i++) index_[key(p[i].level, p[i].gx, p[i].gy)] = i;
+    for (int i = 0; i < np(); i++) index_[key(p[i].inst, p[i].level, p[i].gx, p[i].gy)] = i;
     for (int l = 0; l < 34; l++) lev_off[l] = 0;
     minlevel_present = 99; maxlevel_present = -1;
     {
@@ -103,23 +106,23 @@ bool Forest::build(const std::vector<Leaf>& leaves, std::string& err)
     static const int FDX[4] = {-1, 1, 0, 0}, FDY[4] = {0, 0, -1, 1};
     for (int ip = 0; ip < np(); ip++) {
         PatchInfo& P = p[ip];
-        const int l = P.level;
+        const int l = P.level, in = P.inst;
         P.has_fine_nbr = 0; P.on_cf = 0;
         for (int f = 0; f < 4; f++) {
             const int nx = P.gx + FDX[f], ny = P.gy + FDY[f];
             P.face_nbr[f][0] = P.face_nbr[f][1] = -1;
-            P.phys[f] = !in_domain(l, nx, ny);
+            P.phys[f] = !in_domain(in, l, nx, ny);
             if (P.phys[f]) { P.face_type[f] = NB_BOUNDARY; continue; }
-            int k = lookup(l, nx, ny);
+            int k = lookup(in, l, nx, ny);
             if (k >= 0) { P.face_type[f] = NB_SAME; P.face_nbr[f][0] = k; continue; }
-            k = lookup(l - 1, nx >> 1, ny >> 1);
+            k = lookup(in, l - 1, nx >> 1, ny >> 1);
             if (k >= 0) { P.face_type[f] = NB_DOUBLE; P.face_nbr[f][0] = k; P.on_cf = 1; continue; }
             int c0x, c0y, c1x, c1y;
             if (f == 0) { c0x = 2 * nx + 1; c0y = 2 * ny; c1x = c0x; c1y = 2 * ny + 1; }
             else if (f == 1) { c0x = 2 * nx; c0y = 2 * ny; c1x = c0x; c1y = 2 * ny + 1; }
             else if (f == 2) { c0x = 2 * nx; c0y = 2 * ny + 1; c1x = 2 * nx + 1; c1y = c0y; }
             else { c0x = 2 * nx; c0y = 2 * ny; c1x = 2 * nx + 1; c1y = c0y; }
-            const int a = lookup(l + 1, c0x, c0y), b = lookup(l + 1, c1x, c1y);
+            const int a = lookup(in, l + 1, c0x, c0y), b = lookup(in, l + 1, c1x, c1y);
             if (a < 0 || b < 0) { err = "forest is not 2:1 face balanced"; return false; }
             P.face_type[f] = NB_HALF; P.face_nbr[f][0] = a; P.face_nbr[f][1] = b;
             P.has_fine_nbr = 1; P.on_cf = 1;
@@ -130,14 +133,14 @@ bool Forest::build(const std::vector<Leaf>& leaves, std::string& err)
             if (P.phys[f0] || P.phys[f1]) continue;            // not an interior corner
             const int ddx = (c & 1) ? 1 : -1, ddy = (c & 2) ? 1 : -1;
             const int nx = P.gx + ddx, ny = P.gy + ddy;
-            int k = lookup(l, nx, ny);
+            int k = lookup(in, l, nx, ny);
             if (k >= 0) { P.has_corner[c] = 1; P.corner_type[c] = NB_SAME; P.corner_nbr[c] = k; continue; }
-            k = lookup(l + 1, 2 * nx + (ddx < 0), 2 * ny + (ddy < 0));
+            k = lookup(in, l + 1, 2 * nx + (ddx < 0), 2 * ny + (ddy < 0));
             if (k >= 0) {
                 P.has_corner[c] = 1; P.corner_type[c] = NB_HALF; P.corner_nbr[c] = k;
                 P.has_fine_nbr = 1; P.on_cf = 1; continue;
             }
-            k = lookup(l - 1, nx >> 1, ny >> 1);
+            k = lookup(in, l - 1, nx >> 1, ny >> 1);
             const int cx = P.gx + (c & 1), cy = P.gy + (c >> 1);
             if (k >= 0 && (cx % 2) == 0 && (cy % 2) == 0) {   // corner point is a corner of the big leaf
                 P.has_corner[c] = 1; P.corner_type[c] = NB_DOUBLE; P.corner_nbr[c] = k; P.on_cf = 1;
@@ -161,43 +164,42 @@ std::vector<Leaf> adapt_leaves(const Forest& f, const std::vector<int>& mark, in
         if (done[i]) continue;
         const PatchInfo& P = f.p[i];
         if (mark[i] > 0) {
-            for (int c = 0; c < 4; c++) L.push_back({P.level + 1, 2 * P.gx + (c & 1), 2 * P.gy + (c >> 1)});
+            for (int c = 0; c < 4; c++) L.push_back({P.level + 1, 2 * P.gx + (c & 1), 2 * P.gy + (c >> 1), P.inst});
             changed = 1; done[i] = 1;
         } else if (mark[i] < 0) {
             const int px = P.gx >> 1, py = P.gy >> 1, l = P.level;
             int sib[4]; bool ok = true;
             for (int c = 0; c < 4; c++) {
-                sib[c] = f.lookup(l, 2 * px + (c & 1), 2 * py + (c >> 1));
+                sib[c] = f.lookup(P.inst, l, 2 * px + (c & 1), 2 * py + (c >> 1));
                 if (sib[c] < 0 || mark[sib[c]] >= 0) ok = false;
             }
             if (ok) {
-                L.push_back({l - 1, px, py});
+                L.push_back({l - 1, px, py, P.inst});
                 for (int c = 0; c < 4; c++) done[sib[c]] = 1;
                 changed = 1;
             } else {
-                L.push_back({l, P.gx, P.gy}); done[i] = 1;
+                L.push_back({l, P.gx, P.gy, P.inst}); done[i] = 1;
             }
         } else {
-            L.push_back({P.level, P.gx, P.gy}); done[i] = 1;
+            L.push_back({P.level, P.gx, P.gy, P.inst}); done[i] = 1;
         }
     }
     // 2:1 face+corner balance by refining the coarser side
     for (;;) {
         std::unordered_map<uint64_t, int> idx;
         idx.reserve(L.size() * 2);
-        auto key = [](int l, int x, int y) { return ((uint64_t)l << 56) | ((uint64_t)x << 28) | (uint64_t)y; };
-        for (int i = 0; i < (int)L.size(); i++) idx[key(L[i].level, L[i].gx, L[i].gy)] = i;
+        for (int i = 0; i < (int)L.size(); i++) idx[Forest::key(L[i].inst, L[i].level, L[i].gx, L[i].gy)] = i;
         std::vector<char> ref(L.size(), 0);
         bool any = false;
         for (int i = 0; i < (int)L.size(); i++) {
-            const int l = L[i].level;
+            const int l = L[i].level, in = L[i].inst;
             for (int dy = -1; dy <= 1; dy++)
                 for (int dx = -1; dx <= 1; dx++) {
                     if (!dx && !dy) continue;
                     const int x = L[i].gx + dx, y = L[i].gy + dy;
-                    if (!f.in_domain(l, x, y)) continue;
+                    if (!f.in_domain(in, l, x, y)) continue;
                     for (int k = l - 2; k >= 0; k--) {
-                        auto it = idx.find(key(k, x >> (l - k), y >> (l - k)));
+                        auto it = idx.find(Forest::key(in, k, x >> (l - k), y >> (l - k)));
                         if (it != idx.end()) {
                             if (!ref[it->second]) { ref[it->second] = 1; any = true; }
                             break;
@@ -210,14 +212,14 @@ std::vector<Leaf> adapt_leaves(const Forest& f, const std::vector<int>& mark, in
         M.reserve(L.size() + 64);
         for (int i = 0; i < (int)L.size(); i++) {
             if (!ref[i]) { M.push_back(L[i]); continue; }
-            for (int c = 0; c < 4; c++) M.push_back({L[i].level + 1, 2 * L[i].gx + (c & 1), 2 * L[i].gy + (c >> 1)});
+            for (int c = 0; c < 4; c++) M.push_back({L[i].level + 1, 2 * L[i].gx + (c & 1), 2 * L[i].gy + (c >> 1), L[i].inst});
         }
         L.swap(M);
     }
     if (!changed) {
         bool same = ((int)L.size() == np);
         for (size_t i = 0; same && i < L.size(); i++)
-            if (f.lookup(L[i].level, L[i].gx, L[i].gy) < 0) same = false;
+            if (f.lookup(L[i].inst, L[i].level, L[i].gx, L[i].gy) < 0) same = false;
         if (!same) changed = 1;
     }
     (void)err;

@@ -16,10 +16,13 @@ namespace fcb {
 
 enum { NB_BOUNDARY = 0, NB_HALF = 1, NB_SAME = 2, NB_DOUBLE = 3 };
 
-struct Leaf { int level, gx, gy; };
+// level: forest level (the instance's refinement level minus its lbase); gx, gy:
+// integer patch coordinates over the instance's brick at its refinement level.
+struct Leaf { int level, gx, gy; int inst = 0; };
 
 struct PatchInfo {
     int level, gx, gy, block;
+    int inst;
     uint64_t morton;
     double xlower, ylower, dx, dy;
     int face_type[4];
@@ -33,25 +36,39 @@ struct Geometry {
     Dims d;
     int mi, mj;
     double ax, bx, ay, by;
+    int lbase = 0;    // refinement level of forest level 0 (an instance's minlevel in a batch)
 };
 
 class Forest {
 public:
-    Geometry g;
-    std::vector<PatchInfo> p;        // slot order: level-major, then block, then Morton
+    Geometry g;                      // the single domain, or instance 0
+    std::vector<Geometry> inst;      // per-instance domains of a batch (empty: one domain, g)
+    std::vector<PatchInfo> p;        // slot order: level-major, then instance, block, Morton
     int lev_off[34];                 // patches of level l: [lev_off[l], lev_off[l+1])
     int minlevel_present = 0, maxlevel_present = -1;
 
     // Install leaves (any order).  Returns false (and sets err) if not 2:1 balanced.
     bool build(const std::vector<Leaf>& leaves, std::string& err);
-    int lookup(int l, int x, int y) const;
+    int lookup(int l, int x, int y) const { return lookup(0, l, x, y); }
+    int lookup(int i, int l, int x, int y) const;
     int np() const { return (int)p.size(); }
-    bool in_domain(int l, int x, int y) const { return x >= 0 && y >= 0 && x < (g.mi << l) && y < (g.mj << l); }
+    int ninst() const { return inst.empty() ? 1 : (int)inst.size(); }
+    const Geometry& gi(int i) const { return inst.empty() ? g : inst[i]; }
+    bool in_domain(int l, int x, int y) const { return in_domain(0, l, x, y); }
+    bool in_domain(int i, int l, int x, int y) const
+    {
+        const Geometry& G = gi(i);
+        const int la = l + G.lbase;
+        return l >= 0 && x >= 0 && y >= 0 && x < (G.mi << la) && y < (G.mj << la);
+    }
     void geometry(PatchInfo& q) const;
+    static uint64_t key(int i, int l, int x, int y)
+    {
+        return ((uint64_t)i << 56) | ((uint64_t)l << 50) | ((uint64_t)x << 25) | (uint64_t)y;
+    }
 
 private:
     std::unordered_map<uint64_t, int> index_;
-    static uint64_t key(int l, int x, int y) { return ((uint64_t)l << 56) | ((uint64_t)x << 28) | (uint64_t)y; }
 };
 
 // Refine marked leaves, coarsen fully marked families, then 2:1 balance

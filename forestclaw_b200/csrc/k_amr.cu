@@ -421,6 +421,18 @@ __global__ void k_repop(const RepopOp* __restrict__ ops, int mx, int my, int mbc
 // ---------------------------------------------------------------------------
 // launch wrappers
 // ---------------------------------------------------------------------------
+// Whole-patch copies src -> dst of the listed slots (restores ghost cells).
+__global__ void k_restore_patches(double* __restrict__ dst, const double* __restrict__ src, const int* __restrict__ slots,
+                                  int nq)
+{
+    const size_t base = (size_t)slots[blockIdx.x] * nq;
+    for (int k = threadIdx.x; k < nq; k += blockDim.x) dst[base + k] = src[base + k];
+}
+void launch_restore_patches(const Dims& d, double* dst, const double* src, const int* slots, int n, cudaStream_t st)
+{
+    if (n > 0) k_restore_patches<<<n, 256, 0, st>>>(dst, src, slots, d.nq());
+}
+
 void launch_copy(const Dims& d, double* dst, const double* src, const CopyEnt* e, int n, cudaStream_t st)
 {
     if (n > 0) k_copy<<<nblk(n, 256), 256, 0, st>>>(dst, src, e, n, d.nxy(), d.meqn);

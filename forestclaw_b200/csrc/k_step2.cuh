@@ -136,7 +136,7 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
     if (RP::EXACT64 && tid < 32) nhist[tid] = 0u;
     const PatchDesc pd = desc[p];
     const double dx = pd.dx, dy = pd.dy;
-    const double dt = sp.dt;
+    const double dt = sp.inst_dt ? sp.dt * sp.inst_dt[pd.inst] : sp.dt;
     const double dtdx = dt / dx, dtdy = dt / dy;
     double* qg = q + (size_t)p * MEQN * NXY;
     // save_current_step: only the data time interpolation will read (coarser
@@ -209,6 +209,15 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
 
     double cflmax = 0.0;
     TW cflw = TW(0);
+
+    // Reflecting walls of this patch (FP32-wave path).  Mirror symmetry makes the
+    // mass flux through a wall exactly zero -- first-order part, second-order
+    // correction and the transverse terms of the two rows (columns) beside it
+    // cancel -- but FP32 waves only reproduce that cancellation to FP32 rounding,
+    // which leaks about 1e-8 of the mass per step.  The FP32-wave path therefore
+    // takes the exact value, zero, for the mass component (m = 0) at these faces;
+    // the FP64 path keeps the reference's arithmetic.
+    const int wallf = (F32 && RP::CONS_FLUX) ? (pd.phys_mask & sp.wall_faces) : 0;
 
     // g64: FP64 amdq, apdq of exact solvers (kept for the Godunov update)
     struct State { TW wave[MWAVES][MEQN]; TW s[MWAVES]; TW am[MEQN]; TW ap[MEQN]; TW ex[NEXTRA];
@@ -291,6 +300,9 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
                                 double* faddm, double* faddp) {
         TW cq[MEQN];
         for (int m = 0; m < MEQN; m++) { cq[m] = TW(0); faddm[m] = 0.0; faddp[m] = 0.0; }
+        // wall_lo: ghost on the left (low face), wall_hi: ghost on the right (high face)
+        const bool wall_lo = wallf && pos == lim_lo && (wallf & (ixy == 1 ? 1 : 4));
+        const bool wall_hi = wallf && pos == lim_hi && (wallf & (ixy == 1 ? 2 : 8));
         if (god) {
             if constexpr (RP::EXACT64) {
                 for (int m = 0; m < MEQN; m++) { faddp[m] = faddp[m] - st.g64[MEQN + m]; faddm[m] = faddm[m] + st.g64[m]; }
@@ -304,6 +316,9 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
                 }
                 for (int a = 0; a < MAUX; a++) { aL[a] = As[a * NXY + cL]; aR[a] = As[a * NXY + cR]; }
                 RP::godunov64(ixy, qL, qR, aL, aR, fL, fR, st.ap, am64, ap64, sp.grav);
+                // zero mass flux through a wall: the interior cell's fluctuation cancels its own flux
+                if (wall_lo) { ap64[0] = fR[0]; am64[0] = (fR[0] - fL[0]) - fR[0]; }
+                if (wall_hi) { am64[0] = 0.0 - fL[0]; ap64[0] = (fR[0] - fL[0]) + fL[0]; }
                 for (int m = 0; m < MEQN; m++) { faddp[m] = faddp[m] - ap64[m]; faddm[m] = faddm[m] + am64[m]; }
             } else {
                 for (int m = 0; m < MEQN; m++) { faddp[m] = faddp[m] - (double)st.ap[m]; faddm[m] = faddm[m] + (double)st.am[m]; }
@@ -343,6 +358,7 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
                             c = add_rn(c, mul_rn(mul_rn(sa, sub_rn(TW(1), mul_rn(sa, dave))), st.wave[mw][m]));
                         }
                     }
+                    if (m == 0 && (wall_lo || wall_hi)) c = TW(0);
                     cq[m] = c;
                     if (F32) {
                         const double h = 0.5 * (double)c;
@@ -495,6 +511,7 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
                 { const int kk = (r - 1) * (NX - 1) + ic - 1; if (tflag[kk]) v = v - (double)Tt[(2 * MEQN + m) * NI + kk]; }
                 g = g + v;
             }
+            if (m == 0 && ((jc == MBC && (wallf & 4)) || (jc == MY + MBC && (wallf & 8)))) g = 0.0;
             GMs[m * NXY + c] = g;
             GPs[m * NXY + c] = g;
         }
@@ -503,7 +520,9 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
     auto y3 = [&](int c) {
         const int jc = c / NX, ic = c % NX;
         if (jc < 1) return;
+        const bool wall_edge = (ic == MBC && (wallf & 1)) || (ic == MX + MBC && (wallf & 2));
         for (int m = 0; m < MEQN; m++) {
+            if (m == 0 && wall_edge) continue;
             double fm = FMs[m * NXY + c], fp = FPs[m * NXY + c];
             if (ic - 1 >= 1 && ic - 1 <= NX - 2) {
                 const int col = ic - 1;
@@ -608,7 +627,7 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
         if (tid == 0) {
             unsigned long long bits = (unsigned long long)__double_as_longlong(v);
             if (v != v) bits = 0x7ff8000000000000ull;   // NaN (e.g. negative depth) wins the max
-            atomicMax(cfl_bits, bits);
+            atomicMax(cfl_bits + pd.inst, bits);
         }
     }
     if constexpr (RP::EXACT64) {

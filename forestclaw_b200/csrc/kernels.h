@@ -28,6 +28,7 @@ struct InterpEnt { int dst, src, sub, pad; };      // sub = child position 0..3 
 struct PhysEnt { int dst, src, neg, cst; };        // neg: bit m set => negate field m; cst: constant state
 
 void launch_copy(const Dims& d, double* dst, const double* src, const CopyEnt* e, int n, cudaStream_t st);
+void launch_restore_patches(const Dims& d, double* dst, const double* src, const int* slots, int n, cudaStream_t st);
 void launch_average(const Dims& d, double* dst, const double* src, const CopyEnt* e, int n, cudaStream_t st);
 void launch_interp(const Dims& d, double* dst, const double* src, const InterpEnt* e, int n, cudaStream_t st);
 void launch_phys(const Dims& d, double* q, const PhysEnt* e, int n, const double* bcstate, cudaStream_t st);

@@ -55,3 +55,63 @@ def swirl_dt(mx: int, level: int) -> float:
     u = np.abs((psi(X, Y + dx) - p0) / dx)
     v = np.abs((psi(X + dx, Y) - p0) / dx)
     return 0.9 * dx / float(max(u.max(), v.max()))
+
+
+class _Xoshiro256ss:
+    """xoshiro256** (Blackman and Vigna, 2018) seeded by SplitMix64: a small portable
+    generator so that batch workloads are the same on every machine."""
+
+    M = (1 << 64) - 1
+
+    def __init__(self, seed: int):
+        x = seed & self.M
+        self.s = []
+        for _ in range(4):
+            x = (x + 0x9E3779B97F4A7C15) & self.M
+            z = x
+            z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & self.M
+            z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & self.M
+            self.s.append(z ^ (z >> 31))
+
+    @staticmethod
+    def _rotl(v: int, k: int) -> int:
+        return ((v << k) | (v >> (64 - k))) & _Xoshiro256ss.M
+
+    def next(self) -> int:
+        s = self.s
+        r = (self._rotl((s[1] * 5) & self.M, 7) * 9) & self.M
+        t = (s[1] << 17) & self.M
+        s[2] ^= s[0]
+        s[3] ^= s[1]
+        s[1] ^= s[2]
+        s[0] ^= s[3]
+        s[2] ^= t
+        s[3] = self._rotl(s[3], 45)
+        return r
+
+    def uniform(self, a: float, b: float) -> float:
+        return a + (b - a) * ((self.next() >> 11) * (1.0 / (1 << 53)))
+
+    def choice(self, seq):
+        return seq[self.next() % len(seq)]
+
+
+def tsunami_instances(n: int = 64, base_seed: int = 0, mx: int | None = None):
+    """n independent tsunami forests for a batch: instance k draws from its own
+    generator (seed base_seed + k) minlevel in {2, 3, 4}, maxlevel in minlevel+1..8
+    (at most 5..8), the bathymetry centre in [-0.5, 0.5]^2 and 1 to 3 Gaussian
+    humps of amplitude U[0.05, 0.3], width U[0.05, 0.2] and centre in [-1, 1]^2.
+    Returns (instances, patch sizes): the patch size alternates 8, 16 unless mx is given."""
+    out, sizes = [], []
+    for k in range(n):
+        g = _Xoshiro256ss(base_seed + k)
+        lo = g.choice((2, 3, 4))
+        hi = g.choice(tuple(range(max(lo + 1, 5), 9)))
+        cx, cy = g.uniform(-0.5, 0.5), g.uniform(-0.5, 0.5)
+        nb = g.choice((1, 2, 3))
+        pd = [cx, cy, float(nb)]
+        for _ in range(nb):
+            pd += [g.uniform(0.05, 0.3), g.uniform(0.05, 0.2), g.uniform(-1.0, 1.0), g.uniform(-1.0, 1.0)]
+        out.append(dict(minlevel=lo, maxlevel=hi, ax=-1.0, bx=1.0, ay=-1.0, by=1.0, mi=1, mj=1, pdata=tuple(pd)))
+        sizes.append(mx if mx is not None else (8 if k % 2 == 0 else 16))
+    return out, sizes

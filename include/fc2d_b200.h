@@ -141,6 +141,29 @@ int fc2d_b200_advance(fc2d_b200_solver_t* s, double t, double dt, double* maxcfl
  * device repopulation, ghost update.  *changed = 1 if the forest changed. */
 int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed);
 
+/* ---- batches of independent forests (instances; no counterpart in the reference) ----
+ * One solver can hold up to FC2D_B200_MAX_INSTANCES independent forests with the
+ * same patch size, meqn and solver: every level-step launch then covers the
+ * patches of all instances.  Each instance has its own brick, levels, app
+ * parameters (pdata) and time step; its patches are numbered by levels relative
+ * to its own minlevel, so every instance takes the same subcycled steps as it
+ * would alone.  Set before fc2d_b200_initialize; the app must not depend on t. */
+#define FC2D_B200_MAX_INSTANCES 256
+typedef struct fc2d_b200_instance {
+    int minlevel, maxlevel;
+    double ax, bx, ay, by;
+    int mi, mj;
+    double pdata[32];
+} fc2d_b200_instance_t;
+int fc2d_b200_set_instances(fc2d_b200_solver_t* s, int n, const fc2d_b200_instance_t* inst);
+int fc2d_b200_num_instances(const fc2d_b200_solver_t* s, int* n);
+/* Instance of each patch (level-major order; patch_info reports absolute levels). */
+int fc2d_b200_patch_instance(const fc2d_b200_solver_t* s, int* inst);
+/* One coarse step of every instance, instance i with its own dt[i]; cfl[i] = its CFL. */
+int fc2d_b200_advance_instances(fc2d_b200_solver_t* s, const double* dt, double* cfl);
+/* Kahan-summed mass per instance and field: out[i * meqn + m]. */
+int fc2d_b200_mass_instances(fc2d_b200_solver_t* s, double* out);
+
 /* Kahan-summed mass per field over interior cells, FP64
  * (fclaw2d_clawpatch46_diagnostics.f:13-55). */
 int fc2d_b200_mass(fc2d_b200_solver_t* s, double* out);
