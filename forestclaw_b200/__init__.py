@@ -191,6 +191,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_patch_instance": [P, ip],
         "fc2d_b200_advance_instances": [P, dp, dp],
         "fc2d_b200_mass_instances": [P, dp],
+        "fc2d_b200_num_variants": [P, ip, ip],
+        "fc2d_b200_variant_info": [P, I, ip, ip, ip, ip],
+        "fc2d_b200_set_variant": [P, I],
+        "fc2d_b200_autotune": [P, I, ip, dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -426,6 +430,36 @@ class Solver:
         out = (ctypes.c_ulonglong * 32)()
         self._check("fc2d_b200_newton_histogram", self.lib.fc2d_b200_newton_histogram(self.h, out, int(reset)))
         return np.array(out[:], np.int64)
+
+    # -- patch-to-CTA variants and the autotuner -------------------------------
+    def variants(self) -> list:
+        """Compiled patch-to-CTA variants of this solver's shape (0 = default)."""
+        n, cur = ctypes.c_int(), ctypes.c_int()
+        self._check("fc2d_b200_num_variants", self.lib.fc2d_b200_num_variants(self.h, ctypes.byref(n), ctypes.byref(cur)))
+        out = []
+        for v in range(n.value):
+            a = [ctypes.c_int() for _ in range(4)]
+            self._check("fc2d_b200_variant_info", self.lib.fc2d_b200_variant_info(self.h, v, *[ctypes.byref(x) for x in a]))
+            out.append(dict(threads=a[0].value, min_blocks=a[1].value, reg=a[2].value, smem=a[3].value))
+        return out
+
+    @property
+    def variant(self) -> int:
+        n, cur = ctypes.c_int(), ctypes.c_int()
+        self._check("fc2d_b200_num_variants", self.lib.fc2d_b200_num_variants(self.h, ctypes.byref(n), ctypes.byref(cur)))
+        return cur.value
+
+    def set_variant(self, v: int) -> None:
+        self._check("fc2d_b200_set_variant", self.lib.fc2d_b200_set_variant(self.h, v))
+
+    def autotune(self, reps: int = 3):
+        """Time every variant on the current forest (q unchanged), keep the fastest.
+        Returns (best variant, ms per pass over all levels for each variant)."""
+        n = len(self.variants())
+        ms = np.zeros(n, np.float64)
+        best = ctypes.c_int()
+        self._check("fc2d_b200_autotune", self.lib.fc2d_b200_autotune(self.h, reps, ctypes.byref(best), _dp(ms)))
+        return best.value, ms
 
     # -- batches of independent forests ---------------------------------------
     def set_instances(self, instances) -> None:

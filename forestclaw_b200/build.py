@@ -27,11 +27,15 @@ GXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_UNITS = {
-    "k_step2_f64.cu": ["-fmad=false"],
+    "k_step2_f64_adv.cu": ["-fmad=false"],
+    "k_step2_f64_sw.cu": ["-fmad=false"],
+    "k_step2_f64_euler.cu": ["-fmad=false"],
     "k_amr.cu": ["-fmad=false"],
     "k_mass_noalloc.cu": ["-fmad=false"],
     "k_mlp.cu": [],
-    "k_step2_f32w.cu": ["--use_fast_math"],
+    "k_step2_f32w_adv.cu": ["--use_fast_math"],
+    "k_step2_f32w_sw.cu": ["--use_fast_math"],
+    "k_step2_f32w_euler.cu": ["--use_fast_math"],
 }
 CPP_UNITS = ["host_forest.cpp", "host_api.cpp", "apps.cpp"]
 
@@ -65,22 +69,24 @@ def build(force: bool = False, verbose: bool = False) -> str:
         with open(stamp) as f:
             if f.read().strip() == digest:
                 return OUT
-    objs = []
     common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", CSRC, "-I", INC, "-lineinfo"]
+    jobs = []   # (object, command): the units compile in parallel
     for cu, extra in CU_UNITS.items():
         obj = os.path.join(BUILD, cu + ".o")
-        cmd = [NVCC, *ARCH, *common, *extra, "-Xptxas", "-v" if verbose else "-O3", "-c",
-               os.path.join(CSRC, cu), "-o", obj]
-        r = _run(cmd)
-        if verbose:
-            sys.stderr.write(r.stderr)
-        objs.append(obj)
+        jobs.append((obj, [NVCC, *ARCH, *common, *extra, "-Xptxas", "-v" if verbose else "-O3", "-c",
+                           os.path.join(CSRC, cu), "-o", obj]))
     for cpp in CPP_UNITS:
         obj = os.path.join(BUILD, cpp + ".o")
-        cmd = [GXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
-               "-I", CSRC, "-I", INC, "-I", os.path.join(CUDA, "include"), "-c", os.path.join(CSRC, cpp), "-o", obj]
-        _run(cmd)
-        objs.append(obj)
+        jobs.append((obj, [GXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
+                           "-I", CSRC, "-I", INC, "-I", os.path.join(CUDA, "include"), "-c",
+                           os.path.join(CSRC, cpp), "-o", obj]))
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(lambda j: _run(j[1]), jobs))
+    if verbose:
+        for r in results:
+            sys.stderr.write(r.stderr)
+    objs = [j[0] for j in jobs]
     _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-Xcompiler", "-fPIC", "-o", OUT, *objs])
     with open(stamp, "w") as f:
         f.write(digest)

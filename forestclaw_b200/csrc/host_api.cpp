@@ -22,18 +22,24 @@
 #include "host_forest.hpp"
 #include "kernels.h"
 
-namespace fcb {
-cudaError_t launch_step2_f64(int rp, const Dims& d, double* q, double* qlast, const double* aux, double* regs,
-                             const PatchDesc* desc, int p0, int npatch, const StepParams* sp,
-                             unsigned long long* cfl_bits, cudaStream_t st);
-bool step2_f64_supported(int rp, int mx, int my, int mbc);
-cudaError_t launch_step2_f32w(int rp, const Dims& d, double* q, double* qlast, const double* aux, double* regs,
-                              const PatchDesc* desc, int p0, int npatch, const StepParams* sp,
-                              unsigned long long* cfl_bits, cudaStream_t st);
-bool step2_f32w_supported(int rp, int mx, int my, int mbc);
-}  // namespace fcb
-
 using namespace fcb;
+
+// Patch-to-CTA variants of the fused update compiled for one solver shape (first: default).
+static std::vector<const Step2Variant*> step2_variants(int precision, int rp, int mx, int my, int mbc)
+{
+    using Table = const Step2Variant* (*)(int*);
+    static const Table tables[] = {step2_table_f64_adv, step2_table_f64_sw, step2_table_f64_euler,
+                                   step2_table_f32w_adv, step2_table_f32w_sw, step2_table_f32w_euler};
+    std::vector<const Step2Variant*> out;
+    for (Table t : tables) {
+        int n = 0;
+        const Step2Variant* v = t(&n);
+        for (int i = 0; i < n; i++)
+            if (v[i].precision == precision && v[i].rp == rp && v[i].mx == mx && v[i].my == my && v[i].mbc == mbc)
+                out.push_back(&v[i]);
+    }
+    return out;
+}
 
 static thread_local std::string g_err;
 static int fail(int code, const std::string& msg) { g_err = msg; return code; }
@@ -95,6 +101,9 @@ struct fc2d_b200_solver {
     // fills no ghost cells there by default (init_ghostcell = 0,
     // src/fclaw2d_initialize.c:140), so the first step sees qinit's ghost values.
     unsigned char phys_ok[64] = {};
+    std::vector<const Step2Variant*> vars;         // compiled patch-to-CTA variants of this shape
+    int var = 0;                                   // the one in use
+    StepParams* tune_params = nullptr;             // autotuner: dt = 0 parameters (device)
     DevVec<RepopOp> repop_dev;                     // regrid repopulation ops
     DevVec<double> snap;                           // batch regrid: q of instances whose forest is unchanged
     DevVec<int> keep_dev;
@@ -272,18 +281,11 @@ static cudaEvent_t next_event(fc2d_b200_solver* s)
 // ---------------------------------------------------------------------------
 // level operations
 // ---------------------------------------------------------------------------
-static int update_level(fc2d_b200_solver* s, int level, double t, double dt)
+// Launch parameters of one level update.
+static StepParams make_params(const fc2d_b200_solver* s, int level, double t, double dt)
 {
     const Forest& f = s->forest;
-    if (level < 0 || level > 32) return 0;
-    const int p0 = f.lev_off[level], np = f.lev_off[level + 1] - p0;
-    if (np <= 0) return 0;
-    if (s->n_upd >= fc2d_b200_solver::PCAP) return fail(FC2D_B200_EINVAL, "too many level updates in one advance");
-    const StepParams* spd = s->params_dev + s->n_upd;
-    StepParams& sp = s->params_host[s->n_upd];
-    s->n_upd++;
-    if (!s->fill) goto launch;
-    sp = StepParams{};
+    StepParams sp{};
     sp.order1 = s->o.order[0]; sp.order2 = s->o.order[1];
     for (int k = 0; k < 8; k++) sp.mthlim[k] = s->o.mthlim[k];
     sp.mcapa = s->o.mcapa;
@@ -309,6 +311,21 @@ static int update_level(fc2d_b200_solver* s, int level, double t, double dt)
         const double pi = 4.0 * std::atan(1.0), pi2 = 2.0 * pi;
         sp.vt = std::cos(pi2 * (t + dt / 2.0) / s->o.tperiod);
     }
+    return sp;
+}
+
+static int update_level(fc2d_b200_solver* s, int level, double t, double dt)
+{
+    const Forest& f = s->forest;
+    if (level < 0 || level > 32) return 0;
+    const int p0 = f.lev_off[level], np = f.lev_off[level + 1] - p0;
+    if (np <= 0) return 0;
+    if (s->n_upd >= fc2d_b200_solver::PCAP) return fail(FC2D_B200_EINVAL, "too many level updates in one advance");
+    const StepParams* spd = s->params_dev + s->n_upd;
+    StepParams& sp = s->params_host[s->n_upd];
+    s->n_upd++;
+    if (!s->fill) goto launch;
+    sp = make_params(s, level, t, dt);
     s->cell_updates += (double)np * s->d.mx * s->d.my;
     s->upd_launches++;
     s->total_launches++;
@@ -317,11 +334,7 @@ launch:
     if (!s->emit) return 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (s->timing) { e0 = next_event(s); e1 = next_event(s); CK(cudaEventRecord(e0, s->st)); }
-    cudaError_t e;
-    if (s->o.precision == FC2D_B200_PREC_FP32WAVE)
-        e = launch_step2_f32w(s->o.rp, s->d, s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, spd, s->cfl_dev, s->st);
-    else
-        e = launch_step2_f64(s->o.rp, s->d, s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, spd, s->cfl_dev, s->st);
+    cudaError_t e = s->vars[s->var]->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, spd, s->cfl_dev, s->st);
     if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("step2 launch: ") + cudaGetErrorString(e));
     if (s->timing) {
         CK(cudaEventRecord(e1, s->st));
@@ -488,8 +501,7 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
         return fail(FC2D_B200_EINVAL, "exact Euler solver needs meqn 4, mwaves 3, gamma > 1, newton_tol > 0");
     if (o.minlevel < 0 || o.maxlevel < o.minlevel || o.maxlevel > 20)
         return fail(FC2D_B200_EINVAL, "bad minlevel/maxlevel");
-    const bool sup = (o.precision == FC2D_B200_PREC_FP32WAVE) ? step2_f32w_supported(o.rp, o.mx, o.my, o.mbc)
-                                                              : step2_f64_supported(o.rp, o.mx, o.my, o.mbc);
+    const bool sup = !step2_variants(o.precision, o.rp, o.mx, o.my, o.mbc).empty();
     if (!sup) return fail(FC2D_B200_EINVAL, "no compiled update kernel for this (rp, mx, my, mbc, precision)");
     int ndev = 0;
     CK(cudaGetDeviceCount(&ndev));
@@ -516,10 +528,11 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
     }
     CK(cudaMallocHost(&s->params_host, sizeof(StepParams) * fc2d_b200_solver::PCAP));
     {   // set the kernel's shared-memory attribute outside any stream capture
-        cudaError_t e = (o.precision == FC2D_B200_PREC_FP32WAVE)
-            ? launch_step2_f32w(o.rp, s->d, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st)
-            : launch_step2_f64(o.rp, s->d, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st);
+        s->vars = step2_variants(o.precision, o.rp, o.mx, o.my, o.mbc);
+        s->var = 0;
+        cudaError_t e = s->vars[0]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st);
         if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
+        CK(cudaMalloc(&s->tune_params, sizeof(StepParams)));
     }
     *out = s.release();
     return 0;
@@ -539,6 +552,7 @@ extern "C" int fc2d_b200_destroy(fc2d_b200_solver_t* s)
     cudaFree(s->params_dev); cudaFreeHost(s->params_host);
     if (s->mass_dev) cudaFree(s->mass_dev);
     cudaFree(s->bc_dev); cudaFree(s->newton_hist);
+    if (s->tune_params) cudaFree(s->tune_params);
     if (s->mlp_blob) cudaFree(s->mlp_blob);
     cudaStreamDestroy(s->st);
     delete s;
@@ -548,14 +562,13 @@ extern "C" int fc2d_b200_destroy(fc2d_b200_solver_t* s)
 extern "C" int fc2d_b200_set_riemann(fc2d_b200_solver_t* s, int rp_id)
 {
     if (!s) return fail(FC2D_B200_EINVAL, "null solver");
-    const bool sup = (s->o.precision == FC2D_B200_PREC_FP32WAVE) ? step2_f32w_supported(rp_id, s->o.mx, s->o.my, s->o.mbc)
-                                                                 : step2_f64_supported(rp_id, s->o.mx, s->o.my, s->o.mbc);
-    if (!sup) return fail(FC2D_B200_EINVAL, "Riemann solver id not compiled for these patch dimensions");
+    std::vector<const Step2Variant*> vars = step2_variants(s->o.precision, rp_id, s->o.mx, s->o.my, s->o.mbc);
+    if (vars.empty()) return fail(FC2D_B200_EINVAL, "Riemann solver id not compiled for these patch dimensions");
     s->o.rp = rp_id;
+    s->vars = vars;
+    s->var = 0;
     invalidate_graph(s);
-    cudaError_t e = (s->o.precision == FC2D_B200_PREC_FP32WAVE)
-        ? launch_step2_f32w(rp_id, s->d, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st)
-        : launch_step2_f64(rp_id, s->d, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st);
+    cudaError_t e = s->vars[0]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st);
     if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
     return 0;
 }
@@ -1551,5 +1564,87 @@ extern "C" int fc2d_b200_mass_instances(fc2d_b200_solver_t* s, double* out)
         }
     }
     for (size_t k = 0; k < sum.size(); k++) out[k] = sum[k];
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// patch-to-CTA variants and the autotuner
+// ---------------------------------------------------------------------------
+extern "C" int fc2d_b200_num_variants(const fc2d_b200_solver_t* s, int* n, int* current)
+{
+    if (!s || !n) return fail(FC2D_B200_EINVAL, "null argument");
+    *n = (int)s->vars.size();
+    if (current) *current = s->var;
+    return 0;
+}
+
+extern "C" int fc2d_b200_variant_info(const fc2d_b200_solver_t* s, int v, int* threads, int* min_blocks, int* reg,
+                                      int* smem_bytes)
+{
+    if (!s || v < 0 || v >= (int)s->vars.size()) return fail(FC2D_B200_EINVAL, "no such variant");
+    const Step2Variant* x = s->vars[v];
+    if (threads) *threads = x->threads;
+    if (min_blocks) *min_blocks = x->min_blocks;
+    if (reg) *reg = x->reg;
+    if (smem_bytes) *smem_bytes = x->smem;
+    return 0;
+}
+
+extern "C" int fc2d_b200_set_variant(fc2d_b200_solver_t* s, int v)
+{
+    if (!s || v < 0 || v >= (int)s->vars.size()) return fail(FC2D_B200_EINVAL, "no such variant");
+    cudaError_t e = s->vars[v]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st);
+    if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
+    s->var = v;
+    invalidate_graph(s);
+    return 0;
+}
+
+// Time every variant on the current forest -- one launch per level, as a
+// subcycled step issues them -- and keep the fastest.  The timed launches run
+// with dt = 0 and neither store fluxes, accumulate waves, save q nor count
+// Newton iterations, so they do all of the update's arithmetic but leave q,
+// the registers and the statistics as they were.
+extern "C" int fc2d_b200_autotune(fc2d_b200_solver_t* s, int reps, int* best_out, double* ms_out)
+{
+    if (!s || !s->initialized || reps < 1) return fail(FC2D_B200_EINVAL, "bad arguments");
+    const Forest& f = s->forest;
+    StepParams sp = make_params(s, f.maxlevel_present, s->t_curr, 0.0);
+    sp.store_flux = 0; sp.accumulate_waves = 0; sp.save_last = 0; sp.newton_hist = nullptr;
+    CK(cudaMemcpyAsync(s->tune_params, &sp, sizeof(StepParams), cudaMemcpyHostToDevice, s->st));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto pass = [&](const Step2Variant* v) -> cudaError_t {
+        for (int l = 0; l <= 32; l++) {
+            const int p0 = f.lev_off[l], np = f.lev_off[l + 1] - p0;
+            if (np <= 0) continue;
+            cudaError_t e = v->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, s->tune_params, s->cfl_dev, s->st);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    };
+    int best = s->var;
+    double best_ms = 1e300;
+    cudaError_t err = cudaSuccess;
+    for (int v = 0; v < (int)s->vars.size() && err == cudaSuccess; v++) {
+        err = s->vars[v]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st);
+        if (err == cudaSuccess) err = pass(s->vars[v]);             // warm-up
+        if (err == cudaSuccess) err = cudaEventRecord(e0, s->st);
+        for (int r = 0; r < reps && err == cudaSuccess; r++) err = pass(s->vars[v]);
+        if (err == cudaSuccess) err = cudaEventRecord(e1, s->st);
+        if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+        const double per = (double)ms / reps;
+        if (ms_out) ms_out[v] = per;
+        if (err == cudaSuccess && per < best_ms) { best_ms = per; best = v; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (err != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("autotune: ") + cudaGetErrorString(err));
+    s->var = best;
+    invalidate_graph(s);
+    if (best_out) *best_out = best;
     return 0;
 }

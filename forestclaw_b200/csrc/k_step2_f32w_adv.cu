@@ -1,0 +1,23 @@
+// k_step2_f32w_adv.cu -- FP32-wave instantiations (built with --use_fast_math; FP64 accumulation)
+// of the fused update for scalar advection: the patch-to-CTA variants of each patch size.
+#include "k_step2_variant.cuh"
+#include "fc2d_b200.h"
+
+namespace fcb {
+
+const Step2Variant* step2_table_f32w_adv(int* n)
+{
+    static const Step2Variant table[] = {
+        FCB_STEP2_VARIANT(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_ADVECTION, RPAdvection, 32, false, 512, 2, float),
+        FCB_STEP2_VARIANT(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_ADVECTION, RPAdvection, 32, false, 256, 2, float),
+        FCB_STEP2_VARIANT(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_ADVECTION, RPAdvection, 32, false, 256, 4, float),
+        FCB_STEP2_VARIANT(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_ADVECTION, RPAdvection, 32, false, 1024, 1, float),
+        FCB_STEP2_VARIANT(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_ADVECTION, RPAdvection, 16, false, 416, 2, float),
+        FCB_STEP2_VARIANT(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_ADVECTION, RPAdvection, 16, false, 352, 2, float),
+        FCB_STEP2_VARIANT(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_ADVECTION, RPAdvection, 16, false, 256, 3, float),
+    };
+    *n = (int)(sizeof(table) / sizeof(table[0]));
+    return table;
+}
+
+}  // namespace fcb

@@ -1,0 +1,41 @@
+// k_step2_variant.cuh -- launchers of the fused update, one per patch-to-CTA mapping.
+//
+// A variant fixes how one patch maps onto its CTA: NT threads and a
+// __launch_bounds__ occupancy target of MINB CTAs per SM (which caps the
+// registers per thread).  With NT >= the interfaces of a sweep every interface
+// has its own thread and its normal solve stays in registers (REG); with fewer
+// threads the CTA strides over the interfaces and keeps the per-interface record
+// in shared memory.  The arithmetic of every interface and the order of all
+// accumulations are the same in every variant, so the FP64 variants give
+// identical bits; the autotuner (host side) picks the fastest for a forest.
+#pragma once
+#include "k_step2.cuh"
+#include "kernels.h"
+
+namespace fcb {
+
+template <class RP, int MX, int MBC, bool FW, int NT, int MINB, typename TW>
+cudaError_t run_step2_variant(double* q, double* qlast, const double* aux, double* regs, const PatchDesc* desc,
+                              int p0, int npatch, const StepParams* sp, unsigned long long* cfl_bits,
+                              cudaStream_t st)
+{
+    using G = Step2Geom<RP, MX, MX, MBC, TW, NT>;
+    static bool attr_set = false;
+    auto kern = step2_kernel<RP, MX, MX, MBC, FW, NT, TW, MINB>;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    if (npatch <= 0) return cudaSuccess;
+    kern<<<npatch, NT, G::SMEM_BYTES, st>>>(q, qlast, aux, regs, desc, p0, sp, cfl_bits);
+    return cudaGetLastError();
+}
+
+// One table entry: precision, solver id, square patch size MXV (mbc 2), threads, min CTAs per SM.
+#define FCB_STEP2_VARIANT(PREC, RPID, RPT, MXV, FW, NT, MINB, TW)                                           \
+    Step2Variant{PREC, RPID, MXV, MXV, 2, NT, MINB, Step2Geom<RPT, MXV, MXV, 2, TW, NT>::REG ? 1 : 0,       \
+                 (int)Step2Geom<RPT, MXV, MXV, 2, TW, NT>::SMEM_BYTES,                                      \
+                 &run_step2_variant<RPT, MXV, 2, FW, NT, MINB, TW>}
+
+}  // namespace fcb

@@ -17,8 +17,26 @@ struct Dims {
     int nreg() const { return 4 * my * meqn + 4 * mx * meqn + 4 * my * meqn + 4 * mx * meqn; }
 };
 
-// ---- fused update (k_step2_f64.cu) ------------------------------------------
-// Returns cudaErrorInvalidValue when no specialisation exists for (rp, mx, my, mbc).
+// ---- fused update (k_step2_<precision>_<family>.cu) ---------------------------
+// Each unit holds a table of launchers, one per (solver, patch size, patch-to-CTA
+// mapping); the first entry of a shape is its default.  A launcher called with
+// npatch = 0 only sets the kernel's shared-memory attribute.
+typedef cudaError_t (*Step2Fn)(double* q, double* qlast, const double* aux, double* regs, const PatchDesc* desc,
+                               int p0, int npatch, const StepParams* sp, unsigned long long* cfl_bits,
+                               cudaStream_t st);
+struct Step2Variant {
+    int precision, rp, mx, my, mbc;
+    int threads, min_blocks;   // CTA size and __launch_bounds__ occupancy target
+    int reg;                   // 1: one thread per interface (normal solve kept in registers)
+    int smem;                  // dynamic shared memory per CTA, bytes
+    Step2Fn fn;
+};
+const Step2Variant* step2_table_f64_adv(int* n);
+const Step2Variant* step2_table_f64_sw(int* n);
+const Step2Variant* step2_table_f64_euler(int* n);
+const Step2Variant* step2_table_f32w_adv(int* n);
+const Step2Variant* step2_table_f32w_sw(int* n);
+const Step2Variant* step2_table_f32w_euler(int* n);
 
 // ---- ghost fill (k_amr.cu) ----------------------------------------------------
 // Gather tables: offsets are absolute indices of field 0 in the q slab; fields

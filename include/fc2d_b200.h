@@ -141,6 +141,21 @@ int fc2d_b200_advance(fc2d_b200_solver_t* s, double t, double dt, double* maxcfl
  * device repopulation, ghost update.  *changed = 1 if the forest changed. */
 int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed);
 
+/* ---- patch-to-CTA variants of the fused update (no counterpart in the reference) ----
+ * Each solver shape (precision, Riemann solver, patch size) is compiled with
+ * several mappings of a patch onto its CTA: threads per CTA and an occupancy
+ * target (CTAs per SM, which caps registers per thread); reg = 1 when every
+ * interface of a sweep has its own thread.  Variant 0 is the default.  FP64
+ * variants give identical results.  fc2d_b200_autotune times every variant on
+ * the current forest (reps passes over all levels, dt = 0 so q is unchanged),
+ * keeps the fastest and returns it; ms[v] (may be null, num_variants entries)
+ * receives the time of one pass of variant v. */
+int fc2d_b200_num_variants(const fc2d_b200_solver_t* s, int* n, int* current);
+int fc2d_b200_variant_info(const fc2d_b200_solver_t* s, int v, int* threads, int* min_blocks, int* reg,
+                           int* smem_bytes);
+int fc2d_b200_set_variant(fc2d_b200_solver_t* s, int v);
+int fc2d_b200_autotune(fc2d_b200_solver_t* s, int reps, int* best, double* ms);
+
 /* ---- batches of independent forests (instances; no counterpart in the reference) ----
  * One solver can hold up to FC2D_B200_MAX_INSTANCES independent forests with the
  * same patch size, meqn and solver: every level-step launch then covers the
