@@ -1,8 +1,8 @@
 """Benchmark of the B200 patch-update path (cell-updates/s), one JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload dam|dam-uniform|swirl|shockbubble] [--precision fp64|fp32wave]
-                    [--pstar pvrs|mlp]
+                    [--workload dam|dam-uniform|swirl|shockbubble|batch] [--precision fp32wave|fp64]
+                    [--pstar pvrs|mlp] [--no-fp64-compare] [--no-autotune]
 
 Default workload (the configuration the metric is quoted on): 2D shallow water,
 radial dam break on [-1,1]^2, adaptive quadtree levels 3-7, 16x16 patches, mbc=2,
@@ -14,6 +14,14 @@ subcycled, ghost fill, update, time sync), replayed as one CUDA graph per forest
 The regrid every 4 coarse steps runs between timed steps: its host wall time is
 reported separately and excluded from the device time, while the graph capture of
 the new forest falls inside the next timed step.
+
+The FP32-wave form (FP32 waves and limiter, FP64 q, fluxes and registers) is the
+default; the same run times the plain FP64 kernel (bitwise equal to the CPU
+oracle) on the same workload and protocol ("fp64_kernel", with the speed-up) and
+states the FP32 error against FP64 ("error_vs_fp64").  After the spin-up the
+autotuner picks the patch-to-CTA variant of each arm ("patch_to_cta").
+Workload "batch": 64 seeded tsunami instances (f-waves with bathymetry), one
+solver per patch size (8x8, 16x16), both stepping concurrently on their own streams.
 
 value      : interior cell updates of all ranks / max over ranks of the device time
              of the timed steps (CUDA events on the solver's stream).  L2 (126 MB)
@@ -56,6 +64,8 @@ WORKLOADS = {
                   time_sync=0, regrid_interval=0, spinup=0),
     "shockbubble": dict(name="euler_shockbubble_amr_l4-8_16x16", mx=16, my=16, minlevel=4, maxlevel=8, subcycle=1,
                         time_sync=1, regrid_interval=4, spinup=8),
+    "batch": dict(name="tsunami_batch_64_instances_8x8_16x16", batch=True, instances=64, mx=16, my=16,
+                  minlevel=0, maxlevel=0, subcycle=1, time_sync=1, regrid_interval=4, spinup=8),
 }
 
 
@@ -198,7 +208,10 @@ def cpu_sample(wl: dict, precision: str, max_seconds: float = 20.0, threads: int
 def run_reference(args, wl, rank, world):
     if rank != 0:
         return 0
-    cpu = cpu_sample(wl, args.precision, max_seconds=max(5.0, 25.0 / max(args.steps, 1)), threads=0)
+    if wl.get("batch"):
+        cpu = cpu_sample_batch(wl, max_seconds=max(5.0, 25.0 / max(args.steps, 1)), threads=0)
+    else:
+        cpu = cpu_sample(wl, args.precision, max_seconds=max(5.0, 25.0 / max(args.steps, 1)), threads=0)
     line = {
         "metric": "cell-updates/s", "value": cpu["value"], "unit": "cell-updates/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
@@ -278,24 +291,10 @@ def error_vs_fp64(wl, prob, device, mlp, steps=8):
     return {"steps": steps, "l1_rel_per_field": out}
 
 
-def run_ours(args, wl, rank, world, local_rank):
-    import torch
-    import forestclaw_b200 as fb
-    torch.cuda.set_device(local_rank)
-    prob, gc = _options(wl, args.precision)
-    gc.device = local_rank
-    mlp, mlp_info = None, None
-    if args.pstar == "mlp":
-        mlp, mlp_info = train_pstar_mlp(wl, prob, local_rank, args.mlp_samples, args.mlp_epochs)
-    g = fb.Solver(gc)
-    g.initialize()
-    if mlp is not None:
-        g.set_pstar_seed(mlp)
-    dt = _initial_dt(wl, prob)
-    t = 0.0
-    # spin-up with regrid so the timed forest is representative (not timed)
+def _spinup(g, wl, t, dt, steps):
+    """Untimed coarse steps with the workload's regrid interval; returns (t, dt, regrid ms list)."""
     regrid_ms = []
-    for n in range(wl["spinup"]):
+    for n in range(steps):
         cfl = g.advance(t, dt)
         t += dt
         if wl["time_sync"]:
@@ -304,27 +303,16 @@ def run_ours(args, wl, rank, world, local_rank):
             t0 = time.perf_counter()
             g.regrid()
             regrid_ms.append((time.perf_counter() - t0) * 1e3)
-    for _ in range(args.warmup):
-        cfl = g.advance(t, dt)
-        t += dt
-        if wl["time_sync"]:
-            dt *= 0.9 / cfl
-    g.synchronize()
-    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    # timed steps: each coarse step replays the CUDA graph of the current forest;
-    # the regrid every regrid_interval steps runs between timed steps (host wall
-    # clock, reported separately), and the first step on a new forest includes
-    # its graph capture
-    g.set_timing(False)
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    props = torch.cuda.get_device_properties(local_rank)
-    clk = ClockSampler(f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local_rank))
-    if rank == 0:
-        clk.start()
-    step_ms, cells, launches, timed_regrid_ms = [], 0.0, 0, []
-    for k in range(args.steps):
+    return t, dt, regrid_ms
+
+
+def _timed_steps(g, wl, steps, t, dt, flush):
+    """The timed coarse steps: L2 flushed before each, CUDA events on the solver's
+    stream around each advance (graph replay); the regrid every regrid_interval
+    steps runs between timed steps and is reported separately."""
+    import torch
+    step_ms, cells, launches, regrid_ms = [], 0.0, 0, []
+    for k in range(steps):
         flush.fill_(float(k))
         torch.cuda.synchronize()
         c0 = g.cell_updates
@@ -340,23 +328,111 @@ def run_ours(args, wl, rank, world, local_rank):
         if wl["regrid_interval"] and (k + 1) % wl["regrid_interval"] == 0:
             t0 = time.perf_counter()
             g.regrid()
-            timed_regrid_ms.append((time.perf_counter() - t0) * 1e3)
+            regrid_ms.append((time.perf_counter() - t0) * 1e3)
+    return dict(step_ms=step_ms, cells=cells, launches=launches, regrid_ms=regrid_ms, t=t, dt=dt)
+
+
+def _roofline_pass(solvers, t_dt, flush, steps):
+    """Eager re-run of a few steps with a CUDA event pair around every update
+    launch: (update ms, algorithmic bytes, launches) of the fused update kernel."""
+    import torch
+    ms, by, nl = 0.0, 0.0, 0
+    for g in solvers:
+        g.set_timing(True)
+    for k in range(steps):
+        for i, g in enumerate(solvers):
+            flush.fill_(float(k))
+            torch.cuda.synchronize()
+            t, dt = t_dt[i]
+            if getattr(g, "ninst", 0):
+                g.advance_instances(dt)
+            else:
+                g.advance(t + k * dt, dt)
+            st = g.last_update_stats()
+            ms += st["update_ms"]
+            by += st["update_bytes"]
+            nl += st["update_launches"]
+    for g in solvers:
+        g.set_timing(False)
+    return ms, by, nl
+
+
+def _tune(g, enabled):
+    if not enabled:
+        return {"variant": g.variant, "autotuned": False, **g.variants()[g.variant]}
+    best, ms = g.autotune(reps=3)
+    v = g.variants()
+    return {"variant": best, "autotuned": True, **v[best],
+            "candidates": [dict(ms_per_pass=round(float(m), 4), **x) for m, x in zip(ms, v)]}
+
+
+def _roofline_dict(upd_ms, upd_bytes, upd_launches, traffic, bytes_per_cell):
+    peaks = _peaks()
+    achieved = upd_bytes / (upd_ms * 1e-3) / 1e9 if upd_ms > 0 else None
+    return {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": (achieved / peaks["hbm_gbs"]) if achieved else None, "traffic": traffic,
+            "peak_source": peaks["source"], "kernel": "step2 fused update",
+            "algorithmic_bytes_per_launch": upd_bytes / max(upd_launches, 1),
+            "bytes_per_cell_update": bytes_per_cell, "avg_launch_ms": upd_ms / max(upd_launches, 1)}
+
+
+def _fp64_kernel_arm(args, wl, prob, local_rank, flush):
+    """The plain FP64 B200 kernel (bitwise equal to the CPU oracle) on the same
+    workload and the same timing protocol: the comparator of the metric."""
+    import forestclaw_b200 as fb
+    _, gc = _options(wl, "fp64")
+    gc.device = local_rank
+    g = fb.Solver(gc)
+    g.initialize()
+    t, dt, _ = _spinup(g, wl, 0.0, _initial_dt(wl, prob), wl["spinup"])
+    tune = _tune(g, not args.no_autotune)
+    t, dt, _ = _spinup(g, dict(wl, regrid_interval=0), t, dt, args.warmup)
+    g.synchronize()
+    r = _timed_steps(g, wl, args.steps, t, dt, flush)
+    total_ms = float(np.sum(r["step_ms"]))
+    g.close()
+    return {"value": r["cells"] / (total_ms * 1e-3), "ms_per_step": total_ms / args.steps,
+            "variant": {k: tune[k] for k in ("variant", "threads", "min_blocks", "reg")}}
+
+
+def run_ours(args, wl, rank, world, local_rank):
+    import torch
+    import forestclaw_b200 as fb
+    if wl.get("batch"):
+        return run_batch(args, wl, rank, world, local_rank)
+    torch.cuda.set_device(local_rank)
+    prob, gc = _options(wl, args.precision)
+    gc.device = local_rank
+    mlp, mlp_info = None, None
+    if args.pstar == "mlp":
+        mlp, mlp_info = train_pstar_mlp(wl, prob, local_rank, args.mlp_samples, args.mlp_epochs)
+    g = fb.Solver(gc)
+    g.initialize()
+    if mlp is not None:
+        g.set_pstar_seed(mlp)
+    # spin-up with regrid so the timed forest is representative (not timed),
+    # then the autotuner picks the patch-to-CTA variant on that forest
+    t, dt, regrid_ms = _spinup(g, wl, 0.0, _initial_dt(wl, prob), wl["spinup"])
+    tune = _tune(g, not args.no_autotune)
+    t, dt, _ = _spinup(g, dict(wl, regrid_interval=0), t, dt, args.warmup)
+    g.synchronize()
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    g.set_timing(False)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    props = torch.cuda.get_device_properties(local_rank)
+    clk = ClockSampler(f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local_rank))
+    if rank == 0:
+        clk.start()
+    r = _timed_steps(g, wl, args.steps, t, dt, flush)
     torch.cuda.synchronize()
     clocks = clk.stop() if rank == 0 else None
-    # roofline pass (not part of the timed steps): the same steps launched
-    # eagerly with a CUDA event pair around every update launch
-    g.set_timing(True)
-    upd_ms, upd_bytes, upd_launches = 0.0, 0.0, 0
-    for k in range(max(2, min(args.steps, 4))):
-        flush.fill_(float(k))
-        torch.cuda.synchronize()
-        g.advance(t, dt)
-        st = g.last_update_stats()
-        upd_ms += st["update_ms"]
-        upd_bytes += st["update_bytes"]
-        upd_launches += st["update_launches"]
-        t += dt
-    g.set_timing(False)
+    step_ms, cells, launches, timed_regrid_ms, t, dt = (r["step_ms"], r["cells"], r["launches"], r["regrid_ms"],
+                                                         r["t"], r["dt"])
+    nroof = max(2, min(args.steps, 4))
+    upd_ms, upd_bytes, upd_launches = _roofline_pass([g], [(t, dt)], flush, nroof)
+    t += nroof * dt
     total_ms = float(np.sum(step_ms))
     if world > 1:
         tt = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
@@ -391,45 +467,275 @@ def run_ours(args, wl, rank, world, local_rank):
         e2e_cells *= world
     e2e = {"value": e2e_cells / e2e_s, "unit": "cell-updates/s", "h2d_bytes_per_step": nq * 8,
            "d2h_bytes_per_step": nq * 8}
-    if rank != 0:
-        return 0
-    peaks = _peaks()
-    achieved = upd_bytes / (upd_ms * 1e-3) / 1e9 if upd_ms > 0 else None
-    per_launch_bytes = upd_bytes / max(upd_launches, 1)
-    traffic = _traffic_per_launch(wl, args.precision, per_launch_bytes / (8 * (2 * gc.meqn + gc.maux)))
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": (achieved / peaks["hbm_gbs"]) if achieved else None, "traffic": traffic,
-                "peak_source": peaks["source"], "kernel": "step2 fused update",
-                "algorithmic_bytes_per_launch": per_launch_bytes,
-                "bytes_per_cell_update": 8 * (2 * gc.meqn + gc.maux),
-                "avg_launch_ms": upd_ms / max(upd_launches, 1)}
-    cpu = cpu_sample(wl, args.precision, max_seconds=args.cpu_seconds) if args.cpu_seconds > 0 else None
-    err = error_vs_fp64(wl, prob, local_rank, mlp) if args.precision == "fp32wave" else None
     newton = None
     if wl["name"].startswith("euler"):
         h = g.newton_histogram()
         newton = {"mean_iterations": float((np.arange(32) * h).sum() / max(h.sum(), 1)),
                   "histogram": [int(v) for v in h[:12]], "pstar_start": args.pstar, "mlp": mlp_info}
+    npatch = g.num_patches
+    g.close()
+    fp64 = None
+    if args.precision != "fp64" and not args.no_fp64_compare:
+        fp64 = _fp64_kernel_arm(args, wl, prob, local_rank, flush)
+        fp64["speedup"] = value / fp64["value"] if world == 1 else None
+    if rank != 0:
+        return 0
+    bpc = 8 * (2 * gc.meqn + gc.maux)
+    traffic = _traffic_per_launch(wl, args.precision, upd_bytes / max(upd_launches, 1) / bpc)
+    roofline = _roofline_dict(upd_ms, upd_bytes, upd_launches, traffic, bpc)
+    cpu = cpu_sample(wl, args.precision, max_seconds=args.cpu_seconds) if args.cpu_seconds > 0 else None
+    err = error_vs_fp64(wl, prob, local_rank, mlp) if args.precision == "fp32wave" else None
     line = {
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32-waves/f64-q",
         "data": "synthetic (reference app initial data)",
-        "config": {"workload": wl["name"], "patches": g.num_patches, "precision": args.precision,
+        "config": {"workload": wl["name"], "patches": npatch, "precision": args.precision,
                    "cells_per_step": cells / args.steps,
                    "l2": "flushed between timed steps (512 MB write)",
                    "launch": "CUDA graph per coarse step (captured once per forest)",
                    "regrid": (f"every {wl['regrid_interval']} coarse steps between timed steps, excluded from "
                               "the device time" if wl["regrid_interval"] else "none"),
                    "regrids_in_timed_loop": len(timed_regrid_ms),
-                   "regrid_ms_median": float(np.median(regrid_ms + timed_regrid_ms)) if regrid_ms else None},
+                   "regrid_ms_median": float(np.median(regrid_ms + timed_regrid_ms)) if regrid_ms else None,
+                   "patch_to_cta": tune},
         "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
-        "error_vs_fp64": err, "newton": newton,
+        "fp64_kernel": fp64, "error_vs_fp64": err, "newton": newton,
         "gpu_launches": launches, "update_launches": upd_launches,
     }
     print(json.dumps(line), flush=True)
-    g.close()
+    return 0
+
+
+def _batch_groups(precision, device, n=64, seed=0):
+    """The batched workload: n seeded tsunami instances, one solver per patch size
+    (all instances of a size share every level launch)."""
+    import forestclaw_b200 as fb
+    from forestclaw_b200 import problems
+    insts, sizes = problems.tsunami_instances(n, seed)
+    by = {}
+    for k, (inst, mx) in enumerate(zip(insts, sizes)):
+        by.setdefault(mx, []).append((k, inst))
+    groups = []
+    for mx in sorted(by):
+        gc = problems.options(problems.TSUNAMI, mx=mx, my=mx, minlevel=0, maxlevel=0, subcycle=1, time_sync=1,
+                              device=device)
+        gc.precision = fb.PREC_FP32WAVE if precision == "fp32wave" else fb.PREC_FP64
+        g = fb.Solver(gc)
+        g.set_instances([x for _, x in by[mx]])
+        g.initialize()
+        # coarse dt for CFL ~0.9 at the initial state (max speed ~ sqrt(g * 2))
+        dt = np.array([0.9 * (2.0 / (mx << x["minlevel"])) / 1.5 for _, x in by[mx]])
+        groups.append({"g": g, "dt": dt, "mx": mx, "ids": [k for k, _ in by[mx]]})
+    return groups
+
+
+def _batch_step(groups, events=None):
+    """One coarse step of every instance: all groups launched, then all waited for."""
+    import torch
+    if events is not None:
+        start, ends = events
+        start.record()
+    for k, G in enumerate(groups):
+        if events is not None:
+            ext = torch.cuda.ExternalStream(G["g"].stream_handle())
+            ext.wait_event(start)
+        G["g"].advance_instances_begin(G["dt"])
+        if events is not None:
+            ends[k].record(ext)
+    cfl = [G["g"].advance_instances_end() for G in groups]
+    for G, c in zip(groups, cfl):
+        G["dt"] = G["dt"] * 0.9 / c
+    return cfl
+
+
+def _batch_run(groups, steps, regrid_interval, flush=None, timed=False):
+    import torch
+    step_ms, cells, launches, regrid_ms = [], 0.0, 0, []
+    for k in range(steps):
+        ev = None
+        if timed:
+            flush.fill_(float(k))
+            torch.cuda.synchronize()
+            ev = (torch.cuda.Event(enable_timing=True), [torch.cuda.Event(enable_timing=True) for _ in groups])
+        c0 = sum(G["g"].cell_updates for G in groups)
+        _batch_step(groups, ev)
+        if timed:
+            torch.cuda.synchronize()
+            step_ms.append(max(ev[0].elapsed_time(e) for e in ev[1]))
+            launches += sum(G["g"].last_update_stats()["total_launches"] for G in groups)
+        cells += sum(G["g"].cell_updates for G in groups) - c0
+        if regrid_interval and (k + 1) % regrid_interval == 0:
+            t0 = time.perf_counter()
+            for G in groups:
+                G["g"].regrid()
+            regrid_ms.append((time.perf_counter() - t0) * 1e3)
+    return dict(step_ms=step_ms, cells=cells, launches=launches, regrid_ms=regrid_ms)
+
+
+def _batch_timed_arm(args, wl, precision, local_rank, flush, tune_on, clk=None):
+    import torch
+    groups = _batch_groups(precision, local_rank, wl["instances"])
+    _batch_run(groups, wl["spinup"], wl["regrid_interval"])
+    tunes = {str(G["mx"]): _tune(G["g"], tune_on) for G in groups}
+    _batch_run(groups, args.warmup, 0)
+    torch.cuda.synchronize()
+    if clk is not None:
+        clk.start()
+    r = _batch_run(groups, args.steps, wl["regrid_interval"], flush, timed=True)
+    r["clocks"] = clk.stop() if clk is not None else None
+    return groups, tunes, r
+
+
+def _batch_error(local_rank, n, steps=8):
+    """Per-instance relative L1 error of h of the FP32-wave batch against the
+    FP64 batch (bitwise equal to standalone oracle runs) from the same initial
+    forests, the FP64 CFL setting both dt schedules, and the relative difference
+    of each instance's mass (the instances have outflow boundaries, so mass
+    itself changes in both)."""
+    a = _batch_groups("fp64", local_rank, n)
+    b = _batch_groups("fp32wave", local_rank, n)
+    for k in range(steps):
+        for A, B in zip(a, b):
+            B["dt"] = A["dt"].copy()
+        _batch_step(a)
+        _batch_step(b)
+    errs, dmass = [], []
+    for A, B in zip(a, b):
+        qa, qb = A["g"].get_q(), B["g"].get_q()
+        ia, ib = A["g"].patch_instance(), B["g"].patch_instance()
+        ma, mb = A["g"].mass_instances(), B["g"].mass_instances()
+        for i in range(len(A["ids"])):
+            xa, xb = qa[ia == i][:, 0, 2:-2, 2:-2], qb[ib == i][:, 0, 2:-2, 2:-2]
+            errs.append(float(np.abs(xa - xb).sum() / np.abs(xa).sum()))
+            dmass.append(float(abs(mb[i, 0] - ma[i, 0]) / abs(ma[i, 0])))
+        A["g"].close()
+        B["g"].close()
+    return {"steps": steps, "l1_rel_h_max": max(errs), "l1_rel_h_median": float(np.median(errs)),
+            "mass_rel_diff_vs_fp64_max": max(dmass), "instances": len(errs)}
+
+
+def cpu_sample_batch(wl, max_seconds=15.0, threads=0):
+    """The FP64 CPU oracle on the batch's instances, one after another (each a
+    standalone forest), for a bounded time."""
+    from oracle import pyoracle as po
+    from forestclaw_b200 import problems
+    from tests.cases import TSUNAMI, make
+    insts, sizes = problems.tsunami_instances(wl["instances"], 0)
+    t0 = time.perf_counter()
+    cells, steps, used = 0.0, 0, 0
+    for inst, mx in zip(insts, sizes):
+        kw = {k: inst[k] for k in ("minlevel", "maxlevel", "pdata")}
+        oc, _ = make(TSUNAMI, mx=mx, my=mx, subcycle=1, time_sync=1, nthreads=threads, **kw)
+        o = po.OracleSim(oc)
+        o.initialize()
+        dt = 0.9 * (2.0 / (mx << inst["minlevel"])) / 1.5
+        c0, t = o.cell_updates, 0.0
+        for n in range(4):
+            cfl = o.advance(t, dt)
+            t += dt
+            dt *= 0.9 / cfl
+            steps += 1
+        cells += o.cell_updates - c0
+        used += 1
+        if time.perf_counter() - t0 > max_seconds:
+            break
+    el = time.perf_counter() - t0
+    return {"value": cells / el, "unit": "cell-updates/s", "cores": threads or os.cpu_count(), "kind": "port",
+            "sample": f"4 coarse steps of each of the first {used} instances of {wl['name']}, standalone "
+                      f"({cells:.3e} cell updates, {el:.1f} s, FP64 C oracle, OpenMP; setup included)"}
+
+
+def run_batch(args, wl, rank, world, local_rank):
+    import torch
+    torch.cuda.set_device(local_rank)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    props = torch.cuda.get_device_properties(local_rank)
+    clk = ClockSampler(f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local_rank))
+    if world > 1:
+        torch.distributed.barrier()
+    groups, tunes, r = _batch_timed_arm(args, wl, args.precision, local_rank, flush, not args.no_autotune,
+                                        clk if rank == 0 else None)
+    clocks = r["clocks"]
+    total_ms = float(np.sum(r["step_ms"]))
+    cells = r["cells"]
+    if world > 1:
+        tt = torch.tensor([total_ms, cells], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(tt[:1], op=torch.distributed.ReduceOp.MAX)
+        cc = torch.tensor([cells], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(cc, op=torch.distributed.ReduceOp.SUM)
+        total_ms, cells_all = float(tt[0].item()), float(cc.item())
+    else:
+        cells_all = cells
+    value = cells_all / (total_ms * 1e-3)
+    nroof = max(2, min(args.steps, 4))
+    upd_ms, upd_bytes, upd_launches = _roofline_pass([G["g"] for G in groups], [(0.0, G["dt"]) for G in groups],
+                                                     flush, nroof)
+    # ---- end to end: q of every group from pinned host memory and back, every step ----
+    bufs = []
+    for G in groups:
+        g = G["g"]
+        o = g.opts
+        nq = g.num_patches * o.meqn * (o.mx + 2 * o.mbc) * (o.my + 2 * o.mbc)
+        hq = torch.empty(nq, dtype=torch.float64, pin_memory=True)
+        g.get_q_ptr(hq.data_ptr())
+        bufs.append(hq)
+    e2e_steps = max(2, min(args.steps, 10))
+    torch.cuda.synchronize()
+    te0 = time.perf_counter()
+    e2e_cells = 0.0
+    for _ in range(e2e_steps):
+        c0 = sum(G["g"].cell_updates for G in groups)
+        for G, hq in zip(groups, bufs):
+            G["g"].set_q_ptr(hq.data_ptr())
+        _batch_step(groups)
+        for G, hq in zip(groups, bufs):
+            G["g"].get_q_ptr(hq.data_ptr())
+        e2e_cells += sum(G["g"].cell_updates for G in groups) - c0
+    e2e_s = time.perf_counter() - te0
+    nbytes = int(sum(b.numel() for b in bufs) * 8)
+    e2e = {"value": e2e_cells * world / e2e_s, "unit": "cell-updates/s", "h2d_bytes_per_step": nbytes,
+           "d2h_bytes_per_step": nbytes}
+    info = {str(G["mx"]): {"instances": len(G["ids"]), "patches": G["g"].num_patches} for G in groups}
+    for G in groups:
+        G["g"].close()
+    fp64 = None
+    if args.precision != "fp64" and not args.no_fp64_compare:
+        g64, tune64, r64 = _batch_timed_arm(args, wl, "fp64", local_rank, flush, not args.no_autotune)
+        ms64 = float(np.sum(r64["step_ms"]))
+        fp64 = {"value": r64["cells"] / (ms64 * 1e-3), "ms_per_step": ms64 / args.steps,
+                "variants": {k: {x: v[x] for x in ("variant", "threads", "min_blocks", "reg")}
+                             for k, v in tune64.items()}}
+        fp64["speedup"] = value / fp64["value"] if world == 1 else None
+        for G in g64:
+            G["g"].close()
+    if rank != 0:
+        return 0
+    roofline = _roofline_dict(upd_ms, upd_bytes, upd_launches, None, 8 * (2 * 3 + 1))
+    cpu = cpu_sample_batch(wl, max_seconds=args.cpu_seconds) if args.cpu_seconds > 0 else None
+    err = _batch_error(local_rank, wl["instances"]) if args.precision == "fp32wave" else None
+    line = {
+        "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32-waves/f64-q",
+        "data": "synthetic (seeded instances: xoshiro256** per instance)",
+        "config": {"workload": wl["name"], "instances": wl["instances"], "groups": info,
+                   "precision": args.precision, "cells_per_step": cells / args.steps,
+                   "l2": "flushed between timed steps (512 MB write)",
+                   "launch": "one CUDA graph per patch-size group and coarse step (captured once per forest), "
+                             "the groups on their own streams; step time = max over groups of events "
+                             "from a common start",
+                   "regrid": f"every {wl['regrid_interval']} coarse steps between timed steps, excluded",
+                   "regrids_in_timed_loop": len(r["regrid_ms"]),
+                   "regrid_ms_median": float(np.median(r["regrid_ms"])) if r["regrid_ms"] else None,
+                   "patch_to_cta": tunes},
+        "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+        "fp64_kernel": fp64, "error_vs_fp64": err,
+        "gpu_launches": r["launches"], "update_launches": upd_launches,
+    }
+    print(json.dumps(line), flush=True)
     return 0
 
 
@@ -440,7 +746,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="dam", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32wave"])
+    ap.add_argument("--precision", default="fp32wave", choices=["fp64", "fp32wave"])
+    ap.add_argument("--no-fp64-compare", action="store_true",
+                    help="skip the timed run of the plain FP64 kernel on the same workload")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default patch-to-CTA variant")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--pstar", default="pvrs", choices=["pvrs", "mlp"],
                     help="Euler: Newton start of the exact solver (mlp: trained on the FP64 run first)")

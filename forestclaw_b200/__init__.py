@@ -190,6 +190,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_num_instances": [P, ip],
         "fc2d_b200_patch_instance": [P, ip],
         "fc2d_b200_advance_instances": [P, dp, dp],
+        "fc2d_b200_advance_instances_begin": [P, dp],
+        "fc2d_b200_advance_instances_end": [P, dp],
         "fc2d_b200_mass_instances": [P, dp],
         "fc2d_b200_num_variants": [P, ip, ip],
         "fc2d_b200_variant_info": [P, I, ip, ip, ip, ip],
@@ -486,6 +488,18 @@ class Solver:
         dt = np.ascontiguousarray(dt, np.float64)
         cfl = np.zeros(self.ninst, np.float64)
         self._check("fc2d_b200_advance_instances", self.lib.fc2d_b200_advance_instances(self.h, _dp(dt), _dp(cfl)))
+        return cfl
+
+    def advance_instances_begin(self, dt) -> None:
+        """Launch one coarse step of every instance; returns without waiting."""
+        self._dt_keep = np.ascontiguousarray(dt, np.float64)
+        self._check("fc2d_b200_advance_instances_begin",
+                    self.lib.fc2d_b200_advance_instances_begin(self.h, _dp(self._dt_keep)))
+
+    def advance_instances_end(self) -> np.ndarray:
+        """Wait for the step launched by advance_instances_begin; the CFL of each instance."""
+        cfl = np.zeros(self.ninst, np.float64)
+        self._check("fc2d_b200_advance_instances_end", self.lib.fc2d_b200_advance_instances_end(self.h, _dp(cfl)))
         return cfl
 
     def mass_instances(self) -> np.ndarray:

@@ -95,7 +95,10 @@ struct fc2d_b200_solver {
     // batch of independent forests (instances); empty: one forest of the options
     std::vector<fc2d_b200_instance_t> insts;
     double* inst_dt_dev = nullptr;                 // coarse dt of each instance (device)
+    double* inst_dt_host = nullptr;                // pinned staging copy
     int ncfl = 1;                                  // CFL maxima kept (one per instance)
+    bool pending = false;                          // advance launched, not yet finished
+    double pending_t = 0.0;
     // phys_ok[l]: the ghost cells of level l on physical faces hold physical-BC
     // values (set by a ghost update).  False after initialization: the reference
     // fills no ghost cells there by default (init_ghostcell = 0,
@@ -517,6 +520,7 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
     CK(cudaMalloc(&s->cfl_dev, sizeof(unsigned long long) * FC2D_B200_MAX_INSTANCES));
     CK(cudaMallocHost(&s->cfl_host, sizeof(unsigned long long) * FC2D_B200_MAX_INSTANCES));
     CK(cudaMalloc(&s->inst_dt_dev, sizeof(double) * FC2D_B200_MAX_INSTANCES));
+    CK(cudaMallocHost(&s->inst_dt_host, sizeof(double) * FC2D_B200_MAX_INSTANCES));
     CK(cudaMalloc(&s->params_dev, sizeof(StepParams) * fc2d_b200_solver::PCAP));
     {
         double bc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -547,7 +551,7 @@ extern "C" int fc2d_b200_destroy(fc2d_b200_solver_t* s)
     cudaFree(s->q); cudaFree(s->qlast); if (s->qinterp) cudaFree(s->qinterp);
     if (s->aux) cudaFree(s->aux); cudaFree(s->regs); cudaFree(s->desc);
     free_spare(s);
-    cudaFree(s->cfl_dev); cudaFreeHost(s->cfl_host); cudaFree(s->inst_dt_dev);
+    cudaFree(s->cfl_dev); cudaFreeHost(s->cfl_host); cudaFree(s->inst_dt_dev); cudaFreeHost(s->inst_dt_host);
     invalidate_graph(s);
     cudaFree(s->params_dev); cudaFreeHost(s->params_host);
     if (s->mass_dev) cudaFree(s->mass_dev);
@@ -881,7 +885,9 @@ static int traverse_advance(fc2d_b200_solver* s, double t, double dt)
     return 0;
 }
 
-extern "C" int fc2d_b200_advance(fc2d_b200_solver_t* s, double t, double dt, double* maxcfl)
+// First half of an advance: host traversal, parameter upload and the launches
+// (graph replay); returns without waiting for the device.
+static int advance_launch(fc2d_b200_solver_t* s, double t, double dt)
 {
     if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
     s->ev_used = 0;
@@ -919,7 +925,18 @@ extern "C" int fc2d_b200_advance(fc2d_b200_solver_t* s, double t, double dt, dou
     s->fill = true;
     if (rc) return rc;
     CK(cudaGetLastError());
-    rc = end_cfl(s, maxcfl);
+    s->pending_t = t + dt;
+    s->pending = true;
+    return 0;
+}
+
+// Second half: wait for the solver's stream, CFL maximum (per instance into
+// cfl_inst), timing statistics.
+static int advance_finish(fc2d_b200_solver_t* s, double* maxcfl, double* cfl_inst)
+{
+    if (!s->pending) return fail(FC2D_B200_ESTATE, "no advance in flight");
+    s->pending = false;
+    int rc = end_cfl(s, maxcfl, cfl_inst);
     if (s->timing) {
         double ms = 0, bytes = 0;
         for (auto& pr : s->upd_launch_bytes) {
@@ -931,8 +948,16 @@ extern "C" int fc2d_b200_advance(fc2d_b200_solver_t* s, double t, double dt, dou
         s->upd_ms = ms;
         s->upd_bytes = bytes;
     }
-    s->t_curr = t + dt;
+    s->t_curr = s->pending_t;
     return rc;
+}
+
+extern "C" int fc2d_b200_advance(fc2d_b200_solver_t* s, double t, double dt, double* maxcfl)
+{
+    if (s && s->pending) return fail(FC2D_B200_ESTATE, "an advance is in flight");
+    int rc = advance_launch(s, t, dt);
+    if (rc) return rc;
+    return advance_finish(s, maxcfl, nullptr);
 }
 
 extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
@@ -1522,20 +1547,32 @@ extern "C" int fc2d_b200_patch_instance(const fc2d_b200_solver_t* s, int* inst)
     return 0;
 }
 
-extern "C" int fc2d_b200_advance_instances(fc2d_b200_solver_t* s, const double* dt, double* cfl)
+extern "C" int fc2d_b200_advance_instances_begin(fc2d_b200_solver_t* s, const double* dt)
 {
     if (!s || !s->initialized || !dt) return fail(FC2D_B200_EINVAL, "bad arguments");
     if (s->insts.empty()) return fail(FC2D_B200_ESTATE, "no instances set");
+    if (s->pending) return fail(FC2D_B200_ESTATE, "an advance is in flight");
     const int n = (int)s->insts.size();
     for (int i = 0; i < n; i++)
         if (!(dt[i] > 0.0)) return fail(FC2D_B200_EINVAL, "instance time steps must be positive");
-    CK(cudaMemcpyAsync(s->inst_dt_dev, dt, sizeof(double) * n, cudaMemcpyHostToDevice, s->st));
+    std::memcpy(s->inst_dt_host, dt, sizeof(double) * n);
+    CK(cudaMemcpyAsync(s->inst_dt_dev, s->inst_dt_host, sizeof(double) * n, cudaMemcpyHostToDevice, s->st));
     // the level time steps 2^-l of a unit coarse step scale each instance's own dt
+    return advance_launch(s, 0.0, 1.0);
+}
+
+extern "C" int fc2d_b200_advance_instances_end(fc2d_b200_solver_t* s, double* cfl)
+{
+    if (!s) return fail(FC2D_B200_EINVAL, "null solver");
     double dummy = 0.0;
-    int rc = fc2d_b200_advance(s, 0.0, 1.0, &dummy);
+    return advance_finish(s, &dummy, cfl);
+}
+
+extern "C" int fc2d_b200_advance_instances(fc2d_b200_solver_t* s, const double* dt, double* cfl)
+{
+    int rc = fc2d_b200_advance_instances_begin(s, dt);
     if (rc) return rc;
-    if (cfl) rc = end_cfl(s, nullptr, cfl);
-    return rc;
+    return fc2d_b200_advance_instances_end(s, cfl);
 }
 
 extern "C" int fc2d_b200_mass_instances(fc2d_b200_solver_t* s, double* out)

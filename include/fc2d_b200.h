@@ -176,6 +176,11 @@ int fc2d_b200_num_instances(const fc2d_b200_solver_t* s, int* n);
 int fc2d_b200_patch_instance(const fc2d_b200_solver_t* s, int* inst);
 /* One coarse step of every instance, instance i with its own dt[i]; cfl[i] = its CFL. */
 int fc2d_b200_advance_instances(fc2d_b200_solver_t* s, const double* dt, double* cfl);
+/* The same in two halves: _begin launches the step on the solver's stream and
+ * returns at once, _end waits for it and returns the CFL numbers, so the steps of
+ * several solvers (one per patch size, say) run concurrently. */
+int fc2d_b200_advance_instances_begin(fc2d_b200_solver_t* s, const double* dt);
+int fc2d_b200_advance_instances_end(fc2d_b200_solver_t* s, double* cfl);
 /* Kahan-summed mass per instance and field: out[i * meqn + m]. */
 int fc2d_b200_mass_instances(fc2d_b200_solver_t* s, double* out);
 
