@@ -20,8 +20,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libfc2d_b200.so")
 
-RP_ADVECTION, RP_SW_ROE, RP_SW_FWAVE, RP_EULER_EXACT = 0, 1, 2, 3
-APP_NONE, APP_SWIRL, APP_RADIALDAM, APP_TSUNAMI, APP_SHOCKBUBBLE = 0, 1, 2, 3, 4
+RP_ADVECTION, RP_SW_ROE, RP_SW_FWAVE, RP_EULER_EXACT, RP_ADVECTION_MANIFOLD = 0, 1, 2, 3, 4
+APP_NONE, APP_SWIRL, APP_RADIALDAM, APP_TSUNAMI, APP_SHOCKBUBBLE, APP_SPHERE = 0, 1, 2, 3, 4, 5
 PREC_FP64, PREC_FP32WAVE = 0, 1
 
 

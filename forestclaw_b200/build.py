@@ -32,6 +32,7 @@ CU_UNITS = {
     "k_step2_f64_euler.cu": ["-fmad=false"],
     "k_amr.cu": ["-fmad=false"],
     "k_mass_noalloc.cu": ["-fmad=false"],
+    "k_metric.cu": ["-fmad=false"],
     "k_mlp.cu": [],
     "k_step2_f32w_adv.cu": ["--use_fast_math"],
     "k_step2_f32w_sw.cu": ["--use_fast_math"],

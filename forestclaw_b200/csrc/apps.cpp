@@ -11,10 +11,19 @@
 //               cell centre), inflow of user_4.6/bc2.f:53-60, post-shock state from the
 //               Rankine-Hugoniot relations of setprob.f:59-62 for the pressure ratio of a
 //               Mach-M shock, 1 + 2 gamma (M^2 - 1) / (gamma + 1).
+//   sphere:     advection on the cubed sphere (applications/clawpack/advection/2d/sphere):
+//               solid-body rotation psi = omega (axis . x) (the reference's psi.f rotates about
+//               the y axis), q = background + two Gaussians exp(-(theta/w)^2) of the angle
+//               theta to their centres, evaluated at the mapped cell centres.  The metric and
+//               aux (capacity, edge velocities) are computed on the device (k_metric.cu).
+//               pdata: axis[0..2], omega[3], centre 1 [4..6], centre 2 [7..9], width [10],
+//               background [11].
 //   tagging:    fort_4.6/fclaw2d_clawpatch46_tag4refinement.f / _tag4coarsening.f with the
-//               gradient criterion (fort_user/fclaw2d_clawpatch_gradient_exceeds_th.f90) times dx.
+//               gradient criterion (fort_user/fclaw2d_clawpatch_gradient_exceeds_th.f90) times dx;
+//               the sphere uses the minmax criterion (fclaw2d_clawpatch_minmax_exceeds_th.f90).
 #include "apps.hpp"
 #include <cmath>
+#include "fcb_sphere.h"
 
 namespace fcb {
 
@@ -27,6 +36,21 @@ static double swirl_psi(double x, double y, double pi)
 {
     const double sx = std::sin(pi * x), sy = std::sin(pi * y);
     return ((sx * sx) * (sy * sy)) / pi;
+}
+
+void app_sphere_flow(const fc2d_b200_options_t& o, double axis[3], double* omega)
+{
+    const double a = o.pdata[0], b = o.pdata[1], c = o.pdata[2];
+    const double n = std::sqrt(a * a + b * b + c * c);
+    axis[0] = a / n; axis[1] = b / n; axis[2] = c / n;
+    *omega = o.pdata[3];
+}
+
+// angle between the unit vectors x and c
+static double sphere_angle(const double* x, const double* c)
+{
+    const double cx = x[1] * c[2] - x[2] * c[1], cy = x[2] * c[0] - x[0] * c[2], cz = x[0] * c[1] - x[1] * c[0];
+    return std::atan2(std::sqrt(cx * cx + cy * cy + cz * cz), x[0] * c[0] + x[1] * c[1] + x[2] * c[2]);
 }
 
 void app_setaux(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, double* aux)
@@ -57,6 +81,17 @@ void app_setaux(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P,
 void app_qinit(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, const double* aux, double* q)
 {
     const int mx = d.mx, my = d.my, mbc = d.mbc, meqn = d.meqn;
+    if (o.app == FC2D_B200_APP_SPHERE) {
+        const double w = o.pdata[10], bg = o.pdata[11];
+        for (int j = 1 - mbc; j <= my + mbc; j++)
+            for (int i = 1 - mbc; i <= mx + mbc; i++) {
+                double x[3];
+                cs_map(P.block, P.xlower + (i - 0.5) * P.dx, P.ylower + (j - 0.5) * P.dy, &x[0], &x[1], &x[2]);
+                const double t1 = sphere_angle(x, &o.pdata[4]) / w, t2 = sphere_angle(x, &o.pdata[7]) / w;
+                q[qi(d, i, j, 1)] = bg + std::exp(-(t1 * t1)) + std::exp(-(t2 * t2));
+            }
+        return;
+    }
     if (o.app == FC2D_B200_APP_SWIRL) {
         for (int m = 1; m <= meqn; m++)
             for (int i = 1 - mbc; i <= mx + mbc; i++) {
@@ -137,6 +172,16 @@ static bool grad_exceeds(const Dims& d, const PatchInfo& P, const double* q, int
 
 int app_tag_refine(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, const double* q)
 {
+    if (o.app == FC2D_B200_APP_SPHERE) {
+        // minmax: range of field 1 over the padded patch
+        double lo = q[qi(d, 1, 1, 1)], hi = lo;
+        for (int j = 1 - d.mbc; j <= d.my + d.mbc; j++)
+            for (int i = 1 - d.mbc; i <= d.mx + d.mbc; i++) {
+                lo = std::fmin(lo, q[qi(d, i, j, 1)]);
+                hi = std::fmax(hi, q[qi(d, i, j, 1)]);
+            }
+        return hi - lo > o.refine_threshold ? 1 : 0;
+    }
     for (int j = 1; j <= d.my; j++)
         for (int i = 1; i <= d.mx; i++)
             if (grad_exceeds(d, P, q, i, j, o.refine_threshold)) return 1;

@@ -10,6 +10,8 @@ namespace fcb {
 void app_setaux(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, double* aux);
 // qinit for one patch into q (meqn*nxy doubles, ghosts included).
 void app_qinit(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, const double* aux, double* q);
+// The sphere app's rotation: unit axis and angular speed (psi = omega (axis . x)).
+void app_sphere_flow(const fc2d_b200_options_t& o, double axis[3], double* omega);
 // Constant state imposed by mthbc = 0 sides (shock-bubble inflow); false if the app has none.
 bool app_inflow_state(const fc2d_b200_options_t& o, double* q);
 // Refinement test of one patch (tag4refinement with the dx-scaled gradient criterion).

@@ -14,10 +14,11 @@ struct PatchDesc {
     int face_type;      // 2 bits per face: 0 boundary, 1 half (finer nbr), 2 same, 3 double (coarser nbr)
     int flags;          // PATCH_* bits
     int inst;           // instance of a batch of independent forests (0 otherwise)
-    int pad_;
+    int block;          // block of the domain (the cubed sphere's face 0..5; brick tree number)
 };
 
-enum { PATCH_HAS_FINE_NBR = 1 };
+// PATCH_BCC3 << k: corner k of the patch is a corner of the cubed sphere (three blocks meet)
+enum { PATCH_HAS_FINE_NBR = 1, PATCH_BCC3 = 2 };
 
 // p*-seed network sizes and layouts (k_mlp.cuh).  The network seeds Newton only
 // where the interface carries a wave of strength |dp|/pbar + |du|/cbar above

@@ -85,7 +85,7 @@ struct fc2d_b200_solver {
     // second set of slabs: regrid repopulates into it and swaps, so a regrid
     // allocates only when the forest outgrows the spare's capacity
     struct Spare { double *q = nullptr, *qlast = nullptr, *qinterp = nullptr, *aux = nullptr, *regs = nullptr;
-                   PatchDesc* desc = nullptr; int cap = 0; } spare;
+                   double* area = nullptr; PatchDesc* desc = nullptr; int cap = 0; } spare;
     DevVec<int> flags_dev;                         // regrid tag flags
     bool has_inflow = false;                       // mthbc = 0 sides take bc_dev (app inflow state)
     double* bc_dev = nullptr;                      // 8 doubles
@@ -111,7 +111,13 @@ struct fc2d_b200_solver {
     DevVec<double> snap;                           // batch regrid: q of instances whose forest is unchanged
     DevVec<int> keep_dev;
     std::vector<double> aux_host;                  // static aux mirror (level-major)
-    DevVec<CopyEnt> t_copy, t_avg;
+    DevVec<CopyEnt> t_copy;
+    DevVec<AvgEnt> t_avg;
+    double* area = nullptr;                        // cubed sphere: cell areas per patch (Dims::narea per patch)
+    bool sphere = false;                           // the cubed-sphere app (manifold, 6 blocks)
+    SphereFlow flow{};                             // its rotation: psi = omega (axis . x)
+    DevVec<MetricOp> metric_dev;
+    DevVec<double> minmax_dev;
     DevVec<InterpEnt> t_interp;
     DevVec<PhysEnt> t_phys;
     DevVec<int> t_ti, t_ss_start, t_f2c_start;
@@ -164,8 +170,9 @@ static int alloc_slabs(fc2d_b200_solver* s, int np)
     const Dims& d = s->d;
     if (np <= s->cap && s->q) return 0;
     int cap = np + np / 4 + 16;
-    double *q, *ql, *qi = nullptr, *aux = nullptr, *regs;
+    double *q, *ql, *qi = nullptr, *aux = nullptr, *regs, *area = nullptr;
     PatchDesc* desc;
+    if (s->sphere) CK(cudaMalloc(&area, (size_t)cap * d.narea() * sizeof(double)));
     CK(cudaMalloc(&q, (size_t)cap * d.nq() * sizeof(double)));
     CK(cudaMalloc(&ql, (size_t)cap * d.nq() * sizeof(double)));
     if (s->o.subcycle) CK(cudaMalloc(&qi, (size_t)cap * d.nq() * sizeof(double)));
@@ -180,8 +187,10 @@ static int alloc_slabs(fc2d_b200_solver* s, int np)
         // caller copies what it needs before freeing; here the old slabs are released
         cudaFree(s->q); cudaFree(s->qlast); if (s->qinterp) cudaFree(s->qinterp);
         if (s->aux) cudaFree(s->aux); cudaFree(s->regs); cudaFree(s->desc);
+        if (s->area) cudaFree(s->area);
     }
     s->q = q; s->qlast = ql; s->qinterp = qi; s->aux = aux; s->regs = regs; s->desc = desc; s->cap = cap;
+    s->area = area;
     return 0;
 }
 
@@ -194,6 +203,7 @@ static void free_spare(fc2d_b200_solver* s)
     if (sp.aux) cudaFree(sp.aux);
     if (sp.regs) cudaFree(sp.regs);
     if (sp.desc) cudaFree(sp.desc);
+    if (sp.area) cudaFree(sp.area);
     sp = fc2d_b200_solver::Spare{};
 }
 
@@ -212,13 +222,13 @@ static int ensure_spare(fc2d_b200_solver* s, int np)
     if (d.maux > 0) CK(cudaMalloc(&sp.aux, (size_t)cap * d.naux() * sizeof(double)));
     CK(cudaMalloc(&sp.regs, (size_t)cap * d.nreg() * sizeof(double)));
     CK(cudaMalloc(&sp.desc, (size_t)cap * sizeof(PatchDesc)));
+    if (s->sphere) CK(cudaMalloc(&sp.area, (size_t)cap * d.narea() * sizeof(double)));
     sp.cap = cap;
     return 0;
 }
 
-static int upload_desc_and_tables(fc2d_b200_solver* s)
+static std::vector<PatchDesc> make_desc(const Forest& f)
 {
-    const Forest& f = s->forest;
     std::vector<PatchDesc> hd(f.np());
     for (int i = 0; i < f.np(); i++) {
         const PatchInfo& P = f.p[i];
@@ -230,13 +240,27 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
         for (int k = 0; k < 4; k++) ft |= (P.face_type[k] & 3) << (2 * k);
         pd.face_type = ft;
         pd.flags = P.has_fine_nbr ? PATCH_HAS_FINE_NBR : 0;
+        for (int k = 0; k < 4; k++)
+            if (P.bcc3[k]) pd.flags |= PATCH_BCC3 << k;
         pd.inst = P.inst;
+        pd.block = P.block;
         hd[i] = pd;
     }
+    return hd;
+}
+
+static int upload_desc_and_tables(fc2d_b200_solver* s)
+{
+    const Forest& f = s->forest;
+    const std::vector<PatchDesc> hd = make_desc(f);
     if (!hd.empty()) CK(cudaMemcpyAsync(s->desc, hd.data(), hd.size() * sizeof(PatchDesc), cudaMemcpyHostToDevice, s->st));
     std::vector<LevelTables> T;
-    build_tables(f, s->o.mthbc, s->has_inflow, T);
-    std::vector<CopyEnt> copy, avg;
+    {
+        std::string err;
+        if (!build_tables(f, s->o.mthbc, s->has_inflow, T, err)) return fail(FC2D_B200_EFOREST, err);
+    }
+    std::vector<CopyEnt> copy;
+    std::vector<AvgEnt> avg;
     std::vector<InterpEnt> interp;
     std::vector<PhysEnt> phys;
     std::vector<int> ti, ss_start, f2c_start;
@@ -376,7 +400,7 @@ static void average_range(fc2d_b200_solver* s, int a, int b, int ti)
     const int off = s->lr[a].avg_off, n = s->lr[b].avg_off + s->lr[b].avg_n - off;
     if (n <= 0) return;
     if (s->fill) s->total_launches++;
-    if (s->emit) launch_average(s->d, tsdata(s, ti), s->q, s->t_avg.p + off, n, s->st);
+    if (s->emit) launch_average(s->d, tsdata(s, ti), s->q, s->t_avg.p + off, n, s->area, s->st);
 }
 static void phys_range(fc2d_b200_solver* s, int a, int b, int ti)
 {
@@ -506,6 +530,12 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
         return fail(FC2D_B200_EINVAL, "bad minlevel/maxlevel");
     const bool sup = !step2_variants(o.precision, o.rp, o.mx, o.my, o.mbc).empty();
     if (!sup) return fail(FC2D_B200_EINVAL, "no compiled update kernel for this (rp, mx, my, mbc, precision)");
+    if (o.app == FC2D_B200_APP_SPHERE &&
+        (o.rp != FC2D_B200_RP_ADVECTION_MANIFOLD || o.maux != 3 || o.mcapa != 1 || o.mx != o.my || o.mx < 8))
+        return fail(FC2D_B200_EINVAL, "the cubed-sphere app needs the manifold advection solver, maux 3, mcapa 1, "
+                                      "square patches with mx >= 8");
+    if (o.app == FC2D_B200_APP_SPHERE && o.time_sync)
+        return fail(FC2D_B200_EINVAL, "time sync across cubed-sphere block seams is not built");
     int ndev = 0;
     CK(cudaGetDeviceCount(&ndev));
     if (ndev <= 0) return fail(FC2D_B200_ECUDA, "no CUDA device");
@@ -516,6 +546,14 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
     if (s->o.mj <= 0) s->o.mj = 1;
     s->d = Dims{o.mx, o.my, o.mbc, o.meqn, o.maux};
     s->forest.g = Geometry{s->d, s->o.mi, s->o.mj, o.ax, o.bx, o.ay, o.by};
+    if (o.app == FC2D_B200_APP_SPHERE) {
+        // six blocks [0,1]^2, patch x coordinate = block 2^l + ix
+        s->sphere = true;
+        s->o.mi = 6; s->o.mj = 1; s->o.ax = 0.0; s->o.bx = 1.0; s->o.ay = 0.0; s->o.by = 1.0;
+        s->forest.g = Geometry{s->d, 6, 1, 0.0, 1.0, 0.0, 1.0};
+        s->forest.g.kind = 1;
+        app_sphere_flow(s->o, s->flow.axis, &s->flow.omega);
+    }
     CK(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
     CK(cudaMalloc(&s->cfl_dev, sizeof(unsigned long long) * FC2D_B200_MAX_INSTANCES));
     CK(cudaMallocHost(&s->cfl_host, sizeof(unsigned long long) * FC2D_B200_MAX_INSTANCES));
@@ -557,6 +595,7 @@ extern "C" int fc2d_b200_destroy(fc2d_b200_solver_t* s)
     if (s->mass_dev) cudaFree(s->mass_dev);
     cudaFree(s->bc_dev); cudaFree(s->newton_hist);
     if (s->tune_params) cudaFree(s->tune_params);
+    if (s->area) cudaFree(s->area);
     if (s->mlp_blob) cudaFree(s->mlp_blob);
     cudaStreamDestroy(s->st);
     delete s;
@@ -687,6 +726,16 @@ extern "C" int fc2d_b200_initialize(fc2d_b200_solver_t* s)
     // install_forest sorted identically (same keys) -> same slot order as f
     CK(cudaMemcpyAsync(s->q, q.data(), q.size() * sizeof(double), cudaMemcpyHostToDevice, s->st));
     if (d.maux > 0) CK(cudaMemcpyAsync(s->aux, aux.data(), aux.size() * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    if (s->sphere) {
+        // every patch's metric from scratch (fclaw2d_metric_patch_build), then its aux
+        std::vector<MetricOp> ops(s->forest.np());
+        for (int i = 0; i < s->forest.np(); i++) ops[i] = MetricOp{0, i, {0, 0, 0, 0}};
+        CK(s->metric_dev.assign(ops, s->st));
+        launch_sphere_metric(d, s->metric_dev.p, (int)ops.size(), s->desc, s->o.maxlevel, nullptr, s->area, s->aux,
+                             s->flow, s->st);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(aux.data(), s->aux, aux.size() * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    }
     CK(cudaStreamSynchronize(s->st));
     s->aux_host.swap(aux);
     s->t_curr = 0;
@@ -968,8 +1017,15 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     const int np = f.np();
     std::vector<int> flags(np);
     CK(s->flags_dev.assign(flags, s->st));
-    launch_tag(d, s->q, s->desc, np, s->o.refine_threshold, s->o.coarsen_threshold, s->flags_dev.p, s->st);
+    std::vector<double> mm;
+    if (s->sphere) {
+        mm.assign(2 * (size_t)np, 0.0);
+        CK(s->minmax_dev.assign(mm, s->st));
+    }
+    launch_tag(d, s->q, s->desc, np, s->o.refine_threshold, s->o.coarsen_threshold, s->flags_dev.p, s->st,
+               s->sphere ? s->minmax_dev.p : nullptr);
     CK(cudaMemcpyAsync(flags.data(), s->flags_dev.p, sizeof(int) * (size_t)np, cudaMemcpyDeviceToHost, s->st));
+    if (s->sphere) CK(cudaMemcpyAsync(mm.data(), s->minmax_dev.p, sizeof(double) * mm.size(), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
     // cb_regrid_tag4coarsening (families) then cb_fclaw2d_regrid_tag4refinement
     std::vector<int> mark(np, 0);
@@ -983,7 +1039,14 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
         }
         if (!ok) continue;
         bool coarsen = true;
-        for (int k = 0; k < 4; k++) if (!(flags[sib[k]] & 2)) coarsen = false;
+        if (s->sphere) {
+            // minmax over the family (fclaw2d_clawpatch46_fort_tag4coarsening.f:35-58)
+            double lo = mm[2 * sib[0]], hi = mm[2 * sib[0] + 1];
+            for (int k = 1; k < 4; k++) { lo = std::min(lo, mm[2 * sib[k]]); hi = std::max(hi, mm[2 * sib[k] + 1]); }
+            coarsen = !(hi - lo > s->o.coarsen_threshold);
+        } else {
+            for (int k = 0; k < 4; k++) if (!(flags[sib[k]] & 2)) coarsen = false;
+        }
         if (coarsen) for (int k = 0; k < 4; k++) mark[sib[k]] = -1;
     }
     for (int i = 0; i < np; i++)
@@ -1048,12 +1111,32 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     if (rc) return rc;
     auto& sp = s->spare;
     CK(s->repop_dev.assign(ops, s->st));
-    launch_repop(d, s->repop_dev.p, (int)ops.size(), s->q, sp.q, s->qlast, sp.qlast, s->qinterp, sp.qinterp, s->regs,
-                 sp.regs, s->st);
     if (d.maux > 0) CK(cudaMemcpyAsync(sp.aux, naux.data(), naux.size() * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    std::vector<PatchDesc> hd;
+    if (s->sphere) {
+        // metric of the new forest before repopulation, which weights by the areas:
+        // kept patches copy, refined ones build from scratch, coarsened ones from their
+        // children (cb_fclaw2d_regrid_repopulate: fclaw2d_patch_build / _build_from_fine)
+        std::vector<MetricOp> mops(ops.size());
+        for (size_t i = 0; i < ops.size(); i++) {
+            const RepopOp& o = ops[i];
+            if (o.kind == 0) mops[i] = MetricOp{1, (int)i, {o.src, 0, 0, 0}};
+            else if (o.kind == 1) mops[i] = MetricOp{0, (int)i, {0, 0, 0, 0}};
+            else mops[i] = MetricOp{2, (int)i, {o.child[0], o.child[1], o.child[2], o.child[3]}};
+        }
+        hd = make_desc(nf);
+        CK(cudaMemcpyAsync(sp.desc, hd.data(), hd.size() * sizeof(PatchDesc), cudaMemcpyHostToDevice, s->st));
+        CK(s->metric_dev.assign(mops, s->st));
+        launch_sphere_metric(d, s->metric_dev.p, (int)mops.size(), sp.desc, s->o.maxlevel, s->area, sp.area, sp.aux,
+                             s->flow, s->st);
+        CK(cudaMemcpyAsync(naux.data(), sp.aux, naux.size() * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    }
+    launch_repop(d, s->repop_dev.p, (int)ops.size(), s->q, sp.q, s->qlast, sp.qlast, s->qinterp, sp.qinterp, s->regs,
+                 sp.regs, s->sphere ? s->area : nullptr, s->sphere ? sp.area : nullptr, s->st);
     CK(cudaStreamSynchronize(s->st));
     std::swap(s->q, sp.q); std::swap(s->qlast, sp.qlast); std::swap(s->qinterp, sp.qinterp);
     std::swap(s->aux, sp.aux); std::swap(s->regs, sp.regs); std::swap(s->desc, sp.desc);
+    std::swap(s->area, sp.area);
     std::swap(s->cap, sp.cap);
     s->aux_host.swap(naux);
     s->forest = std::move(nf);
@@ -1094,7 +1177,7 @@ extern "C" int fc2d_b200_mass(fc2d_b200_solver_t* s, double* out)
         s->mass_cap = np * meqn + 1024;
         CK(cudaMalloc(&s->mass_dev, sizeof(double) * (size_t)s->mass_cap));
     }
-    launch_patch_mass(s->d, s->q, s->desc, np, s->mass_dev, s->st);
+    launch_patch_mass(s->d, s->q, s->desc, np, s->mass_dev, s->st, s->area);
     std::vector<double> pm((size_t)np * meqn);
     CK(cudaMemcpyAsync(pm.data(), s->mass_dev, sizeof(double) * pm.size(), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
@@ -1210,6 +1293,7 @@ static int scratch_for_device(int dev, double** out)
 extern "C" int fc2d_b200_mass_noalloc(fc2d_b200_solver_t* s, double* out)
 {
     if (!s || !out || !s->initialized) return fail(FC2D_B200_EINVAL, "bad arguments");
+    if (s->sphere) return fail(FC2D_B200_EINVAL, "fc2d_b200_mass_noalloc weights by dx dy; a manifold needs fc2d_b200_mass");
     const long long np = s->forest.np(), meqn = s->d.meqn;
     if (np * meqn + meqn > (long long)MASS_SCRATCH_DOUBLES)
         return fail(FC2D_B200_EINVAL, "fc2d_b200_mass_noalloc: npatches*meqn + meqn = " + std::to_string(np * meqn + meqn) +
@@ -1584,7 +1668,7 @@ extern "C" int fc2d_b200_mass_instances(fc2d_b200_solver_t* s, double* out)
         s->mass_cap = np * meqn + 1024;
         CK(cudaMalloc(&s->mass_dev, sizeof(double) * (size_t)s->mass_cap));
     }
-    launch_patch_mass(s->d, s->q, s->desc, np, s->mass_dev, s->st);
+    launch_patch_mass(s->d, s->q, s->desc, np, s->mass_dev, s->st, s->area);
     std::vector<double> pm((size_t)np * meqn);
     CK(cudaMemcpyAsync(pm.data(), s->mass_dev, sizeof(double) * pm.size(), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));

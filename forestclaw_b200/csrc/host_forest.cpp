@@ -12,10 +12,120 @@
 // in brick-global cell indices, canonical child order).
 #include "host_forest.hpp"
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <map>
+#include "fcb_sphere.h"
 
 namespace fcb {
+
+// ---------------------------------------------------------------------------
+// cubed-sphere connectivity
+// ---------------------------------------------------------------------------
+// p4est's cubed connectivity (p4est_connectivity_new_cubed, called by
+// fclaw2d_domain_new_cubedsphere, src/fclaw2d_convenience.c:355) is not in the
+// reference tree (p4est is an empty submodule).  The same information follows
+// from the mapping the reference pairs with it: two block faces are joined where
+// their mapped edges coincide, with the edge parameter running the same way
+// (flip 0) or reversed (flip 1).
+namespace {
+struct CSTable {
+    CSFace f[6][4];
+    CSTable()
+    {
+        auto edge = [](int face, double t, double& x, double& y) {
+            if (face == 0) { x = 0.0; y = t; } else if (face == 1) { x = 1.0; y = t; }
+            else if (face == 2) { x = t; y = 0.0; } else { x = t; y = 1.0; }
+        };
+        auto pt = [&](int b, int face, double t, double* p) {
+            double x, y;
+            edge(face, t, x, y);
+            cs_map(b, x, y, &p[0], &p[1], &p[2]);
+        };
+        auto close = [](const double* a, const double* b) {
+            return std::fabs(a[0] - b[0]) + std::fabs(a[1] - b[1]) + std::fabs(a[2] - b[2]) < 1e-9;
+        };
+        for (int b = 0; b < 6; b++)
+            for (int fc = 0; fc < 4; fc++) {
+                double p0[3], p1[3];
+                pt(b, fc, 0.25, p0);
+                pt(b, fc, 0.75, p1);
+                CSFace& F = f[b][fc];
+                F.nb = -1;
+                for (int b2 = 0; b2 < 6 && F.nb < 0; b2++)
+                    for (int f2 = 0; f2 < 4; f2++) {
+                        if (b2 == b) continue;
+                        double q0[3], q1[3];
+                        pt(b2, f2, 0.25, q0);
+                        pt(b2, f2, 0.75, q1);
+                        if (close(p0, q0) && close(p1, q1)) { F.nb = b2; F.nf = f2; F.flip = 0; break; }
+                        if (close(p0, q1) && close(p1, q0)) { F.nb = b2; F.nf = f2; F.flip = 1; break; }
+                    }
+                // depth d beyond face fc and position t along it, into block nb at depth d
+                // inside face nf: an isometry of the plane, so affine with integer M, c
+                auto T = [&](double x, double y, double& x2, double& y2) {
+                    double d, t;
+                    if (fc == 0) { d = -x; t = y; } else if (fc == 1) { d = x - 1.0; t = y; }
+                    else if (fc == 2) { d = -y; t = x; } else { d = y - 1.0; t = x; }
+                    const double sp = F.flip ? 1.0 - t : t;
+                    if (F.nf == 0) { x2 = d; y2 = sp; } else if (F.nf == 1) { x2 = 1.0 - d; y2 = sp; }
+                    else if (F.nf == 2) { x2 = sp; y2 = d; } else { x2 = sp; y2 = 1.0 - d; }
+                };
+                double cx, cy, ax, ay, bx, by;
+                T(0.0, 0.0, cx, cy);
+                T(1.0, 0.0, ax, ay);
+                T(0.0, 1.0, bx, by);
+                F.c[0] = (int)std::lround(cx); F.c[1] = (int)std::lround(cy);
+                F.M[0][0] = (int)std::lround(ax - cx); F.M[1][0] = (int)std::lround(ay - cy);
+                F.M[0][1] = (int)std::lround(bx - cx); F.M[1][1] = (int)std::lround(by - cy);
+            }
+    }
+};
+const CSTable& cs_table()
+{
+    static const CSTable t;
+    return t;
+}
+}  // namespace
+
+const CSFace& cs_face(int b, int f) { return cs_table().f[b][f]; }
+
+int cs_face_to(int a, int b)
+{
+    if (a == b) return -1;
+    for (int f = 0; f < 4; f++)
+        if (cs_face(a, f).nb == b) return f;
+    return -1;
+}
+
+void cs_xform(int b, int f, long N, long X, long Y, long& X2, long& Y2)
+{
+    // cell centres (X + 1/2) / N map by the affine isometry; in integers
+    // 2 X' + 1 = M (2 X + 1) + 2 N c
+    const CSFace& F = cs_face(b, f);
+    X2 = (F.M[0][0] * (2 * X + 1) + F.M[0][1] * (2 * Y + 1) + 2 * N * F.c[0] - 1) / 2;
+    Y2 = (F.M[1][0] * (2 * X + 1) + F.M[1][1] * (2 * Y + 1) + 2 * N * F.c[1] - 1) / 2;
+}
+
+int Forest::step(int i, int l, int x, int y, int dx, int dy, int& ox, int& oy) const
+{
+    const Geometry& G = gi(i);
+    if (G.kind == 0) {
+        ox = x + dx; oy = y + dy;
+        return in_domain(i, l, ox, oy) ? 1 : 0;
+    }
+    const long n = 1L << (l + G.lbase);
+    const int b = (int)(x / n);
+    const long ix = x - b * n + dx, iy = (long)y + dy;
+    const bool outx = ix < 0 || ix >= n, outy = iy < 0 || iy >= n;
+    if (!outx && !outy) { ox = (int)(b * n + ix); oy = (int)iy; return 1; }
+    if (outx && outy) return -1;
+    const int f = outx ? (ix < 0 ? 0 : 1) : (iy < 0 ? 2 : 3);
+    long X2, Y2;
+    cs_xform(b, f, n, ix, iy, X2, Y2);
+    ox = (int)(cs_face(b, f).nb * n + X2); oy = (int)Y2;
+    return 1;
+}
 
 static uint64_t interleave(uint32_t x, uint32_t y)
 {
@@ -49,12 +159,12 @@ void Forest::geometry(PatchInfo& q) const
     const double w = 1.0 / (double)(1 << l);
     const double xl = ix * w, yl = iy * w, xu = (ix + 1) * w, yu = (iy + 1) * w;
     double xlo, ylo, xup, yup;
-    if (g.mi == 1 && g.mj == 1) { xlo = xl; ylo = yl; xup = xu; yup = yu; }
+    if ((g.mi == 1 && g.mj == 1) || g.kind == 1) { xlo = xl; ylo = yl; xup = xu; yup = yu; }
     else {
         xlo = (double)(bx + xl) / g.mi; xup = (double)(bx + xu) / g.mi;
         ylo = (double)(by + yl) / g.mj; yup = (double)(by + yu) / g.mj;
     }
-    q.block = brick_block(g.mi, g.mj, bx, by);
+    q.block = g.kind == 1 ? bx : brick_block(g.mi, g.mj, bx, by);
     q.xlower = g.ax + (g.bx - g.ax) * xlo;
     const double xupper = g.ax + (g.bx - g.ax) * xup;
     q.ylower = g.ay + (g.by - g.ay) * ylo;
@@ -109,19 +219,22 @@ bool Forest::build(const std::vector<Leaf>& leaves, std::string& err)
         const int l = P.level, in = P.inst;
         P.has_fine_nbr = 0; P.on_cf = 0;
         for (int f = 0; f < 4; f++) {
-            const int nx = P.gx + FDX[f], ny = P.gy + FDY[f];
+            int nx, ny;
             P.face_nbr[f][0] = P.face_nbr[f][1] = -1;
-            P.phys[f] = !in_domain(in, l, nx, ny);
+            P.phys[f] = step(in, l, P.gx, P.gy, FDX[f], FDY[f], nx, ny) != 1;
             if (P.phys[f]) { P.face_type[f] = NB_BOUNDARY; continue; }
             int k = lookup(in, l, nx, ny);
             if (k >= 0) { P.face_type[f] = NB_SAME; P.face_nbr[f][0] = k; continue; }
             k = lookup(in, l - 1, nx >> 1, ny >> 1);
             if (k >= 0) { P.face_type[f] = NB_DOUBLE; P.face_nbr[f][0] = k; P.on_cf = 1; continue; }
+            // the two finer leaves across the face: our children touching it, stepped across
             int c0x, c0y, c1x, c1y;
-            if (f == 0) { c0x = 2 * nx + 1; c0y = 2 * ny; c1x = c0x; c1y = 2 * ny + 1; }
-            else if (f == 1) { c0x = 2 * nx; c0y = 2 * ny; c1x = c0x; c1y = 2 * ny + 1; }
-            else if (f == 2) { c0x = 2 * nx; c0y = 2 * ny + 1; c1x = 2 * nx + 1; c1y = c0y; }
-            else { c0x = 2 * nx; c0y = 2 * ny; c1x = 2 * nx + 1; c1y = c0y; }
+            {
+                const int ex = (f == 1) ? 1 : 0, ey = (f == 3) ? 1 : 0;
+                const int kx = (f < 2) ? 0 : 1, ky = (f < 2) ? 1 : 0;
+                step(in, l + 1, 2 * P.gx + ex, 2 * P.gy + ey, FDX[f], FDY[f], c0x, c0y);
+                step(in, l + 1, 2 * P.gx + ex + kx, 2 * P.gy + ey + ky, FDX[f], FDY[f], c1x, c1y);
+            }
             const int a = lookup(in, l + 1, c0x, c0y), b = lookup(in, l + 1, c1x, c1y);
             if (a < 0 || b < 0) { err = "forest is not 2:1 face balanced"; return false; }
             P.face_type[f] = NB_HALF; P.face_nbr[f][0] = a; P.face_nbr[f][1] = b;
@@ -129,13 +242,23 @@ bool Forest::build(const std::vector<Leaf>& leaves, std::string& err)
         }
         for (int c = 0; c < 4; c++) {
             const int f0 = (c & 1) ? 1 : 0, f1 = (c & 2) ? 3 : 2;
-            P.has_corner[c] = 0; P.corner_nbr[c] = -1; P.corner_type[c] = NB_BOUNDARY;
+            P.has_corner[c] = 0; P.corner_nbr[c] = -1; P.corner_type[c] = NB_BOUNDARY; P.bcc3[c] = 0;
             if (P.phys[f0] || P.phys[f1]) continue;            // not an interior corner
             const int ddx = (c & 1) ? 1 : -1, ddy = (c & 2) ? 1 : -1;
-            const int nx = P.gx + ddx, ny = P.gy + ddy;
+            int nx, ny;
+            if (step(in, l, P.gx, P.gy, ddx, ddy, nx, ny) < 0) {
+                // three blocks meet (src/fclaw2d_corner_neighbors.c:250-262): no corner neighbour,
+                // the update's fix_corners fills these ghost cells
+                P.bcc3[c] = 1;
+                continue;
+            }
             int k = lookup(in, l, nx, ny);
             if (k >= 0) { P.has_corner[c] = 1; P.corner_type[c] = NB_SAME; P.corner_nbr[c] = k; continue; }
-            k = lookup(in, l + 1, 2 * nx + (ddx < 0), 2 * ny + (ddy < 0));
+            {
+                int fx, fy;
+                step(in, l + 1, 2 * P.gx + (ddx > 0), 2 * P.gy + (ddy > 0), ddx, ddy, fx, fy);
+                k = lookup(in, l + 1, fx, fy);
+            }
             if (k >= 0) {
                 P.has_corner[c] = 1; P.corner_type[c] = NB_HALF; P.corner_nbr[c] = k;
                 P.has_fine_nbr = 1; P.on_cf = 1; continue;
@@ -196,8 +319,8 @@ std::vector<Leaf> adapt_leaves(const Forest& f, const std::vector<int>& mark, in
             for (int dy = -1; dy <= 1; dy++)
                 for (int dx = -1; dx <= 1; dx++) {
                     if (!dx && !dy) continue;
-                    const int x = L[i].gx + dx, y = L[i].gy + dy;
-                    if (!f.in_domain(in, l, x, y)) continue;
+                    int x, y;
+                    if (f.step(in, l, L[i].gx, L[i].gy, dx, dy, x, y) != 1) continue;
                     for (int k = l - 2; k >= 0; k--) {
                         auto it = idx.find(Forest::key(in, k, x >> (l - k), y >> (l - k)));
                         if (it != idx.end()) {
@@ -234,17 +357,48 @@ namespace {
 struct TableCtx {
     const Forest& f;
     int mx, my, mbc, nx, nq;
+    bool sph;
     TableCtx(const Forest& ff) : f(ff)
     {
         mx = ff.g.d.mx; my = ff.g.d.my; mbc = ff.g.d.mbc; nx = mx + 2 * mbc; nq = ff.g.d.nq();
+        sph = ff.sphere();
     }
     // absolute offset of Fortran cell (i,j), field 0, of slot p
     int cell(int p, int i, int j) const { return p * nq + (j + mbc - 1) * nx + (i + mbc - 1); }
-    // transform_face2 / transform_corner2, same orientation: first child of coarse (i,j)
-    void half_first(const PatchInfo& C, const PatchInfo& F, int i, int j, int& di, int& dj) const
+    // block and cell origin of a patch at its level: brick-global for bricks (one
+    // coordinate system), block-local for the cubed sphere
+    void org(const PatchInfo& P, int& b, long& X0, long& Y0) const
     {
-        di = 1 + (2 * C.gx - F.gx) * mx + 2 * (i - 1);
-        dj = 1 + (2 * C.gy - F.gy) * my + 2 * (j - 1);
+        if (!sph) { b = 0; X0 = (long)P.gx * mx; Y0 = (long)P.gy * my; return; }
+        const long n = 1L << P.level;
+        b = (int)(P.gx / n);
+        X0 = (P.gx - b * n) * mx;
+        Y0 = (long)P.gy * my;
+    }
+    // cell (X, Y) of block b at level L in the coordinates of block b2 (adjacent or equal)
+    void to_block(int b, int b2, int L, long X, long Y, long& X2, long& Y2) const
+    {
+        if (b == b2) { X2 = X; Y2 = Y; return; }
+        const int fc = cs_face_to(b, b2);
+        if (fc < 0) { X2 = Y2 = -(1L << 20); return; }   // not adjacent: outside every patch (tables check)
+        cs_xform(b, fc, (long)mx << L, X, Y, X2, Y2);
+    }
+    // transform_face / transform_corner: cell (i, j) of P as a Fortran index of N, same level
+    void same(const PatchInfo& P, int i, int j, const PatchInfo& N, int& i2, int& j2) const
+    {
+        int b, bn; long X0, Y0, XN, YN, X2, Y2;
+        org(P, b, X0, Y0); org(N, bn, XN, YN);
+        to_block(b, bn, P.level, X0 + i - 1, Y0 + j - 1, X2, Y2);
+        i2 = (int)(X2 - XN + 1); j2 = (int)(Y2 - YN + 1);
+    }
+    // transform_face2 / transform_corner2: child (a, c) -- in the coarse patch's axes -- of
+    // coarse cell (i, j) of C, as a Fortran index of the fine patch F
+    void child(const PatchInfo& C, int i, int j, int a, int c, const PatchInfo& F, int& i2, int& j2) const
+    {
+        int b, bf; long X0, Y0, XF, YF, X2, Y2;
+        org(C, b, X0, Y0); org(F, bf, XF, YF);
+        to_block(b, bf, C.level + 1, 2 * (X0 + i - 1) + a, 2 * (Y0 + j - 1) + c, X2, Y2);
+        i2 = (int)(X2 - XF + 1); j2 = (int)(Y2 - YF + 1);
     }
 };
 
@@ -270,7 +424,26 @@ struct LastWriter {
 
 }  // namespace
 
-void build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<LevelTables>& out)
+// Every gather index must lie in the q slab: a wrong transform would otherwise send the
+// ghost-fill kernels outside it.
+static bool tables_in_bounds(const std::vector<LevelTables>& out, long nall, int& bad_level)
+{
+    auto ok = [&](long k) { return k >= 0 && k < nall; };
+    for (size_t l = 0; l < out.size(); l++) {
+        const LevelTables& T = out[l];
+        bool good = true;
+        for (const CopyEnt& e : T.copy) good = good && ok(e.dst) && ok(e.src);
+        for (const AvgEnt& e : T.avg)
+            good = good && ok(e.dst) && ok(e.src) && ok((long)e.src + e.sx) && ok((long)e.src + e.sy) &&
+                   ok((long)e.src + e.sx + e.sy);
+        for (const InterpEnt& e : T.interp) good = good && ok(e.dst) && ok(e.src) && e.sub >= 0 && e.sub < 4;
+        for (const PhysEnt& e : T.phys) good = good && ok(e.dst) && ok(e.src);
+        if (!good) { bad_level = (int)l; return false; }
+    }
+    return true;
+}
+
+bool build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<LevelTables>& out, std::string& err)
 {
     TableCtx T(f);
     const int mx = T.mx, my = T.my, mbc = T.mbc;
@@ -290,14 +463,16 @@ void build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<
                     if (P.face_type[fc] != NB_SAME) continue;
                     const int n = P.face_nbr[fc][0];
                     const PatchInfo& N = f.p[n];
-                    const int si = (P.gx - N.gx) * mx, sj = (P.gy - N.gy) * my;
                     int ilo, ihi, jlo, jhi;
                     if (fc == 0) { ilo = 1 - mbc; ihi = 0; jlo = 1; jhi = my; }
                     else if (fc == 1) { ilo = mx + 1; ihi = mx + mbc; jlo = 1; jhi = my; }
                     else if (fc == 2) { ilo = 1; ihi = mx; jlo = 1 - mbc; jhi = 0; }
                     else { ilo = 1; ihi = mx; jlo = my + 1; jhi = my + mbc; }
                     for (int j = jlo; j <= jhi; j++)
-                        for (int i = ilo; i <= ihi; i++) W.put({T.cell(ip, i, j), T.cell(n, i + si, j + sj)});
+                        for (int i = ilo; i <= ihi; i++) {
+                            int i2, j2; T.same(P, i, j, N, i2, j2);
+                            W.put({T.cell(ip, i, j), T.cell(n, i2, j2)});
+                        }
                 }
             }
             for (int ip = p0; ip < p1; ip++) {
@@ -306,11 +481,11 @@ void build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<
                     if (!P.has_corner[c] || P.corner_type[c] != NB_SAME) continue;
                     const int n = P.corner_nbr[c];
                     const PatchInfo& N = f.p[n];
-                    const int si = (P.gx - N.gx) * mx, sj = (P.gy - N.gy) * my;
                     for (int ibc = 1; ibc <= mbc; ibc++)
                         for (int jbc = 1; jbc <= mbc; jbc++) {
                             const int i1 = (c & 1) ? mx + ibc : 1 - ibc, j1 = (c & 2) ? my + jbc : 1 - jbc;
-                            W.put({T.cell(ip, i1, j1), T.cell(n, i1 + si, j1 + sj)});
+                            int i2, j2; T.same(P, i1, j1, N, i2, j2);
+                            W.put({T.cell(ip, i1, j1), T.cell(n, i2, j2)});
                         }
                 }
             }
@@ -318,7 +493,19 @@ void build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<
         }
         // ---- average2ghost (coarse = this level) ----
         {
-            LastWriter<CopyEnt> W(slots, T.nq, nxy);
+            LastWriter<AvgEnt> W(slots, T.nq, nxy);
+            auto valid = [&](int i, int j) { return 1 <= i && i <= mx && 1 <= j && j <= my; };
+            // the four children of coarse ghost cell (ic, jc) in F, skipped unless all are
+            // interior cells of F (fclaw2d_clawpatch_is_valid_average)
+            auto emit = [&](int ip, const PatchInfo& C, int ic, int jc, int fi, const PatchInfo& F, bool check) {
+                int ci[4], cj[4];
+                for (int m = 0; m < 4; m++) {
+                    T.child(C, ic, jc, m & 1, m >> 1, F, ci[m], cj[m]);
+                    if (check && !valid(ci[m], cj[m])) return;
+                }
+                const int src = T.cell(fi, ci[0], cj[0]);
+                W.put({T.cell(ip, ic, jc), src, T.cell(fi, ci[1], cj[1]) - src, T.cell(fi, ci[2], cj[2]) - src});
+            };
             for (int ip = p0; ip < p1; ip++) {
                 const PatchInfo& C = f.p[ip];
                 if (!C.on_cf) continue;
@@ -327,23 +514,14 @@ void build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<
                     for (int ig = 0; ig < 2; ig++) {
                         const int fi = C.face_nbr[fc][ig];
                         const PatchInfo& F = f.p[fi];
-                        auto valid = [&](int i, int j) { return 1 <= i && i <= mx && 1 <= j && j <= my; };
                         if (fc < 2) {
                             for (int jc = 1; jc <= my; jc++)
-                                for (int ibc = 1; ibc <= mbc; ibc++) {
-                                    const int ic = (fc == 0) ? 1 - ibc : mx + ibc;
-                                    int di, dj; T.half_first(C, F, ic, jc, di, dj);
-                                    if (!valid(di, dj) || !valid(di + 1, dj + 1)) continue;
-                                    W.put({T.cell(ip, ic, jc), T.cell(fi, di, dj)});
-                                }
+                                for (int ibc = 1; ibc <= mbc; ibc++)
+                                    emit(ip, C, (fc == 0) ? 1 - ibc : mx + ibc, jc, fi, F, true);
                         } else {
                             for (int jbc = 1; jbc <= mbc; jbc++)
-                                for (int ic = 1; ic <= mx; ic++) {
-                                    const int jc = (fc == 2) ? 1 - jbc : my + jbc;
-                                    int di, dj; T.half_first(C, F, ic, jc, di, dj);
-                                    if (!valid(di, dj) || !valid(di + 1, dj + 1)) continue;
-                                    W.put({T.cell(ip, ic, jc), T.cell(fi, di, dj)});
-                                }
+                                for (int ic = 1; ic <= mx; ic++)
+                                    emit(ip, C, ic, (fc == 2) ? 1 - jbc : my + jbc, fi, F, true);
                         }
                     }
                 }
@@ -356,11 +534,8 @@ void build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<
                     const int fi = C.corner_nbr[c];
                     const PatchInfo& F = f.p[fi];
                     for (int ibc = 1; ibc <= mbc; ibc++)
-                        for (int jbc = 1; jbc <= mbc; jbc++) {
-                            const int i1 = (c & 1) ? mx + ibc : 1 - ibc, j1 = (c & 2) ? my + jbc : 1 - jbc;
-                            int di, dj; T.half_first(C, F, i1, j1, di, dj);
-                            W.put({T.cell(ip, i1, j1), T.cell(fi, di, dj)});
-                        }
+                        for (int jbc = 1; jbc <= mbc; jbc++)
+                            emit(ip, C, (c & 1) ? mx + ibc : 1 - ibc, (c & 2) ? my + jbc : 1 - jbc, fi, F, false);
                 }
             }
             LT.avg = std::move(W.v);
@@ -369,11 +544,15 @@ void build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<
         {
             LastWriter<InterpEnt> W(slots, T.nq, nxy);
             auto validi = [&](int i, int j) { return 1 - mbc <= i && i <= mx + mbc && 1 - mbc <= j && j <= my + mbc; };
-            auto emit = [&](int cp, int ic, int jc, int fp, int di, int dj) {
+            // the fine cells of the four children (coarse axes, sub = ii + 2 jj) of coarse
+            // cell (ic, jc), skipped unless all lie in F's padded patch (is_valid_interp)
+            auto emit = [&](int cp, const PatchInfo& C, int ic, int jc, int fp, const PatchInfo& F, bool check) {
+                int ci[4], cj[4];
                 for (int m = 0; m < 4; m++) {
-                    const int ii = m & 1, jj = m >> 1;
-                    W.put({T.cell(fp, di + ii, dj + jj), T.cell(cp, ic, jc), m, 0});
+                    T.child(C, ic, jc, m & 1, m >> 1, F, ci[m], cj[m]);
+                    if (check && !validi(ci[m], cj[m])) return;
                 }
+                for (int m = 0; m < 4; m++) W.put({T.cell(fp, ci[m], cj[m]), T.cell(cp, ic, jc), m, 0});
             };
             for (int ip = p0; ip < p1; ip++) {
                 const PatchInfo& C = f.p[ip];
@@ -386,20 +565,12 @@ void build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<
                         if (fc < 2) {
                             for (int ibc = 1; ibc <= mbc / 2; ibc++) {
                                 const int ic = (fc == 0) ? ibc : mx - ibc + 1;
-                                for (int jc = 1; jc <= mx; jc++) {
-                                    int di, dj; T.half_first(C, F, ic, jc, di, dj);
-                                    if (!validi(di, dj) || !validi(di + 1, dj + 1)) continue;
-                                    emit(ip, ic, jc, fi, di, dj);
-                                }
+                                for (int jc = 1; jc <= mx; jc++) emit(ip, C, ic, jc, fi, F, true);
                             }
                         } else {
                             for (int jbc = 1; jbc <= mbc / 2; jbc++) {
                                 const int jc = (fc == 2) ? jbc : my - jbc + 1;
-                                for (int ic = 1; ic <= mx; ic++) {
-                                    int di, dj; T.half_first(C, F, ic, jc, di, dj);
-                                    if (!validi(di, dj) || !validi(di + 1, dj + 1)) continue;
-                                    emit(ip, ic, jc, fi, di, dj);
-                                }
+                                for (int ic = 1; ic <= mx; ic++) emit(ip, C, ic, jc, fi, F, true);
                             }
                         }
                     }
@@ -413,11 +584,8 @@ void build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<
                     const int fi = C.corner_nbr[c];
                     const PatchInfo& F = f.p[fi];
                     for (int ibc = 1; ibc <= mbc / 2; ibc++)
-                        for (int jbc = 1; jbc <= mbc / 2; jbc++) {
-                            const int ic = (c & 1) ? mx - ibc + 1 : ibc, jc = (c & 2) ? my - jbc + 1 : jbc;
-                            int di, dj; T.half_first(C, F, ic, jc, di, dj);
-                            emit(ip, ic, jc, fi, di, dj);
-                        }
+                        for (int jbc = 1; jbc <= mbc / 2; jbc++)
+                            emit(ip, C, (c & 1) ? mx - ibc + 1 : ibc, (c & 2) ? my - jbc + 1 : jbc, fi, F, false);
                 }
             }
             LT.interp = std::move(W.v);
@@ -472,7 +640,10 @@ void build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<
             const PatchInfo& P = f.p[ip];
             int nops = 0;
             for (int fc = 0; fc < 4; fc++)
-                if (P.face_type[fc] == NB_SAME) { LT.ss.push_back({ip, P.face_nbr[fc][0], fc, 0, 0, {0, 0, 0}}); nops++; }
+                if (P.face_type[fc] == NB_SAME && (!f.sphere() || f.p[P.face_nbr[fc][0]].block == P.block)) {
+                    LT.ss.push_back({ip, P.face_nbr[fc][0], fc, 0, 0, {0, 0, 0}});
+                    nops++;
+                }
             if (nops) LT.ss_start.push_back((int)LT.ss.size());
         }
         LT.f2c_start.push_back(0);
@@ -481,6 +652,7 @@ void build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<
             int nops = 0;
             for (int fc = 0; fc < 4; fc++) {
                 if (C.face_type[fc] != NB_HALF) continue;
+                if (f.sphere() && f.p[C.face_nbr[fc][0]].block != C.block) continue;
                 for (int ig = 0; ig < 2; ig++) {
                     const int fi = C.face_nbr[fc][ig];
                     const PatchInfo& F = f.p[fi];
@@ -492,6 +664,12 @@ void build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<
             if (nops) LT.f2c_start.push_back((int)LT.f2c.size());
         }
     }
+    int bad = -1;
+    if (!tables_in_bounds(out, (long)f.np() * T.nq, bad)) {
+        err = "ghost-fill table of level " + std::to_string(bad) + " indexes outside the patches (bad transform)";
+        return false;
+    }
+    return true;
 }
 
 }  // namespace fcb

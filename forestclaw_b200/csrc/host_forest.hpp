@@ -1,7 +1,8 @@
 // host_forest.hpp -- host-side forest of patches and the device gather tables.
 //
 // The forest plays p4est's role for the B200 package: leaves of a quadtree over
-// a brick of equally oriented blocks, face/corner neighbour relations, 2:1
+// a brick of equally oriented blocks or over the six blocks of the cubed sphere
+// (faces joined with rotations), face/corner neighbour relations, 2:1
 // face+corner balance and adaptation.  From it the host builds, once per
 // regrid, the per-level gather tables that turn the reference's per-patch
 // ghost-fill and time-sync callbacks into single device launches.
@@ -20,6 +21,16 @@ enum { NB_BOUNDARY = 0, NB_HALF = 1, NB_SAME = 2, NB_DOUBLE = 3 };
 // integer patch coordinates over the instance's brick at its refinement level.
 struct Leaf { int level, gx, gy; int inst = 0; };
 
+// Cubed-sphere connectivity, derived from the mapping (fcb_sphere.h): face f of
+// block b touches face nf of block nb; a point (x, y) of block b's coordinates
+// (inside or beyond face f) is (x', y') = M (x, y) + c in block nb's coordinates.
+struct CSFace { int nb, nf, flip; int M[2][2]; int c[2]; };
+const CSFace& cs_face(int b, int f);
+// Cell (or patch) (X, Y) of block b at N cells per block side, in block nb = cs_face(b, f).nb.
+void cs_xform(int b, int f, long N, long X, long Y, long& X2, long& Y2);
+// The face of block a whose neighbour is block b (-1: not adjacent, or a == b).
+int cs_face_to(int a, int b);
+
 struct PatchInfo {
     int level, gx, gy, block;
     int inst;
@@ -29,6 +40,7 @@ struct PatchInfo {
     int face_nbr[4][2];
     int phys[4];
     int has_corner[4], corner_type[4], corner_nbr[4];
+    int bcc3[4];      // corner c is a corner of the cubed sphere (three blocks meet, no corner neighbour)
     int has_fine_nbr, on_cf;
 };
 
@@ -37,6 +49,7 @@ struct Geometry {
     int mi, mj;
     double ax, bx, ay, by;
     int lbase = 0;    // refinement level of forest level 0 (an instance's minlevel in a batch)
+    int kind = 0;     // 0: brick of mi x mj equally oriented blocks; 1: cubed sphere (6 blocks, gx = block 2^l + ix)
 };
 
 class Forest {
@@ -62,6 +75,11 @@ public:
         return l >= 0 && x >= 0 && y >= 0 && x < (G.mi << la) && y < (G.mj << la);
     }
     void geometry(PatchInfo& q) const;
+    bool sphere(int i = 0) const { return gi(i).kind == 1; }
+    // Patch (x, y) of level l stepped by (dx, dy), |dx|, |dy| <= 1, across block faces:
+    // 1 with the neighbour position in (ox, oy); 0 outside the domain (physical boundary);
+    // -1 across a cubed-sphere corner (no diagonal neighbour there).
+    int step(int i, int l, int x, int y, int dx, int dy, int& ox, int& oy) const;
     static uint64_t key(int i, int l, int x, int y)
     {
         return ((uint64_t)i << 56) | ((uint64_t)l << 50) | ((uint64_t)x << 25) | (uint64_t)y;
@@ -79,7 +97,7 @@ std::vector<Leaf> adapt_leaves(const Forest& f, const std::vector<int>& mark, in
 // Gather tables of one level.
 struct LevelTables {
     std::vector<CopyEnt> copy;       // copy2ghost(level)
-    std::vector<CopyEnt> avg;        // average2ghost(level): level is the coarse level
+    std::vector<AvgEnt> avg;         // average2ghost(level): level is the coarse level
     std::vector<InterpEnt> interp;   // interpolate2ghost(level): level is the coarse level
     std::vector<PhysEnt> phys;       // setphysical(level)
     std::vector<int> ti;             // patches with fine-grid neighbours (fclaw2d_timeinterp)
@@ -88,6 +106,7 @@ struct LevelTables {
 };
 
 // inflow: mthbc = 0 sides are set to a constant state (PhysEnt.pad = 1, src unused).
-void build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<LevelTables>& out);
+// False (with err) if a table would index outside the patches.
+bool build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<LevelTables>& out, std::string& err);
 
 }  // namespace fcb

@@ -29,19 +29,39 @@ __global__ void k_copy(double* __restrict__ dst, const double* __restrict__ src,
     for (int m = 0; m < meqn; m++) dst[c.dst + m * nxy] = src[c.src + m * nxy];
 }
 
-__global__ void k_average(double* __restrict__ dst, const double* __restrict__ src, const CopyEnt* __restrict__ e,
-                          int n, int nx, int nxy, int meqn)
+__global__ void k_average(double* __restrict__ dst, const double* __restrict__ src, const AvgEnt* __restrict__ e,
+                          int n, int nq, int nx, int nxy, int meqn, const double* __restrict__ area)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
-    CopyEnt c = e[t];
+    AvgEnt c = e[t];
+    const int o1 = c.sx, o2 = c.sy, o3 = c.sx + c.sy;
+    if (area) {
+        // manifold (fclaw2d_clawpatch46_average.f:96-115): sum(q_f a_f) / sum(a_f); the
+        // area array of a patch has one ring more than q: cell (ic, jc) of q's padded
+        // layout is (ic + 1, jc + 1) of a row of nx + 2
+        const int p = c.src / nq, ny = nxy / nx, na = (nx + 2) * (ny + 2);
+        const double* ap = area + (size_t)p * na;
+        auto ai = [&](int off) { const int cc = c.src - p * nq + off; return (cc / nx + 1) * (nx + 2) + cc % nx + 1; };
+        const double a0 = ap[ai(0)], a1 = ap[ai(o1)], a2 = ap[ai(o2)], a3 = ap[ai(o3)];
+        for (int m = 0; m < meqn; m++) {
+            const double* f = src + c.src + m * nxy;
+            double sum = 0.0, af = 0.0;
+            sum = sum + f[0] * a0;  af = af + a0;
+            sum = sum + f[o1] * a1; af = af + a1;
+            sum = sum + f[o2] * a2; af = af + a2;
+            sum = sum + f[o3] * a3; af = af + a3;
+            dst[c.dst + m * nxy] = sum / af;
+        }
+        return;
+    }
     for (int m = 0; m < meqn; m++) {
         const double* f = src + c.src + m * nxy;
         double sum = 0.0;
         sum = sum + f[0];
-        sum = sum + f[1];
-        sum = sum + f[nx];
-        sum = sum + f[nx + 1];
+        sum = sum + f[o1];
+        sum = sum + f[o2];
+        sum = sum + f[o3];
         dst[c.dst + m * nxy] = sum / 4.0;
     }
 }
@@ -301,7 +321,7 @@ __global__ void k_reset_sync(double* __restrict__ regs, const PatchDesc* __restr
 
 // Per-patch, per-field Kahan sums of q*dx*dy over interior cells in (j, i) order.
 __global__ void k_patch_mass(const double* __restrict__ q, const PatchDesc* __restrict__ desc, int mx, int my,
-                             int mbc, int meqn, double* __restrict__ out)
+                             int mbc, int meqn, double* __restrict__ out, const double* __restrict__ areas)
 {
     const int p = blockIdx.x, m = threadIdx.x;
     if (m >= meqn) return;
@@ -309,10 +329,13 @@ __global__ void k_patch_mass(const double* __restrict__ q, const PatchDesc* __re
     const PatchDesc pd = desc[p];
     const double area = pd.dx * pd.dy;
     const double* qp = q + ((size_t)p * meqn + m) * nx * ny;
+    // manifold: the cell areas (area(i,j), fclaw2d_clawpatch46_diagnostics.f:40-42)
+    const double* ap = areas ? areas + (size_t)p * (nx + 2) * (ny + 2) : nullptr;
     double sum = 0.0, comp = 0.0;
     for (int j = 0; j < my; j++)
         for (int i = 0; i < mx; i++) {
-            double y = qp[(j + mbc) * nx + i + mbc] * area - comp;
+            const double aij = ap ? ap[(j + mbc + 1) * (nx + 2) + i + mbc + 1] : area;
+            double y = qp[(j + mbc) * nx + i + mbc] * aij - comp;
             double t = sum + y;
             comp = (t - sum) - y;
             sum = t;
@@ -322,12 +345,38 @@ __global__ void k_patch_mass(const double* __restrict__ q, const PatchDesc* __re
 
 // Gradient criterion scaled by dx on field 1 (gradient_exceeds_th.f90, unmapped branch).
 __global__ void k_tag(const double* __restrict__ q, const PatchDesc* __restrict__ desc, int mx, int my, int mbc,
-                      int meqn, double rthr, double cthr, int* __restrict__ flags)
+                      int meqn, double rthr, double cthr, int* __restrict__ flags, double* __restrict__ minmax)
 {
     const int p = blockIdx.x;
     const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
     const PatchDesc pd = desc[p];
     const double* qp = q + (size_t)p * meqn * nx * ny;
+    if (minmax) {
+        // minmax criterion (fclaw2d_clawpatch_minmax_exceeds_th.f90 in
+        // fclaw2d_clawpatch46_fort_tag4refinement.f:38-75): range of field 1 over the
+        // padded patch; the family coarsening test combines the ranges on the host
+        __shared__ double smn[128], smx[128];
+        double mn = qp[mbc * nx + mbc], mxv = mn;
+        for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
+            mn = fmin(mn, qp[c]);
+            mxv = fmax(mxv, qp[c]);
+        }
+        smn[threadIdx.x] = mn; smx[threadIdx.x] = mxv;
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if ((int)threadIdx.x < w) {
+                smn[threadIdx.x] = fmin(smn[threadIdx.x], smn[threadIdx.x + w]);
+                smx[threadIdx.x] = fmax(smx[threadIdx.x], smx[threadIdx.x + w]);
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            minmax[2 * p] = smn[0];
+            minmax[2 * p + 1] = smx[0];
+            flags[p] = (smx[0] - smn[0] > rthr) ? 1 : 0;
+        }
+        return;
+    }
     const double dx2 = 2 * pd.dx, dy2 = 2 * pd.dy;
     int refine = 0, exceed_c = 0;
     for (int c = threadIdx.x; c < mx * my; c += blockDim.x) {
@@ -349,10 +398,14 @@ __global__ void k_repop(const RepopOp* __restrict__ ops, int mx, int my, int mbc
                         const double* __restrict__ oq, double* __restrict__ nq,
                         const double* __restrict__ oql, double* __restrict__ nql,
                         const double* __restrict__ oqi, double* __restrict__ nqi,
-                        const double* __restrict__ oregs, double* __restrict__ nregs)
+                        const double* __restrict__ oregs, double* __restrict__ nregs,
+                        const double* __restrict__ oarea, const double* __restrict__ narea)
 {
     const RepopOp op = ops[blockIdx.x];
     const int nx = mx + 2 * mbc, ny = my + 2 * mbc, nxy = nx * ny, nqp = nxy * meqn;
+    const int ax = nx + 2, na = ax * (ny + 2);
+    // area of Fortran cell (i, j) of a manifold patch's area array
+    auto aidx = [&](int i, int j) { return (j + mbc) * ax + (i + mbc); };
     double* d = nq + (size_t)op.dst * nqp;
     if (op.kind == 0) {
         const size_t so = (size_t)op.src * nqp;
@@ -391,11 +444,30 @@ __global__ void k_repop(const RepopOp* __restrict__ ops, int mx, int my, int mbc
             sl = (q0 - c0[-nx]);
             sr = (c0[nx] - q0);
             double grady = compute_slopes(sl, sr);
+            double v[2][2];
             for (int ii = 1; ii <= 2; ii++)
                 for (int jj = 1; jj <= 2; jj++) {
                     const double shx = (ii - 2 / 2.0 - 0.5) / 2, shy = (jj - 2 / 2.0 - 0.5) / 2;
+                    v[ii - 1][jj - 1] = q0 + shx * gradx + shy * grady;
+                }
+            if (narea && i >= 1 && i <= mx / 2 && j >= 1 && j <= my / 2) {
+                // fclaw2d_clawpatch46_fort_fixcapaq2 (interpolate.f:409-470): the four
+                // fine cells get the coarse cell's mass back, (qc kc - sum kf qf) / 4 each
+                const double* af = narea + (size_t)op.dst * na;
+                double sum = 0.0;
+                for (int ii = 1; ii <= 2; ii++)
+                    for (int jj = 1; jj <= 2; jj++)
+                        sum = sum + af[aidx((i - 1) * 2 + ii, (j - 1) * 2 + jj)] * v[ii - 1][jj - 1];
+                const double kc = oarea[(size_t)op.src * na + aidx(ic, jc)];
+                const double cons_diff = (q0 * kc - sum) / 4.0;
+                for (int ii = 1; ii <= 2; ii++)
+                    for (int jj = 1; jj <= 2; jj++)
+                        v[ii - 1][jj - 1] = v[ii - 1][jj - 1] + cons_diff / af[aidx((i - 1) * 2 + ii, (j - 1) * 2 + jj)];
+            }
+            for (int ii = 1; ii <= 2; ii++)
+                for (int jj = 1; jj <= 2; jj++) {
                     const int fi = (i - 1) * 2 + ii, fj = (j - 1) * 2 + jj;
-                    d[(size_t)m * nxy + (fj + mbc - 1) * nx + (fi + mbc - 1)] = q0 + shx * gradx + shy * grady;
+                    d[(size_t)m * nxy + (fj + mbc - 1) * nx + (fi + mbc - 1)] = v[ii - 1][jj - 1];
                 }
         }
     } else {
@@ -407,6 +479,18 @@ __global__ void k_repop(const RepopOp* __restrict__ ops, int mx, int my, int mbc
             for (int t = threadIdx.x; t < (mx / 2) * (my / 2) * meqn; t += blockDim.x) {
                 const int i = 1 + t % (mx / 2), j = 1 + (t / (mx / 2)) % (my / 2), m = t / ((mx / 2) * (my / 2));
                 double sum = 0.0;
+                if (narea) {
+                    // manifold (average.f:340-352): sum(kf qf) / kc with the new coarse areas
+                    const double* af = oarea + (size_t)op.child[c] * na;
+                    for (int jj = 1; jj <= 2; jj++)
+                        for (int ii = 1; ii <= 2; ii++) {
+                            const int fi = (i - 1) * 2 + ii, fj = (j - 1) * 2 + jj;
+                            sum = sum + af[aidx(fi, fj)] * qf[(size_t)m * nxy + (fj + mbc - 1) * nx + (fi + mbc - 1)];
+                        }
+                    const double kc = narea[(size_t)op.dst * na + aidx(i + icadd, j + jcadd)];
+                    d[(size_t)m * nxy + (j + jcadd + mbc - 1) * nx + (i + icadd + mbc - 1)] = sum / kc;
+                    continue;
+                }
                 for (int jj = 1; jj <= 2; jj++)
                     for (int ii = 1; ii <= 2; ii++) {
                         const int fi = (i - 1) * 2 + ii, fj = (j - 1) * 2 + jj;
@@ -437,9 +521,10 @@ void launch_copy(const Dims& d, double* dst, const double* src, const CopyEnt* e
 {
     if (n > 0) k_copy<<<nblk(n, 256), 256, 0, st>>>(dst, src, e, n, d.nxy(), d.meqn);
 }
-void launch_average(const Dims& d, double* dst, const double* src, const CopyEnt* e, int n, cudaStream_t st)
+void launch_average(const Dims& d, double* dst, const double* src, const AvgEnt* e, int n, const double* area,
+                    cudaStream_t st)
 {
-    if (n > 0) k_average<<<nblk(n, 256), 256, 0, st>>>(dst, src, e, n, d.nx(), d.nxy(), d.meqn);
+    if (n > 0) k_average<<<nblk(n, 256), 256, 0, st>>>(dst, src, e, n, d.nq(), d.nx(), d.nxy(), d.meqn, area);
 }
 void launch_interp(const Dims& d, double* dst, const double* src, const InterpEnt* e, int n, cudaStream_t st)
 {
@@ -474,21 +559,23 @@ void launch_reset_sync(const Dims& d, double* regs, const PatchDesc* desc, int p
 {
     if (np > 0) k_reset_sync<<<np, 64, 0, st>>>(regs, desc, p0, d.mx, d.my, d.meqn, d.nreg(), minlevel, maxl);
 }
-void launch_patch_mass(const Dims& d, const double* q, const PatchDesc* desc, int np, double* out, cudaStream_t st)
+void launch_patch_mass(const Dims& d, const double* q, const PatchDesc* desc, int np, double* out, cudaStream_t st,
+                       const double* area)
 {
-    if (np > 0) k_patch_mass<<<np, 32, 0, st>>>(q, desc, d.mx, d.my, d.mbc, d.meqn, out);
+    if (np > 0) k_patch_mass<<<np, 32, 0, st>>>(q, desc, d.mx, d.my, d.mbc, d.meqn, out, area);
 }
 void launch_tag(const Dims& d, const double* q, const PatchDesc* desc, int np, double rthr, double cthr, int* flags,
-                cudaStream_t st)
+                cudaStream_t st, double* minmax)
 {
-    if (np > 0) k_tag<<<np, 128, 0, st>>>(q, desc, d.mx, d.my, d.mbc, d.meqn, rthr, cthr, flags);
+    if (np > 0) k_tag<<<np, 128, 0, st>>>(q, desc, d.mx, d.my, d.mbc, d.meqn, rthr, cthr, flags, minmax);
 }
 void launch_repop(const Dims& d, const RepopOp* ops, int nops, const double* oq, double* nq, const double* oqlast,
-                  double* nqlast, const double* oqi, double* nqi, const double* oregs, double* nregs, cudaStream_t st)
+                  double* nqlast, const double* oqi, double* nqi, const double* oregs, double* nregs,
+                  const double* oarea, const double* narea, cudaStream_t st)
 {
     if (nops > 0)
         k_repop<<<nops, 256, 0, st>>>(ops, d.mx, d.my, d.mbc, d.meqn, d.nreg(), oq, nq, oqlast, nqlast, oqi, nqi,
-                                      oregs, nregs);
+                                      oregs, nregs, oarea, narea);
 }
 
 }  // namespace fcb

@@ -397,6 +397,30 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
         tflag[k] = fl;
     };
 
+    // clawpack46_fix_corners (clawpack46_step2.f:242-310): at a corner of the
+    // cubed sphere (three blocks meet, no corner neighbour) the mbc x mbc corner
+    // ghost cells take rotated copies of face ghost cells before each sweep
+    // (sweep 0: x, 1: y).  Sources are face ghost cells, never corner cells, so
+    // the copies are independent.
+    const int bcc = (pd.flags / PATCH_BCC3) & 15;
+    auto fix_corners = [&](int sweep) {
+        for (int t = tid; t < 4 * MBC * MBC * MEQN; t += NT) {
+            const int m = t / (4 * MBC * MBC), r = t % (4 * MBC * MBC);
+            const int k = r / (MBC * MBC), ibc = 1 + (r % (MBC * MBC)) / MBC, jbc = 1 + r % MBC;
+            if (!((bcc >> k) & 1)) continue;
+            const int i1 = (k & 1) ? MX + ibc : 1 - ibc, j1 = (k & 2) ? MY + jbc : 1 - jbc;
+            // int(ihat - jhat), int(ihat + jhat) with ihat = 0.5 or mx + 0.5, jhat = 0.5 or my + 0.5
+            const int ih = (k & 1) ? MX : 0, jh = (k & 2) ? MY : 0;
+            const int dmi = ih - jh, dpl = ih + jh + 1;
+            const bool use_b = (sweep == 0 && (k == 0 || k == 3)) || (sweep == 1 && (k == 1 || k == 2));
+            const int id = use_b ? j1 + dmi : -j1 + dpl, jd = use_b ? -i1 + dpl : i1 - dmi;
+            const int dst = m * NXY + (j1 + MBC - 1) * NX + (i1 + MBC - 1);
+            const int src = m * NXY + (jd + MBC - 1) * NX + (id + MBC - 1);
+            Qs[dst] = Qs[src];
+            if (F32) Qf[dst] = Qf[src];
+        }
+    };
+
     // cell fluxes for the FP64 remainder of the Godunov split
     auto cell_fluxes = [&](int ixy) {
         if constexpr (G::USE_FLX) {
@@ -545,6 +569,7 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
 
     // =================== x-sweeps (clawpack46_step2.f:113-167) ===================
     State st;
+    if (bcc) { fix_corners(0); __syncthreads(); }
     cell_fluxes(1);
     if constexpr (RP::EXACT64 && F32) __syncthreads();   // the exact solver reads the cell fluxes
     {
@@ -556,6 +581,7 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
     if (REG) { if (tid < G::NIX) x2(tid, st); }
     else for (int k = tid; k < G::NIX; k += NT) { restore(k, st); x2(k, st); }
     __syncthreads();
+    if (bcc) { fix_corners(1); __syncthreads(); }
     // X3 and the y-sweep normal solves touch disjoint data: one phase
     for (int c = tid; c < NXY; c += NT) x3(c);
     cell_fluxes(2);
@@ -613,6 +639,12 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
                 v = v - (dtdx * (FMs[b + c + 1] - FPs[b + c]) + dtdy * (GMs[b + c + NX] - GPs[b + c])) /
                             As[(mcapa - 1) * NXY + c];
             qg[k] = v;
+        } else if (bcc) {
+            // cells the update skips keep the step's (corner-fixed) values, as the
+            // reference fixes the corners of q in place
+            const int kx = ic >= MX + MBC ? 1 : (ic < MBC ? 0 : -1);
+            const int ky = jc >= MY + MBC ? 1 : (jc < MBC ? 0 : -1);
+            if (kx >= 0 && ky >= 0 && ((bcc >> (kx + 2 * ky)) & 1)) qg[k] = Qs[k];
         }
     }
 

@@ -15,6 +15,8 @@ struct Dims {
     int naux() const { return nxy() * maux; }
     // conservation registers per patch (fclaw2d_clawpatch_conservation.h:56-77)
     int nreg() const { return 4 * my * meqn + 4 * mx * meqn + 4 * my * meqn + 4 * mx * meqn; }
+    // cell areas of a manifold patch cover -mbc..mx+mbc+1 (one ring more than q)
+    int narea() const { return (mx + 2 * mbc + 2) * (my + 2 * mbc + 2); }
 };
 
 // ---- fused update (k_step2_<precision>_<family>.cu) ---------------------------
@@ -41,13 +43,19 @@ const Step2Variant* step2_table_f32w_euler(int* n);
 // ---- ghost fill (k_amr.cu) ----------------------------------------------------
 // Gather tables: offsets are absolute indices of field 0 in the q slab; fields
 // follow at +m*nxy.
-struct CopyEnt { int dst, src; };                  // copy / average (src = first child)
+struct CopyEnt { int dst, src; };                  // copy
+// average: the four fine cells of a coarse cell, src, src+sx, src+sy, src+sx+sy, are the
+// children at (0,0), (1,0), (0,1), (1,1) of the coarse cell's own (x, y) axes
+struct AvgEnt { int dst, src, sx, sy; };
 struct InterpEnt { int dst, src, sub, pad; };      // sub = child position 0..3 (ii + 2 jj)
 struct PhysEnt { int dst, src, neg, cst; };        // neg: bit m set => negate field m; cst: constant state
 
 void launch_copy(const Dims& d, double* dst, const double* src, const CopyEnt* e, int n, cudaStream_t st);
 void launch_restore_patches(const Dims& d, double* dst, const double* src, const int* slots, int n, cudaStream_t st);
-void launch_average(const Dims& d, double* dst, const double* src, const CopyEnt* e, int n, cudaStream_t st);
+// area: per-patch cell areas (nxy per patch, q's cell indexing) for the area-weighted
+// average of a manifold, or null for the plain mean.
+void launch_average(const Dims& d, double* dst, const double* src, const AvgEnt* e, int n, const double* area,
+                    cudaStream_t st);
 void launch_interp(const Dims& d, double* dst, const double* src, const InterpEnt* e, int n, cudaStream_t st);
 void launch_phys(const Dims& d, double* q, const PhysEnt* e, int n, const double* bcstate, cudaStream_t st);
 void launch_timeinterp(const Dims& d, const double* q, const double* qlast, double* qinterp,
@@ -71,11 +79,14 @@ void launch_reset_sync(const Dims& d, double* regs, const PatchDesc* desc, int p
                        cudaStream_t st);
 
 // ---- diagnostics / regrid (k_amr.cu) -------------------------------------------
+// area (manifold, else null): the cell areas weight q instead of dx dy
 void launch_patch_mass(const Dims& d, const double* q, const PatchDesc* desc, int np, double* out,
-                       cudaStream_t st);
+                       cudaStream_t st, const double* area = nullptr);
 // flags[p] bit0: some interior cell exceeds refine threshold, bit1: no cell exceeds coarsen threshold
+// (gradient criterion).  With minmax (2 doubles per patch) the minmax criterion: the range of
+// field 1 over the padded patch into minmax, bit0 = range > refine_thr, coarsening decided by the caller.
 void launch_tag(const Dims& d, const double* q, const PatchDesc* desc, int np, double refine_thr,
-                double coarsen_thr, int* flags, cudaStream_t st);
+                double coarsen_thr, int* flags, cudaStream_t st, double* minmax = nullptr);
 // Repopulation after adapt: op kind 0 copy old slot, 1 interpolate2fine from old parent (igrid),
 // 2 average2coarse from 4 old children (src = first child slot; children consecutive by igrid
 // via child_slots).
@@ -105,8 +116,20 @@ void launch_sample_interfaces(const Dims& d, const double* q, int np, double gam
                               double* prim, cudaStream_t st);
 
 struct RepopOp { int kind, dst, src, igrid; int child[4]; };
+// oarea/narea (cubed sphere, else null): old and new cell areas -- interpolate2fine then
+// keeps each coarse cell's mass (fixcapaq2) and average2coarse weights by area.
 void launch_repop(const Dims& d, const RepopOp* ops, int nops, const double* oq, double* nq,
                   const double* oqlast, double* nqlast, const double* oqi, double* nqi,
-                  const double* oregs, double* nregs, cudaStream_t st);
+                  const double* oregs, double* nregs, const double* oarea, const double* narea, cudaStream_t st);
+
+// ---- cubed-sphere metric (k_metric.cu) ----------------------------------------
+// kind 0: areas from scratch; 1: copy of old slot src[0]; 2: from the four old fine
+// slots src[0..3] (igrid order) in cells 0..mx+1, from scratch elsewhere.
+struct MetricOp { int kind, dst; int src[4]; };
+struct SphereFlow { double axis[3]; double omega; };   // psi = omega (axis . x)
+// Areas of every op's patch into narea, then kappa and edge velocities into aux for
+// ops of kind 0 and 2.  desc: the new forest's descriptors.
+void launch_sphere_metric(const Dims& d, const MetricOp* ops, int nops, const PatchDesc* desc, int maxlevel,
+                          const double* oarea, double* narea, double* aux, const SphereFlow& flow, cudaStream_t st);
 
 }  // namespace fcb

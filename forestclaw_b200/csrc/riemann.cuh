@@ -64,6 +64,47 @@ struct RPAdvection {
 };
 
 // ---------------------------------------------------------------------------
+// Scalar advection on a manifold: aux = (capacity kappa, x-edge normal velocity,
+// y-edge normal velocity), the edge velocities scaled by the edge length (psi
+// differences).  applications/clawpack/advection/2d/all/clawpack46_rpn2adv_manifold.f,
+// clawpack46_rpt2adv_manifold.f
+// ---------------------------------------------------------------------------
+struct RPAdvectionManifold {
+    static constexpr int MEQN = 1, MWAVES = 1, MAUX = 3, NEXTRA = 1;
+    static constexpr bool CONS_FLUX = false, EXACT64 = false;
+    __device__ static void flux64(int ixy, const double* q, double grav, double* f) { (void)ixy; (void)grav; f[0] = q[0]; }
+    __device__ static void godunov64(int ixy, const double* qL, const double* qR, const double* aL, const double* aR,
+                                     const double* fL, const double* fR, const float* ap32, double* am, double* ap,
+                                     double grav)
+    {
+        (void)aL; (void)fL; (void)fR; (void)ap32; (void)grav;
+        const double s = aR[ixy], d = qR[0] - qL[0];
+        am[0] = dmin1(s, 0.0) * d;
+        ap[0] = dmax1(s, 0.0) * d;
+    }
+    template <typename T>
+    __device__ static void rpn2(int ixy, const T* qL, const T* qR, const T* auxL, const T* auxR,
+                                T wave[MWAVES][MEQN], T s[MWAVES], T amdq[MEQN], T apdq[MEQN],
+                                T extra[NEXTRA], T grav)
+    {
+        (void)auxL; (void)grav; (void)extra;
+        wave[0][0] = qR[0] - qL[0];                 // ql(i) - qr(i-1)
+        s[0] = auxR[ixy];                           // auxl(i, 1 + ixy)
+        amdq[0] = dmin1(s[0], T(0)) * wave[0][0];
+        apdq[0] = dmax1(s[0], T(0)) * wave[0][0];
+    }
+    template <typename T>
+    __device__ static void rpt2(int ixy, int imp, const T* qL, const T* qR, const T* aux1, const T* aux2,
+                                const T* aux3, const T extra[NEXTRA], const T* asdq, T* bm, T* bp, T grav, T drytol)
+    {
+        (void)imp; (void)qL; (void)qR; (void)aux1; (void)extra; (void)grav; (void)drytol;
+        const int iface = 3 - ixy;                  // aux(i1, iface + 1)
+        bm[0] = dmin1(aux2[iface], T(0)) * asdq[0];
+        bp[0] = dmax1(aux3[iface], T(0)) * asdq[0];
+    }
+};
+
+// ---------------------------------------------------------------------------
 // Shallow water, Roe solver with Harten-Hyman entropy fix.
 // applications/clawpack/shallow/2d/rp/clawpack46_rpn2.f:1-247, clawpack46_rpt2.f:248-321
 // extra = Roe averages (u, v, a) of the interface (the common block /comroe/).

@@ -4,8 +4,8 @@ from __future__ import annotations
 
 import math
 
-from . import (APP_RADIALDAM, APP_SHOCKBUBBLE, APP_SWIRL, APP_TSUNAMI, RP_ADVECTION, RP_EULER_EXACT, RP_SW_FWAVE,
-               RP_SW_ROE)
+from . import (APP_RADIALDAM, APP_SHOCKBUBBLE, APP_SPHERE, APP_SWIRL, APP_TSUNAMI, RP_ADVECTION,
+               RP_ADVECTION_MANIFOLD, RP_EULER_EXACT, RP_SW_FWAVE, RP_SW_ROE)
 
 # applications/clawpack/advection/2d/swirl: MC limiter, T = 8 (velocity factor cos(pi t / 4))
 SWIRL = dict(meqn=1, maux=2, mwaves=1, mthlim=(4,), rp=RP_ADVECTION, app=APP_SWIRL, tperiod=8.0,
@@ -28,6 +28,17 @@ SHOCKBUBBLE = dict(meqn=4, maux=0, mwaves=3, mthlim=(4, 4, 4), rp=RP_EULER_EXACT
                    mthbc=(0, 1, 3, 3), ax=0.0, bx=2.0, ay=0.0, by=1.0, mi=2, mj=1, x0=0.5, y0=0.5, r0=0.2,
                    gamma=1.4, mach=1.22, rhob=0.138, newton_tol=1e-10, refine_threshold=0.05,
                    coarsen_threshold=0.01)
+
+
+# applications/clawpack/advection/2d/sphere on the cubed sphere (6 blocks, manifold metric):
+# solid-body rotation about the axis (0, cos 45, sin 45) (the y axis tilted 45 degrees
+# toward z), one revolution per unit time (omega = 2 pi); q = 0.1 + two Gaussians of width
+# 0.1 rad centred on the rotation's equator at (1, 0, 0) and (0, cos 45, -sin 45);
+# minmax tagging with the reference app's thresholds 0.25 / 0.05, MC limiter, capacity.
+_C45 = math.sqrt(0.5)
+SPHERE = dict(meqn=1, maux=3, mwaves=1, mthlim=(4,), rp=RP_ADVECTION_MANIFOLD, app=APP_SPHERE, mcapa=1,
+              mthbc=(1, 1, 1, 1), refine_threshold=0.25, coarsen_threshold=0.05,
+              pdata=(0.0, _C45, _C45, 2.0 * math.pi, 1.0, 0.0, 0.0, 0.0, _C45, -_C45, 0.1, 0.1))
 
 
 def options(problem: dict, **kw):

@@ -35,6 +35,8 @@ extern "C" {
 #define FC2D_B200_RP_SW_ROE      1   /* shallow/2d/rp/clawpack46_rpn2.f / clawpack46_rpt2.f (Roe + HH fix) */
 #define FC2D_B200_RP_SW_FWAVE    2   /* shallow/2d/rp/rpn2_tsunami.f90 / rpt2_tsunami.f90 (f-waves, bathymetry) */
 #define FC2D_B200_RP_EULER_EXACT 3   /* Euler, exact Riemann solver (Newton on p*) + clawpack46_rpt2_euler4.f transverse */
+#define FC2D_B200_RP_ADVECTION_MANIFOLD 4   /* advection/2d/all/clawpack46_rpn2adv_manifold.f / _rpt2adv_manifold.f
+                                               (aux = capacity, x-edge and y-edge normal velocities) */
 
 /* Built-in application callbacks (qinit / setaux / b4step2 / tagging). */
 #define FC2D_B200_APP_NONE       0   /* q and aux supplied by the caller */
@@ -42,6 +44,9 @@ extern "C" {
 #define FC2D_B200_APP_RADIALDAM  2   /* shallow/2d/radialdam (cell-centre disc) */
 #define FC2D_B200_APP_TSUNAMI    3   /* bathymetry + Gaussian bumps */
 #define FC2D_B200_APP_SHOCKBUBBLE 4  /* euler/2d/shockbubble: Mach-M shock, light bubble, inflow on the left */
+#define FC2D_B200_APP_SPHERE     5   /* advection/2d/sphere: cubed sphere (6 blocks, manifold metric on the device),
+                                        solid-body rotation, two Gaussians; pdata = axis[3], omega, centre 1[3],
+                                        centre 2[3], width, background; minmax tagging */
 
 /* Arithmetic of the update kernel. */
 #define FC2D_B200_PREC_FP64      0   /* FP64 throughout, no FMA contraction (bitwise with the FP64 CPU path) */

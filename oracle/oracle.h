@@ -31,7 +31,8 @@ enum {
     ORC_RP_ADVECTION = 0,     /* applications/clawpack/advection/2d/all/clawpack46_rpn2adv.f, rpt2adv.f */
     ORC_RP_SW_ROE = 1,        /* applications/clawpack/shallow/2d/rp/clawpack46_rpn2.f, clawpack46_rpt2.f */
     ORC_RP_SW_FWAVE = 2,      /* applications/clawpack/shallow/2d/rp/rpn2_tsunami.f90, rpt2_tsunami.f90 */
-    ORC_RP_EULER_EXACT = 3    /* build-originated exact Euler solver (no reference counterpart) */
+    ORC_RP_EULER_EXACT = 3,   /* build-originated exact Euler solver (no reference counterpart) */
+    ORC_RP_ADVECTION_MANIFOLD = 4   /* applications/clawpack/advection/2d/all/clawpack46_rpn2adv_manifold.f, _rpt2adv_manifold.f */
 };
 
 /* Problem (app) identifiers: qinit/b4step2/setprob of the reference apps. */
@@ -40,7 +41,8 @@ enum {
     ORC_PROB_RADIALDAM = 1,   /* applications/clawpack/shallow/2d/radialdam */
     ORC_PROB_UNIFORM_SW = 2,  /* radial dam initial data on a uniform grid (same app) */
     ORC_PROB_TSUNAMI = 3,     /* batched bathymetry problem (rpn2_tsunami) */
-    ORC_PROB_SHOCKBUBBLE = 4  /* applications/clawpack/euler/2d/shockbubble (Mach-M shock, light bubble) */
+    ORC_PROB_SHOCKBUBBLE = 4, /* applications/clawpack/euler/2d/shockbubble (Mach-M shock, light bubble) */
+    ORC_PROB_SPHERE = 5       /* applications/clawpack/advection/2d/sphere on the cubed sphere (6 blocks) */
 };
 
 typedef struct orc_config {

@@ -95,6 +95,9 @@ static void patch_alloc(orc_sim* s, orc_patch* P)
     P->qlast = (double*)calloc(s->nq, sizeof(double));
     P->qinterp = c->subcycle ? (double*)calloc(s->nq, sizeof(double)) : NULL;
     P->aux = c->maux > 0 ? (double*)calloc(s->naux, sizeof(double)) : NULL;
+    P->area = c->problem == ORC_PROB_SPHERE
+                  ? (double*)calloc((size_t)(c->mx + 2 * c->mbc + 2) * (c->my + 2 * c->mbc + 2), sizeof(double))
+                  : NULL;
     const int mx = c->mx, my = c->my, meqn = c->meqn;
     size_t n = 0;
     n += 2 * (size_t)my * meqn * 2 + 2 * (size_t)mx * meqn * 2;   /* fp fm gp gm */
@@ -113,8 +116,8 @@ static void patch_alloc(orc_sim* s, orc_patch* P)
 
 static void patch_free(orc_patch* P)
 {
-    free(P->q); free(P->qlast); free(P->qinterp); free(P->aux); free(P->regs.mem);
-    P->q = P->qlast = P->qinterp = P->aux = NULL; P->regs.mem = NULL;
+    free(P->q); free(P->qlast); free(P->qinterp); free(P->aux); free(P->regs.mem); free(P->area);
+    P->q = P->qlast = P->qinterp = P->aux = P->area = NULL; P->regs.mem = NULL;
 }
 
 /* clawpatch_define (fclaw2d_clawpatch.cpp:192-...) geometry + time_sync_setup
@@ -128,12 +131,13 @@ static void patch_geometry(orc_sim* s, orc_patch* P)
     double w = 1.0 / (double)(1 << l);
     double xl = ix * w, yl = iy * w, xu = (ix + 1) * w, yu = (iy + 1) * w;
     double xlo, ylo, xup, yup;
-    if (c->mi == 1 && c->mj == 1) { xlo = xl; ylo = yl; xup = xu; yup = yu; }
+    const int sphere = c->problem == ORC_PROB_SPHERE;   /* six blocks [0,1]^2, gx = block 2^l + ix */
+    if ((c->mi == 1 && c->mj == 1) || sphere) { xlo = xl; ylo = yl; xup = xu; yup = yu; }
     else {
         xlo = (double)(bx + xl) / c->mi; xup = (double)(bx + xu) / c->mi;
         ylo = (double)(by + yl) / c->mj; yup = (double)(by + yu) / c->mj;
     }
-    P->block = brick_block(c, bx, by);
+    P->block = sphere ? bx : brick_block(c, bx, by);
     P->xlower = c->ax + (c->bx - c->ax) * xlo;
     double xupper = c->ax + (c->bx - c->ax) * xup;
     P->ylower = c->ay + (c->by - c->ay) * ylo;
@@ -175,19 +179,22 @@ static void set_neighbors(orc_sim* s)
         int l = P->level;
         P->has_fine_nbr = 0; P->on_cf = 0;
         for (int f = 0; f < 4; f++) {
-            int nx = P->gx + FDX[f], ny = P->gy + FDY[f];
+            int nx, ny;
             P->face_nbr[f][0] = P->face_nbr[f][1] = -1;
-            P->phys[f] = (nx < 0 || ny < 0 || nx >= (s->cfg.mi << l) || ny >= (s->cfg.mj << l));
+            P->phys[f] = orc_step(s, l, P->gx, P->gy, FDX[f], FDY[f], &nx, &ny) != 1;
             if (P->phys[f]) { P->face_type[f] = NB_BOUNDARY; continue; }
             int k = lookup(s, l, nx, ny);
             if (k >= 0) { P->face_type[f] = NB_SAME; P->face_nbr[f][0] = k; continue; }
             k = lookup(s, l - 1, nx >> 1, ny >> 1);
             if (k >= 0) { P->face_type[f] = NB_DOUBLE; P->face_nbr[f][0] = k; P->on_cf = 1; continue; }
+            /* the two half-size leaves: our children along face f, one step across it */
             int c0x, c0y, c1x, c1y;
-            if (f == 0) { c0x = 2 * nx + 1; c0y = 2 * ny; c1x = 2 * nx + 1; c1y = 2 * ny + 1; }
-            else if (f == 1) { c0x = 2 * nx; c0y = 2 * ny; c1x = 2 * nx; c1y = 2 * ny + 1; }
-            else if (f == 2) { c0x = 2 * nx; c0y = 2 * ny + 1; c1x = 2 * nx + 1; c1y = 2 * ny + 1; }
-            else { c0x = 2 * nx; c0y = 2 * ny; c1x = 2 * nx + 1; c1y = 2 * ny; }
+            {
+                int ax = 2 * P->gx + (f == 1), ay = 2 * P->gy + (f == 3);
+                int bx2 = ax + (f >= 2), by2 = ay + (f < 2);
+                orc_step(s, l + 1, ax, ay, FDX[f], FDY[f], &c0x, &c0y);
+                orc_step(s, l + 1, bx2, by2, FDX[f], FDY[f], &c1x, &c1y);
+            }
             int a = lookup(s, l + 1, c0x, c0y), b = lookup(s, l + 1, c1x, c1y);
             if (a < 0 || b < 0) { fprintf(stderr, "oracle: unbalanced forest at face\n"); abort(); }
             P->face_type[f] = NB_HALF; P->face_nbr[f][0] = a; P->face_nbr[f][1] = b;
@@ -199,10 +206,19 @@ static void set_neighbors(orc_sim* s)
             P->bcc[c] = 0;
             if (P->phys[f0] || P->phys[f1]) continue;
             int dx = (c & 1) ? 1 : -1, dy = (c & 2) ? 1 : -1;
-            int nx = P->gx + dx, ny = P->gy + dy;
+            int nx, ny;
+            if (orc_step(s, l, P->gx, P->gy, dx, dy, &nx, &ny) < 0) {
+                /* cube corner: three blocks meet, no corner neighbour (corner_neighbors.c case 4) */
+                P->bcc[c] = 3;
+                continue;
+            }
             int k = lookup(s, l, nx, ny);
             if (k >= 0) { P->has_corner[c] = 1; P->corner_type[c] = NB_SAME; P->corner_nbr[c] = k; continue; }
-            k = lookup(s, l + 1, 2 * nx + (dx < 0), 2 * ny + (dy < 0));
+            {
+                int fx, fy;
+                orc_step(s, l + 1, 2 * P->gx + (dx > 0), 2 * P->gy + (dy > 0), dx, dy, &fx, &fy);
+                k = lookup(s, l + 1, fx, fy);
+            }
             if (k >= 0) {
                 P->has_corner[c] = 1; P->corner_type[c] = NB_HALF; P->corner_nbr[c] = k;
                 P->has_fine_nbr = 1; P->on_cf = 1; continue;
@@ -573,8 +589,8 @@ static int balance(const orc_sim* s, leaf_t** Lp, int n)
             for (int dy = -1; dy <= 1; dy++)
                 for (int dx = -1; dx <= 1; dx++) {
                     if (!dx && !dy) continue;
-                    int x = L[i].gx + dx, y = L[i].gy + dy;
-                    if (x < 0 || y < 0 || x >= (s->cfg.mi << l) || y >= (s->cfg.mj << l)) continue;
+                    int x, y;
+                    if (orc_step(s, l, L[i].gx, L[i].gy, dx, dy, &x, &y) != 1) continue;
                     for (int k = l - 2; k >= 0; k--) {
                         if (lset_has(&h, k, x >> (l - k), y >> (l - k))) {
                             int j = leaf_find(L, n, k, x >> (l - k), y >> (l - k));
@@ -659,11 +675,14 @@ static int adapt(orc_sim* s, const int* mark, int domain_init)
         }
         patch_alloc(s, Q);
         patch_geometry(s, Q);
+        const int sphere = s->cfg.problem == ORC_PROB_SPHERE;
         int parent = lookup(s, Q->level - 1, Q->gx >> 1, Q->gy >> 1);
         if (parent >= 0) {                                /* HALFSIZE: new fine patch */
+            if (sphere) orc_sphere_area(s, Q, 0);         /* fclaw2d_metric_patch_build */
             orc_setaux(s, Q);
             if (domain_init) orc_qinit(s, Q);
-            else orc_interpolate2fine(s, s->p[parent].q, Q->q, (Q->gx & 1) + 2 * (Q->gy & 1));
+            else orc_interpolate2fine(s, s->p[parent].q, Q->q, (Q->gx & 1) + 2 * (Q->gy & 1),
+                                      s->p[parent].area, Q->area);
             continue;
         }
         int ch[4], all = 1;
@@ -672,9 +691,13 @@ static int adapt(orc_sim* s, const int* mark, int domain_init)
             if (ch[c] < 0) all = 0;
         }
         if (all) {                                        /* DOUBLESIZE: new coarse patch */
+            if (sphere) {                                 /* fclaw2d_metric_patch_build_from_fine */
+                for (int c = 0; c < 4; c++) orc_sphere_area_from_fine(s, Q, &s->p[ch[c]], c);
+                orc_sphere_area(s, Q, 1);
+            }
             orc_setaux(s, Q);
             if (domain_init) orc_qinit(s, Q);
-            else for (int c = 0; c < 4; c++) orc_average2coarse(s, Q->q, s->p[ch[c]].q, c);
+            else for (int c = 0; c < 4; c++) orc_average2coarse(s, Q->q, s->p[ch[c]].q, c, Q->area, s->p[ch[c]].area);
             continue;
         }
         fprintf(stderr, "oracle: adapt produced a patch more than one level from the old forest\n");
@@ -729,6 +752,7 @@ orc_sim* orc_create(const orc_config* cfg)
     s->cfg = *cfg;
     if (s->cfg.mi <= 0) s->cfg.mi = 1;
     if (s->cfg.mj <= 0) s->cfg.mj = 1;
+    if (s->cfg.problem == ORC_PROB_SPHERE) { s->cfg.mi = 6; s->cfg.mj = 1; }
     s->nx = cfg->mx + 2 * cfg->mbc;
     s->ny = cfg->my + 2 * cfg->mbc;
     s->nq = (size_t)s->nx * s->ny * cfg->meqn;
@@ -771,7 +795,11 @@ int orc_initialize(orc_sim* s)
             patch_geometry(s, P);
         }
     forest_finalize(s);
-    for (int i = 0; i < s->np; i++) { orc_setaux(s, &s->p[i]); orc_qinit(s, &s->p[i]); }
+    for (int i = 0; i < s->np; i++) {
+        if (c->problem == ORC_PROB_SPHERE) orc_sphere_area(s, &s->p[i], 0);
+        orc_setaux(s, &s->p[i]);
+        orc_qinit(s, &s->p[i]);
+    }
     if (c->minlevel < c->maxlevel)
         for (int lev = c->minlevel; lev <= c->maxlevel; lev++)
             if (!regrid_impl(s, 1)) break;
@@ -858,6 +886,8 @@ void orc_mass(const orc_sim* s, double* out)
                 double area = P->dx * P->dy;
                 for (int j = 1; j <= my; j++)
                     for (int i = 1; i <= mx; i++) {
+                        /* manifold: area(i,j) (diagnostics.f:40-42) */
+                        if (P->area) area = P->area[ORC_AIDX(i, j, mbc, mx + 2 * mbc + 2)];
                         double y = P->q[QIDX(i, j, m, mbc, nx, ny)] * area - comp;
                         double t = sum + y;
                         comp = (t - sum) - y;

@@ -27,6 +27,7 @@ typedef struct orc_patch {
     int level, block, gx, gy;         /* gx, gy: brick-global integer coords at `level` */
     double xlower, ylower, dx, dy;
     double *q, *qlast, *qinterp, *aux;
+    double* area;                     /* cubed sphere: cell areas, -mbc..mx+mbc+1 in both directions */
     orc_regs regs;
     int face_type[4];
     int face_nbr[4][2];               /* 1 (same/double) or 2 (half) neighbour indices */
@@ -65,8 +66,11 @@ void orc_average_face(const orc_sim* s, double* qc, const double* qf, const orc_
 void orc_average_corner(const orc_sim* s, double* qc, const double* qf, const orc_patch* C, const orc_patch* F, int icorner);
 void orc_interpolate_face(const orc_sim* s, const double* qc, double* qf, const orc_patch* C, const orc_patch* F, int iface_coarse);
 void orc_interpolate_corner(const orc_sim* s, const double* qc, double* qf, const orc_patch* C, const orc_patch* F, int icorner);
-void orc_interpolate2fine(const orc_sim* s, const double* qcoarse, double* qfine, int igrid);
-void orc_average2coarse(const orc_sim* s, double* qcoarse, const double* qfine, int igrid);
+/* acoarse / afine: cell areas on a manifold (fixcapaq2 / area weights), else NULL */
+void orc_interpolate2fine(const orc_sim* s, const double* qcoarse, double* qfine, int igrid,
+                          const double* acoarse, const double* afine);
+void orc_average2coarse(const orc_sim* s, double* qcoarse, const double* qfine, int igrid,
+                        const double* acoarse, const double* afine);
 void orc_timeinterp(const orc_sim* s, const double* qcurr, const double* qlast, double* qinterp, double alpha);
 void orc_time_sync_f2c(const orc_sim* s, orc_patch* C, const orc_patch* F, int iface_coarse);
 void orc_time_sync_samesize(const orc_sim* s, orc_patch* P, const orc_patch* N, int this_iface);
@@ -74,6 +78,19 @@ void orc_store_flux(const orc_sim* s, orc_patch* P, double dt);
 void orc_accumulate_waves(const orc_sim* s, orc_patch* P, double dt, double dx, double dy,
                           const double* fp, const double* fm, const double* gp, const double* gm);
 void orc_regs_reset_face(const orc_sim* s, orc_patch* P, int k);
+
+/* cubed sphere (orc_sphere.c) */
+double orc_tan(double x);
+void orc_cs_map(int block, double xc, double yc, double* xp, double* yp, double* zp);
+int  orc_cs_nb(int b, int f);
+int  orc_step(const orc_sim* s, int l, int x, int y, int dx, int dy, int* ox, int* oy);
+void orc_xf_same(const orc_sim* s, const orc_patch* P, const orc_patch* N, int i, int j, int* i2, int* j2);
+void orc_xf_half(const orc_sim* s, const orc_patch* C, const orc_patch* F, int ic, int jc, int* i2, int* j2);
+void orc_sphere_area(const orc_sim* s, orc_patch* P, int ghost_only);
+void orc_sphere_area_from_fine(const orc_sim* s, orc_patch* C, const orc_patch* F, int igrid);
+void orc_sphere_setaux(const orc_sim* s, orc_patch* P);
+void orc_sphere_flow(const orc_config* c, double* axis, double* omega);
+#define ORC_AIDX(i, j, mbc, ax) ((size_t)((j) + (mbc)) * (size_t)(ax) + (size_t)((i) + (mbc)))
 
 /* problems (orc_problems.c) */
 void orc_setaux(const orc_sim* s, orc_patch* P);

@@ -122,6 +122,41 @@ static void rpt2_adv(orc_rpctx* ctx, int ixy, int maxm, int meqn, int mwaves, in
     }
 }
 
+/* applications/clawpack/advection/2d/all/clawpack46_rpn2adv_manifold.f: speed aux(i, 1 + ixy). */
+static void rpn2_adv_manifold(orc_rpctx* ctx, int ixy, int maxm, int meqn, int mwaves, int maux, int mbc, int mx,
+                              const double* ql, const double* qr, const double* auxl, const double* auxr,
+                              double* wave, double* s, double* amdq, double* apdq)
+{
+    (void)ctx; (void)maux; (void)auxr; (void)mwaves;
+    const int L = maxm + 2 * mbc;
+    for (int i = 2 - mbc; i <= mx + mbc; i++) {
+        for (int m = 1; m <= meqn; m++)
+            wave[I1(i) + (m - 1) * L] = ql[I1(i) + (m - 1) * L] - qr[I1(i - 1) + (m - 1) * L];
+        s[I1(i)] = auxl[I1(i) + ixy * L];
+        for (int m = 1; m <= meqn; m++) {
+            amdq[I1(i) + (m - 1) * L] = dmin1(s[I1(i)], 0.0) * wave[I1(i) + (m - 1) * L];
+            apdq[I1(i) + (m - 1) * L] = dmax1(s[I1(i)], 0.0) * wave[I1(i) + (m - 1) * L];
+        }
+    }
+}
+
+/* applications/clawpack/advection/2d/all/clawpack46_rpt2adv_manifold.f: aux(i1, iface + 1), iface = 3 - ixy. */
+static void rpt2_adv_manifold(orc_rpctx* ctx, int ixy, int maxm, int meqn, int mwaves, int maux, int mbc, int mx,
+                              const double* ql, const double* qr, const double* aux1, const double* aux2,
+                              const double* aux3, int imp, const double* asdq, double* bmasdq, double* bpasdq)
+{
+    (void)ctx; (void)mwaves; (void)maux; (void)ql; (void)qr; (void)aux1;
+    const int L = maxm + 2 * mbc;
+    const int iface = 3 - ixy;
+    for (int i = 2 - mbc; i <= mx + mbc; i++) {
+        int i1 = i - 2 + imp;
+        for (int m = 1; m <= meqn; m++) {
+            bmasdq[I1(i) + (m - 1) * L] = dmin1(aux2[I1(i1) + iface * L], 0.0) * asdq[I1(i) + (m - 1) * L];
+            bpasdq[I1(i) + (m - 1) * L] = dmax1(aux3[I1(i1) + iface * L], 0.0) * asdq[I1(i) + (m - 1) * L];
+        }
+    }
+}
+
 /* applications/clawpack/shallow/2d/rp/clawpack46_rpn2.f:1-247 (Roe + Harten-Hyman fix).
  * The Roe averages are kept in ctx (the Fortran common block /comroe/). */
 static void rpn2_sw_roe(orc_rpctx* ctx, int ixy, int maxm, int meqn, int mwaves, int maux, int mbc, int mx,
@@ -251,6 +286,7 @@ void orc_rp_select(int rp, orc_rpn2_t* rpn2, orc_rpt2_t* rpt2)
     case ORC_RP_SW_ROE:    *rpn2 = rpn2_sw_roe; *rpt2 = rpt2_sw_roe; break;
     case ORC_RP_SW_FWAVE:  *rpn2 = orc_rpn2_fwave; *rpt2 = orc_rpt2_fwave; break;
     case ORC_RP_EULER_EXACT: *rpn2 = orc_rpn2_euler; *rpt2 = orc_rpt2_euler; break;
+    case ORC_RP_ADVECTION_MANIFOLD: *rpn2 = rpn2_adv_manifold; *rpt2 = rpt2_adv_manifold; break;
     default: *rpn2 = NULL; *rpt2 = NULL; break;
     }
 }

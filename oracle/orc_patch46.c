@@ -28,30 +28,17 @@ static double compute_slopes(double sl, double sr)
     return m * fmax(0.0, copysign(1.0, sl * sr)) * copysign(1.0, sc);
 }
 
-/* Offset (in cells) of patch b's index space relative to patch a's, both at the
- * same level: a-index i maps to b-index i + shift (transform_face same-block path,
- * forestclaw2d.c:655-662, and transform_corner, :1180-1185). */
-static void same_shift(const orc_patch* a, const orc_patch* b, int mx, int my, int* si, int* sj)
-{
-    *si = (a->gx - b->gx) * mx;
-    *sj = (a->gy - b->gy) * my;
-}
-
-/* transform_face2 / transform_corner2 (coarse a -> fine b, canonical child order):
- * first child of coarse cell (i,j) is (di,dj) with di = 1 + (2*a.gx - b.gx)*mx + 2(i-1). */
-static void half_first(const orc_patch* a, const orc_patch* b, int mx, int my, int i, int j, int* di, int* dj)
-{
-    *di = 1 + (2 * a->gx - b->gx) * mx + 2 * (i - 1);
-    *dj = 1 + (2 * a->gy - b->gy) * my + 2 * (j - 1);
-}
+/* Index maps between patches (src/forestclaw2d.c:609-980, through
+ * fclaw2d_clawpatch_transform.c:81-190): orc_xf_same maps a cell of P to N's
+ * index space at the same level; orc_xf_half gives the four children of a
+ * coarse cell in the fine patch, in the coarse patch's (x, y) order.  Both go
+ * across cubed-sphere block faces (orc_sphere.c); on a brick they are shifts. */
 
 /* ---------------- copy ---------------- */
 void orc_copy_face(const orc_sim* s, double* qthis, const double* qnbr, const orc_patch* P, const orc_patch* N, int iface)
 {
     const orc_config* c = &s->cfg;
     const int mx = c->mx, my = c->my, mbc = c->mbc, meqn = c->meqn, nx = s->nx, ny = s->ny;
-    int si, sj;
-    same_shift(P, N, mx, my, &si, &sj);
     int ilo, ihi, jlo, jhi;
     if (iface == 0) { ilo = 1 - mbc; ihi = 0; jlo = 1; jhi = my; }
     else if (iface == 1) { ilo = mx + 1; ihi = mx + mbc; jlo = 1; jhi = my; }
@@ -59,84 +46,84 @@ void orc_copy_face(const orc_sim* s, double* qthis, const double* qnbr, const or
     else { ilo = 1; ihi = mx; jlo = my + 1; jhi = my + mbc; }
     for (int m = 1; m <= meqn; m++)
         for (int j = jlo; j <= jhi; j++)
-            for (int i = ilo; i <= ihi; i++)
-                qthis[QIDX(i, j, m, mbc, nx, ny)] = qnbr[QIDX(i + si, j + sj, m, mbc, nx, ny)];
+            for (int i = ilo; i <= ihi; i++) {
+                int i2, j2;
+                orc_xf_same(s, P, N, i, j, &i2, &j2);
+                qthis[QIDX(i, j, m, mbc, nx, ny)] = qnbr[QIDX(i2, j2, m, mbc, nx, ny)];
+            }
 }
 
 void orc_copy_corner(const orc_sim* s, double* qthis, const double* qnbr, const orc_patch* P, const orc_patch* N, int icorner)
 {
     const orc_config* c = &s->cfg;
     const int mx = c->mx, my = c->my, mbc = c->mbc, meqn = c->meqn, nx = s->nx, ny = s->ny;
-    int si, sj;
-    same_shift(P, N, mx, my, &si, &sj);
     for (int m = 1; m <= meqn; m++)
         for (int ibc = 1; ibc <= mbc; ibc++)
             for (int jbc = 1; jbc <= mbc; jbc++) {
                 int i1 = (icorner & 1) ? mx + ibc : 1 - ibc;
                 int j1 = (icorner & 2) ? my + jbc : 1 - jbc;
-                qthis[QIDX(i1, j1, m, mbc, nx, ny)] = qnbr[QIDX(i1 + si, j1 + sj, m, mbc, nx, ny)];
+                int i2, j2;
+                orc_xf_same(s, P, N, i1, j1, &i2, &j2);
+                qthis[QIDX(i1, j1, m, mbc, nx, ny)] = qnbr[QIDX(i2, j2, m, mbc, nx, ny)];
             }
 }
 
 /* ---------------- average ---------------- */
 static int valid_average(int i, int j, int mx, int my) { return 1 <= i && i <= mx && 1 <= j && j <= my; }
 
+/* one coarse ghost cell from its four children (average.f:96-128): the plain mean,
+ * or on a manifold sum(q_f a_f) / sum(a_f) with the fine cells' areas */
+static void average_cell(const orc_sim* s, double* qc, const double* qf, const orc_patch* F, int ic, int jc,
+                         const int* i2, const int* j2, int mq)
+{
+    const orc_config* c = &s->cfg;
+    const int mbc = c->mbc, nx = s->nx, ny = s->ny, ax = c->mx + 2 * mbc + 2;
+    if (F->area) {
+        double sum = 0, af = 0;
+        for (int m = 0; m < 4; m++) {
+            double q = qf[QIDX(i2[m], j2[m], mq, mbc, nx, ny)];
+            double kf = F->area[ORC_AIDX(i2[m], j2[m], mbc, ax)];
+            sum = sum + q * kf;
+            af = af + kf;
+        }
+        qc[QIDX(ic, jc, mq, mbc, nx, ny)] = sum / af;
+        return;
+    }
+    double sum = 0;
+    for (int m = 0; m < 4; m++) sum = sum + qf[QIDX(i2[m], j2[m], mq, mbc, nx, ny)];
+    qc[QIDX(ic, jc, mq, mbc, nx, ny)] = sum / (double)4;
+}
+
 void orc_average_face(const orc_sim* s, double* qc, const double* qf, const orc_patch* C, const orc_patch* F, int iface_coarse)
 {
     const orc_config* c = &s->cfg;
-    const int mx = c->mx, my = c->my, mbc = c->mbc, meqn = c->meqn, nx = s->nx, ny = s->ny;
+    const int mx = c->mx, my = c->my, mbc = c->mbc, meqn = c->meqn;
     const int idir = iface_coarse / 2;
     for (int mq = 1; mq <= meqn; mq++) {
-        if (idir == 0) {
-            for (int jc = 1; jc <= my; jc++)
-                for (int ibc = 1; ibc <= mbc; ibc++) {
-                    int ic = (iface_coarse == 0) ? 1 - ibc : mx + ibc;
-                    int di, dj;
-                    half_first(C, F, mx, my, ic, jc, &di, &dj);
-                    if (!valid_average(di, dj, mx, my) || !valid_average(di + 1, dj + 1, mx, my)) continue;
-                    double sum = 0;
-                    sum = sum + qf[QIDX(di, dj, mq, mbc, nx, ny)];
-                    sum = sum + qf[QIDX(di + 1, dj, mq, mbc, nx, ny)];
-                    sum = sum + qf[QIDX(di, dj + 1, mq, mbc, nx, ny)];
-                    sum = sum + qf[QIDX(di + 1, dj + 1, mq, mbc, nx, ny)];
-                    qc[QIDX(ic, jc, mq, mbc, nx, ny)] = sum / (double)4;
-                }
-        } else {
-            for (int jbc = 1; jbc <= mbc; jbc++)
-                for (int ic = 1; ic <= mx; ic++) {
-                    int jc = (iface_coarse == 2) ? 1 - jbc : my + jbc;
-                    int di, dj;
-                    half_first(C, F, mx, my, ic, jc, &di, &dj);
-                    if (!valid_average(di, dj, mx, my) || !valid_average(di + 1, dj + 1, mx, my)) continue;
-                    double sum = 0;
-                    sum = sum + qf[QIDX(di, dj, mq, mbc, nx, ny)];
-                    sum = sum + qf[QIDX(di + 1, dj, mq, mbc, nx, ny)];
-                    sum = sum + qf[QIDX(di, dj + 1, mq, mbc, nx, ny)];
-                    sum = sum + qf[QIDX(di + 1, dj + 1, mq, mbc, nx, ny)];
-                    qc[QIDX(ic, jc, mq, mbc, nx, ny)] = sum / (double)4;
-                }
-        }
+        for (int a = 1; a <= (idir == 0 ? my : mbc); a++)
+            for (int b = 1; b <= (idir == 0 ? mbc : mx); b++) {
+                int ic, jc;
+                if (idir == 0) { jc = a; ic = (iface_coarse == 0) ? 1 - b : mx + b; }
+                else { ic = b; jc = (iface_coarse == 2) ? 1 - a : my + a; }
+                int i2[4], j2[4], ok = 1;
+                orc_xf_half(s, C, F, ic, jc, i2, j2);
+                for (int m = 0; m < 4; m++) ok = ok && valid_average(i2[m], j2[m], mx, my);
+                if (ok) average_cell(s, qc, qf, F, ic, jc, i2, j2, mq);
+            }
     }
 }
 
 void orc_average_corner(const orc_sim* s, double* qc, const double* qf, const orc_patch* C, const orc_patch* F, int icorner)
 {
     const orc_config* c = &s->cfg;
-    const int mx = c->mx, my = c->my, mbc = c->mbc, meqn = c->meqn, nx = s->nx, ny = s->ny;
+    const int mx = c->mx, my = c->my, mbc = c->mbc, meqn = c->meqn;
     for (int ibc = 1; ibc <= mbc; ibc++)
         for (int jbc = 1; jbc <= mbc; jbc++) {
             int i1 = (icorner & 1) ? mx + ibc : 1 - ibc;
             int j1 = (icorner & 2) ? my + jbc : 1 - jbc;
-            int di, dj;
-            half_first(C, F, mx, my, i1, j1, &di, &dj);
-            for (int mq = 1; mq <= meqn; mq++) {
-                double sum = 0;
-                sum = sum + qf[QIDX(di, dj, mq, mbc, nx, ny)];
-                sum = sum + qf[QIDX(di + 1, dj, mq, mbc, nx, ny)];
-                sum = sum + qf[QIDX(di, dj + 1, mq, mbc, nx, ny)];
-                sum = sum + qf[QIDX(di + 1, dj + 1, mq, mbc, nx, ny)];
-                qc[QIDX(i1, j1, mq, mbc, nx, ny)] = sum / (double)4;
-            }
+            int i2[4], j2[4];
+            orc_xf_half(s, C, F, i1, j1, i2, j2);
+            for (int mq = 1; mq <= meqn; mq++) average_cell(s, qc, qf, F, i1, j1, i2, j2, mq);
         }
 }
 
@@ -146,7 +133,9 @@ static int valid_interp(int i, int j, int mx, int my, int mbc)
     return 1 - mbc <= i && i <= mx + mbc && 1 - mbc <= j && j <= my + mbc;
 }
 
-static void interp_cell(const orc_sim* s, const double* qc, double* qf, int ic, int jc, int di, int dj, int mq)
+/* the four fine cells of coarse cell (ic, jc), at the children's offsets of
+ * +-1/4 in the coarse patch's axes (interpolate.f:84-95, 150-170) */
+static void interp_cell(const orc_sim* s, const double* qc, double* qf, int ic, int jc, const int* i2, const int* j2, int mq)
 {
     const int mbc = s->cfg.mbc, nx = s->nx, ny = s->ny;
     double q0 = qc[QIDX(ic, jc, mq, mbc, nx, ny)];
@@ -159,7 +148,7 @@ static void interp_cell(const orc_sim* s, const double* qc, double* qf, int ic, 
     for (int m = 0; m < 4; m++) {
         int ii = m & 1, jj = m >> 1;
         double shiftx = (ii - 0.5) / 2.0, shifty = (jj - 0.5) / 2.0;
-        qf[QIDX(di + ii, dj + jj, mq, mbc, nx, ny)] = q0 + gradx * shiftx + grady * shifty;
+        qf[QIDX(i2[m], j2[m], mq, mbc, nx, ny)] = q0 + gradx * shiftx + grady * shifty;
     }
 }
 
@@ -168,29 +157,17 @@ void orc_interpolate_face(const orc_sim* s, const double* qc, double* qf, const 
     const orc_config* c = &s->cfg;
     const int mx = c->mx, my = c->my, mbc = c->mbc, meqn = c->meqn;
     const int idir = iface_coarse / 2;
-    for (int mq = 1; mq <= meqn; mq++) {
-        if (idir == 0) {
-            for (int ibc = 1; ibc <= mbc / 2; ibc++) {
-                int ic = (iface_coarse == 0) ? ibc : mx - ibc + 1;
-                for (int jc = 1; jc <= mx; jc++) {
-                    int di, dj;
-                    half_first(C, F, mx, my, ic, jc, &di, &dj);
-                    if (!valid_interp(di, dj, mx, my, mbc) || !valid_interp(di + 1, dj + 1, mx, my, mbc)) continue;
-                    interp_cell(s, qc, qf, ic, jc, di, dj, mq);
-                }
+    for (int mq = 1; mq <= meqn; mq++)
+        for (int b = 1; b <= mbc / 2; b++)
+            for (int a = 1; a <= mx; a++) {
+                int ic, jc;
+                if (idir == 0) { ic = (iface_coarse == 0) ? b : mx - b + 1; jc = a; }
+                else { jc = (iface_coarse == 2) ? b : my - b + 1; ic = a; }
+                int i2[4], j2[4], ok = 1;
+                orc_xf_half(s, C, F, ic, jc, i2, j2);
+                for (int m = 0; m < 4; m++) ok = ok && valid_interp(i2[m], j2[m], mx, my, mbc);
+                if (ok) interp_cell(s, qc, qf, ic, jc, i2, j2, mq);
             }
-        } else {
-            for (int jbc = 1; jbc <= mbc / 2; jbc++) {
-                int jc = (iface_coarse == 2) ? jbc : my - jbc + 1;
-                for (int ic = 1; ic <= mx; ic++) {
-                    int di, dj;
-                    half_first(C, F, mx, my, ic, jc, &di, &dj);
-                    if (!valid_interp(di, dj, mx, my, mbc) || !valid_interp(di + 1, dj + 1, mx, my, mbc)) continue;
-                    interp_cell(s, qc, qf, ic, jc, di, dj, mq);
-                }
-            }
-        }
-    }
 }
 
 void orc_interpolate_corner(const orc_sim* s, const double* qc, double* qf, const orc_patch* C, const orc_patch* F, int icorner)
@@ -201,17 +178,20 @@ void orc_interpolate_corner(const orc_sim* s, const double* qc, double* qf, cons
         for (int jbc = 1; jbc <= mbc / 2; jbc++) {
             int ic = (icorner & 1) ? mx - ibc + 1 : ibc;
             int jc = (icorner & 2) ? my - jbc + 1 : jbc;
-            int di, dj;
-            half_first(C, F, mx, my, ic, jc, &di, &dj);
-            for (int mq = 1; mq <= meqn; mq++) interp_cell(s, qc, qf, ic, jc, di, dj, mq);
+            int i2[4], j2[4];
+            orc_xf_half(s, C, F, ic, jc, i2, j2);
+            for (int mq = 1; mq <= meqn; mq++) interp_cell(s, qc, qf, ic, jc, i2, j2, mq);
         }
 }
 
-/* interpolate2fine (regrid): coarse patch -> child igrid. */
-void orc_interpolate2fine(const orc_sim* s, const double* qcoarse, double* qfine, int igrid)
+/* interpolate2fine (regrid): coarse patch -> child igrid (interpolate.f:324-392); on a
+ * manifold fixcapaq2 (:409-470) then gives each coarse cell's mass back to its children. */
+void orc_interpolate2fine(const orc_sim* s, const double* qcoarse, double* qfine, int igrid,
+                          const double* acoarse, const double* afine)
 {
     const orc_config* c = &s->cfg;
     const int mx = c->mx, my = c->my, mbc = c->mbc, meqn = c->meqn, nx = s->nx, ny = s->ny;
+    const int ax = mx + 2 * mbc + 2;
     int ig = igrid % 2, jg = (igrid - ig) / 2;
     int i1 = 1 - ig, i2 = mx / 2 + (1 - ig), ic_add = ig * mx / 2;
     int j1 = 1 - jg, j2 = my / 2 + (1 - jg), jc_add = jg * my / 2;
@@ -234,13 +214,37 @@ void orc_interpolate2fine(const orc_sim* s, const double* qcoarse, double* qfine
                             q0 + shiftx * gradx + shifty * grady;
                     }
             }
+    if (!acoarse) return;
+    double r2 = 4;
+    for (int m = 1; m <= meqn; m++)
+        for (int i = 1; i <= mx / 2; i++)
+            for (int j = 1; j <= my / 2; j++) {
+                double sum = 0.0;
+                for (int ii = 1; ii <= 2; ii++)
+                    for (int jj = 1; jj <= 2; jj++) {
+                        int ifine = (i - 1) * 2 + ii, jfine = (j - 1) * 2 + jj;
+                        sum = sum + afine[ORC_AIDX(ifine, jfine, mbc, ax)] * qfine[QIDX(ifine, jfine, m, mbc, nx, ny)];
+                    }
+                double kc = acoarse[ORC_AIDX(i + ic_add, j + jc_add, mbc, ax)];
+                double qc = qcoarse[QIDX(i + ic_add, j + jc_add, m, mbc, nx, ny)];
+                double cons_diff = (qc * kc - sum) / r2;
+                for (int ii = 1; ii <= 2; ii++)
+                    for (int jj = 1; jj <= 2; jj++) {
+                        int ifine = (i - 1) * 2 + ii, jfine = (j - 1) * 2 + jj;
+                        qfine[QIDX(ifine, jfine, m, mbc, nx, ny)] =
+                            qfine[QIDX(ifine, jfine, m, mbc, nx, ny)] + cons_diff / afine[ORC_AIDX(ifine, jfine, mbc, ax)];
+                    }
+            }
 }
 
-/* average2coarse (regrid): child igrid -> coarse patch interior quarter. */
-void orc_average2coarse(const orc_sim* s, double* qcoarse, const double* qfine, int igrid)
+/* average2coarse (regrid): child igrid -> coarse patch interior quarter (average.f:282-364);
+ * on a manifold sum(kf qf) / kc with the coarse patch's (new) areas. */
+void orc_average2coarse(const orc_sim* s, double* qcoarse, const double* qfine, int igrid,
+                        const double* acoarse, const double* afine)
 {
     const orc_config* c = &s->cfg;
     const int mx = c->mx, my = c->my, mbc = c->mbc, meqn = c->meqn, nx = s->nx, ny = s->ny;
+    const int ax = mx + 2 * mbc + 2;
     int ig = igrid % 2, jg = (igrid - ig) / 2;
     int ic_add = ig * mx / 2, jc_add = jg * mx / 2;
     for (int mq = 1; mq <= meqn; mq++)
@@ -248,10 +252,30 @@ void orc_average2coarse(const orc_sim* s, double* qcoarse, const double* qfine, 
             for (int i = 1; i <= mx / 2; i++) {
                 double sum = 0;
                 for (int jj = 1; jj <= 2; jj++)
-                    for (int ii = 1; ii <= 2; ii++)
-                        sum = sum + qfine[QIDX((i - 1) * 2 + ii, (j - 1) * 2 + jj, mq, mbc, nx, ny)];
-                qcoarse[QIDX(i + ic_add, j + jc_add, mq, mbc, nx, ny)] = sum / 4;
+                    for (int ii = 1; ii <= 2; ii++) {
+                        int fi = (i - 1) * 2 + ii, fj = (j - 1) * 2 + jj;
+                        double qf = qfine[QIDX(fi, fj, mq, mbc, nx, ny)];
+                        if (acoarse) sum = sum + afine[ORC_AIDX(fi, fj, mbc, ax)] * qf;
+                        else sum = sum + qf;
+                    }
+                if (acoarse) qcoarse[QIDX(i + ic_add, j + jc_add, mq, mbc, nx, ny)] = sum / acoarse[ORC_AIDX(i + ic_add, j + jc_add, mbc, ax)];
+                else qcoarse[QIDX(i + ic_add, j + jc_add, mq, mbc, nx, ny)] = sum / 4;
             }
+}
+
+/* Brick shifts used by the time-sync corrections below (same orientation; the
+ * cubed sphere runs without time sync): transform_face same-block path
+ * (forestclaw2d.c:655-662) and transform_face2's canonical first child. */
+static void same_shift(const orc_patch* a, const orc_patch* b, int mx, int my, int* si, int* sj)
+{
+    *si = (a->gx - b->gx) * mx;
+    *sj = (a->gy - b->gy) * my;
+}
+
+static void half_first(const orc_patch* a, const orc_patch* b, int mx, int my, int i, int j, int* di, int* dj)
+{
+    *di = 1 + (2 * a->gx - b->gx) * mx + 2 * (i - 1);
+    *dj = 1 + (2 * a->gy - b->gy) * my + 2 * (j - 1);
 }
 
 /* ---------------- time interpolation ---------------- */

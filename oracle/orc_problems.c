@@ -9,6 +9,9 @@
  *               gradient criterion of fort_user/fclaw2d_clawpatch_gradient_exceeds_th.f90
  *               scaled by dx (refine where |grad h| dx exceeds the threshold)
  *   bathymetry: tsunami problem, b = -1 + 0.5 exp(-50 |x - c|^2), eta = sum of Gaussian bumps
+ *   sphere:     cubed sphere (applications/clawpack/advection/2d/sphere): metric and aux in
+ *               orc_sphere.c; q = background + exp(-(theta1/w)^2) + exp(-(theta2/w)^2) at the mapped
+ *               cell centres; minmax tagging (fort_user/fclaw2d_clawpatch_minmax_exceeds_th.f90)
  */
 #include <math.h>
 #include <string.h>
@@ -20,10 +23,31 @@ static double swirl_psi(double x, double y, double pi)
     return ((sx * sx) * (sy * sy)) / pi;
 }
 
+/* angle between unit vectors */
+static double sphere_angle(const double* x, const double* c)
+{
+    double cx = x[1] * c[2] - x[2] * c[1], cy = x[2] * c[0] - x[0] * c[2], cz = x[0] * c[1] - x[1] * c[0];
+    return atan2(sqrt(cx * cx + cy * cy + cz * cz), x[0] * c[0] + x[1] * c[1] + x[2] * c[2]);
+}
+
+/* range of field 1 over the padded patch (minmax criterion) */
+static void patch_minmax(const orc_sim* s, const orc_patch* P, double* lo, double* hi)
+{
+    const orc_config* c = &s->cfg;
+    const int mbc = c->mbc, nx = s->nx, ny = s->ny;
+    for (int j = 1 - mbc; j <= c->my + mbc; j++)
+        for (int i = 1 - mbc; i <= c->mx + mbc; i++) {
+            double v = P->q[QIDX(i, j, 1, mbc, nx, ny)];
+            *lo = fmin(*lo, v);
+            *hi = fmax(*hi, v);
+        }
+}
+
 void orc_setaux(const orc_sim* s, orc_patch* P)
 {
     const orc_config* c = &s->cfg;
     const int mx = c->mx, my = c->my, mbc = c->mbc, nx = s->nx, ny = s->ny;
+    if (c->problem == ORC_PROB_SPHERE) { orc_sphere_setaux(s, P); return; }
     if (c->problem == ORC_PROB_TSUNAMI) {
         double cx = c->pdata[0], cy = c->pdata[1];
         for (int j = 1 - mbc; j <= my + mbc; j++)
@@ -39,6 +63,17 @@ void orc_qinit(const orc_sim* s, orc_patch* P)
 {
     const orc_config* c = &s->cfg;
     const int mx = c->mx, my = c->my, mbc = c->mbc, meqn = c->meqn, nx = s->nx, ny = s->ny;
+    if (c->problem == ORC_PROB_SPHERE) {
+        double w = c->pdata[10], bg = c->pdata[11];
+        for (int j = 1 - mbc; j <= my + mbc; j++)
+            for (int i = 1 - mbc; i <= mx + mbc; i++) {
+                double x[3];
+                orc_cs_map(P->block, P->xlower + (i - 0.5) * P->dx, P->ylower + (j - 0.5) * P->dy, &x[0], &x[1], &x[2]);
+                double t1 = sphere_angle(x, &c->pdata[4]) / w, t2 = sphere_angle(x, &c->pdata[7]) / w;
+                P->q[QIDX(i, j, 1, mbc, nx, ny)] = bg + exp(-(t1 * t1)) + exp(-(t2 * t2));
+            }
+        return;
+    }
     if (c->problem == ORC_PROB_SWIRL) {
         for (int m = 1; m <= meqn; m++)
             for (int i = 1 - mbc; i <= mx + mbc; i++) {
@@ -134,6 +169,12 @@ int orc_tag_refine(const orc_sim* s, const orc_patch* P, int init_flag)
 {
     (void)init_flag;
     const orc_config* c = &s->cfg;
+    if (c->problem == ORC_PROB_SPHERE) {
+        int mbc = c->mbc;
+        double lo = P->q[QIDX(1, 1, 1, mbc, s->nx, s->ny)], hi = lo;
+        patch_minmax(s, P, &lo, &hi);
+        return hi - lo > c->refine_threshold;
+    }
     for (int j = 1; j <= c->my; j++)
         for (int i = 1; i <= c->mx; i++)
             if (grad_exceeds(s, P, P->q, i, j, c->refine_threshold)) return 1;
@@ -144,6 +185,13 @@ int orc_tag_coarsen(const orc_sim* s, const orc_patch* const* fam, int init_flag
 {
     const orc_config* c = &s->cfg;
     if (init_flag) return 0;
+    if (c->problem == ORC_PROB_SPHERE) {
+        /* running range over the whole family (tag4coarsening.f:35-58) */
+        int mbc = c->mbc;
+        double lo = fam[0]->q[QIDX(1, 1, 1, mbc, s->nx, s->ny)], hi = lo;
+        for (int k = 0; k < 4; k++) patch_minmax(s, fam[k], &lo, &hi);
+        return !(hi - lo > c->coarsen_threshold);
+    }
     for (int k = 0; k < 4; k++)
         for (int i = 1; i <= c->mx; i++)
             for (int j = 1; j <= c->my; j++)

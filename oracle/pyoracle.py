@@ -15,8 +15,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "liborc.so")
 
-RP_ADVECTION, RP_SW_ROE, RP_SW_FWAVE, RP_EULER_EXACT = 0, 1, 2, 3
-PROB_SWIRL, PROB_RADIALDAM, PROB_UNIFORM_SW, PROB_TSUNAMI, PROB_SHOCKBUBBLE = 0, 1, 2, 3, 4
+RP_ADVECTION, RP_SW_ROE, RP_SW_FWAVE, RP_EULER_EXACT, RP_ADVECTION_MANIFOLD = 0, 1, 2, 3, 4
+PROB_SWIRL, PROB_RADIALDAM, PROB_UNIFORM_SW, PROB_TSUNAMI, PROB_SHOCKBUBBLE, PROB_SPHERE = 0, 1, 2, 3, 4, 5
 
 
 class OrcConfig(ctypes.Structure):

@@ -5,12 +5,13 @@ from __future__ import annotations
 from oracle import pyoracle as po
 import forestclaw_b200 as fb
 from forestclaw_b200.problems import DAM as _DAM, SWIRL as _SWIRL, TSUNAMI as _TSUNAMI, swirl_dt  # noqa: F401
-from forestclaw_b200.problems import SHOCKBUBBLE as _SHOCKBUBBLE
+from forestclaw_b200.problems import SHOCKBUBBLE as _SHOCKBUBBLE, SPHERE as _SPHERE
 
 SWIRL = dict(_SWIRL, problem=po.PROB_SWIRL)
 DAM = dict(_DAM, problem=po.PROB_RADIALDAM)
 TSUNAMI = dict(_TSUNAMI, problem=po.PROB_TSUNAMI)
 SHOCKBUBBLE = dict(_SHOCKBUBBLE, problem=po.PROB_SHOCKBUBBLE)
+SPHERE = dict(_SPHERE, problem=po.PROB_SPHERE)
 
 _ORC_KEYS = {"mx", "my", "mbc", "meqn", "maux", "mwaves", "order", "mthlim", "mthbc", "mcapa", "use_fwaves",
              "rp", "minlevel", "maxlevel", "subcycle", "time_sync", "flux_correction", "fluctuation_correction",
