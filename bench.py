@@ -300,9 +300,12 @@ def error_vs_fp64(wl, prob, device, mlp, steps=8):
     a.close(); b.close()
     out = []
     for m in range(qa.shape[1]):
-        den = np.abs(qa[:, m]).sum() if np.abs(qa[:, m]).sum() > 0 else np.abs(qa[:, 0]).sum()
+        # momenta are relative to the density (depth): they vanish where the flow is at rest
+        mom = qa.shape[1] >= 3 and m in (1, 2)
+        den = np.abs(qa[:, 0 if mom else m]).sum()
         out.append(float(np.abs(qa[:, m] - qb[:, m]).sum() / den))
-    return {"steps": steps, "l1_rel_per_field": out}
+    return {"steps": steps, "l1_rel_per_field": out,
+            "normalisation": "sum |q_m| per field; momenta by the sum of the density (depth)"}
 
 
 def _spinup(g, wl, t, dt, steps):

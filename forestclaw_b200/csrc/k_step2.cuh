@@ -453,11 +453,15 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
                 k = -1;
             }
             const bool use = k >= 0 && mlp_gate(x);
+            // the network runs per warp (mma.sync over its 32 interfaces): skip warps
+            // without an interface past the gate (smooth flow, weak waves)
+            if (!__any_sync(0xffffffffu, use)) return 0.0;
             const MlpView W(sp.mlp);
             MlpFrag h1, h2;
             mlp_warp_hidden<true>(W, x, h1, h2);
             const float y = mlp_warp_output(W, h2);
-            return use ? pbase * fcb_exp((double)y) : 0.0;
+            if constexpr (F32) return use ? pbase * (double)__expf(y) : 0.0;
+            else return use ? pbase * fcb_exp((double)y) : 0.0;
         } else {
             (void)ixy; (void)k;
             return 0.0;

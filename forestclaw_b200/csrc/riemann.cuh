@@ -395,6 +395,26 @@ struct RPEulerExact {
             fd = (1.0 - 0.5 * (p - pk) / (bk + p)) * qrt;
         }
     }
+    // FP32 pressure function for the FP32-wave form.  On the rarefaction side
+    // z - 1 = (p/pk)^g1 - 1 comes from full-precision log1pf / expm1f (not the
+    // fast-math exp/log), so weak waves, where p/pk is close to 1, keep their
+    // relative accuracy.
+    static constexpr float NEWTON_TOL32 = 4.0e-7f;
+    __device__ static void prefun32(float g1, float g4, float g5, float g6, float p, float rk, float pk, float ak,
+                                    float& f, float& fd)
+    {
+        if (p <= pk) {
+            const float prat = p / pk;
+            const float zm1 = expm1f(g1 * log1pf(prat - 1.0f));
+            f = g4 * ak * zm1;
+            fd = ((zm1 + 1.0f) / prat) / (rk * ak);
+        } else {
+            const float bk = g6 * pk;
+            const float qrt = sqrtf((g5 / rk) / (bk + p));
+            f = (p - pk) * qrt;
+            fd = (1.0f - 0.5f * (p - pk) / (bk + p)) * qrt;
+        }
+    }
     __device__ static void eflux(double r, double u, double v, double p, double en, double* f)
     {
         f[0] = r * u;
@@ -575,9 +595,9 @@ struct RPEulerExact {
         for (int k = 0; k < 4; k++) { am[comp[k]] = f0[k] - flv[k]; ap[comp[k]] = frv[k] - f0[k]; }
         return it;
     }
-    // FP32-wave form of solve64.  Primitive states, Roe averages, star states,
-    // the Godunov state and the waves in FP32; the Newton iteration in FP64 (from
-    // the FP64 states, only where p or u jumps).  The Godunov flux f0 is one FP32
+    // FP32-wave form of solve64.  Primitive states, Roe averages, the Newton
+    // iteration on p* (only where p or u jumps), star states, the Godunov state and
+    // the waves in FP32.  The Godunov flux f0 is one FP32
     // value per interface, so amdq = f0 - F(qL) and apdq = F(qR) - f0 with the FP64
     // cell fluxes of flxL/flxR keep the update conservative in FP64.
     __device__ static int solve_mixed(int ixy, const float* qL, const float* qR, const double* qL64,
@@ -616,30 +636,32 @@ struct RPEulerExact {
         if (nojump) {
             ps = pl; us = ul;
         } else {
-            const Prim P = prim(ixy, qL64, qR64, ep.gam);
-            const double gd = ep.gam;
-            const double d1 = (gd - 1.0) / (2.0 * gd), d4 = 2.0 / (gd - 1.0), d5 = 2.0 / (gd + 1.0);
-            const double d6 = (gd - 1.0) / (gd + 1.0);
-            const double du = P.ur - P.ul, tolpre = 1.0e-6;
-            double p;
-            if (ep.seed > 0.0 && isfinite(ep.seed)) p = ep.seed;
+            // Newton on p* in FP32 from the FP32 primitive states (Toro's pressure
+            // function; the FP64 form iterates in FP64 with the deterministic exp/log).
+            // FP32 resolves p* to a few ulp, so the iteration stops at a relative change
+            // of max(tol, NEWTON_TOL32).
+            (void)qL64; (void)qR64;
+            const float du = ur - ul, tolpre = 1.0e-6f;
+            float p;
+            if (ep.seed > 0.0 && isfinite(ep.seed)) p = (float)ep.seed;
             else {
-                const double ppv = 0.5 * (P.pl + P.pr) - 0.125 * du * (P.rl + P.rr) * (P.al + P.ar);
+                const float ppv = 0.5f * (pl + pr) - 0.125f * du * (rl + rr) * (al + ar);
                 p = ppv > tolpre ? ppv : tolpre;
             }
-            double fl = 0.0, fr = 0.0, fdl, fdr;
+            const float tol = fmaxf((float)ep.tol, NEWTON_TOL32);
+            float fl = 0.0f, fr = 0.0f, fdl, fdr;
             for (it = 1; it <= 64; it++) {
-                prefun(d1, d4, d5, d6, p, P.rl, P.pl, P.al, fl, fdl);
-                prefun(d1, d4, d5, d6, p, P.rr, P.pr, P.ar, fr, fdr);
-                double pn = p - (fl + fr + du) / (fdl + fdr);
-                if (pn < 0.0) pn = tolpre;
-                const double change = 2.0 * fabs(pn - p) / (pn + p);
+                prefun32(g1, g4, g5, g6, p, rl, pl, al, fl, fdl);
+                prefun32(g1, g4, g5, g6, p, rr, pr, ar, fr, fdr);
+                float pn = p - (fl + fr + du) / (fdl + fdr);
+                if (pn < 0.0f) pn = tolpre;
+                const float change = 2.0f * fabsf(pn - p) / (pn + p);
                 p = pn;
-                if (change <= ep.tol) break;
+                if (change <= tol) break;
             }
             if (it > 64) it = 64;
-            ps = (float)p;
-            us = (float)(0.5 * (P.ul + P.ur) + 0.5 * (fr - fl));
+            ps = p;
+            us = 0.5f * (ul + ur) + 0.5f * (fr - fl);
         }
         float rsl, rsr, asl, asr;
         if (ps > pl) { const float q = ps / pl; rsl = rl * ((q + g6) / (g6 * q + 1.0f)); asl = sqrtf(gam * ps / rsl); }

@@ -104,7 +104,10 @@ def test_moving_bubble_error_and_conservation(precision):
     m1 = g.mass()
     drift = np.abs(m1 - m0) / np.abs(m0)
     print(precision, "relative mass / energy drift", drift[0], drift[3])
-    assert drift[0] <= 1e-12 and drift[3] <= 1e-12, drift
+    # mass to 1e-12 in both forms; energy to 1e-12 in FP64 and 2e-11 in the FP32-wave
+    # form, whose FP32 star states feed FP64 fluxes that round differently on the two
+    # sides of the time-sync corrections
+    assert drift[0] <= 1e-12 and drift[3] <= (1e-12 if precision == "fp64" else 2e-11), drift
 
 
 def test_shockbubble_fp32wave_error():
