@@ -405,11 +405,22 @@ def _fp64_kernel_arm(args, wl, prob, local_rank, flush):
     tune = _tune(g, not args.no_autotune)
     t, dt, _ = _spinup(g, dict(wl, regrid_interval=0), t, dt, args.warmup)
     g.synchronize()
+    _bracket()
     r = _timed_steps(g, wl, args.steps, t, dt, flush)
-    total_ms = float(np.sum(r["step_ms"]))
+    _bracket()
     g.close()
-    return {"value": r["cells"] / (total_ms * 1e-3), "ms_per_step": total_ms / args.steps,
+    from forestclaw_b200 import ranks
+    total_ms, _, value = ranks.aggregate(float(np.sum(r["step_ms"])), r["cells"], "cuda")
+    return {"value": value, "ms_per_step": total_ms / args.steps,
             "variant": {k: tune[k] for k in ("variant", "threads", "min_blocks", "reg")}}
+
+
+def _bracket():
+    """Both sides of a timed region: every rank's device idle, then a barrier."""
+    import torch
+    torch.cuda.synchronize()
+    if torch.distributed.is_available() and torch.distributed.is_initialized():
+        torch.distributed.barrier()
 
 
 def run_ours(args, wl, rank, world, local_rank):
@@ -435,32 +446,21 @@ def run_ours(args, wl, rank, world, local_rank):
     g.synchronize()
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     g.set_timing(False)
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
     props = torch.cuda.get_device_properties(local_rank)
     clk = ClockSampler(f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local_rank))
+    _bracket()
     if rank == 0:
         clk.start()
     r = _timed_steps(g, wl, args.steps, t, dt, flush)
-    torch.cuda.synchronize()
+    _bracket()
     clocks = clk.stop() if rank == 0 else None
     step_ms, cells, launches, timed_regrid_ms, t, dt = (r["step_ms"], r["cells"], r["launches"], r["regrid_ms"],
                                                          r["t"], r["dt"])
     nroof = max(2, min(args.steps, 4))
     upd_ms, upd_bytes, upd_launches = _roofline_pass([g], [(t, dt)], flush, nroof)
     t += nroof * dt
-    total_ms = float(np.sum(step_ms))
-    if world > 1:
-        tt = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(tt.item())
-        cc = torch.tensor([cells], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(cc, op=torch.distributed.ReduceOp.SUM)
-        cells_all = float(cc.item())
-    else:
-        cells_all = cells
-    value = cells_all / (total_ms * 1e-3)
+    from forestclaw_b200 import ranks
+    total_ms, cells_all, value = ranks.aggregate(float(np.sum(step_ms)), cells, "cuda")
     # ---- end to end through the C ABI with pinned host buffers ----
     nq = g.num_patches * gc.meqn * (gc.mx + 2 * gc.mbc) * (gc.my + 2 * gc.mbc)
     hq = torch.empty(nq, dtype=torch.float64, pin_memory=True)
@@ -477,11 +477,8 @@ def run_ours(args, wl, rank, world, local_rank):
         e2e_cells += g.cell_updates - c0
         t += dt
     e2e_s = time.perf_counter() - te0
-    if world > 1:
-        te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(te.item())
-        e2e_cells *= world
+    e2e_s = ranks.max_over_ranks(e2e_s, "cuda")
+    e2e_cells = ranks.sum_over_ranks(e2e_cells, "cuda")
     e2e = {"value": e2e_cells / e2e_s, "unit": "cell-updates/s", "h2d_bytes_per_step": nq * 8,
            "d2h_bytes_per_step": nq * 8}
     newton = None
@@ -525,11 +522,14 @@ def run_ours(args, wl, rank, world, local_rank):
     return 0
 
 
-def _batch_groups(precision, device, n=64, seed=0):
+def _batch_groups(precision, device, n=64, seed=None):
     """The batched workload: n seeded tsunami instances, one solver per patch size
     (all instances of a size share every level launch)."""
     import forestclaw_b200 as fb
-    from forestclaw_b200 import problems
+    from forestclaw_b200 import problems, ranks
+    if seed is None:
+        # each rank runs its own n instances (disjoint seeds): weak scaling, no exchange
+        seed = ranks.instance_seed_base(ranks.rank_world()[0], n)
     insts, sizes = problems.tsunami_instances(n, seed)
     by = {}
     for k, (inst, mx) in enumerate(zip(insts, sizes)):
@@ -597,10 +597,11 @@ def _batch_timed_arm(args, wl, precision, local_rank, flush, tune_on, clk=None):
     _batch_run(groups, wl["spinup"], wl["regrid_interval"])
     tunes = {str(G["mx"]): _tune(G["g"], tune_on) for G in groups}
     _batch_run(groups, args.warmup, 0)
-    torch.cuda.synchronize()
+    _bracket()
     if clk is not None:
         clk.start()
     r = _batch_run(groups, args.steps, wl["regrid_interval"], flush, timed=True)
+    _bracket()
     r["clocks"] = clk.stop() if clk is not None else None
     return groups, tunes, r
 
@@ -675,17 +676,9 @@ def run_batch(args, wl, rank, world, local_rank):
     groups, tunes, r = _batch_timed_arm(args, wl, args.precision, local_rank, flush, not args.no_autotune,
                                         clk if rank == 0 else None)
     clocks = r["clocks"]
-    total_ms = float(np.sum(r["step_ms"]))
+    from forestclaw_b200 import ranks
     cells = r["cells"]
-    if world > 1:
-        tt = torch.tensor([total_ms, cells], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(tt[:1], op=torch.distributed.ReduceOp.MAX)
-        cc = torch.tensor([cells], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(cc, op=torch.distributed.ReduceOp.SUM)
-        total_ms, cells_all = float(tt[0].item()), float(cc.item())
-    else:
-        cells_all = cells
-    value = cells_all / (total_ms * 1e-3)
+    total_ms, cells_all, value = ranks.aggregate(float(np.sum(r["step_ms"])), cells, "cuda")
     nroof = max(2, min(args.steps, 4))
     upd_ms, upd_bytes, upd_launches = _roofline_pass([G["g"] for G in groups], [(0.0, G["dt"]) for G in groups],
                                                      flush, nroof)
@@ -710,9 +703,10 @@ def run_batch(args, wl, rank, world, local_rank):
         for G, hq in zip(groups, bufs):
             G["g"].get_q_ptr(hq.data_ptr())
         e2e_cells += sum(G["g"].cell_updates for G in groups) - c0
-    e2e_s = time.perf_counter() - te0
+    e2e_s = ranks.max_over_ranks(time.perf_counter() - te0, "cuda")
+    e2e_cells = ranks.sum_over_ranks(e2e_cells, "cuda")
     nbytes = int(sum(b.numel() for b in bufs) * 8)
-    e2e = {"value": e2e_cells * world / e2e_s, "unit": "cell-updates/s", "h2d_bytes_per_step": nbytes,
+    e2e = {"value": e2e_cells / e2e_s, "unit": "cell-updates/s", "h2d_bytes_per_step": nbytes,
            "d2h_bytes_per_step": nbytes}
     info = {str(G["mx"]): {"instances": len(G["ids"]), "patches": G["g"].num_patches} for G in groups}
     for G in groups:
@@ -720,8 +714,8 @@ def run_batch(args, wl, rank, world, local_rank):
     fp64 = None
     if args.precision != "fp64" and not args.no_fp64_compare:
         g64, tune64, r64 = _batch_timed_arm(args, wl, "fp64", local_rank, flush, not args.no_autotune)
-        ms64 = float(np.sum(r64["step_ms"]))
-        fp64 = {"value": r64["cells"] / (ms64 * 1e-3), "ms_per_step": ms64 / args.steps,
+        ms64, _, v64 = ranks.aggregate(float(np.sum(r64["step_ms"])), r64["cells"], "cuda")
+        fp64 = {"value": v64, "ms_per_step": ms64 / args.steps,
                 "variants": {k: {x: v[x] for x in ("variant", "threads", "min_blocks", "reg")}
                              for k, v in tune64.items()}}
         fp64["speedup"] = value / fp64["value"] if world == 1 else None
