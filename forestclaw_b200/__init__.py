@@ -194,7 +194,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_advance_instances_end": [P, dp],
         "fc2d_b200_mass_instances": [P, dp],
         "fc2d_b200_num_variants": [P, ip, ip],
-        "fc2d_b200_variant_info": [P, I, ip, ip, ip, ip],
+        "fc2d_b200_variant_info": [P, I, ip, ip, ip, ip, ip],
         "fc2d_b200_set_variant": [P, I],
         "fc2d_b200_autotune": [P, I, ip, dp],
     }
@@ -440,9 +440,10 @@ class Solver:
         self._check("fc2d_b200_num_variants", self.lib.fc2d_b200_num_variants(self.h, ctypes.byref(n), ctypes.byref(cur)))
         out = []
         for v in range(n.value):
-            a = [ctypes.c_int() for _ in range(4)]
+            a = [ctypes.c_int() for _ in range(5)]
             self._check("fc2d_b200_variant_info", self.lib.fc2d_b200_variant_info(self.h, v, *[ctypes.byref(x) for x in a]))
-            out.append(dict(threads=a[0].value, min_blocks=a[1].value, reg=a[2].value, smem=a[3].value))
+            out.append(dict(threads=a[0].value, min_blocks=a[1].value, reg=a[2].value, smem=a[3].value,
+                            persistent=a[4].value))
         return out
 
     @property

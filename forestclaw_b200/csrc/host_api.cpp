@@ -1700,7 +1700,7 @@ extern "C" int fc2d_b200_num_variants(const fc2d_b200_solver_t* s, int* n, int* 
 }
 
 extern "C" int fc2d_b200_variant_info(const fc2d_b200_solver_t* s, int v, int* threads, int* min_blocks, int* reg,
-                                      int* smem_bytes)
+                                      int* smem_bytes, int* persistent)
 {
     if (!s || v < 0 || v >= (int)s->vars.size()) return fail(FC2D_B200_EINVAL, "no such variant");
     const Step2Variant* x = s->vars[v];
@@ -1708,6 +1708,7 @@ extern "C" int fc2d_b200_variant_info(const fc2d_b200_solver_t* s, int v, int* t
     if (min_blocks) *min_blocks = x->min_blocks;
     if (reg) *reg = x->reg;
     if (smem_bytes) *smem_bytes = x->smem;
+    if (persistent) *persistent = x->persistent;
     return 0;
 }
 

@@ -93,14 +93,15 @@ __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
 
-template <class RP, int MX, int MY, int MBC, bool FWAVE, int NT, typename TW, int MINB = 2>
-__global__ void __launch_bounds__(NT, MINB)
-step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* __restrict__ aux,
-             double* __restrict__ regs, const PatchDesc* __restrict__ desc, int p0,
-             const StepParams* __restrict__ spp, unsigned long long* __restrict__ cfl_bits)
+// The update of patch p by the whole CTA (one call per patch; the CTA may do
+// several patches in turn).  nhist: the CTA's shared Newton-iteration counters.
+template <class RP, int MX, int MY, int MBC, bool FWAVE, int NT, typename TW>
+__device__ __forceinline__ void
+step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __restrict__ aux,
+            double* __restrict__ regs, const PatchDesc* __restrict__ desc, const int p,
+            const StepParams& sp, unsigned long long* __restrict__ cfl_bits, unsigned int* nhist)
 {
     using G = Step2Geom<RP, MX, MY, MBC, TW, NT>;
-    const StepParams sp = *spp;     // per-launch parameters live in device memory (graph replay)
     constexpr bool F32 = G::F32, REG = G::REG;
     static_assert(!RP::EXACT64 || G::REG, "exact solvers keep their FP64 fluctuations in registers");
     constexpr int NX = G::NX, NY = G::NY, NXY = G::NXY, MEQN = G::MEQN, MWAVES = G::MWAVES;
@@ -131,9 +132,7 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
     unsigned char* tflag = reinterpret_cast<unsigned char*>(Qf + (F32 ? MEQN * NXY : 0));
 
     const int tid = threadIdx.x;
-    const int p = p0 + blockIdx.x;
-    __shared__ unsigned int nhist[RP::EXACT64 ? 32 : 1];   // Newton iterations of this patch
-    if (RP::EXACT64 && tid < 32) nhist[tid] = 0u;
+    if (RP::EXACT64 && tid < 32) nhist[tid] = 0u;          // Newton iterations of this patch
     const PatchDesc pd = desc[p];
     const double dx = pd.dx, dy = pd.dy;
     const double dt = sp.inst_dt ? sp.dt * sp.inst_dt[pd.inst] : sp.dt;
@@ -668,6 +667,29 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
     }
     if constexpr (RP::EXACT64) {
         if (tid < 32 && sp.newton_hist && nhist[tid]) atomicAdd(&sp.newton_hist[tid], (unsigned long long)nhist[tid]);
+    }
+}
+
+// The fused update of npatch patches starting at slot p0.  One CTA per patch, or
+// (PERSIST) a grid of a few CTAs per SM, each taking patches p0 + blockIdx.x,
+// + gridDim.x, ... in turn, its shared memory reused patch after patch.
+template <class RP, int MX, int MY, int MBC, bool FWAVE, int NT, typename TW, int MINB = 2, bool PERSIST = false>
+__global__ void __launch_bounds__(NT, MINB)
+step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* __restrict__ aux,
+             double* __restrict__ regs, const PatchDesc* __restrict__ desc, int p0, int npatch,
+             const StepParams* __restrict__ spp, unsigned long long* __restrict__ cfl_bits)
+{
+    const StepParams sp = *spp;     // per-launch parameters live in device memory (graph replay)
+    __shared__ unsigned int nhist[RP::EXACT64 ? 32 : 1];
+    if constexpr (!PERSIST) {
+        (void)npatch;
+        step2_patch<RP, MX, MY, MBC, FWAVE, NT, TW>(q, qlast, aux, regs, desc, p0 + (int)blockIdx.x, sp, cfl_bits,
+                                                    nhist);
+    } else {
+        for (int b = blockIdx.x; b < npatch; b += gridDim.x) {
+            step2_patch<RP, MX, MY, MBC, FWAVE, NT, TW>(q, qlast, aux, regs, desc, p0 + b, sp, cfl_bits, nhist);
+            __syncthreads();   // the next patch restages the shared memory
+        }
     }
 }
 

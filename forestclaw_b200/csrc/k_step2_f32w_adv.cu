@@ -1,5 +1,6 @@
 // k_step2_f32w_adv.cu -- FP32-wave instantiations (built with --use_fast_math; FP64 accumulation)
-// of the fused update for scalar advection (plane and manifold): the patch-to-CTA variants of each patch size.
+// of the fused update for scalar advection (plane and manifold): the patch-to-CTA variants of each patch size
+// (one CTA per patch, then the persistent forms).
 #include "k_step2_variant.cuh"
 #include "fc2d_b200.h"
 
@@ -24,6 +25,13 @@ const Step2Variant* step2_table_f32w_adv(int* n)
         FCB_STEP2_VARIANT(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_ADVECTION_MANIFOLD, RPAdvectionManifold, 16, false, 256, 3, float),
         FCB_STEP2_VARIANT(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_ADVECTION_MANIFOLD, RPAdvectionManifold, 8, false, 160, 2, float),
         FCB_STEP2_VARIANT(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_ADVECTION_MANIFOLD, RPAdvectionManifold, 8, false, 128, 4, float),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_ADVECTION, RPAdvection, 32, false, 512, 2, float),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_ADVECTION, RPAdvection, 32, false, 1024, 1, float),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_ADVECTION, RPAdvection, 16, false, 416, 2, float),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_ADVECTION_MANIFOLD, RPAdvectionManifold, 32, false, 512, 2, float),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_ADVECTION_MANIFOLD, RPAdvectionManifold, 32, false, 1024, 1, float),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_ADVECTION_MANIFOLD, RPAdvectionManifold, 16, false, 416, 2, float),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_ADVECTION_MANIFOLD, RPAdvectionManifold, 8, false, 160, 2, float),
     };
     *n = (int)(sizeof(table) / sizeof(table[0]));
     return table;

@@ -1,5 +1,6 @@
 // k_step2_f32w_sw.cu -- FP32-wave instantiations (built with --use_fast_math; FP64 accumulation)
-// of the fused update for shallow water (Roe and f-wave): the patch-to-CTA variants of each patch size.
+// of the fused update for shallow water (Roe and f-wave): the patch-to-CTA variants of each patch size
+// (one CTA per patch, then the persistent forms).
 #include "k_step2_variant.cuh"
 #include "fc2d_b200.h"
 
@@ -26,6 +27,14 @@ const Step2Variant* step2_table_f32w_sw(int* n)
         FCB_STEP2_VARIANT(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 8, true, 128, 4, float),
         FCB_STEP2_VARIANT(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 8, true, 160, 4, float),
         FCB_STEP2_VARIANT(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 8, true, 64, 8, float),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_SW_ROE, RPShallowRoe, 16, false, 416, 2, float),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_SW_ROE, RPShallowRoe, 16, false, 352, 2, float),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_SW_ROE, RPShallowRoe, 8, false, 160, 2, float),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_SW_ROE, RPShallowRoe, 8, false, 160, 4, float),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 16, true, 416, 2, float),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 16, true, 352, 2, float),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 8, true, 160, 2, float),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP32WAVE, FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 8, true, 160, 4, float),
     };
     *n = (int)(sizeof(table) / sizeof(table[0]));
     return table;

@@ -1,5 +1,6 @@
 // k_step2_f64_sw.cu -- FP64 instantiations (built with -fmad=false: bitwise equal to the FP64 CPU path)
-// of the fused update for shallow water (Roe and f-wave): the patch-to-CTA variants of each patch size.
+// of the fused update for shallow water (Roe and f-wave): the patch-to-CTA variants of each patch size
+// (one CTA per patch, then the persistent forms).
 #include "k_step2_variant.cuh"
 #include "fc2d_b200.h"
 
@@ -24,6 +25,14 @@ const Step2Variant* step2_table_f64_sw(int* n)
         FCB_STEP2_VARIANT(FC2D_B200_PREC_FP64, FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 8, true, 128, 4, double),
         FCB_STEP2_VARIANT(FC2D_B200_PREC_FP64, FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 8, true, 160, 4, double),
         FCB_STEP2_VARIANT(FC2D_B200_PREC_FP64, FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 8, true, 64, 8, double),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP64, FC2D_B200_RP_SW_ROE, RPShallowRoe, 16, false, 352, 2, double),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP64, FC2D_B200_RP_SW_ROE, RPShallowRoe, 16, false, 352, 1, double),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP64, FC2D_B200_RP_SW_ROE, RPShallowRoe, 8, false, 160, 2, double),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP64, FC2D_B200_RP_SW_ROE, RPShallowRoe, 8, false, 128, 4, double),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP64, FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 16, true, 352, 2, double),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP64, FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 16, true, 352, 1, double),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP64, FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 8, true, 160, 2, double),
+        FCB_STEP2_VARIANT_P(FC2D_B200_PREC_FP64, FC2D_B200_RP_SW_FWAVE, RPShallowFWave, 8, true, 128, 4, double),
     };
     *n = (int)(sizeof(table) / sizeof(table[0]));
     return table;

@@ -31,6 +31,7 @@ struct Step2Variant {
     int threads, min_blocks;   // CTA size and __launch_bounds__ occupancy target
     int reg;                   // 1: one thread per interface (normal solve kept in registers)
     int smem;                  // dynamic shared memory per CTA, bytes
+    int persistent;            // 1: a grid of resident CTAs loops over the patches
     Step2Fn fn;
 };
 const Step2Variant* step2_table_f64_adv(int* n);

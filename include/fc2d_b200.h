@@ -150,14 +150,16 @@ int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed);
  * Each solver shape (precision, Riemann solver, patch size) is compiled with
  * several mappings of a patch onto its CTA: threads per CTA and an occupancy
  * target (CTAs per SM, which caps registers per thread); reg = 1 when every
- * interface of a sweep has its own thread.  Variant 0 is the default.  FP64
+ * interface of a sweep has its own thread; persistent = 1 for the persistent
+ * form (a grid of resident CTAs looping over the level's patches, one launch
+ * per level-step however many patches and instances).  Variant 0 is the default.  FP64
  * variants give identical results.  fc2d_b200_autotune times every variant on
  * the current forest (reps passes over all levels, dt = 0 so q is unchanged),
  * keeps the fastest and returns it; ms[v] (may be null, num_variants entries)
  * receives the time of one pass of variant v. */
 int fc2d_b200_num_variants(const fc2d_b200_solver_t* s, int* n, int* current);
 int fc2d_b200_variant_info(const fc2d_b200_solver_t* s, int v, int* threads, int* min_blocks, int* reg,
-                           int* smem_bytes);
+                           int* smem_bytes, int* persistent);
 int fc2d_b200_set_variant(fc2d_b200_solver_t* s, int v);
 int fc2d_b200_autotune(fc2d_b200_solver_t* s, int reps, int* best, double* ms);
 
