@@ -197,6 +197,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_variant_info": [P, I, ip, ip, ip, ip, ip],
         "fc2d_b200_set_variant": [P, I],
         "fc2d_b200_autotune": [P, I, ip, dp],
+        "fc2d_b200_output_ascii": [P, ctypes.c_char_p, I, D],
+        "fc2d_b200_write_ascii_frame": [ctypes.c_char_p, I, D, I, I, I, I, I, I, ip, ip, dp, dp, dp, dp, dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -206,6 +208,23 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fc2d_b200_last_error.argtypes = []
     _lib = L
     return L
+
+
+def write_ascii_frame(directory: str, iframe: int, time: float, q: np.ndarray, level, block, xlower, ylower, dx, dy,
+                      mbc: int = 2, maux: int = 0) -> None:
+    """Write caller-supplied patches as a clawpack 4.6 ASCII frame (host only, no device).
+    q: (npatch, meqn, my + 2 mbc, mx + 2 mbc) in the FArrayBox layout; per-patch level,
+    block, lower corner and spacing; patches are written in the given order."""
+    lib = load_library()
+    q = np.ascontiguousarray(q, np.float64)
+    npatch, meqn, ny, nx = q.shape
+    lv = np.ascontiguousarray(level, np.int32)
+    bk = np.ascontiguousarray(block, np.int32)
+    arr = [np.ascontiguousarray(v, np.float64) for v in (xlower, ylower, dx, dy)]
+    rc = lib.fc2d_b200_write_ascii_frame(os.fsencode(directory), iframe, time, meqn, maux, nx - 2 * mbc,
+                                         ny - 2 * mbc, mbc, npatch, _ip(lv), _ip(bk), *[_dp(v) for v in arr], _dp(q))
+    if rc != 0:
+        raise B200Error("fc2d_b200_write_ascii_frame", rc, "cannot write the frame")
 
 
 def exported_symbols() -> list[str]:
@@ -432,6 +451,12 @@ class Solver:
         out = (ctypes.c_ulonglong * 32)()
         self._check("fc2d_b200_newton_histogram", self.lib.fc2d_b200_newton_histogram(self.h, out, int(reset)))
         return np.array(out[:], np.int64)
+
+    # -- output ----------------------------------------------------------------
+    def output_ascii(self, directory: str, iframe: int, time: float) -> None:
+        """fort.tNNNN / fort.qNNNN of the current forest (clawpack 4.6 ASCII, VisClaw-readable)."""
+        self._check("fc2d_b200_output_ascii",
+                    self.lib.fc2d_b200_output_ascii(self.h, os.fsencode(directory), iframe, time))
 
     # -- patch-to-CTA variants and the autotuner -------------------------------
     def variants(self) -> list:

@@ -38,7 +38,7 @@ CU_UNITS = {
     "k_step2_f32w_sw.cu": ["--use_fast_math"],
     "k_step2_f32w_euler.cu": ["--use_fast_math"],
 }
-CPP_UNITS = ["host_forest.cpp", "host_api.cpp", "apps.cpp"]
+CPP_UNITS = ["host_forest.cpp", "host_api.cpp", "apps.cpp", "host_output.cpp"]
 
 
 def _sources_digest() -> str:

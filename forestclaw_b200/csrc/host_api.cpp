@@ -1770,3 +1770,41 @@ extern "C" int fc2d_b200_autotune(fc2d_b200_solver_t* s, int reps, int* best_out
     if (best_out) *best_out = best;
     return 0;
 }
+
+// ---------------------------------------------------------------------------
+// output (fclaw2d_clawpatch_output_ascii)
+// ---------------------------------------------------------------------------
+extern "C" int fc2d_b200_output_ascii(fc2d_b200_solver_t* s, const char* dir, int iframe, double time)
+{
+    if (!s || !s->initialized || !dir) return fail(FC2D_B200_EINVAL, "bad arguments");
+    const Forest& f = s->forest;
+    const int np = f.np();
+    const size_t nq = (size_t)s->d.nq();
+    std::vector<double> q((size_t)np * nq);
+    CK(cudaMemcpyAsync(q.data(), s->q, q.size() * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    // the reference writes patches block by block, each block's leaves along the curve
+    std::vector<int> order(np);
+    for (int i = 0; i < np; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        const PatchInfo& A = f.p[a];
+        const PatchInfo& B = f.p[b];
+        if (A.inst != B.inst) return A.inst < B.inst;
+        if (A.block != B.block) return A.block < B.block;
+        return A.morton < B.morton;
+    });
+    std::vector<int> lev(np), blk(np);
+    std::vector<double> xl(np), yl(np), dx(np), dy(np), qo((size_t)np * nq);
+    for (int k = 0; k < np; k++) {
+        const PatchInfo& P = f.p[order[k]];
+        lev[k] = P.level + f.gi(P.inst).lbase;
+        blk[k] = P.block;
+        xl[k] = P.xlower; yl[k] = P.ylower; dx[k] = P.dx; dy[k] = P.dy;
+        std::memcpy(&qo[(size_t)k * nq], &q[(size_t)order[k] * nq], nq * sizeof(double));
+    }
+    const int rc = fc2d_b200_write_ascii_frame(dir, iframe, time, s->d.meqn, s->d.maux, s->d.mx, s->d.my, s->d.mbc, np,
+                                               lev.data(), blk.data(), xl.data(), yl.data(), dx.data(), dy.data(),
+                                               qo.data());
+    if (rc) return fail(rc, std::string("cannot write fort.q/fort.t frame into ") + dir);
+    return 0;
+}

@@ -146,6 +146,18 @@ int fc2d_b200_advance(fc2d_b200_solver_t* s, double t, double dt, double* maxcfl
  * device repopulation, ghost update.  *changed = 1 if the forest changed. */
 int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed);
 
+/* ---- output: clawpack 4.6 ASCII frames ----
+ * fclaw2d_clawpatch_output_ascii (src/patches/clawpatch/fclaw2d_clawpatch_output_ascii.c:112-170,
+ * fort_4.6/fclaw2d_clawpatch46_output_ascii.f): <dir>/fort.tNNNN (time, meqn, ngrids, num_aux,
+ * num_dim) and <dir>/fort.qNNNN (per patch a header and the interior cells), patches in
+ * the reference's order (block, then along the space-filling curve), Fortran E format.
+ * fc2d_b200_write_ascii_frame writes caller-supplied patches (host memory, q in the
+ * FArrayBox layout, ghosts included); it needs no device. */
+int fc2d_b200_output_ascii(fc2d_b200_solver_t* s, const char* dir, int iframe, double time);
+int fc2d_b200_write_ascii_frame(const char* dir, int iframe, double time, int meqn, int maux, int mx, int my,
+                                int mbc, int npatch, const int* level, const int* block, const double* xlower,
+                                const double* ylower, const double* dx, const double* dy, const double* q);
+
 /* ---- patch-to-CTA variants of the fused update (no counterpart in the reference) ----
  * Each solver shape (precision, Riemann solver, patch size) is compiled with
  * several mappings of a patch onto its CTA: threads per CTA and an occupancy
