@@ -172,6 +172,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_event_elapsed": [P, I, I, dp],
         "fc2d_b200_get_stream": [P, ctypes.POINTER(P)],
         "fc2d_b200_set_graphs": [P, I],
+        "fc2d_b200_set_programmatic_launch": [P, I],
         "fc2d_b200_mass_noalloc": [P, ctypes.POINTER(ctypes.c_double)],
         "fc2d_b200_newton_histogram": [P, ctypes.POINTER(ctypes.c_ulonglong), I],
         "fc2d_b200_mlp_create": [I, ctypes.c_ulonglong, ctypes.POINTER(P)],
@@ -550,6 +551,10 @@ class Solver:
 
     def set_graphs(self, on: bool) -> None:
         self._check("fc2d_b200_set_graphs", self.lib.fc2d_b200_set_graphs(self.h, int(on)))
+
+    def set_programmatic_launch(self, on: bool) -> None:
+        """Programmatic dependent launch of the advance's kernels (default on)."""
+        self._check("fc2d_b200_set_programmatic_launch", self.lib.fc2d_b200_set_programmatic_launch(self.h, int(on)))
 
     def set_timing(self, on: bool) -> None:
         self._check("fc2d_b200_set_timing", self.lib.fc2d_b200_set_timing(self.h, int(on)))

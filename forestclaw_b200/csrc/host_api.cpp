@@ -149,6 +149,7 @@ struct fc2d_b200_solver {
     bool fill = true;                              // fill params_host / count statistics
     // CUDA graph of one fclaw2d_advance_all_levels for the current forest
     bool use_graphs = true;
+    bool programmatic = true;                      // advance kernels with programmatic dependent launch
     cudaGraphExec_t graph_exec = nullptr;
     int graph_nupd = -1;
 };
@@ -947,6 +948,7 @@ static int advance_launch(fc2d_b200_solver_t* s, double t, double dt)
     s->emit = false; s->fill = true;
     int rc = traverse_advance(s, t, dt);
     if (rc) { s->emit = true; return rc; }
+    ProgrammaticScope pscope(s->programmatic);
     const int nupd = s->n_upd;
     rc = begin_cfl(s);
     if (rc) return rc;
@@ -1252,6 +1254,14 @@ extern "C" int fc2d_b200_get_stream(const fc2d_b200_solver_t* s, void** stream)
 {
     if (!s || !stream) return fail(FC2D_B200_EINVAL, "null argument");
     *stream = (void*)s->st;
+    return 0;
+}
+
+extern "C" int fc2d_b200_set_programmatic_launch(fc2d_b200_solver_t* s, int enable)
+{
+    if (!s) return fail(FC2D_B200_EINVAL, "null solver");
+    s->programmatic = enable != 0;
+    invalidate_graph(s);
     return 0;
 }
 

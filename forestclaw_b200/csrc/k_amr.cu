@@ -14,15 +14,22 @@
 //   time sync             clawpack46_time_sync.f:254-704, clawpatch_conservation.c:207-280
 //   mass                  fort_4.6/fclaw2d_clawpatch46_diagnostics.f:13-55
 //   tagging               fort_4.6/fclaw2d_clawpatch46_tag4refinement.f / _tag4coarsening.f
+#include "fcb_launch.cuh"
 #include "kernels.h"
 
 namespace fcb {
+
+static thread_local bool tl_programmatic = false;
+void set_programmatic_launch(bool on) { tl_programmatic = on; }
+bool programmatic_launch() { return tl_programmatic; }
 
 static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 
 __global__ void k_copy(double* __restrict__ dst, const double* __restrict__ src, const CopyEnt* __restrict__ e,
                        int n, int nxy, int meqn)
 {
+    grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
+    grid_launch_dependents();
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     CopyEnt c = e[t];
@@ -32,6 +39,8 @@ __global__ void k_copy(double* __restrict__ dst, const double* __restrict__ src,
 __global__ void k_average(double* __restrict__ dst, const double* __restrict__ src, const AvgEnt* __restrict__ e,
                           int n, int nq, int nx, int nxy, int meqn, const double* __restrict__ area)
 {
+    grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
+    grid_launch_dependents();
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     AvgEnt c = e[t];
@@ -80,6 +89,8 @@ __device__ __forceinline__ double compute_slopes(double sl, double sr)
 __global__ void k_interp(double* __restrict__ dst, const double* __restrict__ src, const InterpEnt* __restrict__ e,
                          int n, int nx, int nxy, int meqn)
 {
+    grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
+    grid_launch_dependents();
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     InterpEnt c = e[t];
@@ -101,6 +112,8 @@ __global__ void k_interp(double* __restrict__ dst, const double* __restrict__ sr
 __global__ void k_phys(double* __restrict__ q, const PhysEnt* __restrict__ e, int n, int nxy, int meqn,
                        const double* __restrict__ bcstate)
 {
+    grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
+    grid_launch_dependents();
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     PhysEnt c = e[t];
@@ -114,6 +127,8 @@ __global__ void k_phys(double* __restrict__ q, const PhysEnt* __restrict__ e, in
 __global__ void k_timeinterp(const double* __restrict__ q, const double* __restrict__ ql, double* __restrict__ qi,
                              const int* __restrict__ patches, int mx, int my, int mbc, int meqn, double alpha)
 {
+    grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
+    grid_launch_dependents();
     const int p = patches[blockIdx.x];
     const int nx = mx + 2 * mbc, ny = my + 2 * mbc, nxy = nx * ny;
     const size_t base = (size_t)p * nxy * meqn;
@@ -149,6 +164,8 @@ __global__ void k_samesize(double* __restrict__ q, const double* __restrict__ re
                            const SyncOp* __restrict__ ops, const int* __restrict__ op_start,
                            int mx, int my, int mbc, int meqn, int nreg)
 {
+    grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
+    grid_launch_dependents();
     const int o0 = op_start[blockIdx.x], o1 = op_start[blockIdx.x + 1];
     const int nx = mx + 2 * mbc, ny = my + 2 * mbc, nxy = nx * ny;
     RegOff R(mx, my, meqn);
@@ -199,6 +216,8 @@ __global__ void k_f2c(double* __restrict__ q, const double* __restrict__ regs, c
                       const SyncOp* __restrict__ ops, const int* __restrict__ op_start,
                       int mx, int my, int mbc, int meqn, int nreg)
 {
+    grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
+    grid_launch_dependents();
     const int o0 = op_start[blockIdx.x], o1 = op_start[blockIdx.x + 1];
     const int nx = mx + 2 * mbc, ny = my + 2 * mbc, nxy = nx * ny;
     RegOff R(mx, my, meqn);
@@ -248,6 +267,8 @@ __global__ void k_f2c(double* __restrict__ q, const double* __restrict__ regs, c
 __global__ void k_reset(double* __restrict__ regs, const PatchDesc* __restrict__ desc, int p0, int mx, int my,
                         int meqn, int nreg, int coarse_level, int mode)
 {
+    grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
+    grid_launch_dependents();
     const int p = p0 + blockIdx.x;
     const PatchDesc pd = desc[p];
     double* r = regs + (size_t)p * nreg;
@@ -286,6 +307,8 @@ __global__ void k_reset(double* __restrict__ regs, const PatchDesc* __restrict__
 __global__ void k_reset_sync(double* __restrict__ regs, const PatchDesc* __restrict__ desc, int p0, int mx, int my,
                              int meqn, int nreg, int minlevel, int maxl)
 {
+    grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
+    grid_launch_dependents();
     const int p = p0 + blockIdx.x;
     const PatchDesc pd = desc[p];
     const int L = pd.level;
@@ -519,45 +542,45 @@ void launch_restore_patches(const Dims& d, double* dst, const double* src, const
 
 void launch_copy(const Dims& d, double* dst, const double* src, const CopyEnt* e, int n, cudaStream_t st)
 {
-    if (n > 0) k_copy<<<nblk(n, 256), 256, 0, st>>>(dst, src, e, n, d.nxy(), d.meqn);
+    if (n > 0) launch_k(k_copy, nblk(n, 256), 256, 0, st, dst, src, e, n, d.nxy(), d.meqn);
 }
 void launch_average(const Dims& d, double* dst, const double* src, const AvgEnt* e, int n, const double* area,
                     cudaStream_t st)
 {
-    if (n > 0) k_average<<<nblk(n, 256), 256, 0, st>>>(dst, src, e, n, d.nq(), d.nx(), d.nxy(), d.meqn, area);
+    if (n > 0) launch_k(k_average, nblk(n, 256), 256, 0, st, dst, src, e, n, d.nq(), d.nx(), d.nxy(), d.meqn, area);
 }
 void launch_interp(const Dims& d, double* dst, const double* src, const InterpEnt* e, int n, cudaStream_t st)
 {
-    if (n > 0) k_interp<<<nblk(n, 256), 256, 0, st>>>(dst, src, e, n, d.nx(), d.nxy(), d.meqn);
+    if (n > 0) launch_k(k_interp, nblk(n, 256), 256, 0, st, dst, src, e, n, d.nx(), d.nxy(), d.meqn);
 }
 void launch_phys(const Dims& d, double* q, const PhysEnt* e, int n, const double* bcstate, cudaStream_t st)
 {
-    if (n > 0) k_phys<<<nblk(n, 256), 256, 0, st>>>(q, e, n, d.nxy(), d.meqn, bcstate);
+    if (n > 0) launch_k(k_phys, nblk(n, 256), 256, 0, st, q, e, n, d.nxy(), d.meqn, bcstate);
 }
 void launch_timeinterp(const Dims& d, const double* q, const double* qlast, double* qinterp, const int* patches,
                        int npatch, double alpha, cudaStream_t st)
 {
-    if (npatch > 0) k_timeinterp<<<npatch, 256, 0, st>>>(q, qlast, qinterp, patches, d.mx, d.my, d.mbc, d.meqn, alpha);
+    if (npatch > 0) launch_k(k_timeinterp, npatch, 256, 0, st, q, qlast, qinterp, patches, d.mx, d.my, d.mbc, d.meqn, alpha);
 }
 void launch_samesize(const Dims& d, double* q, const double* regs, const PatchDesc* desc, const SyncOp* ops,
                      const int* op_start, int npatch, cudaStream_t st)
 {
-    if (npatch > 0) k_samesize<<<npatch, 64, 0, st>>>(q, regs, desc, ops, op_start, d.mx, d.my, d.mbc, d.meqn, d.nreg());
+    if (npatch > 0) launch_k(k_samesize, npatch, 64, 0, st, q, regs, desc, ops, op_start, d.mx, d.my, d.mbc, d.meqn, d.nreg());
 }
 void launch_f2c(const Dims& d, double* q, const double* regs, const PatchDesc* desc, const SyncOp* ops,
                 const int* op_start, int npatch, cudaStream_t st)
 {
-    if (npatch > 0) k_f2c<<<npatch, 64, 0, st>>>(q, regs, desc, ops, op_start, d.mx, d.my, d.mbc, d.meqn, d.nreg());
+    if (npatch > 0) launch_k(k_f2c, npatch, 64, 0, st, q, regs, desc, ops, op_start, d.mx, d.my, d.mbc, d.meqn, d.nreg());
 }
 void launch_reset(const Dims& d, double* regs, const PatchDesc* desc, int p0, int np, int coarse_level, int mode,
                   cudaStream_t st)
 {
-    if (np > 0) k_reset<<<np, 64, 0, st>>>(regs, desc, p0, d.mx, d.my, d.meqn, d.nreg(), coarse_level, mode);
+    if (np > 0) launch_k(k_reset, np, 64, 0, st, regs, desc, p0, d.mx, d.my, d.meqn, d.nreg(), coarse_level, mode);
 }
 void launch_reset_sync(const Dims& d, double* regs, const PatchDesc* desc, int p0, int np, int minlevel, int maxl,
                        cudaStream_t st)
 {
-    if (np > 0) k_reset_sync<<<np, 64, 0, st>>>(regs, desc, p0, d.mx, d.my, d.meqn, d.nreg(), minlevel, maxl);
+    if (np > 0) launch_k(k_reset_sync, np, 64, 0, st, regs, desc, p0, d.mx, d.my, d.meqn, d.nreg(), minlevel, maxl);
 }
 void launch_patch_mass(const Dims& d, const double* q, const PatchDesc* desc, int np, double* out, cudaStream_t st,
                        const double* area)

@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 #include <type_traits>
 #include "fcb_common.h"
+#include "fcb_launch.cuh"
 #include "riemann.cuh"
 #include "k_mlp.cuh"
 
@@ -679,6 +680,8 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
              double* __restrict__ regs, const PatchDesc* __restrict__ desc, int p0, int npatch,
              const StepParams* __restrict__ spp, unsigned long long* __restrict__ cfl_bits)
 {
+    grid_dependency_wait();         // programmatic launch: the previous grid's writes are visible
+    grid_launch_dependents();
     const StepParams sp = *spp;     // per-launch parameters live in device memory (graph replay)
     __shared__ unsigned int nhist[RP::EXACT64 ? 32 : 1];
     if constexpr (!PERSIST) {

@@ -9,6 +9,7 @@
 // accumulations are the same in every variant, so the FP64 variants give
 // identical bits; the autotuner (host side) picks the fastest for a forest.
 #pragma once
+#include "fcb_launch.cuh"
 #include "k_step2.cuh"
 #include "kernels.h"
 
@@ -38,8 +39,7 @@ cudaError_t run_step2_variant(double* q, double* qlast, const double* aux, doubl
     }
     if (npatch <= 0) return cudaSuccess;
     const int grid = PERSIST ? (npatch < grid_cap ? npatch : grid_cap) : npatch;
-    kern<<<grid, NT, G::SMEM_BYTES, st>>>(q, qlast, aux, regs, desc, p0, npatch, sp, cfl_bits);
-    return cudaGetLastError();
+    return launch_k(kern, grid, NT, G::SMEM_BYTES, st, q, qlast, aux, regs, desc, p0, npatch, sp, cfl_bits);
 }
 
 // One table entry: precision, solver id, square patch size MXV (mbc 2), threads, min CTAs per SM.

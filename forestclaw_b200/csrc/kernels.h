@@ -6,6 +6,16 @@
 
 namespace fcb {
 
+// Programmatic dependent launch of the advance's kernels (fcb_launch.cuh): set
+// for the calling thread while a ProgrammaticScope lives.
+void set_programmatic_launch(bool on);
+bool programmatic_launch();
+struct ProgrammaticScope {
+    bool prev;
+    explicit ProgrammaticScope(bool on) : prev(programmatic_launch()) { set_programmatic_launch(on); }
+    ~ProgrammaticScope() { set_programmatic_launch(prev); }
+};
+
 struct Dims {
     int mx, my, mbc, meqn, maux;
     int nx() const { return mx + 2 * mbc; }

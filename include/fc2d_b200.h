@@ -237,6 +237,13 @@ int fc2d_b200_last_update_stats(const fc2d_b200_solver_t* s, double* update_ms, 
 /* Replay each fclaw2d_advance_all_levels as a CUDA graph captured once per
  * forest (on by default; disabled while update timing is on). */
 int fc2d_b200_set_graphs(fc2d_b200_solver_t* s, int enable);
+/* Launch the kernels of an advance (level updates, ghost-fill stages, time
+ * sync, time interpolation) with programmatic dependent launch: each grid is
+ * scheduled while its predecessor's last CTAs run and waits in-kernel for the
+ * predecessor's completion before touching memory, which hides the launch gap
+ * between the many short dependent grids of a subcycled step.  Results are
+ * identical either way.  On by default. */
+int fc2d_b200_set_programmatic_launch(fc2d_b200_solver_t* s, int enable);
 /* Enable/disable CUDA-event timing of the update kernels (off by default). */
 int fc2d_b200_set_timing(fc2d_b200_solver_t* s, int enable);
 
