@@ -3,8 +3,10 @@
 Test infrastructure (the checker's checker): ``oracle/_ref/libpin_cudaclaw.so``
 is built by ``make -C oracle ref`` from the reference tree's
 ``src/solvers/fc2d_cudaclaw/cuda_source/cudaclaw_flux2.cu`` and
-``cudaclaw_limiters.cu`` plus ``oracle/ref_cudaclaw/pin_harness.cu``.  Calling it
-needs a GPU; only the golden-vector script and the tests load it.
+``cudaclaw_limiters.cu``, the cudaclaw app Riemann solvers (swirl advection,
+radialdam Roe) and ``oracle/ref_cudaclaw/{pin_harness,
+ref_app_solvers}.cu``.  Calling it needs a GPU; only the golden-vector script and
+the tests load it.
 """
 from __future__ import annotations
 
@@ -38,9 +40,9 @@ def lib():
         L = ctypes.CDLL(LIB)
         dp = ctypes.POINTER(ctypes.c_double)
         ip = ctypes.POINTER(ctypes.c_int)
-        L.pin_cudaclaw_advection_step.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ip,
-                                                  ctypes.c_int, ctypes.c_double, dp, dp, dp, dp, dp]
-        L.pin_cudaclaw_advection_step.restype = ctypes.c_int
+        I = ctypes.c_int
+        L.pin_cudaclaw_step.argtypes = [I, I, I, I, I, I, I, I, I, ip, ip, ctypes.c_double, dp, dp, dp, dp, dp, dp]
+        L.pin_cudaclaw_step.restype = ctypes.c_int
         L.pin_cudaclaw_limiter.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int]
         L.pin_cudaclaw_limiter.restype = ctypes.c_int
         _lib = L
@@ -51,21 +53,31 @@ def _dp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
-def advection_step(q, aux, dx, dy, dt, order, mthlim, mbc=2):
-    """One cudaclaw update of scalar-advection patches.  q: (npatch, ny, nx) with
-    mbc ghost cells, aux: (npatch, 2, ny, nx) velocities; returns (q after, cfl per patch)."""
+SWIRL, RADIALDAM = 0, 1          # reference solver pairs
+
+
+def step(solver, q, aux, dx, dt, order, mthlim, use_fwaves=0, grav=1.0, dry_tolerance=1e-3, sea_level=0.0,
+         mbc=2):
+    """One cudaclaw update of square-cell patches.  q: (npatch, meqn, ny, nx) with mbc
+    ghost cells, aux: (npatch, maux, ny, nx) or None; returns (q after, cfl per patch)."""
     q = np.ascontiguousarray(q, np.float64).copy()
+    npatch, meqn, ny, nx = q.shape
+    if aux is None:
+        aux = np.zeros((npatch, 0, ny, nx))
     aux = np.ascontiguousarray(aux, np.float64)
-    npatch, ny, nx = q.shape
+    maux = aux.shape[1]
+    mwaves = len(mthlim)
     mx, my = nx - 2 * mbc, ny - 2 * mbc
-    dx = np.ascontiguousarray(np.broadcast_to(np.asarray(dx, np.float64), (npatch,)))
-    dy = np.ascontiguousarray(np.broadcast_to(np.asarray(dy, np.float64), (npatch,)))
+    d = np.full(npatch, float(dx))
     cfl = np.zeros(npatch)
+    prm = np.array([grav, dry_tolerance, sea_level], np.float64)
     o = (ctypes.c_int * 2)(*order)
-    rc = lib().pin_cudaclaw_advection_step(mx, my, mbc, npatch, o, int(mthlim), float(dt), _dp(dx), _dp(dy),
-                                           _dp(q), _dp(aux), _dp(cfl))
+    lim = (ctypes.c_int * mwaves)(*mthlim)
+    auxp = aux if maux > 0 else np.zeros(1)
+    rc = lib().pin_cudaclaw_step(solver, mx, my, mbc, meqn, maux, mwaves, int(use_fwaves), npatch, o, lim,
+                                 float(dt), _dp(d), _dp(d), _dp(prm), _dp(q), _dp(auxp), _dp(cfl))
     if rc != 0:
-        raise RuntimeError(f"cudaclaw update failed: CUDA error {rc}")
+        raise RuntimeError(f"cudaclaw update failed: code {rc}")
     return q, cfl
 
 

@@ -17,13 +17,8 @@
 // 5 meqn + 6 maux); per-patch scratch as cudaclaw_allocate_fluxes
 // (cudaclaw_allocate.cu:44-90), speeds zeroed.
 //
-// The Riemann solvers are the scalar advection pair of the reference's cudaclaw
-// swirl app (applications/cudaclaw/advection/2d/swirl/user_cuda/rpn2adv.cu:8-30,
-// rpt2adv.cu:6-20), restated here because that app's headers pull in the whole
-// framework: wave = qr - ql, speed = the right cell's velocity component idir,
-// transverse speeds from the aux of the row below / above.  They are the
-// clawpack 4.6 advection solvers (clawpack46_rpn2adv.f, clawpack46_rpt2adv.f)
-// in the cudaclaw calling convention.
+// The Riemann solvers are the reference's own cudaclaw app solvers
+// (ref_app_solvers.cu): swirl advection and radialdam Roe shallow water.
 #include <cuda_runtime.h>
 #include <cstring>
 #include <vector>
@@ -38,31 +33,8 @@ __global__ void cudaclaw_flux2_and_update_batch(const int mx, const int my, cons
 extern "C" void cudaclaw_set_method_parameters(int* order_in, int* mthlim_in, int mwaves, int use_fwaves_in);
 __device__ double cudaclaw_limiter(int lim_choice, double r);
 
-__device__ void pin_rpn2adv(int idir, int meqn, int mwaves, int maux, double ql[], double qr[], double auxl[],
-                            double auxr[], double wave[], double s[], double amdq[], double apdq[])
-{
-    (void)mwaves; (void)maux; (void)auxl;
-    for (int mq = 0; mq < meqn; mq++) wave[mq] = qr[mq] - ql[mq];
-    s[0] = auxr[idir];
-    for (int mq = 0; mq < meqn; mq++) {
-        amdq[mq] = fmin(s[0], 0.0) * wave[mq];
-        apdq[mq] = fmax(s[0], 0.0) * wave[mq];
-    }
-}
-
-__device__ void pin_rpt2adv(int idir, int meqn, int mwaves, int maux, double ql[], double qr[], double aux1[],
-                            double aux2[], double aux3[], int imp, double asdq[], double bmasdq[], double bpasdq[])
-{
-    (void)mwaves; (void)ql; (void)qr; (void)aux1;
-    const int kv = 1 - idir;
-    for (int mq = 0; mq < meqn; mq++) {
-        bmasdq[mq] = fmin(aux2[imp * maux + kv], 0.0) * asdq[mq];
-        bpasdq[mq] = fmax(aux3[imp * maux + kv], 0.0) * asdq[mq];
-    }
-}
-
-__device__ cudaclaw_cuda_rpn2_t pin_rpn2 = pin_rpn2adv;
-__device__ cudaclaw_cuda_rpt2_t pin_rpt2 = pin_rpt2adv;
+extern "C" int pin_ref_solver(int id, double grav, double dry_tolerance, double sea_level,
+                              cudaclaw_cuda_rpn2_t* rpn2, cudaclaw_cuda_rpt2_t* rpt2);
 
 __global__ void pin_limiter_kernel(int lim, const double* r, double* phi, int n)
 {
@@ -74,14 +46,16 @@ __global__ void pin_limiter_kernel(int lim, const double* r, double* phi, int n)
 
 extern "C" {
 
-// One update of npatch scalar-advection patches (meqn = maux-velocity = 1 wave):
-// q[npatch][nx*ny] in/out (fields of a patch i fastest, mbc ghost cells),
-// aux[npatch][2][nx*ny] (u, v), dx[p], dy[p]; cfl[p] = the kernel's block maximum.
-// Returns 0 or the CUDA error code.
-int pin_cudaclaw_advection_step(int mx, int my, int mbc, int npatch, const int* order, int mthlim, double dt,
-                                const double* dx, const double* dy, double* q, const double* aux, double* cfl)
+// One update of npatch patches with reference solver pair `solver`
+// (pin_ref_solver): q[npatch][meqn][ny][nx] in/out (i fastest, mbc ghost cells),
+// aux[npatch][maux][ny][nx], dx[p], dy[p], mthlim[mwaves], prm = (grav,
+// dry_tolerance, sea_level); cfl[p] = what the kernel stores per block.
+// Returns 0, -1 for a bad argument, or the CUDA error code.
+int pin_cudaclaw_step(int solver, int mx, int my, int mbc, int meqn, int maux, int mwaves, int use_fwaves,
+                      int npatch, const int* order, const int* mthlim, double dt, const double* dx, const double* dy,
+                      const double* prm, double* q, const double* aux, double* cfl)
 {
-    const int meqn = 1, maux = 2, mwaves = 1;
+    if (mwaves < 1 || mwaves > FC2D_CUDACLAW_MWAVES || meqn < 1 || maux < 0 || npatch < 1 || mbc < 2) return -1;
     const size_t size = (size_t)(2 * mbc + mx) * (2 * mbc + my);
     cudaError_t err = cudaSuccess;
     std::vector<cudaclaw_fluxes_t> F(npatch);
@@ -90,16 +64,18 @@ int pin_cudaclaw_advection_step(int mx, int my, int mbc, int npatch, const int* 
     cudaclaw_fluxes_t* Fd = nullptr;
     cudaclaw_cuda_rpn2_t rpn2 = nullptr;
     cudaclaw_cuda_rpt2_t rpt2 = nullptr;
-    int ord[2] = {order[0], order[1]}, lim[1] = {mthlim};
+    int ord[2] = {order[0], order[1]};
+    std::vector<int> lim(mthlim, mthlim + mwaves);
     const int mwork1 = 4 * meqn + 2 * maux + mwaves + meqn * mwaves, mwork2 = 5 * meqn + 6 * maux;
     const int mwork = mwork1 > mwork2 ? mwork1 : mwork2;
     const int block = FC2D_CUDACLAW_BLOCK_SIZE;
+    if (pin_ref_solver(solver, prm[0], prm[1], prm[2], &rpn2, &rpt2) != 0) return -1;
     PIN_CK(cudaMalloc(&qd, sizeof(double) * npatch * meqn * size));
-    PIN_CK(cudaMalloc(&ad, sizeof(double) * npatch * maux * size));
+    PIN_CK(cudaMalloc(&ad, sizeof(double) * npatch * (maux > 0 ? maux : 1) * size));
     PIN_CK(cudaMalloc(&cd, sizeof(double) * npatch));
     PIN_CK(cudaMalloc(&Fd, sizeof(cudaclaw_fluxes_t) * npatch));
     PIN_CK(cudaMemcpy(qd, q, sizeof(double) * npatch * meqn * size, cudaMemcpyHostToDevice));
-    PIN_CK(cudaMemcpy(ad, aux, sizeof(double) * npatch * maux * size, cudaMemcpyHostToDevice));
+    if (maux > 0) PIN_CK(cudaMemcpy(ad, aux, sizeof(double) * npatch * maux * size, cudaMemcpyHostToDevice));
     for (int p = 0; p < npatch; p++) {
         cudaclaw_fluxes_t& f = F[p];
         std::memset(&f, 0, sizeof(f));
@@ -118,9 +94,7 @@ int pin_cudaclaw_advection_step(int mx, int my, int mbc, int npatch, const int* 
         f.dx = dx[p]; f.dy = dy[p];
     }
     PIN_CK(cudaMemcpy(Fd, F.data(), sizeof(cudaclaw_fluxes_t) * npatch, cudaMemcpyHostToDevice));
-    PIN_CK(cudaMemcpyFromSymbol(&rpn2, pin_rpn2, sizeof(rpn2)));
-    PIN_CK(cudaMemcpyFromSymbol(&rpt2, pin_rpt2, sizeof(rpt2)));
-    cudaclaw_set_method_parameters(ord, lim, mwaves, 0);
+    cudaclaw_set_method_parameters(ord, lim.data(), mwaves, use_fwaves);
     cudaclaw_flux2_and_update_batch<<<dim3(1, 1, npatch), dim3(block, 1, 1), sizeof(double) * mwork * block>>>(
         mx, my, meqn, mbc, maux, mwaves, mwork, dt, 0.0, Fd, cd, rpn2, rpt2, nullptr);
     PIN_CK(cudaGetLastError());

@@ -1,23 +1,25 @@
 """The CPU oracle pinned against the reference's own CUDA patch update.
 
 The reference's ``cudaclaw_flux2_and_update_batch`` and ``cudaclaw_limiter``
-(src/solvers/fc2d_cudaclaw/cuda_source/cudaclaw_flux2.cu, cudaclaw_limiters.cu),
-compiled from the reference tree into oracle/_ref/libpin_cudaclaw.so, advanced
-seeded scalar-advection patches on a B200; ``tests/golden/make_cudaclaw_pin.py``
-stored the results in ``tests/golden/cudaclaw_advection_pin.npz``.  The oracle's
-clawpack 4.6 update (normal solves, wave limiting with every limiter the
-reference's GPU solver has, second-order corrections, transverse propagation,
-the conservative update) must give the same interior cells to rounding, and the
-same limiter values bit for bit.  The FP64 CUDA kernels are bitwise equal to the
-oracle (test_gpu_parity), so this pins them too.
+(src/solvers/fc2d_cudaclaw/cuda_source/cudaclaw_flux2.cu, cudaclaw_limiters.cu)
+with the reference's cudaclaw app Riemann solvers -- swirl advection (also in
+the f-wave form of the update) and radialdam Roe shallow water -- compiled from
+the reference tree into oracle/_ref/libpin_cudaclaw.so, advanced seeded patches
+on a B200; ``tests/golden/make_cudaclaw_pin.py`` stored the results in
+``tests/golden/cudaclaw_pin.npz``.  The oracle's clawpack 4.6 update (normal
+solves, wave limiting with every limiter the reference's GPU solver has,
+second-order corrections, transverse propagation, the conservative update) with
+its clawpack 4.6 Riemann solvers must give the same interior cells to rounding,
+and the same limiter values bit for bit.  The FP64 CUDA kernels are bitwise
+equal to the oracle (test_gpu_parity), so this pins them too.
 
 Tolerance: the reference adds the transverse terms with atomicAdd in whatever
 order the threads arrive and lets nvcc contract multiply-adds; the oracle keeps
-the Fortran order without contraction.  Per cell the results differ by a few
-units in the last place: |q_oracle - q_reference| <= 2e-15 max |q| (observed
-worst case 1.8e-16).  The reference's per-patch CFL is not compared: every
-thread stores the result of a block reduction that only thread 0 holds
-(cudaclaw_flux2.cu:462).
+the Fortran order without contraction (and the Fortran Roe solver forms apdq as
+the total fluctuation minus amdq).  Per cell the results differ by a few units
+in the last place: |q_oracle - q_reference| <= 2e-15 max |q| per field.  The
+reference's per-patch CFL is not compared: every thread stores the result of a
+block reduction that only thread 0 holds (cudaclaw_flux2.cu:462).
 """
 from __future__ import annotations
 
@@ -32,26 +34,30 @@ REL_TOL = 2e-15
 MBC = 2
 
 
-def _oracle_step(q, aux, dx, dt, order, lim):
+def _oracle_step(family, q, aux, dx, dt, order, lim):
     from oracle import pyoracle as po
-    npatch, n, _ = q.shape
+    solver, meqn, maux, fw, grav, _ = mk.FAMILIES[family]
+    rp = {0: po.RP_ADVECTION, 1: po.RP_SW_ROE}[solver]
+    npatch, _, n, _ = q.shape
     mx = n - 2 * MBC
-    cfg = po.make_config(mx=mx, my=mx, mbc=MBC, meqn=1, maux=2, mwaves=1, rp=po.RP_ADVECTION,
-                         order=tuple(order), mthlim=(int(lim),) * 8)
+    cfg = po.make_config(mx=mx, my=mx, mbc=MBC, meqn=meqn, maux=maux, mwaves=len(lim), rp=rp, use_fwaves=fw,
+                         grav=grav, order=tuple(order), mthlim=tuple(int(v) for v in lim) + (0,) * (8 - len(lim)))
     out = np.empty_like(q)
     for p in range(npatch):
         qq = np.ascontiguousarray(q[p]).ravel().copy()
-        po.patch_step2(cfg, qq, np.ascontiguousarray(aux[p]).ravel().copy(), dx, dx, dt)
-        out[p] = qq.reshape(n, n)
+        a = np.ascontiguousarray(aux[p]).ravel().copy() if aux is not None else None
+        po.patch_step2(cfg, qq, a, dx, dx, dt)
+        out[p] = qq.reshape(q.shape[1:])
     return out
 
 
 def _assert_close(out, ref, what):
     s = slice(MBC, -MBC)
     for p in range(ref.shape[0]):
-        scale = np.abs(ref[p][s, s]).max()
-        err = np.abs(out[p][s, s] - ref[p][s, s]).max()
-        assert err <= REL_TOL * scale, f"{what} patch {p}: max |dq| {err:.3e} > {REL_TOL:g} x {scale:.3e}"
+        for m in range(ref.shape[1]):
+            scale = np.abs(ref[p, m][s, s]).max()
+            err = np.abs(out[p, m][s, s] - ref[p, m][s, s]).max()
+            assert err <= REL_TOL * scale, f"{what} patch {p} field {m}: max |dq| {err:.3e} > {REL_TOL:g} x {scale:.3e}"
 
 
 def _fixture():
@@ -60,25 +66,30 @@ def _fixture():
     return np.load(mk.OUT)
 
 
-def test_fixture_inputs_are_reproducible():
-    """The stored inputs are those of the seeded generator, so the live GPU test
-    below and the fixture exercise the same kind of data."""
+@pytest.mark.parametrize("family", sorted(mk.FAMILIES))
+def test_fixture_inputs_are_reproducible(family):
+    """The stored inputs are those of the seeded generator."""
     d = _fixture()
-    q, aux, dx, dt = mk.inputs()
-    assert np.array_equal(q, d["q_in"]) and np.array_equal(aux, d["aux"])
-    assert float(d["dx"]) == dx and float(d["dt"]) == dt
+    q, aux, dx, dt = mk.inputs(family)
+    assert np.array_equal(q, d[f"{family}_q_in"])
+    assert (aux is None) == (f"{family}_aux" not in d.files)
+    if aux is not None:
+        assert np.array_equal(aux, d[f"{family}_aux"])
+    assert float(d[f"{family}_dx"]) == dx and float(d[f"{family}_dt"]) == dt
 
 
-def test_oracle_update_matches_reference_cudaclaw():
+@pytest.mark.parametrize("family", sorted(mk.FAMILIES))
+def test_oracle_update_matches_reference_cudaclaw(family):
     d = _fixture()
-    q, aux, dx, dt = d["q_in"], d["aux"], float(d["dx"]), float(d["dt"])
-    assert len(d["orders"]) == len(mk.CASES)
-    for k, (order, lim) in enumerate(zip(d["orders"], d["limiters"])):
-        ref = d[f"q_out_{k}"]
+    q = d[f"{family}_q_in"]
+    aux = d[f"{family}_aux"] if f"{family}_aux" in d.files else None
+    dx, dt = float(d[f"{family}_dx"]), float(d[f"{family}_dt"])
+    for k, (order, lim) in enumerate(mk.FAMILIES[family][5]):
+        ref = d[f"{family}_q_out_{k}"]
         # the reference updates the interior only; its ghost cells are the inputs
-        assert np.array_equal(ref[:, :MBC], q[:, :MBC]) and np.array_equal(ref[:, -MBC:], q[:, -MBC:])
+        assert np.array_equal(ref[..., :MBC, :], q[..., :MBC, :]) and np.array_equal(ref[..., -MBC:], q[..., -MBC:])
         assert not np.array_equal(ref, q)
-        _assert_close(_oracle_step(q, aux, dx, dt, order, lim), ref, f"order {tuple(order)} limiter {lim}")
+        _assert_close(_oracle_step(family, q, aux, dx, dt, order, lim), ref, f"{family} order {order} limiters {lim}")
 
 
 def test_oracle_limiters_match_reference_cudaclaw_bitwise():
@@ -91,13 +102,16 @@ def test_oracle_limiters_match_reference_cudaclaw_bitwise():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("seed", [1, 2, 3])
-def test_oracle_update_matches_reference_cudaclaw_live(seed):
+@pytest.mark.parametrize("family", sorted(mk.FAMILIES))
+@pytest.mark.parametrize("seed", [1, 2])
+def test_oracle_update_matches_reference_cudaclaw_live(family, seed):
     """The same comparison on fresh seeds, running the reference's kernel now."""
     from oracle import pin_reference as pr
     if not pr.available():
         pytest.skip("oracle/_ref/libpin_cudaclaw.so not built (reference tree absent at build time)")
-    q, aux, dx, dt = mk.inputs(seed=seed, npatch=8)
-    for order, lim in mk.CASES:
-        ref, _ = pr.advection_step(q, aux, dx, dx, dt, order, lim)
-        _assert_close(_oracle_step(q, aux, dx, dt, order, lim), ref, f"seed {seed} order {order} limiter {lim}")
+    solver, _, _, fw, grav, cases = mk.FAMILIES[family]
+    q, aux, dx, dt = mk.inputs(family, seed=seed, npatch=8)
+    for order, lim in cases:
+        ref, _ = pr.step(solver, q, aux, dx, dt, order, lim, use_fwaves=fw, grav=grav)
+        _assert_close(_oracle_step(family, q, aux, dx, dt, order, lim), ref,
+                      f"{family} seed {seed} order {order} limiters {lim}")
