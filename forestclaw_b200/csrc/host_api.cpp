@@ -71,7 +71,7 @@ struct DevVec {
 
 struct LevelRanges {
     int copy_off = 0, copy_n = 0, avg_off = 0, avg_n = 0, interp_off = 0, interp_n = 0, phys_off = 0, phys_n = 0;
-    int ti_off = 0, ti_n = 0, ss_off = 0, ss_start_off = 0, ss_np = 0, f2c_off = 0, f2c_start_off = 0, f2c_np = 0;
+    int ti_off = 0, ti_n = 0, sync_off = 0, sync_start_off = 0, sync_np = 0;
 };
 
 struct fc2d_b200_solver {
@@ -120,8 +120,8 @@ struct fc2d_b200_solver {
     DevVec<double> minmax_dev;
     DevVec<InterpEnt> t_interp;
     DevVec<PhysEnt> t_phys;
-    DevVec<int> t_ti, t_ss_start, t_f2c_start;
-    DevVec<SyncOp> t_ss, t_f2c;
+    DevVec<int> t_ti, t_sync_start;
+    DevVec<SyncOp> t_sync;
     LevelRanges lr[33];
     unsigned long long* cfl_dev = nullptr;
     unsigned long long* cfl_host = nullptr;
@@ -264,8 +264,8 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
     std::vector<AvgEnt> avg;
     std::vector<InterpEnt> interp;
     std::vector<PhysEnt> phys;
-    std::vector<int> ti, ss_start, f2c_start;
-    std::vector<SyncOp> ss, f2c;
+    std::vector<int> ti, sync_start;
+    std::vector<SyncOp> sync;
     for (int l = 0; l < 33; l++) {
         LevelRanges& r = s->lr[l];
         r = LevelRanges();
@@ -276,22 +276,18 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
         interp.insert(interp.end(), L.interp.begin(), L.interp.end());
         r.phys_off = (int)phys.size(); r.phys_n = (int)L.phys.size(); phys.insert(phys.end(), L.phys.begin(), L.phys.end());
         r.ti_off = (int)ti.size(); r.ti_n = (int)L.ti.size(); ti.insert(ti.end(), L.ti.begin(), L.ti.end());
-        r.ss_off = (int)ss.size(); r.ss_start_off = (int)ss_start.size(); r.ss_np = (int)L.ss_start.size() - 1;
-        ss.insert(ss.end(), L.ss.begin(), L.ss.end());
-        for (int v : L.ss_start) ss_start.push_back(v + r.ss_off);
-        r.f2c_off = (int)f2c.size(); r.f2c_start_off = (int)f2c_start.size(); r.f2c_np = (int)L.f2c_start.size() - 1;
-        f2c.insert(f2c.end(), L.f2c.begin(), L.f2c.end());
-        for (int v : L.f2c_start) f2c_start.push_back(v + r.f2c_off);
+        r.sync_off = (int)sync.size(); r.sync_start_off = (int)sync_start.size();
+        r.sync_np = (int)L.sync_start.size() - 1;
+        sync.insert(sync.end(), L.sync.begin(), L.sync.end());
+        for (int v : L.sync_start) sync_start.push_back(v + r.sync_off);
     }
     CK(s->t_copy.assign(copy, s->st));
     CK(s->t_avg.assign(avg, s->st));
     CK(s->t_interp.assign(interp, s->st));
     CK(s->t_phys.assign(phys, s->st));
     CK(s->t_ti.assign(ti, s->st));
-    CK(s->t_ss.assign(ss, s->st));
-    CK(s->t_ss_start.assign(ss_start, s->st));
-    CK(s->t_f2c.assign(f2c, s->st));
-    CK(s->t_f2c_start.assign(f2c_start, s->st));
+    CK(s->t_sync.assign(sync, s->st));
+    CK(s->t_sync_start.assign(sync_start, s->st));
     CK(cudaStreamSynchronize(s->st));
     return 0;
 }
@@ -439,31 +435,24 @@ static void ghost_update(fc2d_b200_solver* s, int minlevel, int maxlevel, int ti
     if (time_interp) phys_range(s, minlevel - 1, minlevel - 1, 1);
 }
 
-// fclaw2d_time_sync(minlevel, maxlevel) as three launches: the same-size
-// corrections of every synced level, the fine-to-coarse corrections of every
-// synced coarse level, then every register reset.  Per level the reference runs
-// samesize, reset, f2c, reset; the corrections of different levels touch
-// disjoint cells and read only registers no earlier reset of the sync touches
-// (f2c reads half-size faces of the coarse level and double-size faces of the
-// fine level), so the merged order gives the same values.
+// fclaw2d_time_sync(minlevel, maxlevel) as two launches: every correction of
+// the synced levels (same-size and fine-to-coarse, grouped per patch), then
+// every register reset.  Per level the reference runs samesize, reset, f2c,
+// reset; the corrections of different levels touch disjoint cells and read only
+// registers no earlier reset of the sync touches (f2c reads half-size faces of
+// the coarse level and double-size faces of the fine level), so the merged
+// order gives the same values.
 static void time_sync(fc2d_b200_solver* s, int minlevel, int maxlevel)
 {
     (void)maxlevel;
     const int maxl = std::min(s->o.maxlevel, 32);
     int a = std::max(minlevel, 0);
     if (a > maxl) return;
-    {   // samesize, levels [a, maxl]
-        const int g0 = s->lr[a].ss_start_off, g1 = s->lr[maxl].ss_start_off + s->lr[maxl].ss_np;
+    {   // samesize and f2c corrections, levels [a, maxl]
+        const int g0 = s->lr[a].sync_start_off, g1 = s->lr[maxl].sync_start_off + s->lr[maxl].sync_np;
         if (g1 > g0) {
             if (s->fill) s->total_launches++;
-            if (s->emit) launch_samesize(s->d, s->q, s->regs, s->desc, s->t_ss.p, s->t_ss_start.p + g0, g1 - g0, s->st);
-        }
-    }
-    if (a <= maxl - 1) {   // f2c, coarse levels [a, maxl-1]
-        const int g0 = s->lr[a].f2c_start_off, g1 = s->lr[maxl - 1].f2c_start_off + s->lr[maxl - 1].f2c_np;
-        if (g1 > g0) {
-            if (s->fill) s->total_launches++;
-            if (s->emit) launch_f2c(s->d, s->q, s->regs, s->desc, s->t_f2c.p, s->t_f2c_start.p + g0, g1 - g0, s->st);
+            if (s->emit) launch_sync(s->d, s->q, s->regs, s->desc, s->t_sync.p, s->t_sync_start.p + g0, g1 - g0, s->st);
         }
     }
     const int p0 = s->forest.lev_off[a], p1 = s->forest.lev_off[maxl + 1];

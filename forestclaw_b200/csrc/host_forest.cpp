@@ -453,7 +453,7 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<
     for (int l = 0; l < 33; l++) {
         LevelTables& LT = out[l];
         const int p0 = f.lev_off[l], p1 = f.lev_off[l + 1];
-        if (p0 == p1) { LT.ss_start.assign(1, 0); LT.f2c_start.assign(1, 0); continue; }
+        if (p0 == p1) { LT.sync_start.assign(1, 0); continue; }
         // ---- copy2ghost: face pass then corner pass (fclaw2d_clawpatch46_copy.f) ----
         {
             LastWriter<CopyEnt> W(slots, T.nq, nxy);
@@ -635,33 +635,34 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<
         // ---- time interpolation patches ----
         for (int ip = p0; ip < p1; ip++) if (f.p[ip].has_fine_nbr) LT.ti.push_back(ip);
         // ---- time sync ops ----
-        LT.ss_start.push_back(0);
+        // fclaw2d_time_sync applies the same-size corrections of every synced level,
+        // then the fine-to-coarse ones (src/fclaw2d_time_sync.c:118-202); each
+        // correction adds to cells of its own patch p only and reads registers no
+        // correction writes, so per patch the samesize ops (faces 0..3) followed by
+        // the f2c ops ((face, igrid) order) give every cell its additions in the
+        // reference's order.  Levels without finer neighbours have no f2c ops, so
+        // one range of levels [a, maxlevel] covers both kinds.
+        LT.sync_start.push_back(0);
         for (int ip = p0; ip < p1; ip++) {
             const PatchInfo& P = f.p[ip];
             int nops = 0;
             for (int fc = 0; fc < 4; fc++)
                 if (P.face_type[fc] == NB_SAME && (!f.sphere() || f.p[P.face_nbr[fc][0]].block == P.block)) {
-                    LT.ss.push_back({ip, P.face_nbr[fc][0], fc, 0, 0, {0, 0, 0}});
+                    LT.sync.push_back({ip, P.face_nbr[fc][0], fc, 0, 0, SYNC_SAMESIZE, {0, 0}});
                     nops++;
                 }
-            if (nops) LT.ss_start.push_back((int)LT.ss.size());
-        }
-        LT.f2c_start.push_back(0);
-        for (int ip = p0; ip < p1; ip++) {
-            const PatchInfo& C = f.p[ip];
-            int nops = 0;
             for (int fc = 0; fc < 4; fc++) {
-                if (C.face_type[fc] != NB_HALF) continue;
-                if (f.sphere() && f.p[C.face_nbr[fc][0]].block != C.block) continue;
+                if (P.face_type[fc] != NB_HALF) continue;
+                if (f.sphere() && f.p[P.face_nbr[fc][0]].block != P.block) continue;
                 for (int ig = 0; ig < 2; ig++) {
-                    const int fi = C.face_nbr[fc][ig];
+                    const int fi = P.face_nbr[fc][ig];
                     const PatchInfo& F = f.p[fi];
-                    const int noff = (fc < 2) ? (2 * C.gy - F.gy) * my : (2 * C.gx - F.gx) * mx;
-                    LT.f2c.push_back({ip, fi, fc, ig, noff, {0, 0, 0}});
+                    const int noff = (fc < 2) ? (2 * P.gy - F.gy) * my : (2 * P.gx - F.gx) * mx;
+                    LT.sync.push_back({ip, fi, fc, ig, noff, SYNC_F2C, {0, 0}});
                     nops++;
                 }
             }
-            if (nops) LT.f2c_start.push_back((int)LT.f2c.size());
+            if (nops) LT.sync_start.push_back((int)LT.sync.size());
         }
     }
     int bad = -1;

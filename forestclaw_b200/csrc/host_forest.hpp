@@ -101,8 +101,7 @@ struct LevelTables {
     std::vector<InterpEnt> interp;   // interpolate2ghost(level): level is the coarse level
     std::vector<PhysEnt> phys;       // setphysical(level)
     std::vector<int> ti;             // patches with fine-grid neighbours (fclaw2d_timeinterp)
-    std::vector<SyncOp> ss; std::vector<int> ss_start;   // time_sync_samesize ops grouped per patch
-    std::vector<SyncOp> f2c; std::vector<int> f2c_start; // time_sync_f2c ops grouped per coarse patch
+    std::vector<SyncOp> sync; std::vector<int> sync_start;   // time-sync corrections grouped per patch
 };
 
 // inflow: mthbc = 0 sides are set to a constant state (PhysEnt.pad = 1, src unused).

@@ -158,109 +158,117 @@ struct RegOff {
     }
 };
 
-// clawpack46_fort_time_sync_samesize (same orientation, sc = 1): one CTA per
-// patch, faces in order 0..3 so corner cells see both corrections in order.
-__global__ void k_samesize(double* __restrict__ q, const double* __restrict__ regs, const PatchDesc* __restrict__ desc,
-                           const SyncOp* __restrict__ ops, const int* __restrict__ op_start,
-                           int mx, int my, int mbc, int meqn, int nreg)
+// The corrections of a time sync, one CTA per patch with corrections and one
+// thread per (boundary cell of the interior, field).  A face of a patch is
+// either same-size (one samesize op) or half-size (two f2c ops, igrid 0 and 1),
+// so a cell sees at most the ops of its x face and of its y face; the CTA first
+// files the patch's ops by face in shared memory, then each thread applies the
+// ops of its cell in table order -- samesize of the x face, of the y face, then
+// f2c of the x face, of the y face -- which is the reference's order of the
+// additions to that cell.  Every op reads registers only, which no correction
+// writes, so the cells are independent.
+//   samesize: clawpack46_fort_time_sync_samesize (same orientation, sc = 1),
+//             clawpack46_time_sync.f:528-704: delta = (ef_n - ef_t) - (f_n - f_t),
+//             q += 0.5 delta / area
+//   f2c:      clawpack46_fort_time_sync_f2c (same orientation, sc = 1),
+//             clawpack46_time_sync.f:254-498: the fine pair d, d+1 (d = 1 + n_off + 2 j)
+//             of coarse cell j, skipped when outside the fine face; q += deltac / area
+__global__ void k_sync(double* __restrict__ q, const double* __restrict__ regs, const PatchDesc* __restrict__ desc,
+                       const SyncOp* __restrict__ ops, const int* __restrict__ op_start,
+                       int mx, int my, int mbc, int meqn, int nreg)
 {
     grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
+    __shared__ SyncOp s_op[8];
+    __shared__ int s_ss[4], s_fc[4][2];                       // op slots per face (-1: none)
     const int o0 = op_start[blockIdx.x], o1 = op_start[blockIdx.x + 1];
-    const int nx = mx + 2 * mbc, ny = my + 2 * mbc, nxy = nx * ny;
-    RegOff R(mx, my, meqn);
-    for (int o = o0; o < o1; o++) {
-        const SyncOp op = ops[o];
-        const double* rt = regs + (size_t)op.p * nreg;
-        const double* rn = regs + (size_t)op.n * nreg;
-        const PatchDesc pd = desc[op.p];
-        const double area = pd.dx * pd.dy;
-        double* qp = q + (size_t)op.p * nxy * meqn;
-        const int nt = (op.face < 2) ? my : mx;
-        for (int t = threadIdx.x; t < nt * meqn; t += blockDim.x) {
-            const int j = t % nt, m = t / nt;                      // j: 0-based tangential index
-            double delta;
-            int ic, jc;
-            if (op.face == 0) {
-                double fp = rn[R.fp1 + j + m * my];
-                double ef = 1 * rn[R.ef1 + j + m * my + my * meqn];
-                delta = (ef - rt[R.ef0 + j + m * my]) - (fp - rt[R.fp0 + j + m * my]);
-                ic = mbc; jc = mbc + j;
-            } else if (op.face == 1) {
-                double fm = rn[R.fm0 + j + m * my];
-                double ef = 1 * rn[R.ef0 + j + m * my + my * meqn];
-                delta = (rt[R.ef1 + j + m * my] - ef) - (fm - rt[R.fm1 + j + m * my]);
-                ic = mx + mbc - 1; jc = mbc + j;
-            } else if (op.face == 2) {
-                double gp = rn[R.gp1 + j + m * mx];
-                double ef = 1 * rn[R.ef3 + j + m * mx + mx * meqn];
-                delta = (ef - rt[R.ef2 + j + m * mx]) - (gp - rt[R.gp0 + j + m * mx]);
-                ic = mbc + j; jc = mbc;
-            } else {
-                double gm = rn[R.gm0 + j + m * mx];
-                double ef = 1 * rn[R.ef2 + j + m * mx + mx * meqn];
-                delta = (rt[R.ef3 + j + m * mx] - ef) - (gm - rt[R.gm1 + j + m * mx]);
-                ic = mbc + j; jc = my + mbc - 1;
-            }
-            double* qq = qp + (size_t)m * nxy + jc * nx + ic;
-            *qq = *qq + 0.5 * delta / area;
-        }
-        __syncthreads();
+    const int nops = o1 - o0;                                  // <= 8: two ops on each of four faces
+    if (nops <= 0 || nops > 8) return;
+    if (threadIdx.x < 4) { s_ss[threadIdx.x] = -1; s_fc[threadIdx.x][0] = -1; s_fc[threadIdx.x][1] = -1; }
+    __syncthreads();
+    if (threadIdx.x < nops) {
+        const SyncOp op = ops[o0 + threadIdx.x];
+        s_op[threadIdx.x] = op;
+        if (op.kind == SYNC_SAMESIZE) s_ss[op.face & 3] = threadIdx.x;
+        else s_fc[op.face & 3][op.igrid & 1] = threadIdx.x;
     }
-}
-
-// clawpack46_fort_time_sync_f2c (same orientation, sc = 1): one CTA per coarse
-// patch; ops ordered (face, igrid) as in cb_face_fill.  n_off = first fine index
-// offset (2*Cg - Fg)*n along the face.
-__global__ void k_f2c(double* __restrict__ q, const double* __restrict__ regs, const PatchDesc* __restrict__ desc,
-                      const SyncOp* __restrict__ ops, const int* __restrict__ op_start,
-                      int mx, int my, int mbc, int meqn, int nreg)
-{
-    grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
-    grid_launch_dependents();
-    const int o0 = op_start[blockIdx.x], o1 = op_start[blockIdx.x + 1];
+    __syncthreads();
+    const int p = s_op[0].p;                                   // every op of the block corrects patch p
     const int nx = mx + 2 * mbc, ny = my + 2 * mbc, nxy = nx * ny;
+    const int ring = 2 * (mx + my) - 4;                        // interior cells on the patch boundary
+    const double area = desc[p].dx * desc[p].dy;
     RegOff R(mx, my, meqn);
-    for (int o = o0; o < o1; o++) {
-        const SyncOp op = ops[o];
-        const double* rc = regs + (size_t)op.p * nreg;
-        const double* rf = regs + (size_t)op.n * nreg;
-        const PatchDesc pd = desc[op.p];
-        const double areac = pd.dx * pd.dy;
-        double* qp = q + (size_t)op.p * nxy * meqn;
-        const int nt = (op.face < 2) ? my : mx;
-        for (int t = threadIdx.x; t < nt * meqn; t += blockDim.x) {
-            const int jcn = t % nt, m = t / nt;                 // 0-based coarse tangential index
-            const int d = 1 + op.n_off + 2 * jcn;               // first fine child (Fortran index)
-            if (d < 1 || d + 1 > nt) continue;                  // fc46_skip_this_grid
-            const int f0 = d - 1, f1 = d;                       // 0-based fine pair
-            double deltac;
-            int ic, jc;
-            if (op.face == 0) {
-                double fp = rf[R.fp1 + f0 + m * my] + rf[R.fp1 + f1 + m * my];
-                double ef = 1 * (rf[R.ef1 + f0 + m * my + my * meqn] + rf[R.ef1 + f1 + m * my + my * meqn]);
-                deltac = (ef - rc[R.ef0 + jcn + m * my]) - (fp - rc[R.fp0 + jcn + m * my]);
-                ic = mbc; jc = mbc + jcn;
-            } else if (op.face == 1) {
-                double fm = rf[R.fm0 + f0 + m * my] + rf[R.fm0 + f1 + m * my];
-                double ef = 1 * (rf[R.ef0 + f0 + m * my + my * meqn] + rf[R.ef0 + f1 + m * my + my * meqn]);
-                deltac = (rc[R.ef1 + jcn + m * my] - ef) - (fm - rc[R.fm1 + jcn + m * my]);
-                ic = mx + mbc - 1; jc = mbc + jcn;
-            } else if (op.face == 2) {
-                double gp = rf[R.gp1 + f0 + m * mx] + rf[R.gp1 + f1 + m * mx];
-                double ef = 1 * (rf[R.ef3 + f0 + m * mx + mx * meqn] + rf[R.ef3 + f1 + m * mx + mx * meqn]);
-                deltac = (ef - rc[R.ef2 + jcn + m * mx]) - (gp - rc[R.gp0 + jcn + m * mx]);
-                ic = mbc + jcn; jc = mbc;
+    const double* rt = regs + (size_t)p * nreg;
+    for (int t = threadIdx.x; t < ring * meqn; t += blockDim.x) {
+        const int m = t / ring, k = t % ring;
+        int ic, jc;                                            // storage indices of the cell
+        if (k < mx) { ic = mbc + k; jc = mbc; }
+        else if (k < 2 * mx) { ic = mbc + k - mx; jc = my + mbc - 1; }
+        else if (k < 2 * mx + my - 2) { ic = mbc; jc = mbc + 1 + (k - 2 * mx); }
+        else { ic = mx + mbc - 1; jc = mbc + 1 + (k - 2 * mx - (my - 2)); }
+        const int fx = (ic == mbc) ? 0 : (ic == mx + mbc - 1) ? 1 : -1;
+        const int fy = (jc == mbc) ? 2 : (jc == my + mbc - 1) ? 3 : -1;
+        const int slot[6] = {fx >= 0 ? s_ss[fx] : -1, fy >= 0 ? s_ss[fy] : -1,
+                             fx >= 0 ? s_fc[fx][0] : -1, fx >= 0 ? s_fc[fx][1] : -1,
+                             fy >= 0 ? s_fc[fy][0] : -1, fy >= 0 ? s_fc[fy][1] : -1};
+        double* qq = q + (size_t)p * nxy * meqn + (size_t)m * nxy + jc * nx + ic;
+        double v = 0.0;
+        bool touched = false;
+        for (int u = 0; u < 6; u++) {
+            if (slot[u] < 0) continue;
+            const SyncOp& op = s_op[slot[u]];
+            const int j = (op.face < 2) ? jc - mbc : ic - mbc;  // 0-based tangential index along the face
+            const double* rn = regs + (size_t)op.n * nreg;
+            double corr;
+            if (op.kind == SYNC_SAMESIZE) {
+                double delta;
+                if (op.face == 0) {
+                    double fp = rn[R.fp1 + j + m * my];
+                    double ef = 1 * rn[R.ef1 + j + m * my + my * meqn];
+                    delta = (ef - rt[R.ef0 + j + m * my]) - (fp - rt[R.fp0 + j + m * my]);
+                } else if (op.face == 1) {
+                    double fm = rn[R.fm0 + j + m * my];
+                    double ef = 1 * rn[R.ef0 + j + m * my + my * meqn];
+                    delta = (rt[R.ef1 + j + m * my] - ef) - (fm - rt[R.fm1 + j + m * my]);
+                } else if (op.face == 2) {
+                    double gp = rn[R.gp1 + j + m * mx];
+                    double ef = 1 * rn[R.ef3 + j + m * mx + mx * meqn];
+                    delta = (ef - rt[R.ef2 + j + m * mx]) - (gp - rt[R.gp0 + j + m * mx]);
+                } else {
+                    double gm = rn[R.gm0 + j + m * mx];
+                    double ef = 1 * rn[R.ef2 + j + m * mx + mx * meqn];
+                    delta = (rt[R.ef3 + j + m * mx] - ef) - (gm - rt[R.gm1 + j + m * mx]);
+                }
+                corr = 0.5 * delta / area;
             } else {
-                double gm = rf[R.gm0 + f0 + m * mx] + rf[R.gm0 + f1 + m * mx];
-                double ef = 1 * (rf[R.ef2 + f0 + m * mx + mx * meqn] + rf[R.ef2 + f1 + m * mx + mx * meqn]);
-                deltac = (rc[R.ef3 + jcn + m * mx] - ef) - (gm - rc[R.gm1 + jcn + m * mx]);
-                ic = mbc + jcn; jc = my + mbc - 1;
+                const int nt = (op.face < 2) ? my : mx;
+                const int d = 1 + op.n_off + 2 * j;            // first fine child (Fortran index)
+                if (d < 1 || d + 1 > nt) continue;             // fc46_skip_this_grid
+                const int f0 = d - 1, f1 = d;                  // 0-based fine pair
+                double deltac;
+                if (op.face == 0) {
+                    double fp = rn[R.fp1 + f0 + m * my] + rn[R.fp1 + f1 + m * my];
+                    double ef = 1 * (rn[R.ef1 + f0 + m * my + my * meqn] + rn[R.ef1 + f1 + m * my + my * meqn]);
+                    deltac = (ef - rt[R.ef0 + j + m * my]) - (fp - rt[R.fp0 + j + m * my]);
+                } else if (op.face == 1) {
+                    double fm = rn[R.fm0 + f0 + m * my] + rn[R.fm0 + f1 + m * my];
+                    double ef = 1 * (rn[R.ef0 + f0 + m * my + my * meqn] + rn[R.ef0 + f1 + m * my + my * meqn]);
+                    deltac = (rt[R.ef1 + j + m * my] - ef) - (fm - rt[R.fm1 + j + m * my]);
+                } else if (op.face == 2) {
+                    double gp = rn[R.gp1 + f0 + m * mx] + rn[R.gp1 + f1 + m * mx];
+                    double ef = 1 * (rn[R.ef3 + f0 + m * mx + mx * meqn] + rn[R.ef3 + f1 + m * mx + mx * meqn]);
+                    deltac = (ef - rt[R.ef2 + j + m * mx]) - (gp - rt[R.gp0 + j + m * mx]);
+                } else {
+                    double gm = rn[R.gm0 + f0 + m * mx] + rn[R.gm0 + f1 + m * mx];
+                    double ef = 1 * (rn[R.ef2 + f0 + m * mx + mx * meqn] + rn[R.ef2 + f1 + m * mx + mx * meqn]);
+                    deltac = (rt[R.ef3 + j + m * mx] - ef) - (gm - rt[R.gm1 + j + m * mx]);
+                }
+                corr = deltac / area;
             }
-            double* qq = qp + (size_t)m * nxy + jc * nx + ic;
-            *qq = *qq + deltac / areac;
+            if (!touched) { v = *qq; touched = true; }
+            v = v + corr;
         }
-        __syncthreads();
+        if (touched) *qq = v;
     }
 }
 
@@ -562,15 +570,11 @@ void launch_timeinterp(const Dims& d, const double* q, const double* qlast, doub
 {
     if (npatch > 0) launch_k(k_timeinterp, npatch, 256, 0, st, q, qlast, qinterp, patches, d.mx, d.my, d.mbc, d.meqn, alpha);
 }
-void launch_samesize(const Dims& d, double* q, const double* regs, const PatchDesc* desc, const SyncOp* ops,
-                     const int* op_start, int npatch, cudaStream_t st)
+void launch_sync(const Dims& d, double* q, const double* regs, const PatchDesc* desc, const SyncOp* ops,
+                 const int* op_start, int nblocks, cudaStream_t st)
 {
-    if (npatch > 0) launch_k(k_samesize, npatch, 64, 0, st, q, regs, desc, ops, op_start, d.mx, d.my, d.mbc, d.meqn, d.nreg());
-}
-void launch_f2c(const Dims& d, double* q, const double* regs, const PatchDesc* desc, const SyncOp* ops,
-                const int* op_start, int npatch, cudaStream_t st)
-{
-    if (npatch > 0) launch_k(k_f2c, npatch, 64, 0, st, q, regs, desc, ops, op_start, d.mx, d.my, d.mbc, d.meqn, d.nreg());
+    if (nblocks > 0)
+        launch_k(k_sync, nblocks, 192, 0, st, q, regs, desc, ops, op_start, d.mx, d.my, d.mbc, d.meqn, d.nreg());
 }
 void launch_reset(const Dims& d, double* regs, const PatchDesc* desc, int p0, int np, int coarse_level, int mode,
                   cudaStream_t st)

@@ -76,11 +76,15 @@ void launch_timeinterp(const Dims& d, const double* q, const double* qlast, doub
 // One op = (coarse/this patch, fine/neighbour patch, face, igrid).  Ops of one
 // patch are contiguous and in the reference order; op_start[i]..op_start[i+1]
 // are the ops of the i-th patch of the launch.
-struct SyncOp { int p, n, face, igrid; int n_off; int pad[3]; };
-void launch_samesize(const Dims& d, double* q, const double* regs, const PatchDesc* desc,
-                     const SyncOp* ops, const int* op_start, int npatch, cudaStream_t st);
-void launch_f2c(const Dims& d, double* q, const double* regs, const PatchDesc* desc,
-                const SyncOp* ops, const int* op_start, int npatch, cudaStream_t st);
+// One time-sync correction of patch p from neighbour n across face `face`:
+// kind SYNC_SAMESIZE (clawpack46_fort_time_sync_samesize) or SYNC_F2C (coarse p,
+// fine n = child igrid of the face, n_off = first fine index offset along it).
+enum { SYNC_SAMESIZE = 0, SYNC_F2C = 1 };
+struct SyncOp { int p, n, face, igrid; int n_off; int kind; int pad[2]; };
+// The corrections of a time sync: ops grouped per patch (samesize faces 0..3,
+// then f2c ops in (face, igrid) order), op_start[b]..op_start[b+1] for block b.
+void launch_sync(const Dims& d, double* q, const double* regs, const PatchDesc* desc,
+                 const SyncOp* ops, const int* op_start, int nblocks, cudaStream_t st);
 // mode 1 = F2C, 2 = SAMESIZE, 3 = PHYS (fclaw2d_clawpatch_time_sync_reset)
 void launch_reset(const Dims& d, double* regs, const PatchDesc* desc, int p0, int np, int coarse_level,
                   int mode, cudaStream_t st);
