@@ -379,7 +379,10 @@ def _tune(g, enabled):
         return {"variant": g.variant, "autotuned": False, **g.variants()[g.variant]}
     best, ms = g.autotune(reps=3)
     v = g.variants()
+    lev = sorted(set(int(x) for x in g.patch_info()[:, 0]))
+    per_level = g.level_variants()
     return {"variant": best, "autotuned": True, **v[best],
+            "per_level": {str(l): int(per_level[l]) for l in lev if 0 <= l < 33},
             "candidates": [dict(ms_per_pass=round(float(m), 4), **x) for m, x in zip(ms, v)]}
 
 

@@ -198,6 +198,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_variant_info": [P, I, ip, ip, ip, ip, ip],
         "fc2d_b200_set_variant": [P, I],
         "fc2d_b200_autotune": [P, I, ip, dp],
+        "fc2d_b200_level_variants": [P, ip],
         "fc2d_b200_output_ascii": [P, ctypes.c_char_p, I, D],
         "fc2d_b200_write_ascii_frame": [ctypes.c_char_p, I, D, I, I, I, I, I, I, ip, ip, dp, dp, dp, dp, dp],
     }
@@ -481,8 +482,15 @@ class Solver:
     def set_variant(self, v: int) -> None:
         self._check("fc2d_b200_set_variant", self.lib.fc2d_b200_set_variant(self.h, v))
 
+    def level_variants(self) -> np.ndarray:
+        """The variant each level 0..32 uses (per-level choice of the autotuner)."""
+        out = np.zeros(33, np.int32)
+        self._check("fc2d_b200_level_variants", self.lib.fc2d_b200_level_variants(self.h, _ip(out)))
+        return out
+
     def autotune(self, reps: int = 3):
-        """Time every variant on the current forest (q unchanged), keep the fastest.
+        """Time every variant on the current forest (q unchanged), keep the fastest,
+        then keep per level the variant fastest on that level (level_variants()).
         Returns (best variant, ms per pass over all levels for each variant)."""
         n = len(self.variants())
         ms = np.zeros(n, np.float64)

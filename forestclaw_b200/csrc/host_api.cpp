@@ -106,6 +106,7 @@ struct fc2d_b200_solver {
     unsigned char phys_ok[64] = {};
     std::vector<const Step2Variant*> vars;         // compiled patch-to-CTA variants of this shape
     int var = 0;                                   // the one in use
+    int var_lev[33];                               // per level (autotuned), -1: var
     StepParams* tune_params = nullptr;             // autotuner: dt = 0 parameters (device)
     DevVec<RepopOp> repop_dev;                     // regrid repopulation ops
     DevVec<double> snap;                           // batch regrid: q of instances whose forest is unchanged
@@ -358,7 +359,8 @@ launch:
     if (!s->emit) return 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (s->timing) { e0 = next_event(s); e1 = next_event(s); CK(cudaEventRecord(e0, s->st)); }
-    cudaError_t e = s->vars[s->var]->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, spd, s->cfl_dev, s->st);
+    const int v = s->var_lev[level] >= 0 ? s->var_lev[level] : s->var;
+    cudaError_t e = s->vars[v]->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, spd, s->cfl_dev, s->st);
     if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("step2 launch: ") + cudaGetErrorString(e));
     if (s->timing) {
         CK(cudaEventRecord(e1, s->st));
@@ -562,6 +564,7 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
     {   // set the kernel's shared-memory attribute outside any stream capture
         s->vars = step2_variants(o.precision, o.rp, o.mx, o.my, o.mbc);
         s->var = 0;
+        for (int l = 0; l < 33; l++) s->var_lev[l] = -1;
         cudaError_t e = s->vars[0]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st);
         if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
         CK(cudaMalloc(&s->tune_params, sizeof(StepParams)));
@@ -600,6 +603,7 @@ extern "C" int fc2d_b200_set_riemann(fc2d_b200_solver_t* s, int rp_id)
     s->o.rp = rp_id;
     s->vars = vars;
     s->var = 0;
+    for (int l = 0; l < 33; l++) s->var_lev[l] = -1;
     invalidate_graph(s);
     cudaError_t e = s->vars[0]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st);
     if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
@@ -1717,6 +1721,7 @@ extern "C" int fc2d_b200_set_variant(fc2d_b200_solver_t* s, int v)
     cudaError_t e = s->vars[v]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st);
     if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
     s->var = v;
+    for (int l = 0; l < 33; l++) s->var_lev[l] = -1;
     invalidate_graph(s);
     return 0;
 }
@@ -1761,12 +1766,41 @@ extern "C" int fc2d_b200_autotune(fc2d_b200_solver_t* s, int reps, int* best_out
         if (ms_out) ms_out[v] = per;
         if (err == cudaSuccess && per < best_ms) { best_ms = per; best = v; }
     }
+    // then per level: a level's patch count decides how its CTAs fill the waves
+    // of the device, so each level keeps the variant that is fastest on it alone
+    int lev_best[33];
+    for (int l = 0; l <= 32 && err == cudaSuccess; l++) {
+        lev_best[l] = -1;
+        const int p0 = f.lev_off[l], np = f.lev_off[l + 1] - p0;
+        if (np <= 0) continue;
+        double lbest = 1e300;
+        for (int v = 0; v < (int)s->vars.size() && err == cudaSuccess; v++) {
+            const Step2Variant* x = s->vars[v];
+            err = x->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, s->tune_params, s->cfl_dev, s->st);
+            if (err == cudaSuccess) err = cudaEventRecord(e0, s->st);
+            for (int r = 0; r < reps && err == cudaSuccess; r++)
+                err = x->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, s->tune_params, s->cfl_dev, s->st);
+            if (err == cudaSuccess) err = cudaEventRecord(e1, s->st);
+            if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+            float ms = 0.0f;
+            if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+            if (err == cudaSuccess && ms < lbest) { lbest = ms; lev_best[l] = v; }
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (err != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("autotune: ") + cudaGetErrorString(err));
     s->var = best;
+    for (int l = 0; l < 33; l++) s->var_lev[l] = lev_best[l];
     invalidate_graph(s);
     if (best_out) *best_out = best;
+    return 0;
+}
+
+extern "C" int fc2d_b200_level_variants(const fc2d_b200_solver_t* s, int* variant)
+{
+    if (!s || !variant) return fail(FC2D_B200_EINVAL, "bad arguments");
+    for (int l = 0; l < 33; l++) variant[l] = s->var_lev[l] >= 0 ? s->var_lev[l] : s->var;
     return 0;
 }
 

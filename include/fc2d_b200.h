@@ -168,12 +168,17 @@ int fc2d_b200_write_ascii_frame(const char* dir, int iframe, double time, int me
  * variants give identical results.  fc2d_b200_autotune times every variant on
  * the current forest (reps passes over all levels, dt = 0 so q is unchanged),
  * keeps the fastest and returns it; ms[v] (may be null, num_variants entries)
- * receives the time of one pass of variant v. */
+ * receives the time of one pass of variant v.  It then times every variant on
+ * each level alone and keeps, per level, the fastest there (a level's patch
+ * count decides how its CTAs fill the device's waves); fc2d_b200_level_variants
+ * reports the variant each level 0..32 uses.  fc2d_b200_set_variant sets one
+ * variant for every level. */
 int fc2d_b200_num_variants(const fc2d_b200_solver_t* s, int* n, int* current);
 int fc2d_b200_variant_info(const fc2d_b200_solver_t* s, int v, int* threads, int* min_blocks, int* reg,
                            int* smem_bytes, int* persistent);
 int fc2d_b200_set_variant(fc2d_b200_solver_t* s, int v);
 int fc2d_b200_autotune(fc2d_b200_solver_t* s, int reps, int* best, double* ms);
+int fc2d_b200_level_variants(const fc2d_b200_solver_t* s, int* variant /* 33 entries */);
 
 /* ---- batches of independent forests (instances; no counterpart in the reference) ----
  * One solver can hold up to FC2D_B200_MAX_INSTANCES independent forests with the

@@ -82,6 +82,10 @@ def test_autotune_leaves_state_and_picks_a_variant(problem, kw):
     best, ms = g.autotune(reps=2)
     assert 0 <= best < len(ms) and g.variant == best
     assert np.all(ms > 0) and ms[best] == ms.min()
+    # per-level choices: a compiled variant for every level present
+    lv = g.level_variants()
+    for l in set(int(x) for x in g.patch_info()[:, 0]):
+        assert 0 <= lv[l] < len(ms)
     assert np.array_equal(g.get_q(), q0) and np.array_equal(g.get_registers(), r0)
     # the tuned solver continues exactly like an untuned one
     h = _solver(problem, **kw)
