@@ -200,6 +200,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_autotune": [P, I, ip, dp],
         "fc2d_b200_level_variants": [P, ip],
         "fc2d_b200_output_ascii": [P, ctypes.c_char_p, I, D],
+        "fc2d_b200_output_vtk": [P, ctypes.c_char_p, I],
+        "fc2d_b200_write_vtk_file": [ctypes.c_char_p, I, I, I, I, ip, dp, ctypes.POINTER(ctypes.c_float)],
         "fc2d_b200_write_ascii_frame": [ctypes.c_char_p, I, D, I, I, I, I, I, I, ip, ip, dp, dp, dp, dp, dp],
     }
     for name, args in sig.items():
@@ -227,6 +229,45 @@ def write_ascii_frame(directory: str, iframe: int, time: float, q: np.ndarray, l
                                          ny - 2 * mbc, mbc, npatch, _ip(lv), _ip(bk), *[_dp(v) for v in arr], _dp(q))
     if rc != 0:
         raise B200Error("fc2d_b200_write_ascii_frame", rc, "cannot write the frame")
+
+
+def write_vtk_file(path: str, points: np.ndarray, values: np.ndarray, block) -> None:
+    """Write caller-supplied patches as a VTK unstructured grid (host only, no device).
+    points: (npatch, (my+1)(mx+1), 3) float64 (i fastest), values: (npatch, my, mx, meqn)
+    float32, block: per-patch block number; patches are written in the given order."""
+    lib = load_library()
+    v = np.ascontiguousarray(values, np.float32)
+    npatch, my, mx, meqn = v.shape
+    pts = np.ascontiguousarray(points, np.float64)
+    if pts.shape != (npatch, (mx + 1) * (my + 1), 3):
+        raise ValueError("points must be (npatch, (mx+1)(my+1), 3)")
+    bk = np.ascontiguousarray(block, np.int32)
+    rc = lib.fc2d_b200_write_vtk_file(os.fsencode(path), mx, my, meqn, npatch, _ip(bk), _dp(pts),
+                                      v.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+    if rc != 0:
+        raise B200Error("fc2d_b200_write_vtk_file", rc, "cannot write " + path)
+
+
+def read_vtu(path: str) -> dict:
+    """Parse a file written by write_vtk_file / Solver.output_vtk: the header's
+    attributes and every appended array as a numpy array keyed by its Name."""
+    import re
+    with open(path, "rb") as f:
+        raw = f.read()
+    start = raw.index(b'<AppendedData encoding="raw">\n  _') + len(b'<AppendedData encoding="raw">\n  _')
+    end = raw.rindex(b"\n </AppendedData>")
+    head = raw[:start].decode()
+    data = raw[start:end]
+    piece = re.search(r'NumberOfPoints="(\d+)" NumberOfCells="(\d+)"', head)
+    out = {"npoints": int(piece.group(1)), "ncells": int(piece.group(2)), "header": head}
+    types = {"Float64": np.float64, "Float32": np.float32, "Int32": np.int32, "Int64": np.int64, "UInt8": np.uint8}
+    for m in re.finditer(r'<DataArray type="(\w+)" Name="(\w+)"(?: NumberOfComponents="(\d+)")? '
+                         r'format="appended" offset="(\d+)">', head):
+        typ, name, ncomp, off = m.group(1), m.group(2), m.group(3), int(m.group(4))
+        nbytes = int(np.frombuffer(data[off:off + 8], np.uint64)[0])
+        arr = np.frombuffer(data[off + 8:off + 8 + nbytes], types[typ])
+        out[name] = arr.reshape(-1, int(ncomp)) if ncomp else arr
+    return out
 
 
 def exported_symbols() -> list[str]:
@@ -459,6 +500,12 @@ class Solver:
         """fort.tNNNN / fort.qNNNN of the current forest (clawpack 4.6 ASCII, VisClaw-readable)."""
         self._check("fc2d_b200_output_ascii",
                     self.lib.fc2d_b200_output_ascii(self.h, os.fsencode(directory), iframe, time))
+
+    def output_vtk(self, prefix: str, iframe: int) -> str:
+        """<prefix>_frame_NNNN.vtu of the current forest (VTK unstructured grid; points and
+        values packed on the device).  Returns the file name."""
+        self._check("fc2d_b200_output_vtk", self.lib.fc2d_b200_output_vtk(self.h, os.fsencode(prefix), iframe))
+        return f"{prefix}_frame_{iframe:04d}.vtu"
 
     # -- patch-to-CTA variants and the autotuner -------------------------------
     def variants(self) -> list:

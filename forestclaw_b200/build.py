@@ -33,6 +33,7 @@ CU_UNITS = {
     "k_amr.cu": ["-fmad=false"],
     "k_mass_noalloc.cu": ["-fmad=false"],
     "k_metric.cu": ["-fmad=false"],
+    "k_output.cu": ["-fmad=false"],
     "k_mlp.cu": [],
     "k_step2_f32w_adv.cu": ["--use_fast_math"],
     "k_step2_f32w_sw.cu": ["--use_fast_math"],

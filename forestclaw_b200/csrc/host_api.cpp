@@ -1841,3 +1841,56 @@ extern "C" int fc2d_b200_output_ascii(fc2d_b200_solver_t* s, const char* dir, in
     if (rc) return fail(rc, std::string("cannot write fort.q/fort.t frame into ") + dir);
     return 0;
 }
+
+// fclaw2d_clawpatch_output_vtk (src/patches/clawpatch/fclaw2d_clawpatch_output_vtk.c:880-900):
+// <prefix>_frame_NNNN.vtu.  The device packs points and cell values of every patch
+// in the file's patch order (block by block, each block's leaves along the curve);
+// one copy brings them to the host, which writes the file.
+extern "C" int fc2d_b200_output_vtk(fc2d_b200_solver_t* s, const char* prefix, int iframe)
+{
+    if (!s || !s->initialized || !prefix || iframe < 0) return fail(FC2D_B200_EINVAL, "bad arguments");
+    const Forest& f = s->forest;
+    const int np = f.np();
+    std::vector<int> order(np);
+    for (int i = 0; i < np; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        const PatchInfo& A = f.p[a];
+        const PatchInfo& B = f.p[b];
+        if (A.inst != B.inst) return A.inst < B.inst;
+        if (A.block != B.block) return A.block < B.block;
+        return A.morton < B.morton;
+    });
+    std::vector<int> blk(np);
+    for (int k = 0; k < np; k++) blk[k] = f.p[order[k]].block;
+    const size_t npt = (size_t)(s->d.mx + 1) * (s->d.my + 1), ncell = (size_t)s->d.mx * s->d.my;
+    std::vector<double> pts((size_t)np * npt * 3);
+    std::vector<float> vals((size_t)np * ncell * s->d.meqn);
+    int* ord_d = nullptr;
+    double* pts_d = nullptr;
+    float* vals_d = nullptr;
+    cudaError_t e = cudaMalloc(&ord_d, sizeof(int) * (np > 0 ? np : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&pts_d, sizeof(double) * (pts.size() > 0 ? pts.size() : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&vals_d, sizeof(float) * (vals.size() > 0 ? vals.size() : 1));
+    if (e == cudaSuccess && np > 0)
+        e = cudaMemcpyAsync(ord_d, order.data(), sizeof(int) * np, cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess) {
+        launch_vtk_pack(s->d, s->q, s->desc, ord_d, np, s->sphere ? 1 : 0, pts_d, vals_d, s->st);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && np > 0)
+        e = cudaMemcpyAsync(pts.data(), pts_d, sizeof(double) * pts.size(), cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess && np > 0)
+        e = cudaMemcpyAsync(vals.data(), vals_d, sizeof(float) * vals.size(), cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    if (ord_d) cudaFree(ord_d);
+    if (pts_d) cudaFree(pts_d);
+    if (vals_d) cudaFree(vals_d);
+    if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("vtk output: ") + cudaGetErrorString(e));
+    char name[64];
+    std::snprintf(name, sizeof(name), "_frame_%04d.vtu", iframe);
+    const std::string path = std::string(prefix) + name;
+    const int rc = fc2d_b200_write_vtk_file(path.c_str(), s->d.mx, s->d.my, s->d.meqn, np, blk.data(), pts.data(),
+                                            vals.data());
+    if (rc) return fail(rc, "cannot write " + path);
+    return 0;
+}

@@ -1,4 +1,5 @@
-// host_output.cpp -- clawpack 4.6 ASCII frames (fort.tXXXX header, fort.qXXXX patches).
+// host_output.cpp -- clawpack 4.6 ASCII frames (fort.tXXXX header, fort.qXXXX patches)
+// and VTK unstructured-grid files (<prefix>_frame_NNNN.vtu).
 //
 // fclaw2d_clawpatch_output_ascii.c:112-170 and fort_4.6/fclaw2d_clawpatch46_output_ascii.f:
 //   fort.t: time (E30.20), meqn, ngrids, num_aux, num_dim (I5 + label)
@@ -10,7 +11,9 @@
 //           and a blank line after each row.
 // The Fortran E format is restated here: 0.ddd...dE+xx (d digits after the point,
 // correctly rounded), E dropped for three-digit exponents, right-justified.
+#include <climits>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -107,4 +110,137 @@ extern "C" int fc2d_b200_write_ascii_frame(const char* dir, int iframe, double t
     }
     std::fclose(fq);
     return 0;
+}
+
+// ---------------------------------------------------------------------------
+// VTK (fclaw2d_clawpatch_output_vtk.c): one <prefix>_frame_NNNN.vtu, an XML
+// UnstructuredGrid with raw appended data -- per patch (mx+1)(my+1) points
+// (Float64 x3), mx*my quads (VTK type 9) with their connectivity and offsets,
+// the cell fields mpirank (Int32), blockno (Int32), patchno and the meqn fields
+// as Float32 per cell.  Each appended array is preceded by its byte count
+// (UInt64); integer arrays are Int32 when every index fits, else Int64
+// (fclaw2d_vtk_write_file, :593-698; header :97-197; footer :564-591).
+// ---------------------------------------------------------------------------
+extern "C" int fc2d_b200_write_vtk_file(const char* path, int mx, int my, int meqn, int npatch, const int* block,
+                                        const double* points, const float* values)
+{
+    if (!path || mx <= 0 || my <= 0 || meqn <= 0 || npatch < 0 || (npatch > 0 && (!block || !points || !values)))
+        return FC2D_B200_EINVAL;
+    const int64_t ppp = (int64_t)(mx + 1) * (my + 1), cpp = (int64_t)mx * my, np = npatch;
+    const int64_t npts = ppp * np, ncells = cpp * np, nconn = 4 * (ncells + 1);
+    const bool fits32 = npts <= INT32_MAX && nconn <= INT32_MAX;
+    const char* inttype = fits32 ? "Int32" : "Int64";
+    const int64_t isz = fits32 ? 4 : 8, nd = 8;
+    const int64_t ps_pos = ppp * 3 * 8, ps_conn = cpp * 4 * isz, ps_off = cpp * isz, ps_typ = cpp,
+                  ps_rank = cpp * 4, ps_blk = cpp * 4, ps_pno = cpp * isz, ps_q = cpp * meqn * 4;
+    const int64_t o_pos = 0, o_conn = nd + o_pos + ps_pos * np, o_off = nd + o_conn + ps_conn * np,
+                  o_typ = nd + o_off + ps_off * np, o_rank = nd + o_typ + ps_typ * np,
+                  o_blk = nd + o_rank + ps_rank * np, o_pno = nd + o_blk + ps_blk * np,
+                  o_q = nd + o_pno + ps_pno * np;
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return FC2D_B200_EINVAL;
+    bool bad = false;
+    auto pr = [&](const char* fmt, auto... a) { if (!bad && std::fprintf(f, fmt, a...) < 0) bad = true; };
+    pr("<?xml version=\"1.0\"?>\n");
+    pr("<VTKFile type=\"UnstructuredGrid\" version=\"0.1\" byte_order=\"LittleEndian\" header_type=\"UInt64\" >\n");
+    pr(" <UnstructuredGrid>\n");
+    pr("  <Piece NumberOfPoints=\"%lld\" NumberOfCells=\"%lld\">\n", (long long)npts, (long long)ncells);
+    pr("   <Points>\n");
+    pr("    <DataArray type=\"Float64\" Name=\"Position\" NumberOfComponents=\"3\" format=\"appended\" offset=\"%lld\">\n",
+       (long long)o_pos);
+    pr("    </DataArray>\n");
+    pr("   </Points>\n");
+    pr("   <Cells>\n");
+    pr("    <DataArray type=\"%s\" Name=\"connectivity\" format=\"appended\" offset=\"%lld\">\n", inttype,
+       (long long)o_conn);
+    pr("    </DataArray>\n");
+    pr("    <DataArray type=\"%s\" Name=\"offsets\" format=\"appended\" offset=\"%lld\">\n", inttype,
+       (long long)o_off);
+    pr("    </DataArray>\n");
+    pr("    <DataArray type=\"UInt8\" Name=\"types\" format=\"appended\" offset=\"%lld\">\n", (long long)o_typ);
+    pr("    </DataArray>\n");
+    pr("   </Cells>\n");
+    pr("   <CellData Scalars=\"mpirank,blockno,patchno\" Fields=\"meqn\">\n");
+    pr("    <DataArray type=\"Int32\" Name=\"mpirank\" format=\"appended\" offset=\"%lld\">\n", (long long)o_rank);
+    pr("    </DataArray>\n");
+    pr("    <DataArray type=\"Int32\" Name=\"blockno\" format=\"appended\" offset=\"%lld\">\n", (long long)o_blk);
+    pr("    </DataArray>\n");
+    pr("    <DataArray type=\"%s\" Name=\"patchno\" format=\"appended\" offset=\"%lld\">\n", inttype, (long long)o_pno);
+    pr("    </DataArray>\n");
+    if (meqn == 1)
+        pr("    <DataArray type=\"Float32\" Name=\"meqn\" format=\"appended\" offset=\"%lld\">\n", (long long)o_q);
+    else
+        pr("    <DataArray type=\"Float32\" Name=\"meqn\" NumberOfComponents=\"%d\" format=\"appended\" offset=\"%lld\">\n",
+           meqn, (long long)o_q);
+    pr("    </DataArray>\n");
+    pr("   </CellData>\n");
+    pr("   <PointData>\n");
+    pr("   </PointData>\n");
+    pr("  </Piece>\n");
+    pr(" </UnstructuredGrid>\n");
+    pr(" <AppendedData encoding=\"raw\">\n  _");
+    auto put = [&](const void* p, size_t n) { if (!bad && n && std::fwrite(p, n, 1, f) != 1) bad = true; };
+    auto count = [&](int64_t psize) { const uint64_t c = (uint64_t)(psize * np); put(&c, 8); };
+    std::vector<char> buf;
+    // positions
+    count(ps_pos);
+    put(points, (size_t)(ps_pos * np));
+    // connectivity: the quad of cell (i, j) over the patch's own points
+    count(ps_conn);
+    buf.resize((size_t)ps_conn);
+    for (int64_t p = 0; p < np; p++) {
+        const int64_t pb = ppp * p;
+        int64_t t = 0;
+        for (int j = 0; j < my; j++)
+            for (int i = 0; i < mx; i++) {
+                const int64_t l = pb + i + (int64_t)j * (mx + 1);
+                const int64_t v[4] = {l, l + 1, l + (mx + 2), l + (mx + 1)};
+                for (int c = 0; c < 4; c++, t++) {
+                    if (fits32) { const int32_t x = (int32_t)v[c]; std::memcpy(&buf[t * 4], &x, 4); }
+                    else std::memcpy(&buf[t * 8], &v[c], 8);
+                }
+            }
+        put(buf.data(), buf.size());
+    }
+    // offsets: 4 (cell index + 1)
+    count(ps_off);
+    buf.resize((size_t)ps_off);
+    for (int64_t p = 0; p < np; p++) {
+        for (int64_t c = 0; c < cpp; c++) {
+            const int64_t k = 4 * (cpp * p + c + 1);
+            if (fits32) { const int32_t x = (int32_t)k; std::memcpy(&buf[c * 4], &x, 4); }
+            else std::memcpy(&buf[c * 8], &k, 8);
+        }
+        put(buf.data(), buf.size());
+    }
+    // types: VTK_QUAD
+    count(ps_typ);
+    buf.assign((size_t)ps_typ, (char)9);
+    for (int64_t p = 0; p < np; p++) put(buf.data(), buf.size());
+    // mpirank, blockno, patchno
+    count(ps_rank);
+    buf.assign((size_t)ps_rank, 0);
+    for (int64_t p = 0; p < np; p++) put(buf.data(), buf.size());
+    count(ps_blk);
+    buf.resize((size_t)ps_blk);
+    for (int64_t p = 0; p < np; p++) {
+        const int32_t b = block[p];
+        for (int64_t c = 0; c < cpp; c++) std::memcpy(&buf[c * 4], &b, 4);
+        put(buf.data(), buf.size());
+    }
+    count(ps_pno);
+    buf.resize((size_t)ps_pno);
+    for (int64_t p = 0; p < np; p++) {
+        for (int64_t c = 0; c < cpp; c++) {
+            if (fits32) { const int32_t x = (int32_t)p; std::memcpy(&buf[c * 4], &x, 4); }
+            else std::memcpy(&buf[c * 8], &p, 8);
+        }
+        put(buf.data(), buf.size());
+    }
+    // the fields, cell by cell, meqn values each
+    count(ps_q);
+    put(values, (size_t)(ps_q * np));
+    pr("\n </AppendedData>\n</VTKFile>\n");
+    if (std::fclose(f) != 0) bad = true;
+    return bad ? FC2D_B200_EINVAL : 0;
 }

@@ -144,6 +144,10 @@ struct MetricOp { int kind, dst; int src[4]; };
 struct SphereFlow { double axis[3]; double omega; };   // psi = omega (axis . x)
 // Areas of every op's patch into narea, then kappa and edge velocities into aux for
 // ops of kind 0 and 2.  desc: the new forest's descriptors.
+// VTK output: points ((mx+1)(my+1) x 3 doubles) and cell values (mx my x meqn floats)
+// of patches order[0..npatch), packed in that order (k_output.cu).
+void launch_vtk_pack(const Dims& d, const double* q, const PatchDesc* desc, const int* order, int npatch, int manifold,
+                     double* points, float* values, cudaStream_t st);
 void launch_sphere_metric(const Dims& d, const MetricOp* ops, int nops, const PatchDesc* desc, int maxlevel,
                           const double* oarea, double* narea, double* aux, const SphereFlow& flow, cudaStream_t st);
 

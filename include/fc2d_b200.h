@@ -157,6 +157,17 @@ int fc2d_b200_output_ascii(fc2d_b200_solver_t* s, const char* dir, int iframe, d
 int fc2d_b200_write_ascii_frame(const char* dir, int iframe, double time, int meqn, int maux, int mx, int my,
                                 int mbc, int npatch, const int* level, const int* block, const double* xlower,
                                 const double* ylower, const double* dx, const double* dy, const double* q);
+/* fclaw2d_clawpatch_output_vtk (src/patches/clawpatch/fclaw2d_clawpatch_output_vtk.c:593-900):
+ * <prefix>_frame_NNNN.vtu, an XML UnstructuredGrid with raw appended data (UInt64 byte
+ * count before each array): per patch (mx+1)(my+1) points (Float64 x 3; the
+ * cubed-sphere mapping for the sphere app), mx*my quads with connectivity, offsets and
+ * types, cell fields mpirank, blockno, patchno and the meqn values as Float32, patches
+ * block by block along the curve.  Points and values are packed on the device.
+ * fc2d_b200_write_vtk_file writes caller-supplied arrays (host memory, patches in file
+ * order): points[np][(mx+1)(my+1)][3], values[np][mx*my][meqn], block[np]. */
+int fc2d_b200_output_vtk(fc2d_b200_solver_t* s, const char* prefix, int iframe);
+int fc2d_b200_write_vtk_file(const char* path, int mx, int my, int meqn, int npatch, const int* block,
+                             const double* points, const float* values);
 
 /* ---- patch-to-CTA variants of the fused update (no counterpart in the reference) ----
  * Each solver shape (precision, Riemann solver, patch size) is compiled with
