@@ -42,7 +42,9 @@ struct Step2Geom {
     static constexpr int NX = MX + 2 * MBC, NY = MY + 2 * MBC, NXY = NX * NY;
     static constexpr int MEQN = RP::MEQN, MWAVES = RP::MWAVES, MAUX = RP::MAUX, NEXTRA = RP::NEXTRA;
     static constexpr int NIX = (NY - 2) * (NX - 1);          // x-sweep interfaces
-    static constexpr int NIY = (NX - 2) * (NY - 1);          // y-sweep interfaces
+    // y-sweep interfaces, numbered with i fastest (k = (jc-1)(NX-2) + ic-1), so the
+    // threads of a warp touch consecutive cells of a row of the shared-memory arrays
+    static constexpr int NIY = (NX - 2) * (NY - 1);
     static constexpr int NI = NIX > NIY ? NIX : NIY;
     // REG: every interface of a sweep has its own thread, so the normal solve
     // (speeds, fluctuations, Roe averages) stays in registers across the
@@ -327,15 +329,17 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
         const bool second = FWAVE ? (sp.order1 != 1) : (sp.order1 == 2);
         if (second) {
             if (pos >= lim_lo && pos <= lim_hi) {
-                // inline limiter (clawpack46_inlinelimiter.f:267-343) with unlimited neighbours
+                // inline limiter (clawpack46_inlinelimiter.f:267-343) with unlimited neighbours;
+                // the neighbours along the sweep are k -+ 1 (x) or k -+ (NX-2) (y)
+                const int kstep = (ixy == 1) ? 1 : NX - 2;
                 for (int mw = 0; mw < MWAVES; mw++) {
                     const int ml = sp.mthlim[mw];
                     if (ml == 0) continue;
                     TW wnorm2 = TW(0), dotl = TW(0), dotr = TW(0);
                     for (int m = 0; m < MEQN; m++) {
                         const TW w = st.wave[mw][m];
-                        const TW wl = W[(G::W_WAVE + mw * MEQN + m) * NI + k - 1];
-                        const TW wr = W[(G::W_WAVE + mw * MEQN + m) * NI + k + 1];
+                        const TW wl = W[(G::W_WAVE + mw * MEQN + m) * NI + k - kstep];
+                        const TW wr = W[(G::W_WAVE + mw * MEQN + m) * NI + k + kstep];
                         wnorm2 = wnorm2 + w * w;
                         dotl = dotl + wl * w;
                         dotr = dotr + w * wr;
@@ -440,7 +444,7 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
             int cL = 0, cR = 1;
             if (k >= 0) {
                 if (ixy == 1) { const int jc = 1 + k / (NX - 1), ic = 1 + k % (NX - 1); cL = jc * NX + ic - 1; cR = cL + 1; }
-                else { const int ic = 1 + k / (NY - 1), jc = 1 + k % (NY - 1); cL = (jc - 1) * NX + ic; cR = cL + NX; }
+                else { const int jc = 1 + k / (NX - 2), ic = 1 + k % (NX - 2); cL = (jc - 1) * NX + ic; cR = cL + NX; }
             }
             double qL[MEQN], qR[MEQN];
             for (int m = 0; m < MEQN; m++) { qL[m] = Qs[m * NXY + cL]; qR[m] = Qs[m * NXY + cR]; }
@@ -493,15 +497,15 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
             FPs[m * NXY + jc * NX + ic] = 0.0 + faddp[m];
         }
     };
-    // y-sweep interface k -> column ic = 1 + k / (NY-1), interface jc = 1 + k % (NY-1)
+    // y-sweep interface k -> row interface jc = 1 + k / (NX-2), column ic = 1 + k % (NX-2)
     auto y1 = [&](int k, State& st, double seed) {
-        const int ic = 1 + k / (NY - 1), jc = 1 + k % (NY - 1);
+        const int jc = 1 + k / (NX - 2), ic = 1 + k % (NX - 2);
         const bool cr = (jc >= MBC && jc <= MY + MBC);
         normal_solve(2, (jc - 1) * NX + ic, jc * NX + ic, k, cr, cr ? dtdy1d_y(ic, jc) : TW(0),
                      cr ? dtdy1d_y(ic, jc - 1) : TW(0), st, seed);
     };
     auto y2 = [&](int k, State& st) {
-        const int ic = 1 + k / (NY - 1), jc = 1 + k % (NY - 1);
+        const int jc = 1 + k / (NX - 2), ic = 1 + k % (NX - 2);
         const TW dlo = dtdy1d_y(ic, jc - 1);
         const TW dhi = FWAVE ? dlo : dtdy1d_y(ic, jc);
         const TW dave = TW(0.5) * (dtdy1d_y(ic, jc - 1) + dtdy1d_y(ic, jc));
@@ -555,15 +559,15 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
             if (ic - 1 >= 1 && ic - 1 <= NX - 2) {
                 const int col = ic - 1;
                 double v = 0.0;
-                if (jc + 1 <= NY - 1) { const int kk = (col - 1) * (NY - 1) + jc; if (tflag[kk]) v = v - (double)Tt[(1 * MEQN + m) * NI + kk]; }
-                { const int kk = (col - 1) * (NY - 1) + jc - 1; if (tflag[kk]) v = v - (double)Tt[(3 * MEQN + m) * NI + kk]; }
+                if (jc + 1 <= NY - 1) { const int kk = jc * (NX - 2) + col - 1; if (tflag[kk]) v = v - (double)Tt[(1 * MEQN + m) * NI + kk]; }
+                { const int kk = (jc - 1) * (NX - 2) + col - 1; if (tflag[kk]) v = v - (double)Tt[(3 * MEQN + m) * NI + kk]; }
                 fm = fm + v; fp = fp + v;
             }
             if (ic >= 1 && ic <= NX - 2) {
                 const int col = ic;
                 double v = 0.0;
-                if (jc + 1 <= NY - 1) { const int kk = (col - 1) * (NY - 1) + jc; if (tflag[kk]) v = v - (double)Tt[(0 * MEQN + m) * NI + kk]; }
-                { const int kk = (col - 1) * (NY - 1) + jc - 1; if (tflag[kk]) v = v - (double)Tt[(2 * MEQN + m) * NI + kk]; }
+                if (jc + 1 <= NY - 1) { const int kk = jc * (NX - 2) + col - 1; if (tflag[kk]) v = v - (double)Tt[(0 * MEQN + m) * NI + kk]; }
+                { const int kk = (jc - 1) * (NX - 2) + col - 1; if (tflag[kk]) v = v - (double)Tt[(2 * MEQN + m) * NI + kk]; }
                 fm = fm + v; fp = fp + v;
             }
             FMs[m * NXY + c] = fm;
