@@ -107,6 +107,11 @@ struct fc2d_b200_solver {
     std::vector<const Step2Variant*> vars;         // compiled patch-to-CTA variants of this shape
     int var = 0;                                   // the one in use
     int var_lev[33];                               // per level (autotuned), -1: var
+    // level updates issued back to back (a subcycled step starts every level whose
+    // time has come, finest first, with nothing between them) touch disjoint
+    // patches, so they go out as one launch over consecutive levels
+    struct PendingUpdate { bool active = false; int lev_hi = 0, lev_lo = 0, p0 = 0, np = 0, slot = 0, var = 0; };
+    PendingUpdate pend;
     StepParams* tune_params = nullptr;             // autotuner: dt = 0 parameters (device)
     DevVec<RepopOp> repop_dev;                     // regrid repopulation ops
     DevVec<double> snap;                           // batch regrid: q of instances whose forest is unchanged
@@ -339,6 +344,32 @@ static StepParams make_params(const fc2d_b200_solver* s, int level, double t, do
     return sp;
 }
 
+// Launch the pending group of level updates (one launch, levels lev_lo..lev_hi).
+static int flush_updates(fc2d_b200_solver* s)
+{
+    fc2d_b200_solver::PendingUpdate& g = s->pend;
+    if (!g.active) return 0;
+    g.active = false;
+    if (s->fill) { s->upd_launches++; s->total_launches++; }
+    if (!s->emit) return 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (s->timing) { e0 = next_event(s); e1 = next_event(s); CK(cudaEventRecord(e0, s->st)); }
+    const int lev_hi = g.lev_hi > g.lev_lo ? g.lev_hi : -1;
+    cudaError_t e = s->vars[g.var]->fn(s->q, s->qlast, s->aux, s->regs, s->desc, g.p0, g.np, s->params_dev + g.slot,
+                                       lev_hi, s->cfl_dev, s->st);
+    if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("step2 launch: ") + cudaGetErrorString(e));
+    if (s->timing) {
+        CK(cudaEventRecord(e1, s->st));
+        const double cells = (double)g.np * s->d.mx * s->d.my;
+        const double bytes = cells * 8.0 * (2.0 * s->d.meqn + s->d.maux);
+        s->upd_launch_bytes.push_back({s->ev_used - 2, bytes});
+    }
+    return 0;
+}
+
+// One level update (clawpack46_update over the level's patches).  It joins the
+// pending group when it is the next coarser level right after it (same variant,
+// its parameter block the next slot); anything else launches the group first.
 static int update_level(fc2d_b200_solver* s, int level, double t, double dt)
 {
     const Forest& f = s->forest;
@@ -346,28 +377,30 @@ static int update_level(fc2d_b200_solver* s, int level, double t, double dt)
     const int p0 = f.lev_off[level], np = f.lev_off[level + 1] - p0;
     if (np <= 0) return 0;
     if (s->n_upd >= fc2d_b200_solver::PCAP) return fail(FC2D_B200_EINVAL, "too many level updates in one advance");
-    const StepParams* spd = s->params_dev + s->n_upd;
-    StepParams& sp = s->params_host[s->n_upd];
-    s->n_upd++;
-    if (!s->fill) goto launch;
-    sp = make_params(s, level, t, dt);
-    s->cell_updates += (double)np * s->d.mx * s->d.my;
-    s->upd_launches++;
-    s->total_launches++;
-    if (s->emit) CK(cudaMemcpyAsync((void*)spd, &sp, sizeof(StepParams), cudaMemcpyHostToDevice, s->st));
-launch:
-    if (!s->emit) return 0;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (s->timing) { e0 = next_event(s); e1 = next_event(s); CK(cudaEventRecord(e0, s->st)); }
-    const int v = s->var_lev[level] >= 0 ? s->var_lev[level] : s->var;
-    cudaError_t e = s->vars[v]->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, spd, s->cfl_dev, s->st);
-    if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("step2 launch: ") + cudaGetErrorString(e));
-    if (s->timing) {
-        CK(cudaEventRecord(e1, s->st));
-        const double cells = (double)np * s->d.mx * s->d.my;
-        const double bytes = cells * 8.0 * (2.0 * s->d.meqn + s->d.maux);
-        s->upd_launch_bytes.push_back({s->ev_used - 2, bytes});
+    const int slot = s->n_upd++;
+    if (s->fill) {
+        StepParams& sp = s->params_host[slot];
+        sp = make_params(s, level, t, dt);
+        s->cell_updates += (double)np * s->d.mx * s->d.my;
+        if (s->emit)
+            CK(cudaMemcpyAsync((void*)(s->params_dev + slot), &sp, sizeof(StepParams), cudaMemcpyHostToDevice, s->st));
     }
+    const int v = s->var_lev[level] >= 0 ? s->var_lev[level] : s->var;
+    fc2d_b200_solver::PendingUpdate& g = s->pend;
+    if (g.active && level == g.lev_lo - 1 && v == g.var && slot == g.slot + (g.lev_hi - level) && p0 + np == g.p0) {
+        g.lev_lo = level;
+        g.p0 = p0;
+        g.np += np;
+        return 0;
+    }
+    int rc = flush_updates(s);
+    if (rc) return rc;
+    g.active = true;
+    g.lev_hi = g.lev_lo = level;
+    g.p0 = p0;
+    g.np = np;
+    g.slot = slot;
+    g.var = v;
     return 0;
 }
 
@@ -385,33 +418,62 @@ static bool lrange(int& a, int& b)
     if (b > 32) b = 32;
     return a <= b;
 }
-static void copy_range(fc2d_b200_solver* s, int a, int b, int ti)
+// Stage ranges as table segments: levels [a, b] of q, and (c >= 0) level c of the
+// time-interpolated copy.  A stage on q and the same stage on the copy write
+// different arrays and neither reads what the other writes (the copy's stage
+// reads the copy, or fine interiors of q, which no ghost-fill stage writes), so
+// both go out in one launch.
+template <class E>
+static GatherSeg<E> seg(const E* table, int off, int n, double* dst, const double* src)
 {
-    if (!lrange(a, b)) return;
-    const int off = s->lr[a].copy_off, n = s->lr[b].copy_off + s->lr[b].copy_n - off;
-    if (n <= 0) return;
-    if (s->fill) s->total_launches++;
-    if (s->emit) launch_copy(s->d, tsdata(s, ti), tsdata(s, ti), s->t_copy.p + off, n, s->st);
+    return GatherSeg<E>{dst, src, table + off, n};
 }
-static void average_range(fc2d_b200_solver* s, int a, int b, int ti)
+static void copy_range(fc2d_b200_solver* s, int a, int b, int c)
 {
-    if (!lrange(a, b)) return;
-    const int off = s->lr[a].avg_off, n = s->lr[b].avg_off + s->lr[b].avg_n - off;
-    if (n <= 0) return;
+    GatherSeg<CopyEnt> s0{nullptr, nullptr, nullptr, 0}, s1 = s0;
+    if (lrange(a, b)) {
+        const int off = s->lr[a].copy_off, n = s->lr[b].copy_off + s->lr[b].copy_n - off;
+        if (n > 0) s0 = seg(s->t_copy.p, off, n, s->q, s->q);
+    }
+    if (c >= 0 && c <= 32 && s->lr[c].copy_n > 0)
+        s1 = seg(s->t_copy.p, s->lr[c].copy_off, s->lr[c].copy_n, s->qinterp, s->qinterp);
+    if (s0.n + s1.n <= 0) return;
+    (void)flush_updates(s);
     if (s->fill) s->total_launches++;
-    if (s->emit) launch_average(s->d, tsdata(s, ti), s->q, s->t_avg.p + off, n, s->area, s->st);
+    if (s->emit) launch_copy(s->d, s0, s1, s->st);
 }
-static void phys_range(fc2d_b200_solver* s, int a, int b, int ti)
+static void average_range(fc2d_b200_solver* s, int a, int b, int c)
 {
-    if (!lrange(a, b)) return;
-    const int off = s->lr[a].phys_off, n = s->lr[b].phys_off + s->lr[b].phys_n - off;
-    if (n <= 0) return;
+    GatherSeg<AvgEnt> s0{nullptr, nullptr, nullptr, 0}, s1 = s0;
+    if (lrange(a, b)) {
+        const int off = s->lr[a].avg_off, n = s->lr[b].avg_off + s->lr[b].avg_n - off;
+        if (n > 0) s0 = seg(s->t_avg.p, off, n, s->q, s->q);
+    }
+    if (c >= 0 && c <= 32 && s->lr[c].avg_n > 0)
+        s1 = seg(s->t_avg.p, s->lr[c].avg_off, s->lr[c].avg_n, s->qinterp, s->q);
+    if (s0.n + s1.n <= 0) return;
+    (void)flush_updates(s);
     if (s->fill) s->total_launches++;
-    if (s->emit) launch_phys(s->d, tsdata(s, ti), s->t_phys.p + off, n, s->bc_dev, s->st);
+    if (s->emit) launch_average(s->d, s0, s1, s->area, s->st);
+}
+static void phys_range(fc2d_b200_solver* s, int a, int b, int c)
+{
+    GatherSeg<PhysEnt> s0{nullptr, nullptr, nullptr, 0}, s1 = s0;
+    if (lrange(a, b)) {
+        const int off = s->lr[a].phys_off, n = s->lr[b].phys_off + s->lr[b].phys_n - off;
+        if (n > 0) s0 = seg(s->t_phys.p, off, n, s->q, s->q);
+    }
+    if (c >= 0 && c <= 32 && s->lr[c].phys_n > 0)
+        s1 = seg(s->t_phys.p, s->lr[c].phys_off, s->lr[c].phys_n, s->qinterp, s->qinterp);
+    if (s0.n + s1.n <= 0) return;
+    (void)flush_updates(s);
+    if (s->fill) s->total_launches++;
+    if (s->emit) launch_phys(s->d, s0, s1, s->bc_dev, s->st);
 }
 static void interpolate2ghost(fc2d_b200_solver* s, int l, int ti)
 {
     if (l < 0 || l > 32 || !s->lr[l].interp_n) return;
+    (void)flush_updates(s);
     if (s->fill) s->total_launches++;
     if (s->emit)
         launch_interp(s->d, s->q, tsdata(s, ti), s->t_interp.p + s->lr[l].interp_off, s->lr[l].interp_n, s->st);
@@ -422,19 +484,15 @@ static void ghost_update(fc2d_b200_solver* s, int minlevel, int maxlevel, int ti
     if (s->fill)
         for (int l = std::max(minlevel, 0); l <= std::min(maxlevel, 63); l++) s->phys_ok[l] = 1;
     const int mincoarse = minlevel, maxcoarse = maxlevel - 1;
-    average_range(s, mincoarse, maxcoarse, 0);
-    if (time_interp) average_range(s, mincoarse - 1, mincoarse - 1, 1);
-    copy_range(s, minlevel, maxlevel, 0);
-    if (time_interp) copy_range(s, minlevel - 1, minlevel - 1, 1);
-    phys_range(s, mincoarse, maxcoarse, 0);
-    if (time_interp) phys_range(s, mincoarse - 1, mincoarse - 1, 1);
+    const int ti = time_interp ? mincoarse - 1 : -1;      // level of the time-interpolated copy
+    average_range(s, mincoarse, maxcoarse, ti);
+    copy_range(s, minlevel, maxlevel, ti);
+    phys_range(s, mincoarse, maxcoarse, ti);
     for (int l = maxcoarse; l >= mincoarse; l--) interpolate2ghost(s, l, 0);
     if (time_interp) interpolate2ghost(s, mincoarse - 1, 1);
     const int minfine = mincoarse + 1, maxfine = maxlevel;
-    phys_range(s, minfine, maxfine, 0);
-    if (time_interp) phys_range(s, minfine - 1, minfine - 1, 1);
-    phys_range(s, minlevel, maxlevel, 0);
-    if (time_interp) phys_range(s, minlevel - 1, minlevel - 1, 1);
+    phys_range(s, minfine, maxfine, ti);
+    phys_range(s, minlevel, maxlevel, ti);
 }
 
 // fclaw2d_time_sync(minlevel, maxlevel) as two launches: every correction of
@@ -453,12 +511,14 @@ static void time_sync(fc2d_b200_solver* s, int minlevel, int maxlevel)
     {   // samesize and f2c corrections, levels [a, maxl]
         const int g0 = s->lr[a].sync_start_off, g1 = s->lr[maxl].sync_start_off + s->lr[maxl].sync_np;
         if (g1 > g0) {
+            (void)flush_updates(s);
             if (s->fill) s->total_launches++;
             if (s->emit) launch_sync(s->d, s->q, s->regs, s->desc, s->t_sync.p, s->t_sync_start.p + g0, g1 - g0, s->st);
         }
     }
     const int p0 = s->forest.lev_off[a], p1 = s->forest.lev_off[maxl + 1];
     if (p1 > p0) {
+        (void)flush_updates(s);
         if (s->fill) s->total_launches++;
         if (s->emit) launch_reset_sync(s->d, s->regs, s->desc, p0, p1 - p0, a, maxl, s->st);
     }
@@ -467,6 +527,7 @@ static void time_sync(fc2d_b200_solver* s, int minlevel, int maxlevel)
 static void timeinterp(fc2d_b200_solver* s, int level, double alpha)
 {
     if (level < 0 || level > 32 || !s->lr[level].ti_n) return;
+    (void)flush_updates(s);
     if (s->fill) s->total_launches++;
     if (s->emit)
         launch_timeinterp(s->d, s->q, s->qlast, s->qinterp, s->t_ti.p + s->lr[level].ti_off, s->lr[level].ti_n, alpha,
@@ -565,7 +626,7 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
         s->vars = step2_variants(o.precision, o.rp, o.mx, o.my, o.mbc);
         s->var = 0;
         for (int l = 0; l < 33; l++) s->var_lev[l] = -1;
-        cudaError_t e = s->vars[0]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st);
+        cudaError_t e = s->vars[0]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, -1, nullptr, s->st);
         if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
         CK(cudaMalloc(&s->tune_params, sizeof(StepParams)));
     }
@@ -605,7 +666,7 @@ extern "C" int fc2d_b200_set_riemann(fc2d_b200_solver_t* s, int rp_id)
     s->var = 0;
     for (int l = 0; l < 33; l++) s->var_lev[l] = -1;
     invalidate_graph(s);
-    cudaError_t e = s->vars[0]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st);
+    cudaError_t e = s->vars[0]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, -1, nullptr, s->st);
     if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
     return 0;
 }
@@ -839,8 +900,11 @@ extern "C" int fc2d_b200_level_update(fc2d_b200_solver_t* s, int level, double t
     int rc = begin_cfl(s);
     if (rc) return rc;
     s->n_upd = 0;
+    s->pend.active = false;
     s->emit = true; s->fill = true;
     rc = update_level(s, level, t, dt);
+    if (rc) return rc;
+    rc = flush_updates(s);
     if (rc) return rc;
     return end_cfl(s, cfl);
 }
@@ -907,6 +971,7 @@ static int traverse_advance(fc2d_b200_solver* s, double t, double dt)
         for (int l = o.minlevel; l <= o.maxlevel; l++) { ts[l].step_inc = 1; ts[l].dt_step = dt / rf; ts[l].total_steps = rf; }
     }
     s->n_upd = 0;
+    s->pend.active = false;
     const int nfine = ts[maxlevel].total_steps;
     for (int nf = 0; nf < nfine; nf++) {
         int rc = advance_level(s, ts, maxlevel, nf);
@@ -925,7 +990,7 @@ static int traverse_advance(fc2d_b200_solver* s, double t, double dt)
     }
     ghost_update(s, minlevel, maxlevel, 0);
     if (o.time_sync) time_sync(s, minlevel, maxlevel);
-    return 0;
+    return flush_updates(s);
 }
 
 // First half of an advance: host traversal, parameter upload and the launches
@@ -1718,7 +1783,7 @@ extern "C" int fc2d_b200_variant_info(const fc2d_b200_solver_t* s, int v, int* t
 extern "C" int fc2d_b200_set_variant(fc2d_b200_solver_t* s, int v)
 {
     if (!s || v < 0 || v >= (int)s->vars.size()) return fail(FC2D_B200_EINVAL, "no such variant");
-    cudaError_t e = s->vars[v]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st);
+    cudaError_t e = s->vars[v]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, -1, nullptr, s->st);
     if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
     s->var = v;
     for (int l = 0; l < 33; l++) s->var_lev[l] = -1;
@@ -1745,7 +1810,7 @@ extern "C" int fc2d_b200_autotune(fc2d_b200_solver_t* s, int reps, int* best_out
         for (int l = 0; l <= 32; l++) {
             const int p0 = f.lev_off[l], np = f.lev_off[l + 1] - p0;
             if (np <= 0) continue;
-            cudaError_t e = v->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, s->tune_params, s->cfl_dev, s->st);
+            cudaError_t e = v->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, s->tune_params, -1, s->cfl_dev, s->st);
             if (e != cudaSuccess) return e;
         }
         return cudaSuccess;
@@ -1754,7 +1819,7 @@ extern "C" int fc2d_b200_autotune(fc2d_b200_solver_t* s, int reps, int* best_out
     double best_ms = 1e300;
     cudaError_t err = cudaSuccess;
     for (int v = 0; v < (int)s->vars.size() && err == cudaSuccess; v++) {
-        err = s->vars[v]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, s->st);
+        err = s->vars[v]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, -1, nullptr, s->st);
         if (err == cudaSuccess) err = pass(s->vars[v]);             // warm-up
         if (err == cudaSuccess) err = cudaEventRecord(e0, s->st);
         for (int r = 0; r < reps && err == cudaSuccess; r++) err = pass(s->vars[v]);
@@ -1776,10 +1841,10 @@ extern "C" int fc2d_b200_autotune(fc2d_b200_solver_t* s, int reps, int* best_out
         double lbest = 1e300;
         for (int v = 0; v < (int)s->vars.size() && err == cudaSuccess; v++) {
             const Step2Variant* x = s->vars[v];
-            err = x->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, s->tune_params, s->cfl_dev, s->st);
+            err = x->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, s->tune_params, -1, s->cfl_dev, s->st);
             if (err == cudaSuccess) err = cudaEventRecord(e0, s->st);
             for (int r = 0; r < reps && err == cudaSuccess; r++)
-                err = x->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, s->tune_params, s->cfl_dev, s->st);
+                err = x->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, s->tune_params, -1, s->cfl_dev, s->st);
             if (err == cudaSuccess) err = cudaEventRecord(e1, s->st);
             if (err == cudaSuccess) err = cudaEventSynchronize(e1);
             float ms = 0.0f;

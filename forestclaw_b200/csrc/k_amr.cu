@@ -25,25 +25,36 @@ bool programmatic_launch() { return tl_programmatic; }
 
 static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 
-__global__ void k_copy(double* __restrict__ dst, const double* __restrict__ src, const CopyEnt* __restrict__ e,
-                       int n, int nxy, int meqn)
+// The gather kernels take up to two table segments, each with its own arrays:
+// a ghost-fill stage on q and the same stage on the time-interpolated copy
+// write different arrays and read cells the other does not write, so they
+// share a launch (segment 0 first in the thread numbering).
+__global__ void k_copy(GatherSeg<CopyEnt> s0, GatherSeg<CopyEnt> s1, int nxy, int meqn)
 {
     grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
     int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    CopyEnt c = e[t];
-    for (int m = 0; m < meqn; m++) dst[c.dst + m * nxy] = src[c.src + m * nxy];
+    const bool one = t >= s0.n;
+    if (one) t -= s0.n;
+    const GatherSeg<CopyEnt>& g = one ? s1 : s0;
+    if (t >= g.n) return;
+    CopyEnt c = g.e[t];
+    for (int m = 0; m < meqn; m++) g.dst[c.dst + m * nxy] = g.src[c.src + m * nxy];
 }
 
-__global__ void k_average(double* __restrict__ dst, const double* __restrict__ src, const AvgEnt* __restrict__ e,
-                          int n, int nq, int nx, int nxy, int meqn, const double* __restrict__ area)
+__global__ void k_average(GatherSeg<AvgEnt> s0, GatherSeg<AvgEnt> s1, int nq, int nx, int nxy, int meqn,
+                          const double* __restrict__ area)
 {
     grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
     int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    AvgEnt c = e[t];
+    const bool one = t >= s0.n;
+    if (one) t -= s0.n;
+    const GatherSeg<AvgEnt>& g = one ? s1 : s0;
+    if (t >= g.n) return;
+    double* __restrict__ dst = g.dst;
+    const double* __restrict__ src = g.src;
+    AvgEnt c = g.e[t];
     const int o1 = c.sx, o2 = c.sy, o3 = c.sx + c.sy;
     if (area) {
         // manifold (fclaw2d_clawpatch46_average.f:96-115): sum(q_f a_f) / sum(a_f); the
@@ -109,14 +120,18 @@ __global__ void k_interp(double* __restrict__ dst, const double* __restrict__ sr
     }
 }
 
-__global__ void k_phys(double* __restrict__ q, const PhysEnt* __restrict__ e, int n, int nxy, int meqn,
+__global__ void k_phys(GatherSeg<PhysEnt> s0, GatherSeg<PhysEnt> s1, int nxy, int meqn,
                        const double* __restrict__ bcstate)
 {
     grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
     int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    PhysEnt c = e[t];
+    const bool one = t >= s0.n;
+    if (one) t -= s0.n;
+    const GatherSeg<PhysEnt>& g = one ? s1 : s0;
+    if (t >= g.n) return;
+    double* __restrict__ q = g.dst;                 // in place: sources are cells of the same array
+    PhysEnt c = g.e[t];
     for (int m = 0; m < meqn; m++) {
         double v = c.cst ? bcstate[m] : q[c.src + m * nxy];
         q[c.dst + m * nxy] = ((c.neg >> m) & 1) ? -v : v;
@@ -548,22 +563,26 @@ void launch_restore_patches(const Dims& d, double* dst, const double* src, const
     if (n > 0) k_restore_patches<<<n, 256, 0, st>>>(dst, src, slots, d.nq());
 }
 
-void launch_copy(const Dims& d, double* dst, const double* src, const CopyEnt* e, int n, cudaStream_t st)
+void launch_copy(const Dims& d, const GatherSeg<CopyEnt>& s0, const GatherSeg<CopyEnt>& s1, cudaStream_t st)
 {
-    if (n > 0) launch_k(k_copy, nblk(n, 256), 256, 0, st, dst, src, e, n, d.nxy(), d.meqn);
+    const long n = (long)s0.n + s1.n;
+    if (n > 0) launch_k(k_copy, nblk(n, 256), 256, 0, st, s0, s1, d.nxy(), d.meqn);
 }
-void launch_average(const Dims& d, double* dst, const double* src, const AvgEnt* e, int n, const double* area,
+void launch_average(const Dims& d, const GatherSeg<AvgEnt>& s0, const GatherSeg<AvgEnt>& s1, const double* area,
                     cudaStream_t st)
 {
-    if (n > 0) launch_k(k_average, nblk(n, 256), 256, 0, st, dst, src, e, n, d.nq(), d.nx(), d.nxy(), d.meqn, area);
+    const long n = (long)s0.n + s1.n;
+    if (n > 0) launch_k(k_average, nblk(n, 256), 256, 0, st, s0, s1, d.nq(), d.nx(), d.nxy(), d.meqn, area);
 }
 void launch_interp(const Dims& d, double* dst, const double* src, const InterpEnt* e, int n, cudaStream_t st)
 {
     if (n > 0) launch_k(k_interp, nblk(n, 256), 256, 0, st, dst, src, e, n, d.nx(), d.nxy(), d.meqn);
 }
-void launch_phys(const Dims& d, double* q, const PhysEnt* e, int n, const double* bcstate, cudaStream_t st)
+void launch_phys(const Dims& d, const GatherSeg<PhysEnt>& s0, const GatherSeg<PhysEnt>& s1, const double* bcstate,
+                 cudaStream_t st)
 {
-    if (n > 0) launch_k(k_phys, nblk(n, 256), 256, 0, st, q, e, n, d.nxy(), d.meqn, bcstate);
+    const long n = (long)s0.n + s1.n;
+    if (n > 0) launch_k(k_phys, nblk(n, 256), 256, 0, st, s0, s1, d.nxy(), d.meqn, bcstate);
 }
 void launch_timeinterp(const Dims& d, const double* q, const double* qlast, double* qinterp, const int* patches,
                        int npatch, double alpha, cudaStream_t st)

@@ -682,19 +682,23 @@ template <class RP, int MX, int MY, int MBC, bool FWAVE, int NT, typename TW, in
 __global__ void __launch_bounds__(NT, MINB)
 step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* __restrict__ aux,
              double* __restrict__ regs, const PatchDesc* __restrict__ desc, int p0, int npatch,
-             const StepParams* __restrict__ spp, unsigned long long* __restrict__ cfl_bits)
+             const StepParams* __restrict__ spp, int lev_hi, unsigned long long* __restrict__ cfl_bits)
 {
     grid_dependency_wait();         // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
-    const StepParams sp = *spp;     // per-launch parameters live in device memory (graph replay)
+    // per-launch parameters live in device memory (graph replay); a launch over
+    // several levels holds one block per level, highest level first
     __shared__ unsigned int nhist[RP::EXACT64 ? 32 : 1];
     if constexpr (!PERSIST) {
         (void)npatch;
-        step2_patch<RP, MX, MY, MBC, FWAVE, NT, TW>(q, qlast, aux, regs, desc, p0 + (int)blockIdx.x, sp, cfl_bits,
-                                                    nhist);
+        const int p = p0 + (int)blockIdx.x;
+        const StepParams sp = spp[lev_hi < 0 ? 0 : lev_hi - desc[p].level];
+        step2_patch<RP, MX, MY, MBC, FWAVE, NT, TW>(q, qlast, aux, regs, desc, p, sp, cfl_bits, nhist);
     } else {
         for (int b = blockIdx.x; b < npatch; b += gridDim.x) {
-            step2_patch<RP, MX, MY, MBC, FWAVE, NT, TW>(q, qlast, aux, regs, desc, p0 + b, sp, cfl_bits, nhist);
+            const int p = p0 + b;
+            const StepParams sp = spp[lev_hi < 0 ? 0 : lev_hi - desc[p].level];
+            step2_patch<RP, MX, MY, MBC, FWAVE, NT, TW>(q, qlast, aux, regs, desc, p, sp, cfl_bits, nhist);
             __syncthreads();   // the next patch restages the shared memory
         }
     }

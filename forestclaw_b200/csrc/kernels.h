@@ -32,9 +32,11 @@ struct Dims {
 // ---- fused update (k_step2_<precision>_<family>.cu) ---------------------------
 // Each unit holds a table of launchers, one per (solver, patch size, patch-to-CTA
 // mapping); the first entry of a shape is its default.  A launcher called with
-// npatch = 0 only sets the kernel's shared-memory attribute.
+// npatch = 0 only sets the kernel's shared-memory attribute.  lev_hi < 0: every
+// patch takes sp[0]; else the launch covers consecutive levels ..lev_hi and a
+// patch of level L takes sp[lev_hi - L].
 typedef cudaError_t (*Step2Fn)(double* q, double* qlast, const double* aux, double* regs, const PatchDesc* desc,
-                               int p0, int npatch, const StepParams* sp, unsigned long long* cfl_bits,
+                               int p0, int npatch, const StepParams* sp, int lev_hi, unsigned long long* cfl_bits,
                                cudaStream_t st);
 struct Step2Variant {
     int precision, rp, mx, my, mbc;
@@ -61,14 +63,17 @@ struct AvgEnt { int dst, src, sx, sy; };
 struct InterpEnt { int dst, src, sub, pad; };      // sub = child position 0..3 (ii + 2 jj)
 struct PhysEnt { int dst, src, neg, cst; };        // neg: bit m set => negate field m; cst: constant state
 
-void launch_copy(const Dims& d, double* dst, const double* src, const CopyEnt* e, int n, cudaStream_t st);
+// One table segment of a gather stage: entries e[0..n) from src into dst.
+template <class E> struct GatherSeg { double* dst; const double* src; const E* e; int n; };
+void launch_copy(const Dims& d, const GatherSeg<CopyEnt>& s0, const GatherSeg<CopyEnt>& s1, cudaStream_t st);
 void launch_restore_patches(const Dims& d, double* dst, const double* src, const int* slots, int n, cudaStream_t st);
 // area: per-patch cell areas (nxy per patch, q's cell indexing) for the area-weighted
 // average of a manifold, or null for the plain mean.
-void launch_average(const Dims& d, double* dst, const double* src, const AvgEnt* e, int n, const double* area,
+void launch_average(const Dims& d, const GatherSeg<AvgEnt>& s0, const GatherSeg<AvgEnt>& s1, const double* area,
                     cudaStream_t st);
 void launch_interp(const Dims& d, double* dst, const double* src, const InterpEnt* e, int n, cudaStream_t st);
-void launch_phys(const Dims& d, double* q, const PhysEnt* e, int n, const double* bcstate, cudaStream_t st);
+void launch_phys(const Dims& d, const GatherSeg<PhysEnt>& s0, const GatherSeg<PhysEnt>& s1, const double* bcstate,
+                 cudaStream_t st);
 void launch_timeinterp(const Dims& d, const double* q, const double* qlast, double* qinterp,
                        const int* patches, int npatch, double alpha, cudaStream_t st);
 

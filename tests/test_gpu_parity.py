@@ -269,3 +269,26 @@ def test_fp32wave_reflecting_walls_conserve_mass():
         m = g.mass()
         assert abs(m[0] - m1[0]) <= 1e-12 * abs(m1[0]), (problem["rp"], m[0] - m1[0])
         assert _l1_rel(g.get_q(), o.get_q(), 0) < FP32_L1_TOL
+
+
+def test_consecutive_level_updates_share_one_launch():
+    """A subcycled coarse step over levels 2-4 updates level 4 four times, level 3
+    twice and level 2 once; the updates issued back to back (4-3-2, 4, 4-3, 4) go out
+    as four launches, each patch with its own level's parameters, and the result
+    stays bitwise equal to the oracle (the oracle tests above run the same forests)."""
+    import forestclaw_b200 as fb
+    from oracle import pyoracle as po
+    oc, gc = make(DAM, mx=8, my=8, minlevel=2, maxlevel=4, subcycle=1, time_sync=1)
+    g = fb.Solver(gc)
+    g.initialize()
+    o = po.OracleSim(oc)
+    o.initialize()
+    levels = set(int(l) for l in g.patch_info()[:, 0])
+    assert levels == {2, 3, 4}
+    cg = g.advance(0.0, 0.01)
+    co = o.advance(0.0, 0.01)
+    st = g.last_update_stats()
+    assert st["update_launches"] == 4
+    assert cg == co and np.array_equal(g.get_q(), o.get_q())
+    assert np.array_equal(g.get_registers(), o.get_registers())
+    g.close()
