@@ -112,6 +112,10 @@ struct fc2d_b200_solver {
     // patches, so they go out as one launch over consecutive levels
     struct PendingUpdate { bool active = false; int lev_hi = 0, lev_lo = 0, p0 = 0, np = 0, slot = 0, var = 0; };
     PendingUpdate pend;
+    // time interpolations of consecutive coarser levels, issued back to back after
+    // an update, likewise share one launch (each level with its own alpha)
+    struct PendingTimeInterp { bool active = false; int lev_lo = 0, lev_hi = 0; LevelAlpha alpha{}; };
+    PendingTimeInterp pend_ti;
     StepParams* tune_params = nullptr;             // autotuner: dt = 0 parameters (device)
     DevVec<RepopOp> repop_dev;                     // regrid repopulation ops
     DevVec<double> snap;                           // batch regrid: q of instances whose forest is unchanged
@@ -344,6 +348,28 @@ static StepParams make_params(const fc2d_b200_solver* s, int level, double t, do
     return sp;
 }
 
+// Launch the pending group of time interpolations (levels lev_lo..lev_hi).
+static void flush_timeinterp(fc2d_b200_solver* s)
+{
+    fc2d_b200_solver::PendingTimeInterp& g = s->pend_ti;
+    if (!g.active) return;
+    g.active = false;
+    const int off = s->lr[g.lev_lo].ti_off, n = s->lr[g.lev_hi].ti_off + s->lr[g.lev_hi].ti_n - off;
+    if (n <= 0) return;
+    if (s->fill) s->total_launches++;
+    if (s->emit) launch_timeinterp(s->d, s->q, s->qlast, s->qinterp, s->t_ti.p + off, n, s->desc, g.alpha, s->st);
+}
+
+static int flush_updates(fc2d_b200_solver* s);
+// Launch whatever is pending, in issue order (a time-interpolation group always
+// follows the update group it was issued after, which it flushed).
+static int flush_pending(fc2d_b200_solver* s)
+{
+    int rc = flush_updates(s);
+    flush_timeinterp(s);
+    return rc;
+}
+
 // Launch the pending group of level updates (one launch, levels lev_lo..lev_hi).
 static int flush_updates(fc2d_b200_solver* s)
 {
@@ -377,6 +403,7 @@ static int update_level(fc2d_b200_solver* s, int level, double t, double dt)
     const int p0 = f.lev_off[level], np = f.lev_off[level + 1] - p0;
     if (np <= 0) return 0;
     if (s->n_upd >= fc2d_b200_solver::PCAP) return fail(FC2D_B200_EINVAL, "too many level updates in one advance");
+    flush_timeinterp(s);                              // it reads q of levels this update may write
     const int slot = s->n_upd++;
     if (s->fill) {
         StepParams& sp = s->params_host[slot];
@@ -438,7 +465,7 @@ static void copy_range(fc2d_b200_solver* s, int a, int b, int c)
     if (c >= 0 && c <= 32 && s->lr[c].copy_n > 0)
         s1 = seg(s->t_copy.p, s->lr[c].copy_off, s->lr[c].copy_n, s->qinterp, s->qinterp);
     if (s0.n + s1.n <= 0) return;
-    (void)flush_updates(s);
+    (void)flush_pending(s);
     if (s->fill) s->total_launches++;
     if (s->emit) launch_copy(s->d, s0, s1, s->st);
 }
@@ -452,7 +479,7 @@ static void average_range(fc2d_b200_solver* s, int a, int b, int c)
     if (c >= 0 && c <= 32 && s->lr[c].avg_n > 0)
         s1 = seg(s->t_avg.p, s->lr[c].avg_off, s->lr[c].avg_n, s->qinterp, s->q);
     if (s0.n + s1.n <= 0) return;
-    (void)flush_updates(s);
+    (void)flush_pending(s);
     if (s->fill) s->total_launches++;
     if (s->emit) launch_average(s->d, s0, s1, s->area, s->st);
 }
@@ -466,14 +493,14 @@ static void phys_range(fc2d_b200_solver* s, int a, int b, int c)
     if (c >= 0 && c <= 32 && s->lr[c].phys_n > 0)
         s1 = seg(s->t_phys.p, s->lr[c].phys_off, s->lr[c].phys_n, s->qinterp, s->qinterp);
     if (s0.n + s1.n <= 0) return;
-    (void)flush_updates(s);
+    (void)flush_pending(s);
     if (s->fill) s->total_launches++;
     if (s->emit) launch_phys(s->d, s0, s1, s->bc_dev, s->st);
 }
 static void interpolate2ghost(fc2d_b200_solver* s, int l, int ti)
 {
     if (l < 0 || l > 32 || !s->lr[l].interp_n) return;
-    (void)flush_updates(s);
+    (void)flush_pending(s);
     if (s->fill) s->total_launches++;
     if (s->emit)
         launch_interp(s->d, s->q, tsdata(s, ti), s->t_interp.p + s->lr[l].interp_off, s->lr[l].interp_n, s->st);
@@ -511,14 +538,14 @@ static void time_sync(fc2d_b200_solver* s, int minlevel, int maxlevel)
     {   // samesize and f2c corrections, levels [a, maxl]
         const int g0 = s->lr[a].sync_start_off, g1 = s->lr[maxl].sync_start_off + s->lr[maxl].sync_np;
         if (g1 > g0) {
-            (void)flush_updates(s);
+            (void)flush_pending(s);
             if (s->fill) s->total_launches++;
             if (s->emit) launch_sync(s->d, s->q, s->regs, s->desc, s->t_sync.p, s->t_sync_start.p + g0, g1 - g0, s->st);
         }
     }
     const int p0 = s->forest.lev_off[a], p1 = s->forest.lev_off[maxl + 1];
     if (p1 > p0) {
-        (void)flush_updates(s);
+        (void)flush_pending(s);
         if (s->fill) s->total_launches++;
         if (s->emit) launch_reset_sync(s->d, s->regs, s->desc, p0, p1 - p0, a, maxl, s->st);
     }
@@ -526,12 +553,18 @@ static void time_sync(fc2d_b200_solver* s, int minlevel, int maxlevel)
 
 static void timeinterp(fc2d_b200_solver* s, int level, double alpha)
 {
-    if (level < 0 || level > 32 || !s->lr[level].ti_n) return;
+    if (level < 0 || level > 31 || !s->lr[level].ti_n) return;
     (void)flush_updates(s);
-    if (s->fill) s->total_launches++;
-    if (s->emit)
-        launch_timeinterp(s->d, s->q, s->qlast, s->qinterp, s->t_ti.p + s->lr[level].ti_off, s->lr[level].ti_n, alpha,
-                          s->st);
+    fc2d_b200_solver::PendingTimeInterp& g = s->pend_ti;
+    if (g.active && level == g.lev_hi + 1) {        // the lists of consecutive levels are contiguous
+        g.lev_hi = level;
+        g.alpha.a[level] = alpha;
+        return;
+    }
+    flush_timeinterp(s);
+    g.active = true;
+    g.lev_lo = g.lev_hi = level;
+    g.alpha.a[level] = alpha;
 }
 
 struct Tsc { int last_step, step_inc, total_steps; double current_time, dt_step; };
@@ -930,6 +963,7 @@ extern "C" int fc2d_b200_ghost_update(fc2d_b200_solver_t* s, int minlevel, int m
     if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
     if (time_interp && !s->qinterp) return fail(FC2D_B200_EINVAL, "time interpolation needs subcycle");
     ghost_update(s, minlevel, maxlevel, time_interp);
+    (void)flush_pending(s);
     CK(cudaGetLastError());
     return 0;
 }
@@ -938,6 +972,7 @@ extern "C" int fc2d_b200_timeinterp(fc2d_b200_solver_t* s, int level, double alp
 {
     if (!s || !s->initialized || !s->qinterp) return fail(FC2D_B200_ESTATE, "time interpolation needs subcycle");
     timeinterp(s, level, alpha);
+    (void)flush_pending(s);
     CK(cudaGetLastError());
     return 0;
 }
@@ -946,6 +981,7 @@ extern "C" int fc2d_b200_time_sync(fc2d_b200_solver_t* s, int minlevel, int maxl
 {
     if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
     time_sync(s, minlevel, maxlevel);
+    (void)flush_pending(s);
     CK(cudaGetLastError());
     return 0;
 }
@@ -972,6 +1008,7 @@ static int traverse_advance(fc2d_b200_solver* s, double t, double dt)
     }
     s->n_upd = 0;
     s->pend.active = false;
+    s->pend_ti.active = false;
     const int nfine = ts[maxlevel].total_steps;
     for (int nf = 0; nf < nfine; nf++) {
         int rc = advance_level(s, ts, maxlevel, nf);
@@ -990,7 +1027,7 @@ static int traverse_advance(fc2d_b200_solver* s, double t, double dt)
     }
     ghost_update(s, minlevel, maxlevel, 0);
     if (o.time_sync) time_sync(s, minlevel, maxlevel);
-    return flush_updates(s);
+    return flush_pending(s);
 }
 
 // First half of an advance: host traversal, parameter upload and the launches

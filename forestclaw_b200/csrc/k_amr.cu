@@ -139,12 +139,16 @@ __global__ void k_phys(GatherSeg<PhysEnt> s0, GatherSeg<PhysEnt> s1, int nxy, in
 }
 
 // Band of width mbc inside the patch, in the four loops of timeinterp.f:33-70.
+// One CTA per listed patch; a launch may cover the lists of several levels, each
+// with its own alpha (alpha.a[level]).
 __global__ void k_timeinterp(const double* __restrict__ q, const double* __restrict__ ql, double* __restrict__ qi,
-                             const int* __restrict__ patches, int mx, int my, int mbc, int meqn, double alpha)
+                             const int* __restrict__ patches, const PatchDesc* __restrict__ desc, int mx, int my,
+                             int mbc, int meqn, LevelAlpha la)
 {
     grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
     const int p = patches[blockIdx.x];
+    const double alpha = la.a[desc[p].level & 31];
     const int nx = mx + 2 * mbc, ny = my + 2 * mbc, nxy = nx * ny;
     const size_t base = (size_t)p * nxy * meqn;
     for (int c = threadIdx.x; c < nxy; c += blockDim.x) {
@@ -585,9 +589,10 @@ void launch_phys(const Dims& d, const GatherSeg<PhysEnt>& s0, const GatherSeg<Ph
     if (n > 0) launch_k(k_phys, nblk(n, 256), 256, 0, st, s0, s1, d.nxy(), d.meqn, bcstate);
 }
 void launch_timeinterp(const Dims& d, const double* q, const double* qlast, double* qinterp, const int* patches,
-                       int npatch, double alpha, cudaStream_t st)
+                       int npatch, const PatchDesc* desc, const LevelAlpha& alpha, cudaStream_t st)
 {
-    if (npatch > 0) launch_k(k_timeinterp, npatch, 256, 0, st, q, qlast, qinterp, patches, d.mx, d.my, d.mbc, d.meqn, alpha);
+    if (npatch > 0)
+        launch_k(k_timeinterp, npatch, 256, 0, st, q, qlast, qinterp, patches, desc, d.mx, d.my, d.mbc, d.meqn, alpha);
 }
 void launch_sync(const Dims& d, double* q, const double* regs, const PatchDesc* desc, const SyncOp* ops,
                  const int* op_start, int nblocks, cudaStream_t st)

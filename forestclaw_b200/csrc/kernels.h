@@ -74,8 +74,11 @@ void launch_average(const Dims& d, const GatherSeg<AvgEnt>& s0, const GatherSeg<
 void launch_interp(const Dims& d, double* dst, const double* src, const InterpEnt* e, int n, cudaStream_t st);
 void launch_phys(const Dims& d, const GatherSeg<PhysEnt>& s0, const GatherSeg<PhysEnt>& s1, const double* bcstate,
                  cudaStream_t st);
-void launch_timeinterp(const Dims& d, const double* q, const double* qlast, double* qinterp,
-                       const int* patches, int npatch, double alpha, cudaStream_t st);
+// time interpolation factor of each level (levels 0..31) for a launch over the
+// time-interpolation lists of several levels
+struct LevelAlpha { double a[32]; };
+void launch_timeinterp(const Dims& d, const double* q, const double* qlast, double* qinterp, const int* patches,
+                       int npatch, const PatchDesc* desc, const LevelAlpha& alpha, cudaStream_t st);
 
 // ---- time sync (k_amr.cu) -------------------------------------------------------
 // One op = (coarse/this patch, fine/neighbour patch, face, igrid).  Ops of one
