@@ -125,6 +125,9 @@ int  orc_euler_star(double gam, const double* wl, const double* wr, double seed,
 /* conserved (rho, m_n, m_t, E) states -> waves[3][4], speeds[3], amdq, apdq */
 int  orc_euler_interface(double gam, double tol, const double* ql, const double* qr, double seed,
                          double wave[3][4], double s[3], double* amdq, double* apdq);
+/* clawpack46_rpt2_euler4 of one interface with its Roe averages (tests). */
+void orc_euler_rpt2_point(double gam, int ixy, const double* qlo, const double* qhi, const double* asdq, double* bm,
+                          double* bp);
 void orc_euler_postshock(double gam, double mach, double* out);
 /* Newton-iteration histogram of all exact solves so far (32 bins; reset if asked). */
 void orc_newton_hist(long* out, int reset);

@@ -259,6 +259,29 @@ int orc_euler_interface(double gam, double tol, const double* ql, const double* 
     return it;
 }
 
+/* Roe averages of the interface between qlo (cell i-1) and qhi (cell i), states in
+ * (rho, rho u, rho v, E) order, mu / mv the normal and tangential momentum (0-based):
+ * clawpack46_rpn2_euler4.f:84-99 with gamma1 = gamma - 1. */
+static void roe_averages(double gamma1, int mu, int mv, const double* qlo, const double* qhi, double* u_out,
+                         double* v_out, double* enth_out, double* a_out, double* g1a2_out)
+{
+    const double rhsqrtl = sqrt(qlo[0]);
+    const double rhsqrtr = sqrt(qhi[0]);
+    const double pl = gamma1 * (qlo[3] - 0.5 * (qlo[1] * qlo[1] + qlo[2] * qlo[2]) / qlo[0]);
+    const double pr = gamma1 * (qhi[3] - 0.5 * (qhi[1] * qhi[1] + qhi[2] * qhi[2]) / qhi[0]);
+    const double rhsq2 = rhsqrtl + rhsqrtr;
+    const double u = (qlo[mu] / rhsqrtl + qhi[mu] / rhsqrtr) / rhsq2;
+    const double v = (qlo[mv] / rhsqrtl + qhi[mv] / rhsqrtr) / rhsq2;
+    const double enth = ((qlo[3] + pl) / rhsqrtl + (qhi[3] + pr) / rhsqrtr) / rhsq2;
+    const double u2v2 = u * u + v * v;
+    const double a2 = gamma1 * (enth - 0.5 * u2v2);
+    *u_out = u;
+    *v_out = v;
+    *enth_out = enth;
+    *a_out = sqrt(a2);
+    *g1a2_out = gamma1 / a2;
+}
+
 /* rpn2 for the oracle's flux2: exact normal solve + Roe averages for rpt2
  * (clawpack46_rpn2_euler4.f:83-100 with gamma1 = gamma - 1). */
 void orc_rpn2_euler(orc_rpctx* ctx, int ixy, int maxm, int meqn, int mwaves, int maux, int mbc, int mx,
@@ -274,21 +297,10 @@ void orc_rpn2_euler(orc_rpctx* ctx, int ixy, int maxm, int meqn, int mwaves, int
 #define QR(i, m) qr[I1(i) + ((m) - 1) * L]
     for (int i = 2 - mbc; i <= mx + mbc; i++) {
         /* Roe averages, clawpack46_rpn2_euler4.f:84-99 */
-        const double rhsqrtl = sqrt(QR(i - 1, 1));
-        const double rhsqrtr = sqrt(QL(i, 1));
-        const double pl = gamma1 * (QR(i - 1, 4) - 0.5 * (QR(i - 1, 2) * QR(i - 1, 2) + QR(i - 1, 3) * QR(i - 1, 3)) / QR(i - 1, 1));
-        const double pr = gamma1 * (QL(i, 4) - 0.5 * (QL(i, 2) * QL(i, 2) + QL(i, 3) * QL(i, 3)) / QL(i, 1));
-        const double rhsq2 = rhsqrtl + rhsqrtr;
-        const double u = (QR(i - 1, mu) / rhsqrtl + QL(i, mu) / rhsqrtr) / rhsq2;
-        const double v = (QR(i - 1, mv) / rhsqrtl + QL(i, mv) / rhsqrtr) / rhsq2;
-        const double enth = ((QR(i - 1, 4) + pl) / rhsqrtl + (QL(i, 4) + pr) / rhsqrtr) / rhsq2;
-        const double u2v2 = u * u + v * v;
-        const double a2 = gamma1 * (enth - 0.5 * u2v2);
-        ctx->u[I1(i)] = u;
-        ctx->v[I1(i)] = v;
-        ctx->h[I1(i)] = enth;
-        ctx->a[I1(i)] = sqrt(a2);
-        ctx->e[I1(i)] = gamma1 / a2;
+        const double qlo[4] = {QR(i - 1, 1), QR(i - 1, 2), QR(i - 1, 3), QR(i - 1, 4)};
+        const double qhi[4] = {QL(i, 1), QL(i, 2), QL(i, 3), QL(i, 4)};
+        roe_averages(gamma1, mu - 1, mv - 1, qlo, qhi, &ctx->u[I1(i)], &ctx->v[I1(i)], &ctx->h[I1(i)],
+                     &ctx->a[I1(i)], &ctx->e[I1(i)]);
         /* exact normal solve in (rho, m_normal, m_tangential, E) order */
         const double qa[4] = {QR(i - 1, 1), QR(i - 1, mu), QR(i - 1, mv), QR(i - 1, 4)};
         const double qb[4] = {QL(i, 1), QL(i, mu), QL(i, mv), QL(i, 4)};
@@ -347,6 +359,25 @@ void orc_rpt2_euler(orc_rpctx* ctx, int ixy, int maxm, int meqn, int mwaves, int
         }
     }
 #undef AS
+}
+
+/* The transverse split of one interface (test entry): the Roe averages of the
+ * interface between qlo (cell i-1) and qhi (cell i) as rpn2 forms them, then
+ * orc_rpt2_euler on a one-interface strip.  ixy = 1 (x) or 2 (y); states, asdq,
+ * bm, bp in (rho, rho u, rho v, E) order. */
+void orc_euler_rpt2_point(double gam, int ixy, const double* qlo, const double* qhi, const double* asdq, double* bm,
+                          double* bp)
+{
+    enum { mbc = 1, mx = 0, maxm = 0, L = 2 };      /* the strip's loop visits i = 1 only */
+    const int mu = (ixy == 1) ? 2 : 3, mv = (ixy == 1) ? 3 : 2;
+    double u[L], v[L], h[L], a[L], e[L], as[4 * L], bms[4 * L], bps[4 * L];
+    orc_rpctx ctx;
+    memset(&ctx, 0, sizeof(ctx));
+    ctx.u = u; ctx.v = v; ctx.h = h; ctx.a = a; ctx.e = e; ctx.gamma = gam;
+    roe_averages(gam - 1.0, mu - 1, mv - 1, qlo, qhi, &u[I1(1)], &v[I1(1)], &h[I1(1)], &a[I1(1)], &e[I1(1)]);
+    for (int m = 0; m < 4; m++) as[I1(1) + m * L] = asdq[m];
+    orc_rpt2_euler(&ctx, ixy, maxm, 4, 3, 0, mbc, mx, NULL, NULL, NULL, NULL, NULL, 1, as, bms, bps);
+    for (int m = 0; m < 4; m++) { bm[m] = bms[I1(1) + m * L]; bp[m] = bps[I1(1) + m * L]; }
 }
 
 /* Euler flux of one cell in direction idir (0: x, 1: y), the rpn2_cons of the

@@ -4,7 +4,7 @@ Test infrastructure (the checker's checker): ``oracle/_ref/libpin_cudaclaw.so``
 is built by ``make -C oracle ref`` from the reference tree's
 ``src/solvers/fc2d_cudaclaw/cuda_source/cudaclaw_flux2.cu`` and
 ``cudaclaw_limiters.cu``, the cudaclaw app Riemann solvers (swirl advection,
-radialdam Roe) and ``oracle/ref_cudaclaw/{pin_harness,
+radialdam Roe, shock-bubble Euler transverse) and ``oracle/ref_cudaclaw/{pin_harness,
 ref_app_solvers}.cu``.  Calling it needs a GPU; only the golden-vector script and
 the tests load it.
 """
@@ -43,6 +43,8 @@ def lib():
         I = ctypes.c_int
         L.pin_cudaclaw_step.argtypes = [I, I, I, I, I, I, I, I, I, ip, ip, ctypes.c_double, dp, dp, dp, dp, dp, dp]
         L.pin_cudaclaw_step.restype = ctypes.c_int
+        L.pin_ref_euler_rpt2.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp, dp, dp, dp]
+        L.pin_ref_euler_rpt2.restype = ctypes.c_int
         L.pin_cudaclaw_limiter.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int]
         L.pin_cudaclaw_limiter.restype = ctypes.c_int
         _lib = L
@@ -79,6 +81,17 @@ def step(solver, q, aux, dx, dt, order, mthlim, use_fwaves=0, grav=1.0, dry_tole
     if rc != 0:
         raise RuntimeError(f"cudaclaw update failed: code {rc}")
     return q, cfl
+
+
+def euler_rpt2(idir, ql, qr, asdq, gamma=1.4):
+    """The reference's Euler transverse solver (shockbubble_rpt2euler4) on n interfaces:
+    ql, qr the cells below / above, asdq the fluctuation, all (n, 4); returns bm, bp."""
+    a, b, c = (np.ascontiguousarray(x, np.float64) for x in (ql, qr, asdq))
+    bm, bp = np.zeros_like(a), np.zeros_like(a)
+    rc = lib().pin_ref_euler_rpt2(int(idir), a.shape[0], float(gamma), _dp(a), _dp(b), _dp(c), _dp(bm), _dp(bp))
+    if rc != 0:
+        raise RuntimeError(f"reference Euler transverse solver failed: code {rc}")
+    return bm, bp
 
 
 def limiter(lim, r):

@@ -97,6 +97,8 @@ def lib():
         L.orc_euler_interface.restype = ctypes.c_int
         L.orc_euler_interface.argtypes = [ctypes.c_double, ctypes.c_double, dp, dp, ctypes.c_double, dp, dp, dp, dp]
         L.orc_euler_postshock.argtypes = [ctypes.c_double, ctypes.c_double, dp]
+        L.orc_euler_rpt2_point.argtypes = [ctypes.c_double, ctypes.c_int, dp, dp, dp, dp, dp]
+        L.orc_euler_rpt2_point.restype = None
         L.orc_newton_hist.argtypes = [ctypes.POINTER(ctypes.c_long), ctypes.c_int]
         _lib = L
     return _lib
@@ -235,6 +237,14 @@ def euler_interface(gam, ql, qr, seed=0.0, tol=1e-10):
     w, s, am, ap = np.zeros((3, 4)), np.zeros(3), np.zeros(4), np.zeros(4)
     it = lib().orc_euler_interface(gam, tol, _dptr(a), _dptr(b), seed, _dptr(w), _dptr(s), _dptr(am), _dptr(ap))
     return w, s, am, ap, it
+
+
+def euler_rpt2(gam, ixy, qlo, qhi, asdq):
+    """clawpack46_rpt2_euler4 of one interface (Roe averages of qlo | qhi): (bmasdq, bpasdq)."""
+    a, b, c = (np.ascontiguousarray(x, np.float64) for x in (qlo, qhi, asdq))
+    bm, bp = np.zeros(4), np.zeros(4)
+    lib().orc_euler_rpt2_point(gam, int(ixy), _dptr(a), _dptr(b), _dptr(c), _dptr(bm), _dptr(bp))
+    return bm, bp
 
 
 def euler_postshock(gam, mach):

@@ -14,8 +14,11 @@ advances seeded patches once per (order, limiters) case of three families:
                f-waves, corrections scaled by sign(s), transverse f-waves
   radialdam    shallow water, Roe solver (radialdam_cuda/user_cuda/rpn2shallow.cu)
 
-and its limiter function is sampled.  The fixture pins the CPU oracle's update,
-its clawpack 4.6 Riemann solvers and its limiters
+and its limiter function is sampled.  The shock-bubble app's transverse solver
+(applications/cudaclaw/euler/2d/shockbubble/user_cuda/rp2euler.cu,
+shockbubble_rpt2euler4) is evaluated on seeded interface states in both
+directions.  The fixture pins the CPU oracle's update, its clawpack 4.6 Riemann
+solvers, the Euler transverse split and its limiters
 (tests/test_oracle_pin_cudaclaw.py).
 
 Where the reference's GPU path and its clawpack 4.6 path differ by design, the
@@ -96,6 +99,19 @@ def inputs(family: str, seed: int = 20261203, npatch: int = 4, mx: int = 16, mbc
     return q, aux, dx, dt
 
 
+def euler_inputs(seed: int = 20261204, n: int = 512):
+    """Seeded pairs of Euler states (rho, rho u, rho v, E) for gamma 1.4 -- density
+    0.3-3, velocities in [-1.5, 1.5], pressure 0.3-3 -- and fluctuations asdq of
+    both signs."""
+    rng = np.random.default_rng(seed)
+    def states():
+        rho = rng.uniform(0.3, 3.0, n)
+        u, v = rng.uniform(-1.5, 1.5, n), rng.uniform(-1.5, 1.5, n)
+        p = rng.uniform(0.3, 3.0, n)
+        return np.stack([rho, rho * u, rho * v, p / 0.4 + 0.5 * rho * (u * u + v * v)], axis=1)
+    return states(), states(), rng.standard_normal((n, 4))
+
+
 def limiter_samples():
     return np.concatenate([np.linspace(-3.0, 3.0, 121), [0.0, 0.5, 1.0, 2.0, -0.0, 1e-300, 1e300, -1e300]])
 
@@ -117,6 +133,10 @@ def main(out_path: str = OUT) -> None:
             qo, _ = pr.step(solver, q, aux, dx, dt, order, lim, use_fwaves=fw, grav=grav)
             out[f"{fam}_q_out_{k}"] = qo
             total += 1
+    ql, qr, asdq = euler_inputs()
+    out["euler_ql"], out["euler_qr"], out["euler_asdq"] = ql, qr, asdq
+    for idir in (0, 1):
+        out[f"euler_bm_{idir}"], out[f"euler_bp_{idir}"] = pr.euler_rpt2(idir, ql, qr, asdq, 1.4)
     r = limiter_samples()
     out["limiter_r"] = r
     for lim in range(0, 6):

@@ -92,6 +92,31 @@ def test_oracle_update_matches_reference_cudaclaw(family):
         _assert_close(_oracle_step(family, q, aux, dx, dt, order, lim), ref, f"{family} order {order} limiters {lim}")
 
 
+EULER_TOL = 1e-13
+
+
+def _euler_check(ql, qr, asdq, bm_ref, bp_ref, idir):
+    from oracle import pyoracle as po
+    for k in range(ql.shape[0]):
+        bm, bp = po.euler_rpt2(1.4, idir + 1, ql[k], qr[k], asdq[k])
+        scale = max(np.abs(bm_ref[k]).max(), np.abs(bp_ref[k]).max(), np.abs(asdq[k]).max())
+        err = max(np.abs(bm - bm_ref[k]).max(), np.abs(bp - bp_ref[k]).max())
+        assert err <= EULER_TOL * scale, f"interface {k} idir {idir}: {err:.3e} > {EULER_TOL:g} x {scale:.3e}"
+
+
+def test_oracle_euler_transverse_matches_reference_cudaclaw():
+    """clawpack46_rpt2_euler4 as the oracle restates it (Roe averages of the two
+    cells, three waves, split by the sign of their speeds) against the reference's
+    GPU port shockbubble_rpt2euler4.  The port takes 1/(2a) as 0.5 rsqrt(a^2), one
+    unit in the last place from the division, so the outputs agree to 1e-13 of the
+    interface's largest value."""
+    d = _fixture()
+    ql, qr, asdq = mk.euler_inputs()
+    assert np.array_equal(ql, d["euler_ql"]) and np.array_equal(asdq, d["euler_asdq"])
+    for idir in (0, 1):
+        _euler_check(ql, qr, asdq, d[f"euler_bm_{idir}"], d[f"euler_bp_{idir}"], idir)
+
+
 def test_oracle_limiters_match_reference_cudaclaw_bitwise():
     from oracle import pyoracle as po
     d = _fixture()
@@ -115,3 +140,14 @@ def test_oracle_update_matches_reference_cudaclaw_live(family, seed):
         ref, _ = pr.step(solver, q, aux, dx, dt, order, lim, use_fwaves=fw, grav=grav)
         _assert_close(_oracle_step(family, q, aux, dx, dt, order, lim), ref,
                       f"{family} seed {seed} order {order} limiters {lim}")
+
+
+@pytest.mark.gpu
+def test_oracle_euler_transverse_matches_reference_cudaclaw_live():
+    from oracle import pin_reference as pr
+    if not pr.available():
+        pytest.skip("oracle/_ref/libpin_cudaclaw.so not built (reference tree absent at build time)")
+    ql, qr, asdq = mk.euler_inputs(seed=7, n=2048)
+    for idir in (0, 1):
+        bm, bp = pr.euler_rpt2(idir, ql, qr, asdq, 1.4)
+        _euler_check(ql, qr, asdq, bm, bp, idir)
