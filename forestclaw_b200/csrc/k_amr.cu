@@ -177,21 +177,23 @@ struct RegOff {
     }
 };
 
-// The corrections of a time sync, one CTA per patch with corrections and one
-// thread per (boundary cell of the interior, field).  A face of a patch is
-// either same-size (one samesize op) or half-size (two f2c ops, igrid 0 and 1),
-// so a cell sees at most the ops of its x face and of its y face; the CTA first
-// files the patch's ops by face in shared memory, then each thread applies the
-// ops of its cell in table order -- samesize of the x face, of the y face, then
-// f2c of the x face, of the y face -- which is the reference's order of the
+// The corrections of a time sync, one CTA per patch with corrections.  A face of
+// a patch is either same-size (one samesize op) or half-size (two f2c ops, igrid
+// 0 and 1, each covering half the face), so every (face, tangential index,
+// field) has at most one correction.  The CTA files the patch's ops by face in
+// shared memory, computes every correction with one thread each (phase 1), then
+// adds them to the boundary cells with one thread per (cell, field) (phase 2):
+// a corner cell on two corrected faces takes the samesize corrections first,
+// then the f2c ones, each kind in face order -- the order of the reference's
 // additions to that cell.  Every op reads registers only, which no correction
-// writes, so the cells are independent.
+// writes.
 //   samesize: clawpack46_fort_time_sync_samesize (same orientation, sc = 1),
 //             clawpack46_time_sync.f:528-704: delta = (ef_n - ef_t) - (f_n - f_t),
 //             q += 0.5 delta / area
 //   f2c:      clawpack46_fort_time_sync_f2c (same orientation, sc = 1),
 //             clawpack46_time_sync.f:254-498: the fine pair d, d+1 (d = 1 + n_off + 2 j)
 //             of coarse cell j, skipped when outside the fine face; q += deltac / area
+// Dynamic shared memory: 4 * meqn * max(mx, my) doubles and as many flag bytes.
 __global__ void k_sync(double* __restrict__ q, const double* __restrict__ regs, const PatchDesc* __restrict__ desc,
                        const SyncOp* __restrict__ ops, const int* __restrict__ op_start,
                        int mx, int my, int mbc, int meqn, int nreg)
@@ -200,6 +202,9 @@ __global__ void k_sync(double* __restrict__ q, const double* __restrict__ regs, 
     grid_launch_dependents();
     __shared__ SyncOp s_op[8];
     __shared__ int s_ss[4], s_fc[4][2];                       // op slots per face (-1: none)
+    extern __shared__ double s_corr[];                        // [face][field][j]
+    const int nmax = mx > my ? mx : my;
+    unsigned char* s_has = reinterpret_cast<unsigned char*>(s_corr + 4 * meqn * nmax);
     const int o0 = op_start[blockIdx.x], o1 = op_start[blockIdx.x + 1];
     const int nops = o1 - o0;                                  // <= 8: two ops on each of four faces
     if (nops <= 0 || nops > 8) return;
@@ -214,42 +219,29 @@ __global__ void k_sync(double* __restrict__ q, const double* __restrict__ regs, 
     __syncthreads();
     const int p = s_op[0].p;                                   // every op of the block corrects patch p
     const int nx = mx + 2 * mbc, ny = my + 2 * mbc, nxy = nx * ny;
-    const int ring = 2 * (mx + my) - 4;                        // interior cells on the patch boundary
     const double area = desc[p].dx * desc[p].dy;
     RegOff R(mx, my, meqn);
     const double* rt = regs + (size_t)p * nreg;
-    for (int t = threadIdx.x; t < ring * meqn; t += blockDim.x) {
-        const int m = t / ring, k = t % ring;
-        int ic, jc;                                            // storage indices of the cell
-        if (k < mx) { ic = mbc + k; jc = mbc; }
-        else if (k < 2 * mx) { ic = mbc + k - mx; jc = my + mbc - 1; }
-        else if (k < 2 * mx + my - 2) { ic = mbc; jc = mbc + 1 + (k - 2 * mx); }
-        else { ic = mx + mbc - 1; jc = mbc + 1 + (k - 2 * mx - (my - 2)); }
-        const int fx = (ic == mbc) ? 0 : (ic == mx + mbc - 1) ? 1 : -1;
-        const int fy = (jc == mbc) ? 2 : (jc == my + mbc - 1) ? 3 : -1;
-        const int slot[6] = {fx >= 0 ? s_ss[fx] : -1, fy >= 0 ? s_ss[fy] : -1,
-                             fx >= 0 ? s_fc[fx][0] : -1, fx >= 0 ? s_fc[fx][1] : -1,
-                             fy >= 0 ? s_fc[fy][0] : -1, fy >= 0 ? s_fc[fy][1] : -1};
-        double* qq = q + (size_t)p * nxy * meqn + (size_t)m * nxy + jc * nx + ic;
-        double v = 0.0;
-        bool touched = false;
-        for (int u = 0; u < 6; u++) {
-            if (slot[u] < 0) continue;
-            const SyncOp& op = s_op[slot[u]];
-            const int j = (op.face < 2) ? jc - mbc : ic - mbc;  // 0-based tangential index along the face
-            const double* rn = regs + (size_t)op.n * nreg;
-            double corr;
-            if (op.kind == SYNC_SAMESIZE) {
+    // ---- phase 1: the correction of each (face, field, tangential index) ----
+    for (int t = threadIdx.x; t < 4 * meqn * nmax; t += blockDim.x) {
+        const int face = t / (meqn * nmax), r = t % (meqn * nmax), m = r / nmax, j = r % nmax;
+        const int nt = (face < 2) ? my : mx;
+        bool has = false;
+        double corr = 0.0;
+        if (j < nt) {
+            if (s_ss[face] >= 0) {
+                const SyncOp& op = s_op[s_ss[face]];
+                const double* rn = regs + (size_t)op.n * nreg;
                 double delta;
-                if (op.face == 0) {
+                if (face == 0) {
                     double fp = rn[R.fp1 + j + m * my];
                     double ef = 1 * rn[R.ef1 + j + m * my + my * meqn];
                     delta = (ef - rt[R.ef0 + j + m * my]) - (fp - rt[R.fp0 + j + m * my]);
-                } else if (op.face == 1) {
+                } else if (face == 1) {
                     double fm = rn[R.fm0 + j + m * my];
                     double ef = 1 * rn[R.ef0 + j + m * my + my * meqn];
                     delta = (rt[R.ef1 + j + m * my] - ef) - (fm - rt[R.fm1 + j + m * my]);
-                } else if (op.face == 2) {
+                } else if (face == 2) {
                     double gp = rn[R.gp1 + j + m * mx];
                     double ef = 1 * rn[R.ef3 + j + m * mx + mx * meqn];
                     delta = (ef - rt[R.ef2 + j + m * mx]) - (gp - rt[R.gp0 + j + m * mx]);
@@ -259,33 +251,67 @@ __global__ void k_sync(double* __restrict__ q, const double* __restrict__ regs, 
                     delta = (rt[R.ef3 + j + m * mx] - ef) - (gm - rt[R.gm1 + j + m * mx]);
                 }
                 corr = 0.5 * delta / area;
+                has = true;
             } else {
-                const int nt = (op.face < 2) ? my : mx;
-                const int d = 1 + op.n_off + 2 * j;            // first fine child (Fortran index)
-                if (d < 1 || d + 1 > nt) continue;             // fc46_skip_this_grid
-                const int f0 = d - 1, f1 = d;                  // 0-based fine pair
-                double deltac;
-                if (op.face == 0) {
-                    double fp = rn[R.fp1 + f0 + m * my] + rn[R.fp1 + f1 + m * my];
-                    double ef = 1 * (rn[R.ef1 + f0 + m * my + my * meqn] + rn[R.ef1 + f1 + m * my + my * meqn]);
-                    deltac = (ef - rt[R.ef0 + j + m * my]) - (fp - rt[R.fp0 + j + m * my]);
-                } else if (op.face == 1) {
-                    double fm = rn[R.fm0 + f0 + m * my] + rn[R.fm0 + f1 + m * my];
-                    double ef = 1 * (rn[R.ef0 + f0 + m * my + my * meqn] + rn[R.ef0 + f1 + m * my + my * meqn]);
-                    deltac = (rt[R.ef1 + j + m * my] - ef) - (fm - rt[R.fm1 + j + m * my]);
-                } else if (op.face == 2) {
-                    double gp = rn[R.gp1 + f0 + m * mx] + rn[R.gp1 + f1 + m * mx];
-                    double ef = 1 * (rn[R.ef3 + f0 + m * mx + mx * meqn] + rn[R.ef3 + f1 + m * mx + mx * meqn]);
-                    deltac = (ef - rt[R.ef2 + j + m * mx]) - (gp - rt[R.gp0 + j + m * mx]);
-                } else {
-                    double gm = rn[R.gm0 + f0 + m * mx] + rn[R.gm0 + f1 + m * mx];
-                    double ef = 1 * (rn[R.ef2 + f0 + m * mx + mx * meqn] + rn[R.ef2 + f1 + m * mx + mx * meqn]);
-                    deltac = (rt[R.ef3 + j + m * mx] - ef) - (gm - rt[R.gm1 + j + m * mx]);
+                for (int ig = 0; ig < 2 && !has; ig++) {
+                    if (s_fc[face][ig] < 0) continue;
+                    const SyncOp& op = s_op[s_fc[face][ig]];
+                    const int d = 1 + op.n_off + 2 * j;        // first fine child (Fortran index)
+                    if (d < 1 || d + 1 > nt) continue;         // fc46_skip_this_grid
+                    const double* rn = regs + (size_t)op.n * nreg;
+                    const int f0 = d - 1, f1 = d;              // 0-based fine pair
+                    double deltac;
+                    if (face == 0) {
+                        double fp = rn[R.fp1 + f0 + m * my] + rn[R.fp1 + f1 + m * my];
+                        double ef = 1 * (rn[R.ef1 + f0 + m * my + my * meqn] + rn[R.ef1 + f1 + m * my + my * meqn]);
+                        deltac = (ef - rt[R.ef0 + j + m * my]) - (fp - rt[R.fp0 + j + m * my]);
+                    } else if (face == 1) {
+                        double fm = rn[R.fm0 + f0 + m * my] + rn[R.fm0 + f1 + m * my];
+                        double ef = 1 * (rn[R.ef0 + f0 + m * my + my * meqn] + rn[R.ef0 + f1 + m * my + my * meqn]);
+                        deltac = (rt[R.ef1 + j + m * my] - ef) - (fm - rt[R.fm1 + j + m * my]);
+                    } else if (face == 2) {
+                        double gp = rn[R.gp1 + f0 + m * mx] + rn[R.gp1 + f1 + m * mx];
+                        double ef = 1 * (rn[R.ef3 + f0 + m * mx + mx * meqn] + rn[R.ef3 + f1 + m * mx + mx * meqn]);
+                        deltac = (ef - rt[R.ef2 + j + m * mx]) - (gp - rt[R.gp0 + j + m * mx]);
+                    } else {
+                        double gm = rn[R.gm0 + f0 + m * mx] + rn[R.gm0 + f1 + m * mx];
+                        double ef = 1 * (rn[R.ef2 + f0 + m * mx + mx * meqn] + rn[R.ef2 + f1 + m * mx + mx * meqn]);
+                        deltac = (rt[R.ef3 + j + m * mx] - ef) - (gm - rt[R.gm1 + j + m * mx]);
+                    }
+                    corr = deltac / area;
+                    has = true;
                 }
-                corr = deltac / area;
             }
+        }
+        s_corr[t] = corr;
+        s_has[t] = has ? 1 : 0;
+    }
+    __syncthreads();
+    // ---- phase 2: add them to the boundary cells, samesize faces first ----
+    const int ring = 2 * (mx + my) - 4;                        // interior cells on the patch boundary
+    for (int t = threadIdx.x; t < ring * meqn; t += blockDim.x) {
+        const int m = t / ring, k = t % ring;
+        int ic, jc;                                            // storage indices of the cell
+        if (k < mx) { ic = mbc + k; jc = mbc; }
+        else if (k < 2 * mx) { ic = mbc + k - mx; jc = my + mbc - 1; }
+        else if (k < 2 * mx + my - 2) { ic = mbc; jc = mbc + 1 + (k - 2 * mx); }
+        else { ic = mx + mbc - 1; jc = mbc + 1 + (k - 2 * mx - (my - 2)); }
+        const int fx = (ic == mbc) ? 0 : (ic == mx + mbc - 1) ? 1 : -1;
+        const int fy = (jc == mbc) ? 2 : (jc == my + mbc - 1) ? 3 : -1;
+        // slots of the cell's corrections on its x and y faces, in the reference's order
+        int sl[2] = {-1, -1};
+        if (fx >= 0) sl[0] = (fx * meqn + m) * nmax + (jc - mbc);
+        if (fy >= 0) sl[1] = (fy * meqn + m) * nmax + (ic - mbc);
+        const bool xss = fx >= 0 && s_ss[fx] >= 0, yss = fy >= 0 && s_ss[fy] >= 0;
+        const int first = (!xss && yss) ? 1 : 0;               // a samesize y face goes before an f2c x face
+        double* qq = q + (size_t)p * nxy * meqn + (size_t)m * nxy + jc * nx + ic;
+        double v = 0.0;
+        bool touched = false;
+        for (int u = 0; u < 2; u++) {
+            const int s = sl[u ^ first];
+            if (s < 0 || !s_has[s]) continue;
             if (!touched) { v = *qq; touched = true; }
-            v = v + corr;
+            v = v + s_corr[s];
         }
         if (touched) *qq = v;
     }
@@ -598,7 +624,8 @@ void launch_sync(const Dims& d, double* q, const double* regs, const PatchDesc* 
                  const int* op_start, int nblocks, cudaStream_t st)
 {
     if (nblocks > 0)
-        launch_k(k_sync, nblocks, 192, 0, st, q, regs, desc, ops, op_start, d.mx, d.my, d.mbc, d.meqn, d.nreg());
+        launch_k(k_sync, nblocks, 192, (size_t)4 * d.meqn * (d.mx > d.my ? d.mx : d.my) * (sizeof(double) + 1), st,
+                 q, regs, desc, ops, op_start, d.mx, d.my, d.mbc, d.meqn, d.nreg());
 }
 void launch_reset(const Dims& d, double* regs, const PatchDesc* desc, int p0, int np, int coarse_level, int mode,
                   cudaStream_t st)
