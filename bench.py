@@ -753,6 +753,30 @@ def run_batch(args, wl, rank, world, local_rank):
     return 0
 
 
+def launch_profile(args, wl):
+    """The workload after its spin-up, then args.steps untimed coarse steps (graph replay):
+    the launches of the last step are the last entries of an ncu launch list of this run."""
+    import forestclaw_b200 as fb
+    if wl.get("batch"):
+        raise SystemExit("--launch-profile covers single-forest workloads")
+    prob, gc = _options(wl, args.precision)
+    g = fb.Solver(gc)
+    g.initialize()
+    t, dt, _ = _spinup(g, wl, 0.0, _initial_dt(wl, prob), wl["spinup"])
+    for _ in range(args.steps):
+        c = g.advance(t, dt)
+        t += dt
+        if wl.get("adapt_dt", wl["time_sync"]):
+            dt *= 0.9 / c
+    g.synchronize()
+    lev = g.patch_info()[:, 0]
+    print(json.dumps({"launch_profile": wl["name"], "steps": args.steps,
+                      "patches_per_level": {str(int(l)): int((lev == l).sum()) for l in sorted(set(lev.tolist()))},
+                      "last_step": g.last_update_stats()}), flush=True)
+    g.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -769,6 +793,9 @@ def main():
                     help="Euler: Newton start of the exact solver (mlp: trained on the FP64 run first)")
     ap.add_argument("--mlp-samples", type=int, default=1_000_000)
     ap.add_argument("--mlp-epochs", type=int, default=20)
+    ap.add_argument("--launch-profile", action="store_true",
+                    help="profiling aid, no timing: spin up the workload, run --steps coarse steps, print the "
+                         "patches per level and the launches of the last step (for an ncu launch list)")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -776,6 +803,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, wl, rank, world)
+    if args.launch_profile:
+        return launch_profile(args, wl)
     if world > 1:
         import datetime
         import torch
