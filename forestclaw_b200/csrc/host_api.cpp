@@ -116,6 +116,10 @@ struct fc2d_b200_solver {
     // an update, likewise share one launch (each level with its own alpha)
     struct PendingTimeInterp { bool active = false; int lev_lo = 0, lev_hi = 0; LevelAlpha alpha{}; };
     PendingTimeInterp pend_ti;
+    // interp_chain[l]: no cell the interpolation into level l+1 reads (level-l cells
+    // and their stencil neighbours) is written by the interpolation into level l, so
+    // the two (issued finer first) may share a launch; computed per forest
+    unsigned char interp_chain[34] = {};
     StepParams* tune_params = nullptr;             // autotuner: dt = 0 parameters (device)
     DevVec<RepopOp> repop_dev;                     // regrid repopulation ops
     DevVec<double> snap;                           // batch regrid: q of instances whose forest is unchanged
@@ -294,6 +298,24 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
     CK(s->t_copy.assign(copy, s->st));
     CK(s->t_avg.assign(avg, s->st));
     CK(s->t_interp.assign(interp, s->st));
+    {   // interpolation chains: reads of level l's entries against writes of level l-1's
+        std::vector<unsigned char> written((size_t)f.np() * s->d.nq(), 0);
+        const int nx = s->d.nx();
+        for (int l = 0; l < 34; l++) s->interp_chain[l] = 0;
+        for (int l = 1; l <= 32; l++) {
+            const LevelRanges& lo = s->lr[l - 1];
+            const LevelRanges& hi = s->lr[l];
+            for (int k = 0; k < lo.interp_n; k++) written[interp[lo.interp_off + k].dst] = 1;
+            bool clash = false;
+            for (int k = 0; k < hi.interp_n && !clash; k++) {
+                const long c = interp[hi.interp_off + k].src;
+                for (long o : {0L, -1L, 1L, (long)-nx, (long)nx})
+                    if (c + o >= 0 && c + o < (long)written.size() && written[c + o]) { clash = true; break; }
+            }
+            for (int k = 0; k < lo.interp_n; k++) written[interp[lo.interp_off + k].dst] = 0;
+            s->interp_chain[l] = clash ? 0 : 1;
+        }
+    }
     CK(s->t_phys.assign(phys, s->st));
     CK(s->t_ti.assign(ti, s->st));
     CK(s->t_sync.assign(sync, s->st));
@@ -497,13 +519,41 @@ static void phys_range(fc2d_b200_solver* s, int a, int b, int c)
     if (s->fill) s->total_launches++;
     if (s->emit) launch_phys(s->d, s0, s1, s->bc_dev, s->st);
 }
-static void interpolate2ghost(fc2d_b200_solver* s, int l, int ti)
+// clawpack46 interpolate2ghost of levels hi, hi-1, ..., lo on q (finer levels first,
+// one launch when each is chained to the next, interp_chain) and, when c >= 0 and
+// chained too, of level c from the time-interpolated copy in the same launch.
+// Returns whether level c went out.
+static bool interp_run(fc2d_b200_solver* s, int lo, int hi, int c)
 {
-    if (l < 0 || l > 32 || !s->lr[l].interp_n) return;
+    GatherSeg<InterpEnt> s0{nullptr, nullptr, nullptr, 0}, s1 = s0;
+    if (lo < 0) lo = 0;
+    if (hi > 32) hi = 32;
+    if (lo <= hi) {
+        const int off = s->lr[lo].interp_off, n = s->lr[hi].interp_off + s->lr[hi].interp_n - off;
+        if (n > 0) s0 = seg(s->t_interp.p, off, n, s->q, s->q);
+    }
+    if (c >= 0 && c <= 32 && s->lr[c].interp_n > 0)
+        s1 = seg(s->t_interp.p, s->lr[c].interp_off, s->lr[c].interp_n, s->q, s->qinterp);
+    if (s0.n + s1.n <= 0) return c >= 0;
     (void)flush_pending(s);
     if (s->fill) s->total_launches++;
-    if (s->emit)
-        launch_interp(s->d, s->q, tsdata(s, ti), s->t_interp.p + s->lr[l].interp_off, s->lr[l].interp_n, s->st);
+    if (s->emit) launch_interp(s->d, s0, s1, s->st);
+    return c >= 0;
+}
+
+static void interpolate_levels(fc2d_b200_solver* s, int mincoarse, int maxcoarse, int time_interp)
+{
+    const int c = time_interp ? mincoarse - 1 : -1;
+    bool c_done = c < 0;
+    int l = std::min(maxcoarse, 32);
+    while (l >= mincoarse && l >= 0) {
+        int lo = l;
+        while (lo - 1 >= mincoarse && lo - 1 >= 0 && s->interp_chain[lo]) lo--;
+        const bool with_c = !c_done && lo == mincoarse && c >= 0 && c <= 32 && s->interp_chain[mincoarse];
+        if (interp_run(s, lo, l, with_c ? c : -1)) c_done = true;
+        l = lo - 1;
+    }
+    if (!c_done) interp_run(s, 0, -1, c);
 }
 
 static void ghost_update(fc2d_b200_solver* s, int minlevel, int maxlevel, int time_interp)
@@ -515,8 +565,7 @@ static void ghost_update(fc2d_b200_solver* s, int minlevel, int maxlevel, int ti
     average_range(s, mincoarse, maxcoarse, ti);
     copy_range(s, minlevel, maxlevel, ti);
     phys_range(s, mincoarse, maxcoarse, ti);
-    for (int l = maxcoarse; l >= mincoarse; l--) interpolate2ghost(s, l, 0);
-    if (time_interp) interpolate2ghost(s, mincoarse - 1, 1);
+    interpolate_levels(s, mincoarse, maxcoarse, time_interp);
     const int minfine = mincoarse + 1, maxfine = maxlevel;
     phys_range(s, minfine, maxfine, ti);
     phys_range(s, minlevel, maxlevel, ti);

@@ -97,14 +97,18 @@ __device__ __forceinline__ double compute_slopes(double sl, double sr)
     return mn * (s > 0.0 ? s : 0.0) * copysign(1.0, sc);
 }
 
-__global__ void k_interp(double* __restrict__ dst, const double* __restrict__ src, const InterpEnt* __restrict__ e,
-                         int n, int nx, int nxy, int meqn)
+__global__ void k_interp(GatherSeg<InterpEnt> s0, GatherSeg<InterpEnt> s1, int nx, int nxy, int meqn)
 {
     grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
     int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    InterpEnt c = e[t];
+    const bool one = t >= s0.n;
+    if (one) t -= s0.n;
+    const GatherSeg<InterpEnt>& g = one ? s1 : s0;
+    if (t >= g.n) return;
+    double* __restrict__ dst = g.dst;
+    const double* __restrict__ src = g.src;
+    InterpEnt c = g.e[t];
     const double shx = (c.sub & 1) ? 0.25 : -0.25;
     const double shy = (c.sub & 2) ? 0.25 : -0.25;
     for (int m = 0; m < meqn; m++) {
@@ -604,9 +608,10 @@ void launch_average(const Dims& d, const GatherSeg<AvgEnt>& s0, const GatherSeg<
     const long n = (long)s0.n + s1.n;
     if (n > 0) launch_k(k_average, nblk(n, 256), 256, 0, st, s0, s1, d.nq(), d.nx(), d.nxy(), d.meqn, area);
 }
-void launch_interp(const Dims& d, double* dst, const double* src, const InterpEnt* e, int n, cudaStream_t st)
+void launch_interp(const Dims& d, const GatherSeg<InterpEnt>& s0, const GatherSeg<InterpEnt>& s1, cudaStream_t st)
 {
-    if (n > 0) launch_k(k_interp, nblk(n, 256), 256, 0, st, dst, src, e, n, d.nx(), d.nxy(), d.meqn);
+    const long n = (long)s0.n + s1.n;
+    if (n > 0) launch_k(k_interp, nblk(n, 256), 256, 0, st, s0, s1, d.nx(), d.nxy(), d.meqn);
 }
 void launch_phys(const Dims& d, const GatherSeg<PhysEnt>& s0, const GatherSeg<PhysEnt>& s1, const double* bcstate,
                  cudaStream_t st)

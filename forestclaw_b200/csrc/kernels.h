@@ -71,7 +71,7 @@ void launch_restore_patches(const Dims& d, double* dst, const double* src, const
 // average of a manifold, or null for the plain mean.
 void launch_average(const Dims& d, const GatherSeg<AvgEnt>& s0, const GatherSeg<AvgEnt>& s1, const double* area,
                     cudaStream_t st);
-void launch_interp(const Dims& d, double* dst, const double* src, const InterpEnt* e, int n, cudaStream_t st);
+void launch_interp(const Dims& d, const GatherSeg<InterpEnt>& s0, const GatherSeg<InterpEnt>& s1, cudaStream_t st);
 void launch_phys(const Dims& d, const GatherSeg<PhysEnt>& s0, const GatherSeg<PhysEnt>& s1, const double* bcstate,
                  cudaStream_t st);
 // time interpolation factor of each level (levels 0..31) for a launch over the
