@@ -28,18 +28,32 @@ static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 // The gather kernels take up to two table segments, each with its own arrays:
 // a ghost-fill stage on q and the same stage on the time-interpolated copy
 // write different arrays and read cells the other does not write, so they
-// share a launch (segment 0 first in the thread numbering).
+// share a launch.  One thread per (entry, field): segment 0's threads first,
+// field-major within a segment, so a warp handles consecutive entries of one
+// field.  The fields of an entry are independent (same arithmetic per field).
+template <class E>
+__device__ __forceinline__ bool gather_item(const GatherSeg<E>& s0, const GatherSeg<E>& s1, int meqn,
+                                            const GatherSeg<E>*& g, int& e, int& m)
+{
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long n0 = (long)s0.n * meqn;
+    g = &s0;
+    if (t >= n0) { t -= n0; g = &s1; }
+    if (t >= (long)g->n * meqn) return false;
+    m = (int)(t / g->n);
+    e = (int)(t - (long)m * g->n);
+    return true;
+}
+
 __global__ void k_copy(GatherSeg<CopyEnt> s0, GatherSeg<CopyEnt> s1, int nxy, int meqn)
 {
     grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool one = t >= s0.n;
-    if (one) t -= s0.n;
-    const GatherSeg<CopyEnt>& g = one ? s1 : s0;
-    if (t >= g.n) return;
-    CopyEnt c = g.e[t];
-    for (int m = 0; m < meqn; m++) g.dst[c.dst + m * nxy] = g.src[c.src + m * nxy];
+    const GatherSeg<CopyEnt>* g;
+    int e, m;
+    if (!gather_item(s0, s1, meqn, g, e, m)) return;
+    const CopyEnt c = g->e[e];
+    g->dst[c.dst + m * nxy] = g->src[c.src + m * nxy];
 }
 
 __global__ void k_average(GatherSeg<AvgEnt> s0, GatherSeg<AvgEnt> s1, int nq, int nx, int nxy, int meqn,
@@ -47,14 +61,12 @@ __global__ void k_average(GatherSeg<AvgEnt> s0, GatherSeg<AvgEnt> s1, int nq, in
 {
     grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool one = t >= s0.n;
-    if (one) t -= s0.n;
-    const GatherSeg<AvgEnt>& g = one ? s1 : s0;
-    if (t >= g.n) return;
-    double* __restrict__ dst = g.dst;
-    const double* __restrict__ src = g.src;
-    AvgEnt c = g.e[t];
+    const GatherSeg<AvgEnt>* g;
+    int e, m;
+    if (!gather_item(s0, s1, meqn, g, e, m)) return;
+    double* __restrict__ dst = g->dst;
+    const double* __restrict__ src = g->src;
+    const AvgEnt c = g->e[e];
     const int o1 = c.sx, o2 = c.sy, o3 = c.sx + c.sy;
     if (area) {
         // manifold (fclaw2d_clawpatch46_average.f:96-115): sum(q_f a_f) / sum(a_f); the
@@ -64,26 +76,22 @@ __global__ void k_average(GatherSeg<AvgEnt> s0, GatherSeg<AvgEnt> s1, int nq, in
         const double* ap = area + (size_t)p * na;
         auto ai = [&](int off) { const int cc = c.src - p * nq + off; return (cc / nx + 1) * (nx + 2) + cc % nx + 1; };
         const double a0 = ap[ai(0)], a1 = ap[ai(o1)], a2 = ap[ai(o2)], a3 = ap[ai(o3)];
-        for (int m = 0; m < meqn; m++) {
-            const double* f = src + c.src + m * nxy;
-            double sum = 0.0, af = 0.0;
-            sum = sum + f[0] * a0;  af = af + a0;
-            sum = sum + f[o1] * a1; af = af + a1;
-            sum = sum + f[o2] * a2; af = af + a2;
-            sum = sum + f[o3] * a3; af = af + a3;
-            dst[c.dst + m * nxy] = sum / af;
-        }
+        const double* f = src + c.src + m * nxy;
+        double sum = 0.0, af = 0.0;
+        sum = sum + f[0] * a0;  af = af + a0;
+        sum = sum + f[o1] * a1; af = af + a1;
+        sum = sum + f[o2] * a2; af = af + a2;
+        sum = sum + f[o3] * a3; af = af + a3;
+        dst[c.dst + m * nxy] = sum / af;
         return;
     }
-    for (int m = 0; m < meqn; m++) {
-        const double* f = src + c.src + m * nxy;
-        double sum = 0.0;
-        sum = sum + f[0];
-        sum = sum + f[o1];
-        sum = sum + f[o2];
-        sum = sum + f[o3];
-        dst[c.dst + m * nxy] = sum / 4.0;
-    }
+    const double* f = src + c.src + m * nxy;
+    double sum = 0.0;
+    sum = sum + f[0];
+    sum = sum + f[o1];
+    sum = sum + f[o2];
+    sum = sum + f[o3];
+    dst[c.dst + m * nxy] = sum / 4.0;
 }
 
 // AMRClaw limited slopes (fclaw2d_clawpatch_utils.f:52-55, mth = 5)
@@ -101,27 +109,23 @@ __global__ void k_interp(GatherSeg<InterpEnt> s0, GatherSeg<InterpEnt> s1, int n
 {
     grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool one = t >= s0.n;
-    if (one) t -= s0.n;
-    const GatherSeg<InterpEnt>& g = one ? s1 : s0;
-    if (t >= g.n) return;
-    double* __restrict__ dst = g.dst;
-    const double* __restrict__ src = g.src;
-    InterpEnt c = g.e[t];
+    const GatherSeg<InterpEnt>* g;
+    int e, m;
+    if (!gather_item(s0, s1, meqn, g, e, m)) return;
+    double* __restrict__ dst = g->dst;
+    const double* __restrict__ src = g->src;
+    const InterpEnt c = g->e[e];
     const double shx = (c.sub & 1) ? 0.25 : -0.25;
     const double shy = (c.sub & 2) ? 0.25 : -0.25;
-    for (int m = 0; m < meqn; m++) {
-        const double* qc = src + c.src + m * nxy;
-        double q0 = qc[0];
-        double sl = (q0 - qc[-1]);
-        double sr = (qc[1] - q0);
-        double gradx = compute_slopes(sl, sr);
-        sl = (q0 - qc[-nx]);
-        sr = (qc[nx] - q0);
-        double grady = compute_slopes(sl, sr);
-        dst[c.dst + m * nxy] = q0 + gradx * shx + grady * shy;
-    }
+    const double* qc = src + c.src + m * nxy;
+    double q0 = qc[0];
+    double sl = (q0 - qc[-1]);
+    double sr = (qc[1] - q0);
+    double gradx = compute_slopes(sl, sr);
+    sl = (q0 - qc[-nx]);
+    sr = (qc[nx] - q0);
+    double grady = compute_slopes(sl, sr);
+    dst[c.dst + m * nxy] = q0 + gradx * shx + grady * shy;
 }
 
 __global__ void k_phys(GatherSeg<PhysEnt> s0, GatherSeg<PhysEnt> s1, int nxy, int meqn,
@@ -129,17 +133,13 @@ __global__ void k_phys(GatherSeg<PhysEnt> s0, GatherSeg<PhysEnt> s1, int nxy, in
 {
     grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool one = t >= s0.n;
-    if (one) t -= s0.n;
-    const GatherSeg<PhysEnt>& g = one ? s1 : s0;
-    if (t >= g.n) return;
-    double* __restrict__ q = g.dst;                 // in place: sources are cells of the same array
-    PhysEnt c = g.e[t];
-    for (int m = 0; m < meqn; m++) {
-        double v = c.cst ? bcstate[m] : q[c.src + m * nxy];
-        q[c.dst + m * nxy] = ((c.neg >> m) & 1) ? -v : v;
-    }
+    const GatherSeg<PhysEnt>* g;
+    int e, m;
+    if (!gather_item(s0, s1, meqn, g, e, m)) return;
+    double* __restrict__ q = g->dst;                // in place: sources are cells of the same array
+    const PhysEnt c = g->e[e];
+    const double v = c.cst ? bcstate[m] : q[c.src + m * nxy];
+    q[c.dst + m * nxy] = ((c.neg >> m) & 1) ? -v : v;
 }
 
 // Band of width mbc inside the patch, in the four loops of timeinterp.f:33-70.
@@ -599,24 +599,24 @@ void launch_restore_patches(const Dims& d, double* dst, const double* src, const
 
 void launch_copy(const Dims& d, const GatherSeg<CopyEnt>& s0, const GatherSeg<CopyEnt>& s1, cudaStream_t st)
 {
-    const long n = (long)s0.n + s1.n;
+    const long n = ((long)s0.n + s1.n) * d.meqn;
     if (n > 0) launch_k(k_copy, nblk(n, 256), 256, 0, st, s0, s1, d.nxy(), d.meqn);
 }
 void launch_average(const Dims& d, const GatherSeg<AvgEnt>& s0, const GatherSeg<AvgEnt>& s1, const double* area,
                     cudaStream_t st)
 {
-    const long n = (long)s0.n + s1.n;
+    const long n = ((long)s0.n + s1.n) * d.meqn;
     if (n > 0) launch_k(k_average, nblk(n, 256), 256, 0, st, s0, s1, d.nq(), d.nx(), d.nxy(), d.meqn, area);
 }
 void launch_interp(const Dims& d, const GatherSeg<InterpEnt>& s0, const GatherSeg<InterpEnt>& s1, cudaStream_t st)
 {
-    const long n = (long)s0.n + s1.n;
+    const long n = ((long)s0.n + s1.n) * d.meqn;
     if (n > 0) launch_k(k_interp, nblk(n, 256), 256, 0, st, s0, s1, d.nx(), d.nxy(), d.meqn);
 }
 void launch_phys(const Dims& d, const GatherSeg<PhysEnt>& s0, const GatherSeg<PhysEnt>& s1, const double* bcstate,
                  cudaStream_t st)
 {
-    const long n = (long)s0.n + s1.n;
+    const long n = ((long)s0.n + s1.n) * d.meqn;
     if (n > 0) launch_k(k_phys, nblk(n, 256), 256, 0, st, s0, s1, d.nxy(), d.meqn, bcstate);
 }
 void launch_timeinterp(const Dims& d, const double* q, const double* qlast, double* qinterp, const int* patches,
