@@ -198,9 +198,11 @@ struct RegOff {
 //             clawpack46_time_sync.f:254-498: the fine pair d, d+1 (d = 1 + n_off + 2 j)
 //             of coarse cell j, skipped when outside the fine face; q += deltac / area
 // Dynamic shared memory: 4 * meqn * max(mx, my) doubles and as many flag bytes.
-__global__ void k_sync(double* __restrict__ q, const double* __restrict__ regs, const PatchDesc* __restrict__ desc,
-                       const SyncOp* __restrict__ ops, const int* __restrict__ op_start,
-                       int mx, int my, int mbc, int meqn, int nreg)
+// 128 threads and at most 40 registers: 12 CTAs per SM, so a sync of up to ~1800
+// patches with corrections runs in one wave.
+__global__ void __launch_bounds__(128, 12)
+k_sync(double* __restrict__ q, const double* __restrict__ regs, const PatchDesc* __restrict__ desc,
+       const SyncOp* __restrict__ ops, const int* __restrict__ op_start, int mx, int my, int mbc, int meqn, int nreg)
 {
     grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
@@ -629,7 +631,7 @@ void launch_sync(const Dims& d, double* q, const double* regs, const PatchDesc* 
                  const int* op_start, int nblocks, cudaStream_t st)
 {
     if (nblocks > 0)
-        launch_k(k_sync, nblocks, 192, (size_t)4 * d.meqn * (d.mx > d.my ? d.mx : d.my) * (sizeof(double) + 1), st,
+        launch_k(k_sync, nblocks, 128, (size_t)4 * d.meqn * (d.mx > d.my ? d.mx : d.my) * (sizeof(double) + 1), st,
                  q, regs, desc, ops, op_start, d.mx, d.my, d.mbc, d.meqn, d.nreg());
 }
 void launch_reset(const Dims& d, double* regs, const PatchDesc* desc, int p0, int np, int coarse_level, int mode,
