@@ -32,6 +32,14 @@ enum { MLP_BLOB_F_B1 = 0, MLP_BLOB_F_B2 = 64, MLP_BLOB_F_W3 = 128, MLP_BLOB_F_B3
 
 // Parameters of one level update launch (clawpack46 method flags and the
 // per-step scalars the reference passes through common blocks).
+// The levels of one update launch: nlev consecutive levels (1: every patch takes
+// the first parameter block), start[k] = first patch of the k-th level (ascending)
+// relative to the launch's first patch.
+struct LevelGroup {
+    int nlev;
+    int start[34];
+};
+
 struct StepParams {
     int order1, order2;     // method(2), method(3)
     int mthlim[8];

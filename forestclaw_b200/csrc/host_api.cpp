@@ -402,9 +402,11 @@ static int flush_updates(fc2d_b200_solver* s)
     if (!s->emit) return 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (s->timing) { e0 = next_event(s); e1 = next_event(s); CK(cudaEventRecord(e0, s->st)); }
-    const int lev_hi = g.lev_hi > g.lev_lo ? g.lev_hi : -1;
+    LevelGroup lg{};
+    lg.nlev = g.lev_hi - g.lev_lo + 1;
+    for (int i = 0; i < lg.nlev; i++) lg.start[i] = s->forest.lev_off[g.lev_lo + i] - g.p0;
     cudaError_t e = s->vars[g.var]->fn(s->q, s->qlast, s->aux, s->regs, s->desc, g.p0, g.np, s->params_dev + g.slot,
-                                       lev_hi, s->cfl_dev, s->st);
+                                       lg, s->cfl_dev, s->st);
     if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("step2 launch: ") + cudaGetErrorString(e));
     if (s->timing) {
         CK(cudaEventRecord(e1, s->st));
@@ -708,7 +710,7 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
         s->vars = step2_variants(o.precision, o.rp, o.mx, o.my, o.mbc);
         s->var = 0;
         for (int l = 0; l < 33; l++) s->var_lev[l] = -1;
-        cudaError_t e = s->vars[0]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, -1, nullptr, s->st);
+        cudaError_t e = s->vars[0]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, LevelGroup{1, {0}}, nullptr, s->st);
         if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
         CK(cudaMalloc(&s->tune_params, sizeof(StepParams)));
     }
@@ -748,7 +750,7 @@ extern "C" int fc2d_b200_set_riemann(fc2d_b200_solver_t* s, int rp_id)
     s->var = 0;
     for (int l = 0; l < 33; l++) s->var_lev[l] = -1;
     invalidate_graph(s);
-    cudaError_t e = s->vars[0]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, -1, nullptr, s->st);
+    cudaError_t e = s->vars[0]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, LevelGroup{1, {0}}, nullptr, s->st);
     if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
     return 0;
 }
@@ -1869,7 +1871,7 @@ extern "C" int fc2d_b200_variant_info(const fc2d_b200_solver_t* s, int v, int* t
 extern "C" int fc2d_b200_set_variant(fc2d_b200_solver_t* s, int v)
 {
     if (!s || v < 0 || v >= (int)s->vars.size()) return fail(FC2D_B200_EINVAL, "no such variant");
-    cudaError_t e = s->vars[v]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, -1, nullptr, s->st);
+    cudaError_t e = s->vars[v]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, LevelGroup{1, {0}}, nullptr, s->st);
     if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
     s->var = v;
     for (int l = 0; l < 33; l++) s->var_lev[l] = -1;
@@ -1896,7 +1898,7 @@ extern "C" int fc2d_b200_autotune(fc2d_b200_solver_t* s, int reps, int* best_out
         for (int l = 0; l <= 32; l++) {
             const int p0 = f.lev_off[l], np = f.lev_off[l + 1] - p0;
             if (np <= 0) continue;
-            cudaError_t e = v->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, s->tune_params, -1, s->cfl_dev, s->st);
+            cudaError_t e = v->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, s->tune_params, LevelGroup{1, {0}}, s->cfl_dev, s->st);
             if (e != cudaSuccess) return e;
         }
         return cudaSuccess;
@@ -1905,7 +1907,7 @@ extern "C" int fc2d_b200_autotune(fc2d_b200_solver_t* s, int reps, int* best_out
     double best_ms = 1e300;
     cudaError_t err = cudaSuccess;
     for (int v = 0; v < (int)s->vars.size() && err == cudaSuccess; v++) {
-        err = s->vars[v]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, -1, nullptr, s->st);
+        err = s->vars[v]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, LevelGroup{1, {0}}, nullptr, s->st);
         if (err == cudaSuccess) err = pass(s->vars[v]);             // warm-up
         if (err == cudaSuccess) err = cudaEventRecord(e0, s->st);
         for (int r = 0; r < reps && err == cudaSuccess; r++) err = pass(s->vars[v]);
@@ -1927,10 +1929,10 @@ extern "C" int fc2d_b200_autotune(fc2d_b200_solver_t* s, int reps, int* best_out
         double lbest = 1e300;
         for (int v = 0; v < (int)s->vars.size() && err == cudaSuccess; v++) {
             const Step2Variant* x = s->vars[v];
-            err = x->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, s->tune_params, -1, s->cfl_dev, s->st);
+            err = x->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, s->tune_params, LevelGroup{1, {0}}, s->cfl_dev, s->st);
             if (err == cudaSuccess) err = cudaEventRecord(e0, s->st);
             for (int r = 0; r < reps && err == cudaSuccess; r++)
-                err = x->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, s->tune_params, -1, s->cfl_dev, s->st);
+                err = x->fn(s->q, s->qlast, s->aux, s->regs, s->desc, p0, np, s->tune_params, LevelGroup{1, {0}}, s->cfl_dev, s->st);
             if (err == cudaSuccess) err = cudaEventRecord(e1, s->st);
             if (err == cudaSuccess) err = cudaEventSynchronize(e1);
             float ms = 0.0f;

@@ -678,11 +678,19 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
 // The fused update of npatch patches starting at slot p0.  One CTA per patch, or
 // (PERSIST) a grid of a few CTAs per SM, each taking patches p0 + blockIdx.x,
 // + gridDim.x, ... in turn, its shared memory reused patch after patch.
+// Parameter block of relative patch b of a launch over lg.nlev levels.
+__device__ __forceinline__ int group_slot(const LevelGroup& lg, int b)
+{
+    int k = 0;
+    for (int i = 1; i < lg.nlev; i++) k += (b >= lg.start[i]) ? 1 : 0;
+    return lg.nlev - 1 - k;
+}
+
 template <class RP, int MX, int MY, int MBC, bool FWAVE, int NT, typename TW, int MINB = 2, bool PERSIST = false>
 __global__ void __launch_bounds__(NT, MINB)
 step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* __restrict__ aux,
              double* __restrict__ regs, const PatchDesc* __restrict__ desc, int p0, int npatch,
-             const StepParams* __restrict__ spp, int lev_hi, unsigned long long* __restrict__ cfl_bits)
+             const StepParams* __restrict__ spp, const LevelGroup lg, unsigned long long* __restrict__ cfl_bits)
 {
     grid_dependency_wait();         // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
@@ -692,12 +700,12 @@ step2_kernel(double* __restrict__ q, double* __restrict__ qlast, const double* _
     if constexpr (!PERSIST) {
         (void)npatch;
         const int p = p0 + (int)blockIdx.x;
-        const StepParams sp = spp[lev_hi < 0 ? 0 : lev_hi - desc[p].level];
+        const StepParams sp = spp[group_slot(lg, (int)blockIdx.x)];
         step2_patch<RP, MX, MY, MBC, FWAVE, NT, TW>(q, qlast, aux, regs, desc, p, sp, cfl_bits, nhist);
     } else {
         for (int b = blockIdx.x; b < npatch; b += gridDim.x) {
             const int p = p0 + b;
-            const StepParams sp = spp[lev_hi < 0 ? 0 : lev_hi - desc[p].level];
+            const StepParams sp = spp[group_slot(lg, b)];
             step2_patch<RP, MX, MY, MBC, FWAVE, NT, TW>(q, qlast, aux, regs, desc, p, sp, cfl_bits, nhist);
             __syncthreads();   // the next patch restages the shared memory
         }

@@ -17,7 +17,8 @@ namespace fcb {
 
 template <class RP, int MX, int MBC, bool FW, int NT, int MINB, typename TW, bool PERSIST = false>
 cudaError_t run_step2_variant(double* q, double* qlast, const double* aux, double* regs, const PatchDesc* desc,
-                              int p0, int npatch, const StepParams* sp, int lev_hi, unsigned long long* cfl_bits,
+                              int p0, int npatch, const StepParams* sp, const LevelGroup& lg,
+                              unsigned long long* cfl_bits,
                               cudaStream_t st)
 {
     using G = Step2Geom<RP, MX, MX, MBC, TW, NT>;
@@ -39,7 +40,7 @@ cudaError_t run_step2_variant(double* q, double* qlast, const double* aux, doubl
     }
     if (npatch <= 0) return cudaSuccess;
     const int grid = PERSIST ? (npatch < grid_cap ? npatch : grid_cap) : npatch;
-    return launch_k(kern, grid, NT, G::SMEM_BYTES, st, q, qlast, aux, regs, desc, p0, npatch, sp, lev_hi, cfl_bits);
+    return launch_k(kern, grid, NT, G::SMEM_BYTES, st, q, qlast, aux, regs, desc, p0, npatch, sp, lg, cfl_bits);
 }
 
 // One table entry: precision, solver id, square patch size MXV (mbc 2), threads, min CTAs per SM.

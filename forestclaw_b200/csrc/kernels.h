@@ -32,11 +32,14 @@ struct Dims {
 // ---- fused update (k_step2_<precision>_<family>.cu) ---------------------------
 // Each unit holds a table of launchers, one per (solver, patch size, patch-to-CTA
 // mapping); the first entry of a shape is its default.  A launcher called with
-// npatch = 0 only sets the kernel's shared-memory attribute.  lev_hi < 0: every
-// patch takes sp[0]; else the launch covers consecutive levels ..lev_hi and a
-// patch of level L takes sp[lev_hi - L].
+// npatch = 0 only sets the kernel's shared-memory attribute.  A launch covers
+// lg.nlev consecutive levels; the patches of its k-th level (ascending, from
+// relative patch lg.start[k]) take sp[lg.nlev - 1 - k] (the parameter blocks are
+// in issue order, finest level first).  The split is a kernel argument, so no
+// patch reads memory to find its parameters.
 typedef cudaError_t (*Step2Fn)(double* q, double* qlast, const double* aux, double* regs, const PatchDesc* desc,
-                               int p0, int npatch, const StepParams* sp, int lev_hi, unsigned long long* cfl_bits,
+                               int p0, int npatch, const StepParams* sp, const LevelGroup& lg,
+                               unsigned long long* cfl_bits,
                                cudaStream_t st);
 struct Step2Variant {
     int precision, rp, mx, my, mbc;
