@@ -23,6 +23,8 @@ LIB_PATH = os.path.join(_HERE, "libfc2d_b200.so")
 RP_ADVECTION, RP_SW_ROE, RP_SW_FWAVE, RP_EULER_EXACT, RP_ADVECTION_MANIFOLD = 0, 1, 2, 3, 4
 APP_NONE, APP_SWIRL, APP_RADIALDAM, APP_TSUNAMI, APP_SHOCKBUBBLE, APP_SPHERE = 0, 1, 2, 3, 4, 5
 PREC_FP64, PREC_FP32WAVE = 0, 1
+# refinement criteria: FCLAW_REFINE_CRITERIA_* + 1; TAG_APP = the app's built-in one
+TAG_APP, TAG_VALUE, TAG_DIFFERENCE, TAG_MINMAX, TAG_GRADIENT, TAG_GRADIENT_DX = 0, 1, 2, 3, 4, 5
 
 
 class B200Error(RuntimeError):
@@ -50,7 +52,19 @@ class _Options(ctypes.Structure):
         ("gamma", ctypes.c_double), ("mach", ctypes.c_double), ("rhob", ctypes.c_double),
         ("newton_tol", ctypes.c_double),
         ("precision", ctypes.c_int), ("device", ctypes.c_int),
+        ("smooth_refine", ctypes.c_int), ("smooth_level", ctypes.c_int),
+        ("refinement_criteria", ctypes.c_int), ("threshold_variable", ctypes.c_int),
+        ("qinit_cellave", ctypes.c_int),
+        ("regrid_interval", ctypes.c_int), ("nout", ctypes.c_int), ("use_fixed_dt", ctypes.c_int),
+        ("tfinal", ctypes.c_double), ("initial_dt", ctypes.c_double), ("max_cfl", ctypes.c_double),
+        ("desired_cfl", ctypes.c_double),
     ]
+
+
+class _RunStats(ctypes.Structure):
+    _fields_ = [("count_amr_advance", ctypes.c_int), ("count_amr_regrid", ctypes.c_int),
+                ("count_amr_new_domain", ctypes.c_int), ("global_num_patches", ctypes.c_int),
+                ("rejected", ctypes.c_int), ("steps", ctypes.c_int), ("t_final", ctypes.c_double)]
 
 
 class _Instance(ctypes.Structure):
@@ -108,6 +122,18 @@ class Options:
     newton_tol: float = 1e-10
     precision: int = PREC_FP64
     device: int = 0
+    smooth_refine: int = 0
+    smooth_level: int = 0
+    refinement_criteria: int = TAG_APP
+    threshold_variable: int = 1
+    qinit_cellave: int = 0
+    regrid_interval: int = 1
+    nout: int = 1
+    use_fixed_dt: int = 0
+    tfinal: float = 0.0
+    initial_dt: float = 0.0
+    max_cfl: float = 1.0
+    desired_cfl: float = 0.9
 
     def to_c(self) -> _Options:
         o = _Options()
@@ -115,7 +141,9 @@ class Options:
                   "maxlevel", "subcycle", "time_sync", "flux_correction", "fluctuation_correction",
                   "refine_threshold", "coarsen_threshold", "ax", "bx", "ay", "by", "mi", "mj", "app", "grav",
                   "tperiod", "r0", "hin", "hout", "x0", "y0", "gamma", "mach", "rhob", "newton_tol",
-                  "precision", "device"):
+                  "precision", "device", "smooth_refine", "smooth_level", "refinement_criteria",
+                  "threshold_variable", "qinit_cellave", "regrid_interval", "nout", "use_fixed_dt", "tfinal",
+                  "initial_dt", "max_cfl", "desired_cfl"):
             setattr(o, k, getattr(self, k))
         for i, v in enumerate(self.order):
             o.order[i] = v
@@ -163,6 +191,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_time_sync": [P, I, I],
         "fc2d_b200_advance": [P, D, D, dp],
         "fc2d_b200_regrid": [P, ip],
+        "fc2d_b200_save_step": [P],
+        "fc2d_b200_restore_step": [P],
+        "fc2d_b200_run": [P, ctypes.POINTER(_RunStats)],
         "fc2d_b200_mass": [P, dp],
         "fc2d_b200_cell_updates": [P, dp],
         "fc2d_b200_synchronize": [P],
@@ -472,6 +503,19 @@ class Solver:
         c = ctypes.c_int()
         self._check("fc2d_b200_regrid", self.lib.fc2d_b200_regrid(self.h, ctypes.byref(c)))
         return c.value
+
+    def save_step(self) -> None:
+        self._check("fc2d_b200_save_step", self.lib.fc2d_b200_save_step(self.h))
+
+    def restore_step(self) -> None:
+        self._check("fc2d_b200_restore_step", self.lib.fc2d_b200_restore_step(self.h))
+
+    def run(self) -> dict:
+        """fclaw2d_run outstyle 1 from t = 0 (tfinal, nout, initial_dt, max_cfl, desired_cfl,
+        regrid_interval of the options); returns the run's counters."""
+        st = _RunStats()
+        self._check("fc2d_b200_run", self.lib.fc2d_b200_run(self.h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in _RunStats._fields_}
 
     def mass(self) -> np.ndarray:
         out = np.zeros(self.opts.meqn, np.float64)

@@ -4,8 +4,10 @@
 //               The time-independent part of b4step2, psi(x,y+dy)-psi(x,y) and
 //               psi(x+dx,y)-psi(x,y), is stored as aux; the fused update kernel
 //               scales it by cos(2 pi (t+dt/2)/T)/dy and -cos(...)/dx each step.
-//   radial dam: applications/clawpack/shallow/2d/radialdam/user_4.6/qinit.f with the
-//               disc test at the cell centre.
+//   radial dam: applications/clawpack/shallow/2d/radialdam/user_4.6/qinit.f: the disc of
+//               fdisc.f by the cell-centre test, or (qinit_cellave) by the cell averages of
+//               src/fortran_source2d/cellave2.f: the area of the polygon of the cell's inside
+//               corners and its edge crossings, found by Brent's zeroin.
 //   tsunami:    bathymetry b = -1 + 0.5 exp(-50|x-c|^2) in aux(:,:,1), surface eta = sum of bumps.
 //   shock-bubble: applications/clawpack/euler/2d/shockbubble/user_4.6/qinit.f:24-62 (bubble by
 //               cell centre), inflow of user_4.6/bc2.f:53-60, post-shock state from the
@@ -19,8 +21,8 @@
 //               pdata: axis[0..2], omega[3], centre 1 [4..6], centre 2 [7..9], width [10],
 //               background [11].
 //   tagging:    fort_4.6/fclaw2d_clawpatch46_tag4refinement.f / _tag4coarsening.f with the
-//               gradient criterion (fort_user/fclaw2d_clawpatch_gradient_exceeds_th.f90) times dx;
-//               the sphere uses the minmax criterion (fclaw2d_clawpatch_minmax_exceeds_th.f90).
+//               criteria of fort_user/fclaw2d_clawpatch_{value,difference,minmax,gradient}_exceeds_th.f90;
+//               the apps' built-in choice is the gradient times dx, or minmax for the sphere.
 #include "apps.hpp"
 #include <cmath>
 #include "fcb_sphere.h"
@@ -52,6 +54,90 @@ static double sphere_angle(const double* x, const double* c)
     const double cx = x[1] * c[2] - x[2] * c[1], cy = x[2] * c[0] - x[0] * c[2], cz = x[0] * c[1] - x[1] * c[0];
     return std::atan2(std::sqrt(cx * cx + cy * cy + cz * cz), x[0] * c[0] + x[1] * c[1] + x[2] * c[2]);
 }
+
+// ---- cellave2 (src/fortran_source2d/cellave2.f) ----------------------------------
+namespace {
+struct Disc {
+    double x0, y0, r0;
+    double xc0 = 0, yc0 = 0, xc1 = 0, yc1 = 0;   // the edge being searched
+    // fdisc.f (unmapped): negative inside the disc
+    double f(double x, double y) const { return ((x - x0) * (x - x0) + (y - y0) * (y - y0)) - r0 * r0; }
+    // fss: f at fraction s along the current edge
+    double fs(double s) const { return f(xc0 + s * (xc1 - xc0), yc0 + s * (yc1 - yc0)); }
+};
+
+// Brent's root finder (R. Brent, Algorithms for Minimization without Derivatives, 1973,
+// procedure zero) in the netlib form of cellave2.f:120-250, whose short step to the
+// left is -xm rather than -tol1.
+double brent_zero(const Disc& D, double ax, double bx, double tol)
+{
+    double eps = 1.0, tol1;
+    do { eps = eps / 2.0; tol1 = 1.0 + eps; } while (tol1 > 1.0);
+    double a = ax, b = bx, fa = D.fs(a), fb = D.fs(b);
+    double c, fc, d, e, xm, p, q, r, sv;
+    for (;;) {
+        c = a; fc = fa; d = b - a; e = d;
+        for (;;) {
+            if (!(std::fabs(fc) >= std::fabs(fb))) { a = b; b = c; c = a; fa = fb; fb = fc; fc = fa; }
+            tol1 = 2.0 * eps * std::fabs(b) + 0.5 * tol;
+            xm = 0.5 * (c - b);
+            if (std::fabs(xm) <= tol1 || fb == 0.0) return b;
+            bool bisect = std::fabs(e) < tol1 || std::fabs(fa) <= std::fabs(fb);
+            if (!bisect) {
+                if (a == c) { sv = fb / fa; p = 2.0 * xm * sv; q = 1.0 - sv; }
+                else {
+                    q = fa / fc; r = fb / fc; sv = fb / fa;
+                    p = sv * (2.0 * xm * q * (q - r) - (b - a) * (r - 1.0));
+                    q = (q - 1.0) * (r - 1.0) * (sv - 1.0);
+                }
+                if (p > 0.0) q = -q;
+                p = std::fabs(p);
+                if ((2.0 * p) >= (3.0 * xm * q - std::fabs(tol1 * q)) || p >= std::fabs(0.5 * e * q)) bisect = true;
+                else { e = d; d = p / q; }
+            }
+            if (bisect) { d = xm; e = d; }
+            a = b; fa = fb;
+            if (std::fabs(d) > tol1) b = b + d;
+            if (std::fabs(d) <= tol1) b = (xm >= 0) ? b + tol1 : b - xm;
+            fb = D.fs(b);
+            if ((fb * (fc / std::fabs(fc))) > 0.0) break;
+        }
+    }
+}
+
+// Fraction of the cell [xlow, xlow + dx] x [ylow, ylow + dy] inside the disc.
+double disc_fraction(Disc& D, double xlow, double ylow, double dx, double dy)
+{
+    const double xx[5] = {xlow, xlow, xlow + dx, xlow + dx, xlow};
+    const double yy[5] = {ylow, ylow + dy, ylow + dy, ylow, ylow};
+    bool fl[5], all_in = true, all_out = true;
+    for (int i = 0; i < 4; i++) {
+        fl[i] = D.f(xx[i], yy[i]) < 0.0;
+        all_in = all_in && fl[i];
+        all_out = all_out && !fl[i];
+    }
+    fl[4] = fl[0];
+    if (all_in) return 1.0;
+    if (all_out) return 0.0;
+    double x[10], y[10];
+    int n = 0;
+    for (int i = 0; i < 4; i++) {
+        if (fl[i]) { x[n] = xx[i]; y[n] = yy[i]; n++; }
+        if (fl[i] != fl[i + 1]) {
+            D.xc0 = xx[i]; D.yc0 = yy[i]; D.xc1 = xx[i + 1]; D.yc1 = yy[i + 1];
+            const double ss = brent_zero(D, 0.0, 1.0, 1.0e-14);
+            x[n] = xx[i] + ss * (xx[i + 1] - xx[i]);
+            y[n] = yy[i] + ss * (yy[i + 1] - yy[i]);
+            n++;
+        }
+    }
+    if (n == 0) return 0.0;
+    x[n] = x[0]; y[n] = y[0];
+    double area = 0.0;
+    for (int i = 0; i < n; i++) area = area + 0.5 * (y[i] + y[i + 1]) * (x[i + 1] - x[i]);
+    return area / (dx * dy);
+}
+}  // namespace
 
 void app_setaux(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, double* aux)
 {
@@ -99,12 +185,19 @@ void app_qinit(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, 
                 for (int j = 1 - mbc; j <= my + mbc; j++) q[qi(d, i, j, m)] = (xc < 0.5) ? 1.0 : 0.0;
             }
     } else if (o.app == FC2D_B200_APP_RADIALDAM) {
+        Disc D{o.x0, o.y0, o.r0};
         for (int i = 1 - mbc; i <= mx + mbc; i++) {
             const double xc = P.xlower + (i - 0.5) * P.dx;
+            const double xlow = P.xlower + (i - 1.0) * P.dx;
             for (int j = 1 - mbc; j <= my + mbc; j++) {
                 const double yc = P.ylower + (j - 0.5) * P.dy;
-                const double r2 = (xc - o.x0) * (xc - o.x0) + (yc - o.y0) * (yc - o.y0);
-                const double win = (r2 - o.r0 * o.r0 < 0.0) ? 1.0 : 0.0;
+                double win;
+                if (o.qinit_cellave) {
+                    win = disc_fraction(D, xlow, P.ylower + (j - 1.0) * P.dy, P.dx, P.dy);
+                } else {
+                    const double r2 = (xc - o.x0) * (xc - o.x0) + (yc - o.y0) * (yc - o.y0);
+                    win = (r2 - o.r0 * o.r0 < 0.0) ? 1.0 : 0.0;
+                }
                 q[qi(d, i, j, 1)] = o.hin * win + o.hout * (1.0 - win);
                 q[qi(d, i, j, 2)] = 0.0;
                 q[qi(d, i, j, 3)] = 0.0;
@@ -161,39 +254,48 @@ bool app_inflow_state(const fc2d_b200_options_t& o, double* q)
     return true;
 }
 
-static bool grad_exceeds(const Dims& d, const PatchInfo& P, const double* q, int i, int j, double thr)
+int tag_criterion(const fc2d_b200_options_t& o)
 {
+    if (o.refinement_criteria != FC2D_B200_TAG_APP) return o.refinement_criteria;
+    return o.app == FC2D_B200_APP_SPHERE ? FC2D_B200_TAG_MINMAX : FC2D_B200_TAG_GRADIENT_DX;
+}
+
+// Criterion value of cell (i, j) compared with a threshold by the caller; for the
+// stencil criteria only interior cells count.
+static double tag_value(int crit, const Dims& d, const PatchInfo& P, const double* q, int i, int j, int mq)
+{
+    if (crit == FC2D_B200_TAG_VALUE) return q[qi(d, i, j, mq)];
+    if (crit == FC2D_B200_TAG_DIFFERENCE) {
+        const double dqx = std::fabs(q[qi(d, i + 1, j, mq)] - q[qi(d, i - 1, j, mq)]);
+        const double dqy = std::fabs(q[qi(d, i, j + 1, mq)] - q[qi(d, i, j - 1, mq)]);
+        return std::fmax(dqx, dqy);
+    }
     const double dx2 = 2 * P.dx, dy2 = 2 * P.dy;
-    const double dqx = (q[qi(d, i + 1, j, 1)] - q[qi(d, i - 1, j, 1)]) / dx2;
-    const double dqy = (q[qi(d, i, j + 1, 1)] - q[qi(d, i, j - 1, 1)]) / dy2;
+    const double dqx = (q[qi(d, i + 1, j, mq)] - q[qi(d, i - 1, j, mq)]) / dx2;
+    const double dqy = (q[qi(d, i, j + 1, mq)] - q[qi(d, i, j - 1, mq)]) / dy2;
     const double ds = std::sqrt(dqx * dqx + dqy * dqy + 0.0 * 0.0);
-    return ds * P.dx > thr;
+    return crit == FC2D_B200_TAG_GRADIENT_DX ? ds * P.dx : ds;
 }
 
 int app_tag_refine(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, const double* q)
 {
-    if (o.app == FC2D_B200_APP_SPHERE) {
-        // minmax: range of field 1 over the padded patch
-        double lo = q[qi(d, 1, 1, 1)], hi = lo;
+    // clawpatch_tag4refinement (fclaw2d_clawpatch.cpp:800-850): a negative threshold always refines
+    if (o.refine_threshold < 0) return 1;
+    const int crit = tag_criterion(o), mq = o.threshold_variable > 0 ? o.threshold_variable : 1;
+    if (crit == FC2D_B200_TAG_MINMAX) {
+        double lo = q[qi(d, 1, 1, mq)], hi = lo;
         for (int j = 1 - d.mbc; j <= d.my + d.mbc; j++)
             for (int i = 1 - d.mbc; i <= d.mx + d.mbc; i++) {
-                lo = std::fmin(lo, q[qi(d, i, j, 1)]);
-                hi = std::fmax(hi, q[qi(d, i, j, 1)]);
+                lo = std::fmin(lo, q[qi(d, i, j, mq)]);
+                hi = std::fmax(hi, q[qi(d, i, j, mq)]);
             }
         return hi - lo > o.refine_threshold ? 1 : 0;
     }
-    for (int j = 1; j <= d.my; j++)
-        for (int i = 1; i <= d.mx; i++)
-            if (grad_exceeds(d, P, q, i, j, o.refine_threshold)) return 1;
+    const int g = (crit == FC2D_B200_TAG_VALUE) ? d.mbc : 0;   // value tests the ghost cells too
+    for (int j = 1 - g; j <= d.my + g; j++)
+        for (int i = 1 - g; i <= d.mx + g; i++)
+            if (tag_value(crit, d, P, q, i, j, mq) > o.refine_threshold) return 1;
     return 0;
-}
-
-int app_coarsen_ok(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, const double* q)
-{
-    for (int i = 1; i <= d.mx; i++)
-        for (int j = 1; j <= d.my; j++)
-            if (grad_exceeds(d, P, q, i, j, o.coarsen_threshold)) return 0;
-    return 1;
 }
 
 }  // namespace fcb

@@ -14,9 +14,9 @@ void app_qinit(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, 
 void app_sphere_flow(const fc2d_b200_options_t& o, double axis[3], double* omega);
 // Constant state imposed by mthbc = 0 sides (shock-bubble inflow); false if the app has none.
 bool app_inflow_state(const fc2d_b200_options_t& o, double* q);
-// Refinement test of one patch (tag4refinement with the dx-scaled gradient criterion).
+// The tagging criterion in force (FC2D_B200_TAG_*, TAG_APP resolved to the app's own).
+int tag_criterion(const fc2d_b200_options_t& o);
+// Refinement test of one patch on the host (tag4refinement at initialization).
 int app_tag_refine(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, const double* q);
-// True when no interior cell exceeds the coarsening threshold (one member of tag4coarsening).
-int app_coarsen_ok(const fc2d_b200_options_t& o, const Dims& d, const PatchInfo& P, const double* q);
 
 }  // namespace fcb

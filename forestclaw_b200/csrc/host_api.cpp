@@ -141,6 +141,11 @@ struct fc2d_b200_solver {
     unsigned long long* cfl_host = nullptr;
     double* mass_dev = nullptr;
     int mass_cap = 0;
+    double* qsave = nullptr;                       // save_step copy of q
+    size_t qsave_n = 0;                            // doubles it holds (0: nothing saved)
+    size_t qsave_cap = 0;
+    unsigned forest_gen = 0, qsave_gen = 0;        // forest installs so far; the one qsave belongs to
+    unsigned char phys_ok_save[64] = {};
     double cell_updates = 0;
     double t_curr = 0;
     bool initialized = false;
@@ -652,6 +657,52 @@ static double bits_to_double(unsigned long long b)
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
+// Every entry point that touches the device makes the solver's device current for
+// the call and puts the caller's device back on return.
+struct DeviceScope {
+    int prev = -1;
+    explicit DeviceScope(const fc2d_b200_solver* s);
+    explicit DeviceScope(int device);
+    ~DeviceScope() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+// ---------------------------------------------------------------------------
+// Mass without device allocation: the scratch is the file-scope device array of
+// k_mass_noalloc.cu, whose address is resolved once per device (with that
+// device current) and cached.
+// ---------------------------------------------------------------------------
+static_assert(MASS_SCRATCH_DOUBLES == FC2D_B200_MASS_SCRATCH_DOUBLES,
+              "the public scratch limit must equal the size of the device array");
+static std::mutex g_scratch_mu;
+static double* g_scratch_addr[128];
+
+static int scratch_for_device(int dev, double** out)
+{
+    if (dev < 0 || dev >= 128) return fail(FC2D_B200_EINVAL, "device ordinal out of range for the mass scratch");
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    if (!g_scratch_addr[dev]) {
+        int cur = -1;
+        CK(cudaGetDevice(&cur));
+        if (cur != dev) CK(cudaSetDevice(dev));
+        double* p = nullptr;
+        cudaError_t e = mass_scratch_address(&p);
+        if (cur != dev) cudaSetDevice(cur);
+        if (e != cudaSuccess || !p)
+            return fail(FC2D_B200_ECUDA, std::string("cudaGetSymbolAddress(mass scratch): ") + cudaGetErrorString(e));
+        g_scratch_addr[dev] = p;
+    }
+    *out = g_scratch_addr[dev];
+    return 0;
+}
+
+DeviceScope::DeviceScope(int device)
+{
+    int cur = -1;
+    if (device >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != device && cudaSetDevice(device) == cudaSuccess)
+        prev = cur;
+}
+DeviceScope::DeviceScope(const fc2d_b200_solver* s) : DeviceScope(s ? s->o.device : -1) {}
+
 extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver_t** out)
 {
     if (!opt || !out) return fail(FC2D_B200_EINVAL, "null argument");
@@ -673,10 +724,23 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
                                       "square patches with mx >= 8");
     if (o.app == FC2D_B200_APP_SPHERE && o.time_sync)
         return fail(FC2D_B200_EINVAL, "time sync across cubed-sphere block seams is not built");
+    if (o.refinement_criteria < FC2D_B200_TAG_APP || o.refinement_criteria > FC2D_B200_TAG_GRADIENT_DX)
+        return fail(FC2D_B200_EINVAL, "refinement_criteria must be one of FC2D_B200_TAG_*");
+    if (o.threshold_variable < 0 || o.threshold_variable > o.meqn)
+        return fail(FC2D_B200_EINVAL, "threshold_variable must be in 1..meqn (0: field 1)");
+    if (o.smooth_level < 0) return fail(FC2D_B200_EINVAL, "smooth_level must be >= 0");
+    if (o.regrid_interval < 0 || o.nout < 0) return fail(FC2D_B200_EINVAL, "regrid_interval and nout must be >= 0");
     int ndev = 0;
     CK(cudaGetDeviceCount(&ndev));
     if (ndev <= 0) return fail(FC2D_B200_ECUDA, "no CUDA device");
+    if (o.device < 0 || o.device >= ndev) return fail(FC2D_B200_EINVAL, "device ordinal out of range");
     CK(cudaSetDevice(o.device));
+    {   // load the allocation-free mass module and resolve its scratch now, outside any
+        // step or stream capture (module loading is lazy and may allocate)
+        double* scratch = nullptr;
+        int rc = scratch_for_device(o.device, &scratch);
+        if (rc) return rc;
+    }
     auto s = std::make_unique<fc2d_b200_solver>();
     s->o = o;
     if (s->o.mi <= 0) s->o.mi = 1;
@@ -720,6 +784,7 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
 
 extern "C" int fc2d_b200_destroy(fc2d_b200_solver_t* s)
 {
+    DeviceScope dev_scope_(s);
     if (!s) return 0;
     cudaStreamSynchronize(s->st);
     for (auto e : s->ev_pool) cudaEventDestroy(e);
@@ -731,6 +796,7 @@ extern "C" int fc2d_b200_destroy(fc2d_b200_solver_t* s)
     invalidate_graph(s);
     cudaFree(s->params_dev); cudaFreeHost(s->params_host);
     if (s->mass_dev) cudaFree(s->mass_dev);
+    if (s->qsave) cudaFree(s->qsave);
     cudaFree(s->bc_dev); cudaFree(s->newton_hist);
     if (s->tune_params) cudaFree(s->tune_params);
     if (s->area) cudaFree(s->area);
@@ -742,6 +808,7 @@ extern "C" int fc2d_b200_destroy(fc2d_b200_solver_t* s)
 
 extern "C" int fc2d_b200_set_riemann(fc2d_b200_solver_t* s, int rp_id)
 {
+    DeviceScope dev_scope_(s);
     if (!s) return fail(FC2D_B200_EINVAL, "null solver");
     std::vector<const Step2Variant*> vars = step2_variants(s->o.precision, rp_id, s->o.mx, s->o.my, s->o.mbc);
     if (vars.empty()) return fail(FC2D_B200_EINVAL, "Riemann solver id not compiled for these patch dimensions");
@@ -765,6 +832,7 @@ static int install_forest(fc2d_b200_solver* s, const std::vector<Leaf>& leaves)
     nf.inst = s->forest.inst;
     if (!nf.build(leaves, err)) return fail(FC2D_B200_EFOREST, err);
     s->forest = std::move(nf);
+    s->forest_gen++;
     std::memset(s->phys_ok, 0, sizeof(s->phys_ok));
     int rc = alloc_slabs(s, s->forest.np());
     if (rc) return rc;
@@ -773,6 +841,7 @@ static int install_forest(fc2d_b200_solver* s, const std::vector<Leaf>& leaves)
 
 extern "C" int fc2d_b200_set_forest(fc2d_b200_solver_t* s, int np, const int* level, const int* gx, const int* gy)
 {
+    DeviceScope dev_scope_(s);
     if (!s || np <= 0 || !level || !gx || !gy) return fail(FC2D_B200_EINVAL, "bad forest arguments");
     std::vector<Leaf> L(np);
     for (int i = 0; i < np; i++) L[i] = {level[i], gx[i], gy[i]};
@@ -803,6 +872,7 @@ static int inst_maxlev(const fc2d_b200_solver* s, int i)
 
 extern "C" int fc2d_b200_initialize(fc2d_b200_solver_t* s)
 {
+    DeviceScope dev_scope_(s);
     if (!s) return fail(FC2D_B200_EINVAL, "null solver");
     if (s->o.app == FC2D_B200_APP_NONE) return fail(FC2D_B200_EINVAL, "initialize needs a built-in app");
     const Dims& d = s->d;
@@ -835,6 +905,7 @@ extern "C" int fc2d_b200_initialize(fc2d_b200_solver_t* s)
             const PatchInfo& P = f.p[i];
             if (P.level < inst_maxlev(s, P.inst) && app_tag_refine(io[P.inst], d, P, &q[(size_t)i * d.nq()])) mark[i] = 1;
         }
+        if (s->o.smooth_refine) smooth_marks(f, mark, s->o.smooth_level);
         int changed = 0;
         std::vector<Leaf> L = adapt_leaves(f, mark, changed, err);
         if (!changed) break;
@@ -904,6 +975,7 @@ extern "C" int fc2d_b200_patch_info(const fc2d_b200_solver_t* s, int* level, int
 
 extern "C" int fc2d_b200_get_q(fc2d_b200_solver_t* s, double* q)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !q) return fail(FC2D_B200_EINVAL, "null argument");
     CK(cudaMemcpyAsync(q, s->q, (size_t)s->forest.np() * s->d.nq() * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
@@ -912,6 +984,7 @@ extern "C" int fc2d_b200_get_q(fc2d_b200_solver_t* s, double* q)
 
 extern "C" int fc2d_b200_set_q(fc2d_b200_solver_t* s, const double* q)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !q) return fail(FC2D_B200_EINVAL, "null argument");
     CK(cudaMemcpyAsync(s->q, q, (size_t)s->forest.np() * s->d.nq() * sizeof(double), cudaMemcpyHostToDevice, s->st));
     CK(cudaStreamSynchronize(s->st));
@@ -921,6 +994,7 @@ extern "C" int fc2d_b200_set_q(fc2d_b200_solver_t* s, const double* q)
 
 extern "C" int fc2d_b200_get_aux(fc2d_b200_solver_t* s, double* aux)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !aux) return fail(FC2D_B200_EINVAL, "null argument");
     if (s->d.maux == 0) return 0;
     CK(cudaMemcpyAsync(aux, s->aux, (size_t)s->forest.np() * s->d.naux() * sizeof(double), cudaMemcpyDeviceToHost, s->st));
@@ -930,6 +1004,7 @@ extern "C" int fc2d_b200_get_aux(fc2d_b200_solver_t* s, double* aux)
 
 extern "C" int fc2d_b200_set_aux(fc2d_b200_solver_t* s, const double* aux)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !aux) return fail(FC2D_B200_EINVAL, "null argument");
     if (s->d.maux == 0) return 0;
     const size_t n = (size_t)s->forest.np() * s->d.naux();
@@ -948,6 +1023,7 @@ extern "C" int fc2d_b200_registers_size(const fc2d_b200_solver_t* s, int* n)
 
 extern "C" int fc2d_b200_get_registers(fc2d_b200_solver_t* s, double* r)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !r) return fail(FC2D_B200_EINVAL, "null argument");
     CK(cudaMemcpyAsync(r, s->regs, (size_t)s->forest.np() * s->d.nreg() * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
@@ -980,6 +1056,7 @@ static int end_cfl(fc2d_b200_solver* s, double* cfl, double* cfl_inst = nullptr)
 
 extern "C" int fc2d_b200_level_update(fc2d_b200_solver_t* s, int level, double t, double dt, double* cfl)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
     int rc = begin_cfl(s);
     if (rc) return rc;
@@ -996,6 +1073,7 @@ extern "C" int fc2d_b200_level_update(fc2d_b200_solver_t* s, int level, double t
 extern "C" int fc2d_b200_single_step_update(fc2d_b200_solver_t* s, int level, int iter, int total_count, double t,
                                             double dt, double* cfl)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
     if (iter == 0) { s->ss_level = level; s->ss_count = 0; }
     if (level != s->ss_level || iter != s->ss_count) return fail(FC2D_B200_ESTATE, "single_step_update calls out of order");
@@ -1010,6 +1088,7 @@ extern "C" int fc2d_b200_single_step_update(fc2d_b200_solver_t* s, int level, in
 
 extern "C" int fc2d_b200_ghost_update(fc2d_b200_solver_t* s, int minlevel, int maxlevel, double sync_time, int time_interp)
 {
+    DeviceScope dev_scope_(s);
     (void)sync_time;
     if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
     if (time_interp && !s->qinterp) return fail(FC2D_B200_EINVAL, "time interpolation needs subcycle");
@@ -1021,6 +1100,7 @@ extern "C" int fc2d_b200_ghost_update(fc2d_b200_solver_t* s, int minlevel, int m
 
 extern "C" int fc2d_b200_timeinterp(fc2d_b200_solver_t* s, int level, double alpha)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !s->initialized || !s->qinterp) return fail(FC2D_B200_ESTATE, "time interpolation needs subcycle");
     timeinterp(s, level, alpha);
     (void)flush_pending(s);
@@ -1030,6 +1110,7 @@ extern "C" int fc2d_b200_timeinterp(fc2d_b200_solver_t* s, int level, double alp
 
 extern "C" int fc2d_b200_time_sync(fc2d_b200_solver_t* s, int minlevel, int maxlevel)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
     time_sync(s, minlevel, maxlevel);
     (void)flush_pending(s);
@@ -1151,6 +1232,7 @@ static int advance_finish(fc2d_b200_solver_t* s, double* maxcfl, double* cfl_ins
 
 extern "C" int fc2d_b200_advance(fc2d_b200_solver_t* s, double t, double dt, double* maxcfl)
 {
+    DeviceScope dev_scope_(s);
     if (s && s->pending) return fail(FC2D_B200_ESTATE, "an advance is in flight");
     int rc = advance_launch(s, t, dt);
     if (rc) return rc;
@@ -1159,22 +1241,29 @@ extern "C" int fc2d_b200_advance(fc2d_b200_solver_t* s, double t, double dt, dou
 
 extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
     const Dims& d = s->d;
     const Forest& f = s->forest;
     const int np = f.np();
     std::vector<int> flags(np);
     CK(s->flags_dev.assign(flags, s->st));
+    const int crit = tag_criterion(s->o);
+    const bool minmax = crit == FC2D_B200_TAG_MINMAX;
+    const int mq = s->o.threshold_variable > 0 ? s->o.threshold_variable - 1 : 0;
     std::vector<double> mm;
-    if (s->sphere) {
+    if (minmax) {
         mm.assign(2 * (size_t)np, 0.0);
         CK(s->minmax_dev.assign(mm, s->st));
     }
-    launch_tag(d, s->q, s->desc, np, s->o.refine_threshold, s->o.coarsen_threshold, s->flags_dev.p, s->st,
-               s->sphere ? s->minmax_dev.p : nullptr);
+    launch_tag(d, s->q, s->desc, np, crit, mq, s->o.refine_threshold, s->o.coarsen_threshold, s->flags_dev.p, s->st,
+               minmax ? s->minmax_dev.p : nullptr);
     CK(cudaMemcpyAsync(flags.data(), s->flags_dev.p, sizeof(int) * (size_t)np, cudaMemcpyDeviceToHost, s->st));
-    if (s->sphere) CK(cudaMemcpyAsync(mm.data(), s->minmax_dev.p, sizeof(double) * mm.size(), cudaMemcpyDeviceToHost, s->st));
+    if (minmax) CK(cudaMemcpyAsync(mm.data(), s->minmax_dev.p, sizeof(double) * mm.size(), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
+    // clawpatch_tag4refinement / _tag4coarsening (fclaw2d_clawpatch.cpp:800-910): a negative
+    // refine threshold always refines, a threshold <= 0 never coarsens
+    const bool always_refine = s->o.refine_threshold < 0, never_coarsen = !(s->o.coarsen_threshold > 0);
     // cb_regrid_tag4coarsening (families) then cb_fclaw2d_regrid_tag4refinement
     std::vector<int> mark(np, 0);
     for (int i = 0; i < np; i++) {
@@ -1186,8 +1275,9 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
             if (sib[k] < 0) { ok = false; break; }
         }
         if (!ok) continue;
-        bool coarsen = true;
-        if (s->sphere) {
+        bool coarsen = !never_coarsen;
+        if (never_coarsen) {
+        } else if (minmax) {
             // minmax over the family (fclaw2d_clawpatch46_fort_tag4coarsening.f:35-58)
             double lo = mm[2 * sib[0]], hi = mm[2 * sib[0] + 1];
             for (int k = 1; k < 4; k++) { lo = std::min(lo, mm[2 * sib[k]]); hi = std::max(hi, mm[2 * sib[k] + 1]); }
@@ -1198,7 +1288,8 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
         if (coarsen) for (int k = 0; k < 4; k++) mark[sib[k]] = -1;
     }
     for (int i = 0; i < np; i++)
-        if (f.p[i].level < inst_maxlev(s, f.p[i].inst) && (flags[i] & 1)) mark[i] = 1;
+        if (f.p[i].level < inst_maxlev(s, f.p[i].inst) && (always_refine || (flags[i] & 1))) mark[i] = 1;
+    if (s->o.smooth_refine) smooth_marks(f, mark, s->o.smooth_level);
     int changed = 0;
     std::string err;
     std::vector<Leaf> L = adapt_leaves(f, mark, changed, err);
@@ -1288,6 +1379,7 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     std::swap(s->cap, sp.cap);
     s->aux_host.swap(naux);
     s->forest = std::move(nf);
+    s->forest_gen++;
     invalidate_graph(s);
     rc = upload_desc_and_tables(s);
     if (rc) return rc;
@@ -1316,8 +1408,113 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     return 0;
 }
 
+// ---------------------------------------------------------------------------
+// save / restore a step and the run loop (src/fclaw2d_run.c)
+// ---------------------------------------------------------------------------
+extern "C" int fc2d_b200_save_step(fc2d_b200_solver_t* s)
+{
+    DeviceScope dev_scope_(s);
+    if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
+    if (s->pending) return fail(FC2D_B200_ESTATE, "an advance is in flight");
+    CK(cudaSetDevice(s->o.device));
+    const size_t n = (size_t)s->forest.np() * s->d.nq();
+    if (s->qsave_cap < n) {
+        if (s->qsave) CK(cudaFree(s->qsave));
+        s->qsave = nullptr;
+        s->qsave_cap = 0;
+        CK(cudaMalloc(&s->qsave, n * sizeof(double)));
+        s->qsave_cap = n;
+    }
+    CK(cudaMemcpyAsync(s->qsave, s->q, n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+    s->qsave_n = n;
+    s->qsave_gen = s->forest_gen;
+    std::memcpy(s->phys_ok_save, s->phys_ok, sizeof(s->phys_ok));
+    return 0;
+}
+
+extern "C" int fc2d_b200_restore_step(fc2d_b200_solver_t* s)
+{
+    DeviceScope dev_scope_(s);
+    if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
+    if (s->pending) return fail(FC2D_B200_ESTATE, "an advance is in flight");
+    const size_t n = (size_t)s->forest.np() * s->d.nq();
+    if (s->qsave_n != n || s->qsave_gen != s->forest_gen)
+        return fail(FC2D_B200_ESTATE, "no saved step for the current forest");
+    CK(cudaSetDevice(s->o.device));
+    CK(cudaMemcpyAsync(s->q, s->qsave, n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+    // the ghost cells are back to their saved values, physical ones included
+    std::memcpy(s->phys_ok, s->phys_ok_save, sizeof(s->phys_ok));
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+// outstyle_1 (src/fclaw2d_run.c:113-265) with reduce_cfl (one process: the global
+// maximum is the local one) and advance_one_step off.
+extern "C" int fc2d_b200_run(fc2d_b200_solver_t* s, fc2d_b200_run_stats_t* out)
+{
+    DeviceScope dev_scope_(s);
+    if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
+    if (!s->insts.empty()) return fail(FC2D_B200_EINVAL, "fc2d_b200_run drives one forest; batches step by advance_instances");
+    const fc2d_b200_options_t& o = s->o;
+    if (!(o.tfinal > 0) || !(o.initial_dt > 0)) return fail(FC2D_B200_EINVAL, "fc2d_b200_run needs tfinal > 0 and initial_dt > 0");
+    fc2d_b200_run_stats_t st{};
+    const int nout = o.nout > 0 ? o.nout : 1;
+    double dt_minlevel = o.initial_dt;
+    const double t0 = 0;
+    const double dt_outer = (o.tfinal - t0) / ((double)nout);
+    double t_curr = t0;
+    int n_inner = 0;
+    for (int n = 0; n < nout; n++) {
+        const double tstart = t_curr;
+        const double tend = tstart + dt_outer;
+        while (t_curr < tend) {
+            int rc;
+            if (!o.use_fixed_dt && (rc = fc2d_b200_save_step(s))) return rc;
+            // take a slightly larger step now rather than a tiny one to hit tend later
+            double dt_step = dt_minlevel;
+            const double tol = 1e-2 * dt_step;
+            int took_small_step = 0;
+            if (!o.use_fixed_dt) {
+                const double small_step = tend - (t_curr + dt_step);
+                if (small_step < tol) {
+                    dt_step = tend - t_curr;
+                    if (small_step < 0) took_small_step = 1;
+                }
+            }
+            double maxcfl_step = 0;
+            if ((rc = fc2d_b200_advance(s, t_curr, dt_step, &maxcfl_step))) return rc;
+            st.count_amr_advance++;
+            if (maxcfl_step > o.max_cfl && !o.use_fixed_dt) {
+                // retake the step from the saved copy with a smaller dt
+                if ((rc = fc2d_b200_restore_step(s))) return rc;
+                dt_minlevel = dt_minlevel * o.desired_cfl / maxcfl_step;
+                st.rejected++;
+                continue;
+            }
+            n_inner++;
+            t_curr += dt_step;
+            if (!o.use_fixed_dt) {
+                const double dt_new = dt_minlevel * o.desired_cfl / maxcfl_step;
+                if (!took_small_step) dt_minlevel = dt_new;
+            }
+            if (o.regrid_interval > 0 && n_inner % o.regrid_interval == 0) {
+                int changed = 0;
+                if ((rc = fc2d_b200_regrid(s, &changed))) return rc;
+                st.count_amr_regrid++;
+                if (changed) st.count_amr_new_domain++;
+            }
+        }
+    }
+    st.steps = n_inner;
+    st.global_num_patches = s->forest.np();
+    st.t_final = t_curr;
+    if (out) *out = st;
+    return 0;
+}
+
 extern "C" int fc2d_b200_mass(fc2d_b200_solver_t* s, double* out)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !out || !s->initialized) return fail(FC2D_B200_EINVAL, "bad arguments");
     const int np = s->forest.np(), meqn = s->d.meqn;
     if (np * meqn > s->mass_cap) {
@@ -1351,6 +1548,7 @@ extern "C" int fc2d_b200_cell_updates(const fc2d_b200_solver_t* s, double* out)
 
 extern "C" int fc2d_b200_synchronize(fc2d_b200_solver_t* s)
 {
+    DeviceScope dev_scope_(s);
     if (!s) return fail(FC2D_B200_EINVAL, "null solver");
     CK(cudaStreamSynchronize(s->st));
     return 0;
@@ -1369,6 +1567,7 @@ extern "C" int fc2d_b200_last_update_stats(const fc2d_b200_solver_t* s, double* 
 
 extern "C" int fc2d_b200_set_timing(fc2d_b200_solver_t* s, int enable)
 {
+    DeviceScope dev_scope_(s);
     if (!s) return fail(FC2D_B200_EINVAL, "null solver");
     s->timing = enable != 0;
     return 0;
@@ -1376,6 +1575,7 @@ extern "C" int fc2d_b200_set_timing(fc2d_b200_solver_t* s, int enable)
 
 extern "C" int fc2d_b200_event_record(fc2d_b200_solver_t* s, int slot)
 {
+    DeviceScope dev_scope_(s);
     if (!s || slot < 0 || slot >= 64) return fail(FC2D_B200_EINVAL, "bad event slot");
     if (s->user_ev.empty()) {
         s->user_ev.resize(64);
@@ -1387,6 +1587,7 @@ extern "C" int fc2d_b200_event_record(fc2d_b200_solver_t* s, int slot)
 
 extern "C" int fc2d_b200_event_elapsed(fc2d_b200_solver_t* s, int a, int b, double* ms)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !ms || a < 0 || b < 0 || a >= (int)s->user_ev.size() || b >= (int)s->user_ev.size())
         return fail(FC2D_B200_EINVAL, "bad event slots");
     CK(cudaEventSynchronize(s->user_ev[b]));
@@ -1405,6 +1606,7 @@ extern "C" int fc2d_b200_get_stream(const fc2d_b200_solver_t* s, void** stream)
 
 extern "C" int fc2d_b200_set_programmatic_launch(fc2d_b200_solver_t* s, int enable)
 {
+    DeviceScope dev_scope_(s);
     if (!s) return fail(FC2D_B200_EINVAL, "null solver");
     s->programmatic = enable != 0;
     invalidate_graph(s);
@@ -1413,41 +1615,16 @@ extern "C" int fc2d_b200_set_programmatic_launch(fc2d_b200_solver_t* s, int enab
 
 extern "C" int fc2d_b200_set_graphs(fc2d_b200_solver_t* s, int enable)
 {
+    DeviceScope dev_scope_(s);
     if (!s) return fail(FC2D_B200_EINVAL, "null solver");
     s->use_graphs = enable != 0;
     invalidate_graph(s);
     return 0;
 }
 
-// ---------------------------------------------------------------------------
-// Mass without device allocation: the scratch is the file-scope device array of
-// k_mass_noalloc.cu, whose address is resolved once per device (with that
-// device current) and cached.
-// ---------------------------------------------------------------------------
-static std::mutex g_scratch_mu;
-static double* g_scratch_addr[128];
-
-static int scratch_for_device(int dev, double** out)
-{
-    if (dev < 0 || dev >= 128) return fail(FC2D_B200_EINVAL, "device ordinal out of range for the mass scratch");
-    std::lock_guard<std::mutex> lk(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
-        int cur = -1;
-        CK(cudaGetDevice(&cur));
-        if (cur != dev) CK(cudaSetDevice(dev));
-        double* p = nullptr;
-        cudaError_t e = mass_scratch_address(&p);
-        if (cur != dev) cudaSetDevice(cur);
-        if (e != cudaSuccess || !p)
-            return fail(FC2D_B200_ECUDA, std::string("cudaGetSymbolAddress(mass scratch): ") + cudaGetErrorString(e));
-        g_scratch_addr[dev] = p;
-    }
-    *out = g_scratch_addr[dev];
-    return 0;
-}
-
 extern "C" int fc2d_b200_mass_noalloc(fc2d_b200_solver_t* s, double* out)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !out || !s->initialized) return fail(FC2D_B200_EINVAL, "bad arguments");
     if (s->sphere) return fail(FC2D_B200_EINVAL, "fc2d_b200_mass_noalloc weights by dx dy; a manifold needs fc2d_b200_mass");
     const long long np = s->forest.np(), meqn = s->d.meqn;
@@ -1467,6 +1644,7 @@ extern "C" int fc2d_b200_mass_noalloc(fc2d_b200_solver_t* s, double* out)
 
 extern "C" int fc2d_b200_newton_histogram(fc2d_b200_solver_t* s, unsigned long long* out, int reset)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !out) return fail(FC2D_B200_EINVAL, "null argument");
     CK(cudaMemcpyAsync(out, s->newton_hist, 32 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
@@ -1555,6 +1733,7 @@ extern "C" int fc2d_b200_mlp_create(int device, unsigned long long seed, fc2d_b2
 
 extern "C" int fc2d_b200_mlp_destroy(fc2d_b200_mlp_t* m)
 {
+    DeviceScope dev_scope_(m ? m->device : -1);
     if (!m) return 0;
     cudaSetDevice(m->device);
     cudaStreamSynchronize(m->st);
@@ -1569,6 +1748,7 @@ extern "C" int fc2d_b200_mlp_destroy(fc2d_b200_mlp_t* m)
 
 extern "C" int fc2d_b200_mlp_set_params(fc2d_b200_mlp_t* m, const float* params)
 {
+    DeviceScope dev_scope_(m ? m->device : -1);
     if (!m || !params) return fail(FC2D_B200_EINVAL, "null argument");
     CK(cudaSetDevice(m->device));
     CK(cudaMemcpyAsync(m->prm, params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice, m->st));
@@ -1579,6 +1759,7 @@ extern "C" int fc2d_b200_mlp_set_params(fc2d_b200_mlp_t* m, const float* params)
 
 extern "C" int fc2d_b200_mlp_get_params(fc2d_b200_mlp_t* m, float* params)
 {
+    DeviceScope dev_scope_(m ? m->device : -1);
     if (!m || !params) return fail(FC2D_B200_EINVAL, "null argument");
     CK(cudaSetDevice(m->device));
     CK(cudaMemcpyAsync(params, m->prm, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost, m->st));
@@ -1604,6 +1785,7 @@ static int mlp_reserve(fc2d_b200_mlp* m, int n)
 
 extern "C" int fc2d_b200_mlp_set_data(fc2d_b200_mlp_t* m, const double* prim, int n, double gamma, double tol)
 {
+    DeviceScope dev_scope_(m ? m->device : -1);
     if (!m || !prim || n <= 0 || !(gamma > 1.0) || !(tol > 0.0)) return fail(FC2D_B200_EINVAL, "bad arguments");
     CK(cudaSetDevice(m->device));
     int rc = mlp_reserve(m, n);
@@ -1618,6 +1800,7 @@ extern "C" int fc2d_b200_mlp_set_data(fc2d_b200_mlp_t* m, const double* prim, in
 
 extern "C" int fc2d_b200_mlp_get_data(fc2d_b200_mlp_t* m, float* X, float* Y)
 {
+    DeviceScope dev_scope_(m ? m->device : -1);
     if (!m || m->n <= 0) return fail(FC2D_B200_ESTATE, "no training data");
     CK(cudaSetDevice(m->device));
     if (X) CK(cudaMemcpyAsync(X, m->X, sizeof(float) * MLP_IN * (size_t)m->n, cudaMemcpyDeviceToHost, m->st));
@@ -1629,6 +1812,7 @@ extern "C" int fc2d_b200_mlp_get_data(fc2d_b200_mlp_t* m, float* X, float* Y)
 extern "C" int fc2d_b200_mlp_train(fc2d_b200_mlp_t* m, int epochs, int batch, float lr, unsigned long long seed,
                                    double* loss_out)
 {
+    DeviceScope dev_scope_(m ? m->device : -1);
     if (!m || m->n <= 0) return fail(FC2D_B200_ESTATE, "no training data");
     if (epochs <= 0 || batch <= 0 || !(lr > 0.0f)) return fail(FC2D_B200_EINVAL, "bad training arguments");
     CK(cudaSetDevice(m->device));
@@ -1669,6 +1853,7 @@ extern "C" int fc2d_b200_mlp_train(fc2d_b200_mlp_t* m, int epochs, int batch, fl
 extern "C" int fc2d_b200_mlp_gradient(fc2d_b200_mlp_t* m, const float* X, const float* Y, int n, float* grad,
                                       double* loss)
 {
+    DeviceScope dev_scope_(m ? m->device : -1);
     if (!m || !X || !Y || !grad || n <= 0) return fail(FC2D_B200_EINVAL, "bad arguments");
     CK(cudaSetDevice(m->device));
     int rc = mlp_partials(m, n);
@@ -1691,6 +1876,7 @@ extern "C" int fc2d_b200_mlp_gradient(fc2d_b200_mlp_t* m, const float* X, const 
 
 extern "C" int fc2d_b200_mlp_predict(fc2d_b200_mlp_t* m, const float* X, int n, float* Y)
 {
+    DeviceScope dev_scope_(m ? m->device : -1);
     if (!m || !X || !Y || n <= 0) return fail(FC2D_B200_EINVAL, "bad arguments");
     CK(cudaSetDevice(m->device));
     float *Xd, *Yd;
@@ -1706,6 +1892,7 @@ extern "C" int fc2d_b200_mlp_predict(fc2d_b200_mlp_t* m, const float* X, int n, 
 
 extern "C" int fc2d_b200_mlp_newton_histogram(fc2d_b200_mlp_t* m, int use_mlp, long long* hist)
 {
+    DeviceScope dev_scope_(m ? m->device : -1);
     if (!m || !hist || m->n <= 0) return fail(FC2D_B200_ESTATE, "no data");
     CK(cudaSetDevice(m->device));
     if (use_mlp) launch_mlp_predict(m->X, m->n, m->blob, m->Yp, m->st);
@@ -1720,6 +1907,7 @@ extern "C" int fc2d_b200_mlp_newton_histogram(fc2d_b200_mlp_t* m, int use_mlp, l
 
 extern "C" int fc2d_b200_sample_interfaces(fc2d_b200_solver_t* s, int n, unsigned long long seed, double* prim)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !s->initialized || !prim || n <= 0) return fail(FC2D_B200_EINVAL, "bad arguments");
     if (s->o.rp != FC2D_B200_RP_EULER_EXACT) return fail(FC2D_B200_EINVAL, "interface sampling needs the Euler solver");
     double* d = nullptr;
@@ -1734,6 +1922,7 @@ extern "C" int fc2d_b200_sample_interfaces(fc2d_b200_solver_t* s, int n, unsigne
 
 extern "C" int fc2d_b200_set_pstar_seed(fc2d_b200_solver_t* s, const fc2d_b200_mlp_t* m)
 {
+    DeviceScope dev_scope_(s);
     if (!s) return fail(FC2D_B200_EINVAL, "null solver");
     if (!m) { s->use_mlp = false; return 0; }
     if (s->o.rp != FC2D_B200_RP_EULER_EXACT) return fail(FC2D_B200_EINVAL, "the p* seed applies to the Euler solver");
@@ -1749,6 +1938,7 @@ extern "C" int fc2d_b200_set_pstar_seed(fc2d_b200_solver_t* s, const fc2d_b200_m
 // ---------------------------------------------------------------------------
 extern "C" int fc2d_b200_set_instances(fc2d_b200_solver_t* s, int n, const fc2d_b200_instance_t* inst)
 {
+    DeviceScope dev_scope_(s);
     if (!s || n <= 0 || !inst) return fail(FC2D_B200_EINVAL, "bad arguments");
     if (n > FC2D_B200_MAX_INSTANCES) return fail(FC2D_B200_EINVAL, "too many instances");
     if (s->initialized) return fail(FC2D_B200_ESTATE, "instances are set before initialize");
@@ -1789,6 +1979,7 @@ extern "C" int fc2d_b200_patch_instance(const fc2d_b200_solver_t* s, int* inst)
 
 extern "C" int fc2d_b200_advance_instances_begin(fc2d_b200_solver_t* s, const double* dt)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !s->initialized || !dt) return fail(FC2D_B200_EINVAL, "bad arguments");
     if (s->insts.empty()) return fail(FC2D_B200_ESTATE, "no instances set");
     if (s->pending) return fail(FC2D_B200_ESTATE, "an advance is in flight");
@@ -1803,6 +1994,7 @@ extern "C" int fc2d_b200_advance_instances_begin(fc2d_b200_solver_t* s, const do
 
 extern "C" int fc2d_b200_advance_instances_end(fc2d_b200_solver_t* s, double* cfl)
 {
+    DeviceScope dev_scope_(s);
     if (!s) return fail(FC2D_B200_EINVAL, "null solver");
     double dummy = 0.0;
     return advance_finish(s, &dummy, cfl);
@@ -1810,6 +2002,7 @@ extern "C" int fc2d_b200_advance_instances_end(fc2d_b200_solver_t* s, double* cf
 
 extern "C" int fc2d_b200_advance_instances(fc2d_b200_solver_t* s, const double* dt, double* cfl)
 {
+    DeviceScope dev_scope_(s);
     int rc = fc2d_b200_advance_instances_begin(s, dt);
     if (rc) return rc;
     return fc2d_b200_advance_instances_end(s, cfl);
@@ -1817,6 +2010,7 @@ extern "C" int fc2d_b200_advance_instances(fc2d_b200_solver_t* s, const double* 
 
 extern "C" int fc2d_b200_mass_instances(fc2d_b200_solver_t* s, double* out)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !out || !s->initialized) return fail(FC2D_B200_EINVAL, "bad arguments");
     const int np = s->forest.np(), meqn = s->d.meqn, ni = s->forest.ninst();
     if (np * meqn > s->mass_cap) {
@@ -1870,6 +2064,7 @@ extern "C" int fc2d_b200_variant_info(const fc2d_b200_solver_t* s, int v, int* t
 
 extern "C" int fc2d_b200_set_variant(fc2d_b200_solver_t* s, int v)
 {
+    DeviceScope dev_scope_(s);
     if (!s || v < 0 || v >= (int)s->vars.size()) return fail(FC2D_B200_EINVAL, "no such variant");
     cudaError_t e = s->vars[v]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, LevelGroup{1, {0}}, nullptr, s->st);
     if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
@@ -1886,6 +2081,7 @@ extern "C" int fc2d_b200_set_variant(fc2d_b200_solver_t* s, int v)
 // the registers and the statistics as they were.
 extern "C" int fc2d_b200_autotune(fc2d_b200_solver_t* s, int reps, int* best_out, double* ms_out)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !s->initialized || reps < 1) return fail(FC2D_B200_EINVAL, "bad arguments");
     const Forest& f = s->forest;
     StepParams sp = make_params(s, f.maxlevel_present, s->t_curr, 0.0);
@@ -1962,6 +2158,7 @@ extern "C" int fc2d_b200_level_variants(const fc2d_b200_solver_t* s, int* varian
 // ---------------------------------------------------------------------------
 extern "C" int fc2d_b200_output_ascii(fc2d_b200_solver_t* s, const char* dir, int iframe, double time)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !s->initialized || !dir) return fail(FC2D_B200_EINVAL, "bad arguments");
     const Forest& f = s->forest;
     const int np = f.np();
@@ -2001,6 +2198,7 @@ extern "C" int fc2d_b200_output_ascii(fc2d_b200_solver_t* s, const char* dir, in
 // one copy brings them to the host, which writes the file.
 extern "C" int fc2d_b200_output_vtk(fc2d_b200_solver_t* s, const char* prefix, int iframe)
 {
+    DeviceScope dev_scope_(s);
     if (!s || !s->initialized || !prefix || iframe < 0) return fail(FC2D_B200_EINVAL, "bad arguments");
     const Forest& f = s->forest;
     const int np = f.np();

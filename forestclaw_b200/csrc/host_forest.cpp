@@ -349,6 +349,33 @@ std::vector<Leaf> adapt_leaves(const Forest& f, const std::vector<int>& mark, in
     return L;
 }
 
+void smooth_marks(const Forest& f, std::vector<int>& mark, int smooth_level)
+{
+    const int np = f.np();
+    std::vector<int> tl(np);
+    for (int i = 0; i < np; i++) tl[i] = f.p[i].level + mark[i];
+    for (int i = 0; i < np; i++) {
+        const PatchInfo& P = f.p[i];
+        const int level = P.level;
+        int mt = tl[i];
+        // faces first, then corners, each only while no neighbour has raised the target above level
+        for (int fc = 0; mt <= level && fc < 4; fc++) {
+            const int t = P.face_type[fc];
+            if (t == NB_BOUNDARY) continue;
+            for (int k = 0; k < (t == NB_HALF ? 2 : 1); k++) {
+                const int nb = P.face_nbr[fc][k];
+                if (f.p[nb].level + f.gi(f.p[nb].inst).lbase >= smooth_level) mt = std::max(mt, tl[nb]);
+            }
+        }
+        for (int c = 0; mt <= level && c < 4; c++) {
+            if (!P.has_corner[c]) continue;
+            const int nb = P.corner_nbr[c];
+            if (f.p[nb].level + f.gi(f.p[nb].inst).lbase >= smooth_level) mt = std::max(mt, tl[nb]);
+        }
+        mark[i] = (mt < level) ? -1 : (mt > level) ? 1 : 0;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // gather tables
 // ---------------------------------------------------------------------------

@@ -94,6 +94,13 @@ private:
 // Returns the new leaf list; changed = 0 if identical to the old forest.
 std::vector<Leaf> adapt_leaves(const Forest& f, const std::vector<int>& mark, int& changed, std::string& err);
 
+// Refinement smoothing of fclaw2d_domain_adapt (src/fclaw2d_convenience.c:507-645):
+// mark (+1 / -1 / 0 from the tags) sets each leaf's target level; every leaf
+// then takes the largest target level of itself and its face and corner
+// neighbours of level >= smooth_level and is marked by the sign of the
+// difference to its own level.
+void smooth_marks(const Forest& f, std::vector<int>& mark, int smooth_level);
+
 // Gather tables of one level.
 struct LevelTables {
     std::vector<CopyEnt> copy;       // copy2ghost(level)

@@ -425,18 +425,25 @@ __global__ void k_patch_mass(const double* __restrict__ q, const PatchDesc* __re
     out[(size_t)p * meqn + m] = sum;
 }
 
-// Gradient criterion scaled by dx on field 1 (gradient_exceeds_th.f90, unmapped branch).
+// Tagging tests of one patch (fort_4.6/fclaw2d_clawpatch46_tag4refinement.f:11-75 and the
+// per-patch part of _tag4coarsening.f:80-130) with the criteria of
+// fort_user/fclaw2d_clawpatch_*_exceeds_th.f90 on field mq (0-based plane):
+//   value:      q over the padded patch exceeds the threshold;
+//   difference: max(|q(i+1,j)-q(i-1,j)|, |q(i,j+1)-q(i,j-1)|) over interior cells;
+//   gradient:   sqrt(dqx^2 + dqy^2 + 0^2) of central differences over interior cells
+//               (times dx for TAG_GRADIENT_DX);
+//   minmax:     range of q over the padded patch (the family test combines the ranges).
+// Only whether some cell exceeds matters, so the reference's running minimum and
+// maximum reduce to the patch's.
 __global__ void k_tag(const double* __restrict__ q, const PatchDesc* __restrict__ desc, int mx, int my, int mbc,
-                      int meqn, double rthr, double cthr, int* __restrict__ flags, double* __restrict__ minmax)
+                      int meqn, int crit, int mq, double rthr, double cthr, int* __restrict__ flags,
+                      double* __restrict__ minmax)
 {
     const int p = blockIdx.x;
     const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
     const PatchDesc pd = desc[p];
-    const double* qp = q + (size_t)p * meqn * nx * ny;
-    if (minmax) {
-        // minmax criterion (fclaw2d_clawpatch_minmax_exceeds_th.f90 in
-        // fclaw2d_clawpatch46_fort_tag4refinement.f:38-75): range of field 1 over the
-        // padded patch; the family coarsening test combines the ranges on the host
+    const double* qp = q + (size_t)p * meqn * nx * ny + (size_t)mq * nx * ny;
+    if (crit == FC2D_B200_TAG_MINMAX) {
         __shared__ double smn[128], smx[128];
         double mn = qp[mbc * nx + mbc], mxv = mn;
         for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
@@ -459,16 +466,30 @@ __global__ void k_tag(const double* __restrict__ q, const PatchDesc* __restrict_
         }
         return;
     }
-    const double dx2 = 2 * pd.dx, dy2 = 2 * pd.dy;
     int refine = 0, exceed_c = 0;
-    for (int c = threadIdx.x; c < mx * my; c += blockDim.x) {
-        const int i = c % mx + mbc, j = c / mx + mbc;
-        double dqx = (qp[j * nx + i + 1] - qp[j * nx + i - 1]) / dx2;
-        double dqy = (qp[(j + 1) * nx + i] - qp[(j - 1) * nx + i]) / dy2;
-        double ds = sqrt(dqx * dqx + dqy * dqy + 0.0 * 0.0);
-        double v = ds * pd.dx;
-        refine |= (v > rthr);
-        exceed_c |= (v > cthr);
+    if (crit == FC2D_B200_TAG_VALUE) {
+        for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
+            refine |= (qp[c] > rthr);
+            exceed_c |= (qp[c] > cthr);
+        }
+    } else {
+        const double dx2 = 2 * pd.dx, dy2 = 2 * pd.dy;
+        for (int c = threadIdx.x; c < mx * my; c += blockDim.x) {
+            const int i = c % mx + mbc, j = c / mx + mbc;
+            double v;
+            if (crit == FC2D_B200_TAG_DIFFERENCE) {
+                const double dqx = fabs(qp[j * nx + i + 1] - qp[j * nx + i - 1]);
+                const double dqy = fabs(qp[(j + 1) * nx + i] - qp[(j - 1) * nx + i]);
+                v = fmax(dqx, dqy);
+            } else {
+                const double dqx = (qp[j * nx + i + 1] - qp[j * nx + i - 1]) / dx2;
+                const double dqy = (qp[(j + 1) * nx + i] - qp[(j - 1) * nx + i]) / dy2;
+                v = sqrt(dqx * dqx + dqy * dqy + 0.0 * 0.0);
+                if (crit == FC2D_B200_TAG_GRADIENT_DX) v = v * pd.dx;
+            }
+            refine |= (v > rthr);
+            exceed_c |= (v > cthr);
+        }
     }
     refine = __syncthreads_or(refine);
     exceed_c = __syncthreads_or(exceed_c);
@@ -649,10 +670,10 @@ void launch_patch_mass(const Dims& d, const double* q, const PatchDesc* desc, in
 {
     if (np > 0) k_patch_mass<<<np, 32, 0, st>>>(q, desc, d.mx, d.my, d.mbc, d.meqn, out, area);
 }
-void launch_tag(const Dims& d, const double* q, const PatchDesc* desc, int np, double rthr, double cthr, int* flags,
-                cudaStream_t st, double* minmax)
+void launch_tag(const Dims& d, const double* q, const PatchDesc* desc, int np, int crit, int mq, double rthr,
+                double cthr, int* flags, cudaStream_t st, double* minmax)
 {
-    if (np > 0) k_tag<<<np, 128, 0, st>>>(q, desc, d.mx, d.my, d.mbc, d.meqn, rthr, cthr, flags, minmax);
+    if (np > 0) k_tag<<<np, 128, 0, st>>>(q, desc, d.mx, d.my, d.mbc, d.meqn, crit, mq, rthr, cthr, flags, minmax);
 }
 void launch_repop(const Dims& d, const RepopOp* ops, int nops, const double* oq, double* nq, const double* oqlast,
                   double* nqlast, const double* oqi, double* nqi, const double* oregs, double* nregs,

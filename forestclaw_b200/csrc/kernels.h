@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "fcb_common.h"
+#include "fc2d_b200.h"
 
 namespace fcb {
 
@@ -108,11 +109,12 @@ void launch_reset_sync(const Dims& d, double* regs, const PatchDesc* desc, int p
 // area (manifold, else null): the cell areas weight q instead of dx dy
 void launch_patch_mass(const Dims& d, const double* q, const PatchDesc* desc, int np, double* out,
                        cudaStream_t st, const double* area = nullptr);
-// flags[p] bit0: some interior cell exceeds refine threshold, bit1: no cell exceeds coarsen threshold
-// (gradient criterion).  With minmax (2 doubles per patch) the minmax criterion: the range of
-// field 1 over the padded patch into minmax, bit0 = range > refine_thr, coarsening decided by the caller.
-void launch_tag(const Dims& d, const double* q, const PatchDesc* desc, int np, double refine_thr,
-                double coarsen_thr, int* flags, cudaStream_t st, double* minmax = nullptr);
+// Tagging tests of every patch with criterion crit (FC2D_B200_TAG_*, resolved: not TAG_APP) on
+// field plane mq: flags[p] bit0 = some cell exceeds refine_thr, bit1 = no cell exceeds coarsen_thr.
+// TAG_MINMAX writes the range of the padded patch into minmax (2 doubles per patch), bit0 =
+// range > refine_thr, and leaves the family test to the caller.
+void launch_tag(const Dims& d, const double* q, const PatchDesc* desc, int np, int crit, int mq, double refine_thr,
+                double coarsen_thr, int* flags, cudaStream_t st, double* minmax);
 // Repopulation after adapt: op kind 0 copy old slot, 1 interpolate2fine from old parent (igrid),
 // 2 average2coarse from 4 old children (src = first child slot; children consecutive by igrid
 // via child_slots).

@@ -81,7 +81,43 @@ typedef struct fc2d_b200_options {
     /* B200 specifics */
     int precision;         /* FC2D_B200_PREC_* */
     int device;            /* CUDA device ordinal */
+    /* refinement strategy: smooth-refine / smooth-level (fclaw_options.c:203-209,
+     * applied in fclaw2d_domain_adapt, src/fclaw2d_convenience.c:507-645),
+     * refinement-criteria / threshold-variable (fclaw2d_clawpatch_options.c:107-114) */
+    int smooth_refine, smooth_level;
+    int refinement_criteria;   /* FC2D_B200_TAG_* */
+    int threshold_variable;    /* field tested by the criterion, 1..meqn (0 = 1) */
+    int qinit_cellave;         /* radial dam: 1 = cell averages of the disc (cellave2.f), 0 = cell-centre test */
+    /* fclaw2d_run outstyle 1 (fclaw_options.c: regrid_interval, nout, use_fixed_dt,
+     * tfinal, initial_dt, max_cfl, desired_cfl) */
+    int regrid_interval, nout, use_fixed_dt;
+    double tfinal, initial_dt, max_cfl, desired_cfl;
 } fc2d_b200_options_t;
+
+/* Tagging criteria: FCLAW_REFINE_CRITERIA_* (fclaw2d_clawpatch_options.h:48-56) + 1
+ * (fort_user/fclaw2d_clawpatch_{value,difference,minmax,gradient}_exceeds_th.f90 in
+ * fort_4.6/fclaw2d_clawpatch46_tag4refinement.f / _tag4coarsening.f).  TAG_APP keeps
+ * the app's built-in criterion: minmax for the sphere, the gradient times dx
+ * (refine where |grad q| dx exceeds the threshold) for the others. */
+#define FC2D_B200_TAG_APP         0
+#define FC2D_B200_TAG_VALUE       1
+#define FC2D_B200_TAG_DIFFERENCE  2
+#define FC2D_B200_TAG_MINMAX      3
+#define FC2D_B200_TAG_GRADIENT    4
+#define FC2D_B200_TAG_GRADIENT_DX 5
+
+/* Counters of fc2d_b200_run (fclaw2d_global_t count_amr_advance, count_amr_regrid,
+ * count_amr_new_domain; the reference's regression check, src/fclaw2d_finalize.c:119-165,
+ * compares count_amr_advance, global_num_patches and count_amr_new_domain). */
+typedef struct fc2d_b200_run_stats {
+    int count_amr_advance;     /* advances taken, retaken ones included */
+    int count_amr_regrid;      /* regrids called */
+    int count_amr_new_domain;  /* regrids that changed the forest */
+    int global_num_patches;    /* patches at the end */
+    int rejected;              /* steps retaken because max_cfl was exceeded */
+    int steps;                 /* accepted coarse steps */
+    double t_final;
+} fc2d_b200_run_stats_t;
 
 typedef struct fc2d_b200_solver fc2d_b200_solver_t;
 
@@ -145,6 +181,18 @@ int fc2d_b200_advance(fc2d_b200_solver_t* s, double t, double dt, double* maxcfl
 /* fclaw2d_regrid (src/fclaw2d_regrid.c:230-335): device tagging, host tree edit,
  * device repopulation, ghost update.  *changed = 1 if the forest changed. */
 int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed);
+/* patch_vt->save_step / restore_step (fclaw2d_clawpatch.cpp:446-471, called by
+ * save_time_step / restore_time_step of src/fclaw2d_run.c:42-82): a device copy of q
+ * of every patch (ghosts included), and its return.  The forest must not change
+ * in between. */
+int fc2d_b200_save_step(fc2d_b200_solver_t* s);
+int fc2d_b200_restore_step(fc2d_b200_solver_t* s);
+/* fclaw2d_run with outstyle 1 (src/fclaw2d_run.c:113-265) from t = 0 after
+ * fc2d_b200_initialize: nout output intervals up to tfinal, dt from the CFL of the
+ * last step (desired_cfl), a step above max_cfl retaken from the saved copy with a
+ * smaller dt, the last step of an interval stretched or shortened to end on it,
+ * regrid every regrid_interval accepted steps.  *out (may be null) gets the counters. */
+int fc2d_b200_run(fc2d_b200_solver_t* s, fc2d_b200_run_stats_t* out);
 
 /* ---- output: clawpack 4.6 ASCII frames ----
  * fclaw2d_clawpatch_output_ascii (src/patches/clawpatch/fclaw2d_clawpatch_output_ascii.c:112-170,

@@ -75,7 +75,34 @@ typedef struct orc_config {
      * Newton tolerance on p* (relative change); bubble centre/radius in x0, y0, r0 */
     double gamma, mach, rhob, newton_tol;
     int nthreads;          /* OpenMP threads for the patch loops (0 = default) */
+    /* refinement strategy: fclaw_options.c:203-213 (smooth-refine, smooth-level),
+     * fclaw2d_clawpatch_options.c:107-114 (refinement-criteria, threshold-variable) */
+    int smooth_refine, smooth_level;
+    int tag_criteria;      /* ORC_TAG_* */
+    int threshold_variable;   /* 1-based field tested by the criterion (0 = field 1) */
+    /* fclaw2d_run outstyle 1 (fclaw_options.c: tfinal, nout, initial_dt, max_cfl,
+     * desired_cfl, use_fixed_dt, regrid_interval above) */
+    double tfinal, initial_dt, max_cfl, desired_cfl;
+    int nout, use_fixed_dt;
 } orc_config;
+
+/* Tagging criteria: FCLAW_REFINE_CRITERIA_* (fclaw2d_clawpatch_options.h:48-56) + 1;
+ * ORC_TAG_APP keeps each problem's built-in criterion (gradient times dx for the
+ * shallow-water and Euler problems, minmax for the sphere). */
+enum { ORC_TAG_APP = 0, ORC_TAG_VALUE = 1, ORC_TAG_DIFFERENCE = 2, ORC_TAG_MINMAX = 3,
+       ORC_TAG_GRADIENT = 4, ORC_TAG_GRADIENT_DX = 5 };
+
+/* Counters of one fclaw2d_run (fclaw2d_global.h: count_amr_advance, count_amr_regrid,
+ * count_amr_new_domain; src/fclaw2d_finalize.c:119-165 checks three of them). */
+typedef struct orc_run_stats {
+    int count_amr_advance;     /* calls of fclaw2d_advance_all_levels, retaken steps included */
+    int count_amr_regrid;      /* calls of fclaw2d_regrid */
+    int count_amr_new_domain;  /* regrids that changed the forest */
+    int global_num_patches;    /* leaves at the end */
+    int rejected;              /* steps retaken because max_cfl was exceeded */
+    int steps;                 /* accepted coarse steps */
+    double t_final;
+} orc_run_stats;
 
 typedef struct orc_sim orc_sim;
 
@@ -90,6 +117,13 @@ double orc_advance(orc_sim* s, double t, double dt);
 int    orc_regrid(orc_sim* s);
 /* Ghost update over all levels at sync time t (time_interp = 0). */
 void   orc_ghost_update_all(orc_sim* s, double t);
+/* fclaw2d_run outstyle 1 (src/fclaw2d_run.c:113-265) from t = 0 after orc_initialize:
+ * CFL-driven dt, small/big final steps, retake above max_cfl, regrid every
+ * regrid_interval steps.  Returns 0. */
+int    orc_run(orc_sim* s, orc_run_stats* out);
+/* patch_vt->save_step / restore_step (fclaw2d_clawpatch.cpp:446-471): q of every patch. */
+void   orc_save_step(orc_sim* s);
+void   orc_restore_step(orc_sim* s);
 
 int    orc_num_patches(const orc_sim* s);
 /* Patches in level-major order: level, block, ix, iy (integer coordinates at the patch level). */

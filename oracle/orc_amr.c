@@ -116,8 +116,8 @@ static void patch_alloc(orc_sim* s, orc_patch* P)
 
 static void patch_free(orc_patch* P)
 {
-    free(P->q); free(P->qlast); free(P->qinterp); free(P->aux); free(P->regs.mem); free(P->area);
-    P->q = P->qlast = P->qinterp = P->aux = P->area = NULL; P->regs.mem = NULL;
+    free(P->q); free(P->qlast); free(P->qinterp); free(P->aux); free(P->regs.mem); free(P->area); free(P->qsave);
+    P->q = P->qlast = P->qinterp = P->aux = P->area = P->qsave = NULL; P->regs.mem = NULL;
 }
 
 /* clawpatch_define (fclaw2d_clawpatch.cpp:192-...) geometry + time_sync_setup
@@ -710,6 +710,40 @@ static int adapt(orc_sim* s, const int* mark, int domain_init)
     return 1;
 }
 
+/* Refinement smoothing of fclaw2d_domain_adapt (src/fclaw2d_convenience.c:507-645).
+ * The tags set target levels (fclaw2d_patch_mark_refine / _mark_coarsen,
+ * src/forestclaw2d.c:1400-1450: level + 1 / level - 1); each patch then takes the
+ * largest target level among itself and its face and corner neighbours of level
+ * >= smooth_level, looking further only while that maximum does not exceed its
+ * own level, and is marked to refine or coarsen by the sign of the difference. */
+static void smooth_marks(const orc_sim* s, int* mark)
+{
+    const int np = s->np, smooth_level = s->cfg.smooth_level;
+    int* tl = (int*)malloc(sizeof(int) * (size_t)(np > 0 ? np : 1));
+    for (int i = 0; i < np; i++) tl[i] = s->p[i].level + mark[i];
+    for (int i = 0; i < np; i++) {
+        const orc_patch* P = &s->p[i];
+        const int level = P->level;
+        int mt = tl[i];
+        for (int f = 0; mt <= level && f < 4; f++) {
+            const int t = P->face_type[f];
+            if (t == NB_BOUNDARY) continue;
+            const int nn = (t == NB_HALF) ? 2 : 1;
+            for (int k = 0; k < nn; k++) {
+                const int nb = P->face_nbr[f][k];
+                if (s->p[nb].level >= smooth_level && tl[nb] > mt) mt = tl[nb];
+            }
+        }
+        for (int cn = 0; mt <= level && cn < 4; cn++) {
+            if (!P->has_corner[cn]) continue;
+            const int nb = P->corner_nbr[cn];
+            if (s->p[nb].level >= smooth_level && tl[nb] > mt) mt = tl[nb];
+        }
+        mark[i] = (mt < level) ? -1 : (mt > level) ? 1 : 0;
+    }
+    free(tl);
+}
+
 static int regrid_impl(orc_sim* s, int domain_init)
 {
     const orc_config* c = &s->cfg;
@@ -731,6 +765,7 @@ static int regrid_impl(orc_sim* s, int domain_init)
     }
     for (int i = 0; i < s->np; i++)
         if (s->p[i].level < c->maxlevel && orc_tag_refine(s, &s->p[i], domain_init)) mark[i] = 1;
+    if (c->smooth_refine) smooth_marks(s, mark);
     int changed = adapt(s, mark, domain_init);
     free(mark);
     return changed;
@@ -741,6 +776,80 @@ int orc_regrid(orc_sim* s)
     int changed = regrid_impl(s, 0);
     if (changed) ghost_update(s, s->minlevel_present, s->maxlevel_present, 0);
     return changed;
+}
+
+/* ------------------------------------------------------------------------- */
+/* save / restore a step, and the run loop                                     */
+/* ------------------------------------------------------------------------- */
+void orc_save_step(orc_sim* s)
+{
+    for (int i = 0; i < s->np; i++) {
+        orc_patch* P = &s->p[i];
+        if (!P->qsave) P->qsave = (double*)malloc(sizeof(double) * s->nq);
+        memcpy(P->qsave, P->q, sizeof(double) * s->nq);
+    }
+}
+
+void orc_restore_step(orc_sim* s)
+{
+    for (int i = 0; i < s->np; i++)
+        if (s->p[i].qsave) memcpy(s->p[i].q, s->p[i].qsave, sizeof(double) * s->nq);
+}
+
+/* outstyle_1 (src/fclaw2d_run.c:113-265) with reduce_cfl (one process: the global
+ * maximum is the local one) and advance_one_step off. */
+int orc_run(orc_sim* s, orc_run_stats* st)
+{
+    const orc_config* c = &s->cfg;
+    memset(st, 0, sizeof(*st));
+    const double final_time = c->tfinal;
+    const int nout = c->nout > 0 ? c->nout : 1;
+    double dt_minlevel = c->initial_dt;
+    const double t0 = 0;
+    const double dt_outer = (final_time - t0) / ((double)nout);
+    double t_curr = t0;
+    int n_inner = 0;
+    for (int n = 0; n < nout; n++) {
+        const double tstart = t_curr;
+        const double tend = tstart + dt_outer;
+        while (t_curr < tend) {
+            if (!c->use_fixed_dt) orc_save_step(s);
+            double dt_step = dt_minlevel;
+            const double tol = 1e-2 * dt_step;
+            int took_small_step = 0;
+            if (!c->use_fixed_dt) {
+                const double small_step = tend - (t_curr + dt_step);
+                if (small_step < tol) {
+                    dt_step = tend - t_curr;
+                    if (small_step < 0) took_small_step = 1;
+                }
+            }
+            const double maxcfl_step = orc_advance(s, t_curr, dt_step);
+            st->count_amr_advance++;
+            if (maxcfl_step > c->max_cfl) {
+                if (!c->use_fixed_dt) {
+                    orc_restore_step(s);
+                    dt_minlevel = dt_minlevel * c->desired_cfl / maxcfl_step;
+                    st->rejected++;
+                    continue;
+                }
+            }
+            n_inner++;
+            t_curr += dt_step;
+            if (!c->use_fixed_dt) {
+                const double dt_new = dt_minlevel * c->desired_cfl / maxcfl_step;
+                if (!took_small_step) dt_minlevel = dt_new;
+            }
+            if (c->regrid_interval > 0 && n_inner % c->regrid_interval == 0) {
+                if (orc_regrid(s)) st->count_amr_new_domain++;
+                st->count_amr_regrid++;
+            }
+        }
+    }
+    st->steps = n_inner;
+    st->global_num_patches = s->np;
+    st->t_final = t_curr;
+    return 0;
 }
 
 /* ------------------------------------------------------------------------- */

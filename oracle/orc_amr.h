@@ -27,6 +27,7 @@ typedef struct orc_patch {
     int level, block, gx, gy;         /* gx, gy: brick-global integer coords at `level` */
     double xlower, ylower, dx, dy;
     double *q, *qlast, *qinterp, *aux;
+    double* qsave;                    /* save_step copy (allocated on first use) */
     double* area;                     /* cubed sphere: cell areas, -mbc..mx+mbc+1 in both directions */
     orc_regs regs;
     int face_type[4];

@@ -39,7 +39,21 @@ class OrcConfig(ctypes.Structure):
         ("gamma", ctypes.c_double), ("mach", ctypes.c_double), ("rhob", ctypes.c_double),
         ("newton_tol", ctypes.c_double),
         ("nthreads", ctypes.c_int),
+        ("smooth_refine", ctypes.c_int), ("smooth_level", ctypes.c_int),
+        ("tag_criteria", ctypes.c_int), ("threshold_variable", ctypes.c_int),
+        ("tfinal", ctypes.c_double), ("initial_dt", ctypes.c_double),
+        ("max_cfl", ctypes.c_double), ("desired_cfl", ctypes.c_double),
+        ("nout", ctypes.c_int), ("use_fixed_dt", ctypes.c_int),
     ]
+
+
+TAG_APP, TAG_VALUE, TAG_DIFFERENCE, TAG_MINMAX, TAG_GRADIENT, TAG_GRADIENT_DX = 0, 1, 2, 3, 4, 5
+
+
+class OrcRunStats(ctypes.Structure):
+    _fields_ = [("count_amr_advance", ctypes.c_int), ("count_amr_regrid", ctypes.c_int),
+                ("count_amr_new_domain", ctypes.c_int), ("global_num_patches", ctypes.c_int),
+                ("rejected", ctypes.c_int), ("steps", ctypes.c_int), ("t_final", ctypes.c_double)]
 
 
 def build(force: bool = False) -> str:
@@ -72,6 +86,9 @@ def lib():
         L.orc_advance.argtypes = [P, ctypes.c_double, ctypes.c_double]
         L.orc_regrid.argtypes = [P]
         L.orc_ghost_update_all.argtypes = [P, ctypes.c_double]
+        L.orc_run.argtypes = [P, ctypes.POINTER(OrcRunStats)]
+        L.orc_save_step.argtypes = [P]
+        L.orc_restore_step.argtypes = [P]
         L.orc_num_patches.argtypes = [P]
         L.orc_patch_info.argtypes = [P, ip, ip, ip, ip]
         L.orc_get_q.argtypes = [P, dp]
@@ -116,10 +133,12 @@ def make_config(**kw) -> OrcConfig:
     c = OrcConfig()
     defaults = dict(mx=16, my=16, mbc=2, meqn=1, maux=0, mwaves=1, mcapa=0, use_fwaves=0, rp=0,
                     minlevel=0, maxlevel=0, subcycle=0, time_sync=0, flux_correction=1,
-                    fluctuation_correction=1, regrid_interval=0, refine_threshold=0.5,
+                    fluctuation_correction=1, regrid_interval=1, refine_threshold=0.5,
                     coarsen_threshold=0.1, ax=0.0, bx=1.0, ay=0.0, by=1.0, mi=1, mj=1,
                     problem=0, grav=1.0, tperiod=0.0, r0=0.3, hin=2.0, hout=1.0, x0=0.0, y0=0.0,
-                    qinit_sharp=1, gamma=1.4, mach=1.22, rhob=0.138, newton_tol=1e-10, nthreads=0)
+                    qinit_sharp=1, gamma=1.4, mach=1.22, rhob=0.138, newton_tol=1e-10, nthreads=0,
+                    smooth_refine=0, smooth_level=0, tag_criteria=0, threshold_variable=1,
+                    tfinal=0.0, initial_dt=0.0, max_cfl=1.0, desired_cfl=0.9, nout=1, use_fixed_dt=0)
     defaults.update(kw)
     order = defaults.pop("order", (2, 2))
     mthlim = defaults.pop("mthlim", (4,) * 8)
@@ -164,6 +183,18 @@ class OracleSim:
 
     def ghost_update(self, t: float) -> None:
         lib().orc_ghost_update_all(self.h, t)
+
+    def run(self) -> dict:
+        """fclaw2d_run outstyle 1 from t = 0; returns the run's counters."""
+        st = OrcRunStats()
+        lib().orc_run(self.h, ctypes.byref(st))
+        return {k: getattr(st, k) for k, _ in OrcRunStats._fields_}
+
+    def save_step(self) -> None:
+        lib().orc_save_step(self.h)
+
+    def restore_step(self) -> None:
+        lib().orc_restore_step(self.h)
 
     @property
     def num_patches(self) -> int:

@@ -12,7 +12,17 @@ from tests.cases import DAM, make
 
 pytestmark = pytest.mark.gpu
 
-SCRATCH_DOUBLES = 131072
+
+def _scratch_doubles() -> int:
+    """FC2D_B200_MASS_SCRATCH_DOUBLES as the public header declares it."""
+    import os
+    import re
+    hdr = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "fc2d_b200.h")
+    with open(hdr) as f:
+        return int(re.search(r"#define FC2D_B200_MASS_SCRATCH_DOUBLES (\d+)", f.read()).group(1))
+
+
+SCRATCH_DOUBLES = _scratch_doubles()
 
 
 def _solver(**kw):
@@ -35,6 +45,23 @@ def test_mass_noalloc_matches_mass_two_calls_in_a_row():
         c = g.advance(t, dt)
         t += dt
         dt *= 0.9 / c
+    g.close()
+
+
+def test_mass_noalloc_first_and_repeated_calls_leave_device_memory_alone():
+    """On a fresh solver the allocation-free call comes first (before any
+    fc2d_b200_mass, whose buffer would hide an allocation), and free device
+    memory does not change across repeated calls."""
+    import torch
+    g = _solver(mx=16, my=16, minlevel=2, maxlevel=3)
+    dev = g.opts.device
+    first = g.mass_noalloc()
+    free0, _ = torch.cuda.mem_get_info(dev)
+    for _ in range(3):
+        assert np.array_equal(g.mass_noalloc(), first)
+    free1, _ = torch.cuda.mem_get_info(dev)
+    assert free1 == free0
+    assert np.array_equal(first, g.mass())
     g.close()
 
 
