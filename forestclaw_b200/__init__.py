@@ -21,6 +21,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libfc2d_b200.so")
 
 RP_ADVECTION, RP_SW_ROE, RP_SW_FWAVE, RP_EULER_EXACT, RP_ADVECTION_MANIFOLD = 0, 1, 2, 3, 4
+RP_USER = 100   # application __device__ solvers (include/fc2d_b200_user.cuh)
 APP_NONE, APP_SWIRL, APP_RADIALDAM, APP_TSUNAMI, APP_SHOCKBUBBLE, APP_SPHERE = 0, 1, 2, 3, 4, 5
 PREC_FP64, PREC_FP32WAVE = 0, 1
 # refinement criteria: FCLAW_REFINE_CRITERIA_* + 1; TAG_APP = the app's built-in one
@@ -186,12 +187,14 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_get_registers": [P, dp],
         "fc2d_b200_level_update": [P, I, D, D, dp],
         "fc2d_b200_single_step_update": [P, I, I, I, D, D, dp],
+        "fc2d_b200_single_step_update_host": [P, I, I, I, dp, dp, I, I, D, D, dp],
         "fc2d_b200_ghost_update": [P, I, I, D, I],
         "fc2d_b200_timeinterp": [P, I, D],
         "fc2d_b200_time_sync": [P, I, I],
         "fc2d_b200_advance": [P, D, D, dp],
         "fc2d_b200_regrid": [P, ip],
         "fc2d_b200_save_step": [P],
+        "fc2d_b200_set_user_variants": [P, P, I, I, I, I, I],
         "fc2d_b200_restore_step": [P],
         "fc2d_b200_run": [P, ctypes.POINTER(_RunStats)],
         "fc2d_b200_mass": [P, dp],

@@ -95,6 +95,33 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return OUT
 
 
+USER_EXAMPLES = os.path.join(os.path.dirname(HERE), "tests", "user_solvers")
+
+
+def build_user_examples(force: bool = False) -> list:
+    """Compile the application-solver examples of tests/user_solvers (each .cu with its own
+    __device__ solvers, registered through include/fc2d_b200_user.cuh) into lib<name>.so
+    beside its source, linked against libfc2d_b200.so."""
+    out = []
+    if not os.path.isdir(USER_EXAMPLES):
+        return out
+    build(force=force)
+    for name in sorted(os.listdir(USER_EXAMPLES)):
+        if not name.endswith(".cu"):
+            continue
+        src = os.path.join(USER_EXAMPLES, name)
+        so = os.path.join(USER_EXAMPLES, "lib" + name[:-3] + ".so")
+        deps = [src, OUT, os.path.join(INC, "fc2d_b200_user.cuh")] + \
+            [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+        if not force and os.path.exists(so) and os.path.getmtime(so) >= max(os.path.getmtime(d) for d in deps):
+            out.append(so)
+            continue
+        _run([NVCC, *ARCH, "-std=c++17", "-O3", "-fmad=false", "-I", INC, "-I", CSRC, "-Xcompiler", "-fPIC",
+              "-shared", src, "-o", so, "-L", HERE, "-lfc2d_b200", "-Xlinker", "-rpath,$ORIGIN/../../forestclaw_b200"])
+        out.append(so)
+    return out
+
+
 if __name__ == "__main__":
     p = build(force="--force" in sys.argv, verbose="-v" in sys.argv)
     print(p)

@@ -151,6 +151,11 @@ struct fc2d_b200_solver {
     bool initialized = false;
     // single_step_update protocol
     int ss_level = -1, ss_count = 0;
+    // host-data protocol: the caller's patch arrays of the level being buffered
+    struct HostPatch { int slot; double* q; const double* aux; };
+    std::vector<HostPatch> ss_host;
+    double* ss_stage = nullptr;                    // pinned staging of one level's q
+    size_t ss_stage_cap = 0;
     // timing
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -431,6 +436,7 @@ static int update_level(fc2d_b200_solver* s, int level, double t, double dt)
     if (level < 0 || level > 32) return 0;
     const int p0 = f.lev_off[level], np = f.lev_off[level + 1] - p0;
     if (np <= 0) return 0;
+    if (s->vars.empty()) return fail(FC2D_B200_ESTATE, "no update kernel: register the application solver first");
     if (s->n_upd >= fc2d_b200_solver::PCAP) return fail(FC2D_B200_EINVAL, "too many level updates in one advance");
     flush_timeinterp(s);                              // it reads q of levels this update may write
     const int slot = s->n_upd++;
@@ -716,8 +722,11 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
         return fail(FC2D_B200_EINVAL, "exact Euler solver needs meqn 4, mwaves 3, gamma > 1, newton_tol > 0");
     if (o.minlevel < 0 || o.maxlevel < o.minlevel || o.maxlevel > 20)
         return fail(FC2D_B200_EINVAL, "bad minlevel/maxlevel");
-    const bool sup = !step2_variants(o.precision, o.rp, o.mx, o.my, o.mbc).empty();
+    const bool user = o.rp == FC2D_B200_RP_USER;
+    const bool sup = user || !step2_variants(o.precision, o.rp, o.mx, o.my, o.mbc).empty();
     if (!sup) return fail(FC2D_B200_EINVAL, "no compiled update kernel for this (rp, mx, my, mbc, precision)");
+    if (user && (o.precision != FC2D_B200_PREC_FP64 || o.time_sync || o.mx != o.my || o.mbc != 2))
+        return fail(FC2D_B200_EINVAL, "application solvers run in FP64, without time sync, on square patches with mbc 2");
     if (o.app == FC2D_B200_APP_SPHERE &&
         (o.rp != FC2D_B200_RP_ADVECTION_MANIFOLD || o.maux != 3 || o.mcapa != 1 || o.mx != o.my || o.mx < 8))
         return fail(FC2D_B200_EINVAL, "the cubed-sphere app needs the manifold advection solver, maux 3, mcapa 1, "
@@ -774,8 +783,10 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
         s->vars = step2_variants(o.precision, o.rp, o.mx, o.my, o.mbc);
         s->var = 0;
         for (int l = 0; l < 33; l++) s->var_lev[l] = -1;
-        cudaError_t e = s->vars[0]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, LevelGroup{1, {0}}, nullptr, s->st);
-        if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
+        if (!s->vars.empty()) {   // application solvers arrive with fc2d_b200_set_user_variants
+            cudaError_t e = s->vars[0]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, LevelGroup{1, {0}}, nullptr, s->st);
+            if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
+        }
         CK(cudaMalloc(&s->tune_params, sizeof(StepParams)));
     }
     *out = s.release();
@@ -797,6 +808,7 @@ extern "C" int fc2d_b200_destroy(fc2d_b200_solver_t* s)
     cudaFree(s->params_dev); cudaFreeHost(s->params_host);
     if (s->mass_dev) cudaFree(s->mass_dev);
     if (s->qsave) cudaFree(s->qsave);
+    if (s->ss_stage) cudaFreeHost(s->ss_stage);
     cudaFree(s->bc_dev); cudaFree(s->newton_hist);
     if (s->tune_params) cudaFree(s->tune_params);
     if (s->area) cudaFree(s->area);
@@ -819,6 +831,33 @@ extern "C" int fc2d_b200_set_riemann(fc2d_b200_solver_t* s, int rp_id)
     invalidate_graph(s);
     cudaError_t e = s->vars[0]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, LevelGroup{1, {0}}, nullptr, s->st);
     if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
+    return 0;
+}
+
+extern "C" int fc2d_b200_set_user_variants(fc2d_b200_solver_t* s, const void* table, int n, int abi, int meqn,
+                                           int mwaves, int maux)
+{
+    DeviceScope dev_scope_(s);
+    if (!s || !table || n <= 0) return fail(FC2D_B200_EINVAL, "null solver or empty variant table");
+    if (abi != device_abi())
+        return fail(FC2D_B200_EINVAL, "the application was built against another version of the kernel headers");
+    if (s->o.rp != FC2D_B200_RP_USER) return fail(FC2D_B200_EINVAL, "the solver was not created with rp = FC2D_B200_RP_USER");
+    if (meqn != s->o.meqn || mwaves != s->o.mwaves || maux != s->o.maux)
+        return fail(FC2D_B200_EINVAL, "meqn / mwaves / maux of the application solver differ from the options");
+    const Step2Variant* v = static_cast<const Step2Variant*>(table);
+    std::vector<const Step2Variant*> vars;
+    for (int i = 0; i < n; i++) {
+        if (v[i].precision != FC2D_B200_PREC_FP64 || v[i].rp != FC2D_B200_RP_USER || v[i].mx != s->o.mx ||
+            v[i].my != s->o.my || v[i].mbc != s->o.mbc || !v[i].fn)
+            return fail(FC2D_B200_EINVAL, "variant " + std::to_string(i) + " does not fit the solver's patch shape");
+        vars.push_back(&v[i]);
+    }
+    cudaError_t e = vars[0]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, LevelGroup{1, {0}}, nullptr, s->st);
+    if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
+    s->vars = vars;
+    s->var = 0;
+    for (int l = 0; l < 33; l++) s->var_lev[l] = -1;
+    invalidate_graph(s);
     return 0;
 }
 
@@ -1084,6 +1123,71 @@ extern "C" int fc2d_b200_single_step_update(fc2d_b200_solver_t* s, int level, in
     if (total_count != np) return fail(FC2D_B200_ESTATE, "total_count differs from the patch count of the level");
     s->ss_level = -1;
     return fc2d_b200_level_update(s, level, t, dt, cfl);
+}
+
+// The buffering protocol with the patch data in the caller's host arrays.  The last
+// call gathers the level's arrays into pinned staging in slot order, copies them to
+// the level's (contiguous) device slots in one transfer, updates the level and
+// scatters the result back the same way.
+extern "C" int fc2d_b200_single_step_update_host(fc2d_b200_solver_t* s, int level, int gx, int gy, double* q,
+                                                 const double* aux, int iter, int total_count, double t, double dt,
+                                                 double* cfl)
+{
+    DeviceScope dev_scope_(s);
+    if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
+    if (!q) return fail(FC2D_B200_EINVAL, "null patch array");
+    if (!s->insts.empty()) return fail(FC2D_B200_EINVAL, "the host-data protocol drives one forest");
+    if (iter == 0) { s->ss_level = level; s->ss_count = 0; s->ss_host.clear(); }
+    if (level != s->ss_level || iter != s->ss_count) return fail(FC2D_B200_ESTATE, "single_step_update calls out of order");
+    const Forest& f = s->forest;
+    const int slot = f.lookup(0, level, gx, gy);
+    if (slot < 0) return fail(FC2D_B200_EINVAL, "no patch of level " + std::to_string(level) + " at (" +
+                                                     std::to_string(gx) + ", " + std::to_string(gy) + ")");
+    s->ss_host.push_back({slot, q, aux});
+    s->ss_count++;
+    if (cfl) *cfl = 0.0;
+    if (iter + 1 < total_count) return 0;
+    s->ss_level = -1;
+    const int p0 = f.lev_off[level], np = f.lev_off[level + 1] - p0;
+    if (total_count != np || (int)s->ss_host.size() != np)
+        return fail(FC2D_B200_ESTATE, "total_count differs from the patch count of the level");
+    std::vector<char> seen(np, 0);
+    for (const auto& h : s->ss_host) {
+        if (seen[h.slot - p0]) return fail(FC2D_B200_EINVAL, "a patch was handed over twice");
+        seen[h.slot - p0] = 1;
+    }
+    const size_t nq = s->d.nq(), na = s->d.naux();
+    const size_t need = (size_t)np * (nq > na ? nq : na);
+    if (s->ss_stage_cap < need) {
+        if (s->ss_stage) CK(cudaFreeHost(s->ss_stage));
+        s->ss_stage = nullptr;
+        s->ss_stage_cap = 0;
+        CK(cudaMallocHost(&s->ss_stage, need * sizeof(double)));
+        s->ss_stage_cap = need;
+    }
+    CK(cudaStreamSynchronize(s->st));                  // the staging buffer is free
+    if (na > 0 && s->ss_host[0].aux) {
+        for (const auto& h : s->ss_host) {
+            if (!h.aux) return fail(FC2D_B200_EINVAL, "aux given for some patches of the level only");
+            std::memcpy(s->ss_stage + (size_t)(h.slot - p0) * na, h.aux, na * sizeof(double));
+        }
+        CK(cudaMemcpyAsync(s->aux + (size_t)p0 * na, s->ss_stage, (size_t)np * na * sizeof(double),
+                           cudaMemcpyHostToDevice, s->st));
+        CK(cudaStreamSynchronize(s->st));
+        for (const auto& h : s->ss_host)               // keep the host mirror of aux in step
+            std::memcpy(&s->aux_host[(size_t)h.slot * na], h.aux, na * sizeof(double));
+    }
+    for (const auto& h : s->ss_host) std::memcpy(s->ss_stage + (size_t)(h.slot - p0) * nq, h.q, nq * sizeof(double));
+    CK(cudaMemcpyAsync(s->q + (size_t)p0 * nq, s->ss_stage, (size_t)np * nq * sizeof(double), cudaMemcpyHostToDevice,
+                       s->st));
+    int rc = fc2d_b200_level_update(s, level, t, dt, cfl);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(s->ss_stage, s->q + (size_t)p0 * nq, (size_t)np * nq * sizeof(double), cudaMemcpyDeviceToHost,
+                       s->st));
+    CK(cudaStreamSynchronize(s->st));
+    for (const auto& h : s->ss_host) std::memcpy(h.q, s->ss_stage + (size_t)(h.slot - p0) * nq, nq * sizeof(double));
+    s->ss_host.clear();
+    return 0;
 }
 
 extern "C" int fc2d_b200_ghost_update(fc2d_b200_solver_t* s, int minlevel, int maxlevel, double sync_time, int time_interp)
@@ -1463,7 +1567,7 @@ extern "C" int fc2d_b200_run(fc2d_b200_solver_t* s, fc2d_b200_run_stats_t* out)
     const double t0 = 0;
     const double dt_outer = (o.tfinal - t0) / ((double)nout);
     double t_curr = t0;
-    int n_inner = 0;
+    int n_inner = 0, retakes = 0;
     for (int n = 0; n < nout; n++) {
         const double tstart = t_curr;
         const double tend = tstart + dt_outer;
@@ -1481,16 +1585,24 @@ extern "C" int fc2d_b200_run(fc2d_b200_solver_t* s, fc2d_b200_run_stats_t* out)
                     if (small_step < 0) took_small_step = 1;
                 }
             }
+            if (!(dt_step > 0) || !std::isfinite(dt_step))
+                return fail(FC2D_B200_EDEVICE, "fc2d_b200_run: the time step is " + std::to_string(dt_step) +
+                                                   " at t = " + std::to_string(t_curr));
             double maxcfl_step = 0;
             if ((rc = fc2d_b200_advance(s, t_curr, dt_step, &maxcfl_step))) return rc;
             st.count_amr_advance++;
+            if (!std::isfinite(maxcfl_step))
+                return fail(FC2D_B200_EDEVICE, "fc2d_b200_run: non-finite CFL number (negative depth or NaN in q) at t = " +
+                                                   std::to_string(t_curr));
             if (maxcfl_step > o.max_cfl && !o.use_fixed_dt) {
                 // retake the step from the saved copy with a smaller dt
                 if ((rc = fc2d_b200_restore_step(s))) return rc;
+                if (++retakes > 64) return fail(FC2D_B200_EDEVICE, "fc2d_b200_run: 64 retakes of one step");
                 dt_minlevel = dt_minlevel * o.desired_cfl / maxcfl_step;
                 st.rejected++;
                 continue;
             }
+            retakes = 0;
             n_inner++;
             t_curr += dt_step;
             if (!o.use_fixed_dt) {

@@ -36,6 +36,18 @@ namespace fcb {
 
 enum { APP_NONE = 0, APP_SWIRL = 1, APP_RADIALDAM = 2, APP_TSUNAMI = 3, APP_SHOCKBUBBLE = 4 };
 
+// Optional solver hooks.  A solver struct that declares USER_HOOKS = true may also
+// declare HAS_B4STEP2 / HAS_SRC2 with the cell-wise b4step2 / src2 of
+// include/fc2d_b200_user.cuh, and AUX_BOTH = true to receive in rpt2 the aux of
+// both cells beside the interface, cudaclaw's layout (cudaclaw_flux2.cu:682-694):
+// aux1/aux2/aux3[imp * maux + m], imp = 0 for the left cell, 1 for the right.
+template <class RP, class = void>
+struct RPHooks { static constexpr bool B4 = false, SRC = false, AUX_BOTH = false; };
+template <class RP>
+struct RPHooks<RP, std::void_t<decltype(RP::USER_HOOKS)>> {
+    static constexpr bool B4 = RP::HAS_B4STEP2, SRC = RP::HAS_SRC2, AUX_BOTH = RP::AUX_BOTH;
+};
+
 template <class RP, int MX, int MY, int MBC, typename TW, int NT = 0>
 struct Step2Geom {
     static constexpr bool F32 = std::is_same<TW, float>::value;
@@ -168,6 +180,19 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
         }
     }
     __syncthreads();
+    if constexpr (RPHooks<RP>::B4) {
+        // user b4step2, cell by cell over the padded patch (cudaclaw_flux2.cu:111-150):
+        // it may set the cell's aux from its q, position and time
+        for (int c = tid; c < NXY; c += NT) {
+            double qc[MEQN], ac[G::AUXS > 0 ? G::AUXS : 1];
+            for (int m = 0; m < MEQN; m++) qc[m] = Qs[m * NXY + c];
+            for (int a = 0; a < G::AUXS; a++) ac[a] = As[a * NXY + c];
+            RP::b4step2(MBC, MX, MY, MEQN, qc, pd.xlower, pd.ylower, dx, dy, sp.t, dt, G::AUXS, ac,
+                        c % NX - MBC + 1, c / NX - MBC + 1);
+            for (int a = 0; a < G::AUXS; a++) As[a * NXY + c] = ac[a];
+        }
+        __syncthreads();
+    }
 
     const int mcapa = sp.mcapa;
     auto dtdx1d_x = [&](int ic, int jc) -> TW {
@@ -383,14 +408,25 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
                 for (int m = 0; m < MEQN; m++) { am[m] = am[m] + cq[m]; ap[m] = ap[m] - cq[m]; }
             TW qL[MEQN], qR[MEQN];
             for (int m = 0; m < MEQN; m++) { qL[m] = qload(m, cL); qR[m] = qload(m, cR); }
-            TW a1[MA], a2[MA], a3[MA], bm[MEQN], bp[MEQN];
-            for (int a = 0; a < MAUX; a++) { a1[a] = (TW)As[a * NXY + a1c[0]]; a2[a] = (TW)As[a * NXY + a2c[0]]; a3[a] = (TW)As[a * NXY + a3c[0]]; }
+            constexpr bool BOTH = RPHooks<RP>::AUX_BOTH;
+            TW a1[BOTH ? 2 * MA : MA], a2[BOTH ? 2 * MA : MA], a3[BOTH ? 2 * MA : MA], bm[MEQN], bp[MEQN];
+            if constexpr (BOTH) {
+                for (int h = 0; h < 2; h++)
+                    for (int a = 0; a < MAUX; a++) {
+                        a1[h * MA + a] = (TW)As[a * NXY + a1c[h]];
+                        a2[h * MA + a] = (TW)As[a * NXY + a2c[h]];
+                        a3[h * MA + a] = (TW)As[a * NXY + a3c[h]];
+                    }
+            } else {
+                for (int a = 0; a < MAUX; a++) { a1[a] = (TW)As[a * NXY + a1c[0]]; a2[a] = (TW)As[a * NXY + a2c[0]]; a3[a] = (TW)As[a * NXY + a3c[0]]; }
+            }
             RP::template rpt2<TW>(ixy, 1, qL, qR, a1, a2, a3, st.ex, am, bm, bp, gravw, drytolw);
             for (int m = 0; m < MEQN; m++) {
                 Tt[(0 * MEQN + m) * NI + k] = TW(0.5) * dlo * bm[m];
                 Tt[(1 * MEQN + m) * NI + k] = TW(0.5) * dlo * bp[m];
             }
-            for (int a = 0; a < MAUX; a++) { a1[a] = (TW)As[a * NXY + a1c[1]]; a2[a] = (TW)As[a * NXY + a2c[1]]; a3[a] = (TW)As[a * NXY + a3c[1]]; }
+            if constexpr (!BOTH)
+                for (int a = 0; a < MAUX; a++) { a1[a] = (TW)As[a * NXY + a1c[1]]; a2[a] = (TW)As[a * NXY + a2c[1]]; a3[a] = (TW)As[a * NXY + a3c[1]]; }
             RP::template rpt2<TW>(ixy, 2, qL, qR, a1, a2, a3, st.ex, ap, bm, bp, gravw, drytolw);
             for (int m = 0; m < MEQN; m++) {
                 Tt[(2 * MEQN + m) * NI + k] = TW(0.5) * dhi * bm[m];
@@ -635,6 +671,31 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
     }
 
     // ---- q update over i,j = 1-mbc..mx+mbc-1 (clawpack46_step2_wrap.f:107-125) ----
+    if constexpr (RPHooks<RP>::SRC) {
+        // with a user src2 (clawpack46_update, fc2d_clawpack46.cpp:436-441: src2 after
+        // step2), every padded cell gets its updated q (cells the update skips keep
+        // theirs) passed through the cell-wise source term before it is stored
+        for (int c = tid; c < NXY; c += NT) {
+            const int jc = c / NX, ic = c % NX;
+            double qc[MEQN], ac[G::AUXS > 0 ? G::AUXS : 1];
+            for (int m = 0; m < MEQN; m++) {
+                const int b = m * NXY;
+                double v = Qs[b + c];
+                if (ic <= NX - 2 && jc <= NY - 2) {
+                    if (mcapa == 0)
+                        v = v - dtdx * (FMs[b + c + 1] - FPs[b + c]) - dtdy * (GMs[b + c + NX] - GPs[b + c]);
+                    else
+                        v = v - (dtdx * (FMs[b + c + 1] - FPs[b + c]) + dtdy * (GMs[b + c + NX] - GPs[b + c])) /
+                                    As[(mcapa - 1) * NXY + c];
+                }
+                qc[m] = v;
+            }
+            for (int a = 0; a < G::AUXS; a++) ac[a] = As[a * NXY + c];
+            RP::src2(MBC, MX, MY, MEQN, qc, pd.xlower, pd.ylower, dx, dy, sp.t, dt, G::AUXS, ac, ic - MBC + 1,
+                     jc - MBC + 1);
+            for (int m = 0; m < MEQN; m++) qg[m * NXY + c] = qc[m];
+        }
+    } else
     for (int k = tid; k < MEQN * NXY; k += NT) {
         const int m = k / NXY, c = k % NXY;
         const int jc = c / NX, ic = c % NX;

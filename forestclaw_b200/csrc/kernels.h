@@ -50,6 +50,12 @@ struct Step2Variant {
     int persistent;            // 1: a grid of resident CTAs loops over the patches
     Step2Fn fn;
 };
+// Layout version of the kernel parameter structs, checked when an application
+// registers update kernels compiled in its own module (include/fc2d_b200_user.cuh).
+constexpr int device_abi()
+{
+    return 1000000 + 1000 * (int)sizeof(StepParams) + 10 * (int)sizeof(PatchDesc) + (int)(sizeof(LevelGroup) % 10);
+}
 const Step2Variant* step2_table_f64_adv(int* n);
 const Step2Variant* step2_table_f64_sw(int* n);
 const Step2Variant* step2_table_f64_euler(int* n);

@@ -37,6 +37,8 @@ extern "C" {
 #define FC2D_B200_RP_EULER_EXACT 3   /* Euler, exact Riemann solver (Newton on p*) + clawpack46_rpt2_euler4.f transverse */
 #define FC2D_B200_RP_ADVECTION_MANIFOLD 4   /* advection/2d/all/clawpack46_rpn2adv_manifold.f / _rpt2adv_manifold.f
                                                (aux = capacity, x-edge and y-edge normal velocities) */
+#define FC2D_B200_RP_USER      100   /* application __device__ solvers installed by fc2d_b200_set_user_variants
+                                        (include/fc2d_b200_user.cuh); FP64, no time sync */
 
 /* Built-in application callbacks (qinit / setaux / b4step2 / tagging). */
 #define FC2D_B200_APP_NONE       0   /* q and aux supplied by the caller */
@@ -133,6 +135,16 @@ int fc2d_b200_destroy(fc2d_b200_solver_t* s);
  * fc2d_clawpack46.h:161-188; cudaclaw's cuda_rpn2 / cuda_rpt2). */
 int fc2d_b200_set_riemann(fc2d_b200_solver_t* s, int rp_id);
 
+/* Install update kernels an application compiled with its own __device__ rpn2 / rpt2
+ * (and optional b4step2 / src2): the cudaclaw vtable fields cuda_rpn2, cuda_rpt2,
+ * cuda_b4step2 (fc2d_cudaclaw.h:156-162) and clawpack46's src2 (fc2d_clawpack46.h:161-188).
+ * table / n: the variant table the FC2D_B200_USER_SOLVER* macros of
+ * include/fc2d_b200_user.cuh build in the application's module; abi: that header's
+ * FC2D_B200_USER_ABI.  The solver must have rp = FC2D_B200_RP_USER, precision FP64,
+ * time sync off, and the given meqn, mwaves, maux. */
+int fc2d_b200_set_user_variants(fc2d_b200_solver_t* s, const void* table, int n, int abi, int meqn, int mwaves,
+                                int maux);
+
 /* fclaw2d_initialize (src/fclaw2d_initialize.c:75-250): uniform forest at minlevel,
  * setaux + qinit, then the initial-refinement loop.  Needs app != NONE. */
 int fc2d_b200_initialize(fc2d_b200_solver_t* s);
@@ -169,6 +181,18 @@ int fc2d_b200_level_update(fc2d_b200_solver_t* s, int level, double t, double dt
  * happens on the last call, which returns the level CFL in *cfl (0 before). */
 int fc2d_b200_single_step_update(fc2d_b200_solver_t* s, int level, int iter, int total_count,
                                  double t, double dt, double* cfl);
+/* The same protocol for callers whose patch data lives in host arrays, as
+ * ForestClaw's FArrayBoxes do (fclaw2d_clawpatch.hpp:46-81) when its own ghost fill
+ * (fclaw2d_ghost_update on host data) runs between the level updates: each call
+ * hands over one patch of `level` -- its brick-global position gx, gy and its q (and
+ * aux, or NULL to keep the device's) in the FArrayBox layout, ghost cells included.
+ * The last call (iter + 1 == total_count, every patch of the level handed over once,
+ * in any order) copies the arrays into their device slots, updates the level
+ * (clawpack46_update on each patch), writes the new q back into every array and
+ * returns the level CFL.  Time-sync registers stay on the device. */
+int fc2d_b200_single_step_update_host(fc2d_b200_solver_t* s, int level, int gx, int gy, double* q,
+                                      const double* aux, int iter, int total_count, double t, double dt,
+                                      double* cfl);
 
 /* fclaw2d_ghost_update (src/fclaw2d_ghost_fill.c:838-856). */
 int fc2d_b200_ghost_update(fc2d_b200_solver_t* s, int minlevel, int maxlevel, double sync_time, int time_interp);

@@ -32,7 +32,9 @@ enum {
     ORC_RP_SW_ROE = 1,        /* applications/clawpack/shallow/2d/rp/clawpack46_rpn2.f, clawpack46_rpt2.f */
     ORC_RP_SW_FWAVE = 2,      /* applications/clawpack/shallow/2d/rp/rpn2_tsunami.f90, rpt2_tsunami.f90 */
     ORC_RP_EULER_EXACT = 3,   /* build-originated exact Euler solver (no reference counterpart) */
-    ORC_RP_ADVECTION_MANIFOLD = 4   /* applications/clawpack/advection/2d/all/clawpack46_rpn2adv_manifold.f, _rpt2adv_manifold.f */
+    ORC_RP_ADVECTION_MANIFOLD = 4,  /* applications/clawpack/advection/2d/all/clawpack46_rpn2adv_manifold.f, _rpt2adv_manifold.f */
+    ORC_RP_ACOUSTICS = 5      /* applications/cudaclaw/acoustics/2d/radial/user_cuda/rpn2acoustics.cu, rpt2acoustics.cu
+                                 (an application's own device solver; rho, bulk in pdata[24], pdata[25]) */
 };
 
 /* Problem (app) identifiers: qinit/b4step2/setprob of the reference apps. */
@@ -42,7 +44,10 @@ enum {
     ORC_PROB_UNIFORM_SW = 2,  /* radial dam initial data on a uniform grid (same app) */
     ORC_PROB_TSUNAMI = 3,     /* batched bathymetry problem (rpn2_tsunami) */
     ORC_PROB_SHOCKBUBBLE = 4, /* applications/clawpack/euler/2d/shockbubble (Mach-M shock, light bubble) */
-    ORC_PROB_SPHERE = 5       /* applications/clawpack/advection/2d/sphere on the cubed sphere (6 blocks) */
+    ORC_PROB_SPHERE = 5,      /* applications/clawpack/advection/2d/sphere on the cubed sphere (6 blocks) */
+    ORC_PROB_ROTATION = 6,    /* test app of the application-solver interface: b4step2 sets edge velocities
+                                 from a quadratic stream function, q = disc (cell centre) */
+    ORC_PROB_ACOUSTICS = 7    /* test app: pressure disc at rest (cell centre) for ORC_RP_ACOUSTICS */
 };
 
 typedef struct orc_config {
@@ -84,6 +89,10 @@ typedef struct orc_config {
      * desired_cfl, use_fixed_dt, regrid_interval above) */
     double tfinal, initial_dt, max_cfl, desired_cfl;
     int nout, use_fixed_dt;
+    /* src2 after step2 (fc2d_clawpack46.cpp:436-441): 0 none, 1 q(:,:,1) -= dt*rate*q(:,:,1)
+     * over the padded patch (the test source of the application-solver interface) */
+    int src_kind;
+    double src_rate;
 } orc_config;
 
 /* Tagging criteria: FCLAW_REFINE_CRITERIA_* (fclaw2d_clawpatch_options.h:48-56) + 1;

@@ -451,6 +451,11 @@ static double update_level(orc_sim* s, int level, double t, double dt)
             double cfl = orc_step2(c, rpn2, rpt2, work, P->q, P->aux, P->dx, P->dy, dt, fm, fp, gm, gp, P->bcc);
             if (c->time_sync && c->fluctuation_correction)
                 orc_accumulate_waves(s, P, dt, P->dx, P->dy, fp, fm, gp, gm);
+            if (c->src_kind == 1) {
+                /* src2 (clawpack46_update, fc2d_clawpack46.cpp:436-441): linear damping of field 1 */
+                const size_t ncell = (size_t)s->nx * s->ny;
+                for (size_t k = 0; k < ncell; k++) P->q[k] = P->q[k] - dt * c->src_rate * P->q[k];
+            }
             if (cfl > maxcfl) maxcfl = cfl;
         }
         free(work); free(fl);

@@ -279,6 +279,64 @@ static void rpt2_sw_roe(orc_rpctx* ctx, int ixy, int maxm, int meqn, int mwaves,
     }
 }
 
+/* An application's own device solver restated in the 1-D array form: the radial
+ * acoustics pair of applications/cudaclaw/acoustics/2d/radial/user_cuda/rpn2acoustics.cu:30-68
+ * (waves -alpha1 z / alpha1 and alpha2 z / alpha2 with speeds -c, c) and
+ * rpt2acoustics.cu:88-118, with c = sqrt(bulk/rho), z = c rho (setprob_cuda, :10-27).
+ * The left state of interface i is qr(i-1), the right one ql(i). */
+static void acoustics_cz(const orc_rpctx* ctx, double* c, double* z)
+{
+    const double rho = ctx->cfg->pdata[24], bulk = ctx->cfg->pdata[25];
+    *c = sqrt(bulk / rho);
+    *z = *c * rho;
+}
+
+static void rpn2_acoustics(orc_rpctx* ctx, int ixy, int maxm, int meqn, int mwaves, int maux, int mbc, int mx,
+                           const double* ql, const double* qr, const double* auxl, const double* auxr,
+                           double* wave, double* s, double* amdq, double* apdq)
+{
+    (void)mwaves; (void)maux; (void)auxl; (void)auxr;
+    const int L = maxm + 2 * mbc;
+    const int mu = ixy, mv = 3 - ixy;                 /* 0-based: 1 + idir, 2 - idir */
+    double c, z;
+    acoustics_cz(ctx, &c, &z);
+    for (int i = 2 - mbc; i <= mx + mbc; i++) {
+        double qlv[3], qrv[3], w0[3], w1[3];
+        for (int m = 0; m < 3; m++) { qlv[m] = qr[I1(i - 1) + m * L]; qrv[m] = ql[I1(i) + m * L]; }
+        const double s0 = -c, s1 = c;
+        const double d0 = qrv[0] - qlv[0], d1 = qrv[mu] - qlv[mu];
+        const double alpha1 = (-d0 + z * d1) / (2.0 * z);
+        const double alpha2 = (d0 + z * d1) / (2.0 * z);
+        w0[0] = -alpha1 * z; w0[mu] = alpha1; w0[mv] = 0;
+        w1[0] = alpha2 * z;  w1[mu] = alpha2; w1[mv] = 0;
+        s[I1(i)] = s0; s[I1(i) + L] = s1;
+        for (int m = 0; m < meqn; m++) {
+            wave[I1(i) + m * L] = w0[m];
+            wave[I1(i) + m * L + L * meqn] = w1[m];
+            amdq[I1(i) + m * L] = s0 * w0[m];
+            apdq[I1(i) + m * L] = s1 * w1[m];
+        }
+    }
+}
+
+static void rpt2_acoustics(orc_rpctx* ctx, int ixy, int maxm, int meqn, int mwaves, int maux, int mbc, int mx,
+                           const double* ql, const double* qr, const double* aux1, const double* aux2,
+                           const double* aux3, int imp, const double* asdq, double* bmasdq, double* bpasdq)
+{
+    (void)mwaves; (void)maux; (void)ql; (void)qr; (void)aux1; (void)aux2; (void)aux3; (void)imp; (void)meqn;
+    const int L = maxm + 2 * mbc;
+    const int mu = ixy, mv = 3 - ixy;
+    double c, z;
+    acoustics_cz(ctx, &c, &z);
+    for (int i = 2 - mbc; i <= mx + mbc; i++) {
+        const double d0 = asdq[I1(i)], d1 = asdq[I1(i) + mv * L];
+        const double alpha1 = (-d0 + z * d1) / (2.0 * z);
+        const double alpha2 = (d0 + z * d1) / (2.0 * z);
+        bmasdq[I1(i)] = c * alpha1 * z; bmasdq[I1(i) + mu * L] = 0; bmasdq[I1(i) + mv * L] = -c * alpha1;
+        bpasdq[I1(i)] = c * alpha2 * z; bpasdq[I1(i) + mu * L] = 0; bpasdq[I1(i) + mv * L] = c * alpha2;
+    }
+}
+
 void orc_rp_select(int rp, orc_rpn2_t* rpn2, orc_rpt2_t* rpt2)
 {
     switch (rp) {
@@ -287,6 +345,7 @@ void orc_rp_select(int rp, orc_rpn2_t* rpn2, orc_rpt2_t* rpt2)
     case ORC_RP_SW_FWAVE:  *rpn2 = orc_rpn2_fwave; *rpt2 = orc_rpt2_fwave; break;
     case ORC_RP_EULER_EXACT: *rpn2 = orc_rpn2_euler; *rpt2 = orc_rpt2_euler; break;
     case ORC_RP_ADVECTION_MANIFOLD: *rpn2 = rpn2_adv_manifold; *rpt2 = rpt2_adv_manifold; break;
+    case ORC_RP_ACOUSTICS: *rpn2 = rpn2_acoustics; *rpt2 = rpt2_acoustics; break;
     default: *rpn2 = NULL; *rpt2 = NULL; break;
     }
 }

@@ -205,6 +205,22 @@ void orc_qinit(const orc_sim* s, orc_patch* P)
                 P->q[QIDX(i, j, 3, mbc, nx, ny)] = 0.0;
             }
         }
+    } else if (c->problem == ORC_PROB_ROTATION || c->problem == ORC_PROB_ACOUSTICS) {
+        /* a disc of radius r0 at (x0, y0) by the cell centre: q = 1 inside (rotation), or
+         * pressure hin inside and hout outside with the fluid at rest (acoustics) */
+        for (int i = 1 - mbc; i <= mx + mbc; i++) {
+            const double xc = P->xlower + (i - 0.5) * P->dx;
+            for (int j = 1 - mbc; j <= my + mbc; j++) {
+                const double yc = P->ylower + (j - 0.5) * P->dy;
+                const double r2 = (xc - c->x0) * (xc - c->x0) + (yc - c->y0) * (yc - c->y0);
+                const int in = r2 < c->r0 * c->r0;
+                if (c->problem == ORC_PROB_ROTATION) P->q[QIDX(i, j, 1, mbc, nx, ny)] = in ? 1.0 : 0.0;
+                else {
+                    P->q[QIDX(i, j, 1, mbc, nx, ny)] = in ? c->hin : c->hout;
+                    for (int m = 2; m <= meqn; m++) P->q[QIDX(i, j, m, mbc, nx, ny)] = 0.0;
+                }
+            }
+        }
     } else if (c->problem == ORC_PROB_SHOCKBUBBLE) {
         /* shockbubble/user_4.6/qinit.f:24-62: bubble (by cell centre) of density rhob
          * at pressure 1, ambient (1, 0, 0, 1/(gamma-1)), post-shock state where the
@@ -246,10 +262,39 @@ void orc_qinit(const orc_sim* s, orc_patch* P)
     }
 }
 
+/* Test app of the application-solver interface (ORC_PROB_ROTATION): the stream function
+ * psi = omega ((x - 1/2)^2 + (y - 1/2)^2) / 2 and the factor vt = 1 - (t + dt/2)/2, applied
+ * the way applications/cudaclaw/advection/2d/swirl/user_cuda/b4step2.cu:22-45 applies its
+ * own (differences over dy and dx, then times vt); omega = pdata[26]. */
+static double rot_psi(double x, double y, double omega)
+{
+    return omega * ((x - 0.5) * (x - 0.5) + (y - 0.5) * (y - 0.5)) / 2.0;
+}
+
+static void rotation_b4step2(const orc_sim* s, orc_patch* P, double t, double dt)
+{
+    const orc_config* c = &s->cfg;
+    const int mx = c->mx, my = c->my, mbc = c->mbc, nx = s->nx, ny = s->ny;
+    const double omega = c->pdata[26];
+    const double vt = 1.0 - (t + dt / 2.0) / 2.0;
+    for (int j = 1 - mbc; j <= my + mbc; j++)
+        for (int i = 1 - mbc; i <= mx + mbc; i++) {
+            const double xll = P->xlower + (i - 1) * P->dx, yll = P->ylower + (j - 1) * P->dy;
+            const double p1 = rot_psi(xll, yll + P->dy, omega), p2 = rot_psi(xll, yll, omega),
+                         p3 = rot_psi(xll + P->dx, yll, omega);
+            double a0 = (p1 - p2) / P->dy, a1 = -(p3 - p2) / P->dx;
+            a0 = a0 * vt;
+            a1 = a1 * vt;
+            P->aux[QIDX(i, j, 1, mbc, nx, ny)] = a0;
+            P->aux[QIDX(i, j, 2, mbc, nx, ny)] = a1;
+        }
+}
+
 /* swirl b4step2.f:25-36: edge velocities from stream-function differences at t + dt/2. */
 void orc_b4step2(const orc_sim* s, orc_patch* P, double t, double dt)
 {
     const orc_config* c = &s->cfg;
+    if (c->problem == ORC_PROB_ROTATION) { rotation_b4step2(s, P, t, dt); return; }
     if (c->problem != ORC_PROB_SWIRL || c->tperiod == 0.0) return;
     const int mx = c->mx, my = c->my, mbc = c->mbc, nx = s->nx, ny = s->ny;
     const double pi = 4.0 * atan(1.0), pi2 = 2.0 * pi;

@@ -23,9 +23,10 @@ _lib = None
 
 
 def build() -> bool:
-    """Compile the library when the reference tree and nvcc are present; True if it exists."""
-    ref = os.environ.get("FCB_REFERENCE_TREE", "/root/reference")
-    if os.path.isdir(os.path.join(ref, "src", "solvers", "fc2d_cudaclaw")) and shutil.which("make"):
+    """Compile the library when the reference tree (FCB_REFERENCE_TREE) and nvcc are
+    present; True if the library exists.  Without the variable nothing is compiled."""
+    ref = os.environ.get("FCB_REFERENCE_TREE", "")
+    if ref and os.path.isdir(os.path.join(ref, "src", "solvers", "fc2d_cudaclaw")) and shutil.which("make"):
         subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={ref}"], check=True)
     return os.path.exists(LIB)
 

@@ -15,8 +15,9 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "liborc.so")
 
-RP_ADVECTION, RP_SW_ROE, RP_SW_FWAVE, RP_EULER_EXACT, RP_ADVECTION_MANIFOLD = 0, 1, 2, 3, 4
+RP_ADVECTION, RP_SW_ROE, RP_SW_FWAVE, RP_EULER_EXACT, RP_ADVECTION_MANIFOLD, RP_ACOUSTICS = 0, 1, 2, 3, 4, 5
 PROB_SWIRL, PROB_RADIALDAM, PROB_UNIFORM_SW, PROB_TSUNAMI, PROB_SHOCKBUBBLE, PROB_SPHERE = 0, 1, 2, 3, 4, 5
+PROB_ROTATION, PROB_ACOUSTICS = 6, 7
 
 
 class OrcConfig(ctypes.Structure):
@@ -44,6 +45,7 @@ class OrcConfig(ctypes.Structure):
         ("tfinal", ctypes.c_double), ("initial_dt", ctypes.c_double),
         ("max_cfl", ctypes.c_double), ("desired_cfl", ctypes.c_double),
         ("nout", ctypes.c_int), ("use_fixed_dt", ctypes.c_int),
+        ("src_kind", ctypes.c_int), ("src_rate", ctypes.c_double),
     ]
 
 
@@ -138,7 +140,8 @@ def make_config(**kw) -> OrcConfig:
                     problem=0, grav=1.0, tperiod=0.0, r0=0.3, hin=2.0, hout=1.0, x0=0.0, y0=0.0,
                     qinit_sharp=1, gamma=1.4, mach=1.22, rhob=0.138, newton_tol=1e-10, nthreads=0,
                     smooth_refine=0, smooth_level=0, tag_criteria=0, threshold_variable=1,
-                    tfinal=0.0, initial_dt=0.0, max_cfl=1.0, desired_cfl=0.9, nout=1, use_fixed_dt=0)
+                    tfinal=0.0, initial_dt=0.0, max_cfl=1.0, desired_cfl=0.9, nout=1, use_fixed_dt=0,
+                    src_kind=0, src_rate=0.0)
     defaults.update(kw)
     order = defaults.pop("order", (2, 2))
     mthlim = defaults.pop("mthlim", (4,) * 8)

@@ -40,3 +40,27 @@ def test_unsupported_kernel_shape_rejected():
     rc = L.fc2d_b200_create(ctypes.byref(o), ctypes.byref(h))
     assert rc == -1
     assert b"no compiled update kernel" in L.fc2d_b200_last_error()
+
+
+def test_c_binding_compiles_against_public_header(tmp_path):
+    """The C program that plays ForestClaw's single-step caller builds from the
+    public header alone (plain C11, warnings are errors)."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    obj = str(tmp_path / "shim.o")
+    r = subprocess.run(["gcc", "-std=c11", "-Wall", "-Wextra", "-Werror", "-c", "-I", os.path.join(root, "include"),
+                        os.path.join(root, "tests", "c_shim", "shim_protocol.c"), "-o", obj],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+def test_user_solver_modules_register_through_the_abi():
+    """The application-solver examples are built and export their registration
+    functions; the package exports the entry point they call."""
+    from forestclaw_b200 import build
+    libs = build.build_user_examples()
+    assert any(p.endswith("libacoustics_user.so") for p in libs)
+    for p in libs:
+        m = ctypes.CDLL(p)
+        name = os.path.basename(p)[3:-8]          # lib<app>_user.so -> <app>
+        assert hasattr(m, name + "_register_inline")
+    assert hasattr(ctypes.CDLL(fb.LIB_PATH), "fc2d_b200_set_user_variants")
