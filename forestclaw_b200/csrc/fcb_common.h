@@ -59,6 +59,12 @@ struct StepParams {
     unsigned long long* newton_hist;   // Euler: 32-bin histogram of Newton iterations (or null)
     const void* mlp;        // Euler: p*-seed network blob (null: PVRS start)
     const double* inst_dt;  // batch: coarse time step of each instance, dt = this[inst] * (level factor in dt)
+    unsigned int* status;   // device status word: STATUS_* bits or'ed in by the kernels (or null)
 };
+
+// Kernel-side failures reported through the status word (read by the host after a step).
+enum { STATUS_NEWTON = 1,       // exact Euler: Newton did not converge from the seed nor from PVRS
+       STATUS_DEPTH = 2,        // shallow water: negative depth in a patch
+       STATUS_NONFINITE = 4 };  // a non-finite value in q
 
 }  // namespace fcb

@@ -139,6 +139,8 @@ struct fc2d_b200_solver {
     LevelRanges lr[33];
     unsigned long long* cfl_dev = nullptr;
     unsigned long long* cfl_host = nullptr;
+    unsigned int* status_dev = nullptr;            // device status word (STATUS_* bits)
+    unsigned int* status_host = nullptr;           // pinned copy read with the CFL
     double* mass_dev = nullptr;
     int mass_cap = 0;
     double* qsave = nullptr;                       // save_step copy of q
@@ -373,6 +375,7 @@ static StepParams make_params(const fc2d_b200_solver* s, int level, double t, do
     sp.newton_hist = s->newton_hist;
     sp.mlp = s->use_mlp ? s->mlp_blob : nullptr;
     sp.inst_dt = s->insts.empty() ? nullptr : s->inst_dt_dev;
+    sp.status = s->status_dev;
     if (s->o.app == FC2D_B200_APP_SWIRL && s->o.tperiod != 0.0) {
         const double pi = 4.0 * std::atan(1.0), pi2 = 2.0 * pi;
         sp.vt = std::cos(pi2 * (t + dt / 2.0) / s->o.tperiod);
@@ -767,6 +770,9 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
     CK(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
     CK(cudaMalloc(&s->cfl_dev, sizeof(unsigned long long) * FC2D_B200_MAX_INSTANCES));
     CK(cudaMallocHost(&s->cfl_host, sizeof(unsigned long long) * FC2D_B200_MAX_INSTANCES));
+    CK(cudaMalloc(&s->status_dev, sizeof(unsigned int)));
+    CK(cudaMemset(s->status_dev, 0, sizeof(unsigned int)));
+    CK(cudaMallocHost(&s->status_host, sizeof(unsigned int)));
     CK(cudaMalloc(&s->inst_dt_dev, sizeof(double) * FC2D_B200_MAX_INSTANCES));
     CK(cudaMallocHost(&s->inst_dt_host, sizeof(double) * FC2D_B200_MAX_INSTANCES));
     CK(cudaMalloc(&s->params_dev, sizeof(StepParams) * fc2d_b200_solver::PCAP));
@@ -804,6 +810,7 @@ extern "C" int fc2d_b200_destroy(fc2d_b200_solver_t* s)
     if (s->aux) cudaFree(s->aux); cudaFree(s->regs); cudaFree(s->desc);
     free_spare(s);
     cudaFree(s->cfl_dev); cudaFreeHost(s->cfl_host); cudaFree(s->inst_dt_dev); cudaFreeHost(s->inst_dt_host);
+    cudaFree(s->status_dev); cudaFreeHost(s->status_host);
     invalidate_graph(s);
     cudaFree(s->params_dev); cudaFreeHost(s->params_host);
     if (s->mass_dev) cudaFree(s->mass_dev);
@@ -1072,14 +1079,31 @@ extern "C" int fc2d_b200_get_registers(fc2d_b200_solver_t* s, double* r)
 static int begin_cfl(fc2d_b200_solver* s)
 {
     CK(cudaMemsetAsync(s->cfl_dev, 0, sizeof(unsigned long long) * s->ncfl, s->st));
+    CK(cudaMemsetAsync(s->status_dev, 0, sizeof(unsigned int), s->st));
     return 0;
+}
+
+// The kernels' failure reports (device status word) as an error message, or "".
+static std::string status_message(unsigned st)
+{
+    std::string m;
+    if (st & STATUS_NONFINITE) m += "a non-finite value in q; ";
+    if (st & STATUS_DEPTH) m += "negative water depth; ";
+    if (st & STATUS_NEWTON) m += "the exact Riemann solver's Newton iteration on p* converged neither from its seed nor from PVRS; ";
+    if (!m.empty()) m.resize(m.size() - 2);
+    return m;
 }
 
 // Level CFL maximum (over all instances); per instance into cfl_inst if given.
 static int end_cfl(fc2d_b200_solver* s, double* cfl, double* cfl_inst = nullptr)
 {
     CK(cudaMemcpyAsync(s->cfl_host, s->cfl_dev, sizeof(unsigned long long) * s->ncfl, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(s->status_host, s->status_dev, sizeof(unsigned int), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
+    if (*s->status_host) {
+        if (cfl) *cfl = bits_to_double(0x7ff8000000000000ull);
+        return fail(FC2D_B200_EDEVICE, "device status: " + status_message(*s->status_host));
+    }
     double v = 0.0;
     bool bad = false;
     for (int i = 0; i < s->ncfl; i++) {

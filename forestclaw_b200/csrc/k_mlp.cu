@@ -59,7 +59,7 @@ __global__ void k_mlp_targets(const double* __restrict__ prim, int n, double gam
     const double ps = RPEulerExact::pstar(w[0], w[1], w[2], w[3], w[4], w[5], gam, tol, 0.0, it);
     for (int c = 0; c < MLP_IN; c++) X[(size_t)k * MLP_IN + c] = x[c];
     Y[k] = (float)log(ps / pbase);
-    if (iters) iters[k] = it;
+    if (iters) iters[k] = it & 0xff;
 }
 
 // ---- forward + backward of one minibatch ---------------------------------------
@@ -233,7 +233,7 @@ __global__ void k_mlp_newton_iters(const double* __restrict__ prim, const float*
     }
     int it = 0;
     RPEulerExact::pstar(w[0], w[1], w[2], w[3], w[4], w[5], gam, tol, seed, it);
-    iters[k] = it;
+    iters[k] = it & 0xff;
 }
 
 // ---- uniform sample of the normal-direction interfaces of a forest ---------------

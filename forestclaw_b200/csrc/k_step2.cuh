@@ -41,6 +41,11 @@ enum { APP_NONE = 0, APP_SWIRL = 1, APP_RADIALDAM = 2, APP_TSUNAMI = 3, APP_SHOC
 // include/fc2d_b200_user.cuh, and AUX_BOTH = true to receive in rpt2 the aux of
 // both cells beside the interface, cudaclaw's layout (cudaclaw_flux2.cu:682-694):
 // aux1/aux2/aux3[imp * maux + m], imp = 0 for the left cell, 1 for the right.
+// Solvers whose field 0 is a water depth declare DEPTH = true: a negative depth is
+// reported through the status word.
+template <class RP, class = void> struct RPDepth { static constexpr bool value = false; };
+template <class RP> struct RPDepth<RP, std::void_t<decltype(RP::DEPTH)>> { static constexpr bool value = RP::DEPTH; };
+
 template <class RP, class = void>
 struct RPHooks { static constexpr bool B4 = false, SRC = false, AUX_BOTH = false; };
 template <class RP>
@@ -158,13 +163,17 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
     const bool save = sp.save_last && (pd.flags & PATCH_HAS_FINE_NBR);
 
     // ---- stage q (and aux) in shared memory --------------------------------
+    unsigned bad = 0;        // STATUS_* found in this thread's cells
     for (int k = tid; k < MEQN * NXY; k += NT) {
         double v = qg[k];
+        if (!isfinite(v)) bad |= STATUS_NONFINITE;
+        if constexpr (RPDepth<RP>::value) { if (k < NXY && v < 0.0) bad |= STATUS_DEPTH; }
         Qs[k] = v;
         if (F32) Qf[k] = (TW)v;
         if (save) qlast[(size_t)p * MEQN * NXY + k] = v;
         FMs[k] = 0.0; FPs[k] = 0.0; GMs[k] = 0.0; GPs[k] = 0.0;
     }
+    if (bad && sp.status) atomicOr(sp.status, bad);
     if (MAUX > 0) {
         const double* ag = aux + (size_t)p * G::AUXS * NXY;
         if (sp.app == APP_SWIRL) {
@@ -261,8 +270,10 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
                 fL[m] = FLX[m * NXY + cL]; fR[m] = FLX[m * NXY + cR];
             }
             const EulerParams ep{sp.gamma, sp.newton_tol, seed};
-            const int it = RP::solve_mixed(ixy, qL, qR, qL64, qR64, fL, fR, ep, w32, s32, am64, ap64, ex32);
+            const int r = RP::solve_mixed(ixy, qL, qR, qL64, qR64, fL, fR, ep, w32, s32, am64, ap64, ex32);
+            const int it = r & 0xff;
             atomicAdd(&nhist[it < 31 ? it : 31], 1u);
+            if ((r & RP::NEWTON_FAILED) && sp.status) atomicOr(sp.status, (unsigned)STATUS_NEWTON);
             for (int mw = 0; mw < MWAVES; mw++) {
                 st.s[mw] = (TW)s32[mw];
                 for (int m = 0; m < MEQN; m++) st.wave[mw][m] = (TW)w32[mw][m];
@@ -276,8 +287,10 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
             double qL64[MEQN], qR64[MEQN], w64[MWAVES][MEQN], s64[MWAVES], am64[MEQN], ap64[MEQN], ex64[NEXTRA];
             for (int m = 0; m < MEQN; m++) { qL64[m] = Qs[m * NXY + cL]; qR64[m] = Qs[m * NXY + cR]; }
             const EulerParams ep{sp.gamma, sp.newton_tol, seed};
-            const int it = RP::solve64(ixy, qL64, qR64, ep, w64, s64, am64, ap64, ex64);
+            const int r = RP::solve64(ixy, qL64, qR64, ep, w64, s64, am64, ap64, ex64);
+            const int it = r & 0xff;
             atomicAdd(&nhist[it < 31 ? it : 31], 1u);
+            if ((r & RP::NEWTON_FAILED) && sp.status) atomicOr(sp.status, (unsigned)STATUS_NEWTON);
             for (int mw = 0; mw < MWAVES; mw++) {
                 st.s[mw] = (TW)s64[mw];
                 for (int m = 0; m < MEQN; m++) st.wave[mw][m] = (TW)w64[mw][m];

@@ -112,6 +112,7 @@ struct RPAdvectionManifold {
 struct RPShallowRoe {
     static constexpr int MEQN = 3, MWAVES = 3, MAUX = 0, NEXTRA = 3;
     static constexpr bool CONS_FLUX = true, EXACT64 = false;
+    static constexpr bool DEPTH = true;     // field 0 is a depth: negative values are a failure
     // normal flux in direction ixy, FP64 (one division per cell)
     __device__ static void flux64(int ixy, const double* q, double grav, double* f)
     {
@@ -225,6 +226,7 @@ struct RPShallowRoe {
 struct RPShallowFWave {
     static constexpr int MEQN = 3, MWAVES = 3, MAUX = 1, NEXTRA = 1;
     static constexpr bool CONS_FLUX = true, EXACT64 = false;
+    static constexpr bool DEPTH = true;
     // normal flux in direction ixy, FP64 (one division per cell)
     __device__ static void flux64(int ixy, const double* q, double grav, double* f)
     {
@@ -463,20 +465,32 @@ struct RPEulerExact {
             p = ppv > tolpre ? ppv : tolpre;
         }
         if (pl == pr && ul == ur) { iters = 0; return pl; }
-        int it;
-        for (it = 1; it <= 64; it++) {
-            double fl, fdl, fr, fdr;
-            prefun(g1, g4, g5, g6, p, rl, pl, al, fl, fdl);
-            prefun(g1, g4, g5, g6, p, rr, pr, ar, fr, fdr);
-            double pn = p - (fl + fr + du) / (fdl + fdr);
-            if (pn < 0.0) pn = tolpre;
-            const double change = 2.0 * fabs(pn - p) / (pn + p);
-            p = pn;
-            if (change <= tol) break;
+        const bool seeded = seed > 0.0 && isfinite(seed);
+        int it = 0;
+        bool ok = false;
+        for (int pass = 0; pass < (seeded ? 2 : 1) && !ok; pass++) {
+            if (pass == 1) {        // the seed failed: start again from PVRS
+                const double ppv = 0.5 * (pl + pr) - 0.125 * du * (rl + rr) * (al + ar);
+                p = ppv > tolpre ? ppv : tolpre;
+            }
+            for (int k = 1; k <= 64; k++) {
+                double fl, fdl, fr, fdr;
+                prefun(g1, g4, g5, g6, p, rl, pl, al, fl, fdl);
+                prefun(g1, g4, g5, g6, p, rr, pr, ar, fr, fdr);
+                double pn = p - (fl + fr + du) / (fdl + fdr);
+                if (pn < 0.0) pn = tolpre;
+                const double change = 2.0 * fabs(pn - p) / (pn + p);
+                p = pn;
+                it++;
+                if (change <= tol) { ok = true; break; }
+            }
+            ok = ok && isfinite(p);
         }
-        iters = it > 64 ? 64 : it;
+        iters = (it > 64 ? 64 : it) | (ok ? 0 : NEWTON_FAILED);
         return p;
     }
+    // Returned with the iteration count when Newton converged neither from the seed nor from PVRS.
+    static constexpr int NEWTON_FAILED = 0x100;
     // One interface, FP64.  w[mw][m], am/ap in natural component order.
     // Returns the Newton iteration count.
     __device__ static int solve64(int ixy, const double* qL, const double* qR, const EulerParams& ep,
@@ -512,19 +526,31 @@ struct RPEulerExact {
         }
         double fl = 0.0, fr = 0.0, fdl, fdr;
         int it = 0;
+        bool ok = true;
         if (P.pl == P.pr && P.ul == P.ur) {
             // no pressure or normal-velocity jump: p* = p, u* = u exactly (the first
             // Newton step's values, bit for bit), no iteration
             p = P.pl;
         } else {
-            for (it = 1; it <= 64; it++) {
-                prefun(g1, g4, g5, g6, p, P.rl, P.pl, P.al, fl, fdl);
-                prefun(g1, g4, g5, g6, p, P.rr, P.pr, P.ar, fr, fdr);
-                double pn = p - (fl + fr + du) / (fdl + fdr);
-                if (pn < 0.0) pn = tolpre;
-                const double change = 2.0 * fabs(pn - p) / (pn + p);
-                p = pn;
-                if (change <= ep.tol) break;
+            // Newton from the seed; where it does not converge, again from PVRS
+            const bool seeded = ep.seed > 0.0 && isfinite(ep.seed);
+            ok = false;
+            for (int pass = 0; pass < (seeded ? 2 : 1) && !ok; pass++) {
+                if (pass == 1) {
+                    const double ppv = 0.5 * (P.pl + P.pr) - 0.125 * du * (P.rl + P.rr) * (P.al + P.ar);
+                    p = ppv > tolpre ? ppv : tolpre;
+                }
+                for (int k = 1; k <= 64; k++) {
+                    prefun(g1, g4, g5, g6, p, P.rl, P.pl, P.al, fl, fdl);
+                    prefun(g1, g4, g5, g6, p, P.rr, P.pr, P.ar, fr, fdr);
+                    double pn = p - (fl + fr + du) / (fdl + fdr);
+                    if (pn < 0.0) pn = tolpre;
+                    const double change = 2.0 * fabs(pn - p) / (pn + p);
+                    p = pn;
+                    it++;
+                    if (change <= ep.tol) { ok = true; break; }
+                }
+                ok = ok && isfinite(p);
             }
             if (it > 64) it = 64;
         }
@@ -593,7 +619,7 @@ struct RPEulerExact {
         eflux(P.rl, P.ul, P.vl, P.pl, qL[3], flv);
         eflux(P.rr, P.ur, P.vr, P.pr, qR[3], frv);
         for (int k = 0; k < 4; k++) { am[comp[k]] = f0[k] - flv[k]; ap[comp[k]] = frv[k] - f0[k]; }
-        return it;
+        return it | (ok ? 0 : NEWTON_FAILED);
     }
     // FP32-wave form of solve64.  Primitive states, Roe averages, the Newton
     // iteration on p* (only where p or u jumps), star states, the Godunov state and
@@ -631,6 +657,7 @@ struct RPEulerExact {
         const float rr = qR[0], ur = __fdiv_rn(qR[mu], rr), vr = __fdiv_rn(qR[mv], rr), pr = pres(qR);
         const float al = sqrtf(gam * pl / rl), ar = sqrtf(gam * pr / rr);
         int it = 0;
+        bool ok = true;
         float ps, us;
         const bool nojump = (pl == pr && ul == ur);
         if (nojump) {
@@ -650,15 +677,27 @@ struct RPEulerExact {
             }
             const float tol = fmaxf((float)ep.tol, NEWTON_TOL32);
             float fl = 0.0f, fr = 0.0f, fdl, fdr;
-            for (it = 1; it <= 64; it++) {
-                prefun32(g1, g4, g5, g6, p, rl, pl, al, fl, fdl);
-                prefun32(g1, g4, g5, g6, p, rr, pr, ar, fr, fdr);
-                float pn = p - (fl + fr + du) / (fdl + fdr);
-                if (pn < 0.0f) pn = tolpre;
-                const float change = 2.0f * fabsf(pn - p) / (pn + p);
-                p = pn;
-                if (change <= tol) break;
+            // Newton from the seed; where it does not converge, again from PVRS
+            const bool seeded = ep.seed > 0.0 && isfinite(ep.seed);
+            bool conv = false;
+            for (int pass = 0; pass < (seeded ? 2 : 1) && !conv; pass++) {
+                if (pass == 1) {
+                    const float ppv = 0.5f * (pl + pr) - 0.125f * du * (rl + rr) * (al + ar);
+                    p = ppv > tolpre ? ppv : tolpre;
+                }
+                for (int k = 1; k <= 64; k++) {
+                    prefun32(g1, g4, g5, g6, p, rl, pl, al, fl, fdl);
+                    prefun32(g1, g4, g5, g6, p, rr, pr, ar, fr, fdr);
+                    float pn = p - (fl + fr + du) / (fdl + fdr);
+                    if (pn < 0.0f) pn = tolpre;
+                    const float change = 2.0f * fabsf(pn - p) / (pn + p);
+                    p = pn;
+                    it++;
+                    if (change <= tol) { conv = true; break; }
+                }
+                conv = conv && isfinite(p);
             }
+            ok = conv;
             if (it > 64) it = 64;
             ps = p;
             us = 0.5f * (ul + ur) + 0.5f * (fr - fl);
@@ -733,7 +772,7 @@ struct RPEulerExact {
             am[comp[k]] = f - flxL[comp[k]];
             ap[comp[k]] = flxR[comp[k]] - f;
         }
-        return it;
+        return it | (ok ? 0 : NEWTON_FAILED);
     }
     // clawpack46_rpt2_euler4.f:56-94 with the Roe averages of the interface
     template <typename T>

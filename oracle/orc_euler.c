@@ -153,14 +153,26 @@ int orc_euler_star(double gam, const double* wl, const double* wr, double seed, 
          * first Newton step returns bit for bit); no iteration is needed */
         p = pl;
     } else {
-        for (it = 1; it <= 64; it++) {
-            prefun(&E, p, rl, pl, al, &fl, &fdl);
-            prefun(&E, p, rr, pr, ar, &fr, &fdr);
-            double pn = p - (fl + fr + du) / (fdl + fdr);
-            if (pn < 0.0) pn = tolpre;
-            const double change = 2.0 * fabs(pn - p) / (pn + p);
-            p = pn;
-            if (change <= tol) break;
+        /* Newton from the seed; where it does not converge (or leaves the finite
+         * numbers), once more from the PVRS estimate: Newton stays the judge */
+        const int seeded = seed > 0.0 && seed < INFINITY;
+        int ok = 0;
+        for (int pass = 0; pass < (seeded ? 2 : 1) && !ok; pass++) {
+            if (pass == 1) {
+                const double ppv = 0.5 * (pl + pr) - 0.125 * du * (rl + rr) * (al + ar);
+                p = ppv > tolpre ? ppv : tolpre;
+            }
+            for (int k = 1; k <= 64; k++) {
+                prefun(&E, p, rl, pl, al, &fl, &fdl);
+                prefun(&E, p, rr, pr, ar, &fr, &fdr);
+                double pn = p - (fl + fr + du) / (fdl + fdr);
+                if (pn < 0.0) pn = tolpre;
+                const double change = 2.0 * fabs(pn - p) / (pn + p);
+                p = pn;
+                it++;
+                if (change <= tol) { ok = 1; break; }
+            }
+            ok = ok && isfinite(p);
         }
         if (it > 64) it = 64;
     }
