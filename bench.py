@@ -183,8 +183,13 @@ def _initial_dt(wl: dict, prob) -> float:
     return 0.9 * dx / (2.0 ** 0.5 * 1.5)
 
 
-def cpu_sample(wl: dict, precision: str, max_seconds: float = 20.0, threads: int = 0):
-    """Time the FP64 CPU oracle on the workload's initial forest for a bounded number of steps."""
+def cpu_sample(wl: dict, precision: str, max_seconds: float = 20.0, threads: int = 0, steps: int = 200,
+               warmup: int = 0):
+    """The FP64 CPU oracle on the workload after the GPU arm's spin-up protocol (spinup
+    coarse steps with a regrid every regrid_interval, untimed), then `warmup` untimed and
+    up to `steps` timed coarse steps on the spun-up forest, stopping early once
+    max_seconds of timed work are done.  Timed: fclaw2d_advance_all_levels only; the
+    regrids between timed steps are excluded, as in the GPU arm."""
     from oracle import pyoracle as po
     from tests.cases import DAM, SHOCKBUBBLE, SWIRL, make
     from tests.cases import SPHERE
@@ -197,26 +202,47 @@ def cpu_sample(wl: dict, precision: str, max_seconds: float = 20.0, threads: int
     oc, _ = make(case, nthreads=threads, **kw)
     s = po.OracleSim(oc)
     s.initialize()
-    dt = _initial_dt(wl, prob)
-    t, steps = 0.0, 0
-    c0 = s.cell_updates
-    t0 = time.perf_counter()
-    while True:
+    adapt = wl.get("adapt_dt", wl["time_sync"])
+    ri = wl["regrid_interval"]
+    t, dt = 0.0, _initial_dt(wl, prob)
+    ts0 = time.perf_counter()
+    for n in range(wl["spinup"]):
         cfl = s.advance(t, dt)
         t += dt
-        steps += 1
-        if wl.get("adapt_dt", wl["time_sync"]):
+        if adapt:
             dt *= 0.9 / cfl
-        if time.perf_counter() - t0 > max_seconds or steps >= 200:
+        if ri and (n + 1) % ri == 0:
+            s.regrid()
+    for _ in range(warmup):
+        cfl = s.advance(t, dt)
+        t += dt
+        if adapt:
+            dt *= 0.9 / cfl
+    spin_s = time.perf_counter() - ts0
+    step_s, cells = [], 0.0
+    for k in range(steps):
+        c0 = s.cell_updates
+        t0 = time.perf_counter()
+        cfl = s.advance(t, dt)
+        step_s.append(time.perf_counter() - t0)
+        cells += s.cell_updates - c0
+        t += dt
+        if adapt:
+            dt *= 0.9 / cfl
+        if sum(step_s) > max_seconds:
             break
-    el = time.perf_counter() - t0
-    cells = s.cell_updates - c0
+        if ri and (k + 1) % ri == 0:
+            s.regrid()
+    el = sum(step_s)
     ncores = threads or os.cpu_count()
     return {"value": cells / el, "unit": "cell-updates/s", "cores": ncores, "kind": "port",
-            "sample": f"{steps} coarse steps of {wl['name']}"
+            "ms_per_step": 1e3 * el / len(step_s), "steps_timed": len(step_s),
+            "sample": f"{len(step_s)} timed coarse steps of {wl['name']}"
                       + (f" with maxlevel {wl['cpu_maxlevel']} (the host metric at the full maxlevel is too slow)"
-                         if "cpu_maxlevel" in wl else "") + " from the initial refinement "
-                      f"({s.num_patches} patches, {cells:.3e} cell updates, {el:.1f} s, FP64 C oracle, OpenMP)"}
+                         if "cpu_maxlevel" in wl else "")
+                      + f" after the GPU arm's spin-up ({wl['spinup']} steps, regrid every {ri}; {spin_s:.1f} s, "
+                        f"untimed), regrid between timed steps excluded ({s.num_patches} patches at the end, "
+                        f"{cells:.3e} cell updates in {el:.1f} s, FP64 C oracle, OpenMP)"}
 
 
 def run_reference(args, wl, rank, world):
@@ -224,11 +250,15 @@ def run_reference(args, wl, rank, world):
         return 0
     if wl.get("batch"):
         cpu = cpu_sample_batch(wl, max_seconds=max(5.0, 25.0 / max(args.steps, 1)), threads=0)
+        steps, ms = args.steps, None
     else:
-        cpu = cpu_sample(wl, args.precision, max_seconds=max(5.0, 25.0 / max(args.steps, 1)), threads=0)
+        # the same forest protocol as the GPU arm, bounded to ~90 s of timed CPU work
+        cpu = cpu_sample(wl, args.precision, max_seconds=90.0, threads=0, steps=args.steps, warmup=args.warmup)
+        steps, ms = cpu["steps_timed"], cpu["ms_per_step"]
     line = {
         "metric": "cell-updates/s", "value": cpu["value"], "unit": "cell-updates/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+        "steps": steps, "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": wl["name"], "l2": "n/a (CPU)"}, "impl": "reference",
         "cpu_baseline": cpu,
@@ -306,6 +336,50 @@ def error_vs_fp64(wl, prob, device, mlp, steps=8):
         out.append(float(np.abs(qa[:, m] - qb[:, m]).sum() / den))
     return {"steps": steps, "l1_rel_per_field": out,
             "normalisation": "sum |q_m| per field; momenta by the sum of the density (depth)"}
+
+
+def error_vs_oracle(wl, prob, device, mlp, steps=8):
+    """Per-field error of the FP32-wave run against the FP64 CPU oracle from the same
+    initial forest: `steps` coarse steps with the oracle's CFL setting both dt
+    schedules, no regrid.  Relative L1 = sum |dq| area / sum |q| area and relative
+    Linf = max |dq| / max |q| over interior cells (momenta normalised by the depth or
+    density, which vanish nowhere), and the relative difference of the mass (field 0)."""
+    import forestclaw_b200 as fb
+    from forestclaw_b200 import problems
+    from oracle import pyoracle as po
+    from tests.cases import DAM, SHOCKBUBBLE, make
+    case = SHOCKBUBBLE if wl["name"].startswith("euler") else DAM
+    kw = {k: wl[k] for k in ("mx", "my", "minlevel", "maxlevel", "subcycle", "time_sync")}
+    oc, _ = make(case, **kw)
+    o = po.OracleSim(oc)
+    o.initialize()
+    b = fb.Solver(problems.options(prob, device=device, precision=fb.PREC_FP32WAVE, **kw))
+    b.initialize()
+    if mlp is not None:
+        b.set_pstar_seed(mlp)
+    t, dt = 0.0, _initial_dt(wl, prob)
+    for _ in range(steps):
+        co = o.advance(t, dt)
+        b.advance(t, dt)
+        t += dt
+        dt *= 0.9 / co
+    qo, qb = o.get_q()[:, :, 2:-2, 2:-2], b.get_q()[:, :, 2:-2, 2:-2]
+    mo, mb = o.mass(), b.mass()
+    lev = o.patch_info()[:, 0]
+    b.close()
+    area = ((prob["bx"] - prob["ax"]) / (wl["mx"] * (prob.get("mi", 1) * 2.0 ** lev))) * \
+           ((prob["by"] - prob["ay"]) / (wl["my"] * (prob.get("mj", 1) * 2.0 ** lev)))
+    w = area[:, None, None]
+    l1, linf = [], []
+    for m in range(qo.shape[1]):
+        mom = qo.shape[1] >= 3 and m in (1, 2)
+        ref = qo[:, 0 if mom else m]
+        d = np.abs(qo[:, m] - qb[:, m])
+        l1.append(float((d * w).sum() / (np.abs(ref) * w).sum()))
+        linf.append(float(d.max() / np.abs(ref).max()))
+    return {"against": "FP64 CPU oracle", "steps": steps, "patches": int(len(lev)), "l1_rel_per_field": l1,
+            "linf_rel_per_field": linf, "mass_rel_diff": float(abs(mb[0] - mo[0]) / abs(mo[0])),
+            "normalisation": "per field sum |q_m| area (L1) and max |q_m| (Linf); momenta by the depth/density"}
 
 
 def _spinup(g, wl, t, dt, steps):
@@ -427,6 +501,7 @@ def _bracket():
 
 
 def run_ours(args, wl, rank, world, local_rank):
+    """The measurement of one single-forest workload; the JSON dict on rank 0, else None."""
     import torch
     import forestclaw_b200 as fb
     if wl.get("batch"):
@@ -464,26 +539,41 @@ def run_ours(args, wl, rank, world, local_rank):
     t += nroof * dt
     from forestclaw_b200 import ranks
     total_ms, cells_all, value = ranks.aggregate(float(np.sum(step_ms)), cells, "cuda")
-    # ---- end to end through the C ABI with pinned host buffers ----
-    nq = g.num_patches * gc.meqn * (gc.mx + 2 * gc.mbc) * (gc.my + 2 * gc.mbc)
-    hq = torch.empty(nq, dtype=torch.float64, pin_memory=True)
+    # ---- end to end through the C ABI with pinned host buffers, regrids included ----
+    per_patch = gc.meqn * (gc.mx + 2 * gc.mbc) * (gc.my + 2 * gc.mbc)
+    cap = 2 * g.num_patches * per_patch
+    hq = torch.empty(cap, dtype=torch.float64, pin_memory=True)
     g.get_q_ptr(hq.data_ptr())
-    e2e_steps = max(2, min(args.steps, 10))
+    e2e_steps = max(2 * max(wl["regrid_interval"], 1), min(args.steps, 40))
     torch.cuda.synchronize()
     te0 = time.perf_counter()
-    e2e_cells = 0.0
-    for _ in range(e2e_steps):
+    e2e_cells, e2e_bytes, e2e_regrids = 0.0, 0.0, 0
+    for k in range(e2e_steps):
         c0 = g.cell_updates
+        nq = g.num_patches * per_patch
+        if nq > cap:                       # the forest outgrew the pinned buffer
+            cap = 2 * nq
+            hq = torch.empty(cap, dtype=torch.float64, pin_memory=True)
         g.set_q_ptr(hq.data_ptr())
-        g.advance(t, dt)
+        cfl = g.advance(t, dt)
         g.get_q_ptr(hq.data_ptr())
         e2e_cells += g.cell_updates - c0
+        e2e_bytes += nq * 8
         t += dt
+        if wl.get("adapt_dt", wl["time_sync"]):
+            dt *= 0.9 / cfl
+        if wl["regrid_interval"] and (k + 1) % wl["regrid_interval"] == 0:
+            g.regrid()
+            e2e_regrids += 1
     e2e_s = time.perf_counter() - te0
     e2e_s = ranks.max_over_ranks(e2e_s, "cuda")
     e2e_cells = ranks.sum_over_ranks(e2e_cells, "cuda")
-    e2e = {"value": e2e_cells / e2e_s, "unit": "cell-updates/s", "h2d_bytes_per_step": nq * 8,
-           "d2h_bytes_per_step": nq * 8}
+    e2e = {"value": e2e_cells / e2e_s, "unit": "cell-updates/s",
+           "h2d_bytes_per_step": int(e2e_bytes / e2e_steps), "d2h_bytes_per_step": int(e2e_bytes / e2e_steps),
+           "steps": e2e_steps, "regrids": e2e_regrids,
+           "protocol": "per coarse step: set_q from pinned host memory, advance, get_q to pinned host memory; "
+                       "the workload's regrid (host tree edit, device repopulation, graph recapture) inside "
+                       "the wall-clock region"}
     newton = None
     if wl["name"].startswith("euler"):
         h = g.newton_histogram()
@@ -496,12 +586,17 @@ def run_ours(args, wl, rank, world, local_rank):
         fp64 = _fp64_kernel_arm(args, wl, prob, local_rank, flush)
         fp64["speedup"] = value / fp64["value"] if world == 1 else None
     if rank != 0:
-        return 0
+        return None
     bpc = 8 * (2 * gc.meqn + gc.maux)
     traffic = _traffic_per_launch(wl, args.precision, upd_bytes / max(upd_launches, 1) / bpc)
     roofline = _roofline_dict(upd_ms, upd_bytes, upd_launches, traffic, bpc)
-    cpu = cpu_sample(wl, args.precision, max_seconds=args.cpu_seconds) if args.cpu_seconds > 0 else None
-    err = error_vs_fp64(wl, prob, local_rank, mlp) if args.precision == "fp32wave" else None
+    cpu = (cpu_sample(wl, args.precision, max_seconds=args.cpu_seconds, steps=args.steps)
+           if args.cpu_seconds > 0 else None)
+    err = None
+    if args.precision == "fp32wave":
+        oracle_ok = wl["name"].startswith(("radialdam", "euler"))
+        err = (error_vs_oracle(wl, prob, local_rank, mlp) if oracle_ok
+               else error_vs_fp64(wl, prob, local_rank, mlp))
     line = {
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
@@ -518,11 +613,10 @@ def run_ours(args, wl, rank, world, local_rank):
                    "regrid_ms_median": float(np.median(regrid_ms + timed_regrid_ms)) if regrid_ms else None,
                    "patch_to_cta": tune},
         "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
-        "fp64_kernel": fp64, "error_vs_fp64": err, "newton": newton,
-        "gpu_launches": launches, "update_launches": upd_launches,
+        "fp64_kernel": fp64, ("error_vs_oracle" if err and "against" in err else "error_vs_fp64"): err,
+        "newton": newton, "gpu_launches": launches, "update_launches": upd_launches,
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def _batch_groups(precision, device, n=64, seed=None):
@@ -725,7 +819,7 @@ def run_batch(args, wl, rank, world, local_rank):
         for G in g64:
             G["g"].close()
     if rank != 0:
-        return 0
+        return None
     roofline = _roofline_dict(upd_ms, upd_bytes, upd_launches, None, 8 * (2 * 3 + 1))
     cpu = cpu_sample_batch(wl, max_seconds=args.cpu_seconds) if args.cpu_seconds > 0 else None
     err = _batch_error(local_rank, wl["instances"]) if args.precision == "fp32wave" else None
@@ -749,8 +843,7 @@ def run_batch(args, wl, rank, world, local_rank):
         "fp64_kernel": fp64, "error_vs_fp64": err,
         "gpu_launches": r["launches"], "update_launches": upd_launches,
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def launch_profile(args, wl):
@@ -780,7 +873,7 @@ def launch_profile(args, wl):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="dam", choices=sorted(WORKLOADS))
@@ -793,6 +886,9 @@ def main():
                     help="Euler: Newton start of the exact solver (mlp: trained on the FP64 run first)")
     ap.add_argument("--mlp-samples", type=int, default=1_000_000)
     ap.add_argument("--mlp-epochs", type=int, default=20)
+    ap.add_argument("--no-secondary", dest="secondary", action="store_false",
+                    help="skip the second measurement (shock-bubble with the learned p* start) of the default line")
+    ap.add_argument("--secondary-steps", type=int, default=20)
     ap.add_argument("--launch-profile", action="store_true",
                     help="profiling aid, no timing: spin up the workload, run --steps coarse steps, print the "
                          "patches per level and the launches of the last step (for an ncu launch list)")
@@ -811,7 +907,17 @@ def main():
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        return run_ours(args, wl, rank, world, local_rank)
+        line = run_ours(args, wl, rank, world, local_rank)
+        if args.secondary and args.workload == "dam" and world == 1:
+            # the Euler configuration with the learned p* start, as a second key of the line
+            sargs = argparse.Namespace(**vars(args))
+            sargs.steps, sargs.pstar, sargs.cpu_seconds = args.secondary_steps, "mlp", min(args.cpu_seconds, 10.0)
+            sec = run_ours(sargs, WORKLOADS["shockbubble"], rank, world, local_rank)
+            if line is not None and sec is not None:
+                line["secondary"] = {"shockbubble_mlp": sec}
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return 0
     finally:
         if world > 1:
             import torch

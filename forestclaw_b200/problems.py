@@ -112,7 +112,8 @@ def tsunami_instances(n: int = 64, base_seed: int = 0, mx: int | None = None):
     generator (seed base_seed + k) minlevel in {2, 3, 4}, maxlevel in minlevel+1..8
     (at most 5..8), the bathymetry centre in [-0.5, 0.5]^2 and 1 to 3 Gaussian
     humps of amplitude U[0.05, 0.3], width U[0.05, 0.2] and centre in [-1, 1]^2.
-    Returns (instances, patch sizes): the patch size alternates 8, 16 unless mx is given."""
+    Returns (instances, patch sizes): the patch size (8 or 16) is the instance's last
+    draw unless mx is given."""
     out, sizes = [], []
     for k in range(n):
         g = _Xoshiro256ss(base_seed + k)
@@ -124,5 +125,6 @@ def tsunami_instances(n: int = 64, base_seed: int = 0, mx: int | None = None):
         for _ in range(nb):
             pd += [g.uniform(0.05, 0.3), g.uniform(0.05, 0.2), g.uniform(-1.0, 1.0), g.uniform(-1.0, 1.0)]
         out.append(dict(minlevel=lo, maxlevel=hi, ax=-1.0, bx=1.0, ay=-1.0, by=1.0, mi=1, mj=1, pdata=tuple(pd)))
-        sizes.append(mx if mx is not None else (8 if k % 2 == 0 else 16))
+        size = g.choice((8, 16))
+        sizes.append(mx if mx is not None else size)
     return out, sizes
