@@ -547,7 +547,7 @@ def run_ours(args, wl, rank, world, local_rank):
     e2e_steps = max(2 * max(wl["regrid_interval"], 1), min(args.steps, 40))
     torch.cuda.synchronize()
     te0 = time.perf_counter()
-    e2e_cells, e2e_bytes, e2e_regrids = 0.0, 0.0, 0
+    e2e_cells, e2e_h2d, e2e_d2h, e2e_regrids = 0.0, 0.0, 0.0, 0
     for k in range(e2e_steps):
         c0 = g.cell_updates
         nq = g.num_patches * per_patch
@@ -558,18 +558,26 @@ def run_ours(args, wl, rank, world, local_rank):
         cfl = g.advance(t, dt)
         g.get_q_ptr(hq.data_ptr())
         e2e_cells += g.cell_updates - c0
-        e2e_bytes += nq * 8
+        e2e_h2d += nq * 8
+        e2e_d2h += nq * 8
         t += dt
         if wl.get("adapt_dt", wl["time_sync"]):
             dt *= 0.9 / cfl
         if wl["regrid_interval"] and (k + 1) % wl["regrid_interval"] == 0:
             g.regrid()
             e2e_regrids += 1
+            # the new forest's data back to the host copy (counted with the step's d2h bytes)
+            nq = g.num_patches * per_patch
+            if nq > cap:
+                cap = 2 * nq
+                hq = torch.empty(cap, dtype=torch.float64, pin_memory=True)
+            g.get_q_ptr(hq.data_ptr())
+            e2e_d2h += nq * 8
     e2e_s = time.perf_counter() - te0
     e2e_s = ranks.max_over_ranks(e2e_s, "cuda")
     e2e_cells = ranks.sum_over_ranks(e2e_cells, "cuda")
     e2e = {"value": e2e_cells / e2e_s, "unit": "cell-updates/s",
-           "h2d_bytes_per_step": int(e2e_bytes / e2e_steps), "d2h_bytes_per_step": int(e2e_bytes / e2e_steps),
+           "h2d_bytes_per_step": int(e2e_h2d / e2e_steps), "d2h_bytes_per_step": int(e2e_d2h / e2e_steps),
            "steps": e2e_steps, "regrids": e2e_regrids,
            "protocol": "per coarse step: set_q from pinned host memory, advance, get_q to pinned host memory; "
                        "the workload's regrid (host tree edit, device repopulation, graph recapture) inside "

@@ -195,6 +195,11 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_regrid": [P, ip],
         "fc2d_b200_save_step": [P],
         "fc2d_b200_set_user_variants": [P, P, I, I, I, I, I],
+        "fc2d_b200_set_partition": [P, P],
+        "fc2d_b200_partition_owner": [P, ip],
+        "fc2d_b200_sync_replicas": [P],
+        "fc2d_b200_partition_plan": [ctypes.POINTER(_Options), I, ip, ip, ip, I, I, ip, ip, ip,
+                                     ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong)],
         "fc2d_b200_restore_step": [P],
         "fc2d_b200_run": [P, ctypes.POINTER(_RunStats)],
         "fc2d_b200_mass": [P, dp],
@@ -519,6 +524,15 @@ class Solver:
         st = _RunStats()
         self._check("fc2d_b200_run", self.lib.fc2d_b200_run(self.h, ctypes.byref(st)))
         return {k: getattr(st, k) for k, _ in _RunStats._fields_}
+
+    def partition_owner(self) -> np.ndarray:
+        out = np.zeros(self.num_patches, np.int32)
+        self._check("fc2d_b200_partition_owner", self.lib.fc2d_b200_partition_owner(self.h, _ip(out)))
+        return out
+
+    def sync_replicas(self) -> None:
+        """Every rank of a partitioned forest gets every patch's current data."""
+        self._check("fc2d_b200_sync_replicas", self.lib.fc2d_b200_sync_replicas(self.h))
 
     def mass(self) -> np.ndarray:
         out = np.zeros(self.opts.meqn, np.float64)

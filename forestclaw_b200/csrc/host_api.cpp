@@ -143,6 +143,18 @@ struct fc2d_b200_solver {
     unsigned int* status_host = nullptr;           // pinned copy read with the CFL
     double* mass_dev = nullptr;
     int mass_cap = 0;
+    // one forest partitioned over ranks (fc2d_b200_set_partition); null: one rank
+    struct PartState {
+        fc2d_b200_comm_t comm{};
+        PartitionPlan plan;
+        DevVec<int> slots;                         // halo send slots, then halo recv slots
+        size_t nsend = 0, nrecv = 0;
+        double* buf = nullptr;                     // packed send segments, then recv segments
+        size_t buf_cap = 0;
+        bool graphs_before = true;
+        bool failed = false;                       // an exchange inside an advance failed
+    };
+    std::unique_ptr<PartState> part;
     double* qsave = nullptr;                       // save_step copy of q
     size_t qsave_n = 0;                            // doubles it holds (0: nothing saved)
     size_t qsave_cap = 0;
@@ -286,6 +298,43 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
         std::string err;
         if (!build_tables(f, s->o.mthbc, s->has_inflow, T, err)) return fail(FC2D_B200_EFOREST, err);
     }
+    if (s->part) {
+        // partitioned: a new plan for this forest; the ghost-fill stages write only the
+        // ghost cells of owned and ring-1 patches, interpolation and the time sync only
+        // those of owned patches
+        auto& P = *s->part;
+        make_partition(f, P.comm.rank, P.comm.size, P.plan);
+        const std::vector<char>& fill = P.plan.fill;
+        const std::vector<int>& own = P.plan.owner;
+        const int me = P.comm.rank, nq = s->d.nq();
+        for (LevelTables& L : T) {
+            auto keep = [&](int dst) { return fill[dst / nq] != 0; };
+            auto mine = [&](int dst) { return own[dst / nq] == me; };
+            L.copy.erase(std::remove_if(L.copy.begin(), L.copy.end(), [&](const CopyEnt& e) { return !keep(e.dst); }), L.copy.end());
+            L.avg.erase(std::remove_if(L.avg.begin(), L.avg.end(), [&](const AvgEnt& e) { return !keep(e.dst); }), L.avg.end());
+            L.phys.erase(std::remove_if(L.phys.begin(), L.phys.end(), [&](const PhysEnt& e) { return !keep(e.dst); }), L.phys.end());
+            L.interp.erase(std::remove_if(L.interp.begin(), L.interp.end(), [&](const InterpEnt& e) { return !mine(e.dst); }), L.interp.end());
+            L.ti.erase(std::remove_if(L.ti.begin(), L.ti.end(), [&](int p) { return !fill[p]; }), L.ti.end());
+            std::vector<SyncOp> ops;
+            std::vector<int> start{0};
+            for (size_t g = 0; g + 1 < L.sync_start.size(); g++) {
+                const int a = L.sync_start[g], b = L.sync_start[g + 1];
+                if (b > a && own[L.sync[a].p] == me) {
+                    ops.insert(ops.end(), L.sync.begin() + a, L.sync.begin() + b);
+                    start.push_back((int)ops.size());
+                }
+            }
+            L.sync.swap(ops);
+            L.sync_start.swap(start);
+        }
+        // halo slot lists (send, then receive), uploaded once per forest
+        std::vector<int> slots;
+        for (const auto& v : P.plan.send) slots.insert(slots.end(), v.begin(), v.end());
+        P.nsend = slots.size();
+        for (const auto& v : P.plan.recv) slots.insert(slots.end(), v.begin(), v.end());
+        P.nrecv = slots.size() - P.nsend;
+        if (!slots.empty()) CK(P.slots.assign(slots, s->st));
+    }
     std::vector<CopyEnt> copy;
     std::vector<AvgEnt> avg;
     std::vector<InterpEnt> interp;
@@ -417,7 +466,8 @@ static int flush_updates(fc2d_b200_solver* s)
     if (s->timing) { e0 = next_event(s); e1 = next_event(s); CK(cudaEventRecord(e0, s->st)); }
     LevelGroup lg{};
     lg.nlev = g.lev_hi - g.lev_lo + 1;
-    for (int i = 0; i < lg.nlev; i++) lg.start[i] = s->forest.lev_off[g.lev_lo + i] - g.p0;
+    for (int i = 0; i < lg.nlev; i++)
+        lg.start[i] = (s->part ? s->part->plan.own_lo[g.lev_lo + i] : s->forest.lev_off[g.lev_lo + i]) - g.p0;
     cudaError_t e = s->vars[g.var]->fn(s->q, s->qlast, s->aux, s->regs, s->desc, g.p0, g.np, s->params_dev + g.slot,
                                        lg, s->cfl_dev, s->st);
     if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("step2 launch: ") + cudaGetErrorString(e));
@@ -437,7 +487,8 @@ static int update_level(fc2d_b200_solver* s, int level, double t, double dt)
 {
     const Forest& f = s->forest;
     if (level < 0 || level > 32) return 0;
-    const int p0 = f.lev_off[level], np = f.lev_off[level + 1] - p0;
+    const int p0 = s->part ? s->part->plan.own_lo[level] : f.lev_off[level];
+    const int np = (s->part ? s->part->plan.own_hi[level] : f.lev_off[level + 1]) - p0;
     if (np <= 0) return 0;
     if (s->vars.empty()) return fail(FC2D_B200_ESTATE, "no update kernel: register the application solver first");
     if (s->n_upd >= fc2d_b200_solver::PCAP) return fail(FC2D_B200_EINVAL, "too many level updates in one advance");
@@ -572,8 +623,85 @@ static void interpolate_levels(fc2d_b200_solver* s, int mincoarse, int maxcoarse
     if (!c_done) interp_run(s, 0, -1, c);
 }
 
+// Partitioned forest: send q, qlast and registers of this rank's patches in the
+// other ranks' halos and receive theirs (full: every patch to every rank).  The
+// solver's stream is idle while the caller's transport runs.
+static int halo_exchange(fc2d_b200_solver* s, bool full)
+{
+    auto& P = *s->part;
+    const PartitionPlan& pl = P.plan;
+    const int me = P.comm.rank, np = s->forest.np();
+    std::vector<int> peers;
+    std::vector<size_t> ns, nr;
+    const int* sl = nullptr;
+    std::vector<int> all;
+    size_t nsend = 0, nrecv = 0;
+    if (full) {
+        std::vector<int> own;
+        std::vector<std::vector<int>> theirs(P.comm.size);
+        for (int i = 0; i < np; i++) {
+            if (pl.owner[i] == me) own.push_back(i);
+            else theirs[pl.owner[i]].push_back(i);
+        }
+        for (int r = 0; r < P.comm.size; r++) {
+            if (r == me) continue;
+            peers.push_back(r);
+            ns.push_back(own.size());
+            all.insert(all.end(), own.begin(), own.end());
+        }
+        nsend = all.size();
+        for (int r = 0; r < P.comm.size; r++) {
+            if (r == me) continue;
+            nr.push_back(theirs[r].size());
+            all.insert(all.end(), theirs[r].begin(), theirs[r].end());
+        }
+        nrecv = all.size() - nsend;
+    } else {
+        peers = pl.peers;
+        for (size_t k = 0; k < peers.size(); k++) { ns.push_back(pl.send[k].size()); nr.push_back(pl.recv[k].size()); }
+        nsend = P.nsend; nrecv = P.nrecv;
+        sl = P.slots.p;
+    }
+    if (peers.empty()) return 0;
+    DevVec<int> tmp;
+    if (full) {
+        CK(tmp.assign(all, s->st));
+        sl = tmp.p;
+    }
+    const size_t per = 2 * (size_t)s->d.nq() + s->d.nreg();
+    const size_t need = (nsend + nrecv) * per;
+    if (P.buf_cap < need) {
+        if (P.buf) CK(cudaFree(P.buf));
+        P.buf = nullptr;
+        P.buf_cap = 0;
+        CK(cudaMalloc(&P.buf, need * sizeof(double)));
+        P.buf_cap = need;
+    }
+    launch_pack_patches(s->d, sl, (int)nsend, s->q, s->qlast, s->regs, P.buf, s->st);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s->st));
+    std::vector<void*> sp(peers.size()), rp(peers.size());
+    std::vector<size_t> sb(peers.size()), rb(peers.size());
+    size_t so = 0, ro = nsend;
+    for (size_t k = 0; k < peers.size(); k++) {
+        sp[k] = P.buf + so * per; sb[k] = ns[k] * per * sizeof(double); so += ns[k];
+        rp[k] = P.buf + ro * per; rb[k] = nr[k] * per * sizeof(double); ro += nr[k];
+    }
+    if (P.comm.exchange(P.comm.user, (int)peers.size(), peers.data(), sp.data(), sb.data(), rp.data(), rb.data()))
+        return fail(FC2D_B200_ECUDA, "the halo exchange callback failed");
+    launch_unpack_patches(s->d, sl + nsend, (int)nrecv, s->q, s->qlast, s->regs, P.buf + nsend * per, s->st);
+    CK(cudaGetLastError());
+    if (full) CK(cudaStreamSynchronize(s->st));   // tmp's slots are freed on return
+    return 0;
+}
+
 static void ghost_update(fc2d_b200_solver* s, int minlevel, int maxlevel, int time_interp)
 {
+    if (s->part && s->emit) {
+        // the halo arrives before any stage reads it (the time-interpolated copies of
+        // halo patches, still pending, are computed after it)
+        if (flush_updates(s) || halo_exchange(s, false)) s->part->failed = true;
+    }
     if (s->fill)
         for (int l = std::max(minlevel, 0); l <= std::min(maxlevel, 63); l++) s->phys_ok[l] = 1;
     const int mincoarse = minlevel, maxcoarse = maxlevel - 1;
@@ -816,6 +944,7 @@ extern "C" int fc2d_b200_destroy(fc2d_b200_solver_t* s)
     if (s->mass_dev) cudaFree(s->mass_dev);
     if (s->qsave) cudaFree(s->qsave);
     if (s->ss_stage) cudaFreeHost(s->ss_stage);
+    if (s->part && s->part->buf) cudaFree(s->part->buf);
     cudaFree(s->bc_dev); cudaFree(s->newton_hist);
     if (s->tune_params) cudaFree(s->tune_params);
     if (s->area) cudaFree(s->area);
@@ -1100,10 +1229,7 @@ static int end_cfl(fc2d_b200_solver* s, double* cfl, double* cfl_inst = nullptr)
     CK(cudaMemcpyAsync(s->cfl_host, s->cfl_dev, sizeof(unsigned long long) * s->ncfl, cudaMemcpyDeviceToHost, s->st));
     CK(cudaMemcpyAsync(s->status_host, s->status_dev, sizeof(unsigned int), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
-    if (*s->status_host) {
-        if (cfl) *cfl = bits_to_double(0x7ff8000000000000ull);
-        return fail(FC2D_B200_EDEVICE, "device status: " + status_message(*s->status_host));
-    }
+    unsigned status = *s->status_host;
     double v = 0.0;
     bool bad = false;
     for (int i = 0; i < s->ncfl; i++) {
@@ -1111,6 +1237,20 @@ static int end_cfl(fc2d_b200_solver* s, double* cfl, double* cfl_inst = nullptr)
         if (!(c == c)) bad = true;
         if (c > v) v = c;
         if (cfl_inst) cfl_inst[i] = c;
+    }
+    if (s->part) {
+        // the CFL number and the failures of every rank (src/fclaw2d_run.c:206)
+        double r[3] = {v, (double)status, bad ? 1.0 : 0.0};
+        const bool xfail = s->part->failed;
+        s->part->failed = false;
+        if (s->part->comm.allreduce_max(s->part->comm.user, r, 3))
+            return fail(FC2D_B200_ECUDA, "the allreduce callback failed");
+        v = r[0]; status = (unsigned)r[1]; bad = r[2] != 0.0;
+        if (xfail) return fail(FC2D_B200_ECUDA, "a halo exchange of this advance failed");
+    }
+    if (status) {
+        if (cfl) *cfl = bits_to_double(0x7ff8000000000000ull);
+        return fail(FC2D_B200_EDEVICE, "device status: " + status_message(status));
     }
     if (cfl) *cfl = bad ? bits_to_double(0x7ff8000000000000ull) : v;
     if (bad) return fail(FC2D_B200_EDEVICE, "non-finite CFL (negative depth or NaN in the update)");
@@ -1160,7 +1300,7 @@ extern "C" int fc2d_b200_single_step_update_host(fc2d_b200_solver_t* s, int leve
     DeviceScope dev_scope_(s);
     if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
     if (!q) return fail(FC2D_B200_EINVAL, "null patch array");
-    if (!s->insts.empty()) return fail(FC2D_B200_EINVAL, "the host-data protocol drives one forest");
+    if (!s->insts.empty() || s->part) return fail(FC2D_B200_EINVAL, "the host-data protocol drives one forest on one rank");
     if (iter == 0) { s->ss_level = level; s->ss_count = 0; s->ss_host.clear(); }
     if (level != s->ss_level || iter != s->ss_count) return fail(FC2D_B200_ESTATE, "single_step_update calls out of order");
     const Forest& f = s->forest;
@@ -1239,6 +1379,10 @@ extern "C" int fc2d_b200_timeinterp(fc2d_b200_solver_t* s, int level, double alp
 extern "C" int fc2d_b200_time_sync(fc2d_b200_solver_t* s, int minlevel, int maxlevel)
 {
     DeviceScope dev_scope_(s);
+    if (s && s->part && s->initialized) {
+        int rc = halo_exchange(s, false);          // the registers of other ranks' patches
+        if (rc) return rc;
+    }
     if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
     time_sync(s, minlevel, maxlevel);
     (void)flush_pending(s);
@@ -1389,6 +1533,26 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     CK(cudaMemcpyAsync(flags.data(), s->flags_dev.p, sizeof(int) * (size_t)np, cudaMemcpyDeviceToHost, s->st));
     if (minmax) CK(cudaMemcpyAsync(mm.data(), s->minmax_dev.p, sizeof(double) * mm.size(), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
+    if (s->part) {
+        // each rank's tags are valid for its own patches only: reduce them over ranks
+        // (other ranks' entries as -1, ranges as +inf / -inf)
+        auto& P = *s->part;
+        std::vector<double> r((size_t)np * (minmax ? 3 : 1));
+        for (int i = 0; i < np; i++) {
+            const bool me = P.plan.owner[i] == P.comm.rank;
+            r[i] = me ? (double)flags[i] : -1.0;
+            if (minmax) {
+                r[np + i] = me ? -mm[2 * i] : -INFINITY;
+                r[2 * (size_t)np + i] = me ? mm[2 * i + 1] : -INFINITY;
+            }
+        }
+        if (P.comm.allreduce_max(P.comm.user, r.data(), (int)r.size()))
+            return fail(FC2D_B200_ECUDA, "the allreduce callback failed");
+        for (int i = 0; i < np; i++) {
+            flags[i] = (int)r[i];
+            if (minmax) { mm[2 * i] = -r[np + i]; mm[2 * i + 1] = r[2 * (size_t)np + i]; }
+        }
+    }
     // clawpatch_tag4refinement / _tag4coarsening (fclaw2d_clawpatch.cpp:800-910): a negative
     // refine threshold always refines, a threshold <= 0 never coarsens
     const bool always_refine = s->o.refine_threshold < 0, never_coarsen = !(s->o.coarsen_threshold > 0);
@@ -1423,6 +1587,11 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     std::vector<Leaf> L = adapt_leaves(f, mark, changed, err);
     if (changed_out) *changed_out = changed;
     if (!changed) return 0;
+    if (s->part) {
+        // repopulation reads old patches any rank may own: every rank gets all of them
+        int rc = halo_exchange(s, true);
+        if (rc) return rc;
+    }
     Forest nf;
     nf.g = f.g;
     nf.inst = f.inst;
@@ -1648,6 +1817,94 @@ extern "C" int fc2d_b200_run(fc2d_b200_solver_t* s, fc2d_b200_run_stats_t* out)
     return 0;
 }
 
+// ---------------------------------------------------------------------------
+// one forest over several ranks
+// ---------------------------------------------------------------------------
+extern "C" int fc2d_b200_set_partition(fc2d_b200_solver_t* s, const fc2d_b200_comm_t* comm)
+{
+    DeviceScope dev_scope_(s);
+    if (!s) return fail(FC2D_B200_EINVAL, "null solver");
+    if (s->pending) return fail(FC2D_B200_ESTATE, "an advance is in flight");
+    if (!comm) {
+        if (s->part) {
+            if (s->initialized) {                     // every rank gets the whole forest back
+                int rc = halo_exchange(s, true);
+                if (rc) return rc;
+            }
+            const bool g = s->part->graphs_before;
+            if (s->part->buf) cudaFree(s->part->buf);
+            s->part.reset();
+            s->use_graphs = g;
+            invalidate_graph(s);
+            if (s->initialized) return upload_desc_and_tables(s);
+        }
+        return 0;
+    }
+    if (comm->size < 1 || comm->rank < 0 || comm->rank >= comm->size || !comm->exchange || !comm->allreduce_max ||
+        !comm->allreduce_sum)
+        return fail(FC2D_B200_EINVAL, "bad communicator (rank, size or a callback missing)");
+    if (!s->insts.empty()) return fail(FC2D_B200_EINVAL, "batches of instances are distributed by instance, not partitioned");
+    const bool g = s->part ? s->part->graphs_before : s->use_graphs;
+    if (!s->part) s->part = std::make_unique<fc2d_b200_solver::PartState>();
+    s->part->comm = *comm;
+    s->part->graphs_before = g;
+    s->use_graphs = false;                            // transfers run between the launches of an advance
+    invalidate_graph(s);
+    if (s->initialized) return upload_desc_and_tables(s);
+    return 0;
+}
+
+extern "C" int fc2d_b200_partition_owner(const fc2d_b200_solver_t* s, int* owner)
+{
+    if (!s || !owner) return fail(FC2D_B200_EINVAL, "null argument");
+    const int np = s->forest.np();
+    for (int i = 0; i < np; i++) owner[i] = s->part ? s->part->plan.owner[i] : 0;
+    return 0;
+}
+
+extern "C" int fc2d_b200_sync_replicas(fc2d_b200_solver_t* s)
+{
+    DeviceScope dev_scope_(s);
+    if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
+    if (s->pending) return fail(FC2D_B200_ESTATE, "an advance is in flight");
+    if (!s->part) return 0;
+    return halo_exchange(s, true);
+}
+
+extern "C" int fc2d_b200_partition_plan(const fc2d_b200_options_t* opt, int np, const int* level, const int* gx,
+                                        const int* gy, int rank, int size, int* owner, int* nsend, int* nrecv,
+                                        unsigned long long* send_sum, unsigned long long* recv_sum)
+{
+    if (!opt || np <= 0 || !level || !gx || !gy || !owner || size < 1 || rank < 0 || rank >= size)
+        return fail(FC2D_B200_EINVAL, "bad arguments");
+    const fc2d_b200_options_t& o = *opt;
+    Forest f;
+    const Dims d{o.mx, o.my, o.mbc, o.meqn, o.maux};
+    f.g = Geometry{d, o.mi > 0 ? o.mi : 1, o.mj > 0 ? o.mj : 1, o.ax, o.bx, o.ay, o.by};
+    if (o.app == FC2D_B200_APP_SPHERE) { f.g = Geometry{d, 6, 1, 0.0, 1.0, 0.0, 1.0}; f.g.kind = 1; }
+    std::vector<Leaf> L(np);
+    for (int i = 0; i < np; i++) L[i] = Leaf{level[i], gx[i], gy[i], 0};
+    std::string err;
+    if (!f.build(L, err)) return fail(FC2D_B200_EFOREST, err);
+    PartitionPlan pl;
+    make_partition(f, rank, size, pl);
+    for (int i = 0; i < np; i++) owner[i] = pl.owner[i];
+    for (int r = 0; r < size; r++) {
+        if (nsend) nsend[r] = 0;
+        if (nrecv) nrecv[r] = 0;
+        if (send_sum) send_sum[r] = 0;
+        if (recv_sum) recv_sum[r] = 0;
+    }
+    for (size_t k = 0; k < pl.peers.size(); k++) {
+        const int r = pl.peers[k];
+        if (nsend) nsend[r] = (int)pl.send[k].size();
+        if (nrecv) nrecv[r] = (int)pl.recv[k].size();
+        for (int v : pl.send[k]) if (send_sum) send_sum[r] += (unsigned long long)v * 2654435761ull + 1ull;
+        for (int v : pl.recv[k]) if (recv_sum) recv_sum[r] += (unsigned long long)v * 2654435761ull + 1ull;
+    }
+    return 0;
+}
+
 extern "C" int fc2d_b200_mass(fc2d_b200_solver_t* s, double* out)
 {
     DeviceScope dev_scope_(s);
@@ -1662,6 +1919,16 @@ extern "C" int fc2d_b200_mass(fc2d_b200_solver_t* s, double* out)
     std::vector<double> pm((size_t)np * meqn);
     CK(cudaMemcpyAsync(pm.data(), s->mass_dev, sizeof(double) * pm.size(), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
+    if (s->part) {
+        // each patch's partial from its owner (the others add exact zeros), then the
+        // Kahan sum over patches in order, as on one rank
+        auto& P = *s->part;
+        for (int p = 0; p < np; p++)
+            if (P.plan.owner[p] != P.comm.rank)
+                for (int m = 0; m < meqn; m++) pm[(size_t)p * meqn + m] = 0.0;
+        if (P.comm.allreduce_sum(P.comm.user, pm.data(), (int)pm.size()))
+            return fail(FC2D_B200_ECUDA, "the allreduce callback failed");
+    }
     for (int m = 0; m < meqn; m++) {
         double sum = 0.0, comp = 0.0;
         for (int p = 0; p < np; p++) {
@@ -1753,6 +2020,7 @@ extern "C" int fc2d_b200_set_graphs(fc2d_b200_solver_t* s, int enable)
 {
     DeviceScope dev_scope_(s);
     if (!s) return fail(FC2D_B200_EINVAL, "null solver");
+    if (s->part) { s->part->graphs_before = enable != 0; return 0; }   // eager while partitioned
     s->use_graphs = enable != 0;
     invalidate_graph(s);
     return 0;
@@ -1762,6 +2030,7 @@ extern "C" int fc2d_b200_mass_noalloc(fc2d_b200_solver_t* s, double* out)
 {
     DeviceScope dev_scope_(s);
     if (!s || !out || !s->initialized) return fail(FC2D_B200_EINVAL, "bad arguments");
+    if (s->part) return fail(FC2D_B200_EINVAL, "fc2d_b200_mass_noalloc covers one rank; a partitioned forest uses fc2d_b200_mass");
     if (s->sphere) return fail(FC2D_B200_EINVAL, "fc2d_b200_mass_noalloc weights by dx dy; a manifold needs fc2d_b200_mass");
     const long long np = s->forest.np(), meqn = s->d.meqn;
     if (np * meqn + meqn > (long long)MASS_SCRATCH_DOUBLES)
@@ -2075,6 +2344,7 @@ extern "C" int fc2d_b200_set_pstar_seed(fc2d_b200_solver_t* s, const fc2d_b200_m
 extern "C" int fc2d_b200_set_instances(fc2d_b200_solver_t* s, int n, const fc2d_b200_instance_t* inst)
 {
     DeviceScope dev_scope_(s);
+    if (s && s->part) return fail(FC2D_B200_EINVAL, "a partitioned solver holds one forest");
     if (!s || n <= 0 || !inst) return fail(FC2D_B200_EINVAL, "bad arguments");
     if (n > FC2D_B200_MAX_INSTANCES) return fail(FC2D_B200_EINVAL, "too many instances");
     if (s->initialized) return fail(FC2D_B200_ESTATE, "instances are set before initialize");

@@ -377,6 +377,89 @@ void smooth_marks(const Forest& f, std::vector<int>& mark, int smooth_level)
 }
 
 // ---------------------------------------------------------------------------
+// partition along the space-filling curve
+// ---------------------------------------------------------------------------
+void make_partition(const Forest& f, int rank, int size, PartitionPlan& out)
+{
+    const int np = f.np();
+    out.rank = rank;
+    out.size = size;
+    out.owner.assign(np, 0);
+    // SFC order over all levels: (instance, block, Morton of the lower-left corner at the finest scale)
+    std::vector<int> sfc(np);
+    for (int i = 0; i < np; i++) sfc[i] = i;
+    std::sort(sfc.begin(), sfc.end(), [&](int a, int b) {
+        const PatchInfo &A = f.p[a], &B = f.p[b];
+        if (A.inst != B.inst) return A.inst < B.inst;
+        if (A.block != B.block) return A.block < B.block;
+        return A.morton < B.morton;
+    });
+    // weight: substeps per coarse step; a leaf goes to the rank whose share of the
+    // total weight holds the middle of the leaf's weight interval
+    const int lmin = f.minlevel_present;
+    double W = 0.0;
+    for (int i = 0; i < np; i++) W += std::ldexp(1.0, f.p[i].level - lmin);
+    double cw = 0.0;
+    for (int k = 0; k < np; k++) {
+        const int i = sfc[k];
+        const double w = std::ldexp(1.0, f.p[i].level - lmin);
+        const int r = (int)std::floor((cw + 0.5 * w) * size / W);
+        out.owner[i] = std::min(std::max(r, 0), size - 1);
+        cw += w;
+    }
+    // neighbours across faces and corners
+    auto nbrs = [&](int i, std::vector<int>& v) {
+        v.clear();
+        const PatchInfo& P = f.p[i];
+        for (int fc = 0; fc < 4; fc++) {
+            if (P.face_type[fc] == NB_BOUNDARY) continue;
+            for (int k = 0; k < (P.face_type[fc] == NB_HALF ? 2 : 1); k++) v.push_back(P.face_nbr[fc][k]);
+        }
+        for (int c = 0; c < 4; c++)
+            if (P.has_corner[c]) v.push_back(P.corner_nbr[c]);
+    };
+    // ring[r][i]: 1 (ring 1) or 2 (ring 2) of rank r, for patches r does not own
+    std::vector<std::vector<char>> ring(size, std::vector<char>(np, 0));
+    std::vector<int> nb;
+    for (int i = 0; i < np; i++) {
+        nbrs(i, nb);
+        for (int j : nb)
+            if (out.owner[j] != out.owner[i]) ring[out.owner[i]][j] = 1;
+    }
+    for (int r = 0; r < size; r++)
+        for (int i = 0; i < np; i++) {
+            if (ring[r][i] != 1) continue;
+            nbrs(i, nb);
+            for (int j : nb)
+                if (out.owner[j] != r && ring[r][j] == 0) ring[r][j] = 2;
+        }
+    out.fill.assign(np, 0);
+    for (int i = 0; i < np; i++) out.fill[i] = (out.owner[i] == rank || ring[rank][i] == 1) ? 1 : 0;
+    out.peers.clear(); out.send.clear(); out.recv.clear();
+    for (int r = 0; r < size; r++) {
+        if (r == rank) continue;
+        std::vector<int> snd, rcv;
+        for (int i = 0; i < np; i++) {
+            if (out.owner[i] == rank && ring[r][i]) snd.push_back(i);
+            if (out.owner[i] == r && ring[rank][i]) rcv.push_back(i);
+        }
+        if (snd.empty() && rcv.empty()) continue;
+        out.peers.push_back(r);
+        out.send.push_back(snd);
+        out.recv.push_back(rcv);
+    }
+    // owned slots of each level: one range, since a level's slots follow the SFC order
+    for (int l = 0; l < 34; l++) { out.own_lo[l] = 0; out.own_hi[l] = 0; }
+    for (int l = 0; l < 33; l++) {
+        int lo = -1, hi = -1;
+        for (int i = f.lev_off[l]; i < f.lev_off[l + 1]; i++)
+            if (out.owner[i] == rank) { if (lo < 0) lo = i; hi = i + 1; }
+        if (lo >= 0) { out.own_lo[l] = lo; out.own_hi[l] = hi; }
+        else { out.own_lo[l] = out.own_hi[l] = f.lev_off[l]; }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // gather tables
 // ---------------------------------------------------------------------------
 namespace {

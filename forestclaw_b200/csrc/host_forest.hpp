@@ -101,6 +101,27 @@ std::vector<Leaf> adapt_leaves(const Forest& f, const std::vector<int>& mark, in
 // difference to its own level.
 void smooth_marks(const Forest& f, std::vector<int>& mark, int smooth_level);
 
+// Partition of a single forest over ranks along the space-filling curve (p4est's
+// leaf order: block, then Morton order) with weight 2^(level - minlevel present) per
+// leaf, its number of substeps in a coarse step (src/fclaw2d_partition.c:113 uses
+// p4est's weighted partition).  Every rank keeps the whole tree; it owns one SFC
+// range, updates its own patches and fills the ghost cells of its own patches and
+// of ring 1 (the other ranks' patches touching its own across a face or corner,
+// which its interpolations read as coarse sources).  Ring 2 (the patches touching
+// ring 1) supplies those fills; rings 1 and 2 make the halo it receives before each
+// ghost update.
+struct PartitionPlan {
+    int rank = 0, size = 1;
+    std::vector<int> owner;                  // per slot
+    std::vector<char> fill;                  // per slot: owned or ring 1 (ghost cells filled here)
+    std::vector<int> peers;                  // ranks this one exchanges with (ascending)
+    std::vector<std::vector<int>> send;      // per peer: own slots in the peer's halo (ascending)
+    std::vector<std::vector<int>> recv;      // per peer: the peer's slots in this halo (ascending)
+    int own_lo[34], own_hi[34];              // owned slots of level l: [own_lo[l], own_hi[l])
+};
+// The plan of `rank` among `size` ranks for forest f (pure host computation).
+void make_partition(const Forest& f, int rank, int size, PartitionPlan& out);
+
 // Gather tables of one level.
 struct LevelTables {
     std::vector<CopyEnt> copy;       // copy2ghost(level)

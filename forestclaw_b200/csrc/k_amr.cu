@@ -496,6 +496,40 @@ __global__ void k_tag(const double* __restrict__ q, const PatchDesc* __restrict_
     if (threadIdx.x == 0) flags[p] = (refine ? 1 : 0) | (exceed_c ? 0 : 2);
 }
 
+// Halo payload of a partitioned forest: per listed patch its q, qlast and
+// registers, one after another (nq + nq + nreg doubles), patch after patch.
+__global__ void k_pack_patches(const int* __restrict__ slots, int n, const double* __restrict__ q,
+                               const double* __restrict__ qlast, const double* __restrict__ regs, int nq, int nreg,
+                               double* __restrict__ out)
+{
+    const int k = blockIdx.x;
+    if (k >= n) return;
+    const size_t per = 2 * (size_t)nq + nreg;
+    const int p = slots[k];
+    double* o = out + (size_t)k * per;
+    for (int i = threadIdx.x; i < nq; i += blockDim.x) {
+        o[i] = q[(size_t)p * nq + i];
+        o[nq + i] = qlast[(size_t)p * nq + i];
+    }
+    for (int i = threadIdx.x; i < nreg; i += blockDim.x) o[2 * nq + i] = regs[(size_t)p * nreg + i];
+}
+
+__global__ void k_unpack_patches(const int* __restrict__ slots, int n, double* __restrict__ q,
+                                 double* __restrict__ qlast, double* __restrict__ regs, int nq, int nreg,
+                                 const double* __restrict__ in)
+{
+    const int k = blockIdx.x;
+    if (k >= n) return;
+    const size_t per = 2 * (size_t)nq + nreg;
+    const int p = slots[k];
+    const double* v = in + (size_t)k * per;
+    for (int i = threadIdx.x; i < nq; i += blockDim.x) {
+        q[(size_t)p * nq + i] = v[i];
+        qlast[(size_t)p * nq + i] = v[nq + i];
+    }
+    for (int i = threadIdx.x; i < nreg; i += blockDim.x) regs[(size_t)p * nreg + i] = v[2 * nq + i];
+}
+
 // Regrid repopulation (cb_fclaw2d_regrid_repopulate, fclaw2d_regrid.c:93-205).
 __global__ void k_repop(const RepopOp* __restrict__ ops, int mx, int my, int mbc, int meqn, int nreg,
                         const double* __restrict__ oq, double* __restrict__ nq,
@@ -674,6 +708,16 @@ void launch_tag(const Dims& d, const double* q, const PatchDesc* desc, int np, i
                 double cthr, int* flags, cudaStream_t st, double* minmax)
 {
     if (np > 0) k_tag<<<np, 128, 0, st>>>(q, desc, d.mx, d.my, d.mbc, d.meqn, crit, mq, rthr, cthr, flags, minmax);
+}
+void launch_pack_patches(const Dims& d, const int* slots, int n, const double* q, const double* qlast,
+                         const double* regs, double* out, cudaStream_t st)
+{
+    if (n > 0) k_pack_patches<<<n, 256, 0, st>>>(slots, n, q, qlast, regs, d.nq(), d.nreg(), out);
+}
+void launch_unpack_patches(const Dims& d, const int* slots, int n, double* q, double* qlast, double* regs,
+                           const double* in, cudaStream_t st)
+{
+    if (n > 0) k_unpack_patches<<<n, 256, 0, st>>>(slots, n, q, qlast, regs, d.nq(), d.nreg(), in);
 }
 void launch_repop(const Dims& d, const RepopOp* ops, int nops, const double* oq, double* nq, const double* oqlast,
                   double* nqlast, const double* oqi, double* nqi, const double* oregs, double* nregs,

@@ -121,6 +121,12 @@ void launch_patch_mass(const Dims& d, const double* q, const PatchDesc* desc, in
 // range > refine_thr, and leaves the family test to the caller.
 void launch_tag(const Dims& d, const double* q, const PatchDesc* desc, int np, int crit, int mq, double refine_thr,
                 double coarsen_thr, int* flags, cudaStream_t st, double* minmax);
+// Halo payload of a partitioned forest: q, qlast and registers of the listed slots,
+// nq + nq + nreg doubles per patch, packed into (or unpacked from) one buffer.
+void launch_pack_patches(const Dims& d, const int* slots, int n, const double* q, const double* qlast,
+                         const double* regs, double* out, cudaStream_t st);
+void launch_unpack_patches(const Dims& d, const int* slots, int n, double* q, double* qlast, double* regs,
+                           const double* in, cudaStream_t st);
 // Repopulation after adapt: op kind 0 copy old slot, 1 interpolate2fine from old parent (igrid),
 // 2 average2coarse from 4 old children (src = first child slot; children consecutive by igrid
 // via child_slots).

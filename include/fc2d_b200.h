@@ -16,6 +16,8 @@
 #ifndef FC2D_B200_H
 #define FC2D_B200_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -240,6 +242,52 @@ int fc2d_b200_write_ascii_frame(const char* dir, int iframe, double time, int me
 int fc2d_b200_output_vtk(fc2d_b200_solver_t* s, const char* prefix, int iframe);
 int fc2d_b200_write_vtk_file(const char* path, int mx, int my, int meqn, int npatch, const int* block,
                              const double* points, const float* values);
+
+/* ---- one forest partitioned over ranks (one process per GPU) ----
+ * The reference partitions the leaves along the space-filling curve
+ * (src/fclaw2d_partition.c:113, p4est_partition with weights), exchanges ghost
+ * patches once per ghost update (fclaw2d_exchange_ghost_patches_begin/end,
+ * src/fclaw2d_exchange.c:308-413, called from src/fclaw2d_ghost_fill.c:700-720) with the
+ * time-sync registers packed in the payload (fclaw2d_clawpatch_conservation.c:112-203),
+ * and reduces the CFL number (src/fclaw2d_run.c:206) and the mass over ranks.  Here every
+ * rank keeps the whole tree and the same slot numbering; it owns one range of the
+ * curve (leaf weight 2^(level - minlevel present), its substeps per coarse step),
+ * updates its own patches, fills the ghost cells of its own patches and of the first
+ * ring of other ranks' patches around them, and before each ghost update receives
+ * q, qlast and registers of the two rings of other ranks' patches around its own.
+ * A regrid tags each rank's own patches, reduces the tags over ranks, gathers every
+ * patch's q on every rank, adapts the (identical) tree and partitions it again.
+ * The transport is the caller's, through these callbacks (return 0 on success):
+ *   exchange:      for k < npeers, send send_bytes[k] bytes at send[k] to rank peers[k]
+ *                  and receive recv_bytes[k] bytes from it into recv[k]; the buffers are
+ *                  device memory of the solver's device, the solver's stream is idle on
+ *                  entry, and the data must be in place on return (NCCL send/recv, or
+ *                  host staging for gloo);
+ *   allreduce_max / allreduce_sum: in place over ranks, n doubles in host memory.
+ * Results are bitwise those of one rank holding the whole forest. */
+typedef struct fc2d_b200_comm {
+    int rank, size;
+    void* user;
+    int (*exchange)(void* user, int npeers, const int* peers, void* const* send, const size_t* send_bytes,
+                    void* const* recv, const size_t* recv_bytes);
+    int (*allreduce_max)(void* user, double* v, int n);
+    int (*allreduce_sum)(void* user, double* v, int n);
+} fc2d_b200_comm_t;
+/* Partition this solver's forest among comm->size ranks (comm NULL: back to one rank,
+ * every rank then holding the whole forest).  Every rank calls it with the same forest;
+ * CUDA-graph replay is off while partitioned. */
+int fc2d_b200_set_partition(fc2d_b200_solver_t* s, const fc2d_b200_comm_t* comm);
+/* Owner rank of each patch (level-major order). */
+int fc2d_b200_partition_owner(const fc2d_b200_solver_t* s, int* owner);
+/* Gather every patch's current q, qlast and registers on every rank (before reading
+ * the whole forest with fc2d_b200_get_q, writing output, or checkpointing). */
+int fc2d_b200_sync_replicas(fc2d_b200_solver_t* s);
+/* The partition plan of `rank` among `size` for a forest given by its leaves, computed
+ * on the host without a device: owner[np], and per rank r the number of patches sent to
+ * and received from r and a checksum of each list (sum over slots p of p * 2654435761 + 1). */
+int fc2d_b200_partition_plan(const fc2d_b200_options_t* opt, int np, const int* level, const int* gx,
+                             const int* gy, int rank, int size, int* owner, int* nsend, int* nrecv,
+                             unsigned long long* send_sum, unsigned long long* recv_sum);
 
 /* ---- patch-to-CTA variants of the fused update (no counterpart in the reference) ----
  * Each solver shape (precision, Riemann solver, patch size) is compiled with

@@ -66,7 +66,8 @@ def test_c2_radialdam_levels_3_7_20_steps_regrid_bitwise():
     _bitwise(o.get_q(), g.get_q(), "q after 20 coarse steps")
     _bitwise(o.get_registers(), g.get_registers(), "conservation registers")
     mo, mg = o.mass(), g.mass()
-    assert np.all(np.abs(mo - mg) <= 1e-12 * np.abs(mo) + 1e-300)
+    # per field to 1e-12 of the depth's mass (the momenta sum to round-off around zero)
+    assert np.all(np.abs(mo - mg) <= 1e-12 * abs(mo[0])), (mo, mg)
     g.close()
 
 
