@@ -37,8 +37,19 @@ cpu_baseline: the FP64 CPU oracle (OpenMP over patches, all host cores) on a bou
 --impl reference times the reference's CPU implementation of the path: the
 reference's Fortran cannot be compiled here, so it is the C restatement (oracle)
 with all host threads, on the same config.
-Multi-GPU (torchrun): every rank runs its own instance of the workload
-(independent simulations, weak scaling, no data-path collective).
+Multi-GPU (torchrun): a single-forest workload is one forest partitioned over the
+ranks along the space-filling curve (fc2d_b200_set_partition: each rank updates
+its own patches, a halo of q, qlast and registers moves over NCCL before each ghost
+update, the CFL number, regrid tags and mass are reduced; strong scaling), or with
+--no-partition one replica per rank (weak scaling).  The batch workload gives each
+rank its own instances (weak scaling, no data-path collective).
+e2e, per step: set_q from pinned host memory, advance, get_q back; every
+regrid_interval steps the regrid (and a get_q of the new forest) inside the
+wall-clock region.
+error_vs_oracle: the FP32-wave run against the FP64 CPU oracle from the same
+initial forest (per-field relative L1 and Linf, mass).
+The default line carries a second measurement under "secondary": the shock-bubble
+(Euler, exact solver) with the learned p* start (--no-secondary skips it).
 """
 from __future__ import annotations
 
@@ -477,6 +488,7 @@ def _fp64_kernel_arm(args, wl, prob, local_rank, flush):
     _, gc = _options(wl, "fp64")
     gc.device = local_rank
     g = fb.Solver(gc)
+    _maybe_partition(g, args, local_rank)
     g.initialize()
     t, dt, _ = _spinup(g, wl, 0.0, _initial_dt(wl, prob), wl["spinup"])
     tune = _tune(g, not args.no_autotune)
@@ -490,6 +502,21 @@ def _fp64_kernel_arm(args, wl, prob, local_rank, flush):
     total_ms, _, value = ranks.aggregate(float(np.sum(r["step_ms"])), r["cells"], "cuda")
     return {"value": value, "ms_per_step": total_ms / args.steps,
             "variant": {k: tune[k] for k in ("variant", "threads", "min_blocks", "reg")}}
+
+
+def _partitioned(args) -> bool:
+    import torch.distributed as dist
+    return bool(getattr(args, "partition", False)) and dist.is_available() and dist.is_initialized() \
+        and dist.get_world_size() > 1
+
+
+def _maybe_partition(g, args, local_rank):
+    """With several ranks (and --partition, the default), the one forest is split
+    over them along the space-filling curve with a halo exchange per ghost update
+    (NCCL, device to device)."""
+    if _partitioned(args):
+        from forestclaw_b200 import partition as pt
+        pt.partition(g, pt.TorchComm(device=local_rank))
 
 
 def _bracket():
@@ -513,6 +540,7 @@ def run_ours(args, wl, rank, world, local_rank):
     if args.pstar == "mlp":
         mlp, mlp_info = train_pstar_mlp(wl, prob, local_rank, args.mlp_samples, args.mlp_epochs)
     g = fb.Solver(gc)
+    _maybe_partition(g, args, local_rank)
     g.initialize()
     if mlp is not None:
         g.set_pstar_seed(mlp)
@@ -608,10 +636,13 @@ def run_ours(args, wl, rank, world, local_rank):
     line = {
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "higher_is_better": True, "scaling": "strong" if _partitioned(args) else "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32-waves/f64-q",
         "data": "synthetic (reference app initial data)",
         "config": {"workload": wl["name"], "patches": npatch, "precision": args.precision,
+                   "multi_gpu": ("one forest partitioned along the space-filling curve, halo exchange per ghost "
+                                 "update over NCCL" if _partitioned(args) else
+                                 ("one replica of the forest per rank" if world > 1 else "one GPU")),
                    "cells_per_step": cells / args.steps,
                    "l2": "flushed between timed steps (512 MB write)",
                    "launch": "CUDA graph per coarse step (captured once per forest)",
@@ -894,6 +925,9 @@ def main():
                     help="Euler: Newton start of the exact solver (mlp: trained on the FP64 run first)")
     ap.add_argument("--mlp-samples", type=int, default=1_000_000)
     ap.add_argument("--mlp-epochs", type=int, default=20)
+    ap.add_argument("--no-partition", dest="partition", action="store_false",
+                    help="with several ranks, run one replica of a single-forest workload per rank instead of "
+                         "partitioning the one forest over them")
     ap.add_argument("--no-secondary", dest="secondary", action="store_false",
                     help="skip the second measurement (shock-bubble with the learned p* start) of the default line")
     ap.add_argument("--secondary-steps", type=int, default=20)

@@ -71,7 +71,7 @@ struct DevVec {
 
 struct LevelRanges {
     int copy_off = 0, copy_n = 0, avg_off = 0, avg_n = 0, interp_off = 0, interp_n = 0, phys_off = 0, phys_n = 0;
-    int ti_off = 0, ti_n = 0, sync_off = 0, sync_start_off = 0, sync_np = 0;
+    int ti_off = 0, ti_n = 0, sync_start_off = 0, sync_np = 0;   // sync groups [sync_start_off, + sync_np)
 };
 
 struct fc2d_b200_solver {
@@ -136,6 +136,9 @@ struct fc2d_b200_solver {
     DevVec<PhysEnt> t_phys;
     DevVec<int> t_ti, t_sync_start;
     DevVec<SyncOp> t_sync;
+    Tables tables;                                 // host copy of the gather tables (buffers reused)
+    TableWork table_work;
+    std::vector<unsigned char> interp_written;     // interpolation-chain scratch, all zero between uses
     LevelRanges lr[33];
     unsigned long long* cfl_dev = nullptr;
     unsigned long long* cfl_host = nullptr;
@@ -293,10 +296,10 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
     const Forest& f = s->forest;
     const std::vector<PatchDesc> hd = make_desc(f);
     if (!hd.empty()) CK(cudaMemcpyAsync(s->desc, hd.data(), hd.size() * sizeof(PatchDesc), cudaMemcpyHostToDevice, s->st));
-    std::vector<LevelTables> T;
+    Tables& T = s->tables;
     {
         std::string err;
-        if (!build_tables(f, s->o.mthbc, s->has_inflow, T, err)) return fail(FC2D_B200_EFOREST, err);
+        if (!build_tables(f, s->o.mthbc, s->has_inflow, T, s->table_work, err)) return fail(FC2D_B200_EFOREST, err);
     }
     if (s->part) {
         // partitioned: a new plan for this forest; the ghost-fill stages write only the
@@ -307,26 +310,39 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
         const std::vector<char>& fill = P.plan.fill;
         const std::vector<int>& own = P.plan.owner;
         const int me = P.comm.rank, nq = s->d.nq();
-        for (LevelTables& L : T) {
-            auto keep = [&](int dst) { return fill[dst / nq] != 0; };
-            auto mine = [&](int dst) { return own[dst / nq] == me; };
-            L.copy.erase(std::remove_if(L.copy.begin(), L.copy.end(), [&](const CopyEnt& e) { return !keep(e.dst); }), L.copy.end());
-            L.avg.erase(std::remove_if(L.avg.begin(), L.avg.end(), [&](const AvgEnt& e) { return !keep(e.dst); }), L.avg.end());
-            L.phys.erase(std::remove_if(L.phys.begin(), L.phys.end(), [&](const PhysEnt& e) { return !keep(e.dst); }), L.phys.end());
-            L.interp.erase(std::remove_if(L.interp.begin(), L.interp.end(), [&](const InterpEnt& e) { return !mine(e.dst); }), L.interp.end());
-            L.ti.erase(std::remove_if(L.ti.begin(), L.ti.end(), [&](int p) { return !fill[p]; }), L.ti.end());
-            std::vector<SyncOp> ops;
-            std::vector<int> start{0};
-            for (size_t g = 0; g + 1 < L.sync_start.size(); g++) {
-                const int a = L.sync_start[g], b = L.sync_start[g + 1];
-                if (b > a && own[L.sync[a].p] == me) {
-                    ops.insert(ops.end(), L.sync.begin() + a, L.sync.begin() + b);
+        // keep the entries that pass, level by level, and move the level offsets
+        auto filter = [](auto& v, int* off, auto keep) {
+            size_t n = 0;
+            for (int l = 0; l < 33; l++) {
+                const size_t a = off[l], b = off[l + 1];
+                off[l] = (int)n;
+                for (size_t k = a; k < b; k++)
+                    if (keep(v[k])) v[n++] = v[k];
+            }
+            off[33] = (int)n;
+            v.resize(n);
+        };
+        filter(T.copy, T.copy_off, [&](const CopyEnt& e) { return fill[e.dst / nq] != 0; });
+        filter(T.avg, T.avg_off, [&](const AvgEnt& e) { return fill[e.dst / nq] != 0; });
+        filter(T.phys, T.phys_off, [&](const PhysEnt& e) { return fill[e.dst / nq] != 0; });
+        filter(T.interp, T.interp_off, [&](const InterpEnt& e) { return own[e.dst / nq] == me; });
+        filter(T.ti, T.ti_off, [&](int p) { return fill[p] != 0; });
+        std::vector<SyncOp> ops;
+        std::vector<int> start{0};
+        for (int l = 0; l < 33; l++) {
+            const int g0 = T.grp_off[l], g1 = T.grp_off[l + 1];
+            T.grp_off[l] = (int)start.size() - 1;
+            for (int g = g0; g < g1; g++) {
+                const int a = T.sync_start[g], b = T.sync_start[g + 1];
+                if (b > a && own[T.sync[a].p] == me) {
+                    ops.insert(ops.end(), T.sync.begin() + a, T.sync.begin() + b);
                     start.push_back((int)ops.size());
                 }
             }
-            L.sync.swap(ops);
-            L.sync_start.swap(start);
         }
+        T.grp_off[33] = (int)start.size() - 1;
+        T.sync.swap(ops);
+        T.sync_start.swap(start);
         // halo slot lists (send, then receive), uploaded once per forest
         std::vector<int> slots;
         for (const auto& v : P.plan.send) slots.insert(slots.end(), v.begin(), v.end());
@@ -335,32 +351,29 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
         P.nrecv = slots.size() - P.nsend;
         if (!slots.empty()) CK(P.slots.assign(slots, s->st));
     }
-    std::vector<CopyEnt> copy;
-    std::vector<AvgEnt> avg;
-    std::vector<InterpEnt> interp;
-    std::vector<PhysEnt> phys;
-    std::vector<int> ti, sync_start;
-    std::vector<SyncOp> sync;
     for (int l = 0; l < 33; l++) {
         LevelRanges& r = s->lr[l];
         r = LevelRanges();
-        const LevelTables& L = T[l];
-        r.copy_off = (int)copy.size(); r.copy_n = (int)L.copy.size(); copy.insert(copy.end(), L.copy.begin(), L.copy.end());
-        r.avg_off = (int)avg.size(); r.avg_n = (int)L.avg.size(); avg.insert(avg.end(), L.avg.begin(), L.avg.end());
-        r.interp_off = (int)interp.size(); r.interp_n = (int)L.interp.size();
-        interp.insert(interp.end(), L.interp.begin(), L.interp.end());
-        r.phys_off = (int)phys.size(); r.phys_n = (int)L.phys.size(); phys.insert(phys.end(), L.phys.begin(), L.phys.end());
-        r.ti_off = (int)ti.size(); r.ti_n = (int)L.ti.size(); ti.insert(ti.end(), L.ti.begin(), L.ti.end());
-        r.sync_off = (int)sync.size(); r.sync_start_off = (int)sync_start.size();
-        r.sync_np = (int)L.sync_start.size() - 1;
-        sync.insert(sync.end(), L.sync.begin(), L.sync.end());
-        for (int v : L.sync_start) sync_start.push_back(v + r.sync_off);
+        r.copy_off = T.copy_off[l]; r.copy_n = T.copy_off[l + 1] - T.copy_off[l];
+        r.avg_off = T.avg_off[l]; r.avg_n = T.avg_off[l + 1] - T.avg_off[l];
+        r.interp_off = T.interp_off[l]; r.interp_n = T.interp_off[l + 1] - T.interp_off[l];
+        r.phys_off = T.phys_off[l]; r.phys_n = T.phys_off[l + 1] - T.phys_off[l];
+        r.ti_off = T.ti_off[l]; r.ti_n = T.ti_off[l + 1] - T.ti_off[l];
+        r.sync_start_off = T.grp_off[l]; r.sync_np = T.grp_off[l + 1] - T.grp_off[l];
     }
+    const std::vector<CopyEnt>& copy = T.copy;
+    const std::vector<AvgEnt>& avg = T.avg;
+    const std::vector<InterpEnt>& interp = T.interp;
+    const std::vector<PhysEnt>& phys = T.phys;
+    const std::vector<int>& ti = T.ti;
+    const std::vector<SyncOp>& sync = T.sync;
+    const std::vector<int>& sync_start = T.sync_start;
     CK(s->t_copy.assign(copy, s->st));
     CK(s->t_avg.assign(avg, s->st));
     CK(s->t_interp.assign(interp, s->st));
     {   // interpolation chains: reads of level l's entries against writes of level l-1's
-        std::vector<unsigned char> written((size_t)f.np() * s->d.nq(), 0);
+        std::vector<unsigned char>& written = s->interp_written;
+        if (written.size() < (size_t)f.np() * s->d.nq()) written.resize((size_t)f.np() * s->d.nq(), 0);
         const int nx = s->d.nx();
         for (int l = 0; l < 34; l++) s->interp_chain[l] = 0;
         for (int l = 1; l <= 32; l++) {

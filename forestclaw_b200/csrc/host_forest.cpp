@@ -15,6 +15,8 @@
 #include <cmath>
 #include <cstdio>
 #include <map>
+#include <thread>
+#include <atomic>
 #include "fcb_sphere.h"
 
 namespace fcb {
@@ -178,8 +180,7 @@ void Forest::geometry(PatchInfo& q) const
 int Forest::lookup(int i, int l, int x, int y) const
 {
     if (l < 0 || !in_domain(i, l, x, y)) return -1;
-    auto it = index_.find(key(i, l, x, y));
-    return it == index_.end() ? -1 : it->second;
+    return index_.get(key(i, l, x, y));
 }
 
 bool Forest::build(const std::vector<Leaf>& leaves, std::string& err)
@@ -199,9 +200,8 @@ bool Forest::build(const std::vector<Leaf>& leaves, std::string& err)
         if (a.block != b.block) return a.block < b.block;
         return a.morton < b.morton;
     });
-    index_.clear();
-    index_.reserve(p.size() * 2);
-    for (int i = 0; i < np(); i++) index_[key(p[i].inst, p[i].level, p[i].gx, p[i].gy)] = i;
+    index_.reset(p.size());
+    for (int i = 0; i < np(); i++) index_.put(key(p[i].inst, p[i].level, p[i].gx, p[i].gy), i);
     for (int l = 0; l < 34; l++) lev_off[l] = 0;
     minlevel_present = 99; maxlevel_present = -1;
     {
@@ -307,36 +307,56 @@ std::vector<Leaf> adapt_leaves(const Forest& f, const std::vector<int>& mark, in
             L.push_back({P.level, P.gx, P.gy, P.inst}); done[i] = 1;
         }
     }
-    // 2:1 face+corner balance by refining the coarser side
-    for (;;) {
-        std::unordered_map<uint64_t, int> idx;
-        idx.reserve(L.size() * 2);
-        for (int i = 0; i < (int)L.size(); i++) idx[Forest::key(L[i].inst, L[i].level, L[i].gx, L[i].gy)] = i;
-        std::vector<char> ref(L.size(), 0);
-        bool any = false;
-        for (int i = 0; i < (int)L.size(); i++) {
-            const int l = L[i].level, in = L[i].inst;
-            for (int dy = -1; dy <= 1; dy++)
-                for (int dx = -1; dx <= 1; dx++) {
-                    if (!dx && !dy) continue;
-                    int x, y;
-                    if (f.step(in, l, L[i].gx, L[i].gy, dx, dy, x, y) != 1) continue;
-                    for (int k = l - 2; k >= 0; k--) {
-                        auto it = idx.find(Forest::key(in, k, x >> (l - k), y >> (l - k)));
-                        if (it != idx.end()) {
-                            if (!ref[it->second]) { ref[it->second] = 1; any = true; }
-                            break;
+    // 2:1 face+corner balance by refining the coarser side.  The first pass checks
+    // every leaf; a later pass checks only the children the previous pass created and
+    // the leaves that found a too-coarse neighbour (its children may still be too coarse).
+    {
+        KeyIndex idx;
+        idx.reset(L.size() * 4);
+        for (int i = 0; i < (int)L.size(); i++) idx.put(Forest::key(L[i].inst, L[i].level, L[i].gx, L[i].gy), i);
+        std::vector<char> dead(L.size(), 0);
+        std::vector<int> check(L.size());
+        for (int i = 0; i < (int)L.size(); i++) check[i] = i;
+        std::vector<int> ref, again;
+        std::vector<char> queued(L.size(), 0);
+        while (!check.empty()) {
+            ref.clear();
+            again.clear();
+            for (int i : check) {
+                const int l = L[i].level, in = L[i].inst;
+                for (int dy = -1; dy <= 1; dy++)
+                    for (int dx = -1; dx <= 1; dx++) {
+                        if (!dx && !dy) continue;
+                        int x, y;
+                        if (f.step(in, l, L[i].gx, L[i].gy, dx, dy, x, y) != 1) continue;
+                        for (int k = l - 2; k >= 0; k--) {
+                            const int j = idx.get(Forest::key(in, k, x >> (l - k), y >> (l - k)));
+                            if (j >= 0) {
+                                if (!dead[j]) { dead[j] = 1; ref.push_back(j); }
+                                if (!queued[i]) { queued[i] = 1; again.push_back(i); }
+                                break;
+                            }
                         }
                     }
+            }
+            check.clear();
+            for (int i : again) { queued[i] = 0; if (!dead[i]) check.push_back(i); }
+            for (int j : ref) {
+                idx.put(Forest::key(L[j].inst, L[j].level, L[j].gx, L[j].gy), -1);
+                const Leaf P = L[j];
+                for (int c = 0; c < 4; c++) {
+                    const int n = (int)L.size();
+                    L.push_back({P.level + 1, 2 * P.gx + (c & 1), 2 * P.gy + (c >> 1), P.inst});
+                    dead.push_back(0);
+                    queued.push_back(0);
+                    idx.put(Forest::key(L[n].inst, L[n].level, L[n].gx, L[n].gy), n);
+                    check.push_back(n);
                 }
+            }
         }
-        if (!any) break;
         std::vector<Leaf> M;
-        M.reserve(L.size() + 64);
-        for (int i = 0; i < (int)L.size(); i++) {
-            if (!ref[i]) { M.push_back(L[i]); continue; }
-            for (int c = 0; c < 4; c++) M.push_back({L[i].level + 1, 2 * L[i].gx + (c & 1), 2 * L[i].gy + (c >> 1), L[i].inst});
-        }
+        M.reserve(L.size());
+        for (size_t i = 0; i < L.size(); i++) if (!dead[i]) M.push_back(L[i]);
         L.swap(M);
     }
     if (!changed) {
@@ -493,213 +513,318 @@ struct TableCtx {
         if (fc < 0) { X2 = Y2 = -(1L << 20); return; }   // not adjacent: outside every patch (tables check)
         cs_xform(b, fc, (long)mx << L, X, Y, X2, Y2);
     }
+    // An index map (x, y) -> (c + M (x, y)) with integer M.  to_block is the identity
+    // or an isometry of the plane between adjacent blocks (a constant outside point
+    // otherwise), so the transforms below are affine and three evaluations give them.
+    struct Aff {
+        long ci, cj, ii, ij, ji, jj;
+        void map(long x, long y, int& i2, int& j2) const
+        {
+            i2 = (int)(ci + ii * x + ij * y);
+            j2 = (int)(cj + ji * x + jj * y);
+        }
+    };
     // transform_face / transform_corner: cell (i, j) of P as a Fortran index of N, same level
-    void same(const PatchInfo& P, int i, int j, const PatchInfo& N, int& i2, int& j2) const
+    void same(const PatchInfo& P, long i, long j, const PatchInfo& N, long& i2, long& j2) const
     {
         int b, bn; long X0, Y0, XN, YN, X2, Y2;
         org(P, b, X0, Y0); org(N, bn, XN, YN);
         to_block(b, bn, P.level, X0 + i - 1, Y0 + j - 1, X2, Y2);
-        i2 = (int)(X2 - XN + 1); j2 = (int)(Y2 - YN + 1);
+        i2 = X2 - XN + 1; j2 = Y2 - YN + 1;
+    }
+    Aff same_map(const PatchInfo& P, const PatchInfo& N) const
+    {
+        long a0, b0, a1, b1, a2, b2;
+        same(P, 0, 0, N, a0, b0); same(P, 1, 0, N, a1, b1); same(P, 0, 1, N, a2, b2);
+        return {a0, b0, a1 - a0, a2 - a0, b1 - b0, b2 - b0};
     }
     // transform_face2 / transform_corner2: child (a, c) -- in the coarse patch's axes -- of
-    // coarse cell (i, j) of C, as a Fortran index of the fine patch F
-    void child(const PatchInfo& C, int i, int j, int a, int c, const PatchInfo& F, int& i2, int& j2) const
+    // coarse cell (i, j) of C, as a Fortran index of the fine patch F; affine in
+    // (x, y) = (2 i + a, 2 j + c)
+    void child(const PatchInfo& C, long x, long y, const PatchInfo& F, long& i2, long& j2) const
     {
         int b, bf; long X0, Y0, XF, YF, X2, Y2;
         org(C, b, X0, Y0); org(F, bf, XF, YF);
-        to_block(b, bf, C.level + 1, 2 * (X0 + i - 1) + a, 2 * (Y0 + j - 1) + c, X2, Y2);
-        i2 = (int)(X2 - XF + 1); j2 = (int)(Y2 - YF + 1);
+        to_block(b, bf, C.level + 1, 2 * (X0 - 1) + x, 2 * (Y0 - 1) + y, X2, Y2);
+        i2 = X2 - XF + 1; j2 = Y2 - YF + 1;
+    }
+    Aff child_map(const PatchInfo& C, const PatchInfo& F) const
+    {
+        long a0, b0, a1, b1, a2, b2;
+        child(C, 0, 0, F, a0, b0); child(C, 1, 0, F, a1, b1); child(C, 0, 1, F, a2, b2);
+        return {a0, b0, a1 - a0, a2 - a0, b1 - b0, b2 - b0};
     }
 };
 
 // Keeps the last entry written to each destination, in first-write order.  The
-// destination cell (slot p, plane-0 offset c) indexes a dense slot map shared by
-// all tables of a build; the touched slots are cleared again on destruction.
+// destination cell (patch p >= p0, plane-0 offset within p) indexes a dense map
+// over the patches from p0 on; the touched cells are cleared again on destruction.
 template <class E>
 struct LastWriter {
-    std::vector<E> v;
+    std::vector<E>& v;
     std::vector<int>& at;
-    int nq, nxy;
+    int nq, nxy, p0;
     std::vector<int> touched;
-    LastWriter(std::vector<int>& slots, int nq_, int nxy_) : at(slots), nq(nq_), nxy(nxy_) {}
+    bool outside = false;                  // a destination outside the map (not a finer neighbour)
+    LastWriter(std::vector<E>& out, std::vector<int>& slots, int nq_, int nxy_, int p0_)
+        : v(out), at(slots), nq(nq_), nxy(nxy_), p0(p0_) {}
     ~LastWriter() { for (int k : touched) at[k] = -1; }
-    void put(const E& e)
+    void put(const E& e, int p)
     {
-        const int k = (e.dst / nq) * nxy + e.dst % nq;
+        const long k = (long)(p - p0) * nxy + (e.dst - (long)p * nq);
+        if (k < 0 || k >= (long)at.size()) { outside = true; return; }
         int& a = at[k];
-        if (a < 0) { a = (int)v.size(); touched.push_back(k); v.push_back(e); }
+        if (a < 0) { a = (int)v.size(); touched.push_back((int)k); v.push_back(e); }
         else v[a] = e;
     }
 };
 
+// Entries of the tables whose destinations are cells of the patch being visited (copy:
+// its ghost cells from its same-size neighbours; average: a coarse patch's ghost cells
+// from its finer neighbours).  These need no last-writer map: the four face strips
+// (ghost rows along 1..mx or 1..my) and the four corner blocks are disjoint, each face
+// or corner has one same-size neighbour, and the children of one coarse ghost cell lie
+// in one of the two half-size neighbours of its face, so no cell is written twice.
+inline bool src_in(const CopyEnt& e, long nall) { return e.src >= 0 && e.src < nall; }
+inline bool src_in(const AvgEnt& e, long nall)
+{
+    const long s = e.src, s3 = s + e.sx + e.sy;
+    return s >= 0 && s < nall && s + e.sx >= 0 && s + e.sx < nall && s + e.sy >= 0 && s + e.sy < nall && s3 >= 0 && s3 < nall;
+}
+template <class E>
+struct PatchWriter {
+    std::vector<E>& v;
+    int base, nxy;                         // absolute offset of the visited patch's cell 0; cells per plane
+    long nall;                             // cells of the q slab (sources index into it)
+    bool outside = false;
+    void put(const E& e)
+    {
+        const int k = e.dst - base;
+        if (k < 0 || k >= nxy || !src_in(e, nall)) { outside = true; return; }
+        v.push_back(e);
+    }
+};
+
+// Runs tasks 0..n-1 on up to nt threads (the calling one included).
+template <class Fn>
+void run_tasks(int n, int nt, Fn fn)
+{
+    nt = std::max(1, std::min(nt, n));
+    if (nt == 1) { for (int i = 0; i < n; i++) fn(i); return; }
+    std::atomic<int> next{0};
+    auto loop = [&]() { for (int i; (i = next.fetch_add(1)) < n;) fn(i); };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; t++) th.emplace_back(loop);
+    loop();
+    for (auto& x : th) x.join();
+}
+
 }  // namespace
 
 // Every gather index must lie in the q slab: a wrong transform would otherwise send the
-// ghost-fill kernels outside it.
-static bool tables_in_bounds(const std::vector<LevelTables>& out, long nall, int& bad_level)
+// ghost-fill kernels outside it (copy and average entries are checked as they are made).
+static bool tables_in_bounds(const Tables& T, long nall)
 {
     auto ok = [&](long k) { return k >= 0 && k < nall; };
-    for (size_t l = 0; l < out.size(); l++) {
-        const LevelTables& T = out[l];
-        bool good = true;
-        for (const CopyEnt& e : T.copy) good = good && ok(e.dst) && ok(e.src);
-        for (const AvgEnt& e : T.avg)
-            good = good && ok(e.dst) && ok(e.src) && ok((long)e.src + e.sx) && ok((long)e.src + e.sy) &&
-                   ok((long)e.src + e.sx + e.sy);
-        for (const InterpEnt& e : T.interp) good = good && ok(e.dst) && ok(e.src) && e.sub >= 0 && e.sub < 4;
-        for (const PhysEnt& e : T.phys) good = good && ok(e.dst) && ok(e.src);
-        if (!good) { bad_level = (int)l; return false; }
-    }
-    return true;
+    bool good = true;
+    for (const InterpEnt& e : T.interp) good = good && ok(e.dst) && ok(e.src) && e.sub >= 0 && e.sub < 4;
+    for (const PhysEnt& e : T.phys) good = good && ok(e.dst) && ok(e.src);
+    return good;
 }
 
-bool build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<LevelTables>& out, std::string& err)
+bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out, TableWork& w, std::string& err)
 {
     TableCtx T(f);
-    const int mx = T.mx, my = T.my, mbc = T.mbc;
+    const int mx = T.mx, my = T.my, mbc = T.mbc, nq = T.nq, np = f.np();
     const int nxy = T.nx * (my + 2 * mbc);
-    std::vector<int> slots((size_t)f.np() * nxy, -1);
-    out.assign(33, LevelTables());
-    for (int l = 0; l < 33; l++) {
-        LevelTables& LT = out[l];
-        const int p0 = f.lev_off[l], p1 = f.lev_off[l + 1];
-        if (p0 == p1) { LT.sync_start.assign(1, 0); continue; }
-        // ---- copy2ghost: face pass then corner pass (fclaw2d_clawpatch46_copy.f) ----
-        {
-            LastWriter<CopyEnt> W(slots, T.nq, nxy);
-            for (int ip = p0; ip < p1; ip++) {
-                const PatchInfo& P = f.p[ip];
-                for (int fc = 0; fc < 4; fc++) {
-                    if (P.face_type[fc] != NB_SAME) continue;
-                    const int n = P.face_nbr[fc][0];
-                    const PatchInfo& N = f.p[n];
-                    int ilo, ihi, jlo, jhi;
-                    if (fc == 0) { ilo = 1 - mbc; ihi = 0; jlo = 1; jhi = my; }
-                    else if (fc == 1) { ilo = mx + 1; ihi = mx + mbc; jlo = 1; jhi = my; }
-                    else if (fc == 2) { ilo = 1; ihi = mx; jlo = 1 - mbc; jhi = 0; }
-                    else { ilo = 1; ihi = mx; jlo = my + 1; jhi = my + mbc; }
-                    for (int j = jlo; j <= jhi; j++)
-                        for (int i = ilo; i <= ihi; i++) {
-                            int i2, j2; T.same(P, i, j, N, i2, j2);
-                            W.put({T.cell(ip, i, j), T.cell(n, i2, j2)});
-                        }
-                }
+    int nt = (int)std::thread::hardware_concurrency();
+    nt = std::max(1, std::min(nt, std::min(16, np / 64)));
+    // one chunk of patches per task for copy and average (destinations in the visited
+    // patch); interpolation (destinations in the next finer level) one task per level
+    const int nchunk = nt == 1 ? 1 : 4 * nt;
+    int nlev = 0;
+    for (int l = 0; l < 33; l++) if (f.lev_off[l + 1] > f.lev_off[l]) nlev = l + 1;
+    w.copy.resize(nchunk); w.avg.resize(nchunk); w.interp.resize(33); w.slots.resize(33);
+    w.copy_first.assign(np + 1, 0); w.avg_first.assign(np + 1, 0);
+    std::atomic<int> bad{0};
+
+    // ---- copy2ghost (faces, then corners, of each patch: fclaw2d_clawpatch46_copy.f) and
+    // ---- average2ghost (coarse = this patch: faces, then corners) ----
+    auto copy_avg = [&](int c) {
+        const int a = (int)((long)np * c / nchunk), b = (int)((long)np * (c + 1) / nchunk);
+        std::vector<CopyEnt>& vc = w.copy[c];
+        std::vector<AvgEnt>& va = w.avg[c];
+        vc.clear(); va.clear();
+        PatchWriter<CopyEnt> WC{vc, 0, nxy, (long)np * nq};
+        for (int ip = a; ip < b; ip++) {
+            w.copy_first[ip] = (int)vc.size();
+            WC.base = ip * nq;
+            const PatchInfo& P = f.p[ip];
+            for (int fc = 0; fc < 4; fc++) {
+                if (P.face_type[fc] != NB_SAME) continue;
+                const int n = P.face_nbr[fc][0];
+                const TableCtx::Aff A = T.same_map(P, f.p[n]);
+                int ilo, ihi, jlo, jhi;
+                if (fc == 0) { ilo = 1 - mbc; ihi = 0; jlo = 1; jhi = my; }
+                else if (fc == 1) { ilo = mx + 1; ihi = mx + mbc; jlo = 1; jhi = my; }
+                else if (fc == 2) { ilo = 1; ihi = mx; jlo = 1 - mbc; jhi = 0; }
+                else { ilo = 1; ihi = mx; jlo = my + 1; jhi = my + mbc; }
+                for (int j = jlo; j <= jhi; j++)
+                    for (int i = ilo; i <= ihi; i++) {
+                        int i2, j2; A.map(i, j, i2, j2);
+                        WC.put({T.cell(ip, i, j), T.cell(n, i2, j2)});
+                    }
             }
-            for (int ip = p0; ip < p1; ip++) {
-                const PatchInfo& P = f.p[ip];
-                for (int c = 0; c < 4; c++) {
-                    if (!P.has_corner[c] || P.corner_type[c] != NB_SAME) continue;
-                    const int n = P.corner_nbr[c];
-                    const PatchInfo& N = f.p[n];
-                    for (int ibc = 1; ibc <= mbc; ibc++)
-                        for (int jbc = 1; jbc <= mbc; jbc++) {
-                            const int i1 = (c & 1) ? mx + ibc : 1 - ibc, j1 = (c & 2) ? my + jbc : 1 - jbc;
-                            int i2, j2; T.same(P, i1, j1, N, i2, j2);
-                            W.put({T.cell(ip, i1, j1), T.cell(n, i2, j2)});
-                        }
-                }
+            for (int cr = 0; cr < 4; cr++) {
+                if (!P.has_corner[cr] || P.corner_type[cr] != NB_SAME) continue;
+                const int n = P.corner_nbr[cr];
+                const TableCtx::Aff A = T.same_map(P, f.p[n]);
+                for (int ibc = 1; ibc <= mbc; ibc++)
+                    for (int jbc = 1; jbc <= mbc; jbc++) {
+                        const int i1 = (cr & 1) ? mx + ibc : 1 - ibc, j1 = (cr & 2) ? my + jbc : 1 - jbc;
+                        int i2, j2; A.map(i1, j1, i2, j2);
+                        WC.put({T.cell(ip, i1, j1), T.cell(n, i2, j2)});
+                    }
             }
-            LT.copy = std::move(W.v);
         }
-        // ---- average2ghost (coarse = this level) ----
-        {
-            LastWriter<AvgEnt> W(slots, T.nq, nxy);
-            auto valid = [&](int i, int j) { return 1 <= i && i <= mx && 1 <= j && j <= my; };
+        PatchWriter<AvgEnt> WA{va, 0, nxy, (long)np * nq};
+        auto valid = [&](int i, int j) { return 1 <= i && i <= mx && 1 <= j && j <= my; };
+        for (int ip = a; ip < b; ip++) {
+            w.avg_first[ip] = (int)va.size();
+            WA.base = ip * nq;
+            const PatchInfo& C = f.p[ip];
+            if (!C.on_cf) continue;
             // the four children of coarse ghost cell (ic, jc) in F, skipped unless all are
             // interior cells of F (fclaw2d_clawpatch_is_valid_average)
-            auto emit = [&](int ip, const PatchInfo& C, int ic, int jc, int fi, const PatchInfo& F, bool check) {
+            auto emit = [&](int ic, int jc, int fi, const TableCtx::Aff& F, bool check) {
                 int ci[4], cj[4];
                 for (int m = 0; m < 4; m++) {
-                    T.child(C, ic, jc, m & 1, m >> 1, F, ci[m], cj[m]);
+                    F.map(2 * ic + (m & 1), 2 * jc + (m >> 1), ci[m], cj[m]);
                     if (check && !valid(ci[m], cj[m])) return;
                 }
                 const int src = T.cell(fi, ci[0], cj[0]);
-                W.put({T.cell(ip, ic, jc), src, T.cell(fi, ci[1], cj[1]) - src, T.cell(fi, ci[2], cj[2]) - src});
+                WA.put({T.cell(ip, ic, jc), src, T.cell(fi, ci[1], cj[1]) - src, T.cell(fi, ci[2], cj[2]) - src});
             };
-            for (int ip = p0; ip < p1; ip++) {
-                const PatchInfo& C = f.p[ip];
-                if (!C.on_cf) continue;
-                for (int fc = 0; fc < 4; fc++) {
-                    if (C.face_type[fc] != NB_HALF) continue;
-                    for (int ig = 0; ig < 2; ig++) {
-                        const int fi = C.face_nbr[fc][ig];
-                        const PatchInfo& F = f.p[fi];
-                        if (fc < 2) {
-                            for (int jc = 1; jc <= my; jc++)
-                                for (int ibc = 1; ibc <= mbc; ibc++)
-                                    emit(ip, C, (fc == 0) ? 1 - ibc : mx + ibc, jc, fi, F, true);
-                        } else {
-                            for (int jbc = 1; jbc <= mbc; jbc++)
-                                for (int ic = 1; ic <= mx; ic++)
-                                    emit(ip, C, ic, (fc == 2) ? 1 - jbc : my + jbc, fi, F, true);
-                        }
-                    }
-                }
-            }
-            for (int ip = p0; ip < p1; ip++) {
-                const PatchInfo& C = f.p[ip];
-                if (!C.on_cf) continue;
-                for (int c = 0; c < 4; c++) {
-                    if (!C.has_corner[c] || C.corner_type[c] != NB_HALF) continue;
-                    const int fi = C.corner_nbr[c];
-                    const PatchInfo& F = f.p[fi];
-                    for (int ibc = 1; ibc <= mbc; ibc++)
+            for (int fc = 0; fc < 4; fc++) {
+                if (C.face_type[fc] != NB_HALF) continue;
+                for (int ig = 0; ig < 2; ig++) {
+                    const int fi = C.face_nbr[fc][ig];
+                    const TableCtx::Aff F = T.child_map(C, f.p[fi]);
+                    if (fc < 2) {
+                        for (int jc = 1; jc <= my; jc++)
+                            for (int ibc = 1; ibc <= mbc; ibc++) emit((fc == 0) ? 1 - ibc : mx + ibc, jc, fi, F, true);
+                    } else {
                         for (int jbc = 1; jbc <= mbc; jbc++)
-                            emit(ip, C, (c & 1) ? mx + ibc : 1 - ibc, (c & 2) ? my + jbc : 1 - jbc, fi, F, false);
+                            for (int ic = 1; ic <= mx; ic++) emit(ic, (fc == 2) ? 1 - jbc : my + jbc, fi, F, true);
+                    }
                 }
             }
-            LT.avg = std::move(W.v);
+            for (int cr = 0; cr < 4; cr++) {
+                if (!C.has_corner[cr] || C.corner_type[cr] != NB_HALF) continue;
+                const int fi = C.corner_nbr[cr];
+                const TableCtx::Aff F = T.child_map(C, f.p[fi]);
+                for (int ibc = 1; ibc <= mbc; ibc++)
+                    for (int jbc = 1; jbc <= mbc; jbc++)
+                        emit((cr & 1) ? mx + ibc : 1 - ibc, (cr & 2) ? my + jbc : 1 - jbc, fi, F, false);
+            }
         }
-        // ---- interpolate2ghost (coarse = this level) ----
-        {
-            LastWriter<InterpEnt> W(slots, T.nq, nxy);
-            auto validi = [&](int i, int j) { return 1 - mbc <= i && i <= mx + mbc && 1 - mbc <= j && j <= my + mbc; };
-            // the fine cells of the four children (coarse axes, sub = ii + 2 jj) of coarse
-            // cell (ic, jc), skipped unless all lie in F's padded patch (is_valid_interp)
-            auto emit = [&](int cp, const PatchInfo& C, int ic, int jc, int fp, const PatchInfo& F, bool check) {
-                int ci[4], cj[4];
-                for (int m = 0; m < 4; m++) {
-                    T.child(C, ic, jc, m & 1, m >> 1, F, ci[m], cj[m]);
-                    if (check && !validi(ci[m], cj[m])) return;
-                }
-                for (int m = 0; m < 4; m++) W.put({T.cell(fp, ci[m], cj[m]), T.cell(cp, ic, jc), m, 0});
-            };
-            for (int ip = p0; ip < p1; ip++) {
-                const PatchInfo& C = f.p[ip];
-                if (!C.on_cf) continue;
-                for (int fc = 0; fc < 4; fc++) {
-                    if (C.face_type[fc] != NB_HALF) continue;
-                    for (int ig = 0; ig < 2; ig++) {
-                        const int fi = C.face_nbr[fc][ig];
-                        const PatchInfo& F = f.p[fi];
-                        if (fc < 2) {
-                            for (int ibc = 1; ibc <= mbc / 2; ibc++) {
-                                const int ic = (fc == 0) ? ibc : mx - ibc + 1;
-                                for (int jc = 1; jc <= mx; jc++) emit(ip, C, ic, jc, fi, F, true);
-                            }
-                        } else {
-                            for (int jbc = 1; jbc <= mbc / 2; jbc++) {
-                                const int jc = (fc == 2) ? jbc : my - jbc + 1;
-                                for (int ic = 1; ic <= mx; ic++) emit(ip, C, ic, jc, fi, F, true);
-                            }
+        if (WC.outside || WA.outside) bad = 1;
+    };
+
+    // ---- interpolate2ghost (coarse = level l): faces of all coarse patches, then corners ----
+    auto interp = [&](int l) {
+        std::vector<InterpEnt>& v = w.interp[l];
+        v.clear();
+        const int p0 = f.lev_off[l], p1 = f.lev_off[l + 1];
+        if (p0 == p1 || l >= 32) return;
+        std::vector<int>& slots = w.slots[l];
+        slots.assign((size_t)(f.lev_off[l + 2] - p1) * nxy, -1);
+        LastWriter<InterpEnt> W(v, slots, nq, nxy, p1);
+        auto validi = [&](int i, int j) { return 1 - mbc <= i && i <= mx + mbc && 1 - mbc <= j && j <= my + mbc; };
+        // the fine cells of the four children (coarse axes, sub = ii + 2 jj) of coarse
+        // cell (ic, jc), skipped unless all lie in F's padded patch (is_valid_interp)
+        auto emit = [&](int cp, int ic, int jc, int fp, const TableCtx::Aff& F, bool check) {
+            int ci[4], cj[4];
+            for (int m = 0; m < 4; m++) {
+                F.map(2 * ic + (m & 1), 2 * jc + (m >> 1), ci[m], cj[m]);
+                if (check && !validi(ci[m], cj[m])) return;
+            }
+            for (int m = 0; m < 4; m++) W.put({T.cell(fp, ci[m], cj[m]), T.cell(cp, ic, jc), m, 0}, fp);
+        };
+        for (int ip = p0; ip < p1; ip++) {
+            const PatchInfo& C = f.p[ip];
+            if (!C.on_cf) continue;
+            for (int fc = 0; fc < 4; fc++) {
+                if (C.face_type[fc] != NB_HALF) continue;
+                for (int ig = 0; ig < 2; ig++) {
+                    const int fi = C.face_nbr[fc][ig];
+                    const TableCtx::Aff F = T.child_map(C, f.p[fi]);
+                    if (fc < 2) {
+                        for (int ibc = 1; ibc <= mbc / 2; ibc++) {
+                            const int ic = (fc == 0) ? ibc : mx - ibc + 1;
+                            for (int jc = 1; jc <= mx; jc++) emit(ip, ic, jc, fi, F, true);
+                        }
+                    } else {
+                        for (int jbc = 1; jbc <= mbc / 2; jbc++) {
+                            const int jc = (fc == 2) ? jbc : my - jbc + 1;
+                            for (int ic = 1; ic <= mx; ic++) emit(ip, ic, jc, fi, F, true);
                         }
                     }
                 }
             }
-            for (int ip = p0; ip < p1; ip++) {
-                const PatchInfo& C = f.p[ip];
-                if (!C.on_cf) continue;
-                for (int c = 0; c < 4; c++) {
-                    if (!C.has_corner[c] || C.corner_type[c] != NB_HALF) continue;
-                    const int fi = C.corner_nbr[c];
-                    const PatchInfo& F = f.p[fi];
-                    for (int ibc = 1; ibc <= mbc / 2; ibc++)
-                        for (int jbc = 1; jbc <= mbc / 2; jbc++)
-                            emit(ip, C, (c & 1) ? mx - ibc + 1 : ibc, (c & 2) ? my - jbc + 1 : jbc, fi, F, false);
-                }
-            }
-            LT.interp = std::move(W.v);
         }
+        for (int ip = p0; ip < p1; ip++) {
+            const PatchInfo& C = f.p[ip];
+            if (!C.on_cf) continue;
+            for (int cr = 0; cr < 4; cr++) {
+                if (!C.has_corner[cr] || C.corner_type[cr] != NB_HALF) continue;
+                const int fi = C.corner_nbr[cr];
+                const TableCtx::Aff F = T.child_map(C, f.p[fi]);
+                for (int ibc = 1; ibc <= mbc / 2; ibc++)
+                    for (int jbc = 1; jbc <= mbc / 2; jbc++)
+                        emit(ip, (cr & 1) ? mx - ibc + 1 : ibc, (cr & 2) ? my - jbc + 1 : jbc, fi, F, false);
+            }
+        }
+        if (W.outside) bad = 1;
+    };
+    // the finest levels hold most patches: their interpolation tasks go first
+    run_tasks(nchunk + nlev, nt, [&](int k) {
+        if (k < nlev) interp(nlev - 1 - k);
+        else copy_avg(k - nlev);
+    });
+    if (bad) { err = "a ghost-fill table writes outside its destination patches"; return false; }
+
+    // flat tables in level order: the chunks are contiguous in slot order, so are the levels
+    auto concat = [&](std::vector<std::vector<CopyEnt>>* pc, std::vector<std::vector<AvgEnt>>* pa) {
+        size_t tot = 0;
+        if (pc) for (auto& v : *pc) tot += v.size();
+        if (pa) for (auto& v : *pa) tot += v.size();
+        return tot;
+    };
+    out.copy.resize(concat(&w.copy, nullptr));
+    out.avg.resize(concat(nullptr, &w.avg));
+    {
+        size_t oc = 0, oa = 0;
+        for (int c = 0; c < nchunk; c++) {
+            const int a = (int)((long)np * c / nchunk), b = (int)((long)np * (c + 1) / nchunk);
+            for (int ip = a; ip < b; ip++) { w.copy_first[ip] += (int)oc; w.avg_first[ip] += (int)oa; }
+            std::copy(w.copy[c].begin(), w.copy[c].end(), out.copy.begin() + oc);
+            std::copy(w.avg[c].begin(), w.avg[c].end(), out.avg.begin() + oa);
+            oc += w.copy[c].size(); oa += w.avg[c].size();
+        }
+        w.copy_first[np] = (int)oc; w.avg_first[np] = (int)oa;
+    }
+    out.interp.clear(); out.phys.clear(); out.ti.clear(); out.sync.clear(); out.sync_start.assign(1, 0);
+    for (int l = 0; l < 33; l++) {
+        const int p0 = f.lev_off[l], p1 = f.lev_off[l + 1];
+        out.copy_off[l] = w.copy_first[p0];
+        out.avg_off[l] = w.avg_first[p0];
+        out.interp_off[l] = (int)out.interp.size();
+        out.phys_off[l] = (int)out.phys.size();
+        out.ti_off[l] = (int)out.ti.size();
+        out.grp_off[l] = (int)out.sync_start.size() - 1;
+        if (p0 == p1) continue;
+        out.interp.insert(out.interp.end(), w.interp[l].begin(), w.interp[l].end());
         // ---- setphysical: clawpack46_bc2_default with chains resolved per patch ----
         {
             std::vector<int> wsrc(nxy, -1), wneg(nxy, 0), wconst(nxy, 0);
@@ -739,11 +864,11 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<
                 if (bc[2] == 3) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, 1 - jbc, i, jbc, NEG3);
                 if (bc[3] == 1) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, my + jbc, i, my, 0);
                 if (bc[3] == 3) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, my + jbc, i, my + 1 - jbc, NEG3);
-                for (int dst : order) LT.phys.push_back({dst, wsrc[dst - base], wneg[dst - base], wconst[dst - base]});
+                for (int dst : order) out.phys.push_back({dst, wsrc[dst - base], wneg[dst - base], wconst[dst - base]});
             }
         }
         // ---- time interpolation patches ----
-        for (int ip = p0; ip < p1; ip++) if (f.p[ip].has_fine_nbr) LT.ti.push_back(ip);
+        for (int ip = p0; ip < p1; ip++) if (f.p[ip].has_fine_nbr) out.ti.push_back(ip);
         // ---- time sync ops ----
         // fclaw2d_time_sync applies the same-size corrections of every synced level,
         // then the fine-to-coarse ones (src/fclaw2d_time_sync.c:118-202); each
@@ -752,13 +877,12 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<
         // the f2c ops ((face, igrid) order) give every cell its additions in the
         // reference's order.  Levels without finer neighbours have no f2c ops, so
         // one range of levels [a, maxlevel] covers both kinds.
-        LT.sync_start.push_back(0);
         for (int ip = p0; ip < p1; ip++) {
             const PatchInfo& P = f.p[ip];
             int nops = 0;
             for (int fc = 0; fc < 4; fc++)
                 if (P.face_type[fc] == NB_SAME && (!f.sphere() || f.p[P.face_nbr[fc][0]].block == P.block)) {
-                    LT.sync.push_back({ip, P.face_nbr[fc][0], fc, 0, 0, SYNC_SAMESIZE, {0, 0}});
+                    out.sync.push_back({ip, P.face_nbr[fc][0], fc, 0, 0, SYNC_SAMESIZE, {0, 0}});
                     nops++;
                 }
             for (int fc = 0; fc < 4; fc++) {
@@ -768,16 +892,21 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<
                     const int fi = P.face_nbr[fc][ig];
                     const PatchInfo& F = f.p[fi];
                     const int noff = (fc < 2) ? (2 * P.gy - F.gy) * my : (2 * P.gx - F.gx) * mx;
-                    LT.sync.push_back({ip, fi, fc, ig, noff, SYNC_F2C, {0, 0}});
+                    out.sync.push_back({ip, fi, fc, ig, noff, SYNC_F2C, {0, 0}});
                     nops++;
                 }
             }
-            if (nops) LT.sync_start.push_back((int)LT.sync.size());
+            if (nops) out.sync_start.push_back((int)out.sync.size());
         }
     }
-    int bad = -1;
-    if (!tables_in_bounds(out, (long)f.np() * T.nq, bad)) {
-        err = "ghost-fill table of level " + std::to_string(bad) + " indexes outside the patches (bad transform)";
+    out.copy_off[33] = (int)out.copy.size();
+    out.avg_off[33] = (int)out.avg.size();
+    out.interp_off[33] = (int)out.interp.size();
+    out.phys_off[33] = (int)out.phys.size();
+    out.ti_off[33] = (int)out.ti.size();
+    out.grp_off[33] = (int)out.sync_start.size() - 1;
+    if (!tables_in_bounds(out, (long)np * nq)) {
+        err = "a ghost-fill table indexes outside the patches (bad transform)";
         return false;
     }
     return true;

@@ -31,6 +31,43 @@ void cs_xform(int b, int f, long N, long X, long Y, long& X2, long& Y2);
 // The face of block a whose neighbour is block b (-1: not adjacent, or a == b).
 int cs_face_to(int a, int b);
 
+// Open-addressing map from 64-bit keys (Forest::key) to slots, for the lookups of
+// neighbour searches and balance: linear probing over a power-of-two table.
+class KeyIndex {
+public:
+    void reset(size_t n)
+    {
+        size_t cap = 16;
+        while (cap < 2 * n + 16) cap <<= 1;
+        keys_.assign(cap, EMPTY);
+        vals_.assign(cap, -1);
+        mask_ = cap - 1;
+    }
+    void put(uint64_t k, int v)
+    {
+        size_t h = hash(k);
+        while (keys_[h] != EMPTY && keys_[h] != k) h = (h + 1) & mask_;
+        keys_[h] = k;
+        vals_[h] = v;
+    }
+    int get(uint64_t k) const
+    {
+        if (keys_.empty()) return -1;
+        size_t h = hash(k);
+        while (keys_[h] != EMPTY) {
+            if (keys_[h] == k) return vals_[h];
+            h = (h + 1) & mask_;
+        }
+        return -1;
+    }
+private:
+    static constexpr uint64_t EMPTY = ~0ull;
+    size_t hash(uint64_t k) const { return (size_t)((k * 0x9E3779B97F4A7C15ull) >> 17) & mask_; }
+    std::vector<uint64_t> keys_;
+    std::vector<int> vals_;
+    size_t mask_ = 0;
+};
+
 struct PatchInfo {
     int level, gx, gy, block;
     int inst;
@@ -86,7 +123,7 @@ public:
     }
 
 private:
-    std::unordered_map<uint64_t, int> index_;
+    KeyIndex index_;
 };
 
 // Refine marked leaves, coarsen fully marked families, then 2:1 balance
@@ -122,18 +159,33 @@ struct PartitionPlan {
 // The plan of `rank` among `size` ranks for forest f (pure host computation).
 void make_partition(const Forest& f, int rank, int size, PartitionPlan& out);
 
-// Gather tables of one level.
-struct LevelTables {
+// Gather tables of a forest, flat in level order: level l's entries of table x are
+// x[x_off[l], x_off[l + 1]).
+struct Tables {
     std::vector<CopyEnt> copy;       // copy2ghost(level)
     std::vector<AvgEnt> avg;         // average2ghost(level): level is the coarse level
     std::vector<InterpEnt> interp;   // interpolate2ghost(level): level is the coarse level
     std::vector<PhysEnt> phys;       // setphysical(level)
     std::vector<int> ti;             // patches with fine-grid neighbours (fclaw2d_timeinterp)
-    std::vector<SyncOp> sync; std::vector<int> sync_start;   // time-sync corrections grouped per patch
+    // time-sync corrections grouped per patch: group g is sync[sync_start[g], sync_start[g + 1]),
+    // level l's groups are [grp_off[l], grp_off[l + 1])
+    std::vector<SyncOp> sync;
+    std::vector<int> sync_start;
+    int copy_off[34], avg_off[34], interp_off[34], phys_off[34], ti_off[34], grp_off[34];
 };
 
-// inflow: mthbc = 0 sides are set to a constant state (PhysEnt.pad = 1, src unused).
+// Buffers build_tables keeps between calls (their pages stay mapped from one regrid
+// to the next).
+struct TableWork {
+    std::vector<std::vector<CopyEnt>> copy;
+    std::vector<std::vector<AvgEnt>> avg;
+    std::vector<std::vector<InterpEnt>> interp;
+    std::vector<std::vector<int>> slots;
+    std::vector<int> copy_first, avg_first;
+};
+
+// inflow: mthbc = 0 sides are set to a constant state (PhysEnt.cst = 1, src unused).
 // False (with err) if a table would index outside the patches.
-bool build_tables(const Forest& f, const int mthbc[4], bool inflow, std::vector<LevelTables>& out, std::string& err);
+bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out, TableWork& w, std::string& err);
 
 }  // namespace fcb
