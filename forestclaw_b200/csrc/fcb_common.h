@@ -65,6 +65,7 @@ struct StepParams {
 // Kernel-side failures reported through the status word (read by the host after a step).
 enum { STATUS_NEWTON = 1,       // exact Euler: Newton did not converge from the seed nor from PVRS
        STATUS_DEPTH = 2,        // shallow water: negative depth in a patch
-       STATUS_NONFINITE = 4 };  // a non-finite value in q
+       STATUS_NONFINITE = 4,    // a non-finite value in q
+       STATUS_STAGING = 8 };    // a patch's asynchronous copy into shared memory did not arrive
 
 }  // namespace fcb

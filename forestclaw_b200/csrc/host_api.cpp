@@ -25,20 +25,38 @@
 using namespace fcb;
 
 // Patch-to-CTA variants of the fused update compiled for one solver shape (first: default).
-static std::vector<const Step2Variant*> step2_variants(int precision, int rp, int mx, int my, int mbc)
+// A specialised kernel (spec = its limiter) applies to the second-order method with
+// second-order transverse terms, that limiter on every one of 3 waves of 3 fields, no
+// capacity, no aux and no cubed sphere.
+static bool spec_applies(const Step2Variant& v, const fc2d_b200_options_t& o)
+{
+    if (v.spec == 0) return true;
+    if (o.order[0] != 2 || o.order[1] != 2 || o.mcapa != 0 || o.maux != 0 || o.meqn != 3 || o.mwaves != 3 ||
+        o.app == FC2D_B200_APP_SPHERE)
+        return false;
+    for (int w = 0; w < 3; w++)
+        if (o.mthlim[w] != v.spec) return false;
+    return true;
+}
+
+// Patch-to-CTA variants of the fused update compiled for one solver shape (first: default).
+// Where a specialised kernel applies, only its variants are offered, so that every
+// variant the autotuner may pick gives the same results.
+static std::vector<const Step2Variant*> step2_variants(const fc2d_b200_options_t& o, int rp)
 {
     using Table = const Step2Variant* (*)(int*);
     static const Table tables[] = {step2_table_f64_adv, step2_table_f64_sw, step2_table_f64_euler,
                                    step2_table_f32w_adv, step2_table_f32w_sw, step2_table_f32w_euler};
-    std::vector<const Step2Variant*> out;
+    std::vector<const Step2Variant*> out, spec;
     for (Table t : tables) {
         int n = 0;
         const Step2Variant* v = t(&n);
         for (int i = 0; i < n; i++)
-            if (v[i].precision == precision && v[i].rp == rp && v[i].mx == mx && v[i].my == my && v[i].mbc == mbc)
-                out.push_back(&v[i]);
+            if (v[i].precision == o.precision && v[i].rp == rp && v[i].mx == o.mx && v[i].my == o.my &&
+                v[i].mbc == o.mbc && spec_applies(v[i], o))
+                (v[i].spec ? spec : out).push_back(&v[i]);
     }
-    return out;
+    return spec.empty() ? out : spec;
 }
 
 static thread_local std::string g_err;
@@ -557,33 +575,29 @@ static GatherSeg<E> seg(const E* table, int off, int n, double* dst, const doubl
 {
     return GatherSeg<E>{dst, src, table + off, n};
 }
-static void copy_range(fc2d_b200_solver* s, int a, int b, int c)
+// average2ghost of coarse levels [a, b] and copy2ghost of levels [ca, cb] (with level c
+// of the time-interpolated copy for both) in one launch: the two stages write disjoint
+// ghost cells and read interior cells only, so their order does not matter
+static void average_copy_range(fc2d_b200_solver* s, int a, int b, int ca, int cb, int c)
 {
-    GatherSeg<CopyEnt> s0{nullptr, nullptr, nullptr, 0}, s1 = s0;
-    if (lrange(a, b)) {
-        const int off = s->lr[a].copy_off, n = s->lr[b].copy_off + s->lr[b].copy_n - off;
-        if (n > 0) s0 = seg(s->t_copy.p, off, n, s->q, s->q);
-    }
-    if (c >= 0 && c <= 32 && s->lr[c].copy_n > 0)
-        s1 = seg(s->t_copy.p, s->lr[c].copy_off, s->lr[c].copy_n, s->qinterp, s->qinterp);
-    if (s0.n + s1.n <= 0) return;
-    (void)flush_pending(s);
-    if (s->fill) s->total_launches++;
-    if (s->emit) launch_copy(s->d, s0, s1, s->st);
-}
-static void average_range(fc2d_b200_solver* s, int a, int b, int c)
-{
-    GatherSeg<AvgEnt> s0{nullptr, nullptr, nullptr, 0}, s1 = s0;
+    GatherSeg<AvgEnt> a0{nullptr, nullptr, nullptr, 0}, a1 = a0;
+    GatherSeg<CopyEnt> c0{nullptr, nullptr, nullptr, 0}, c1 = c0;
     if (lrange(a, b)) {
         const int off = s->lr[a].avg_off, n = s->lr[b].avg_off + s->lr[b].avg_n - off;
-        if (n > 0) s0 = seg(s->t_avg.p, off, n, s->q, s->q);
+        if (n > 0) a0 = seg(s->t_avg.p, off, n, s->q, s->q);
     }
     if (c >= 0 && c <= 32 && s->lr[c].avg_n > 0)
-        s1 = seg(s->t_avg.p, s->lr[c].avg_off, s->lr[c].avg_n, s->qinterp, s->q);
-    if (s0.n + s1.n <= 0) return;
+        a1 = seg(s->t_avg.p, s->lr[c].avg_off, s->lr[c].avg_n, s->qinterp, s->q);
+    if (lrange(ca, cb)) {
+        const int off = s->lr[ca].copy_off, n = s->lr[cb].copy_off + s->lr[cb].copy_n - off;
+        if (n > 0) c0 = seg(s->t_copy.p, off, n, s->q, s->q);
+    }
+    if (c >= 0 && c <= 32 && s->lr[c].copy_n > 0)
+        c1 = seg(s->t_copy.p, s->lr[c].copy_off, s->lr[c].copy_n, s->qinterp, s->qinterp);
+    if (a0.n + a1.n + c0.n + c1.n <= 0) return;
     (void)flush_pending(s);
     if (s->fill) s->total_launches++;
-    if (s->emit) launch_average(s->d, s0, s1, s->area, s->st);
+    if (s->emit) launch_average_copy(s->d, a0, a1, c0, c1, s->area, s->st);
 }
 static void phys_range(fc2d_b200_solver* s, int a, int b, int c)
 {
@@ -719,12 +733,13 @@ static void ghost_update(fc2d_b200_solver* s, int minlevel, int maxlevel, int ti
         for (int l = std::max(minlevel, 0); l <= std::min(maxlevel, 63); l++) s->phys_ok[l] = 1;
     const int mincoarse = minlevel, maxcoarse = maxlevel - 1;
     const int ti = time_interp ? mincoarse - 1 : -1;      // level of the time-interpolated copy
-    average_range(s, mincoarse, maxcoarse, ti);
-    copy_range(s, minlevel, maxlevel, ti);
+    average_copy_range(s, mincoarse, maxcoarse, minlevel, maxlevel, ti);
     phys_range(s, mincoarse, maxcoarse, ti);
     interpolate_levels(s, mincoarse, maxcoarse, time_interp);
-    const int minfine = mincoarse + 1, maxfine = maxlevel;
-    phys_range(s, minfine, maxfine, ti);
+    // the reference applies the physical BC to the fine levels [mincoarse+1, maxlevel],
+    // then to every level [minlevel, maxlevel]; a physical-BC entry reads no cell any
+    // physical-BC entry writes, so the second pass rewrites the first's values and one
+    // pass over [minlevel, maxlevel] leaves the same fields
     phys_range(s, minlevel, maxlevel, ti);
 }
 
@@ -867,7 +882,7 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
     if (o.minlevel < 0 || o.maxlevel < o.minlevel || o.maxlevel > 20)
         return fail(FC2D_B200_EINVAL, "bad minlevel/maxlevel");
     const bool user = o.rp == FC2D_B200_RP_USER;
-    const bool sup = user || !step2_variants(o.precision, o.rp, o.mx, o.my, o.mbc).empty();
+    const bool sup = user || !step2_variants(o, o.rp).empty();
     if (!sup) return fail(FC2D_B200_EINVAL, "no compiled update kernel for this (rp, mx, my, mbc, precision)");
     if (user && (o.precision != FC2D_B200_PREC_FP64 || o.time_sync || o.mx != o.my || o.mbc != 2))
         return fail(FC2D_B200_EINVAL, "application solvers run in FP64, without time sync, on square patches with mbc 2");
@@ -927,7 +942,7 @@ extern "C" int fc2d_b200_create(const fc2d_b200_options_t* opt, fc2d_b200_solver
     }
     CK(cudaMallocHost(&s->params_host, sizeof(StepParams) * fc2d_b200_solver::PCAP));
     {   // set the kernel's shared-memory attribute outside any stream capture
-        s->vars = step2_variants(o.precision, o.rp, o.mx, o.my, o.mbc);
+        s->vars = step2_variants(o, o.rp);
         s->var = 0;
         for (int l = 0; l < 33; l++) s->var_lev[l] = -1;
         if (!s->vars.empty()) {   // application solvers arrive with fc2d_b200_set_user_variants
@@ -971,7 +986,7 @@ extern "C" int fc2d_b200_set_riemann(fc2d_b200_solver_t* s, int rp_id)
 {
     DeviceScope dev_scope_(s);
     if (!s) return fail(FC2D_B200_EINVAL, "null solver");
-    std::vector<const Step2Variant*> vars = step2_variants(s->o.precision, rp_id, s->o.mx, s->o.my, s->o.mbc);
+    std::vector<const Step2Variant*> vars = step2_variants(s->o, rp_id);
     if (vars.empty()) return fail(FC2D_B200_EINVAL, "Riemann solver id not compiled for these patch dimensions");
     s->o.rp = rp_id;
     s->vars = vars;
@@ -1232,6 +1247,7 @@ static std::string status_message(unsigned st)
     if (st & STATUS_NONFINITE) m += "a non-finite value in q; ";
     if (st & STATUS_DEPTH) m += "negative water depth; ";
     if (st & STATUS_NEWTON) m += "the exact Riemann solver's Newton iteration on p* converged neither from its seed nor from PVRS; ";
+    if (st & STATUS_STAGING) m += "a patch's copy into shared memory did not complete; ";
     if (!m.empty()) m.resize(m.size() - 2);
     return m;
 }

@@ -32,6 +32,18 @@ static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 // field-major within a segment, so a warp handles consecutive entries of one
 // field.  The fields of an entry are independent (same arithmetic per field).
 template <class E>
+__device__ __forceinline__ bool gather_index(const GatherSeg<E>& s0, const GatherSeg<E>& s1, int meqn, long t,
+                                             const GatherSeg<E>*& g, int& e, int& m)
+{
+    const long n0 = (long)s0.n * meqn;
+    g = &s0;
+    if (t >= n0) { t -= n0; g = &s1; }
+    if (t >= (long)g->n * meqn) return false;
+    m = (int)(t / g->n);
+    e = (int)(t - (long)m * g->n);
+    return true;
+}
+template <class E>
 __device__ __forceinline__ bool gather_item(const GatherSeg<E>& s0, const GatherSeg<E>& s1, int meqn,
                                             const GatherSeg<E>*& g, int& e, int& m)
 {
@@ -45,25 +57,15 @@ __device__ __forceinline__ bool gather_item(const GatherSeg<E>& s0, const Gather
     return true;
 }
 
-__global__ void k_copy(GatherSeg<CopyEnt> s0, GatherSeg<CopyEnt> s1, int nxy, int meqn)
+__device__ __forceinline__ void copy_item(const GatherSeg<CopyEnt>* g, int e, int m, int nxy)
 {
-    grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
-    grid_launch_dependents();
-    const GatherSeg<CopyEnt>* g;
-    int e, m;
-    if (!gather_item(s0, s1, meqn, g, e, m)) return;
     const CopyEnt c = g->e[e];
     g->dst[c.dst + m * nxy] = g->src[c.src + m * nxy];
 }
 
-__global__ void k_average(GatherSeg<AvgEnt> s0, GatherSeg<AvgEnt> s1, int nq, int nx, int nxy, int meqn,
-                          const double* __restrict__ area)
+__device__ __forceinline__ void average_item(const GatherSeg<AvgEnt>* g, int e, int m, int nq, int nx, int nxy,
+                                             const double* __restrict__ area)
 {
-    grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
-    grid_launch_dependents();
-    const GatherSeg<AvgEnt>* g;
-    int e, m;
-    if (!gather_item(s0, s1, meqn, g, e, m)) return;
     double* __restrict__ dst = g->dst;
     const double* __restrict__ src = g->src;
     const AvgEnt c = g->e[e];
@@ -92,6 +94,28 @@ __global__ void k_average(GatherSeg<AvgEnt> s0, GatherSeg<AvgEnt> s1, int nq, in
     sum = sum + f[o2];
     sum = sum + f[o3];
     dst[c.dst + m * nxy] = sum / 4.0;
+}
+
+// The average and copy stages of one ghost update in one launch: averaging writes
+// the ghost cells a coarse patch has beside finer neighbours, copying those beside
+// same-size neighbours (disjoint cells), and both read interior cells only, which
+// neither writes.  The average segments' threads come first.
+__global__ void k_average_copy(GatherSeg<AvgEnt> a0, GatherSeg<AvgEnt> a1, GatherSeg<CopyEnt> c0,
+                               GatherSeg<CopyEnt> c1, int nq, int nx, int nxy, int meqn,
+                               const double* __restrict__ area)
+{
+    grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
+    grid_launch_dependents();
+    const long na = ((long)a0.n + a1.n) * meqn;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    int e, m;
+    if (t < na) {
+        const GatherSeg<AvgEnt>* g;
+        if (gather_index(a0, a1, meqn, t, g, e, m)) average_item(g, e, m, nq, nx, nxy, area);
+    } else {
+        const GatherSeg<CopyEnt>* g;
+        if (gather_index(c0, c1, meqn, t - na, g, e, m)) copy_item(g, e, m, nxy);
+    }
 }
 
 // AMRClaw limited slopes (fclaw2d_clawpatch_utils.f:52-55, mth = 5)
@@ -654,16 +678,13 @@ void launch_restore_patches(const Dims& d, double* dst, const double* src, const
     if (n > 0) k_restore_patches<<<n, 256, 0, st>>>(dst, src, slots, d.nq());
 }
 
-void launch_copy(const Dims& d, const GatherSeg<CopyEnt>& s0, const GatherSeg<CopyEnt>& s1, cudaStream_t st)
+void launch_average_copy(const Dims& d, const GatherSeg<AvgEnt>& a0, const GatherSeg<AvgEnt>& a1,
+                         const GatherSeg<CopyEnt>& c0, const GatherSeg<CopyEnt>& c1, const double* area,
+                         cudaStream_t st)
 {
-    const long n = ((long)s0.n + s1.n) * d.meqn;
-    if (n > 0) launch_k(k_copy, nblk(n, 256), 256, 0, st, s0, s1, d.nxy(), d.meqn);
-}
-void launch_average(const Dims& d, const GatherSeg<AvgEnt>& s0, const GatherSeg<AvgEnt>& s1, const double* area,
-                    cudaStream_t st)
-{
-    const long n = ((long)s0.n + s1.n) * d.meqn;
-    if (n > 0) launch_k(k_average, nblk(n, 256), 256, 0, st, s0, s1, d.nq(), d.nx(), d.nxy(), d.meqn, area);
+    const long n = ((long)a0.n + a1.n + c0.n + c1.n) * d.meqn;
+    if (n > 0)
+        launch_k(k_average_copy, nblk(n, 256), 256, 0, st, a0, a1, c0, c1, d.nq(), d.nx(), d.nxy(), d.meqn, area);
 }
 void launch_interp(const Dims& d, const GatherSeg<InterpEnt>& s0, const GatherSeg<InterpEnt>& s1, cudaStream_t st)
 {

@@ -191,14 +191,17 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
     __syncthreads();
     if constexpr (RPHooks<RP>::B4) {
         // user b4step2, cell by cell over the padded patch (cudaclaw_flux2.cu:111-150):
-        // it may set the cell's aux from its q, position and time
+        // it may set the cell's aux from its q, position and time.  As the reference's
+        // b4step2 it changes the patch's aux in place (the only write to the aux slab
+        // during an update; each CTA writes its own patch)
+        double* ag = const_cast<double*>(aux) + (size_t)p * G::AUXS * NXY;
         for (int c = tid; c < NXY; c += NT) {
             double qc[MEQN], ac[G::AUXS > 0 ? G::AUXS : 1];
             for (int m = 0; m < MEQN; m++) qc[m] = Qs[m * NXY + c];
             for (int a = 0; a < G::AUXS; a++) ac[a] = As[a * NXY + c];
             RP::b4step2(MBC, MX, MY, MEQN, qc, pd.xlower, pd.ylower, dx, dy, sp.t, dt, G::AUXS, ac,
                         c % NX - MBC + 1, c / NX - MBC + 1);
-            for (int a = 0; a < G::AUXS; a++) As[a * NXY + c] = ac[a];
+            for (int a = 0; a < G::AUXS; a++) { As[a * NXY + c] = ac[a]; ag[a * NXY + c] = ac[a]; }
         }
         __syncthreads();
     }

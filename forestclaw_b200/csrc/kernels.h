@@ -49,6 +49,7 @@ struct Step2Variant {
     int smem;                  // dynamic shared memory per CTA, bytes
     int persistent;            // 1: a grid of resident CTAs loops over the patches
     Step2Fn fn;
+    int spec;                  // 0: any method flags; k > 0: a kernel specialised for limiter k (host checks the options)
 };
 // Layout version of the kernel parameter structs, checked when an application
 // registers update kernels compiled in its own module (include/fc2d_b200_user.cuh).
@@ -75,12 +76,13 @@ struct PhysEnt { int dst, src, neg, cst; };        // neg: bit m set => negate f
 
 // One table segment of a gather stage: entries e[0..n) from src into dst.
 template <class E> struct GatherSeg { double* dst; const double* src; const E* e; int n; };
-void launch_copy(const Dims& d, const GatherSeg<CopyEnt>& s0, const GatherSeg<CopyEnt>& s1, cudaStream_t st);
+// average segments and copy segments of one ghost update in one launch (disjoint ghost
+// cells); area: per-patch cell areas (nxy per patch, q's cell indexing) for the
+// area-weighted average of a manifold, or null for the plain mean.
+void launch_average_copy(const Dims& d, const GatherSeg<AvgEnt>& a0, const GatherSeg<AvgEnt>& a1,
+                         const GatherSeg<CopyEnt>& c0, const GatherSeg<CopyEnt>& c1, const double* area,
+                         cudaStream_t st);
 void launch_restore_patches(const Dims& d, double* dst, const double* src, const int* slots, int n, cudaStream_t st);
-// area: per-patch cell areas (nxy per patch, q's cell indexing) for the area-weighted
-// average of a manifold, or null for the plain mean.
-void launch_average(const Dims& d, const GatherSeg<AvgEnt>& s0, const GatherSeg<AvgEnt>& s1, const double* area,
-                    cudaStream_t st);
 void launch_interp(const Dims& d, const GatherSeg<InterpEnt>& s0, const GatherSeg<InterpEnt>& s1, cudaStream_t st);
 void launch_phys(const Dims& d, const GatherSeg<PhysEnt>& s0, const GatherSeg<PhysEnt>& s1, const double* bcstate,
                  cudaStream_t st);
