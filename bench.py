@@ -413,7 +413,7 @@ def _timed_steps(g, wl, steps, t, dt, flush):
     stream around each advance (graph replay); the regrid every regrid_interval
     steps runs between timed steps and is reported separately."""
     import torch
-    step_ms, cells, launches, regrid_ms = [], 0.0, 0, []
+    step_ms, cells, launches, regrid_ms, phases = [], 0.0, 0, [], []
     for k in range(steps):
         flush.fill_(float(k))
         torch.cuda.synchronize()
@@ -431,7 +431,9 @@ def _timed_steps(g, wl, steps, t, dt, flush):
             t0 = time.perf_counter()
             g.regrid()
             regrid_ms.append((time.perf_counter() - t0) * 1e3)
-    return dict(step_ms=step_ms, cells=cells, launches=launches, regrid_ms=regrid_ms, t=t, dt=dt)
+            phases.append(g.last_regrid_stats())
+    return dict(step_ms=step_ms, cells=cells, launches=launches, regrid_ms=regrid_ms, t=t, dt=dt,
+                regrid_phases=phases)
 
 
 def _roofline_pass(solvers, t_dt, flush, steps):
@@ -650,6 +652,8 @@ def run_ours(args, wl, rank, world, local_rank):
                               "the device time" if wl["regrid_interval"] else "none"),
                    "regrids_in_timed_loop": len(timed_regrid_ms),
                    "regrid_ms_median": float(np.median(regrid_ms + timed_regrid_ms)) if regrid_ms else None,
+                   "regrid_phase_ms_median": ({k: round(float(np.median([p[k] for p in r["regrid_phases"]])), 3)
+                                               for k in r["regrid_phases"][0]} if r.get("regrid_phases") else None),
                    "patch_to_cta": tune},
         "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
         "fp64_kernel": fp64, ("error_vs_oracle" if err and "against" in err else "error_vs_fp64"): err,

@@ -206,6 +206,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_cell_updates": [P, dp],
         "fc2d_b200_synchronize": [P],
         "fc2d_b200_last_update_stats": [P, dp, dp, ip, ip],
+        "fc2d_b200_last_regrid_stats": [P, dp],
         "fc2d_b200_set_timing": [P, I],
         "fc2d_b200_event_record": [P, I],
         "fc2d_b200_event_elapsed": [P, I, I, dp],
@@ -694,6 +695,13 @@ class Solver:
 
     def get_q_ptr(self, ptr: int) -> None:
         self._check("fc2d_b200_get_q", self.lib.fc2d_b200_get_q(self.h, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double))))
+
+    def last_regrid_stats(self) -> dict:
+        """Wall-clock milliseconds of the last regrid by phase (fc2d_b200_last_regrid_stats)."""
+        ms = np.zeros(8, np.float64)
+        self._check("fc2d_b200_last_regrid_stats", self.lib.fc2d_b200_last_regrid_stats(self.h, _dp(ms)))
+        keys = ("tag", "adapt", "forest", "repopulate", "tables", "upload", "ghost_update", "total")
+        return dict(zip(keys, ms.tolist()))
 
     def last_update_stats(self) -> dict:
         ms, by = ctypes.c_double(), ctypes.c_double()

@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <string>
 #include <vector>
+#include <chrono>
 #include "apps.hpp"
 #include "fc2d_b200.h"
 #include "host_forest.hpp"
@@ -24,7 +25,11 @@
 
 using namespace fcb;
 
-// Patch-to-CTA variants of the fused update compiled for one solver shape (first: default).
+static double wall_ms()
+{
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 // A specialised kernel (spec = its limiter) applies to the second-order method with
 // second-order transverse terms, that limiter on every one of 3 waves of 3 fields, no
 // capacity, no aux and no cubed sphere.
@@ -157,6 +162,7 @@ struct fc2d_b200_solver {
     Tables tables;                                 // host copy of the gather tables (buffers reused)
     TableWork table_work;
     std::vector<unsigned char> interp_written;     // interpolation-chain scratch, all zero between uses
+    double regrid_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // fc2d_b200_last_regrid_stats
     LevelRanges lr[33];
     unsigned long long* cfl_dev = nullptr;
     unsigned long long* cfl_host = nullptr;
@@ -317,7 +323,9 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
     Tables& T = s->tables;
     {
         std::string err;
+        const double t0 = wall_ms();
         if (!build_tables(f, s->o.mthbc, s->has_inflow, T, s->table_work, err)) return fail(FC2D_B200_EFOREST, err);
+        s->regrid_ms[4] = wall_ms() - t0;
     }
     if (s->part) {
         // partitioned: a new plan for this forest; the ghost-fill stages write only the
@@ -1544,6 +1552,8 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
 {
     DeviceScope dev_scope_(s);
     if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
+    const double t_start = wall_ms();
+    for (double& v : s->regrid_ms) v = 0.0;
     const Dims& d = s->d;
     const Forest& f = s->forest;
     const int np = f.np();
@@ -1582,6 +1592,8 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
             if (minmax) { mm[2 * i] = -r[np + i]; mm[2 * i + 1] = r[2 * (size_t)np + i]; }
         }
     }
+    const double t_mark = wall_ms();
+    s->regrid_ms[0] = t_mark - t_start;
     // clawpatch_tag4refinement / _tag4coarsening (fclaw2d_clawpatch.cpp:800-910): a negative
     // refine threshold always refines, a threshold <= 0 never coarsens
     const bool always_refine = s->o.refine_threshold < 0, never_coarsen = !(s->o.coarsen_threshold > 0);
@@ -1615,7 +1627,9 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     std::string err;
     std::vector<Leaf> L = adapt_leaves(f, mark, changed, err);
     if (changed_out) *changed_out = changed;
-    if (!changed) return 0;
+    const double t_adapt = wall_ms();
+    s->regrid_ms[1] = t_adapt - t_mark;
+    if (!changed) { s->regrid_ms[7] = t_adapt - t_start; return 0; }
     if (s->part) {
         // repopulation reads old patches any rank may own: every rank gets all of them
         int rc = halo_exchange(s, true);
@@ -1625,6 +1639,8 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     nf.g = f.g;
     nf.inst = f.inst;
     if (!nf.build(L, err)) return fail(FC2D_B200_EFOREST, err);
+    const double t_build = wall_ms();
+    s->regrid_ms[2] = t_build - t_adapt;
     // batch: an instance without an applied refinement or family coarsening
     // keeps its ghost cells, as it would alone (fclaw2d_regrid does no ghost
     // update then); a coarsening that balance refines again still counts as a change
@@ -1707,8 +1723,12 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     s->forest = std::move(nf);
     s->forest_gen++;
     invalidate_graph(s);
+    const double t_repop = wall_ms();
+    s->regrid_ms[3] = t_repop - t_build;
     rc = upload_desc_and_tables(s);
     if (rc) return rc;
+    const double t_upload = wall_ms();
+    s->regrid_ms[5] = t_upload - t_repop - s->regrid_ms[4];
     if (!keep.empty()) {
         const size_t nq_all = (size_t)s->forest.np() * d.nq();
         if (s->snap.cap < nq_all) {
@@ -1731,6 +1751,16 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     }
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s->st));
+    const double t_end = wall_ms();
+    s->regrid_ms[6] = t_end - t_upload;
+    s->regrid_ms[7] = t_end - t_start;
+    return 0;
+}
+
+extern "C" int fc2d_b200_last_regrid_stats(const fc2d_b200_solver_t* s, double* ms)
+{
+    if (!s || !ms) return fail(FC2D_B200_EINVAL, "null argument");
+    for (int k = 0; k < 8; k++) ms[k] = s->regrid_ms[k];
     return 0;
 }
 

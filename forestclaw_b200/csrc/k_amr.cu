@@ -222,9 +222,9 @@ struct RegOff {
 //             clawpack46_time_sync.f:254-498: the fine pair d, d+1 (d = 1 + n_off + 2 j)
 //             of coarse cell j, skipped when outside the fine face; q += deltac / area
 // Dynamic shared memory: 4 * meqn * max(mx, my) doubles and as many flag bytes.
-// 128 threads and at most 40 registers: 12 CTAs per SM, so a sync of up to ~1800
-// patches with corrections runs in one wave.
-__global__ void __launch_bounds__(128, 12)
+// 128 threads and at most 32 registers (no spills): 16 CTAs per SM, so a sync of up
+// to ~2300 patches with corrections runs in one wave.
+__global__ void __launch_bounds__(128, 16)
 k_sync(double* __restrict__ q, const double* __restrict__ regs, const PatchDesc* __restrict__ desc,
        const SyncOp* __restrict__ ops, const int* __restrict__ op_start, int mx, int my, int mbc, int meqn, int nreg)
 {

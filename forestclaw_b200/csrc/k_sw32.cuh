@@ -51,8 +51,7 @@ struct SW32Geom {
     static constexpr size_t OFF_GY = OFF_GX + (size_t)QB * 8;
     static constexpr size_t OFF_RED = OFF_GY + (size_t)QB * 8;       // 64 doubles
     static constexpr size_t OFF_BAR = OFF_RED + 64 * 8;              // 2 mbarriers + flag
-    static constexpr size_t OFF_QF = OFF_BAR + 32;                   // [MEQN][NXY] float
-    static constexpr size_t OFF_W = OFF_QF + (size_t)QB * 4;         // [7][NI] float
+    static constexpr size_t OFF_W = OFF_BAR + 32;                    // [7][NI] float
     static constexpr size_t OFF_T = OFF_W + 7 * (size_t)NI * 4;      // [12][NI] float
     static constexpr size_t BYTES = OFF_T + 12 * (size_t)NI * 4;
 };
@@ -114,7 +113,6 @@ __device__ __forceinline__ void sw32_patch(unsigned char* sm, const double* __re
     double* GX = reinterpret_cast<double*>(sm + G::OFF_GX);
     double* GY = reinterpret_cast<double*>(sm + G::OFF_GY);
     double* red = reinterpret_cast<double*>(sm + G::OFF_RED);
-    float* Qf = reinterpret_cast<float*>(sm + G::OFF_QF);
     float* W = reinterpret_cast<float*>(sm + G::OFF_W);
     float* Tt = reinterpret_cast<float*>(sm + G::OFF_T);
 
@@ -131,13 +129,12 @@ __device__ __forceinline__ void sw32_patch(unsigned char* sm, const double* __re
     auto fx = [&](int m, int c) -> double { return m == 0 ? Qs[NXY + c] : (m == 1 ? FXX[c] : FXY[c]); };
     auto fy = [&](int m, int c) -> double { return m == 0 ? Qs[2 * NXY + c] : (m == 1 ? FXY[c] : FYY[c]); };
 
-    // ---- cells: status, FP32 copy, FP64 fluxes, faces no sweep writes -----------
+    // ---- cells: status, FP64 fluxes, faces no sweep writes ----------------------
     unsigned bad = 0;
     for (int c = tid; c < NXY; c += NT) {
         const double h = Qs[c], hu = Qs[NXY + c], hv = Qs[2 * NXY + c];
         if (!isfinite(h) || !isfinite(hu) || !isfinite(hv)) bad |= STATUS_NONFINITE;
         if (h < 0.0) bad |= STATUS_DEPTH;
-        Qf[c] = (float)h; Qf[NXY + c] = (float)hu; Qf[2 * NXY + c] = (float)hv;
         const double inv = 1.0 / h;
         FXX[c] = hu * hu * inv + 0.5 * grav * h * h;
         FYY[c] = hv * hv * inv + 0.5 * grav * h * h;
@@ -186,7 +183,7 @@ __device__ __forceinline__ void sw32_patch(unsigned char* sm, const double* __re
     // normal solve of interface k (cells cL, cR) of sweep ixy; waves to W
     auto normal = [&](int ixy, int k, int cL, int cR, bool cfl_range, float d) {
         float qL[3], qR[3];
-        for (int m = 0; m < 3; m++) { qL[m] = Qf[m * NXY + cL]; qR[m] = Qf[m * NXY + cR]; }
+        for (int m = 0; m < 3; m++) { qL[m] = (float)Qs[m * NXY + cL]; qR[m] = (float)Qs[m * NXY + cR]; }
         RPShallowRoe::rpn2<float>(ixy, qL, qR, nullptr, nullptr, wave, s, am, ap, ex, gravw);
         const int mv = ixy == 1 ? 2 : 1;
         W[0 * NI + k] = wave[0][0]; W[1 * NI + k] = wave[0][1]; W[2 * NI + k] = wave[0][2];
@@ -255,6 +252,7 @@ __device__ __forceinline__ void sw32_patch(unsigned char* sm, const double* __re
 
     // =================== x-sweeps (clawpack46_step2.f:113-167) ===================
     const int kx = tid, jx = 1 + kx / (NX - 1), ix = 1 + kx % (NX - 1);
+    const int ky = tid, jy = 1 + ky / (NX - 2), iy = 1 + ky % (NX - 2);
     if (kx < G::NIX) normal(1, kx, jx * NX + ix - 1, jx * NX + ix, ix >= MBC && ix <= MX + MBC, dtdxw);
     __syncthreads();
     if (kx < G::NIX) {
@@ -263,10 +261,12 @@ __device__ __forceinline__ void sw32_patch(unsigned char* sm, const double* __re
         for (int m = 0; m < 3; m++) GX[m * NXY + jx * NX + ix] = 0.0 + fpv[m];
     }
     __syncthreads();
-    // transverse terms of the x-sweep into the y-faces: gp = gm = this (before the y-sweep)
-    for (int c = tid; c < NXY; c += NT) {
-        const int jc = c / NX, ic = c % NX;
-        if (ic < 1 || jc < 1) continue;
+    // transverse terms of the x-sweep into the y-faces: gp = gm = this (before the y-sweep).
+    // The faces read later are those of the y-sweep's interfaces (columns 1..NX-2, rows
+    // 1..NY-1), one per thread, numbered as the y-interfaces; faces in column 0 or row 0
+    // stay zero.
+    if (tid < G::NIY) {
+        const int jc = jy, ic = iy, c = jc * NX + ic;
         for (int m = 0; m < 3; m++) {
             double g = 0.0;
             if (jc - 1 >= 1 && jc - 1 <= NY - 2) {       // row jc-1, its gadd(:,2)
@@ -288,7 +288,6 @@ __device__ __forceinline__ void sw32_patch(unsigned char* sm, const double* __re
         }
     }
     // =================== y-sweeps (clawpack46_step2.f:182-236) ===================
-    const int ky = tid, jy = 1 + ky / (NX - 2), iy = 1 + ky % (NX - 2);
     if (ky < G::NIY) normal(2, ky, (jy - 1) * NX + iy, jy * NX + iy, jy >= MBC && jy <= MY + MBC, dtdyw);
     __syncthreads();
     if (ky < G::NIY) {
@@ -297,10 +296,10 @@ __device__ __forceinline__ void sw32_patch(unsigned char* sm, const double* __re
         for (int m = 0; m < 3; m++) GY[m * NXY + jy * NX + iy] = GY[m * NXY + jy * NX + iy] + fpv[m];
     }
     __syncthreads();
-    // transverse terms of the y-sweep into the x-faces
-    for (int c = tid; c < NXY; c += NT) {
-        const int jc = c / NX, ic = c % NX;
-        if (jc < 1 || jc > NY - 2) continue;
+    // transverse terms of the y-sweep into the x-faces: the faces of the x-sweep's interfaces
+    // (columns 1..NX-1, rows 1..NY-2), one per thread; faces in column 0 get none
+    if (tid < G::NIX) {
+        const int jc = jx, ic = ix, c = jc * NX + ic;
         const bool wall_edge = (ic == MBC && (wallf & 1)) || (ic == MX + MBC && (wallf & 2));
         for (int m = 0; m < 3; m++) {
             if (m == 0 && wall_edge) continue;
@@ -366,11 +365,22 @@ __device__ __forceinline__ void sw32_patch(unsigned char* sm, const double* __re
     }
 
     // ---- q update over i,j = 1-mbc..mx+mbc-1 (clawpack46_step2_wrap.f:107-125) ----
+    // (fm_x / gm_y of the cell's right and top faces written out: one flux plane per field)
     for (int k = tid; k < G::QB; k += NT) {
-        const int m = k / NXY, c = k % NXY;
-        const int jc = c / NX, ic = c % NX;
-        if (ic <= NX - 2 && jc <= NY - 2)
-            qg[k] = Qs[k] - dtdx * (fm_x(m, c + 1) - GX[k]) - dtdy * (gm_y(m, c + NX) - GY[k]);
+        const int m = k / NXY, c = k - m * NXY;
+        const int jc = c / NX, ic = c - jc * NX;
+        if (ic > NX - 2 || jc > NY - 2) continue;
+        const double* fxp = m == 0 ? Qs + NXY : (m == 1 ? FXX : FXY);
+        const double* fyp = m == 0 ? Qs + 2 * NXY : (m == 1 ? FXY : FYY);
+        const double* gx = GX + m * NXY;
+        const double* gy = GY + m * NXY;
+        double fmv = gx[c + 1];
+        if (jc >= 1 && ic + 1 <= NX - 2)
+            fmv = (m == 0 && (wallf & 2) && ic + 1 == MX + MBC) ? 0.0 - fxp[c] : (fxp[c + 1] - fxp[c]) + fmv;
+        double gmv = gy[c + NX];
+        if (ic >= 1 && ic <= NX - 2 && jc + 1 <= NY - 2)
+            gmv = (m == 0 && (wallf & 8) && jc + 1 == MY + MBC) ? 0.0 - fyp[c] : (fyp[c + NX] - fyp[c]) + gmv;
+        qg[k] = Qs[k] - dtdx * (fmv - gx[c]) - dtdy * (gmv - gy[c]);
     }
 
     // ---- CFL maximum: warp shuffles, then one atomic per CTA -----------------

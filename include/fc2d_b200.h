@@ -370,6 +370,13 @@ int fc2d_b200_synchronize(fc2d_b200_solver_t* s);
  * cells, q read + write + aux read). */
 int fc2d_b200_last_update_stats(const fc2d_b200_solver_t* s, double* update_ms, double* update_bytes,
                                 int* update_launches, int* total_launches);
+/* Wall-clock breakdown of the most recent fc2d_b200_regrid, milliseconds
+ * (ms[8]): 0 tagging on the device and the flags back on the host, 1 coarsen /
+ * refine marks, smoothing and the 2:1-balanced leaves, 2 the new forest (neighbour
+ * search), 3 repopulation (ops, aux, device copies), 4 gather-table build on the
+ * host, 5 descriptor and table upload (partition plan included), 6 the ghost
+ * update on the new forest, 7 the whole call. */
+int fc2d_b200_last_regrid_stats(const fc2d_b200_solver_t* s, double* ms);
 /* Replay each fclaw2d_advance_all_levels as a CUDA graph captured once per
  * forest (on by default; disabled while update timing is on). */
 int fc2d_b200_set_graphs(fc2d_b200_solver_t* s, int enable);
