@@ -214,8 +214,8 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
         return mcapa > 0 ? (TW)(dtdy / As[(mcapa - 1) * NXY + jc * NX + ic]) : (TW)dtdy;
     };
     auto qload = [&](int m, int c) -> TW {
-        if constexpr (F32) return Qf[m * NXY + c];
-        else return (TW)Qs[m * NXY + c];
+        if constexpr (F32) { return Qf[m * NXY + c]; }
+        else { return (TW)Qs[m * NXY + c]; }
     };
     const TW gravw = (TW)sp.grav, drytolw = (TW)sp.dry_tolerance;
 
@@ -234,8 +234,8 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
             else { ic = MBC + j; jc = MY + MBC - 1 + k; }
             double qv[MEQN >= 3 ? MEQN : 3], fl[MEQN >= 3 ? MEQN : 3];
             for (int m = 0; m < MEQN; m++) qv[m] = Qs[m * NXY + jc * NX + ic];
-            if constexpr (RP::EXACT64) RP::cons_flux(face / 2, qv, sp.gamma, fl);
-            else rpn2_cons_sw<double>(face / 2, qv, sp.grav, fl);
+            if constexpr (RP::EXACT64) { RP::cons_flux(face / 2, qv, sp.gamma, fl); }
+            else { rpn2_cons_sw<double>(face / 2, qv, sp.grav, fl); }
             const int n = (face < 2) ? MY : MX;
             const double el = (face < 2) ? dy : dx;
             const int base = (face == 0) ? G::R_EF0 : (face == 1) ? G::R_EF1 : (face == 2) ? G::R_EF2 : G::R_EF3;
@@ -441,8 +441,11 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
                 Tt[(0 * MEQN + m) * NI + k] = TW(0.5) * dlo * bm[m];
                 Tt[(1 * MEQN + m) * NI + k] = TW(0.5) * dlo * bp[m];
             }
-            if constexpr (!BOTH)
+            // (every if-constexpr body here is braced: inside a lambda of a template, nvcc
+            // 12.9 also discards the statement that follows an unbraced discarded `for`)
+            if constexpr (!BOTH) {
                 for (int a = 0; a < MAUX; a++) { a1[a] = (TW)As[a * NXY + a1c[1]]; a2[a] = (TW)As[a * NXY + a2c[1]]; a3[a] = (TW)As[a * NXY + a3c[1]]; }
+            }
             RP::template rpt2<TW>(ixy, 2, qL, qR, a1, a2, a3, st.ex, ap, bm, bp, gravw, drytolw);
             for (int m = 0; m < MEQN; m++) {
                 Tt[(2 * MEQN + m) * NI + k] = TW(0.5) * dhi * bm[m];
@@ -516,8 +519,8 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
             MlpFrag h1, h2;
             mlp_warp_hidden<true>(W, x, h1, h2);
             const float y = mlp_warp_output(W, h2);
-            if constexpr (F32) return use ? pbase * (double)__expf(y) : 0.0;
-            else return use ? pbase * fcb_exp((double)y) : 0.0;
+            if constexpr (F32) { return use ? pbase * (double)__expf(y) : 0.0; }
+            else { return use ? pbase * fcb_exp((double)y) : 0.0; }
         } else {
             (void)ixy; (void)k;
             return 0.0;
@@ -631,7 +634,7 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
     State st;
     if (bcc) { fix_corners(0); __syncthreads(); }
     cell_fluxes(1);
-    if constexpr (RP::EXACT64 && F32) __syncthreads();   // the exact solver reads the cell fluxes
+    if constexpr (RP::EXACT64 && F32) { __syncthreads(); }   // the exact solver reads the cell fluxes
     {
         const double seed = (RP::EXACT64 && sp.mlp) ? mlp_seed(1, tid < G::NIX ? tid : -1) : 0.0;
         if (REG) { if (tid < G::NIX) x1(tid, st, seed); }
@@ -645,7 +648,7 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
     // X3 and the y-sweep normal solves touch disjoint data: one phase
     for (int c = tid; c < NXY; c += NT) x3(c);
     cell_fluxes(2);
-    if constexpr (RP::EXACT64 && F32) __syncthreads();
+    if constexpr (RP::EXACT64 && F32) { __syncthreads(); }
     // =================== y-sweeps (clawpack46_step2.f:182-236) ===================
     {
         const double seed = (RP::EXACT64 && sp.mlp) ? mlp_seed(2, tid < G::NIY ? tid : -1) : 0.0;
