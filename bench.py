@@ -578,15 +578,25 @@ def run_ours(args, wl, rank, world, local_rank):
     torch.cuda.synchronize()
     te0 = time.perf_counter()
     e2e_cells, e2e_h2d, e2e_d2h, e2e_regrids = 0.0, 0.0, 0.0, 0
+    ph = {"set_q": 0.0, "advance": 0.0, "advance_after_regrid": 0.0, "get_q": 0.0, "regrid": 0.0}
+    after_regrid = False
     for k in range(e2e_steps):
         c0 = g.cell_updates
         nq = g.num_patches * per_patch
         if nq > cap:                       # the forest outgrew the pinned buffer
             cap = 2 * nq
             hq = torch.empty(cap, dtype=torch.float64, pin_memory=True)
+        p0 = time.perf_counter()
         g.set_q_ptr(hq.data_ptr())
+        p1 = time.perf_counter()
         cfl = g.advance(t, dt)
+        p2 = time.perf_counter()
         g.get_q_ptr(hq.data_ptr())
+        p3 = time.perf_counter()
+        ph["set_q"] += p1 - p0
+        ph["advance_after_regrid" if after_regrid else "advance"] += p2 - p1
+        ph["get_q"] += p3 - p2
+        after_regrid = False
         e2e_cells += g.cell_updates - c0
         e2e_h2d += nq * 8
         e2e_d2h += nq * 8
@@ -594,8 +604,10 @@ def run_ours(args, wl, rank, world, local_rank):
         if wl.get("adapt_dt", wl["time_sync"]):
             dt *= 0.9 / cfl
         if wl["regrid_interval"] and (k + 1) % wl["regrid_interval"] == 0:
+            p4 = time.perf_counter()
             g.regrid()
             e2e_regrids += 1
+            after_regrid = True
             # the new forest's data back to the host copy (counted with the step's d2h bytes)
             nq = g.num_patches * per_patch
             if nq > cap:
@@ -603,12 +615,14 @@ def run_ours(args, wl, rank, world, local_rank):
                 hq = torch.empty(cap, dtype=torch.float64, pin_memory=True)
             g.get_q_ptr(hq.data_ptr())
             e2e_d2h += nq * 8
+            ph["regrid"] += time.perf_counter() - p4
     e2e_s = time.perf_counter() - te0
     e2e_s = ranks.max_over_ranks(e2e_s, "cuda")
     e2e_cells = ranks.sum_over_ranks(e2e_cells, "cuda")
     e2e = {"value": e2e_cells / e2e_s, "unit": "cell-updates/s",
            "h2d_bytes_per_step": int(e2e_h2d / e2e_steps), "d2h_bytes_per_step": int(e2e_d2h / e2e_steps),
            "steps": e2e_steps, "regrids": e2e_regrids,
+           "wall_ms_per_step": {k: round(v * 1e3 / e2e_steps, 4) for k, v in ph.items()},
            "protocol": "per coarse step: set_q from pinned host memory, advance, get_q to pinned host memory; "
                        "the workload's regrid (host tree edit, device repopulation, graph recapture) inside "
                        "the wall-clock region"}

@@ -216,13 +216,20 @@ struct fc2d_b200_solver {
     bool use_graphs = true;
     bool programmatic = true;                      // advance kernels with programmatic dependent launch
     cudaGraphExec_t graph_exec = nullptr;
+    bool graph_stale = true;                       // the launches changed: update (or rebuild) before replay
     int graph_nupd = -1;
+    int graph_builds = 0, graph_updates = 0;       // instantiations / in-place updates so far
 };
 
-static void invalidate_graph(fc2d_b200_solver* s)
+// The launches of an advance changed (new forest, tables, variant, launch mode): the
+// next advance captures them again and updates the executable graph in place when
+// the new capture has the same shape, else instantiates a new one.
+static void invalidate_graph(fc2d_b200_solver* s) { s->graph_stale = true; }
+static void release_graph(fc2d_b200_solver* s)
 {
     if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
     s->graph_exec = nullptr;
+    s->graph_stale = true;
     s->graph_nupd = -1;
 }
 
@@ -975,7 +982,7 @@ extern "C" int fc2d_b200_destroy(fc2d_b200_solver_t* s)
     free_spare(s);
     cudaFree(s->cfl_dev); cudaFreeHost(s->cfl_host); cudaFree(s->inst_dt_dev); cudaFreeHost(s->inst_dt_host);
     cudaFree(s->status_dev); cudaFreeHost(s->status_host);
-    invalidate_graph(s);
+    release_graph(s);
     cudaFree(s->params_dev); cudaFreeHost(s->params_host);
     if (s->mass_dev) cudaFree(s->mass_dev);
     if (s->qsave) cudaFree(s->qsave);
@@ -1492,17 +1499,33 @@ static int advance_launch(fc2d_b200_solver_t* s, double t, double dt)
     // pass 2: the launches, captured once per forest into a CUDA graph and replayed
     s->emit = true; s->fill = false;
     if (s->use_graphs && !s->timing) {
-        if (!s->graph_exec || s->graph_nupd != nupd) {
-            invalidate_graph(s);
+        if (s->graph_stale || !s->graph_exec || s->graph_nupd != nupd) {
             cudaGraph_t g = nullptr;
             CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
             rc = traverse_advance(s, t, dt);
             cudaError_t ec = cudaStreamEndCapture(s->st, &g);
             if (rc) { if (g) cudaGraphDestroy(g); s->fill = true; return rc; }
             if (ec != cudaSuccess) { s->fill = true; return fail(FC2D_B200_ECUDA, std::string("graph capture: ") + cudaGetErrorString(ec)); }
-            ec = cudaGraphInstantiate(&s->graph_exec, g, 0);
+            bool updated = false;
+            if (s->graph_exec) {
+                // same launches with new grids and arguments (a regrid): new parameters in place
+                cudaGraphExecUpdateResultInfo info{};
+                updated = cudaGraphExecUpdate(s->graph_exec, g, &info) == cudaSuccess;
+                if (!updated) { (void)cudaGetLastError(); release_graph(s); }
+            }
+            if (!updated) {
+                ec = cudaGraphInstantiate(&s->graph_exec, g, 0);
+                if (ec != cudaSuccess) {
+                    cudaGraphDestroy(g);
+                    s->graph_exec = nullptr; s->fill = true;
+                    return fail(FC2D_B200_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(ec));
+                }
+                s->graph_builds++;
+            } else {
+                s->graph_updates++;
+            }
             cudaGraphDestroy(g);
-            if (ec != cudaSuccess) { s->graph_exec = nullptr; s->fill = true; return fail(FC2D_B200_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(ec)); }
+            s->graph_stale = false;
             s->graph_nupd = nupd;
         }
         CK(cudaGraphLaunch(s->graph_exec, s->st));

@@ -185,21 +185,28 @@ int Forest::lookup(int i, int l, int x, int y) const
 
 bool Forest::build(const std::vector<Leaf>& leaves, std::string& err)
 {
-    p.clear();
-    p.reserve(leaves.size());
-    for (const Leaf& lf : leaves) {
-        PatchInfo q{};
-        q.level = lf.level; q.gx = lf.gx; q.gy = lf.gy; q.inst = lf.inst;
-        if (q.inst < 0 || q.inst >= ninst()) { err = "leaf of an unknown instance"; return false; }
-        geometry(q);
-        p.push_back(q);
+    std::vector<PatchInfo> q(leaves.size());
+    for (size_t i = 0; i < leaves.size(); i++) {
+        const Leaf& lf = leaves[i];
+        PatchInfo& P = q[i];
+        P = PatchInfo{};
+        P.level = lf.level; P.gx = lf.gx; P.gy = lf.gy; P.inst = lf.inst;
+        if (P.inst < 0 || P.inst >= ninst()) { err = "leaf of an unknown instance"; return false; }
+        geometry(P);
     }
-    std::sort(p.begin(), p.end(), [](const PatchInfo& a, const PatchInfo& b) {
+    // slot order: level, instance, block, Morton (sorted as indices: the records are large)
+    std::vector<int> ord(q.size());
+    for (size_t i = 0; i < ord.size(); i++) ord[i] = (int)i;
+    std::sort(ord.begin(), ord.end(), [&](int ia, int ib) {
+        const PatchInfo& a = q[ia];
+        const PatchInfo& b = q[ib];
         if (a.level != b.level) return a.level < b.level;
         if (a.inst != b.inst) return a.inst < b.inst;
         if (a.block != b.block) return a.block < b.block;
         return a.morton < b.morton;
     });
+    p.resize(q.size());
+    for (size_t i = 0; i < ord.size(); i++) p[i] = q[ord[i]];
     index_.reset(p.size());
     for (int i = 0; i < np(); i++) index_.put(key(p[i].inst, p[i].level, p[i].gx, p[i].gy), i);
     for (int l = 0; l < 34; l++) lev_off[l] = 0;
@@ -214,7 +221,9 @@ bool Forest::build(const std::vector<Leaf>& leaves, std::string& err)
         lev_off[33] = k;
     }
     static const int FDX[4] = {-1, 1, 0, 0}, FDY[4] = {0, 0, -1, 1};
-    for (int ip = 0; ip < np(); ip++) {
+    // neighbours of every patch (independent per patch: chunks on worker threads)
+    std::atomic<int> unbalanced{0};
+    auto neighbours = [&](int ip) {
         PatchInfo& P = p[ip];
         const int l = P.level, in = P.inst;
         P.has_fine_nbr = 0; P.on_cf = 0;
@@ -236,7 +245,7 @@ bool Forest::build(const std::vector<Leaf>& leaves, std::string& err)
                 step(in, l + 1, 2 * P.gx + ex + kx, 2 * P.gy + ey + ky, FDX[f], FDY[f], c1x, c1y);
             }
             const int a = lookup(in, l + 1, c0x, c0y), b = lookup(in, l + 1, c1x, c1y);
-            if (a < 0 || b < 0) { err = "forest is not 2:1 face balanced"; return false; }
+            if (a < 0 || b < 0) { unbalanced = 1; return; }
             P.face_type[f] = NB_HALF; P.face_nbr[f][0] = a; P.face_nbr[f][1] = b;
             P.has_fine_nbr = 1; P.on_cf = 1;
         }
@@ -269,7 +278,22 @@ bool Forest::build(const std::vector<Leaf>& leaves, std::string& err)
                 P.has_corner[c] = 1; P.corner_type[c] = NB_DOUBLE; P.corner_nbr[c] = k; P.on_cf = 1;
             }
         }
+    };
+    const int n = np();
+    int nt = (int)std::thread::hardware_concurrency();
+    nt = std::max(1, std::min(nt, std::min(16, n / 256)));
+    auto chunk = [&](int t) {
+        const int a = (int)((long)n * t / nt), b = (int)((long)n * (t + 1) / nt);
+        for (int ip = a; ip < b; ip++) neighbours(ip);
+    };
+    if (nt == 1) chunk(0);
+    else {
+        std::vector<std::thread> th;
+        for (int t = 1; t < nt; t++) th.emplace_back(chunk, t);
+        chunk(0);
+        for (auto& x : th) x.join();
     }
+    if (unbalanced) { err = "forest is not 2:1 face balanced"; return false; }
     return true;
 }
 
