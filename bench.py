@@ -2,7 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload dam|dam-uniform|swirl|shockbubble|batch] [--precision fp32wave|fp64]
-                    [--pstar pvrs|mlp] [--no-fp64-compare] [--no-autotune]
+                    [--pstar pvrs|mlp] [--no-fp64-compare] [--no-autotune] [--variant V]
 
 Default workload (the configuration the metric is quoted on): 2D shallow water,
 radial dam break on [-1,1]^2, adaptive quadtree levels 3-7, 16x16 patches, mbc=2,
@@ -461,7 +461,10 @@ def _roofline_pass(solvers, t_dt, flush, steps):
     return ms, by, nl
 
 
-def _tune(g, enabled):
+def _tune(g, enabled, variant=None):
+    if variant is not None:                       # a fixed patch-to-CTA variant, no tuning
+        g.set_variant(variant)
+        return {"variant": g.variant, "autotuned": False, **g.variants()[g.variant]}
     if not enabled:
         return {"variant": g.variant, "autotuned": False, **g.variants()[g.variant]}
     best, ms = g.autotune(reps=3)
@@ -493,7 +496,7 @@ def _fp64_kernel_arm(args, wl, prob, local_rank, flush):
     _maybe_partition(g, args, local_rank)
     g.initialize()
     t, dt, _ = _spinup(g, wl, 0.0, _initial_dt(wl, prob), wl["spinup"])
-    tune = _tune(g, not args.no_autotune)
+    tune = _tune(g, not args.no_autotune)         # --variant names a variant of the main arm
     t, dt, _ = _spinup(g, dict(wl, regrid_interval=0), t, dt, args.warmup)
     g.synchronize()
     _bracket()
@@ -549,7 +552,7 @@ def run_ours(args, wl, rank, world, local_rank):
     # spin-up with regrid so the timed forest is representative (not timed),
     # then the autotuner picks the patch-to-CTA variant on that forest
     t, dt, regrid_ms = _spinup(g, wl, 0.0, _initial_dt(wl, prob), wl["spinup"])
-    tune = _tune(g, not args.no_autotune)
+    tune = _tune(g, not args.no_autotune, args.variant)
     t, dt, _ = _spinup(g, dict(wl, regrid_interval=0), t, dt, args.warmup)
     g.synchronize()
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -938,6 +941,8 @@ def main():
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="skip the timed run of the plain FP64 kernel on the same workload")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default patch-to-CTA variant")
+    ap.add_argument("--variant", type=int, default=None,
+                    help="use this patch-to-CTA variant (index into Solver.variants()), no autotuning")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--pstar", default="pvrs", choices=["pvrs", "mlp"],
                     help="Euler: Newton start of the exact solver (mlp: trained on the FP64 run first)")

@@ -60,6 +60,10 @@ struct StepParams {
     const void* mlp;        // Euler: p*-seed network blob (null: PVRS start)
     const double* inst_dt;  // batch: coarse time step of each instance, dt = this[inst] * (level factor in dt)
     unsigned int* status;   // device status word: STATUS_* bits or'ed in by the kernels (or null)
+    // Time-sync registers reset since this level's last update, by face type (bit t for
+    // face type t: 0 boundary, 1 half, 2 same, 3 double): the update's first
+    // accumulation into such a face's registers starts from zero instead of reading them.
+    int reg_reset;
 };
 
 // Kernel-side failures reported through the status word (read by the host after a step).

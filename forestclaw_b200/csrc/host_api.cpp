@@ -163,6 +163,11 @@ struct fc2d_b200_solver {
     TableWork table_work;
     std::vector<unsigned char> interp_written;     // interpolation-chain scratch, all zero between uses
     double regrid_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // fc2d_b200_last_regrid_stats
+    // Time-sync register resets not yet applied, per level: bit t for face type t (see
+    // StepParams::reg_reset).  Inside an advance a time sync's resets are left to the
+    // next update of each level, which starts those faces' accumulation from zero; the
+    // sync at the end of an advance applies them.
+    int reg_pending[34] = {0};
     LevelRanges lr[33];
     unsigned long long* cfl_dev = nullptr;
     unsigned long long* cfl_host = nullptr;
@@ -471,6 +476,7 @@ static StepParams make_params(const fc2d_b200_solver* s, int level, double t, do
     sp.mlp = s->use_mlp ? s->mlp_blob : nullptr;
     sp.inst_dt = s->insts.empty() ? nullptr : s->inst_dt_dev;
     sp.status = s->status_dev;
+    sp.reg_reset = 0;
     if (s->o.app == FC2D_B200_APP_SWIRL && s->o.tperiod != 0.0) {
         const double pi = 4.0 * std::atan(1.0), pi2 = 2.0 * pi;
         sp.vt = std::cos(pi2 * (t + dt / 2.0) / s->o.tperiod);
@@ -543,6 +549,8 @@ static int update_level(fc2d_b200_solver* s, int level, double t, double dt)
     if (s->fill) {
         StepParams& sp = s->params_host[slot];
         sp = make_params(s, level, t, dt);
+        sp.reg_reset = s->reg_pending[level];      // resets a time sync left to this update
+        s->reg_pending[level] = 0;
         s->cell_updates += (double)np * s->d.mx * s->d.my;
         if (s->emit)
             CK(cudaMemcpyAsync((void*)(s->params_dev + slot), &sp, sizeof(StepParams), cudaMemcpyHostToDevice, s->st));
@@ -765,7 +773,20 @@ static void ghost_update(fc2d_b200_solver* s, int minlevel, int maxlevel, int ti
 // registers no earlier reset of the sync touches (f2c reads half-size faces of
 // the coarse level and double-size faces of the fine level), so the merged
 // order gives the same values.
-static void time_sync(fc2d_b200_solver* s, int minlevel, int maxlevel)
+// Reset rule of fclaw2d_time_sync(minlevel a, maxlevel maxl) for a patch of level L, by
+// face type (k_reset_sync): same-size and physical faces always, faces with finer
+// neighbours below maxl, faces with coarser neighbours when the coarser level is synced.
+static int reset_mask(int L, int a, int maxl)
+{
+    int m = (1 << 0) | (1 << 2);
+    if (L < maxl) m |= 1 << 1;
+    if (L - 1 >= a && L - 1 < maxl) m |= 1 << 3;
+    return m;
+}
+
+// defer: leave the register resets to the next update of each synced level (inside an
+// advance: no register is read between a sync and that update but by that update)
+static void time_sync(fc2d_b200_solver* s, int minlevel, int maxlevel, bool defer = false)
 {
     (void)maxlevel;
     const int maxl = std::min(s->o.maxlevel, 32);
@@ -779,6 +800,13 @@ static void time_sync(fc2d_b200_solver* s, int minlevel, int maxlevel)
             if (s->emit) launch_sync(s->d, s->q, s->regs, s->desc, s->t_sync.p, s->t_sync_start.p + g0, g1 - g0, s->st);
         }
     }
+    if (defer) {
+        if (s->fill)
+            for (int L = a; L <= maxl; L++) s->reg_pending[L] |= reset_mask(L, a, maxl);
+        return;
+    }
+    // applied now: every reset of this sync, which covers any left pending since
+    for (int L = a; L <= maxl; L++) s->reg_pending[L] &= ~reset_mask(L, a, maxl);
     const int p0 = s->forest.lev_off[a], p1 = s->forest.lev_off[maxl + 1];
     if (p1 > p0) {
         (void)flush_pending(s);
@@ -1466,10 +1494,10 @@ static int traverse_advance(fc2d_b200_solver* s, double t, double dt)
                 int ti = maxlevel - 1;
                 while (ts[maxlevel].last_step % ts[ti].step_inc == 0) ti--;
                 ghost_update(s, ti + 1, maxlevel, 1);
-                if (o.time_sync) time_sync(s, ti + 1, maxlevel);
+                if (o.time_sync) time_sync(s, ti + 1, maxlevel, true);
             } else {
                 ghost_update(s, minlevel, maxlevel, 0);
-                if (o.time_sync) time_sync(s, minlevel, maxlevel);
+                if (o.time_sync) time_sync(s, minlevel, maxlevel, true);
             }
         }
     }

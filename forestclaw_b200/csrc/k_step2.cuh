@@ -239,9 +239,10 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
             const int n = (face < 2) ? MY : MX;
             const double el = (face < 2) ? dy : dx;
             const int base = (face == 0) ? G::R_EF0 : (face == 1) ? G::R_EF1 : (face == 2) ? G::R_EF2 : G::R_EF3;
+            const bool zero = (sp.reg_reset >> ((pd.face_type >> (2 * face)) & 3)) & 1;
             for (int m = 0; m < MEQN; m++) {
                 double* r = &rg[base + j + m * n + k * n * MEQN];
-                *r = *r + dt * el * fl[m];
+                *r = (zero ? 0.0 : *r) + dt * el * fl[m];
             }
         }
     }
@@ -665,26 +666,29 @@ step2_patch(double* __restrict__ q, double* __restrict__ qlast, const double* __
     // ---- time-sync wave accumulation (clawpack46_time_sync.f:163-226), FP64 ----
     if (sp.accumulate_waves) {
         const double dtdyv = dt * dy, dtdxv = dt * dx;
+        // registers of a face reset since the last update start from zero
+        auto z = [&](int face) { return ((sp.reg_reset >> ((pd.face_type >> (2 * face)) & 3)) & 1) != 0; };
+        const bool z0 = z(0), z1 = z(1), z2 = z(2), z3 = z(3);
         for (int it = tid; it < (MY + MX) * MEQN; it += NT) {
             if (it < MY * MEQN) {
                 const int j = it % MY, m = it / MY;
                 const int jc = MBC + j;
                 const int cl = m * NXY + jc * NX + MBC, cr = m * NXY + jc * NX + MX + MBC;
                 double* r;
-                r = &rg[G::R_FP0 + j + m * MY]; *r = *r - dtdyv * FPs[cl];
-                r = &rg[G::R_FM0 + j + m * MY]; *r = *r + dtdyv * FMs[cl];
-                r = &rg[G::R_FP1 + j + m * MY]; *r = *r - dtdyv * FPs[cr];
-                r = &rg[G::R_FM1 + j + m * MY]; *r = *r + dtdyv * FMs[cr];
+                r = &rg[G::R_FP0 + j + m * MY]; *r = (z0 ? 0.0 : *r) - dtdyv * FPs[cl];
+                r = &rg[G::R_FM0 + j + m * MY]; *r = (z0 ? 0.0 : *r) + dtdyv * FMs[cl];
+                r = &rg[G::R_FP1 + j + m * MY]; *r = (z1 ? 0.0 : *r) - dtdyv * FPs[cr];
+                r = &rg[G::R_FM1 + j + m * MY]; *r = (z1 ? 0.0 : *r) + dtdyv * FMs[cr];
             } else {
                 const int i2 = it - MY * MEQN;
                 const int i = i2 % MX, m = i2 / MX;
                 const int ic = MBC + i;
                 const int cb = m * NXY + MBC * NX + ic, ct = m * NXY + (MY + MBC) * NX + ic;
                 double* r;
-                r = &rg[G::R_GP0 + i + m * MX]; *r = *r - dtdxv * GPs[cb];
-                r = &rg[G::R_GM0 + i + m * MX]; *r = *r + dtdxv * GMs[cb];
-                r = &rg[G::R_GP1 + i + m * MX]; *r = *r - dtdxv * GPs[ct];
-                r = &rg[G::R_GM1 + i + m * MX]; *r = *r + dtdxv * GMs[ct];
+                r = &rg[G::R_GP0 + i + m * MX]; *r = (z2 ? 0.0 : *r) - dtdxv * GPs[cb];
+                r = &rg[G::R_GM0 + i + m * MX]; *r = (z2 ? 0.0 : *r) + dtdxv * GMs[cb];
+                r = &rg[G::R_GP1 + i + m * MX]; *r = (z3 ? 0.0 : *r) - dtdxv * GPs[ct];
+                r = &rg[G::R_GM1 + i + m * MX]; *r = (z3 ? 0.0 : *r) + dtdxv * GMs[ct];
             }
         }
     }

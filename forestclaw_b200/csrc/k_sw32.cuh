@@ -167,9 +167,10 @@ __device__ __forceinline__ void sw32_patch(unsigned char* sm, const double* __re
             const int n = (face < 2) ? MY : MX;
             const double el = (face < 2) ? dy : dx;
             const int base = (face == 0) ? R::R_EF0 : (face == 1) ? R::R_EF1 : (face == 2) ? R::R_EF2 : R::R_EF3;
+            const bool zero = (sp.reg_reset >> ((pd.face_type >> (2 * face)) & 3)) & 1;
             for (int m = 0; m < 3; m++) {
                 double* r = &rg[base + j + m * n + k * n * 3];
-                *r = *r + dt * el * fl[m];
+                *r = (zero ? 0.0 : *r) + dt * el * fl[m];
             }
         }
     }
@@ -340,26 +341,29 @@ __device__ __forceinline__ void sw32_patch(unsigned char* sm, const double* __re
     // ---- time-sync wave accumulation (clawpack46_time_sync.f:163-226), FP64 ----
     if (sp.accumulate_waves) {
         const double dtdyv = dt * dy, dtdxv = dt * dx;
+        // registers of a face reset since the last update start from zero
+        auto z = [&](int face) { return ((sp.reg_reset >> ((pd.face_type >> (2 * face)) & 3)) & 1) != 0; };
+        const bool z0 = z(0), z1 = z(1), z2 = z(2), z3 = z(3);
         for (int it = tid; it < (MY + MX) * 3; it += NT) {
             if (it < MY * 3) {
                 const int j = it % MY, m = it / MY;
                 const int jc = MBC + j;
                 const int cl = jc * NX + MBC, cr = jc * NX + MX + MBC;
                 double* r;
-                r = &rg[R::R_FP0 + j + m * MY]; *r = *r - dtdyv * GX[m * NXY + cl];
-                r = &rg[R::R_FM0 + j + m * MY]; *r = *r + dtdyv * fm_x(m, cl);
-                r = &rg[R::R_FP1 + j + m * MY]; *r = *r - dtdyv * GX[m * NXY + cr];
-                r = &rg[R::R_FM1 + j + m * MY]; *r = *r + dtdyv * fm_x(m, cr);
+                r = &rg[R::R_FP0 + j + m * MY]; *r = (z0 ? 0.0 : *r) - dtdyv * GX[m * NXY + cl];
+                r = &rg[R::R_FM0 + j + m * MY]; *r = (z0 ? 0.0 : *r) + dtdyv * fm_x(m, cl);
+                r = &rg[R::R_FP1 + j + m * MY]; *r = (z1 ? 0.0 : *r) - dtdyv * GX[m * NXY + cr];
+                r = &rg[R::R_FM1 + j + m * MY]; *r = (z1 ? 0.0 : *r) + dtdyv * fm_x(m, cr);
             } else {
                 const int i2 = it - MY * 3;
                 const int i = i2 % MX, m = i2 / MX;
                 const int ic = MBC + i;
                 const int cb = MBC * NX + ic, ct = (MY + MBC) * NX + ic;
                 double* r;
-                r = &rg[R::R_GP0 + i + m * MX]; *r = *r - dtdxv * GY[m * NXY + cb];
-                r = &rg[R::R_GM0 + i + m * MX]; *r = *r + dtdxv * gm_y(m, cb);
-                r = &rg[R::R_GP1 + i + m * MX]; *r = *r - dtdxv * GY[m * NXY + ct];
-                r = &rg[R::R_GM1 + i + m * MX]; *r = *r + dtdxv * gm_y(m, ct);
+                r = &rg[R::R_GP0 + i + m * MX]; *r = (z2 ? 0.0 : *r) - dtdxv * GY[m * NXY + cb];
+                r = &rg[R::R_GM0 + i + m * MX]; *r = (z2 ? 0.0 : *r) + dtdxv * gm_y(m, cb);
+                r = &rg[R::R_GP1 + i + m * MX]; *r = (z3 ? 0.0 : *r) - dtdxv * GY[m * NXY + ct];
+                r = &rg[R::R_GM1 + i + m * MX]; *r = (z3 ? 0.0 : *r) + dtdxv * gm_y(m, ct);
             }
         }
     }
