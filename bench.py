@@ -553,7 +553,8 @@ def run_ours(args, wl, rank, world, local_rank):
     # then the autotuner picks the patch-to-CTA variant on that forest
     t, dt, regrid_ms = _spinup(g, wl, 0.0, _initial_dt(wl, prob), wl["spinup"])
     tune = _tune(g, not args.no_autotune, args.variant)
-    t, dt, _ = _spinup(g, dict(wl, regrid_interval=0), t, dt, args.warmup)
+    t_start, dt_start = _spinup(g, dict(wl, regrid_interval=0), t, dt, args.warmup)[:2]
+    t, dt = t_start, dt_start
     g.synchronize()
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     g.set_timing(False)
@@ -572,12 +573,33 @@ def run_ours(args, wl, rank, world, local_rank):
     t += nroof * dt
     from forestclaw_b200 import ranks
     total_ms, cells_all, value = ranks.aggregate(float(np.sum(step_ms)), cells, "cuda")
+    newton = None
+    if wl["name"].startswith("euler"):
+        h = g.newton_histogram()
+        newton = {"mean_iterations": float((np.arange(32) * h).sum() / max(h.sum(), 1)),
+                  "histogram": [int(v) for v in h[:12]], "pstar_start": args.pstar, "mlp": mlp_info}
+    npatch = g.num_patches
+    level_variants = g.level_variants()
+    g.close()
     # ---- end to end through the C ABI with pinned host buffers, regrids included ----
+    # The same K coarse steps as the timed loop: a second solver spun up the same way
+    # (same steps, regrids and variants) starts from the timed loop's first state.
+    g = fb.Solver(gc)
+    _maybe_partition(g, args, local_rank)
+    g.initialize()
+    if mlp is not None:
+        g.set_pstar_seed(mlp)
+    t, dt, _ = _spinup(g, wl, 0.0, _initial_dt(wl, prob), wl["spinup"])
+    g.set_variant(tune["variant"])
+    g.set_level_variants(level_variants)
+    t, dt = _spinup(g, dict(wl, regrid_interval=0), t, dt, args.warmup)[:2]
+    if (t, dt) != (t_start, dt_start):
+        raise SystemExit("the end-to-end solver did not reach the timed loop's first state")
     per_patch = gc.meqn * (gc.mx + 2 * gc.mbc) * (gc.my + 2 * gc.mbc)
     cap = 2 * g.num_patches * per_patch
     hq = torch.empty(cap, dtype=torch.float64, pin_memory=True)
     g.get_q_ptr(hq.data_ptr())
-    e2e_steps = max(2 * max(wl["regrid_interval"], 1), min(args.steps, 40))
+    e2e_steps = args.steps
     torch.cuda.synchronize()
     te0 = time.perf_counter()
     e2e_cells, e2e_h2d, e2e_d2h, e2e_regrids = 0.0, 0.0, 0.0, 0
@@ -628,13 +650,9 @@ def run_ours(args, wl, rank, world, local_rank):
            "wall_ms_per_step": {k: round(v * 1e3 / e2e_steps, 4) for k, v in ph.items()},
            "protocol": "per coarse step: set_q from pinned host memory, advance, get_q to pinned host memory; "
                        "the workload's regrid (host tree edit, device repopulation, graph recapture) inside "
-                       "the wall-clock region"}
-    newton = None
-    if wl["name"].startswith("euler"):
-        h = g.newton_histogram()
-        newton = {"mean_iterations": float((np.arange(32) * h).sum() / max(h.sum(), 1)),
-                  "histogram": [int(v) for v in h[:12]], "pstar_start": args.pstar, "mlp": mlp_info}
-    npatch = g.num_patches
+                       "the wall-clock region; the same coarse steps as the device-timed loop, from the same "
+                       "state (a second solver spun up the same way)",
+           "cells_match_timed_loop": bool(e2e_cells == cells_all)}
     g.close()
     fp64 = None
     if args.precision != "fp64" and not args.no_fp64_compare:

@@ -206,6 +206,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_cell_updates": [P, dp],
         "fc2d_b200_synchronize": [P],
         "fc2d_b200_last_update_stats": [P, dp, dp, ip, ip],
+        "fc2d_b200_last_step_timing": [P, dp, dp],
         "fc2d_b200_last_regrid_stats": [P, dp],
         "fc2d_b200_set_timing": [P, I],
         "fc2d_b200_event_record": [P, I],
@@ -239,6 +240,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_set_variant": [P, I],
         "fc2d_b200_autotune": [P, I, ip, dp],
         "fc2d_b200_level_variants": [P, ip],
+        "fc2d_b200_set_level_variants": [P, ip],
         "fc2d_b200_output_ascii": [P, ctypes.c_char_p, I, D],
         "fc2d_b200_output_vtk": [P, ctypes.c_char_p, I],
         "fc2d_b200_write_vtk_file": [ctypes.c_char_p, I, I, I, I, ip, dp, ctypes.POINTER(ctypes.c_float)],
@@ -597,6 +599,13 @@ class Solver:
         self._check("fc2d_b200_level_variants", self.lib.fc2d_b200_level_variants(self.h, _ip(out)))
         return out
 
+    def set_level_variants(self, variants) -> None:
+        """Each level's variant (33 entries), e.g. another solver's level_variants()."""
+        v = np.ascontiguousarray(variants, dtype=np.int32)
+        if v.shape != (33,):
+            raise ValueError("33 per-level variants expected")
+        self._check("fc2d_b200_set_level_variants", self.lib.fc2d_b200_set_level_variants(self.h, _ip(v)))
+
     def autotune(self, reps: int = 3):
         """Time every variant on the current forest (q unchanged), keep the fastest,
         then keep per level the variant fastest on that level (level_variants()).
@@ -711,3 +720,10 @@ class Solver:
                                                          ctypes.byref(ul), ctypes.byref(tl)))
         return {"update_ms": ms.value, "update_bytes": by.value, "update_launches": ul.value,
                 "total_launches": tl.value}
+
+    def last_step_timing(self) -> dict:
+        """The most recent advance: host schedule time and the device span of its work (ms)."""
+        h, d = ctypes.c_double(), ctypes.c_double()
+        self._check("fc2d_b200_last_step_timing",
+                    self.lib.fc2d_b200_last_step_timing(self.h, ctypes.byref(h), ctypes.byref(d)))
+        return {"host_ms": h.value, "device_ms": d.value}

@@ -92,6 +92,52 @@ struct DevVec {
     }
 };
 
+// A typed range of a TableArena.
+template <class T>
+struct DevView {
+    T* p = nullptr;
+    size_t n = 0;
+};
+
+// The ghost-fill and time-sync tables of a forest: one device allocation filled from
+// one pinned host buffer, so a regrid uploads them with one copy.  Both grow by a
+// quarter beyond the largest forest seen and are reused from one regrid to the next.
+struct TableArena {
+    char* dev = nullptr;
+    char* host = nullptr;
+    size_t cap = 0, used = 0;
+    ~TableArena()
+    {
+        if (dev) cudaFree(dev);
+        if (host) cudaFreeHost(host);
+    }
+    cudaError_t reserve(size_t bytes)
+    {
+        if (bytes <= cap) return cudaSuccess;
+        if (dev) cudaFree(dev);
+        if (host) cudaFreeHost(host);
+        dev = nullptr; host = nullptr; cap = 0;
+        const size_t c = bytes + bytes / 4 + (64 << 10);
+        cudaError_t e = cudaMalloc(&dev, c);
+        if (e == cudaSuccess) e = cudaHostAlloc(&host, c, cudaHostAllocDefault);
+        if (e != cudaSuccess) return e;
+        cap = c;
+        return cudaSuccess;
+    }
+    static size_t span(size_t bytes) { return (bytes + 255) & ~(size_t)255; }
+    // stage v at the next 256-byte boundary; its device range
+    template <class T>
+    DevView<T> put(const std::vector<T>& v)
+    {
+        DevView<T> r;
+        r.p = reinterpret_cast<T*>(dev + used);
+        r.n = v.size();
+        if (!v.empty()) std::memcpy(host + used, v.data(), v.size() * sizeof(T));
+        used += span(v.size() * sizeof(T));
+        return r;
+    }
+};
+
 struct LevelRanges {
     int copy_off = 0, copy_n = 0, avg_off = 0, avg_n = 0, interp_off = 0, interp_n = 0, phys_off = 0, phys_n = 0;
     int ti_off = 0, ti_n = 0, sync_start_off = 0, sync_np = 0;   // sync groups [sync_start_off, + sync_np)
@@ -148,17 +194,18 @@ struct fc2d_b200_solver {
     DevVec<double> snap;                           // batch regrid: q of instances whose forest is unchanged
     DevVec<int> keep_dev;
     std::vector<double> aux_host;                  // static aux mirror (level-major)
-    DevVec<CopyEnt> t_copy;
-    DevVec<AvgEnt> t_avg;
+    TableArena arena;                              // the tables below, on the device
+    DevView<FillOp> t_copy;                        // copy2ghost region ops
+    DevView<FillOp> t_avg;                         // average2ghost region ops
     double* area = nullptr;                        // cubed sphere: cell areas per patch (Dims::narea per patch)
     bool sphere = false;                           // the cubed-sphere app (manifold, 6 blocks)
     SphereFlow flow{};                             // its rotation: psi = omega (axis . x)
     DevVec<MetricOp> metric_dev;
     DevVec<double> minmax_dev;
-    DevVec<InterpEnt> t_interp;
-    DevVec<PhysEnt> t_phys;
-    DevVec<int> t_ti, t_sync_start;
-    DevVec<SyncOp> t_sync;
+    DevView<InterpEnt> t_interp;
+    DevView<PhysEnt> t_phys;
+    DevView<int> t_ti, t_sync_start;
+    DevView<SyncOp> t_sync;
     Tables tables;                                 // host copy of the gather tables (buffers reused)
     TableWork table_work;
     std::vector<unsigned char> interp_written;     // interpolation-chain scratch, all zero between uses
@@ -210,6 +257,11 @@ struct fc2d_b200_solver {
     double upd_ms = 0, upd_bytes = 0;
     int upd_launches = 0, total_launches = 0;
     std::vector<cudaEvent_t> user_ev;
+    // the most recent advance: host time building its schedule (the first traversal),
+    // and the span of its work on the stream (events before the first copy and after
+    // the last launch), fc2d_b200_last_step_timing
+    cudaEvent_t step_ev[2] = {nullptr, nullptr};
+    double step_host_ms = 0, step_device_ms = 0;
     // per-launch update parameters in device memory (filled each advance)
     static constexpr int PCAP = 1 << 14;
     StepParams* params_dev = nullptr;
@@ -331,7 +383,6 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
 {
     const Forest& f = s->forest;
     const std::vector<PatchDesc> hd = make_desc(f);
-    if (!hd.empty()) CK(cudaMemcpyAsync(s->desc, hd.data(), hd.size() * sizeof(PatchDesc), cudaMemcpyHostToDevice, s->st));
     Tables& T = s->tables;
     {
         std::string err;
@@ -360,8 +411,8 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
             off[33] = (int)n;
             v.resize(n);
         };
-        filter(T.copy, T.copy_off, [&](const CopyEnt& e) { return fill[e.dst / nq] != 0; });
-        filter(T.avg, T.avg_off, [&](const AvgEnt& e) { return fill[e.dst / nq] != 0; });
+        filter(T.copy, T.copy_off, [&](const FillOp& e) { return fill[e.dst] != 0; });
+        filter(T.avg, T.avg_off, [&](const FillOp& e) { return fill[e.dst] != 0; });
         filter(T.phys, T.phys_off, [&](const PhysEnt& e) { return fill[e.dst / nq] != 0; });
         filter(T.interp, T.interp_off, [&](const InterpEnt& e) { return own[e.dst / nq] == me; });
         filter(T.ti, T.ti_off, [&](int p) { return fill[p] != 0; });
@@ -399,16 +450,24 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
         r.ti_off = T.ti_off[l]; r.ti_n = T.ti_off[l + 1] - T.ti_off[l];
         r.sync_start_off = T.grp_off[l]; r.sync_np = T.grp_off[l + 1] - T.grp_off[l];
     }
-    const std::vector<CopyEnt>& copy = T.copy;
-    const std::vector<AvgEnt>& avg = T.avg;
     const std::vector<InterpEnt>& interp = T.interp;
-    const std::vector<PhysEnt>& phys = T.phys;
-    const std::vector<int>& ti = T.ti;
-    const std::vector<SyncOp>& sync = T.sync;
-    const std::vector<int>& sync_start = T.sync_start;
-    CK(s->t_copy.assign(copy, s->st));
-    CK(s->t_avg.assign(avg, s->st));
-    CK(s->t_interp.assign(interp, s->st));
+    {
+        TableArena& A = s->arena;
+        auto sz = [](const auto& v) { return TableArena::span(v.size() * sizeof(v[0])); };
+        CK(A.reserve(sz(hd) + sz(T.copy) + sz(T.avg) + sz(T.interp) + sz(T.phys) + sz(T.ti) + sz(T.sync) +
+                     sz(T.sync_start)));
+        A.used = 0;
+        const DevView<PatchDesc> dv = A.put(hd);       // staged here, then copied into the slab's descriptors
+        s->t_copy = A.put(T.copy);
+        s->t_avg = A.put(T.avg);
+        s->t_interp = A.put(T.interp);
+        s->t_phys = A.put(T.phys);
+        s->t_ti = A.put(T.ti);
+        s->t_sync = A.put(T.sync);
+        s->t_sync_start = A.put(T.sync_start);
+        if (A.used) CK(cudaMemcpyAsync(A.dev, A.host, A.used, cudaMemcpyHostToDevice, s->st));
+        if (dv.n) CK(cudaMemcpyAsync(s->desc, dv.p, dv.n * sizeof(PatchDesc), cudaMemcpyDeviceToDevice, s->st));
+    }
     {   // interpolation chains: reads of level l's entries against writes of level l-1's
         std::vector<unsigned char>& written = s->interp_written;
         if (written.size() < (size_t)f.np() * s->d.nq()) written.resize((size_t)f.np() * s->d.nq(), 0);
@@ -428,10 +487,6 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
             s->interp_chain[l] = clash ? 0 : 1;
         }
     }
-    CK(s->t_phys.assign(phys, s->st));
-    CK(s->t_ti.assign(ti, s->st));
-    CK(s->t_sync.assign(sync, s->st));
-    CK(s->t_sync_start.assign(sync_start, s->st));
     CK(cudaStreamSynchronize(s->st));
     return 0;
 }
@@ -603,8 +658,7 @@ static GatherSeg<E> seg(const E* table, int off, int n, double* dst, const doubl
 // ghost cells and read interior cells only, so their order does not matter
 static void average_copy_range(fc2d_b200_solver* s, int a, int b, int ca, int cb, int c)
 {
-    GatherSeg<AvgEnt> a0{nullptr, nullptr, nullptr, 0}, a1 = a0;
-    GatherSeg<CopyEnt> c0{nullptr, nullptr, nullptr, 0}, c1 = c0;
+    GatherSeg<FillOp> a0{nullptr, nullptr, nullptr, 0}, a1 = a0, c0 = a0, c1 = a0;
     if (lrange(a, b)) {
         const int off = s->lr[a].avg_off, n = s->lr[b].avg_off + s->lr[b].avg_n - off;
         if (n > 0) a0 = seg(s->t_avg.p, off, n, s->q, s->q);
@@ -1005,6 +1059,7 @@ extern "C" int fc2d_b200_destroy(fc2d_b200_solver_t* s)
     cudaStreamSynchronize(s->st);
     for (auto e : s->ev_pool) cudaEventDestroy(e);
     for (auto e : s->user_ev) cudaEventDestroy(e);
+    for (auto e : s->step_ev) if (e) cudaEventDestroy(e);
     cudaFree(s->q); cudaFree(s->qlast); if (s->qinterp) cudaFree(s->qinterp);
     if (s->aux) cudaFree(s->aux); cudaFree(s->regs); cudaFree(s->desc);
     free_spare(s);
@@ -1511,6 +1566,7 @@ static int traverse_advance(fc2d_b200_solver* s, double t, double dt)
 static int advance_launch(fc2d_b200_solver_t* s, double t, double dt)
 {
     if (!s || !s->initialized) return fail(FC2D_B200_ESTATE, "solver not initialized");
+    const double h0 = wall_ms();
     s->ev_used = 0;
     s->upd_launch_bytes.clear();
     s->upd_launches = 0;
@@ -1519,6 +1575,12 @@ static int advance_launch(fc2d_b200_solver_t* s, double t, double dt)
     s->emit = false; s->fill = true;
     int rc = traverse_advance(s, t, dt);
     if (rc) { s->emit = true; return rc; }
+    s->step_host_ms = wall_ms() - h0;
+    if (!s->step_ev[0]) {
+        CK(cudaEventCreate(&s->step_ev[0]));
+        CK(cudaEventCreate(&s->step_ev[1]));
+    }
+    CK(cudaEventRecord(s->step_ev[0], s->st));
     ProgrammaticScope pscope(s->programmatic);
     const int nupd = s->n_upd;
     rc = begin_cfl(s);
@@ -1563,6 +1625,7 @@ static int advance_launch(fc2d_b200_solver_t* s, double t, double dt)
     s->fill = true;
     if (rc) return rc;
     CK(cudaGetLastError());
+    CK(cudaEventRecord(s->step_ev[1], s->st));
     s->pending_t = t + dt;
     s->pending = true;
     return 0;
@@ -1575,6 +1638,11 @@ static int advance_finish(fc2d_b200_solver_t* s, double* maxcfl, double* cfl_ins
     if (!s->pending) return fail(FC2D_B200_ESTATE, "no advance in flight");
     s->pending = false;
     int rc = end_cfl(s, maxcfl, cfl_inst);
+    {
+        float m = 0;
+        if (s->step_ev[0] && cudaEventElapsedTime(&m, s->step_ev[0], s->step_ev[1]) == cudaSuccess) s->step_device_ms = m;
+        else { (void)cudaGetLastError(); s->step_device_ms = 0; }
+    }
     if (s->timing) {
         double ms = 0, bytes = 0;
         for (auto& pr : s->upd_launch_bytes) {
@@ -2075,6 +2143,14 @@ extern "C" int fc2d_b200_last_update_stats(const fc2d_b200_solver_t* s, double* 
     if (update_bytes) *update_bytes = s->upd_bytes;
     if (update_launches) *update_launches = s->upd_launches;
     if (total_launches) *total_launches = s->total_launches;
+    return 0;
+}
+
+extern "C" int fc2d_b200_last_step_timing(const fc2d_b200_solver_t* s, double* host_ms, double* device_ms)
+{
+    if (!s) return fail(FC2D_B200_EINVAL, "null solver");
+    if (host_ms) *host_ms = s->step_host_ms;
+    if (device_ms) *device_ms = s->step_device_ms;
     return 0;
 }
 
@@ -2666,6 +2742,28 @@ extern "C" int fc2d_b200_level_variants(const fc2d_b200_solver_t* s, int* varian
 {
     if (!s || !variant) return fail(FC2D_B200_EINVAL, "bad arguments");
     for (int l = 0; l < 33; l++) variant[l] = s->var_lev[l] >= 0 ? s->var_lev[l] : s->var;
+    return 0;
+}
+
+// A per-level choice made earlier (fc2d_b200_level_variants of a tuned solver of the
+// same shape) applied without timing anything.
+extern "C" int fc2d_b200_set_level_variants(fc2d_b200_solver_t* s, const int* variant)
+{
+    DeviceScope dev_scope_(s);
+    if (!s || !variant) return fail(FC2D_B200_EINVAL, "bad arguments");
+    for (int l = 0; l < 33; l++)
+        if (variant[l] < 0 || variant[l] >= (int)s->vars.size())
+            return fail(FC2D_B200_EINVAL, "no such variant for level " + std::to_string(l));
+    for (int l = 0; l < 33; l++) {
+        bool seen = false;
+        for (int k = 0; k < l; k++) seen = seen || variant[k] == variant[l];
+        if (seen) continue;
+        cudaError_t e = s->vars[variant[l]]->fn(nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr,
+                                                LevelGroup{1, {0}}, nullptr, s->st);
+        if (e != cudaSuccess) return fail(FC2D_B200_ECUDA, std::string("kernel setup: ") + cudaGetErrorString(e));
+    }
+    for (int l = 0; l < 33; l++) s->var_lev[l] = variant[l];
+    invalidate_graph(s);
     return 0;
 }
 

@@ -603,32 +603,6 @@ struct LastWriter {
     }
 };
 
-// Entries of the tables whose destinations are cells of the patch being visited (copy:
-// its ghost cells from its same-size neighbours; average: a coarse patch's ghost cells
-// from its finer neighbours).  These need no last-writer map: the four face strips
-// (ghost rows along 1..mx or 1..my) and the four corner blocks are disjoint, each face
-// or corner has one same-size neighbour, and the children of one coarse ghost cell lie
-// in one of the two half-size neighbours of its face, so no cell is written twice.
-inline bool src_in(const CopyEnt& e, long nall) { return e.src >= 0 && e.src < nall; }
-inline bool src_in(const AvgEnt& e, long nall)
-{
-    const long s = e.src, s3 = s + e.sx + e.sy;
-    return s >= 0 && s < nall && s + e.sx >= 0 && s + e.sx < nall && s + e.sy >= 0 && s + e.sy < nall && s3 >= 0 && s3 < nall;
-}
-template <class E>
-struct PatchWriter {
-    std::vector<E>& v;
-    int base, nxy;                         // absolute offset of the visited patch's cell 0; cells per plane
-    long nall;                             // cells of the q slab (sources index into it)
-    bool outside = false;
-    void put(const E& e)
-    {
-        const int k = e.dst - base;
-        if (k < 0 || k >= nxy || !src_in(e, nall)) { outside = true; return; }
-        v.push_back(e);
-    }
-};
-
 // Runs tasks 0..n-1 on up to nt threads (the calling one included).
 template <class Fn>
 void run_tasks(int n, int nt, Fn fn)
@@ -663,96 +637,99 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out,
     const int nxy = T.nx * (my + 2 * mbc);
     int nt = (int)std::thread::hardware_concurrency();
     nt = std::max(1, std::min(nt, std::min(16, np / 64)));
-    // one chunk of patches per task for copy and average (destinations in the visited
-    // patch); interpolation (destinations in the next finer level) one task per level
-    const int nchunk = nt == 1 ? 1 : 4 * nt;
     int nlev = 0;
     for (int l = 0; l < 33; l++) if (f.lev_off[l + 1] > f.lev_off[l]) nlev = l + 1;
-    w.copy.resize(nchunk); w.avg.resize(nchunk); w.interp.resize(33); w.slots.resize(33);
-    w.copy_first.assign(np + 1, 0); w.avg_first.assign(np + 1, 0);
+    w.interp.resize(33); w.slots.resize(33);
     std::atomic<int> bad{0};
 
     // ---- copy2ghost (faces, then corners, of each patch: fclaw2d_clawpatch46_copy.f) and
-    // ---- average2ghost (coarse = this patch: faces, then corners) ----
-    auto copy_avg = [&](int c) {
-        const int a = (int)((long)np * c / nchunk), b = (int)((long)np * (c + 1) / nchunk);
-        std::vector<CopyEnt>& vc = w.copy[c];
-        std::vector<AvgEnt>& va = w.avg[c];
-        vc.clear(); va.clear();
-        PatchWriter<CopyEnt> WC{vc, 0, nxy, (long)np * nq};
-        for (int ip = a; ip < b; ip++) {
-            w.copy_first[ip] = (int)vc.size();
-            WC.base = ip * nq;
-            const PatchInfo& P = f.p[ip];
-            for (int fc = 0; fc < 4; fc++) {
-                if (P.face_type[fc] != NB_SAME) continue;
-                const int n = P.face_nbr[fc][0];
-                const TableCtx::Aff A = T.same_map(P, f.p[n]);
-                int ilo, ihi, jlo, jhi;
-                if (fc == 0) { ilo = 1 - mbc; ihi = 0; jlo = 1; jhi = my; }
-                else if (fc == 1) { ilo = mx + 1; ihi = mx + mbc; jlo = 1; jhi = my; }
-                else if (fc == 2) { ilo = 1; ihi = mx; jlo = 1 - mbc; jhi = 0; }
-                else { ilo = 1; ihi = mx; jlo = my + 1; jhi = my + mbc; }
-                for (int j = jlo; j <= jhi; j++)
-                    for (int i = ilo; i <= ihi; i++) {
-                        int i2, j2; A.map(i, j, i2, j2);
-                        WC.put({T.cell(ip, i, j), T.cell(n, i2, j2)});
-                    }
-            }
-            for (int cr = 0; cr < 4; cr++) {
-                if (!P.has_corner[cr] || P.corner_type[cr] != NB_SAME) continue;
-                const int n = P.corner_nbr[cr];
-                const TableCtx::Aff A = T.same_map(P, f.p[n]);
-                for (int ibc = 1; ibc <= mbc; ibc++)
-                    for (int jbc = 1; jbc <= mbc; jbc++) {
-                        const int i1 = (cr & 1) ? mx + ibc : 1 - ibc, j1 = (cr & 2) ? my + jbc : 1 - jbc;
-                        int i2, j2; A.map(i1, j1, i2, j2);
-                        WC.put({T.cell(ip, i1, j1), T.cell(n, i2, j2)});
-                    }
-            }
+    // ---- average2ghost (coarse = this patch: faces, then corners) as region ops ----
+    // The ghost-fill kernel enumerates each op's cells and applies its map.  Copy
+    // destinations (the four face strips along 1..mx or 1..my and the four corner
+    // blocks) are disjoint, each face or corner has one same-size neighbour, and the
+    // children of one coarse ghost cell lie in one of the two half-size neighbours of
+    // its face, so no cell is written twice and the ops' order does not matter.
+    auto in_box = [&](int i, int j) { return 1 - mbc <= i && i <= mx + mbc && 1 - mbc <= j && j <= my + mbc; };
+    auto region_box = [&](int region, int& ilo, int& ihi, int& jlo, int& jhi) {
+        if (region == 0) { ilo = 1 - mbc; ihi = 0; jlo = 1; jhi = my; }
+        else if (region == 1) { ilo = mx + 1; ihi = mx + mbc; jlo = 1; jhi = my; }
+        else if (region == 2) { ilo = 1; ihi = mx; jlo = 1 - mbc; jhi = 0; }
+        else if (region == 3) { ilo = 1; ihi = mx; jlo = my + 1; jhi = my + mbc; }
+        else {
+            const int cr = region - 4;
+            ilo = (cr & 1) ? mx + 1 : 1 - mbc; ihi = ilo + mbc - 1;
+            jlo = (cr & 2) ? my + 1 : 1 - mbc; jhi = jlo + mbc - 1;
         }
-        PatchWriter<AvgEnt> WA{va, 0, nxy, (long)np * nq};
-        auto valid = [&](int i, int j) { return 1 <= i && i <= mx && 1 <= j && j <= my; };
-        for (int ip = a; ip < b; ip++) {
-            w.avg_first[ip] = (int)va.size();
-            WA.base = ip * nq;
-            const PatchInfo& C = f.p[ip];
-            if (!C.on_cf) continue;
-            // the four children of coarse ghost cell (ic, jc) in F, skipped unless all are
-            // interior cells of F (fclaw2d_clawpatch_is_valid_average)
-            auto emit = [&](int ic, int jc, int fi, const TableCtx::Aff& F, bool check) {
-                int ci[4], cj[4];
+    };
+    auto op = [](int dst, int src, int region, const TableCtx::Aff& A) {
+        return FillOp{dst, src, region, 0, (int)A.ci, (int)A.cj, (int)A.ii, (int)A.ij, (int)A.ji, (int)A.jj};
+    };
+    // a copy region's sources: the map is affine, so the region's four corner cells
+    // bound them; all must lie in the source patch (with its ghost cells)
+    auto copy_ok = [&](int region, const TableCtx::Aff& A) {
+        int ilo, ihi, jlo, jhi, i2, j2;
+        region_box(region, ilo, ihi, jlo, jhi);
+        for (int c = 0; c < 4; c++) {
+            A.map((c & 1) ? ihi : ilo, (c & 2) ? jhi : jlo, i2, j2);
+            if (!in_box(i2, j2)) return false;
+        }
+        return true;
+    };
+    // an average corner's children (its face ops keep only cells whose children are
+    // interior cells of the fine patch, in the kernel)
+    auto avg_corner_ok = [&](int region, const TableCtx::Aff& F) {
+        int ilo, ihi, jlo, jhi, i2, j2;
+        region_box(region, ilo, ihi, jlo, jhi);
+        for (int jc = jlo; jc <= jhi; jc++)
+            for (int ic = ilo; ic <= ihi; ic++)
                 for (int m = 0; m < 4; m++) {
-                    F.map(2 * ic + (m & 1), 2 * jc + (m >> 1), ci[m], cj[m]);
-                    if (check && !valid(ci[m], cj[m])) return;
+                    F.map(2 * ic + (m & 1), 2 * jc + (m >> 1), i2, j2);
+                    if (!in_box(i2, j2)) return false;
                 }
-                const int src = T.cell(fi, ci[0], cj[0]);
-                WA.put({T.cell(ip, ic, jc), src, T.cell(fi, ci[1], cj[1]) - src, T.cell(fi, ci[2], cj[2]) - src});
-            };
-            for (int fc = 0; fc < 4; fc++) {
-                if (C.face_type[fc] != NB_HALF) continue;
-                for (int ig = 0; ig < 2; ig++) {
-                    const int fi = C.face_nbr[fc][ig];
-                    const TableCtx::Aff F = T.child_map(C, f.p[fi]);
-                    if (fc < 2) {
-                        for (int jc = 1; jc <= my; jc++)
-                            for (int ibc = 1; ibc <= mbc; ibc++) emit((fc == 0) ? 1 - ibc : mx + ibc, jc, fi, F, true);
-                    } else {
-                        for (int jbc = 1; jbc <= mbc; jbc++)
-                            for (int ic = 1; ic <= mx; ic++) emit(ic, (fc == 2) ? 1 - jbc : my + jbc, fi, F, true);
+        return true;
+    };
+    auto regions = [&]() {
+        out.copy.clear(); out.avg.clear();
+        bool good = true;
+        for (int l = 0; l < 33; l++) {
+            out.copy_off[l] = (int)out.copy.size();
+            out.avg_off[l] = (int)out.avg.size();
+            for (int ip = f.lev_off[l]; ip < f.lev_off[l + 1]; ip++) {
+                const PatchInfo& P = f.p[ip];
+                for (int fc = 0; fc < 4; fc++) {
+                    if (P.face_type[fc] != NB_SAME) continue;
+                    const int n = P.face_nbr[fc][0];
+                    const TableCtx::Aff A = T.same_map(P, f.p[n]);
+                    good = good && copy_ok(fc, A);
+                    out.copy.push_back(op(ip, n, fc, A));
+                }
+                for (int cr = 0; cr < 4; cr++) {
+                    if (!P.has_corner[cr] || P.corner_type[cr] != NB_SAME) continue;
+                    const int n = P.corner_nbr[cr];
+                    const TableCtx::Aff A = T.same_map(P, f.p[n]);
+                    good = good && copy_ok(4 + cr, A);
+                    out.copy.push_back(op(ip, n, 4 + cr, A));
+                }
+                if (!P.on_cf) continue;
+                for (int fc = 0; fc < 4; fc++) {
+                    if (P.face_type[fc] != NB_HALF) continue;
+                    for (int ig = 0; ig < 2; ig++) {
+                        const int fi = P.face_nbr[fc][ig];
+                        out.avg.push_back(op(ip, fi, fc, T.child_map(P, f.p[fi])));
                     }
                 }
-            }
-            for (int cr = 0; cr < 4; cr++) {
-                if (!C.has_corner[cr] || C.corner_type[cr] != NB_HALF) continue;
-                const int fi = C.corner_nbr[cr];
-                const TableCtx::Aff F = T.child_map(C, f.p[fi]);
-                for (int ibc = 1; ibc <= mbc; ibc++)
-                    for (int jbc = 1; jbc <= mbc; jbc++)
-                        emit((cr & 1) ? mx + ibc : 1 - ibc, (cr & 2) ? my + jbc : 1 - jbc, fi, F, false);
+                for (int cr = 0; cr < 4; cr++) {
+                    if (!P.has_corner[cr] || P.corner_type[cr] != NB_HALF) continue;
+                    const int fi = P.corner_nbr[cr];
+                    const TableCtx::Aff F = T.child_map(P, f.p[fi]);
+                    good = good && avg_corner_ok(4 + cr, F);
+                    out.avg.push_back(op(ip, fi, 4 + cr, F));
+                }
             }
         }
-        if (WC.outside || WA.outside) bad = 1;
+        out.copy_off[33] = (int)out.copy.size();
+        out.avg_off[33] = (int)out.avg.size();
+        if (!good) bad = 1;
     };
 
     // ---- interpolate2ghost (coarse = level l): faces of all coarse patches, then corners ----
@@ -812,37 +789,15 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out,
         if (W.outside) bad = 1;
     };
     // the finest levels hold most patches: their interpolation tasks go first
-    run_tasks(nchunk + nlev, nt, [&](int k) {
+    run_tasks(nlev + 1, nt, [&](int k) {
         if (k < nlev) interp(nlev - 1 - k);
-        else copy_avg(k - nlev);
+        else regions();
     });
     if (bad) { err = "a ghost-fill table writes outside its destination patches"; return false; }
 
-    // flat tables in level order: the chunks are contiguous in slot order, so are the levels
-    auto concat = [&](std::vector<std::vector<CopyEnt>>* pc, std::vector<std::vector<AvgEnt>>* pa) {
-        size_t tot = 0;
-        if (pc) for (auto& v : *pc) tot += v.size();
-        if (pa) for (auto& v : *pa) tot += v.size();
-        return tot;
-    };
-    out.copy.resize(concat(&w.copy, nullptr));
-    out.avg.resize(concat(nullptr, &w.avg));
-    {
-        size_t oc = 0, oa = 0;
-        for (int c = 0; c < nchunk; c++) {
-            const int a = (int)((long)np * c / nchunk), b = (int)((long)np * (c + 1) / nchunk);
-            for (int ip = a; ip < b; ip++) { w.copy_first[ip] += (int)oc; w.avg_first[ip] += (int)oa; }
-            std::copy(w.copy[c].begin(), w.copy[c].end(), out.copy.begin() + oc);
-            std::copy(w.avg[c].begin(), w.avg[c].end(), out.avg.begin() + oa);
-            oc += w.copy[c].size(); oa += w.avg[c].size();
-        }
-        w.copy_first[np] = (int)oc; w.avg_first[np] = (int)oa;
-    }
     out.interp.clear(); out.phys.clear(); out.ti.clear(); out.sync.clear(); out.sync_start.assign(1, 0);
     for (int l = 0; l < 33; l++) {
         const int p0 = f.lev_off[l], p1 = f.lev_off[l + 1];
-        out.copy_off[l] = w.copy_first[p0];
-        out.avg_off[l] = w.avg_first[p0];
         out.interp_off[l] = (int)out.interp.size();
         out.phys_off[l] = (int)out.phys.size();
         out.ti_off[l] = (int)out.ti.size();
@@ -923,8 +878,6 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out,
             if (nops) out.sync_start.push_back((int)out.sync.size());
         }
     }
-    out.copy_off[33] = (int)out.copy.size();
-    out.avg_off[33] = (int)out.avg.size();
     out.interp_off[33] = (int)out.interp.size();
     out.phys_off[33] = (int)out.phys.size();
     out.ti_off[33] = (int)out.ti.size();

@@ -159,11 +159,11 @@ struct PartitionPlan {
 // The plan of `rank` among `size` ranks for forest f (pure host computation).
 void make_partition(const Forest& f, int rank, int size, PartitionPlan& out);
 
-// Gather tables of a forest, flat in level order: level l's entries of table x are
+// Ghost-fill tables of a forest, flat in level order: level l's entries of table x are
 // x[x_off[l], x_off[l + 1]).
 struct Tables {
-    std::vector<CopyEnt> copy;       // copy2ghost(level)
-    std::vector<AvgEnt> avg;         // average2ghost(level): level is the coarse level
+    std::vector<FillOp> copy;        // copy2ghost(level): region ops of the level's patches
+    std::vector<FillOp> avg;         // average2ghost(level): level is the coarse level
     std::vector<InterpEnt> interp;   // interpolate2ghost(level): level is the coarse level
     std::vector<PhysEnt> phys;       // setphysical(level)
     std::vector<int> ti;             // patches with fine-grid neighbours (fclaw2d_timeinterp)
@@ -177,11 +177,8 @@ struct Tables {
 // Buffers build_tables keeps between calls (their pages stay mapped from one regrid
 // to the next).
 struct TableWork {
-    std::vector<std::vector<CopyEnt>> copy;
-    std::vector<std::vector<AvgEnt>> avg;
     std::vector<std::vector<InterpEnt>> interp;
     std::vector<std::vector<int>> slots;
-    std::vector<int> copy_first, avg_first;
 };
 
 // inflow: mthbc = 0 sides are set to a constant state (PhysEnt.cst = 1, src unused).

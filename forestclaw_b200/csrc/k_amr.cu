@@ -28,21 +28,9 @@ static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 // The gather kernels take up to two table segments, each with its own arrays:
 // a ghost-fill stage on q and the same stage on the time-interpolated copy
 // write different arrays and read cells the other does not write, so they
-// share a launch.  One thread per (entry, field): segment 0's threads first,
-// field-major within a segment, so a warp handles consecutive entries of one
-// field.  The fields of an entry are independent (same arithmetic per field).
-template <class E>
-__device__ __forceinline__ bool gather_index(const GatherSeg<E>& s0, const GatherSeg<E>& s1, int meqn, long t,
-                                             const GatherSeg<E>*& g, int& e, int& m)
-{
-    const long n0 = (long)s0.n * meqn;
-    g = &s0;
-    if (t >= n0) { t -= n0; g = &s1; }
-    if (t >= (long)g->n * meqn) return false;
-    m = (int)(t / g->n);
-    e = (int)(t - (long)m * g->n);
-    return true;
-}
+// share a launch.  Interpolation and physical BCs: one thread per (entry, field),
+// segment 0's threads first, field-major within a segment, so a warp handles
+// consecutive entries of one field (the fields of an entry are independent).
 template <class E>
 __device__ __forceinline__ bool gather_item(const GatherSeg<E>& s0, const GatherSeg<E>& s1, int meqn,
                                             const GatherSeg<E>*& g, int& e, int& m)
@@ -57,64 +45,135 @@ __device__ __forceinline__ bool gather_item(const GatherSeg<E>& s0, const Gather
     return true;
 }
 
-__device__ __forceinline__ void copy_item(const GatherSeg<CopyEnt>* g, int e, int m, int nxy)
+// Fortran cell (i, j) of the k-th ghost cell of a region op (FillOp): faces row by row
+// with i fastest, corners likewise; the cells a region covers, below.
+__device__ __forceinline__ int region_cells(int region, int mx, int my, int mbc)
 {
-    const CopyEnt c = g->e[e];
-    g->dst[c.dst + m * nxy] = g->src[c.src + m * nxy];
+    return region < 2 ? mbc * my : (region < 4 ? mx * mbc : mbc * mbc);
+}
+__device__ __forceinline__ void region_cell(int region, int k, int mx, int my, int mbc, int& i, int& j)
+{
+    if (region < 2) {
+        i = (region == 0 ? 1 - mbc : mx + 1) + k % mbc;
+        j = 1 + k / mbc;
+    } else if (region < 4) {
+        i = 1 + k % mx;
+        j = (region == 2 ? 1 - mbc : my + 1) + k / mx;
+    } else {
+        const int cr = region - 4;
+        i = ((cr & 1) ? mx + 1 : 1 - mbc) + k % mbc;
+        j = ((cr & 2) ? my + 1 : 1 - mbc) + k / mbc;
+    }
 }
 
-__device__ __forceinline__ void average_item(const GatherSeg<AvgEnt>* g, int e, int m, int nq, int nx, int nxy,
-                                             const double* __restrict__ area)
+// One ghost cell of a copy op, every field: the fields are read before any is written.
+__device__ __forceinline__ void copy_cell(const GatherSeg<FillOp>* g, int o, int k, int mx, int my, int mbc,
+                                          int meqn, int nx, int nxy)
 {
-    double* __restrict__ dst = g->dst;
-    const double* __restrict__ src = g->src;
-    const AvgEnt c = g->e[e];
-    const int o1 = c.sx, o2 = c.sy, o3 = c.sx + c.sy;
+    const FillOp op = g->e[o];
+    if (k >= region_cells(op.region, mx, my, mbc)) return;
+    int i, j;
+    region_cell(op.region, k, mx, my, mbc, i, j);
+    const int i2 = op.ci + op.ii * i + op.ij * j, j2 = op.cj + op.ji * i + op.jj * j;
+    const long nq = (long)nxy * meqn;
+    double* d = g->dst + op.dst * nq + (j + mbc - 1) * nx + (i + mbc - 1);
+    const double* s = g->src + op.src * nq + (j2 + mbc - 1) * nx + (i2 + mbc - 1);
+    for (int m0 = 0; m0 < meqn; m0 += 4) {
+        double v[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (m0 + u < meqn) v[u] = s[(m0 + u) * nxy];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (m0 + u < meqn) d[(m0 + u) * nxy] = v[u];
+    }
+}
+
+// One coarse ghost cell of an average op, every field: the mean of its four children
+// (fine cells at (0,0), (1,0), (0,1), (1,1) of the coarse cell's own axes), in that order.
+__device__ __forceinline__ void average_cell(const GatherSeg<FillOp>* g, int o, int k, int mx, int my, int mbc,
+                                             int meqn, int nx, int nxy, const double* __restrict__ area)
+{
+    const FillOp op = g->e[o];
+    if (k >= region_cells(op.region, mx, my, mbc)) return;
+    int ic, jc;
+    region_cell(op.region, k, mx, my, mbc, ic, jc);
+    int cc[4];                                      // children: plane-0 offsets in the fine patch
+    for (int c = 0; c < 4; c++) {
+        const int x = 2 * ic + (c & 1), y = 2 * jc + (c >> 1);
+        const int i2 = op.ci + op.ii * x + op.ij * y, j2 = op.cj + op.ji * x + op.jj * y;
+        // a face keeps the coarse cells whose children are all interior fine cells
+        if (op.region < 4 && (i2 < 1 || i2 > mx || j2 < 1 || j2 > my)) return;
+        cc[c] = (j2 + mbc - 1) * nx + (i2 + mbc - 1);
+    }
+    const int o1 = cc[1] - cc[0], o2 = cc[2] - cc[0], o3 = o1 + o2;
+    const long nq = (long)nxy * meqn;
+    double* __restrict__ d = g->dst + op.dst * nq + (jc + mbc - 1) * nx + (ic + mbc - 1);
+    const double* __restrict__ src = g->src + op.src * nq + cc[0];
     if (area) {
         // manifold (fclaw2d_clawpatch46_average.f:96-115): sum(q_f a_f) / sum(a_f); the
         // area array of a patch has one ring more than q: cell (ic, jc) of q's padded
         // layout is (ic + 1, jc + 1) of a row of nx + 2
-        const int p = c.src / nq, ny = nxy / nx, na = (nx + 2) * (ny + 2);
-        const double* ap = area + (size_t)p * na;
-        auto ai = [&](int off) { const int cc = c.src - p * nq + off; return (cc / nx + 1) * (nx + 2) + cc % nx + 1; };
+        const int na = (nx + 2) * (nxy / nx + 2);
+        const double* ap = area + (size_t)op.src * na;
+        auto ai = [&](int off) { const int c = cc[0] + off; return (c / nx + 1) * (nx + 2) + c % nx + 1; };
         const double a0 = ap[ai(0)], a1 = ap[ai(o1)], a2 = ap[ai(o2)], a3 = ap[ai(o3)];
-        const double* f = src + c.src + m * nxy;
-        double sum = 0.0, af = 0.0;
-        sum = sum + f[0] * a0;  af = af + a0;
-        sum = sum + f[o1] * a1; af = af + a1;
-        sum = sum + f[o2] * a2; af = af + a2;
-        sum = sum + f[o3] * a3; af = af + a3;
-        dst[c.dst + m * nxy] = sum / af;
+        for (int m = 0; m < meqn; m++) {
+            const double* f = src + m * nxy;
+            double sum = 0.0, af = 0.0;
+            sum = sum + f[0] * a0;  af = af + a0;
+            sum = sum + f[o1] * a1; af = af + a1;
+            sum = sum + f[o2] * a2; af = af + a2;
+            sum = sum + f[o3] * a3; af = af + a3;
+            d[m * nxy] = sum / af;
+        }
         return;
     }
-    const double* f = src + c.src + m * nxy;
-    double sum = 0.0;
-    sum = sum + f[0];
-    sum = sum + f[o1];
-    sum = sum + f[o2];
-    sum = sum + f[o3];
-    dst[c.dst + m * nxy] = sum / 4.0;
+    for (int m = 0; m < meqn; m++) {
+        const double* f = src + m * nxy;
+        double sum = 0.0;
+        sum = sum + f[0];
+        sum = sum + f[o1];
+        sum = sum + f[o2];
+        sum = sum + f[o3];
+        d[m * nxy] = sum / 4.0;
+    }
+}
+
+// thread t of two op segments of `slot` threads per op: segment, op, cell
+__device__ __forceinline__ bool op_index(const GatherSeg<FillOp>& s0, const GatherSeg<FillOp>& s1, int slot, long t,
+                                         const GatherSeg<FillOp>*& g, int& o, int& k)
+{
+    const long n0 = (long)s0.n * slot;
+    g = &s0;
+    if (t >= n0) { t -= n0; g = &s1; }
+    if (t >= (long)g->n * slot) return false;
+    o = (int)(t / slot);
+    k = (int)(t - (long)o * slot);
+    return true;
 }
 
 // The average and copy stages of one ghost update in one launch: averaging writes
 // the ghost cells a coarse patch has beside finer neighbours, copying those beside
 // same-size neighbours (disjoint cells), and both read interior cells only, which
-// neither writes.  The average segments' threads come first.
-__global__ void k_average_copy(GatherSeg<AvgEnt> a0, GatherSeg<AvgEnt> a1, GatherSeg<CopyEnt> c0,
-                               GatherSeg<CopyEnt> c1, int nq, int nx, int nxy, int meqn,
+// neither writes.  One thread per (op, cell) with mbc * max(mx, my) threads per op
+// (a face's cells; a corner uses mbc * mbc of them); the average segments come first.
+__global__ void k_average_copy(GatherSeg<FillOp> a0, GatherSeg<FillOp> a1, GatherSeg<FillOp> c0,
+                               GatherSeg<FillOp> c1, int mx, int my, int mbc, int meqn,
                                const double* __restrict__ area)
 {
     grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
-    const long na = ((long)a0.n + a1.n) * meqn;
+    const int slot = mbc * (mx > my ? mx : my);
+    const int nx = mx + 2 * mbc, nxy = nx * (my + 2 * mbc);
+    const long na = ((long)a0.n + a1.n) * slot;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    int e, m;
+    const GatherSeg<FillOp>* g;
+    int o, k;
     if (t < na) {
-        const GatherSeg<AvgEnt>* g;
-        if (gather_index(a0, a1, meqn, t, g, e, m)) average_item(g, e, m, nq, nx, nxy, area);
-    } else {
-        const GatherSeg<CopyEnt>* g;
-        if (gather_index(c0, c1, meqn, t - na, g, e, m)) copy_item(g, e, m, nxy);
+        if (op_index(a0, a1, slot, t, g, o, k)) average_cell(g, o, k, mx, my, mbc, meqn, nx, nxy, area);
+    } else if (op_index(c0, c1, slot, t - na, g, o, k)) {
+        copy_cell(g, o, k, mx, my, mbc, meqn, nx, nxy);
     }
 }
 
@@ -678,13 +737,12 @@ void launch_restore_patches(const Dims& d, double* dst, const double* src, const
     if (n > 0) k_restore_patches<<<n, 256, 0, st>>>(dst, src, slots, d.nq());
 }
 
-void launch_average_copy(const Dims& d, const GatherSeg<AvgEnt>& a0, const GatherSeg<AvgEnt>& a1,
-                         const GatherSeg<CopyEnt>& c0, const GatherSeg<CopyEnt>& c1, const double* area,
+void launch_average_copy(const Dims& d, const GatherSeg<FillOp>& a0, const GatherSeg<FillOp>& a1,
+                         const GatherSeg<FillOp>& c0, const GatherSeg<FillOp>& c1, const double* area,
                          cudaStream_t st)
 {
-    const long n = ((long)a0.n + a1.n + c0.n + c1.n) * d.meqn;
-    if (n > 0)
-        launch_k(k_average_copy, nblk(n, 256), 256, 0, st, a0, a1, c0, c1, d.nq(), d.nx(), d.nxy(), d.meqn, area);
+    const long n = ((long)a0.n + a1.n + c0.n + c1.n) * d.mbc * (d.mx > d.my ? d.mx : d.my);
+    if (n > 0) launch_k(k_average_copy, nblk(n, 256), 256, 0, st, a0, a1, c0, c1, d.mx, d.my, d.mbc, d.meqn, area);
 }
 void launch_interp(const Dims& d, const GatherSeg<InterpEnt>& s0, const GatherSeg<InterpEnt>& s1, cudaStream_t st)
 {

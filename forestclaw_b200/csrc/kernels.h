@@ -67,20 +67,26 @@ const Step2Variant* step2_table_f32w_euler(int* n);
 // ---- ghost fill (k_amr.cu) ----------------------------------------------------
 // Gather tables: offsets are absolute indices of field 0 in the q slab; fields
 // follow at +m*nxy.
-struct CopyEnt { int dst, src; };                  // copy
-// average: the four fine cells of a coarse cell, src, src+sx, src+sy, src+sx+sy, are the
-// children at (0,0), (1,0), (0,1), (1,1) of the coarse cell's own (x, y) axes
-struct AvgEnt { int dst, src, sx, sy; };
+// Copy and average run from region ops instead: one op fills the ghost cells of patch
+// `dst` on one face (region 0..3: x-low, x-high, y-low, y-high) or corner (4..7: 4 + cr,
+// cr = 1 * (x-high) + 2 * (y-high)) from patch `src`, through the integer affine map
+// (x, y) -> (ci + ii x + ij y, cj + ji x + jj y) into src's Fortran cell indices:
+//   copy     (x, y) = (i, j), a ghost cell of dst; its same-size cell in src
+//   average  (x, y) = (2 ic + a, 2 jc + c), child (a, c) -- in dst's axes -- of dst's coarse
+//            ghost cell (ic, jc); face ops skip cells whose four children are not all
+//            interior cells of src (fclaw2d_clawpatch_is_valid_average)
+// A face covers mbc x my (x faces) or mx x mbc (y faces) cells, a corner mbc x mbc.
+struct FillOp { int dst, src, region, pad; int ci, cj, ii, ij, ji, jj; };
 struct InterpEnt { int dst, src, sub, pad; };      // sub = child position 0..3 (ii + 2 jj)
 struct PhysEnt { int dst, src, neg, cst; };        // neg: bit m set => negate field m; cst: constant state
 
 // One table segment of a gather stage: entries e[0..n) from src into dst.
 template <class E> struct GatherSeg { double* dst; const double* src; const E* e; int n; };
 // average segments and copy segments of one ghost update in one launch (disjoint ghost
-// cells); area: per-patch cell areas (nxy per patch, q's cell indexing) for the
+// cells); area: per-patch cell areas (one ring more than q per patch) for the
 // area-weighted average of a manifold, or null for the plain mean.
-void launch_average_copy(const Dims& d, const GatherSeg<AvgEnt>& a0, const GatherSeg<AvgEnt>& a1,
-                         const GatherSeg<CopyEnt>& c0, const GatherSeg<CopyEnt>& c1, const double* area,
+void launch_average_copy(const Dims& d, const GatherSeg<FillOp>& a0, const GatherSeg<FillOp>& a1,
+                         const GatherSeg<FillOp>& c0, const GatherSeg<FillOp>& c1, const double* area,
                          cudaStream_t st);
 void launch_restore_patches(const Dims& d, double* dst, const double* src, const int* slots, int n, cudaStream_t st);
 void launch_interp(const Dims& d, const GatherSeg<InterpEnt>& s0, const GatherSeg<InterpEnt>& s1, cudaStream_t st);

@@ -303,13 +303,15 @@ int fc2d_b200_partition_plan(const fc2d_b200_options_t* opt, int np, const int* 
  * each level alone and keeps, per level, the fastest there (a level's patch
  * count decides how its CTAs fill the device's waves); fc2d_b200_level_variants
  * reports the variant each level 0..32 uses.  fc2d_b200_set_variant sets one
- * variant for every level. */
+ * variant for every level; fc2d_b200_set_level_variants sets each level's (33
+ * entries, e.g. another solver's fc2d_b200_level_variants) without timing. */
 int fc2d_b200_num_variants(const fc2d_b200_solver_t* s, int* n, int* current);
 int fc2d_b200_variant_info(const fc2d_b200_solver_t* s, int v, int* threads, int* min_blocks, int* reg,
                            int* smem_bytes, int* persistent);
 int fc2d_b200_set_variant(fc2d_b200_solver_t* s, int v);
 int fc2d_b200_autotune(fc2d_b200_solver_t* s, int reps, int* best, double* ms);
 int fc2d_b200_level_variants(const fc2d_b200_solver_t* s, int* variant /* 33 entries */);
+int fc2d_b200_set_level_variants(fc2d_b200_solver_t* s, const int* variant /* 33 entries */);
 
 /* ---- batches of independent forests (instances; no counterpart in the reference) ----
  * One solver can hold up to FC2D_B200_MAX_INSTANCES independent forests with the
@@ -370,6 +372,12 @@ int fc2d_b200_synchronize(fc2d_b200_solver_t* s);
  * cells, q read + write + aux read). */
 int fc2d_b200_last_update_stats(const fc2d_b200_solver_t* s, double* update_ms, double* update_bytes,
                                 int* update_launches, int* total_launches);
+/* The most recent advance (fc2d_b200_advance or _advance_instances): host_ms, the
+ * wall time the host spent building its launch schedule before any device work;
+ * device_ms, the CUDA-event span of its work on the solver's stream, from the
+ * first copy of its parameters to the end of its last launch (a graph rebuilt
+ * after a regrid is captured inside that span). */
+int fc2d_b200_last_step_timing(const fc2d_b200_solver_t* s, double* host_ms, double* device_ms);
 /* Wall-clock breakdown of the most recent fc2d_b200_regrid, milliseconds
  * (ms[8]): 0 tagging on the device and the flags back on the host, 1 coarsen /
  * refine marks, smoothing and the 2:1-balanced leaves, 2 the new forest (neighbour

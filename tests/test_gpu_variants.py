@@ -91,3 +91,25 @@ def test_autotune_leaves_state_and_picks_a_variant(problem, kw):
     h = _solver(problem, **kw)
     _run(h, 0.002, 2)
     assert np.array_equal(_run(g, 0.002, 2), _run(h, 0.002, 2))
+
+
+def test_level_variants_carry_over_to_a_new_solver():
+    """A tuned solver's per-level choice applied to a fresh solver of the same shape
+    (fc2d_b200_set_level_variants): the same variants, the same trajectory, and an
+    index outside the compiled variants is refused."""
+    import forestclaw_b200 as fb
+    kw = dict(mx=16, my=16, minlevel=2, maxlevel=4, subcycle=1, time_sync=1)
+    g = _solver(DAM, fb.PREC_FP32WAVE, **kw)
+    _run(g, 0.002, 2)
+    g.autotune(reps=1)
+    lv = g.level_variants()
+    h = _solver(DAM, fb.PREC_FP32WAVE, **kw)
+    _run(h, 0.002, 2)
+    h.set_level_variants(lv)
+    assert np.array_equal(h.level_variants(), lv)
+    assert np.array_equal(_run(g, 0.002, 2), _run(h, 0.002, 2))
+    bad = lv.copy()
+    bad[3] = len(g.variants())
+    with pytest.raises(fb.B200Error):
+        h.set_level_variants(bad)
+    assert np.array_equal(h.level_variants(), lv)
