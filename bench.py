@@ -436,9 +436,11 @@ def _timed_steps(g, wl, steps, t, dt, flush):
                 regrid_phases=phases)
 
 
-def _roofline_pass(solvers, t_dt, flush, steps):
-    """Eager re-run of a few steps with a CUDA event pair around every update
-    launch: (update ms, algorithmic bytes, launches) of the fused update kernel."""
+def _roofline_pass(solvers, t_dt, flush, steps, wl=None):
+    """Eager run of `steps` steps with a CUDA event pair around every update launch:
+    (update ms, algorithmic bytes, launches) of the fused update kernel.  With `wl`
+    (one forest) the steps follow the workload's dt rule and regrids, as the timed
+    loop does; without it each solver takes steps of its fixed dt."""
     import torch
     ms, by, nl = 0.0, 0.0, 0
     for g in solvers:
@@ -450,12 +452,18 @@ def _roofline_pass(solvers, t_dt, flush, steps):
             t, dt = t_dt[i]
             if getattr(g, "ninst", 0):
                 g.advance_instances(dt)
+            elif wl is not None:
+                cfl = g.advance(t, dt)
+                dt1 = dt * 0.9 / cfl if wl.get("adapt_dt", wl["time_sync"]) else dt
+                t_dt[i] = (t + dt, dt1)
             else:
                 g.advance(t + k * dt, dt)
             st = g.last_update_stats()
             ms += st["update_ms"]
             by += st["update_bytes"]
             nl += st["update_launches"]
+            if wl is not None and wl["regrid_interval"] and (k + 1) % wl["regrid_interval"] == 0:
+                g.regrid()
     for g in solvers:
         g.set_timing(False)
     return ms, by, nl
@@ -532,6 +540,24 @@ def _bracket():
         torch.distributed.barrier()
 
 
+def _twin(gc, wl, prob, args, local_rank, mlp, variant, level_variants, start):
+    """A second solver brought to the timed loop's first state: the same spin-up,
+    regrids and variants, then the warm-up steps."""
+    import forestclaw_b200 as fb
+    g = fb.Solver(gc)
+    _maybe_partition(g, args, local_rank)
+    g.initialize()
+    if mlp is not None:
+        g.set_pstar_seed(mlp)
+    t, dt, _ = _spinup(g, wl, 0.0, _initial_dt(wl, prob), wl["spinup"])
+    g.set_variant(variant)
+    g.set_level_variants(level_variants)
+    t, dt = _spinup(g, dict(wl, regrid_interval=0), t, dt, args.warmup)[:2]
+    if (t, dt) != start:
+        raise SystemExit("a second solver did not reach the timed loop's first state")
+    return g, t, dt
+
+
 def run_ours(args, wl, rank, world, local_rank):
     """The measurement of one single-forest workload; the JSON dict on rank 0, else None."""
     import torch
@@ -568,9 +594,6 @@ def run_ours(args, wl, rank, world, local_rank):
     clocks = clk.stop() if rank == 0 else None
     step_ms, cells, launches, timed_regrid_ms, t, dt = (r["step_ms"], r["cells"], r["launches"], r["regrid_ms"],
                                                          r["t"], r["dt"])
-    nroof = max(2, min(args.steps, 4))
-    upd_ms, upd_bytes, upd_launches = _roofline_pass([g], [(t, dt)], flush, nroof)
-    t += nroof * dt
     from forestclaw_b200 import ranks
     total_ms, cells_all, value = ranks.aggregate(float(np.sum(step_ms)), cells, "cuda")
     newton = None
@@ -581,20 +604,14 @@ def run_ours(args, wl, rank, world, local_rank):
     npatch = g.num_patches
     level_variants = g.level_variants()
     g.close()
+    twin = lambda: _twin(gc, wl, prob, args, local_rank, mlp, tune["variant"], level_variants, (t_start, dt_start))
+    # ---- roofline: every update launch event-timed over the timed loop's K steps ----
+    g, t, dt = twin()
+    upd_ms, upd_bytes, upd_launches = _roofline_pass([g], [(t, dt)], flush, args.steps, wl)
+    g.close()
     # ---- end to end through the C ABI with pinned host buffers, regrids included ----
-    # The same K coarse steps as the timed loop: a second solver spun up the same way
-    # (same steps, regrids and variants) starts from the timed loop's first state.
-    g = fb.Solver(gc)
-    _maybe_partition(g, args, local_rank)
-    g.initialize()
-    if mlp is not None:
-        g.set_pstar_seed(mlp)
-    t, dt, _ = _spinup(g, wl, 0.0, _initial_dt(wl, prob), wl["spinup"])
-    g.set_variant(tune["variant"])
-    g.set_level_variants(level_variants)
-    t, dt = _spinup(g, dict(wl, regrid_interval=0), t, dt, args.warmup)[:2]
-    if (t, dt) != (t_start, dt_start):
-        raise SystemExit("the end-to-end solver did not reach the timed loop's first state")
+    # the same K coarse steps as the timed loop, from its first state
+    g, t, dt = twin()
     per_patch = gc.meqn * (gc.mx + 2 * gc.mbc) * (gc.my + 2 * gc.mbc)
     cap = 2 * g.num_patches * per_patch
     hq = torch.empty(cap, dtype=torch.float64, pin_memory=True)

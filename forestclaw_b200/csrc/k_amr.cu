@@ -25,17 +25,16 @@ bool programmatic_launch() { return tl_programmatic; }
 
 static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 
-// The gather kernels take up to two table segments, each with its own arrays:
+// The gather stages take up to two table segments, each with its own arrays:
 // a ghost-fill stage on q and the same stage on the time-interpolated copy
 // write different arrays and read cells the other does not write, so they
 // share a launch.  Interpolation and physical BCs: one thread per (entry, field),
 // segment 0's threads first, field-major within a segment, so a warp handles
 // consecutive entries of one field (the fields of an entry are independent).
 template <class E>
-__device__ __forceinline__ bool gather_item(const GatherSeg<E>& s0, const GatherSeg<E>& s1, int meqn,
-                                            const GatherSeg<E>*& g, int& e, int& m)
+__device__ __forceinline__ bool seg_item(const GatherSeg<E>& s0, const GatherSeg<E>& s1, int meqn, long t,
+                                         const GatherSeg<E>*& g, int& e, int& m)
 {
-    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long n0 = (long)s0.n * meqn;
     g = &s0;
     if (t >= n0) { t -= n0; g = &s1; }
@@ -44,6 +43,7 @@ __device__ __forceinline__ bool gather_item(const GatherSeg<E>& s0, const Gather
     e = (int)(t - (long)m * g->n);
     return true;
 }
+__device__ __forceinline__ long flat_index() { return (long)blockIdx.x * blockDim.x + threadIdx.x; }
 
 // Fortran cell (i, j) of the k-th ghost cell of a region op (FillOp): faces row by row
 // with i fastest, corners likewise; the cells a region covers, below.
@@ -98,25 +98,27 @@ __device__ __forceinline__ void average_cell(const GatherSeg<FillOp>* g, int o, 
     if (k >= region_cells(op.region, mx, my, mbc)) return;
     int ic, jc;
     region_cell(op.region, k, mx, my, mbc, ic, jc);
-    int cc[4];                                      // children: plane-0 offsets in the fine patch
-    for (int c = 0; c < 4; c++) {
-        const int x = 2 * ic + (c & 1), y = 2 * jc + (c >> 1);
-        const int i2 = op.ci + op.ii * x + op.ij * y, j2 = op.cj + op.ji * x + op.jj * y;
+    // children (0,0), (1,0), (0,1), (1,1) of (ic, jc) at (i0, j0), + (ii, ji), + (ij, jj)
+    // and + both: the map is an isometry, so the extremes of their indices are these sums
+    const int i0 = op.ci + op.ii * (2 * ic) + op.ij * (2 * jc), j0 = op.cj + op.ji * (2 * ic) + op.jj * (2 * jc);
+    if (op.region < 4) {
         // a face keeps the coarse cells whose children are all interior fine cells
-        if (op.region < 4 && (i2 < 1 || i2 > mx || j2 < 1 || j2 > my)) return;
-        cc[c] = (j2 + mbc - 1) * nx + (i2 + mbc - 1);
+        const int ilo = i0 + min(op.ii, 0) + min(op.ij, 0), ihi = i0 + max(op.ii, 0) + max(op.ij, 0);
+        const int jlo = j0 + min(op.ji, 0) + min(op.jj, 0), jhi = j0 + max(op.ji, 0) + max(op.jj, 0);
+        if (ilo < 1 || ihi > mx || jlo < 1 || jhi > my) return;
     }
-    const int o1 = cc[1] - cc[0], o2 = cc[2] - cc[0], o3 = o1 + o2;
+    const int c0 = (j0 + mbc - 1) * nx + (i0 + mbc - 1);   // child (0,0): plane-0 offset in the fine patch
+    const int o1 = op.ii + op.ji * nx, o2 = op.ij + op.jj * nx, o3 = o1 + o2;
     const long nq = (long)nxy * meqn;
     double* __restrict__ d = g->dst + op.dst * nq + (jc + mbc - 1) * nx + (ic + mbc - 1);
-    const double* __restrict__ src = g->src + op.src * nq + cc[0];
+    const double* __restrict__ src = g->src + op.src * nq + c0;
     if (area) {
         // manifold (fclaw2d_clawpatch46_average.f:96-115): sum(q_f a_f) / sum(a_f); the
         // area array of a patch has one ring more than q: cell (ic, jc) of q's padded
         // layout is (ic + 1, jc + 1) of a row of nx + 2
         const int na = (nx + 2) * (nxy / nx + 2);
         const double* ap = area + (size_t)op.src * na;
-        auto ai = [&](int off) { const int c = cc[0] + off; return (c / nx + 1) * (nx + 2) + c % nx + 1; };
+        auto ai = [&](int off) { const int c = c0 + off; return (c / nx + 1) * (nx + 2) + c % nx + 1; };
         const double a0 = ap[ai(0)], a1 = ap[ai(o1)], a2 = ap[ai(o2)], a3 = ap[ai(o3)];
         for (int m = 0; m < meqn; m++) {
             const double* f = src + m * nxy;
@@ -153,21 +155,24 @@ __device__ __forceinline__ bool op_index(const GatherSeg<FillOp>& s0, const Gath
     return true;
 }
 
-// The average and copy stages of one ghost update in one launch: averaging writes
-// the ghost cells a coarse patch has beside finer neighbours, copying those beside
-// same-size neighbours (disjoint cells), and both read interior cells only, which
-// neither writes.  One thread per (op, cell) with mbc * max(mx, my) threads per op
-// (a face's cells; a corner uses mbc * mbc of them); the average segments come first.
-__global__ void k_average_copy(GatherSeg<FillOp> a0, GatherSeg<FillOp> a1, GatherSeg<FillOp> c0,
-                               GatherSeg<FillOp> c1, int mx, int my, int mbc, int meqn,
-                               const double* __restrict__ area)
+// The average and copy stages of one ghost update as one index space: averaging
+// writes the ghost cells a coarse patch has beside finer neighbours, copying those
+// beside same-size neighbours (disjoint cells), and both read interior cells only,
+// which neither writes.  One index per (op, cell) with mbc * max(mx, my) indices per
+// op (a face's cells; a corner uses mbc * mbc of them); the average segments first.
+__device__ __forceinline__ long average_copy_items(const GatherSeg<FillOp>& a0, const GatherSeg<FillOp>& a1,
+                                                   const GatherSeg<FillOp>& c0, const GatherSeg<FillOp>& c1,
+                                                   int mx, int my, int mbc)
 {
-    grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
-    grid_launch_dependents();
+    return ((long)a0.n + a1.n + c0.n + c1.n) * mbc * (mx > my ? mx : my);
+}
+__device__ __forceinline__ void average_copy_at(const GatherSeg<FillOp>& a0, const GatherSeg<FillOp>& a1,
+                                                const GatherSeg<FillOp>& c0, const GatherSeg<FillOp>& c1, long t,
+                                                int mx, int my, int mbc, int meqn, const double* __restrict__ area)
+{
     const int slot = mbc * (mx > my ? mx : my);
     const int nx = mx + 2 * mbc, nxy = nx * (my + 2 * mbc);
     const long na = ((long)a0.n + a1.n) * slot;
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const GatherSeg<FillOp>* g;
     int o, k;
     if (t < na) {
@@ -175,6 +180,14 @@ __global__ void k_average_copy(GatherSeg<FillOp> a0, GatherSeg<FillOp> a1, Gathe
     } else if (op_index(c0, c1, slot, t - na, g, o, k)) {
         copy_cell(g, o, k, mx, my, mbc, meqn, nx, nxy);
     }
+}
+__global__ void k_average_copy(GatherSeg<FillOp> a0, GatherSeg<FillOp> a1, GatherSeg<FillOp> c0,
+                               GatherSeg<FillOp> c1, int mx, int my, int mbc, int meqn,
+                               const double* __restrict__ area)
+{
+    grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
+    grid_launch_dependents();
+    average_copy_at(a0, a1, c0, c1, flat_index(), mx, my, mbc, meqn, area);
 }
 
 // AMRClaw limited slopes (fclaw2d_clawpatch_utils.f:52-55, mth = 5)
@@ -188,13 +201,12 @@ __device__ __forceinline__ double compute_slopes(double sl, double sr)
     return mn * (s > 0.0 ? s : 0.0) * copysign(1.0, sc);
 }
 
-__global__ void k_interp(GatherSeg<InterpEnt> s0, GatherSeg<InterpEnt> s1, int nx, int nxy, int meqn)
+__device__ __forceinline__ void interp_at(const GatherSeg<InterpEnt>& s0, const GatherSeg<InterpEnt>& s1, long t,
+                                          int nx, int nxy, int meqn)
 {
-    grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
-    grid_launch_dependents();
     const GatherSeg<InterpEnt>* g;
     int e, m;
-    if (!gather_item(s0, s1, meqn, g, e, m)) return;
+    if (!seg_item(s0, s1, meqn, t, g, e, m)) return;
     double* __restrict__ dst = g->dst;
     const double* __restrict__ src = g->src;
     const InterpEnt c = g->e[e];
@@ -210,45 +222,64 @@ __global__ void k_interp(GatherSeg<InterpEnt> s0, GatherSeg<InterpEnt> s1, int n
     double grady = compute_slopes(sl, sr);
     dst[c.dst + m * nxy] = q0 + gradx * shx + grady * shy;
 }
-
-__global__ void k_phys(GatherSeg<PhysEnt> s0, GatherSeg<PhysEnt> s1, int nxy, int meqn,
-                       const double* __restrict__ bcstate)
+__global__ void k_interp(GatherSeg<InterpEnt> s0, GatherSeg<InterpEnt> s1, int nx, int nxy, int meqn)
 {
     grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
+    interp_at(s0, s1, flat_index(), nx, nxy, meqn);
+}
+
+__device__ __forceinline__ void phys_at(const GatherSeg<PhysEnt>& s0, const GatherSeg<PhysEnt>& s1, long t, int nxy,
+                                        int meqn, const double* __restrict__ bcstate)
+{
     const GatherSeg<PhysEnt>* g;
     int e, m;
-    if (!gather_item(s0, s1, meqn, g, e, m)) return;
+    if (!seg_item(s0, s1, meqn, t, g, e, m)) return;
     double* __restrict__ q = g->dst;                // in place: sources are cells of the same array
     const PhysEnt c = g->e[e];
     const double v = c.cst ? bcstate[m] : q[c.src + m * nxy];
     q[c.dst + m * nxy] = ((c.neg >> m) & 1) ? -v : v;
 }
-
-// Band of width mbc inside the patch, in the four loops of timeinterp.f:33-70.
-// One CTA per listed patch; a launch may cover the lists of several levels, each
-// with its own alpha (alpha.a[level]).
-__global__ void k_timeinterp(const double* __restrict__ q, const double* __restrict__ ql, double* __restrict__ qi,
-                             const int* __restrict__ patches, const PatchDesc* __restrict__ desc, int mx, int my,
-                             int mbc, int meqn, LevelAlpha la)
+__global__ void k_phys(GatherSeg<PhysEnt> s0, GatherSeg<PhysEnt> s1, int nxy, int meqn,
+                       const double* __restrict__ bcstate)
 {
     grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
-    const int p = patches[blockIdx.x];
-    const double alpha = la.a[desc[p].level & 31];
+    phys_at(s0, s1, flat_index(), nxy, meqn, bcstate);
+}
+
+// Band of width mbc inside the patch, in the four loops of timeinterp.f:33-70: one
+// index per (listed patch, cell of the padded patch); a stage may cover the lists
+// of several levels, each with its own alpha (alpha.a[level]).
+__device__ __forceinline__ void timeinterp_at(const double* __restrict__ q, const double* __restrict__ ql,
+                                              double* __restrict__ qi, const int* __restrict__ patches,
+                                              const PatchDesc* __restrict__ desc, int mx, int my, int mbc, int meqn,
+                                              const LevelAlpha& la, long t)
+{
     const int nx = mx + 2 * mbc, ny = my + 2 * mbc, nxy = nx * ny;
+    const int pi = (int)(t / nxy), c = (int)(t - (long)pi * nxy);
+    const int ic = c % nx, jc = c / nx;
+    const int i = ic - mbc + 1, j = jc - mbc + 1;         // Fortran indices
+    if (i < 1 || i > mx || j < 1 || j > my) return;
+    const bool band = (i <= mbc) || (i > mx - mbc) || (j <= mbc) || (j > my - mbc);
+    if (!band) return;
+    const int p = patches[pi];
+    const double alpha = la.a[desc[p].level & 31];
     const size_t base = (size_t)p * nxy * meqn;
-    for (int c = threadIdx.x; c < nxy; c += blockDim.x) {
-        const int ic = c % nx, jc = c / nx;
-        const int i = ic - mbc + 1, j = jc - mbc + 1;     // Fortran indices
-        if (i < 1 || i > mx || j < 1 || j > my) continue;
-        const bool band = (i <= mbc) || (i > mx - mbc) || (j <= mbc) || (j > my - mbc);
-        if (!band) continue;
-        for (int m = 0; m < meqn; m++) {
-            const size_t k = base + (size_t)m * nxy + c;
-            qi[k] = ql[k] + alpha * (q[k] - ql[k]);
-        }
+    for (int m = 0; m < meqn; m++) {
+        const size_t k = base + (size_t)m * nxy + c;
+        qi[k] = ql[k] + alpha * (q[k] - ql[k]);
     }
+}
+__global__ void k_timeinterp(const double* __restrict__ q, const double* __restrict__ ql, double* __restrict__ qi,
+                             const int* __restrict__ patches, int npatch, const PatchDesc* __restrict__ desc, int mx,
+                             int my, int mbc, int meqn, LevelAlpha la)
+{
+    grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
+    grid_launch_dependents();
+    const long t = flat_index();
+    if (t < (long)npatch * (mx + 2 * mbc) * (my + 2 * mbc))
+        timeinterp_at(q, ql, qi, patches, desc, mx, my, mbc, meqn, la, t);
 }
 
 // ---------------------------------------------------------------------------
@@ -264,9 +295,9 @@ struct RegOff {
     }
 };
 
-// The corrections of a time sync, one CTA per patch with corrections.  A face of
-// a patch is either same-size (one samesize op) or half-size (two f2c ops, igrid
-// 0 and 1, each covering half the face), so every (face, tangential index,
+// The corrections of a time sync, one CTA per patch with corrections.  A face of a
+// patch is either same-size (one samesize op) or half-size (two f2c ops,
+// igrid 0 and 1, each covering half the face), so every (face, tangential index,
 // field) has at most one correction.  The CTA files the patch's ops by face in
 // shared memory, computes every correction with one thread each (phase 1), then
 // adds them to the boundary cells with one thread per (cell, field) (phase 2):
@@ -280,46 +311,46 @@ struct RegOff {
 //   f2c:      clawpack46_fort_time_sync_f2c (same orientation, sc = 1),
 //             clawpack46_time_sync.f:254-498: the fine pair d, d+1 (d = 1 + n_off + 2 j)
 //             of coarse cell j, skipped when outside the fine face; q += deltac / area
-// Dynamic shared memory: 4 * meqn * max(mx, my) doubles and as many flag bytes.
-// 128 threads and at most 32 registers (no spills): 16 CTAs per SM, so a sync of up
-// to ~2300 patches with corrections runs in one wave.
-__global__ void __launch_bounds__(128, 16)
-k_sync(double* __restrict__ q, const double* __restrict__ regs, const PatchDesc* __restrict__ desc,
-       const SyncOp* __restrict__ ops, const int* __restrict__ op_start, int mx, int my, int mbc, int meqn, int nreg)
+// Scratch: the ops below and 4 * meqn * max(mx, my) doubles (corrections) followed
+// by as many flag bytes (sync_scratch_bytes, dynamic shared memory).
+struct SyncSmem { SyncOp op[8]; int ss[4]; int fc[4][2]; };   // op slots per face (-1: none)
+__host__ __device__ constexpr size_t sync_scratch_bytes(int mx, int my, int meqn)
 {
-    grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
-    grid_launch_dependents();
-    __shared__ SyncOp s_op[8];
-    __shared__ int s_ss[4], s_fc[4][2];                       // op slots per face (-1: none)
-    extern __shared__ double s_corr[];                        // [face][field][j]
+    return ((size_t)4 * meqn * (mx > my ? mx : my) * (sizeof(double) + 1) + 15) / 16 * 16;
+}
+__device__ void sync_group(int g, int tid, int nthr, SyncSmem& S, double* s_corr,
+                           double* __restrict__ q, const double* __restrict__ regs,
+                           const PatchDesc* __restrict__ desc, const SyncOp* __restrict__ ops,
+                           const int* __restrict__ op_start, int mx, int my, int mbc, int meqn, int nreg)
+{
     const int nmax = mx > my ? mx : my;
     unsigned char* s_has = reinterpret_cast<unsigned char*>(s_corr + 4 * meqn * nmax);
-    const int o0 = op_start[blockIdx.x], o1 = op_start[blockIdx.x + 1];
+    const int o0 = op_start[g], o1 = op_start[g + 1];
     const int nops = o1 - o0;                                  // <= 8: two ops on each of four faces
     if (nops <= 0 || nops > 8) return;
-    if (threadIdx.x < 4) { s_ss[threadIdx.x] = -1; s_fc[threadIdx.x][0] = -1; s_fc[threadIdx.x][1] = -1; }
+    if (tid < 4) { S.ss[tid] = -1; S.fc[tid][0] = -1; S.fc[tid][1] = -1; }
     __syncthreads();
-    if (threadIdx.x < nops) {
-        const SyncOp op = ops[o0 + threadIdx.x];
-        s_op[threadIdx.x] = op;
-        if (op.kind == SYNC_SAMESIZE) s_ss[op.face & 3] = threadIdx.x;
-        else s_fc[op.face & 3][op.igrid & 1] = threadIdx.x;
+    if (tid < nops) {
+        const SyncOp op = ops[o0 + tid];
+        S.op[tid] = op;
+        if (op.kind == SYNC_SAMESIZE) S.ss[op.face & 3] = tid;
+        else S.fc[op.face & 3][op.igrid & 1] = tid;
     }
     __syncthreads();
-    const int p = s_op[0].p;                                   // every op of the block corrects patch p
+    const int p = S.op[0].p;                                   // every op of the group corrects patch p
     const int nx = mx + 2 * mbc, ny = my + 2 * mbc, nxy = nx * ny;
     const double area = desc[p].dx * desc[p].dy;
     RegOff R(mx, my, meqn);
     const double* rt = regs + (size_t)p * nreg;
     // ---- phase 1: the correction of each (face, field, tangential index) ----
-    for (int t = threadIdx.x; t < 4 * meqn * nmax; t += blockDim.x) {
+    for (int t = tid; t < 4 * meqn * nmax; t += nthr) {
         const int face = t / (meqn * nmax), r = t % (meqn * nmax), m = r / nmax, j = r % nmax;
         const int nt = (face < 2) ? my : mx;
         bool has = false;
         double corr = 0.0;
         if (j < nt) {
-            if (s_ss[face] >= 0) {
-                const SyncOp& op = s_op[s_ss[face]];
+            if (S.ss[face] >= 0) {
+                const SyncOp& op = S.op[S.ss[face]];
                 const double* rn = regs + (size_t)op.n * nreg;
                 double delta;
                 if (face == 0) {
@@ -343,8 +374,8 @@ k_sync(double* __restrict__ q, const double* __restrict__ regs, const PatchDesc*
                 has = true;
             } else {
                 for (int ig = 0; ig < 2 && !has; ig++) {
-                    if (s_fc[face][ig] < 0) continue;
-                    const SyncOp& op = s_op[s_fc[face][ig]];
+                    if (S.fc[face][ig] < 0) continue;
+                    const SyncOp& op = S.op[S.fc[face][ig]];
                     const int d = 1 + op.n_off + 2 * j;        // first fine child (Fortran index)
                     if (d < 1 || d + 1 > nt) continue;         // fc46_skip_this_grid
                     const double* rn = regs + (size_t)op.n * nreg;
@@ -378,7 +409,7 @@ k_sync(double* __restrict__ q, const double* __restrict__ regs, const PatchDesc*
     __syncthreads();
     // ---- phase 2: add them to the boundary cells, samesize faces first ----
     const int ring = 2 * (mx + my) - 4;                        // interior cells on the patch boundary
-    for (int t = threadIdx.x; t < ring * meqn; t += blockDim.x) {
+    for (int t = tid; t < ring * meqn; t += nthr) {
         const int m = t / ring, k = t % ring;
         int ic, jc;                                            // storage indices of the cell
         if (k < mx) { ic = mbc + k; jc = mbc; }
@@ -391,7 +422,7 @@ k_sync(double* __restrict__ q, const double* __restrict__ regs, const PatchDesc*
         int sl[2] = {-1, -1};
         if (fx >= 0) sl[0] = (fx * meqn + m) * nmax + (jc - mbc);
         if (fy >= 0) sl[1] = (fy * meqn + m) * nmax + (ic - mbc);
-        const bool xss = fx >= 0 && s_ss[fx] >= 0, yss = fy >= 0 && s_ss[fy] >= 0;
+        const bool xss = fx >= 0 && S.ss[fx] >= 0, yss = fy >= 0 && S.ss[fy] >= 0;
         const int first = (!xss && yss) ? 1 : 0;               // a samesize y face goes before an f2c x face
         double* qq = q + (size_t)p * nxy * meqn + (size_t)m * nxy + jc * nx + ic;
         double v = 0.0;
@@ -405,83 +436,66 @@ k_sync(double* __restrict__ q, const double* __restrict__ regs, const PatchDesc*
         if (touched) *qq = v;
     }
 }
-
-__global__ void k_reset(double* __restrict__ regs, const PatchDesc* __restrict__ desc, int p0, int mx, int my,
-                        int meqn, int nreg, int coarse_level, int mode)
+// 128 threads and at most 32 registers (no spills): 16 CTAs per SM, so a sync of up
+// to ~2300 patches with corrections runs in one wave.
+__global__ void __launch_bounds__(128, 16)
+k_sync(double* __restrict__ q, const double* __restrict__ regs, const PatchDesc* __restrict__ desc,
+       const SyncOp* __restrict__ ops, const int* __restrict__ op_start, int mx, int my, int mbc, int meqn, int nreg)
 {
     grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
-    const int p = p0 + blockIdx.x;
-    const PatchDesc pd = desc[p];
-    double* r = regs + (size_t)p * nreg;
-    RegOff R(mx, my, meqn);
-    for (int k = 0; k < 4; k++) {
-        const int ft = (pd.face_type >> (2 * k)) & 3;        // 0 bnd, 1 half, 2 same, 3 double
-        bool reset;
-        if (mode == 1) reset = (ft == 1 && pd.level == coarse_level) || (ft == 3 && pd.level == coarse_level + 1);
-        else if (mode == 2) reset = (ft == 2 && pd.level == coarse_level);
-        else reset = (ft == 0);
-        if (!reset) continue;
-        if (k < 2) {
-            for (int t = threadIdx.x; t < meqn * my; t += blockDim.x) {
-                r[(k == 0 ? R.fm0 : R.fm1) + t] = 0.0;
-                r[(k == 0 ? R.fp0 : R.fp1) + t] = 0.0;
-                const int ef = (k == 0) ? R.ef0 : R.ef1;
-                r[ef + t] = 0.0;
-                r[ef + t + meqn * my] = 0.0;
-            }
-        } else {
-            for (int t = threadIdx.x; t < meqn * mx; t += blockDim.x) {
-                r[(k == 2 ? R.gm0 : R.gm1) + t] = 0.0;
-                r[(k == 2 ? R.gp0 : R.gp1) + t] = 0.0;
-                const int ef = (k == 2) ? R.ef2 : R.ef3;
-                r[ef + t] = 0.0;
-                r[ef + t + meqn * mx] = 0.0;
-            }
-        }
-    }
+    __shared__ SyncSmem S;
+    extern __shared__ double s_corr[];
+    sync_group(blockIdx.x, threadIdx.x, blockDim.x, S, s_corr, q, regs, desc, ops, op_start, mx, my, mbc, meqn, nreg);
 }
 
 // fclaw2d_time_sync's resets for levels [minlevel, maxl] (src/fclaw2d_time_sync.c:118-154):
 // same-size faces of every synced level, coarse/fine faces of each synced pair
 // (half-size faces of levels < maxl, double-size faces of levels > minlevel) and
-// physical faces.
-__global__ void k_reset_sync(double* __restrict__ regs, const PatchDesc* __restrict__ desc, int p0, int mx, int my,
-                             int meqn, int nreg, int minlevel, int maxl)
+// physical faces.  One index per (patch, face, register entry of that face).
+__device__ __forceinline__ long reset_sync_items(int np, int mx, int my, int meqn)
+{
+    return (long)np * 4 * meqn * (mx > my ? mx : my);
+}
+__device__ __forceinline__ void reset_sync_at(double* __restrict__ regs, const PatchDesc* __restrict__ desc, int p0,
+                                              int mx, int my, int meqn, int nreg, int minlevel, int maxl, long t)
+{
+    const int per = meqn * (mx > my ? mx : my);
+    const int pi = (int)(t / (4 * per)), r = (int)(t - (long)pi * 4 * per), k = r / per, u = r - k * per;
+    if (u >= meqn * (k < 2 ? my : mx)) return;
+    const int p = p0 + pi;
+    const PatchDesc& pd = desc[p];
+    const int L = pd.level;
+    const int ft = (pd.face_type >> (2 * k)) & 3;            // 0 bnd, 1 half, 2 same, 3 double
+    bool reset;
+    if (ft == 2) reset = true;
+    else if (ft == 1) reset = L < maxl;
+    else if (ft == 3) reset = L - 1 >= minlevel && L - 1 < maxl;
+    else reset = true;
+    if (!reset) return;
+    double* r0 = regs + (size_t)p * nreg;
+    RegOff R(mx, my, meqn);
+    if (k < 2) {
+        r0[(k == 0 ? R.fm0 : R.fm1) + u] = 0.0;
+        r0[(k == 0 ? R.fp0 : R.fp1) + u] = 0.0;
+        const int ef = (k == 0) ? R.ef0 : R.ef1;
+        r0[ef + u] = 0.0;
+        r0[ef + u + meqn * my] = 0.0;
+    } else {
+        r0[(k == 2 ? R.gm0 : R.gm1) + u] = 0.0;
+        r0[(k == 2 ? R.gp0 : R.gp1) + u] = 0.0;
+        const int ef = (k == 2) ? R.ef2 : R.ef3;
+        r0[ef + u] = 0.0;
+        r0[ef + u + meqn * mx] = 0.0;
+    }
+}
+__global__ void k_reset_sync(double* __restrict__ regs, const PatchDesc* __restrict__ desc, int p0, int np, int mx,
+                             int my, int meqn, int nreg, int minlevel, int maxl)
 {
     grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
-    const int p = p0 + blockIdx.x;
-    const PatchDesc pd = desc[p];
-    const int L = pd.level;
-    double* r = regs + (size_t)p * nreg;
-    RegOff R(mx, my, meqn);
-    for (int k = 0; k < 4; k++) {
-        const int ft = (pd.face_type >> (2 * k)) & 3;        // 0 bnd, 1 half, 2 same, 3 double
-        bool reset;
-        if (ft == 2) reset = true;
-        else if (ft == 1) reset = L < maxl;
-        else if (ft == 3) reset = L - 1 >= minlevel && L - 1 < maxl;
-        else reset = true;
-        if (!reset) continue;
-        if (k < 2) {
-            for (int t = threadIdx.x; t < meqn * my; t += blockDim.x) {
-                r[(k == 0 ? R.fm0 : R.fm1) + t] = 0.0;
-                r[(k == 0 ? R.fp0 : R.fp1) + t] = 0.0;
-                const int ef = (k == 0) ? R.ef0 : R.ef1;
-                r[ef + t] = 0.0;
-                r[ef + t + meqn * my] = 0.0;
-            }
-        } else {
-            for (int t = threadIdx.x; t < meqn * mx; t += blockDim.x) {
-                r[(k == 2 ? R.gm0 : R.gm1) + t] = 0.0;
-                r[(k == 2 ? R.gp0 : R.gp1) + t] = 0.0;
-                const int ef = (k == 2) ? R.ef2 : R.ef3;
-                r[ef + t] = 0.0;
-                r[ef + t + meqn * mx] = 0.0;
-            }
-        }
-    }
+    const long t = flat_index();
+    if (t < reset_sync_items(np, mx, my, meqn)) reset_sync_at(regs, desc, p0, mx, my, meqn, nreg, minlevel, maxl, t);
 }
 
 // Per-patch, per-field Kahan sums of q*dx*dy over interior cells in (j, i) order.
@@ -759,24 +773,21 @@ void launch_timeinterp(const Dims& d, const double* q, const double* qlast, doub
                        int npatch, const PatchDesc* desc, const LevelAlpha& alpha, cudaStream_t st)
 {
     if (npatch > 0)
-        launch_k(k_timeinterp, npatch, 256, 0, st, q, qlast, qinterp, patches, desc, d.mx, d.my, d.mbc, d.meqn, alpha);
+        launch_k(k_timeinterp, nblk((long)npatch * d.nxy(), 256), 256, 0, st, q, qlast, qinterp, patches, npatch, desc,
+                 d.mx, d.my, d.mbc, d.meqn, alpha);
 }
 void launch_sync(const Dims& d, double* q, const double* regs, const PatchDesc* desc, const SyncOp* ops,
                  const int* op_start, int nblocks, cudaStream_t st)
 {
     if (nblocks > 0)
-        launch_k(k_sync, nblocks, 128, (size_t)4 * d.meqn * (d.mx > d.my ? d.mx : d.my) * (sizeof(double) + 1), st,
-                 q, regs, desc, ops, op_start, d.mx, d.my, d.mbc, d.meqn, d.nreg());
-}
-void launch_reset(const Dims& d, double* regs, const PatchDesc* desc, int p0, int np, int coarse_level, int mode,
-                  cudaStream_t st)
-{
-    if (np > 0) launch_k(k_reset, np, 64, 0, st, regs, desc, p0, d.mx, d.my, d.meqn, d.nreg(), coarse_level, mode);
+        launch_k(k_sync, nblocks, 128, sync_scratch_bytes(d.mx, d.my, d.meqn), st, q, regs, desc, ops, op_start, d.mx,
+                 d.my, d.mbc, d.meqn, d.nreg());
 }
 void launch_reset_sync(const Dims& d, double* regs, const PatchDesc* desc, int p0, int np, int minlevel, int maxl,
                        cudaStream_t st)
 {
-    if (np > 0) launch_k(k_reset_sync, np, 64, 0, st, regs, desc, p0, d.mx, d.my, d.meqn, d.nreg(), minlevel, maxl);
+    const long n = (long)np * 4 * d.meqn * (d.mx > d.my ? d.mx : d.my);
+    if (np > 0) launch_k(k_reset_sync, nblk(n, 256), 256, 0, st, regs, desc, p0, np, d.mx, d.my, d.meqn, d.nreg(), minlevel, maxl);
 }
 void launch_patch_mass(const Dims& d, const double* q, const PatchDesc* desc, int np, double* out, cudaStream_t st,
                        const double* area)

@@ -111,9 +111,6 @@ struct SyncOp { int p, n, face, igrid; int n_off; int kind; int pad[2]; };
 // then f2c ops in (face, igrid) order), op_start[b]..op_start[b+1] for block b.
 void launch_sync(const Dims& d, double* q, const double* regs, const PatchDesc* desc,
                  const SyncOp* ops, const int* op_start, int nblocks, cudaStream_t st);
-// mode 1 = F2C, 2 = SAMESIZE, 3 = PHYS (fclaw2d_clawpatch_time_sync_reset)
-void launch_reset(const Dims& d, double* regs, const PatchDesc* desc, int p0, int np, int coarse_level,
-                  int mode, cudaStream_t st);
 // All register resets of one fclaw2d_time_sync(minlevel, maxl) call in one launch
 // over the patches of levels [minlevel, maxl].
 void launch_reset_sync(const Dims& d, double* regs, const PatchDesc* desc, int p0, int np, int minlevel, int maxl,
