@@ -140,7 +140,7 @@ struct TableArena {
 
 struct LevelRanges {
     int copy_off = 0, copy_n = 0, avg_off = 0, avg_n = 0, interp_off = 0, interp_n = 0, phys_off = 0, phys_n = 0;
-    int ti_off = 0, ti_n = 0, sync_start_off = 0, sync_np = 0;   // sync groups [sync_start_off, + sync_np)
+    int ti_off = 0, ti_n = 0;
 };
 
 struct fc2d_b200_solver {
@@ -204,7 +204,7 @@ struct fc2d_b200_solver {
     DevVec<double> minmax_dev;
     DevView<InterpEnt> t_interp;
     DevView<PhysEnt> t_phys;
-    DevView<int> t_ti, t_sync_start;
+    DevView<int> t_ti;
     DevView<SyncOp> t_sync;
     Tables tables;                                 // host copy of the gather tables (buffers reused)
     TableWork table_work;
@@ -416,22 +416,9 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
         filter(T.phys, T.phys_off, [&](const PhysEnt& e) { return fill[e.dst / nq] != 0; });
         filter(T.interp, T.interp_off, [&](const InterpEnt& e) { return own[e.dst / nq] == me; });
         filter(T.ti, T.ti_off, [&](int p) { return fill[p] != 0; });
-        std::vector<SyncOp> ops;
-        std::vector<int> start{0};
-        for (int l = 0; l < 33; l++) {
-            const int g0 = T.grp_off[l], g1 = T.grp_off[l + 1];
-            T.grp_off[l] = (int)start.size() - 1;
-            for (int g = g0; g < g1; g++) {
-                const int a = T.sync_start[g], b = T.sync_start[g + 1];
-                if (b > a && own[T.sync[a].p] == me) {
-                    ops.insert(ops.end(), T.sync.begin() + a, T.sync.begin() + b);
-                    start.push_back((int)ops.size());
-                }
-            }
-        }
-        T.grp_off[33] = (int)start.size() - 1;
-        T.sync.swap(ops);
-        T.sync_start.swap(start);
+        for (int i = 0; i < f.np(); i++)          // the corrections of owned patches only
+            if (own[i] != me)
+                for (int k = 0; k < SYNC_SLOTS; k++) T.sync[(size_t)i * SYNC_SLOTS + k].kind = SYNC_NONE;
         // halo slot lists (send, then receive), uploaded once per forest
         std::vector<int> slots;
         for (const auto& v : P.plan.send) slots.insert(slots.end(), v.begin(), v.end());
@@ -448,14 +435,12 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
         r.interp_off = T.interp_off[l]; r.interp_n = T.interp_off[l + 1] - T.interp_off[l];
         r.phys_off = T.phys_off[l]; r.phys_n = T.phys_off[l + 1] - T.phys_off[l];
         r.ti_off = T.ti_off[l]; r.ti_n = T.ti_off[l + 1] - T.ti_off[l];
-        r.sync_start_off = T.grp_off[l]; r.sync_np = T.grp_off[l + 1] - T.grp_off[l];
     }
     const std::vector<InterpEnt>& interp = T.interp;
     {
         TableArena& A = s->arena;
         auto sz = [](const auto& v) { return TableArena::span(v.size() * sizeof(v[0])); };
-        CK(A.reserve(sz(hd) + sz(T.copy) + sz(T.avg) + sz(T.interp) + sz(T.phys) + sz(T.ti) + sz(T.sync) +
-                     sz(T.sync_start)));
+        CK(A.reserve(sz(hd) + sz(T.copy) + sz(T.avg) + sz(T.interp) + sz(T.phys) + sz(T.ti) + sz(T.sync)));
         A.used = 0;
         const DevView<PatchDesc> dv = A.put(hd);       // staged here, then copied into the slab's descriptors
         s->t_copy = A.put(T.copy);
@@ -464,7 +449,6 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
         s->t_phys = A.put(T.phys);
         s->t_ti = A.put(T.ti);
         s->t_sync = A.put(T.sync);
-        s->t_sync_start = A.put(T.sync_start);
         if (A.used) CK(cudaMemcpyAsync(A.dev, A.host, A.used, cudaMemcpyHostToDevice, s->st));
         if (dv.n) CK(cudaMemcpyAsync(s->desc, dv.p, dv.n * sizeof(PatchDesc), cudaMemcpyDeviceToDevice, s->st));
     }
@@ -846,13 +830,11 @@ static void time_sync(fc2d_b200_solver* s, int minlevel, int maxlevel, bool defe
     const int maxl = std::min(s->o.maxlevel, 32);
     int a = std::max(minlevel, 0);
     if (a > maxl) return;
-    {   // samesize and f2c corrections, levels [a, maxl]
-        const int g0 = s->lr[a].sync_start_off, g1 = s->lr[maxl].sync_start_off + s->lr[maxl].sync_np;
-        if (g1 > g0) {
-            (void)flush_pending(s);
-            if (s->fill) s->total_launches++;
-            if (s->emit) launch_sync(s->d, s->q, s->regs, s->desc, s->t_sync.p, s->t_sync_start.p + g0, g1 - g0, s->st);
-        }
+    const int p0 = s->forest.lev_off[a], p1 = s->forest.lev_off[maxl + 1];
+    if (p1 > p0) {   // samesize and f2c corrections, levels [a, maxl]
+        (void)flush_pending(s);
+        if (s->fill) s->total_launches++;
+        if (s->emit) launch_sync(s->d, s->q, s->regs, s->desc, s->t_sync.p, p0, p1 - p0, s->st);
     }
     if (defer) {
         if (s->fill)
@@ -861,7 +843,6 @@ static void time_sync(fc2d_b200_solver* s, int minlevel, int maxlevel, bool defe
     }
     // applied now: every reset of this sync, which covers any left pending since
     for (int L = a; L <= maxl; L++) s->reg_pending[L] &= ~reset_mask(L, a, maxl);
-    const int p0 = s->forest.lev_off[a], p1 = s->forest.lev_off[maxl + 1];
     if (p1 > p0) {
         (void)flush_pending(s);
         if (s->fill) s->total_launches++;

@@ -795,13 +795,13 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out,
     });
     if (bad) { err = "a ghost-fill table writes outside its destination patches"; return false; }
 
-    out.interp.clear(); out.phys.clear(); out.ti.clear(); out.sync.clear(); out.sync_start.assign(1, 0);
+    out.interp.clear(); out.phys.clear(); out.ti.clear();
+    out.sync.assign((size_t)np * SYNC_SLOTS, SyncOp{0, 0, 0, 0, 0, SYNC_NONE, {0, 0}});
     for (int l = 0; l < 33; l++) {
         const int p0 = f.lev_off[l], p1 = f.lev_off[l + 1];
         out.interp_off[l] = (int)out.interp.size();
         out.phys_off[l] = (int)out.phys.size();
         out.ti_off[l] = (int)out.ti.size();
-        out.grp_off[l] = (int)out.sync_start.size() - 1;
         if (p0 == p1) continue;
         out.interp.insert(out.interp.end(), w.interp[l].begin(), w.interp[l].end());
         // ---- setphysical: clawpack46_bc2_default with chains resolved per patch ----
@@ -855,15 +855,15 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out,
         // correction writes, so per patch the samesize ops (faces 0..3) followed by
         // the f2c ops ((face, igrid) order) give every cell its additions in the
         // reference's order.  Levels without finer neighbours have no f2c ops, so
-        // one range of levels [a, maxlevel] covers both kinds.
+        // one range of levels [a, maxlevel] covers both kinds.  A patch has at most
+        // eight ops (one samesize or two f2c per face): slots 8 p .. 8 p + 7.
         for (int ip = p0; ip < p1; ip++) {
             const PatchInfo& P = f.p[ip];
+            SyncOp* slot = &out.sync[(size_t)ip * SYNC_SLOTS];
             int nops = 0;
             for (int fc = 0; fc < 4; fc++)
-                if (P.face_type[fc] == NB_SAME && (!f.sphere() || f.p[P.face_nbr[fc][0]].block == P.block)) {
-                    out.sync.push_back({ip, P.face_nbr[fc][0], fc, 0, 0, SYNC_SAMESIZE, {0, 0}});
-                    nops++;
-                }
+                if (P.face_type[fc] == NB_SAME && (!f.sphere() || f.p[P.face_nbr[fc][0]].block == P.block))
+                    slot[nops++] = {ip, P.face_nbr[fc][0], fc, 0, 0, SYNC_SAMESIZE, {0, 0}};
             for (int fc = 0; fc < 4; fc++) {
                 if (P.face_type[fc] != NB_HALF) continue;
                 if (f.sphere() && f.p[P.face_nbr[fc][0]].block != P.block) continue;
@@ -871,17 +871,14 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out,
                     const int fi = P.face_nbr[fc][ig];
                     const PatchInfo& F = f.p[fi];
                     const int noff = (fc < 2) ? (2 * P.gy - F.gy) * my : (2 * P.gx - F.gx) * mx;
-                    out.sync.push_back({ip, fi, fc, ig, noff, SYNC_F2C, {0, 0}});
-                    nops++;
+                    slot[nops++] = {ip, fi, fc, ig, noff, SYNC_F2C, {0, 0}};
                 }
             }
-            if (nops) out.sync_start.push_back((int)out.sync.size());
         }
     }
     out.interp_off[33] = (int)out.interp.size();
     out.phys_off[33] = (int)out.phys.size();
     out.ti_off[33] = (int)out.ti.size();
-    out.grp_off[33] = (int)out.sync_start.size() - 1;
     if (!tables_in_bounds(out, (long)np * nq)) {
         err = "a ghost-fill table indexes outside the patches (bad transform)";
         return false;

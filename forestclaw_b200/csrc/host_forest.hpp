@@ -167,11 +167,10 @@ struct Tables {
     std::vector<InterpEnt> interp;   // interpolate2ghost(level): level is the coarse level
     std::vector<PhysEnt> phys;       // setphysical(level)
     std::vector<int> ti;             // patches with fine-grid neighbours (fclaw2d_timeinterp)
-    // time-sync corrections grouped per patch: group g is sync[sync_start[g], sync_start[g + 1]),
-    // level l's groups are [grp_off[l], grp_off[l + 1])
+    // time-sync corrections of patch p: sync[SYNC_SLOTS p .. SYNC_SLOTS p + 7], in the
+    // reference's order, unused slots SYNC_NONE
     std::vector<SyncOp> sync;
-    std::vector<int> sync_start;
-    int copy_off[34], avg_off[34], interp_off[34], phys_off[34], ti_off[34], grp_off[34];
+    int copy_off[34], avg_off[34], interp_off[34], phys_off[34], ti_off[34];
 };
 
 // Buffers build_tables keeps between calls (their pages stay mapped from one regrid

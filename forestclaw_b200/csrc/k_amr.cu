@@ -33,51 +33,70 @@ static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 // consecutive entries of one field (the fields of an entry are independent).
 template <class E>
 __device__ __forceinline__ bool seg_item(const GatherSeg<E>& s0, const GatherSeg<E>& s1, int meqn, long t,
-                                         const GatherSeg<E>*& g, int& e, int& m)
+                                         GatherSeg<E>& g, int& e, int& m)
 {
     const long n0 = (long)s0.n * meqn;
-    g = &s0;
-    if (t >= n0) { t -= n0; g = &s1; }
-    if (t >= (long)g->n * meqn) return false;
-    m = (int)(t / g->n);
-    e = (int)(t - (long)m * g->n);
+    if (t < n0) {
+        g = s0;
+    } else {
+        t -= n0;
+        g = s1;
+    }
+    if (t >= (long)g.n * meqn) return false;
+    m = (int)(t / g.n);
+    e = (int)(t - (long)m * g.n);
     return true;
 }
 __device__ __forceinline__ long flat_index() { return (long)blockIdx.x * blockDim.x + threadIdx.x; }
 
+// Patch shape of the region-op index arithmetic: compile-time for the common square
+// patches with mbc 2 (the divisions by mbc and mx become shifts), run-time otherwise.
+template <int MX, int MBC>
+struct FixedShape {
+    static constexpr int mx = MX, my = MX, mbc = MBC;
+    __device__ FixedShape(int, int, int) {}
+};
+struct RunShape {
+    int mx, my, mbc;
+    __device__ RunShape(int mx_, int my_, int mbc_) : mx(mx_), my(my_), mbc(mbc_) {}
+};
+
 // Fortran cell (i, j) of the k-th ghost cell of a region op (FillOp): faces row by row
 // with i fastest, corners likewise; the cells a region covers, below.
-__device__ __forceinline__ int region_cells(int region, int mx, int my, int mbc)
+template <class S>
+__device__ __forceinline__ int region_cells(const S& P, int region)
 {
-    return region < 2 ? mbc * my : (region < 4 ? mx * mbc : mbc * mbc);
+    return region < 2 ? P.mbc * P.my : (region < 4 ? P.mx * P.mbc : P.mbc * P.mbc);
 }
-__device__ __forceinline__ void region_cell(int region, int k, int mx, int my, int mbc, int& i, int& j)
+template <class S>
+__device__ __forceinline__ void region_cell(const S& P, int region, int k, int& i, int& j)
 {
     if (region < 2) {
-        i = (region == 0 ? 1 - mbc : mx + 1) + k % mbc;
-        j = 1 + k / mbc;
+        i = (region == 0 ? 1 - P.mbc : P.mx + 1) + k % P.mbc;
+        j = 1 + k / P.mbc;
     } else if (region < 4) {
-        i = 1 + k % mx;
-        j = (region == 2 ? 1 - mbc : my + 1) + k / mx;
+        i = 1 + k % P.mx;
+        j = (region == 2 ? 1 - P.mbc : P.my + 1) + k / P.mx;
     } else {
         const int cr = region - 4;
-        i = ((cr & 1) ? mx + 1 : 1 - mbc) + k % mbc;
-        j = ((cr & 2) ? my + 1 : 1 - mbc) + k / mbc;
+        i = ((cr & 1) ? P.mx + 1 : 1 - P.mbc) + k % P.mbc;
+        j = ((cr & 2) ? P.my + 1 : 1 - P.mbc) + k / P.mbc;
     }
 }
 
 // One ghost cell of a copy op, every field: the fields are read before any is written.
-__device__ __forceinline__ void copy_cell(const GatherSeg<FillOp>* g, int o, int k, int mx, int my, int mbc,
-                                          int meqn, int nx, int nxy)
+template <class S>
+__device__ __forceinline__ void copy_cell(const S& P, const GatherSeg<FillOp>& g, int o, int k, int meqn)
 {
-    const FillOp op = g->e[o];
-    if (k >= region_cells(op.region, mx, my, mbc)) return;
+    const FillOp op = g.e[o];
+    if (k >= region_cells(P, op.region)) return;
+    const int nx = P.mx + 2 * P.mbc, nxy = nx * (P.my + 2 * P.mbc);
     int i, j;
-    region_cell(op.region, k, mx, my, mbc, i, j);
+    region_cell(P, op.region, k, i, j);
     const int i2 = op.ci + op.ii * i + op.ij * j, j2 = op.cj + op.ji * i + op.jj * j;
     const long nq = (long)nxy * meqn;
-    double* d = g->dst + op.dst * nq + (j + mbc - 1) * nx + (i + mbc - 1);
-    const double* s = g->src + op.src * nq + (j2 + mbc - 1) * nx + (i2 + mbc - 1);
+    double* d = g.dst + op.dst * nq + (j + P.mbc - 1) * nx + (i + P.mbc - 1);
+    const double* s = g.src + op.src * nq + (j2 + P.mbc - 1) * nx + (i2 + P.mbc - 1);
     for (int m0 = 0; m0 < meqn; m0 += 4) {
         double v[4];
 #pragma unroll
@@ -91,13 +110,15 @@ __device__ __forceinline__ void copy_cell(const GatherSeg<FillOp>* g, int o, int
 
 // One coarse ghost cell of an average op, every field: the mean of its four children
 // (fine cells at (0,0), (1,0), (0,1), (1,1) of the coarse cell's own axes), in that order.
-__device__ __forceinline__ void average_cell(const GatherSeg<FillOp>* g, int o, int k, int mx, int my, int mbc,
-                                             int meqn, int nx, int nxy, const double* __restrict__ area)
+template <bool AREA, class S>
+__device__ __forceinline__ void average_cell(const S& P, const GatherSeg<FillOp>& g, int o, int k, int meqn,
+                                             const double* __restrict__ area)
 {
-    const FillOp op = g->e[o];
-    if (k >= region_cells(op.region, mx, my, mbc)) return;
+    const FillOp op = g.e[o];
+    if (k >= region_cells(P, op.region)) return;
+    const int nx = P.mx + 2 * P.mbc, nxy = nx * (P.my + 2 * P.mbc);
     int ic, jc;
-    region_cell(op.region, k, mx, my, mbc, ic, jc);
+    region_cell(P, op.region, k, ic, jc);
     // children (0,0), (1,0), (0,1), (1,1) of (ic, jc) at (i0, j0), + (ii, ji), + (ij, jj)
     // and + both: the map is an isometry, so the extremes of their indices are these sums
     const int i0 = op.ci + op.ii * (2 * ic) + op.ij * (2 * jc), j0 = op.cj + op.ji * (2 * ic) + op.jj * (2 * jc);
@@ -105,18 +126,18 @@ __device__ __forceinline__ void average_cell(const GatherSeg<FillOp>* g, int o, 
         // a face keeps the coarse cells whose children are all interior fine cells
         const int ilo = i0 + min(op.ii, 0) + min(op.ij, 0), ihi = i0 + max(op.ii, 0) + max(op.ij, 0);
         const int jlo = j0 + min(op.ji, 0) + min(op.jj, 0), jhi = j0 + max(op.ji, 0) + max(op.jj, 0);
-        if (ilo < 1 || ihi > mx || jlo < 1 || jhi > my) return;
+        if (ilo < 1 || ihi > P.mx || jlo < 1 || jhi > P.my) return;
     }
-    const int c0 = (j0 + mbc - 1) * nx + (i0 + mbc - 1);   // child (0,0): plane-0 offset in the fine patch
+    const int c0 = (j0 + P.mbc - 1) * nx + (i0 + P.mbc - 1);   // child (0,0): plane-0 offset in the fine patch
     const int o1 = op.ii + op.ji * nx, o2 = op.ij + op.jj * nx, o3 = o1 + o2;
     const long nq = (long)nxy * meqn;
-    double* __restrict__ d = g->dst + op.dst * nq + (jc + mbc - 1) * nx + (ic + mbc - 1);
-    const double* __restrict__ src = g->src + op.src * nq + c0;
-    if (area) {
+    double* __restrict__ d = g.dst + op.dst * nq + (jc + P.mbc - 1) * nx + (ic + P.mbc - 1);
+    const double* __restrict__ src = g.src + op.src * nq + c0;
+    if constexpr (AREA) {
         // manifold (fclaw2d_clawpatch46_average.f:96-115): sum(q_f a_f) / sum(a_f); the
         // area array of a patch has one ring more than q: cell (ic, jc) of q's padded
         // layout is (ic + 1, jc + 1) of a row of nx + 2
-        const int na = (nx + 2) * (nxy / nx + 2);
+        const int na = (nx + 2) * (P.my + 2 * P.mbc + 2);
         const double* ap = area + (size_t)op.src * na;
         auto ai = [&](int off) { const int c = c0 + off; return (c / nx + 1) * (nx + 2) + c % nx + 1; };
         const double a0 = ap[ai(0)], a1 = ap[ai(o1)], a2 = ap[ai(o2)], a3 = ap[ai(o3)];
@@ -142,52 +163,48 @@ __device__ __forceinline__ void average_cell(const GatherSeg<FillOp>* g, int o, 
     }
 }
 
-// thread t of two op segments of `slot` threads per op: segment, op, cell
+// thread t of two op segments of `slot` threads per op: segment (by value: the
+// parameters stay in the constant bank), op, cell
 __device__ __forceinline__ bool op_index(const GatherSeg<FillOp>& s0, const GatherSeg<FillOp>& s1, int slot, long t,
-                                         const GatherSeg<FillOp>*& g, int& o, int& k)
+                                         GatherSeg<FillOp>& g, int& o, int& k)
 {
     const long n0 = (long)s0.n * slot;
-    g = &s0;
-    if (t >= n0) { t -= n0; g = &s1; }
-    if (t >= (long)g->n * slot) return false;
+    const bool second = t >= n0;
+    if (second) t -= n0;
+    g.dst = second ? s1.dst : s0.dst;
+    g.src = second ? s1.src : s0.src;
+    g.e = second ? s1.e : s0.e;
+    g.n = second ? s1.n : s0.n;
+    if (t >= (long)g.n * slot) return false;
     o = (int)(t / slot);
     k = (int)(t - (long)o * slot);
     return true;
 }
 
-// The average and copy stages of one ghost update as one index space: averaging
-// writes the ghost cells a coarse patch has beside finer neighbours, copying those
-// beside same-size neighbours (disjoint cells), and both read interior cells only,
-// which neither writes.  One index per (op, cell) with mbc * max(mx, my) indices per
-// op (a face's cells; a corner uses mbc * mbc of them); the average segments first.
-__device__ __forceinline__ long average_copy_items(const GatherSeg<FillOp>& a0, const GatherSeg<FillOp>& a1,
-                                                   const GatherSeg<FillOp>& c0, const GatherSeg<FillOp>& c1,
-                                                   int mx, int my, int mbc)
-{
-    return ((long)a0.n + a1.n + c0.n + c1.n) * mbc * (mx > my ? mx : my);
-}
-__device__ __forceinline__ void average_copy_at(const GatherSeg<FillOp>& a0, const GatherSeg<FillOp>& a1,
-                                                const GatherSeg<FillOp>& c0, const GatherSeg<FillOp>& c1, long t,
-                                                int mx, int my, int mbc, int meqn, const double* __restrict__ area)
-{
-    const int slot = mbc * (mx > my ? mx : my);
-    const int nx = mx + 2 * mbc, nxy = nx * (my + 2 * mbc);
-    const long na = ((long)a0.n + a1.n) * slot;
-    const GatherSeg<FillOp>* g;
-    int o, k;
-    if (t < na) {
-        if (op_index(a0, a1, slot, t, g, o, k)) average_cell(g, o, k, mx, my, mbc, meqn, nx, nxy, area);
-    } else if (op_index(c0, c1, slot, t - na, g, o, k)) {
-        copy_cell(g, o, k, mx, my, mbc, meqn, nx, nxy);
-    }
-}
-__global__ void k_average_copy(GatherSeg<FillOp> a0, GatherSeg<FillOp> a1, GatherSeg<FillOp> c0,
-                               GatherSeg<FillOp> c1, int mx, int my, int mbc, int meqn,
-                               const double* __restrict__ area)
+// The average and copy stages of one ghost update in one launch: averaging writes
+// the ghost cells a coarse patch has beside finer neighbours, copying those beside
+// same-size neighbours (disjoint cells), and both read interior cells only, which
+// neither writes.  One thread per (op, cell) with mbc * max(mx, my) threads per op
+// (a face's cells; a corner uses mbc * mbc of them); the average segments first.
+// AREA: the area-weighted average of a manifold (cell areas in `area`).
+template <class S, bool AREA>
+__global__ void __launch_bounds__(256, AREA ? 4 : 8)
+k_average_copy(GatherSeg<FillOp> a0, GatherSeg<FillOp> a1, GatherSeg<FillOp> c0, GatherSeg<FillOp> c1, int mx,
+               int my, int mbc, int meqn, const double* __restrict__ area)
 {
     grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
-    average_copy_at(a0, a1, c0, c1, flat_index(), mx, my, mbc, meqn, area);
+    const S P(mx, my, mbc);
+    const int slot = P.mbc * (P.mx > P.my ? P.mx : P.my);
+    const long t = flat_index();
+    const long na = ((long)a0.n + a1.n) * slot;
+    GatherSeg<FillOp> g;
+    int o, k;
+    if (t < na) {
+        if (op_index(a0, a1, slot, t, g, o, k)) average_cell<AREA>(P, g, o, k, meqn, area);
+    } else if (op_index(c0, c1, slot, t - na, g, o, k)) {
+        copy_cell(P, g, o, k, meqn);
+    }
 }
 
 // AMRClaw limited slopes (fclaw2d_clawpatch_utils.f:52-55, mth = 5)
@@ -204,12 +221,12 @@ __device__ __forceinline__ double compute_slopes(double sl, double sr)
 __device__ __forceinline__ void interp_at(const GatherSeg<InterpEnt>& s0, const GatherSeg<InterpEnt>& s1, long t,
                                           int nx, int nxy, int meqn)
 {
-    const GatherSeg<InterpEnt>* g;
+    GatherSeg<InterpEnt> g;
     int e, m;
     if (!seg_item(s0, s1, meqn, t, g, e, m)) return;
-    double* __restrict__ dst = g->dst;
-    const double* __restrict__ src = g->src;
-    const InterpEnt c = g->e[e];
+    double* __restrict__ dst = g.dst;
+    const double* __restrict__ src = g.src;
+    const InterpEnt c = g.e[e];
     const double shx = (c.sub & 1) ? 0.25 : -0.25;
     const double shy = (c.sub & 2) ? 0.25 : -0.25;
     const double* qc = src + c.src + m * nxy;
@@ -232,11 +249,11 @@ __global__ void k_interp(GatherSeg<InterpEnt> s0, GatherSeg<InterpEnt> s1, int n
 __device__ __forceinline__ void phys_at(const GatherSeg<PhysEnt>& s0, const GatherSeg<PhysEnt>& s1, long t, int nxy,
                                         int meqn, const double* __restrict__ bcstate)
 {
-    const GatherSeg<PhysEnt>* g;
+    GatherSeg<PhysEnt> g;
     int e, m;
     if (!seg_item(s0, s1, meqn, t, g, e, m)) return;
-    double* __restrict__ q = g->dst;                // in place: sources are cells of the same array
-    const PhysEnt c = g->e[e];
+    double* __restrict__ q = g.dst;                 // in place: sources are cells of the same array
+    const PhysEnt c = g.e[e];
     const double v = c.cst ? bcstate[m] : q[c.src + m * nxy];
     q[c.dst + m * nxy] = ((c.neg >> m) & 1) ? -v : v;
 }
@@ -295,7 +312,7 @@ struct RegOff {
     }
 };
 
-// The corrections of a time sync, one CTA per patch with corrections.  A face of a
+// The corrections of a time sync, one CTA per patch of the synced levels.  A face of a
 // patch is either same-size (one samesize op) or half-size (two f2c ops,
 // igrid 0 and 1, each covering half the face), so every (face, tangential index,
 // field) has at most one correction.  The CTA files the patch's ops by face in
@@ -312,43 +329,111 @@ struct RegOff {
 //             clawpack46_time_sync.f:254-498: the fine pair d, d+1 (d = 1 + n_off + 2 j)
 //             of coarse cell j, skipped when outside the fine face; q += deltac / area
 // Scratch: the ops below and 4 * meqn * max(mx, my) doubles (corrections) followed
-// by as many flag bytes (sync_scratch_bytes, dynamic shared memory).
+// by as many flag bytes (sync_scratch_bytes), then the prefetched registers and cells
+// (sync_prefetch_bytes), in dynamic shared memory.
 struct SyncSmem { SyncOp op[8]; int ss[4]; int fc[4][2]; };   // op slots per face (-1: none)
 __host__ __device__ constexpr size_t sync_scratch_bytes(int mx, int my, int meqn)
 {
     return ((size_t)4 * meqn * (mx > my ? mx : my) * (sizeof(double) + 1) + 15) / 16 * 16;
 }
-__device__ void sync_group(int g, int tid, int nthr, SyncSmem& S, double* s_corr,
-                           double* __restrict__ q, const double* __restrict__ regs,
-                           const PatchDesc* __restrict__ desc, const SyncOp* __restrict__ ops,
-                           const int* __restrict__ op_start, int mx, int my, int mbc, int meqn, int nreg)
+__host__ __device__ constexpr size_t sync_prefetch_bytes(int mx, int my, int meqn)
 {
+    return ((size_t)2 * 4 * meqn * (mx > my ? mx : my) + (size_t)(2 * (mx + my) - 4) * meqn) * sizeof(double);
+}
+// 8-byte asynchronous copy global -> shared (cp.async, sm_80+), and the wait for this
+// thread's copies
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// Patch shape and field count of the time sync: compile-time for the common shapes
+// (the index arithmetic and register offsets fold), run-time otherwise.
+template <int MX, int MEQN>
+struct FixedSync {
+    static constexpr int mx = MX, my = MX, mbc = 2, meqn = MEQN;
+    __device__ FixedSync(int, int, int, int) {}
+};
+struct RunSync {
+    int mx, my, mbc, meqn;
+    __device__ RunSync(int mx_, int my_, int mbc_, int meqn_) : mx(mx_), my(my_), mbc(mbc_), meqn(meqn_) {}
+};
+template <class PS>
+__device__ void sync_group(const PS& P, int p, int tid, int nthr, SyncSmem& S, double* s_corr,
+                           double* __restrict__ q, const double* __restrict__ regs,
+                           const PatchDesc* __restrict__ desc, const SyncOp* __restrict__ ops, int nreg)
+{
+    const int mx = P.mx, my = P.my, mbc = P.mbc, meqn = P.meqn;
     const int nmax = mx > my ? mx : my;
     unsigned char* s_has = reinterpret_cast<unsigned char*>(s_corr + 4 * meqn * nmax);
-    const int o0 = op_start[g], o1 = op_start[g + 1];
-    const int nops = o1 - o0;                                  // <= 8: two ops on each of four faces
-    if (nops <= 0 || nops > 8) return;
-    if (tid < 4) { S.ss[tid] = -1; S.fc[tid][0] = -1; S.fc[tid][1] = -1; }
-    __syncthreads();
-    if (tid < nops) {
-        const SyncOp op = ops[o0 + tid];
-        S.op[tid] = op;
-        if (op.kind == SYNC_SAMESIZE) S.ss[op.face & 3] = tid;
-        else S.fc[op.face & 3][op.igrid & 1] = tid;
-    }
-    __syncthreads();
-    const int p = S.op[0].p;                                   // every op of the group corrects patch p
     const int nx = mx + 2 * mbc, ny = my + 2 * mbc, nxy = nx * ny;
-    const double area = desc[p].dx * desc[p].dy;
+    const int n1 = 4 * meqn * nmax;                            // phase-1 items: (face, field, index)
+    const int ring = 2 * (mx + my) - 4;                        // interior cells on the patch boundary
+    const int n2 = ring * meqn;                                // phase-2 items: (cell, field)
     RegOff R(mx, my, meqn);
     const double* rt = regs + (size_t)p * nreg;
+    // phase-1 item t: face, field, index, its length, and this patch's two registers the
+    // correction reads (A: edge flux, B: fluctuation sum) at the face's side
+    auto item1 = [&](int t, int& face, int& m, int& j, int& nt, int& ra, int& rb) {
+        face = t / (meqn * nmax);
+        const int r = t % (meqn * nmax);
+        m = r / nmax;
+        j = r % nmax;
+        nt = (face < 2) ? my : mx;
+        const int o = j + m * nt;
+        ra = (face == 0 ? R.ef0 : face == 1 ? R.ef1 : face == 2 ? R.ef2 : R.ef3) + o;
+        rb = (face == 0 ? R.fp0 : face == 1 ? R.fm1 : face == 2 ? R.gp0 : R.gm1) + o;
+    };
+    // phase-2 item t: the cell's offset in q (field m plane) and its x and y faces
+    auto item2 = [&](int t, int& m, int& ic, int& jc) {
+        m = t / ring;
+        const int k = t % ring;
+        if (k < mx) { ic = mbc + k; jc = mbc; }
+        else if (k < 2 * mx) { ic = mbc + k - mx; jc = my + mbc - 1; }
+        else if (k < 2 * mx + my - 2) { ic = mbc; jc = mbc + 1 + (k - 2 * mx); }
+        else { ic = mx + mbc - 1; jc = mbc + 1 + (k - 2 * mx - (my - 2)); }
+    };
+    double* qp = q + (size_t)p * nxy * meqn;
+    // this patch's registers of every phase-1 item and boundary cells of every phase-2
+    // item, copied into shared memory (asynchronously, no registers held) while the
+    // ops arrive: neither depends on them.  Each thread reads back only its own items.
+    double* pre_r = s_corr + sync_scratch_bytes(mx, my, meqn) / sizeof(double);   // [n1][2]
+    double* pre_q = pre_r + 2 * n1;                                                // [n2]
+    for (int t = tid; t < n1; t += nthr) {
+        int face, m, j, nt, ra, rb;
+        item1(t, face, m, j, nt, ra, rb);
+        if (j < nt) { cp_async8(pre_r + 2 * t, rt + ra); cp_async8(pre_r + 2 * t + 1, rt + rb); }
+    }
+    for (int t = tid; t < n2; t += nthr) {
+        int m, ic, jc;
+        item2(t, m, ic, jc);
+        cp_async8(pre_q + t, qp + (size_t)m * nxy + jc * nx + ic);
+    }
+    const double area = desc[p].dx * desc[p].dy;
+    if (tid < 4) { S.ss[tid] = -1; S.fc[tid][0] = -1; S.fc[tid][1] = -1; }
+    if (tid < SYNC_SLOTS) S.op[tid] = ops[(size_t)p * SYNC_SLOTS + tid];
+    __syncthreads();
+    if (S.op[0].kind == SYNC_NONE) {                           // no corrections for this patch
+        cp_async_wait_all();
+        return;
+    }
+    if (tid < SYNC_SLOTS) {
+        const SyncOp& op = S.op[tid];
+        if (op.kind == SYNC_SAMESIZE) S.ss[op.face & 3] = tid;
+        else if (op.kind == SYNC_F2C) S.fc[op.face & 3][op.igrid & 1] = tid;
+    }
+    __syncthreads();
+    cp_async_wait_all();
     // ---- phase 1: the correction of each (face, field, tangential index) ----
-    for (int t = tid; t < 4 * meqn * nmax; t += nthr) {
-        const int face = t / (meqn * nmax), r = t % (meqn * nmax), m = r / nmax, j = r % nmax;
-        const int nt = (face < 2) ? my : mx;
+    for (int t = tid; t < n1; t += nthr) {
+        int face, m, j, nt, ra, rb;
+        item1(t, face, m, j, nt, ra, rb);
         bool has = false;
         double corr = 0.0;
         if (j < nt) {
+            const double rA = pre_r[2 * t], rB = pre_r[2 * t + 1];
             if (S.ss[face] >= 0) {
                 const SyncOp& op = S.op[S.ss[face]];
                 const double* rn = regs + (size_t)op.n * nreg;
@@ -356,19 +441,19 @@ __device__ void sync_group(int g, int tid, int nthr, SyncSmem& S, double* s_corr
                 if (face == 0) {
                     double fp = rn[R.fp1 + j + m * my];
                     double ef = 1 * rn[R.ef1 + j + m * my + my * meqn];
-                    delta = (ef - rt[R.ef0 + j + m * my]) - (fp - rt[R.fp0 + j + m * my]);
+                    delta = (ef - rA) - (fp - rB);
                 } else if (face == 1) {
                     double fm = rn[R.fm0 + j + m * my];
                     double ef = 1 * rn[R.ef0 + j + m * my + my * meqn];
-                    delta = (rt[R.ef1 + j + m * my] - ef) - (fm - rt[R.fm1 + j + m * my]);
+                    delta = (rA - ef) - (fm - rB);
                 } else if (face == 2) {
                     double gp = rn[R.gp1 + j + m * mx];
                     double ef = 1 * rn[R.ef3 + j + m * mx + mx * meqn];
-                    delta = (ef - rt[R.ef2 + j + m * mx]) - (gp - rt[R.gp0 + j + m * mx]);
+                    delta = (ef - rA) - (gp - rB);
                 } else {
                     double gm = rn[R.gm0 + j + m * mx];
                     double ef = 1 * rn[R.ef2 + j + m * mx + mx * meqn];
-                    delta = (rt[R.ef3 + j + m * mx] - ef) - (gm - rt[R.gm1 + j + m * mx]);
+                    delta = (rA - ef) - (gm - rB);
                 }
                 corr = 0.5 * delta / area;
                 has = true;
@@ -384,19 +469,19 @@ __device__ void sync_group(int g, int tid, int nthr, SyncSmem& S, double* s_corr
                     if (face == 0) {
                         double fp = rn[R.fp1 + f0 + m * my] + rn[R.fp1 + f1 + m * my];
                         double ef = 1 * (rn[R.ef1 + f0 + m * my + my * meqn] + rn[R.ef1 + f1 + m * my + my * meqn]);
-                        deltac = (ef - rt[R.ef0 + j + m * my]) - (fp - rt[R.fp0 + j + m * my]);
+                        deltac = (ef - rA) - (fp - rB);
                     } else if (face == 1) {
                         double fm = rn[R.fm0 + f0 + m * my] + rn[R.fm0 + f1 + m * my];
                         double ef = 1 * (rn[R.ef0 + f0 + m * my + my * meqn] + rn[R.ef0 + f1 + m * my + my * meqn]);
-                        deltac = (rt[R.ef1 + j + m * my] - ef) - (fm - rt[R.fm1 + j + m * my]);
+                        deltac = (rA - ef) - (fm - rB);
                     } else if (face == 2) {
                         double gp = rn[R.gp1 + f0 + m * mx] + rn[R.gp1 + f1 + m * mx];
                         double ef = 1 * (rn[R.ef3 + f0 + m * mx + mx * meqn] + rn[R.ef3 + f1 + m * mx + mx * meqn]);
-                        deltac = (ef - rt[R.ef2 + j + m * mx]) - (gp - rt[R.gp0 + j + m * mx]);
+                        deltac = (ef - rA) - (gp - rB);
                     } else {
                         double gm = rn[R.gm0 + f0 + m * mx] + rn[R.gm0 + f1 + m * mx];
                         double ef = 1 * (rn[R.ef2 + f0 + m * mx + mx * meqn] + rn[R.ef2 + f1 + m * mx + mx * meqn]);
-                        deltac = (rt[R.ef3 + j + m * mx] - ef) - (gm - rt[R.gm1 + j + m * mx]);
+                        deltac = (rA - ef) - (gm - rB);
                     }
                     corr = deltac / area;
                     has = true;
@@ -408,14 +493,9 @@ __device__ void sync_group(int g, int tid, int nthr, SyncSmem& S, double* s_corr
     }
     __syncthreads();
     // ---- phase 2: add them to the boundary cells, samesize faces first ----
-    const int ring = 2 * (mx + my) - 4;                        // interior cells on the patch boundary
-    for (int t = tid; t < ring * meqn; t += nthr) {
-        const int m = t / ring, k = t % ring;
-        int ic, jc;                                            // storage indices of the cell
-        if (k < mx) { ic = mbc + k; jc = mbc; }
-        else if (k < 2 * mx) { ic = mbc + k - mx; jc = my + mbc - 1; }
-        else if (k < 2 * mx + my - 2) { ic = mbc; jc = mbc + 1 + (k - 2 * mx); }
-        else { ic = mx + mbc - 1; jc = mbc + 1 + (k - 2 * mx - (my - 2)); }
+    for (int t = tid; t < n2; t += nthr) {
+        int m, ic, jc;                                         // storage indices of the cell
+        item2(t, m, ic, jc);
         const int fx = (ic == mbc) ? 0 : (ic == mx + mbc - 1) ? 1 : -1;
         const int fy = (jc == mbc) ? 2 : (jc == my + mbc - 1) ? 3 : -1;
         // slots of the cell's corrections on its x and y faces, in the reference's order
@@ -424,29 +504,30 @@ __device__ void sync_group(int g, int tid, int nthr, SyncSmem& S, double* s_corr
         if (fy >= 0) sl[1] = (fy * meqn + m) * nmax + (ic - mbc);
         const bool xss = fx >= 0 && S.ss[fx] >= 0, yss = fy >= 0 && S.ss[fy] >= 0;
         const int first = (!xss && yss) ? 1 : 0;               // a samesize y face goes before an f2c x face
-        double* qq = q + (size_t)p * nxy * meqn + (size_t)m * nxy + jc * nx + ic;
+        double* qq = qp + (size_t)m * nxy + jc * nx + ic;
         double v = 0.0;
         bool touched = false;
-        for (int u = 0; u < 2; u++) {
-            const int s = sl[u ^ first];
+        for (int w = 0; w < 2; w++) {
+            const int s = sl[w ^ first];
             if (s < 0 || !s_has[s]) continue;
-            if (!touched) { v = *qq; touched = true; }
+            if (!touched) { v = pre_q[t]; touched = true; }
             v = v + s_corr[s];
         }
         if (touched) *qq = v;
     }
 }
-// 128 threads and at most 32 registers (no spills): 16 CTAs per SM, so a sync of up
-// to ~2300 patches with corrections runs in one wave.
+// One CTA per patch of the synced levels: 128 threads and at most 32 registers, 16
+// CTAs per SM, so a sync of up to ~2300 patches runs in one wave.
+template <class PS>
 __global__ void __launch_bounds__(128, 16)
 k_sync(double* __restrict__ q, const double* __restrict__ regs, const PatchDesc* __restrict__ desc,
-       const SyncOp* __restrict__ ops, const int* __restrict__ op_start, int mx, int my, int mbc, int meqn, int nreg)
+       const SyncOp* __restrict__ ops, int p0, int mx, int my, int mbc, int meqn, int nreg)
 {
     grid_dependency_wait();       // programmatic launch: the previous grid's writes are visible
     grid_launch_dependents();
     __shared__ SyncSmem S;
     extern __shared__ double s_corr[];
-    sync_group(blockIdx.x, threadIdx.x, blockDim.x, S, s_corr, q, regs, desc, ops, op_start, mx, my, mbc, meqn, nreg);
+    sync_group(PS(mx, my, mbc, meqn), p0 + blockIdx.x, threadIdx.x, blockDim.x, S, s_corr, q, regs, desc, ops, nreg);
 }
 
 // fclaw2d_time_sync's resets for levels [minlevel, maxl] (src/fclaw2d_time_sync.c:118-154):
@@ -756,7 +837,14 @@ void launch_average_copy(const Dims& d, const GatherSeg<FillOp>& a0, const Gathe
                          cudaStream_t st)
 {
     const long n = ((long)a0.n + a1.n + c0.n + c1.n) * d.mbc * (d.mx > d.my ? d.mx : d.my);
-    if (n > 0) launch_k(k_average_copy, nblk(n, 256), 256, 0, st, a0, a1, c0, c1, d.mx, d.my, d.mbc, d.meqn, area);
+    if (n <= 0) return;
+    auto kern = area ? &k_average_copy<RunShape, true> : &k_average_copy<RunShape, false>;
+    if (!area && d.mx == d.my && d.mbc == 2) {
+        if (d.mx == 8) kern = &k_average_copy<FixedShape<8, 2>, false>;
+        else if (d.mx == 16) kern = &k_average_copy<FixedShape<16, 2>, false>;
+        else if (d.mx == 32) kern = &k_average_copy<FixedShape<32, 2>, false>;
+    }
+    launch_k(kern, nblk(n, 256), 256, 0, st, a0, a1, c0, c1, d.mx, d.my, d.mbc, d.meqn, area);
 }
 void launch_interp(const Dims& d, const GatherSeg<InterpEnt>& s0, const GatherSeg<InterpEnt>& s1, cudaStream_t st)
 {
@@ -776,18 +864,26 @@ void launch_timeinterp(const Dims& d, const double* q, const double* qlast, doub
         launch_k(k_timeinterp, nblk((long)npatch * d.nxy(), 256), 256, 0, st, q, qlast, qinterp, patches, npatch, desc,
                  d.mx, d.my, d.mbc, d.meqn, alpha);
 }
-void launch_sync(const Dims& d, double* q, const double* regs, const PatchDesc* desc, const SyncOp* ops,
-                 const int* op_start, int nblocks, cudaStream_t st)
+void launch_sync(const Dims& d, double* q, const double* regs, const PatchDesc* desc, const SyncOp* ops, int p0,
+                 int np, cudaStream_t st)
 {
-    if (nblocks > 0)
-        launch_k(k_sync, nblocks, 128, sync_scratch_bytes(d.mx, d.my, d.meqn), st, q, regs, desc, ops, op_start, d.mx,
-                 d.my, d.mbc, d.meqn, d.nreg());
+    if (np <= 0) return;
+    auto kern = &k_sync<RunSync>;
+    if (d.mx == d.my && d.mbc == 2) {
+        if (d.mx == 16 && d.meqn == 3) kern = &k_sync<FixedSync<16, 3>>;
+        else if (d.mx == 16 && d.meqn == 4) kern = &k_sync<FixedSync<16, 4>>;
+        else if (d.mx == 8 && d.meqn == 3) kern = &k_sync<FixedSync<8, 3>>;
+    }
+    launch_k(kern, np, 128, sync_scratch_bytes(d.mx, d.my, d.meqn) + sync_prefetch_bytes(d.mx, d.my, d.meqn), st, q,
+             regs, desc, ops, p0, d.mx, d.my, d.mbc, d.meqn, d.nreg());
 }
 void launch_reset_sync(const Dims& d, double* regs, const PatchDesc* desc, int p0, int np, int minlevel, int maxl,
                        cudaStream_t st)
 {
     const long n = (long)np * 4 * d.meqn * (d.mx > d.my ? d.mx : d.my);
-    if (np > 0) launch_k(k_reset_sync, nblk(n, 256), 256, 0, st, regs, desc, p0, np, d.mx, d.my, d.meqn, d.nreg(), minlevel, maxl);
+    if (np > 0)
+        launch_k(k_reset_sync, nblk(n, 256), 256, 0, st, regs, desc, p0, np, d.mx, d.my, d.meqn, d.nreg(), minlevel,
+                 maxl);
 }
 void launch_patch_mass(const Dims& d, const double* q, const PatchDesc* desc, int np, double* out, cudaStream_t st,
                        const double* area)

@@ -105,12 +105,14 @@ void launch_timeinterp(const Dims& d, const double* q, const double* qlast, doub
 // One time-sync correction of patch p from neighbour n across face `face`:
 // kind SYNC_SAMESIZE (clawpack46_fort_time_sync_samesize) or SYNC_F2C (coarse p,
 // fine n = child igrid of the face, n_off = first fine index offset along it).
-enum { SYNC_SAMESIZE = 0, SYNC_F2C = 1 };
+enum { SYNC_SAMESIZE = 0, SYNC_F2C = 1, SYNC_NONE = -1 };
 struct SyncOp { int p, n, face, igrid; int n_off; int kind; int pad[2]; };
-// The corrections of a time sync: ops grouped per patch (samesize faces 0..3,
-// then f2c ops in (face, igrid) order), op_start[b]..op_start[b+1] for block b.
-void launch_sync(const Dims& d, double* q, const double* regs, const PatchDesc* desc,
-                 const SyncOp* ops, const int* op_start, int nblocks, cudaStream_t st);
+constexpr int SYNC_SLOTS = 8;      // ops of a patch: at most one samesize or two f2c per face
+// The corrections of a time sync over patches p0 .. p0 + np - 1: the ops of patch p are
+// ops[SYNC_SLOTS p ..] (samesize faces 0..3, then f2c ops in (face, igrid) order; the
+// rest SYNC_NONE).
+void launch_sync(const Dims& d, double* q, const double* regs, const PatchDesc* desc, const SyncOp* ops, int p0,
+                 int np, cudaStream_t st);
 // All register resets of one fclaw2d_time_sync(minlevel, maxl) call in one launch
 // over the patches of levels [minlevel, maxl].
 void launch_reset_sync(const Dims& d, double* regs, const PatchDesc* desc, int p0, int np, int minlevel, int maxl,
