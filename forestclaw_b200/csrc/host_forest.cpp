@@ -580,29 +580,6 @@ struct TableCtx {
     }
 };
 
-// Keeps the last entry written to each destination, in first-write order.  The
-// destination cell (patch p >= p0, plane-0 offset within p) indexes a dense map
-// over the patches from p0 on; the touched cells are cleared again on destruction.
-template <class E>
-struct LastWriter {
-    std::vector<E>& v;
-    std::vector<int>& at;
-    int nq, nxy, p0;
-    std::vector<int> touched;
-    bool outside = false;                  // a destination outside the map (not a finer neighbour)
-    LastWriter(std::vector<E>& out, std::vector<int>& slots, int nq_, int nxy_, int p0_)
-        : v(out), at(slots), nq(nq_), nxy(nxy_), p0(p0_) {}
-    ~LastWriter() { for (int k : touched) at[k] = -1; }
-    void put(const E& e, int p)
-    {
-        const long k = (long)(p - p0) * nxy + (e.dst - (long)p * nq);
-        if (k < 0 || k >= (long)at.size()) { outside = true; return; }
-        int& a = at[k];
-        if (a < 0) { a = (int)v.size(); touched.push_back((int)k); v.push_back(e); }
-        else v[a] = e;
-    }
-};
-
 // Runs tasks 0..n-1 on up to nt threads (the calling one included).
 template <class Fn>
 void run_tasks(int n, int nt, Fn fn)
@@ -639,7 +616,7 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out,
     nt = std::max(1, std::min(nt, std::min(16, np / 64)));
     int nlev = 0;
     for (int l = 0; l < 33; l++) if (f.lev_off[l + 1] > f.lev_off[l]) nlev = l + 1;
-    w.interp.resize(33); w.slots.resize(33);
+    w.copy.resize(33); w.avg.resize(33);
     std::atomic<int> bad{0};
 
     // ---- copy2ghost (faces, then corners, of each patch: fclaw2d_clawpatch46_copy.f) and
@@ -688,122 +665,181 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out,
                 }
         return true;
     };
-    auto regions = [&]() {
-        out.copy.clear(); out.avg.clear();
+    // the ops of level l's patches (one task per level)
+    auto regions = [&](int l) {
+        std::vector<FillOp>& vc = w.copy[l];
+        std::vector<FillOp>& va = w.avg[l];
+        vc.clear(); va.clear();
         bool good = true;
-        for (int l = 0; l < 33; l++) {
-            out.copy_off[l] = (int)out.copy.size();
-            out.avg_off[l] = (int)out.avg.size();
-            for (int ip = f.lev_off[l]; ip < f.lev_off[l + 1]; ip++) {
-                const PatchInfo& P = f.p[ip];
-                for (int fc = 0; fc < 4; fc++) {
-                    if (P.face_type[fc] != NB_SAME) continue;
-                    const int n = P.face_nbr[fc][0];
-                    const TableCtx::Aff A = T.same_map(P, f.p[n]);
-                    good = good && copy_ok(fc, A);
-                    out.copy.push_back(op(ip, n, fc, A));
-                }
-                for (int cr = 0; cr < 4; cr++) {
-                    if (!P.has_corner[cr] || P.corner_type[cr] != NB_SAME) continue;
-                    const int n = P.corner_nbr[cr];
-                    const TableCtx::Aff A = T.same_map(P, f.p[n]);
-                    good = good && copy_ok(4 + cr, A);
-                    out.copy.push_back(op(ip, n, 4 + cr, A));
-                }
-                if (!P.on_cf) continue;
-                for (int fc = 0; fc < 4; fc++) {
-                    if (P.face_type[fc] != NB_HALF) continue;
-                    for (int ig = 0; ig < 2; ig++) {
-                        const int fi = P.face_nbr[fc][ig];
-                        out.avg.push_back(op(ip, fi, fc, T.child_map(P, f.p[fi])));
-                    }
-                }
-                for (int cr = 0; cr < 4; cr++) {
-                    if (!P.has_corner[cr] || P.corner_type[cr] != NB_HALF) continue;
-                    const int fi = P.corner_nbr[cr];
-                    const TableCtx::Aff F = T.child_map(P, f.p[fi]);
-                    good = good && avg_corner_ok(4 + cr, F);
-                    out.avg.push_back(op(ip, fi, 4 + cr, F));
+        for (int ip = f.lev_off[l]; ip < f.lev_off[l + 1]; ip++) {
+            const PatchInfo& P = f.p[ip];
+            for (int fc = 0; fc < 4; fc++) {
+                if (P.face_type[fc] != NB_SAME) continue;
+                const int n = P.face_nbr[fc][0];
+                const TableCtx::Aff A = T.same_map(P, f.p[n]);
+                good = good && copy_ok(fc, A);
+                vc.push_back(op(ip, n, fc, A));
+            }
+            for (int cr = 0; cr < 4; cr++) {
+                if (!P.has_corner[cr] || P.corner_type[cr] != NB_SAME) continue;
+                const int n = P.corner_nbr[cr];
+                const TableCtx::Aff A = T.same_map(P, f.p[n]);
+                good = good && copy_ok(4 + cr, A);
+                vc.push_back(op(ip, n, 4 + cr, A));
+            }
+            if (!P.on_cf) continue;
+            for (int fc = 0; fc < 4; fc++) {
+                if (P.face_type[fc] != NB_HALF) continue;
+                for (int ig = 0; ig < 2; ig++) {
+                    const int fi = P.face_nbr[fc][ig];
+                    va.push_back(op(ip, fi, fc, T.child_map(P, f.p[fi])));
                 }
             }
+            for (int cr = 0; cr < 4; cr++) {
+                if (!P.has_corner[cr] || P.corner_type[cr] != NB_HALF) continue;
+                const int fi = P.corner_nbr[cr];
+                const TableCtx::Aff F = T.child_map(P, f.p[fi]);
+                good = good && avg_corner_ok(4 + cr, F);
+                va.push_back(op(ip, fi, 4 + cr, F));
+            }
         }
-        out.copy_off[33] = (int)out.copy.size();
-        out.avg_off[33] = (int)out.avg.size();
         if (!good) bad = 1;
     };
 
     // ---- interpolate2ghost (coarse = level l): faces of all coarse patches, then corners ----
-    auto interp = [&](int l) {
-        std::vector<InterpEnt>& v = w.interp[l];
-        v.clear();
-        const int p0 = f.lev_off[l], p1 = f.lev_off[l + 1];
-        if (p0 == p1 || l >= 32) return;
-        std::vector<int>& slots = w.slots[l];
-        slots.assign((size_t)(f.lev_off[l + 2] - p1) * nxy, -1);
-        LastWriter<InterpEnt> W(v, slots, nq, nxy, p1);
-        auto validi = [&](int i, int j) { return 1 - mbc <= i && i <= mx + mbc && 1 - mbc <= j && j <= my + mbc; };
-        // the fine cells of the four children (coarse axes, sub = ii + 2 jj) of coarse
-        // cell (ic, jc), skipped unless all lie in F's padded patch (is_valid_interp)
-        auto emit = [&](int cp, int ic, int jc, int fp, const TableCtx::Aff& F, bool check) {
-            int ci[4], cj[4];
-            for (int m = 0; m < 4; m++) {
-                F.map(2 * ic + (m & 1), 2 * jc + (m >> 1), ci[m], cj[m]);
-                if (check && !validi(ci[m], cj[m])) return;
-            }
-            for (int m = 0; m < 4; m++) W.put({T.cell(fp, ci[m], cj[m]), T.cell(cp, ic, jc), m, 0}, fp);
+    // Two writes to one fine ghost cell come from ops into the same fine patch, so the
+    // last-writer rule of the reference's order (faces of every coarse patch in patch
+    // order, then corners) is kept per fine patch: the ops are listed per fine patch in
+    // that order (one pass here), then the fine patches are expanded in parallel chunks,
+    // each with a map of one patch's cells.
+    w.iops.resize(33); w.iop_first.resize(33);
+    struct Chunk { int l, a, b; };                       // fine patches [a, b) of coarse level l
+    std::vector<Chunk> chunks;
+    for (int l = 0; l < 32; l++) {
+        std::vector<InterpOp>& ops = w.iops[l];
+        std::vector<int>& first = w.iop_first[l];
+        ops.clear();
+        const int p0 = f.lev_off[l], p1 = f.lev_off[l + 1], nf = f.lev_off[l + 2] - p1;
+        first.assign(nf + 1, 0);
+        if (p0 == p1 || nf == 0) continue;
+        auto iop = [&](int cp, int fp, int region) {
+            const TableCtx::Aff F = T.child_map(f.p[cp], f.p[fp]);
+            return InterpOp{cp, fp, region, 0, F.ci, F.cj, F.ii, F.ij, F.ji, F.jj};
         };
-        for (int ip = p0; ip < p1; ip++) {
-            const PatchInfo& C = f.p[ip];
-            if (!C.on_cf) continue;
-            for (int fc = 0; fc < 4; fc++) {
-                if (C.face_type[fc] != NB_HALF) continue;
-                for (int ig = 0; ig < 2; ig++) {
-                    const int fi = C.face_nbr[fc][ig];
-                    const TableCtx::Aff F = T.child_map(C, f.p[fi]);
-                    if (fc < 2) {
-                        for (int ibc = 1; ibc <= mbc / 2; ibc++) {
-                            const int ic = (fc == 0) ? ibc : mx - ibc + 1;
-                            for (int jc = 1; jc <= mx; jc++) emit(ip, ic, jc, fi, F, true);
-                        }
-                    } else {
-                        for (int jbc = 1; jbc <= mbc / 2; jbc++) {
-                            const int jc = (fc == 2) ? jbc : my - jbc + 1;
-                            for (int ic = 1; ic <= mx; ic++) emit(ip, ic, jc, fi, F, true);
-                        }
+        for (int pass = 0; pass < 2; pass++) {           // count, then fill, in the reference's order
+            std::vector<int> at(first.begin(), first.end() - 1);
+            auto add = [&](int cp, int fp, int region) {
+                if (fp < p1 || fp >= p1 + nf) { bad = 1; return; }
+                if (pass == 0) first[fp - p1 + 1]++;
+                else ops[at[fp - p1]++] = iop(cp, fp, region);
+            };
+            for (int ip = p0; ip < p1; ip++) {
+                const PatchInfo& C = f.p[ip];
+                if (!C.on_cf) continue;
+                for (int fc = 0; fc < 4; fc++)
+                    if (C.face_type[fc] == NB_HALF)
+                        for (int ig = 0; ig < 2; ig++) add(ip, C.face_nbr[fc][ig], fc);
+            }
+            for (int ip = p0; ip < p1; ip++) {
+                const PatchInfo& C = f.p[ip];
+                if (!C.on_cf) continue;
+                for (int cr = 0; cr < 4; cr++)
+                    if (C.has_corner[cr] && C.corner_type[cr] == NB_HALF) add(ip, C.corner_nbr[cr], 4 + cr);
+            }
+            if (pass == 0) {
+                for (int k = 0; k < nf; k++) first[k + 1] += first[k];
+                ops.resize(first[nf]);
+            }
+        }
+        for (int a = 0; a < nf; a += 64) chunks.push_back({l, a, std::min(nf, a + 64)});
+    }
+    w.interp.resize(chunks.size());
+    auto interp = [&](int c) {
+        const Chunk& ch = chunks[c];
+        const int l = ch.l, p1 = f.lev_off[l + 1];
+        std::vector<InterpEnt>& v = w.interp[c];
+        v.clear();
+        std::vector<int> at(nxy, -1);                    // cell of the current fine patch -> entry
+        auto validi = [&](long i, long j) { return 1 - mbc <= i && i <= mx + mbc && 1 - mbc <= j && j <= my + mbc; };
+        bool outside = false;
+        for (int k = ch.a; k < ch.b; k++) {
+            const int fp = p1 + k;
+            const size_t v0 = v.size();
+            // the fine cells of the four children (coarse axes, sub = ii + 2 jj) of coarse
+            // cell (ic, jc), skipped unless all lie in the fine patch's padded patch
+            // (is_valid_interp)
+            auto emit = [&](const InterpOp& o, int ic, int jc, bool check) {
+                long ci[4], cj[4];
+                for (int m = 0; m < 4; m++) {
+                    const long x = 2 * ic + (m & 1), y = 2 * jc + (m >> 1);
+                    ci[m] = o.ci + o.ii * x + o.ij * y;
+                    cj[m] = o.cj + o.ji * x + o.jj * y;
+                    if (check && !validi(ci[m], cj[m])) return;
+                }
+                for (int m = 0; m < 4; m++) {
+                    if (!validi(ci[m], cj[m])) { outside = true; return; }
+                    const InterpEnt e{T.cell(fp, (int)ci[m], (int)cj[m]), T.cell(o.cp, ic, jc), m, 0};
+                    int& a = at[e.dst - fp * nq];
+                    if (a < 0) { a = (int)v.size(); v.push_back(e); }
+                    else v[a] = e;
+                }
+            };
+            for (int q = w.iop_first[l][k]; q < w.iop_first[l][k + 1]; q++) {
+                const InterpOp& o = w.iops[l][q];
+                if (o.region < 2) {
+                    for (int ibc = 1; ibc <= mbc / 2; ibc++) {
+                        const int ic = (o.region == 0) ? ibc : mx - ibc + 1;
+                        for (int jc = 1; jc <= mx; jc++) emit(o, ic, jc, true);
                     }
+                } else if (o.region < 4) {
+                    for (int jbc = 1; jbc <= mbc / 2; jbc++) {
+                        const int jc = (o.region == 2) ? jbc : my - jbc + 1;
+                        for (int ic = 1; ic <= mx; ic++) emit(o, ic, jc, true);
+                    }
+                } else {
+                    const int cr = o.region - 4;
+                    for (int ibc = 1; ibc <= mbc / 2; ibc++)
+                        for (int jbc = 1; jbc <= mbc / 2; jbc++)
+                            emit(o, (cr & 1) ? mx - ibc + 1 : ibc, (cr & 2) ? my - jbc + 1 : jbc, false);
                 }
             }
+            for (size_t i = v0; i < v.size(); i++) at[v[i].dst - fp * nq] = -1;
         }
-        for (int ip = p0; ip < p1; ip++) {
-            const PatchInfo& C = f.p[ip];
-            if (!C.on_cf) continue;
-            for (int cr = 0; cr < 4; cr++) {
-                if (!C.has_corner[cr] || C.corner_type[cr] != NB_HALF) continue;
-                const int fi = C.corner_nbr[cr];
-                const TableCtx::Aff F = T.child_map(C, f.p[fi]);
-                for (int ibc = 1; ibc <= mbc / 2; ibc++)
-                    for (int jbc = 1; jbc <= mbc / 2; jbc++)
-                        emit(ip, (cr & 1) ? mx - ibc + 1 : ibc, (cr & 2) ? my - jbc + 1 : jbc, fi, F, false);
-            }
-        }
-        if (W.outside) bad = 1;
+        if (outside) bad = 1;
     };
-    // the finest levels hold most patches: their interpolation tasks go first
-    run_tasks(nlev + 1, nt, [&](int k) {
-        if (k < nlev) interp(nlev - 1 - k);
-        else regions();
+    // the interpolation chunks first (most of the work), then the region ops per level
+    const int nchunk = (int)chunks.size();
+    run_tasks(nchunk + nlev, nt, [&](int k) {
+        if (k < nchunk) interp(k);
+        else regions(k - nchunk);
     });
     if (bad) { err = "a ghost-fill table writes outside its destination patches"; return false; }
 
-    out.interp.clear(); out.phys.clear(); out.ti.clear();
+    // flat tables in level order
+    out.copy.clear(); out.avg.clear(); out.interp.clear();
+    for (int l = 0; l < 33; l++) {
+        out.copy_off[l] = (int)out.copy.size();
+        out.avg_off[l] = (int)out.avg.size();
+        if (l < nlev) {
+            out.copy.insert(out.copy.end(), w.copy[l].begin(), w.copy[l].end());
+            out.avg.insert(out.avg.end(), w.avg[l].begin(), w.avg[l].end());
+        }
+    }
+    out.copy_off[33] = (int)out.copy.size();
+    out.avg_off[33] = (int)out.avg.size();
+    for (int l = 0, c = 0; l < 33; l++) {
+        out.interp_off[l] = (int)out.interp.size();
+        for (; c < nchunk && chunks[c].l == l; c++) out.interp.insert(out.interp.end(), w.interp[c].begin(), w.interp[c].end());
+    }
+    out.interp_off[33] = (int)out.interp.size();
+
+    out.phys.clear(); out.ti.clear();
     out.sync.assign((size_t)np * SYNC_SLOTS, SyncOp{0, 0, 0, 0, 0, SYNC_NONE, {0, 0}});
     for (int l = 0; l < 33; l++) {
         const int p0 = f.lev_off[l], p1 = f.lev_off[l + 1];
-        out.interp_off[l] = (int)out.interp.size();
         out.phys_off[l] = (int)out.phys.size();
         out.ti_off[l] = (int)out.ti.size();
         if (p0 == p1) continue;
-        out.interp.insert(out.interp.end(), w.interp[l].begin(), w.interp[l].end());
         // ---- setphysical: clawpack46_bc2_default with chains resolved per patch ----
         {
             std::vector<int> wsrc(nxy, -1), wneg(nxy, 0), wconst(nxy, 0);
@@ -876,7 +912,6 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out,
             }
         }
     }
-    out.interp_off[33] = (int)out.interp.size();
     out.phys_off[33] = (int)out.phys.size();
     out.ti_off[33] = (int)out.ti.size();
     if (!tables_in_bounds(out, (long)np * nq)) {

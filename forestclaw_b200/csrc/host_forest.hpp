@@ -175,9 +175,15 @@ struct Tables {
 
 // Buffers build_tables keeps between calls (their pages stay mapped from one regrid
 // to the next).
+// One interpolation op of the table build: coarse patch cp fills ghost cells of fine
+// patch fp through face (region 0..3) or corner (4..7) of cp; the child map of the pair
+// (x, y) -> (ci + ii x + ij y, cj + ji x + jj y).
+struct InterpOp { int cp, fp, region, pad; long ci, cj, ii, ij, ji, jj; };
 struct TableWork {
-    std::vector<std::vector<InterpEnt>> interp;
-    std::vector<std::vector<int>> slots;
+    std::vector<std::vector<FillOp>> copy, avg;            // region ops per level
+    std::vector<std::vector<InterpOp>> iops;               // interpolation ops per coarse level, by fine patch
+    std::vector<std::vector<int>> iop_first;               // per coarse level: CSR offsets over its fine patches
+    std::vector<std::vector<InterpEnt>> interp;            // interpolation entries per task
 };
 
 // inflow: mthbc = 0 sides are set to a constant state (PhysEnt.cst = 1, src unused).
