@@ -193,7 +193,8 @@ struct fc2d_b200_solver {
     DevVec<RepopOp> repop_dev;                     // regrid repopulation ops
     DevVec<double> snap;                           // batch regrid: q of instances whose forest is unchanged
     DevVec<int> keep_dev;
-    std::vector<double> aux_host;                  // static aux mirror (level-major)
+    DevVec<int> aux_src_dev;                       // regrid: where each new patch's aux comes from
+    DevVec<double> aux_staged_dev;                 // regrid: aux of new patches from the app's setaux
     TableArena arena;                              // the tables below, on the device
     DevView<FillOp> t_copy;                        // copy2ghost region ops
     DevView<FillOp> t_avg;                         // average2ghost region ops
@@ -1129,7 +1130,6 @@ extern "C" int fc2d_b200_set_forest(fc2d_b200_solver_t* s, int np, const int* le
     for (int i = 0; i < np; i++) L[i] = {level[i], gx[i], gy[i]};
     int rc = install_forest(s, L);
     if (rc) return rc;
-    if (s->d.maux > 0) s->aux_host.assign((size_t)np * s->d.naux(), 0.0);
     s->initialized = true;
     return 0;
 }
@@ -1223,13 +1223,11 @@ extern "C" int fc2d_b200_initialize(fc2d_b200_solver_t* s)
         std::vector<MetricOp> ops(s->forest.np());
         for (int i = 0; i < s->forest.np(); i++) ops[i] = MetricOp{0, i, {0, 0, 0, 0}};
         CK(s->metric_dev.assign(ops, s->st));
-        launch_sphere_metric(d, s->metric_dev.p, (int)ops.size(), s->desc, s->o.maxlevel, nullptr, s->area, s->aux,
+        launch_sphere_metric(d, s->metric_dev.p, (int)ops.size(), 0, s->desc, s->o.maxlevel, nullptr, s->area, s->aux,
                              s->flow, s->st);
         CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(aux.data(), s->aux, aux.size() * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     }
     CK(cudaStreamSynchronize(s->st));
-    s->aux_host.swap(aux);
     s->t_curr = 0;
     s->initialized = true;
     return 0;
@@ -1290,7 +1288,6 @@ extern "C" int fc2d_b200_set_aux(fc2d_b200_solver_t* s, const double* aux)
     if (!s || !aux) return fail(FC2D_B200_EINVAL, "null argument");
     if (s->d.maux == 0) return 0;
     const size_t n = (size_t)s->forest.np() * s->d.naux();
-    s->aux_host.assign(aux, aux + n);
     CK(cudaMemcpyAsync(s->aux, aux, n * sizeof(double), cudaMemcpyHostToDevice, s->st));
     CK(cudaStreamSynchronize(s->st));
     return 0;
@@ -1446,8 +1443,6 @@ extern "C" int fc2d_b200_single_step_update_host(fc2d_b200_solver_t* s, int leve
         CK(cudaMemcpyAsync(s->aux + (size_t)p0 * na, s->ss_stage, (size_t)np * na * sizeof(double),
                            cudaMemcpyHostToDevice, s->st));
         CK(cudaStreamSynchronize(s->st));
-        for (const auto& h : s->ss_host)               // keep the host mirror of aux in step
-            std::memcpy(&s->aux_host[(size_t)h.slot * na], h.aux, na * sizeof(double));
     }
     for (const auto& h : s->ss_host) std::memcpy(s->ss_stage + (size_t)(h.slot - p0) * nq, h.q, nq * sizeof(double));
     CK(cudaMemcpyAsync(s->q + (size_t)p0 * nq, s->ss_stage, (size_t)np * nq * sizeof(double), cudaMemcpyHostToDevice,
@@ -1764,7 +1759,11 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     }
     // repopulation ops (cb_fclaw2d_regrid_repopulate)
     std::vector<RepopOp> ops(nf.np());
-    std::vector<double> naux((size_t)nf.np() * d.naux(), 0.0);
+    // aux of the new forest, filled on the device: a kept patch's from the old slab
+    // (asrc = old slot), a new patch's from the app's setaux on the host (staged,
+    // asrc = -2 - k) or from the cubed-sphere metric (asrc = -1)
+    std::vector<int> asrc(d.maux > 0 ? nf.np() : 0);
+    std::vector<double> staged;
     for (int i = 0; i < nf.np(); i++) {
         const PatchInfo& P = nf.p[i];
         RepopOp op{};
@@ -1772,7 +1771,7 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
         const int old = f.lookup(P.inst, P.level, P.gx, P.gy);
         if (old >= 0) {
             op.kind = 0; op.src = old;
-            if (d.maux > 0) std::memcpy(&naux[(size_t)i * d.naux()], &s->aux_host[(size_t)old * d.naux()], sizeof(double) * d.naux());
+            if (d.maux > 0) asrc[i] = old;
         } else {
             const int parent = f.lookup(P.inst, P.level - 1, P.gx >> 1, P.gy >> 1);
             if (parent >= 0) { op.kind = 1; op.src = parent; op.igrid = (P.gx & 1) + 2 * (P.gy & 1); }
@@ -1783,7 +1782,13 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
                     if (op.child[c] < 0) return fail(FC2D_B200_EFOREST, "adapt jumped more than one level");
                 }
             }
-            if (d.maux > 0) app_setaux(inst_options(s, P.inst), d, P, &naux[(size_t)i * d.naux()]);
+            if (d.maux > 0 && s->sphere) asrc[i] = -1;
+            else if (d.maux > 0) {
+                const size_t k = staged.size() / d.naux();
+                staged.resize(staged.size() + d.naux(), 0.0);
+                app_setaux(inst_options(s, P.inst), d, P, &staged[k * d.naux()]);
+                asrc[i] = -2 - (int)k;
+            }
         }
         ops[i] = op;
     }
@@ -1792,25 +1797,31 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     if (rc) return rc;
     auto& sp = s->spare;
     CK(s->repop_dev.assign(ops, s->st));
-    if (d.maux > 0) CK(cudaMemcpyAsync(sp.aux, naux.data(), naux.size() * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    if (d.maux > 0) {
+        CK(s->aux_src_dev.assign(asrc, s->st));
+        if (!staged.empty()) CK(s->aux_staged_dev.assign(staged, s->st));
+        launch_aux_repop(d, s->aux_src_dev.p, nf.np(), s->aux, s->aux_staged_dev.p, sp.aux, s->st);
+    }
     std::vector<PatchDesc> hd;
     if (s->sphere) {
         // metric of the new forest before repopulation, which weights by the areas:
         // kept patches copy, refined ones build from scratch, coarsened ones from their
         // children (cb_fclaw2d_regrid_repopulate: fclaw2d_patch_build / _build_from_fine)
-        std::vector<MetricOp> mops(ops.size());
+        // (new patches first, then the kept ones)
+        std::vector<MetricOp> mops, kept;
         for (size_t i = 0; i < ops.size(); i++) {
             const RepopOp& o = ops[i];
-            if (o.kind == 0) mops[i] = MetricOp{1, (int)i, {o.src, 0, 0, 0}};
-            else if (o.kind == 1) mops[i] = MetricOp{0, (int)i, {0, 0, 0, 0}};
-            else mops[i] = MetricOp{2, (int)i, {o.child[0], o.child[1], o.child[2], o.child[3]}};
+            if (o.kind == 0) kept.push_back(MetricOp{1, (int)i, {o.src, 0, 0, 0}});
+            else if (o.kind == 1) mops.push_back(MetricOp{0, (int)i, {0, 0, 0, 0}});
+            else mops.push_back(MetricOp{2, (int)i, {o.child[0], o.child[1], o.child[2], o.child[3]}});
         }
+        const int nnew = (int)mops.size(), nkept = (int)kept.size();
+        mops.insert(mops.end(), kept.begin(), kept.end());
         hd = make_desc(nf);
         CK(cudaMemcpyAsync(sp.desc, hd.data(), hd.size() * sizeof(PatchDesc), cudaMemcpyHostToDevice, s->st));
         CK(s->metric_dev.assign(mops, s->st));
-        launch_sphere_metric(d, s->metric_dev.p, (int)mops.size(), sp.desc, s->o.maxlevel, s->area, sp.area, sp.aux,
+        launch_sphere_metric(d, s->metric_dev.p, nnew, nkept, sp.desc, s->o.maxlevel, s->area, sp.area, sp.aux,
                              s->flow, s->st);
-        CK(cudaMemcpyAsync(naux.data(), sp.aux, naux.size() * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     }
     launch_repop(d, s->repop_dev.p, (int)ops.size(), s->q, sp.q, s->qlast, sp.qlast, s->qinterp, sp.qinterp, s->regs,
                  sp.regs, s->sphere ? s->area : nullptr, s->sphere ? sp.area : nullptr, s->st);
@@ -1819,7 +1830,6 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     std::swap(s->aux, sp.aux); std::swap(s->regs, sp.regs); std::swap(s->desc, sp.desc);
     std::swap(s->area, sp.area);
     std::swap(s->cap, sp.cap);
-    s->aux_host.swap(naux);
     s->forest = std::move(nf);
     s->forest_gen++;
     invalidate_graph(s);

@@ -905,6 +905,23 @@ void launch_unpack_patches(const Dims& d, const int* slots, int n, double* q, do
 {
     if (n > 0) k_unpack_patches<<<n, 256, 0, st>>>(slots, n, q, qlast, regs, d.nq(), d.nreg(), in);
 }
+// aux of a new forest, one CTA per new slot: src >= 0 the old slot's, src <= -2 staged
+// patch -2 - src, src = -1 left to the cubed-sphere metric
+__global__ void k_aux_repop(const int* __restrict__ src, int naux, const double* __restrict__ oaux,
+                            const double* __restrict__ staged, double* __restrict__ aux)
+{
+    const int i = blockIdx.x, sidx = src[i];
+    if (sidx == -1) return;
+    const double* from = sidx >= 0 ? oaux + (size_t)sidx * naux : staged + (size_t)(-2 - sidx) * naux;
+    double* to = aux + (size_t)i * naux;
+    for (int k = threadIdx.x; k < naux; k += blockDim.x) to[k] = from[k];
+}
+void launch_aux_repop(const Dims& d, const int* src, int n, const double* oaux, const double* staged, double* aux,
+                      cudaStream_t st)
+{
+    if (n > 0 && d.maux > 0) k_aux_repop<<<n, 256, 0, st>>>(src, d.naux(), oaux, staged, aux);
+}
+
 void launch_repop(const Dims& d, const RepopOp* ops, int nops, const double* oq, double* nq, const double* oqlast,
                   double* nqlast, const double* oqi, double* nqi, const double* oregs, double* nregs,
                   const double* oarea, const double* narea, cudaStream_t st)

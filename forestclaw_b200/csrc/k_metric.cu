@@ -21,70 +21,82 @@
 
 namespace fcb {
 
-__device__ double cell_area_scratch(int block, double xlower, double ylower, double dx, double dy, int i, int j,
-                                    int rfactor)
+// Areas of new patches (ops of kind 0 and 2 first in the op list): one warp per (op,
+// cell).  A cell from scratch has (2^(maxlevel-level))^2 sub-quads: the lanes compute
+// their areas (ii outer, jj inner; each corner mapped from the same arguments as in a
+// column sweep) into shared memory in chunks of METRIC_CHUNK, and lane 0 adds each
+// chunk in order, so the sum is the sequential one.
+constexpr int METRIC_WARPS = 4, METRIC_CHUNK = 1024;
+__global__ void __launch_bounds__(32 * METRIC_WARPS)
+k_sphere_area(const MetricOp* __restrict__ ops, const PatchDesc* __restrict__ desc, int mx, int my, int mbc,
+              int maxlevel, const double* __restrict__ oarea, double* __restrict__ narea)
 {
-    const double dxf = dx / rfactor, dyf = dy / rfactor;
-    const double xe = xlower + (i - 1) * dx, ye = ylower + (j - 1) * dy;
-    double sum = 0.0;
-    for (int ii = 0; ii < rfactor; ii++) {
-        double p[4][3];
-        // corners (ii, jj), (ii+1, jj) of the first sub-quad of this column
-        cs_map(block, xe + ii * dxf, ye + 0 * dyf, &p[0][0], &p[0][1], &p[0][2]);
-        cs_map(block, xe + (ii + 1) * dxf, ye + 0 * dyf, &p[1][0], &p[1][1], &p[1][2]);
-        for (int jj = 0; jj < rfactor; jj++) {
-            cs_map(block, xe + ii * dxf, ye + (jj + 1) * dyf, &p[2][0], &p[2][1], &p[2][2]);
-            cs_map(block, xe + (ii + 1) * dxf, ye + (jj + 1) * dyf, &p[3][0], &p[3][1], &p[3][2]);
-            sum = sum + cs_quad_area(p);
-            for (int m = 0; m < 3; m++) { p[0][m] = p[2][m]; p[1][m] = p[3][m]; }
-        }
-    }
-    return sum;
-}
-
-// One CTA per op.  ops: kind 0 scratch, 1 copy (src[0] old slot), 2 from fine (src = old
-// slots of children igrid 0..3).
-__global__ void k_sphere_area(const MetricOp* __restrict__ ops, const PatchDesc* __restrict__ desc, int mx, int my,
-                              int mbc, int maxlevel, const double* __restrict__ oarea, double* __restrict__ narea)
-{
+    __shared__ double sub[METRIC_WARPS][METRIC_CHUNK];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const MetricOp op = ops[blockIdx.x];
     const int ax = mx + 2 * mbc + 2, ay = my + 2 * mbc + 2, na = ax * ay;
+    const int k = blockIdx.y * METRIC_WARPS + w;
+    if (k >= na) return;                                      // the whole warp
     double* a = narea + (size_t)op.dst * na;
-    if (op.kind == 1) {
-        const double* s = oarea + (size_t)op.src[0] * na;
-        for (int k = threadIdx.x; k < na; k += blockDim.x) a[k] = s[k];
+    const PatchDesc pd = desc[op.dst];
+    const int i = k % ax - mbc, j = k / ax - mbc;              // -mbc .. mx+mbc+1
+    const bool interior = i >= 0 && i <= mx + 1 && j >= 0 && j <= my + 1;
+    if (op.kind == 2 && interior) {
+        // fclaw2d_metric_fort_average_area: child igrid covers coarse cells
+        // (i, j) - (ig mx/2, jg my/2) in 0 .. mx/2+1; the last covering child wins
+        if (lane != 0) return;
+        int g = -1, ic = 0, jc = 0;
+        for (int igrid = 0; igrid < 4; igrid++) {
+            const int ig = igrid % 2, jg = igrid / 2;
+            const int ii = i - ig * mx / 2, jj = j - jg * mx / 2;
+            if (ii >= 0 && ii <= mx / 2 + 1 && jj >= 0 && jj <= my / 2 + 1) { g = igrid; ic = ii; jc = jj; }
+        }
+        const double* f = oarea + (size_t)op.src[g] * na;
+        double sum = 0.0;
+        for (int jj = 1; jj <= 2; jj++)
+            for (int ii = 1; ii <= 2; ii++) {
+                const int fi = (ic - 1) * 2 + ii, fj = (jc - 1) * 2 + jj;
+                sum = sum + f[(fj + mbc) * ax + (fi + mbc)];
+            }
+        a[k] = sum;
         return;
     }
-    const PatchDesc pd = desc[op.dst];
-    const int rfactor = 1 << (maxlevel - pd.level);
-    const int block = pd.block;
-    for (int k = threadIdx.x; k < na; k += blockDim.x) {
-        const int i = k % ax - mbc, j = k / ax - mbc;          // -mbc .. mx+mbc+1
-        const bool interior = i >= 0 && i <= mx + 1 && j >= 0 && j <= my + 1;
-        if (op.kind == 2 && interior) {
-            // fclaw2d_metric_fort_average_area: child igrid covers coarse cells
-            // (i, j) - (ig mx/2, jg my/2) in 0 .. mx/2+1; the last covering child wins
-            int g = -1, ic = 0, jc = 0;
-            for (int igrid = 0; igrid < 4; igrid++) {
-                const int ig = igrid % 2, jg = igrid / 2;
-                const int ii = i - ig * mx / 2, jj = j - jg * mx / 2;
-                if (ii >= 0 && ii <= mx / 2 + 1 && jj >= 0 && jj <= my / 2 + 1) { g = igrid; ic = ii; jc = jj; }
-            }
-            const double* f = oarea + (size_t)op.src[g] * na;
-            double sum = 0.0;
-            for (int jj = 1; jj <= 2; jj++)
-                for (int ii = 1; ii <= 2; ii++) {
-                    const int fi = (ic - 1) * 2 + ii, fj = (jc - 1) * 2 + jj;
-                    sum = sum + f[(fj + mbc) * ax + (fi + mbc)];
-                }
-            a[k] = sum;
-        } else {
-            a[k] = cell_area_scratch(block, pd.xlower, pd.ylower, pd.dx, pd.dy, i, j, rfactor);
+    // from scratch: fclaw2d_metric_fort_compute_area_general
+    const int rf = 1 << (maxlevel - pd.level), block = pd.block;
+    const long nsub = (long)rf * rf;
+    const double dxf = pd.dx / rf, dyf = pd.dy / rf;
+    const double xe = pd.xlower + (i - 1) * pd.dx, ye = pd.ylower + (j - 1) * pd.dy;
+    double sum = 0.0;
+    for (long s0 = 0; s0 < nsub; s0 += METRIC_CHUNK) {
+        const int n = (int)(nsub - s0 < METRIC_CHUNK ? nsub - s0 : METRIC_CHUNK);
+        for (int t = lane; t < n; t += 32) {
+            const long sq = s0 + t;
+            const int ii = (int)(sq / rf), jj = (int)(sq % rf);
+            double p[4][3];
+            cs_map(block, xe + ii * dxf, ye + jj * dyf, &p[0][0], &p[0][1], &p[0][2]);
+            cs_map(block, xe + (ii + 1) * dxf, ye + jj * dyf, &p[1][0], &p[1][1], &p[1][2]);
+            cs_map(block, xe + ii * dxf, ye + (jj + 1) * dyf, &p[2][0], &p[2][1], &p[2][2]);
+            cs_map(block, xe + (ii + 1) * dxf, ye + (jj + 1) * dyf, &p[3][0], &p[3][1], &p[3][2]);
+            sub[w][t] = cs_quad_area(p);
         }
+        __syncwarp();
+        if (lane == 0)
+            for (int t = 0; t < n; t++) sum = sum + sub[w][t];
+        __syncwarp();
     }
+    if (lane == 0) a[k] = sum;
 }
 
-// aux of new patches (ops of kind 0 and 2): one CTA per op.
+// Areas of kept patches (ops of kind 1): copied, one thread per (op, cell).
+__global__ void k_sphere_area_copy(const MetricOp* __restrict__ ops, int na, const double* __restrict__ oarea,
+                                   double* __restrict__ narea)
+{
+    const MetricOp op = ops[blockIdx.x];
+    const int k = blockIdx.y * blockDim.x + threadIdx.x;
+    if (k < na) narea[(size_t)op.dst * na + k] = oarea[(size_t)op.src[0] * na + k];
+}
+
+// aux of new patches (ops of kind 0 and 2): one thread per (op, cell).
 __global__ void k_sphere_aux(const MetricOp* __restrict__ ops, const PatchDesc* __restrict__ desc, int mx, int my,
                              int mbc, const double* __restrict__ area, double* __restrict__ aux,
                              SphereFlow flow)
@@ -103,7 +115,8 @@ __global__ void k_sphere_aux(const MetricOp* __restrict__ ops, const PatchDesc* 
         cs_map(block, pd.xlower + (i - 1) * pd.dx, pd.ylower + (j - 1) * pd.dy, &xp, &yp, &zp);
         return cs_psi(flow.axis, flow.omega, xp, yp, zp);
     };
-    for (int k = threadIdx.x; k < nxy; k += blockDim.x) {
+    const int k = blockIdx.y * blockDim.x + threadIdx.x;
+    if (k < nxy) {
         const int i = k % nx + 1 - mbc, j = k / nx + 1 - mbc;
         x[k] = a[(j + mbc) * ax + (i + mbc)] / dxdy;
         const double p00 = psi_node(i, j);
@@ -112,12 +125,16 @@ __global__ void k_sphere_aux(const MetricOp* __restrict__ ops, const PatchDesc* 
     }
 }
 
-void launch_sphere_metric(const Dims& d, const MetricOp* ops, int nops, const PatchDesc* desc, int maxlevel,
+void launch_sphere_metric(const Dims& d, const MetricOp* ops, int nnew, int nkept, const PatchDesc* desc, int maxlevel,
                           const double* oarea, double* narea, double* aux, const SphereFlow& flow, cudaStream_t st)
 {
-    if (nops <= 0) return;
-    k_sphere_area<<<nops, 256, 0, st>>>(ops, desc, d.mx, d.my, d.mbc, maxlevel, oarea, narea);
-    k_sphere_aux<<<nops, 256, 0, st>>>(ops, desc, d.mx, d.my, d.mbc, narea, aux, flow);
+    const int na = (d.mx + 2 * d.mbc + 2) * (d.my + 2 * d.mbc + 2);
+    if (nnew > 0) {
+        k_sphere_area<<<dim3(nnew, (na + METRIC_WARPS - 1) / METRIC_WARPS), 32 * METRIC_WARPS, 0, st>>>(
+            ops, desc, d.mx, d.my, d.mbc, maxlevel, oarea, narea);
+        k_sphere_aux<<<dim3(nnew, (d.nxy() + 127) / 128), 128, 0, st>>>(ops, desc, d.mx, d.my, d.mbc, narea, aux, flow);
+    }
+    if (nkept > 0) k_sphere_area_copy<<<dim3(nkept, (na + 255) / 256), 256, 0, st>>>(ops + nnew, na, oarea, narea);
 }
 
 }  // namespace fcb

@@ -99,9 +99,6 @@ void launch_timeinterp(const Dims& d, const double* q, const double* qlast, doub
                        int npatch, const PatchDesc* desc, const LevelAlpha& alpha, cudaStream_t st);
 
 // ---- time sync (k_amr.cu) -------------------------------------------------------
-// One op = (coarse/this patch, fine/neighbour patch, face, igrid).  Ops of one
-// patch are contiguous and in the reference order; op_start[i]..op_start[i+1]
-// are the ops of the i-th patch of the launch.
 // One time-sync correction of patch p from neighbour n across face `face`:
 // kind SYNC_SAMESIZE (clawpack46_fort_time_sync_samesize) or SYNC_F2C (coarse p,
 // fine n = child igrid of the face, n_off = first fine index offset along it).
@@ -165,6 +162,10 @@ void launch_sample_interfaces(const Dims& d, const double* q, int np, double gam
 struct RepopOp { int kind, dst, src, igrid; int child[4]; };
 // oarea/narea (cubed sphere, else null): old and new cell areas -- interpolate2fine then
 // keeps each coarse cell's mass (fixcapaq2) and average2coarse weights by area.
+// aux of the n patches of a new forest from the old slab or staged host values (src codes
+// at k_aux_repop)
+void launch_aux_repop(const Dims& d, const int* src, int n, const double* oaux, const double* staged, double* aux,
+                      cudaStream_t st);
 void launch_repop(const Dims& d, const RepopOp* ops, int nops, const double* oq, double* nq,
                   const double* oqlast, double* nqlast, const double* oqi, double* nqi,
                   const double* oregs, double* nregs, const double* oarea, const double* narea, cudaStream_t st);
@@ -180,7 +181,8 @@ struct SphereFlow { double axis[3]; double omega; };   // psi = omega (axis . x)
 // of patches order[0..npatch), packed in that order (k_output.cu).
 void launch_vtk_pack(const Dims& d, const double* q, const PatchDesc* desc, const int* order, int npatch, int manifold,
                      double* points, float* values, cudaStream_t st);
-void launch_sphere_metric(const Dims& d, const MetricOp* ops, int nops, const PatchDesc* desc, int maxlevel,
+// ops: the nnew new patches (kind 0 or 2) first, then the nkept kept ones (kind 1)
+void launch_sphere_metric(const Dims& d, const MetricOp* ops, int nnew, int nkept, const PatchDesc* desc, int maxlevel,
                           const double* oarea, double* narea, double* aux, const SphereFlow& flow, cudaStream_t st);
 
 }  // namespace fcb
