@@ -616,7 +616,6 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out,
     nt = std::max(1, std::min(nt, std::min(16, np / 64)));
     int nlev = 0;
     for (int l = 0; l < 33; l++) if (f.lev_off[l + 1] > f.lev_off[l]) nlev = l + 1;
-    w.copy.resize(33); w.avg.resize(33);
     std::atomic<int> bad{0};
 
     // ---- copy2ghost (faces, then corners, of each patch: fclaw2d_clawpatch46_copy.f) and
@@ -665,13 +664,94 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out,
                 }
         return true;
     };
-    // the ops of level l's patches (one task per level)
-    auto regions = [&](int l) {
-        std::vector<FillOp>& vc = w.copy[l];
-        std::vector<FillOp>& va = w.avg[l];
-        vc.clear(); va.clear();
+    // ---- the tables of each patch: region ops, physical BCs, time-interpolation list and
+    // time-sync ops, in chunks of up to 64 patches of one level (one task each) ----
+    struct PChunk { int l, a, b; };
+    std::vector<PChunk> pch;
+    for (int l = 0; l < nlev; l++)
+        for (int a = f.lev_off[l]; a < f.lev_off[l + 1]; a += 64) pch.push_back({l, a, std::min(f.lev_off[l + 1], a + 64)});
+    w.copy.resize(pch.size()); w.avg.resize(pch.size()); w.phys.resize(pch.size()); w.ti.resize(pch.size());
+    out.sync.assign((size_t)np * SYNC_SLOTS, SyncOp{0, 0, 0, 0, 0, SYNC_NONE, {0, 0}});
+    auto phys_sync = [&](int c) {
+        const int a0 = pch[c].a, a1 = pch[c].b;
+        // ---- setphysical: clawpack46_bc2_default with chains resolved per patch ----
+        {
+            std::vector<int> wsrc(nxy, -1), wneg(nxy, 0), wconst(nxy, 0);
+            for (int ip = a0; ip < a1; ip++) {
+                const PatchInfo& P = f.p[ip];
+                if (!(P.phys[0] || P.phys[1] || P.phys[2] || P.phys[3])) continue;
+                // written cell -> (source cell, negate mask), within this bc2 call;
+                // indexed by the plane-0 offset of the cell inside the patch
+                const int base = T.cell(ip, 1 - mbc, 1 - mbc);
+                std::fill(wsrc.begin(), wsrc.end(), -1);
+                std::vector<int> order;
+                auto put = [&](int di, int dj, int si, int sj, int neg) {
+                    const int dst = T.cell(ip, di, dj);
+                    int src = T.cell(ip, si, sj), cst = 0;
+                    if (wsrc[src - base] >= 0) { neg ^= wneg[src - base]; cst = wconst[src - base]; src = wsrc[src - base]; }
+                    if (wsrc[dst - base] < 0) order.push_back(dst);
+                    wsrc[dst - base] = src;
+                    wneg[dst - base] = neg;
+                    wconst[dst - base] = cst;
+                };
+                auto put_const = [&](int di, int dj) {
+                    const int dst = T.cell(ip, di, dj);
+                    if (wsrc[dst - base] < 0) order.push_back(dst);
+                    wsrc[dst - base] = dst;
+                    wneg[dst - base] = 0;
+                    wconst[dst - base] = 1;
+                };
+                const int NEG2 = 1 << 1, NEG3 = 1 << 2;   // field 2 (x momentum) / field 3 (y momentum)
+                int bc[4];
+                for (int k = 0; k < 4; k++) bc[k] = P.phys[k] ? mthbc[k] : -1;
+                if (bc[0] == 0 && inflow) for (int ibc = 1; ibc <= mbc; ibc++) for (int j = 1 - mbc; j <= my + mbc; j++) put_const(1 - ibc, j);
+                if (bc[0] == 1) for (int ibc = 1; ibc <= mbc; ibc++) for (int j = 1 - mbc; j <= my + mbc; j++) put(1 - ibc, j, 1, j, 0);
+                if (bc[0] == 3) for (int ibc = 1; ibc <= mbc; ibc++) for (int j = 1 - mbc; j <= my + mbc; j++) put(1 - ibc, j, ibc, j, NEG2);
+                if (bc[1] == 1) for (int ibc = 1; ibc <= mbc; ibc++) for (int j = 1 - mbc; j <= my + mbc; j++) put(mx + ibc, j, mx, j, 0);
+                if (bc[1] == 3) for (int ibc = 1; ibc <= mbc; ibc++) for (int j = 1 - mbc; j <= my + mbc; j++) put(mx + ibc, j, mx + 1 - ibc, j, NEG2);
+                if (bc[2] == 1) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, 1 - jbc, i, 1, 0);
+                if (bc[2] == 3) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, 1 - jbc, i, jbc, NEG3);
+                if (bc[3] == 1) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, my + jbc, i, my, 0);
+                if (bc[3] == 3) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, my + jbc, i, my + 1 - jbc, NEG3);
+                for (int dst : order) w.phys[c].push_back({dst, wsrc[dst - base], wneg[dst - base], wconst[dst - base]});
+            }
+        }
+        // ---- time interpolation patches ----
+        for (int ip = a0; ip < a1; ip++) if (f.p[ip].has_fine_nbr) w.ti[c].push_back(ip);
+        // ---- time sync ops ----
+        // fclaw2d_time_sync applies the same-size corrections of every synced level,
+        // then the fine-to-coarse ones (src/fclaw2d_time_sync.c:118-202); each
+        // correction adds to cells of its own patch p only and reads registers no
+        // correction writes, so per patch the samesize ops (faces 0..3) followed by
+        // the f2c ops ((face, igrid) order) give every cell its additions in the
+        // reference's order.  Levels without finer neighbours have no f2c ops, so
+        // one range of levels [a, maxlevel] covers both kinds.  A patch has at most
+        // eight ops (one samesize or two f2c per face): slots 8 p .. 8 p + 7.
+        for (int ip = a0; ip < a1; ip++) {
+            const PatchInfo& P = f.p[ip];
+            SyncOp* slot = &out.sync[(size_t)ip * SYNC_SLOTS];
+            int nops = 0;
+            for (int fc = 0; fc < 4; fc++)
+                if (P.face_type[fc] == NB_SAME && (!f.sphere() || f.p[P.face_nbr[fc][0]].block == P.block))
+                    slot[nops++] = {ip, P.face_nbr[fc][0], fc, 0, 0, SYNC_SAMESIZE, {0, 0}};
+            for (int fc = 0; fc < 4; fc++) {
+                if (P.face_type[fc] != NB_HALF) continue;
+                if (f.sphere() && f.p[P.face_nbr[fc][0]].block != P.block) continue;
+                for (int ig = 0; ig < 2; ig++) {
+                    const int fi = P.face_nbr[fc][ig];
+                    const PatchInfo& F = f.p[fi];
+                    const int noff = (fc < 2) ? (2 * P.gy - F.gy) * my : (2 * P.gx - F.gx) * mx;
+                    slot[nops++] = {ip, fi, fc, ig, noff, SYNC_F2C, {0, 0}};
+                }
+            }
+        }
+    };
+    auto patches = [&](int c) {
+        std::vector<FillOp>& vc = w.copy[c];
+        std::vector<FillOp>& va = w.avg[c];
+        vc.clear(); va.clear(); w.phys[c].clear(); w.ti[c].clear();
         bool good = true;
-        for (int ip = f.lev_off[l]; ip < f.lev_off[l + 1]; ip++) {
+        for (int ip = pch[c].a; ip < pch[c].b; ip++) {
             const PatchInfo& P = f.p[ip];
             for (int fc = 0; fc < 4; fc++) {
                 if (P.face_type[fc] != NB_SAME) continue;
@@ -703,6 +783,7 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out,
                 va.push_back(op(ip, fi, 4 + cr, F));
             }
         }
+        phys_sync(c);
         if (!good) bad = 1;
     };
 
@@ -807,113 +888,36 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out,
         }
         if (outside) bad = 1;
     };
-    // the interpolation chunks first (most of the work), then the region ops per level
-    const int nchunk = (int)chunks.size();
-    run_tasks(nchunk + nlev, nt, [&](int k) {
+    // the interpolation chunks first, then the per-patch chunks
+    const int nchunk = (int)chunks.size(), npch = (int)pch.size();
+    run_tasks(nchunk + npch, nt, [&](int k) {
         if (k < nchunk) interp(k);
-        else regions(k - nchunk);
+        else patches(k - nchunk);
     });
     if (bad) { err = "a ghost-fill table writes outside its destination patches"; return false; }
 
-    // flat tables in level order
-    out.copy.clear(); out.avg.clear(); out.interp.clear();
-    for (int l = 0; l < 33; l++) {
+    // flat tables in level order (the chunks of a level are consecutive)
+    out.copy.clear(); out.avg.clear(); out.interp.clear(); out.phys.clear(); out.ti.clear();
+    for (int l = 0, c = 0, ci = 0; l < 33; l++) {
         out.copy_off[l] = (int)out.copy.size();
         out.avg_off[l] = (int)out.avg.size();
-        if (l < nlev) {
-            out.copy.insert(out.copy.end(), w.copy[l].begin(), w.copy[l].end());
-            out.avg.insert(out.avg.end(), w.avg[l].begin(), w.avg[l].end());
+        out.phys_off[l] = (int)out.phys.size();
+        out.ti_off[l] = (int)out.ti.size();
+        out.interp_off[l] = (int)out.interp.size();
+        for (; c < npch && pch[c].l == l; c++) {
+            out.copy.insert(out.copy.end(), w.copy[c].begin(), w.copy[c].end());
+            out.avg.insert(out.avg.end(), w.avg[c].begin(), w.avg[c].end());
+            out.phys.insert(out.phys.end(), w.phys[c].begin(), w.phys[c].end());
+            out.ti.insert(out.ti.end(), w.ti[c].begin(), w.ti[c].end());
         }
+        for (; ci < nchunk && chunks[ci].l == l; ci++)
+            out.interp.insert(out.interp.end(), w.interp[ci].begin(), w.interp[ci].end());
     }
     out.copy_off[33] = (int)out.copy.size();
     out.avg_off[33] = (int)out.avg.size();
-    for (int l = 0, c = 0; l < 33; l++) {
-        out.interp_off[l] = (int)out.interp.size();
-        for (; c < nchunk && chunks[c].l == l; c++) out.interp.insert(out.interp.end(), w.interp[c].begin(), w.interp[c].end());
-    }
-    out.interp_off[33] = (int)out.interp.size();
-
-    out.phys.clear(); out.ti.clear();
-    out.sync.assign((size_t)np * SYNC_SLOTS, SyncOp{0, 0, 0, 0, 0, SYNC_NONE, {0, 0}});
-    for (int l = 0; l < 33; l++) {
-        const int p0 = f.lev_off[l], p1 = f.lev_off[l + 1];
-        out.phys_off[l] = (int)out.phys.size();
-        out.ti_off[l] = (int)out.ti.size();
-        if (p0 == p1) continue;
-        // ---- setphysical: clawpack46_bc2_default with chains resolved per patch ----
-        {
-            std::vector<int> wsrc(nxy, -1), wneg(nxy, 0), wconst(nxy, 0);
-            for (int ip = p0; ip < p1; ip++) {
-                const PatchInfo& P = f.p[ip];
-                if (!(P.phys[0] || P.phys[1] || P.phys[2] || P.phys[3])) continue;
-                // written cell -> (source cell, negate mask), within this bc2 call;
-                // indexed by the plane-0 offset of the cell inside the patch
-                const int base = T.cell(ip, 1 - mbc, 1 - mbc);
-                std::fill(wsrc.begin(), wsrc.end(), -1);
-                std::vector<int> order;
-                auto put = [&](int di, int dj, int si, int sj, int neg) {
-                    const int dst = T.cell(ip, di, dj);
-                    int src = T.cell(ip, si, sj), cst = 0;
-                    if (wsrc[src - base] >= 0) { neg ^= wneg[src - base]; cst = wconst[src - base]; src = wsrc[src - base]; }
-                    if (wsrc[dst - base] < 0) order.push_back(dst);
-                    wsrc[dst - base] = src;
-                    wneg[dst - base] = neg;
-                    wconst[dst - base] = cst;
-                };
-                auto put_const = [&](int di, int dj) {
-                    const int dst = T.cell(ip, di, dj);
-                    if (wsrc[dst - base] < 0) order.push_back(dst);
-                    wsrc[dst - base] = dst;
-                    wneg[dst - base] = 0;
-                    wconst[dst - base] = 1;
-                };
-                const int NEG2 = 1 << 1, NEG3 = 1 << 2;   // field 2 (x momentum) / field 3 (y momentum)
-                int bc[4];
-                for (int k = 0; k < 4; k++) bc[k] = P.phys[k] ? mthbc[k] : -1;
-                if (bc[0] == 0 && inflow) for (int ibc = 1; ibc <= mbc; ibc++) for (int j = 1 - mbc; j <= my + mbc; j++) put_const(1 - ibc, j);
-                if (bc[0] == 1) for (int ibc = 1; ibc <= mbc; ibc++) for (int j = 1 - mbc; j <= my + mbc; j++) put(1 - ibc, j, 1, j, 0);
-                if (bc[0] == 3) for (int ibc = 1; ibc <= mbc; ibc++) for (int j = 1 - mbc; j <= my + mbc; j++) put(1 - ibc, j, ibc, j, NEG2);
-                if (bc[1] == 1) for (int ibc = 1; ibc <= mbc; ibc++) for (int j = 1 - mbc; j <= my + mbc; j++) put(mx + ibc, j, mx, j, 0);
-                if (bc[1] == 3) for (int ibc = 1; ibc <= mbc; ibc++) for (int j = 1 - mbc; j <= my + mbc; j++) put(mx + ibc, j, mx + 1 - ibc, j, NEG2);
-                if (bc[2] == 1) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, 1 - jbc, i, 1, 0);
-                if (bc[2] == 3) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, 1 - jbc, i, jbc, NEG3);
-                if (bc[3] == 1) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, my + jbc, i, my, 0);
-                if (bc[3] == 3) for (int jbc = 1; jbc <= mbc; jbc++) for (int i = 1 - mbc; i <= mx + mbc; i++) put(i, my + jbc, i, my + 1 - jbc, NEG3);
-                for (int dst : order) out.phys.push_back({dst, wsrc[dst - base], wneg[dst - base], wconst[dst - base]});
-            }
-        }
-        // ---- time interpolation patches ----
-        for (int ip = p0; ip < p1; ip++) if (f.p[ip].has_fine_nbr) out.ti.push_back(ip);
-        // ---- time sync ops ----
-        // fclaw2d_time_sync applies the same-size corrections of every synced level,
-        // then the fine-to-coarse ones (src/fclaw2d_time_sync.c:118-202); each
-        // correction adds to cells of its own patch p only and reads registers no
-        // correction writes, so per patch the samesize ops (faces 0..3) followed by
-        // the f2c ops ((face, igrid) order) give every cell its additions in the
-        // reference's order.  Levels without finer neighbours have no f2c ops, so
-        // one range of levels [a, maxlevel] covers both kinds.  A patch has at most
-        // eight ops (one samesize or two f2c per face): slots 8 p .. 8 p + 7.
-        for (int ip = p0; ip < p1; ip++) {
-            const PatchInfo& P = f.p[ip];
-            SyncOp* slot = &out.sync[(size_t)ip * SYNC_SLOTS];
-            int nops = 0;
-            for (int fc = 0; fc < 4; fc++)
-                if (P.face_type[fc] == NB_SAME && (!f.sphere() || f.p[P.face_nbr[fc][0]].block == P.block))
-                    slot[nops++] = {ip, P.face_nbr[fc][0], fc, 0, 0, SYNC_SAMESIZE, {0, 0}};
-            for (int fc = 0; fc < 4; fc++) {
-                if (P.face_type[fc] != NB_HALF) continue;
-                if (f.sphere() && f.p[P.face_nbr[fc][0]].block != P.block) continue;
-                for (int ig = 0; ig < 2; ig++) {
-                    const int fi = P.face_nbr[fc][ig];
-                    const PatchInfo& F = f.p[fi];
-                    const int noff = (fc < 2) ? (2 * P.gy - F.gy) * my : (2 * P.gx - F.gx) * mx;
-                    slot[nops++] = {ip, fi, fc, ig, noff, SYNC_F2C, {0, 0}};
-                }
-            }
-        }
-    }
     out.phys_off[33] = (int)out.phys.size();
     out.ti_off[33] = (int)out.ti.size();
+    out.interp_off[33] = (int)out.interp.size();
     if (!tables_in_bounds(out, (long)np * nq)) {
         err = "a ghost-fill table indexes outside the patches (bad transform)";
         return false;

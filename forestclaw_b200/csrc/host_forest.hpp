@@ -180,7 +180,9 @@ struct Tables {
 // (x, y) -> (ci + ii x + ij y, cj + ji x + jj y).
 struct InterpOp { int cp, fp, region, pad; long ci, cj, ii, ij, ji, jj; };
 struct TableWork {
-    std::vector<std::vector<FillOp>> copy, avg;            // region ops per level
+    std::vector<std::vector<FillOp>> copy, avg;            // region ops per chunk of patches
+    std::vector<std::vector<PhysEnt>> phys;                // physical-BC entries per chunk of patches
+    std::vector<std::vector<int>> ti;                      // time-interpolation patches per chunk
     std::vector<std::vector<InterpOp>> iops;               // interpolation ops per coarse level, by fine patch
     std::vector<std::vector<int>> iop_first;               // per coarse level: CSR offsets over its fine patches
     std::vector<std::vector<InterpEnt>> interp;            // interpolation entries per task
