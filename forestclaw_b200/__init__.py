@@ -225,6 +225,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_mlp_train": [P, I, I, ctypes.c_float, ctypes.c_ulonglong, dp],
         "fc2d_b200_mlp_gradient": [P, fp, fp, I, fp, dp],
         "fc2d_b200_mlp_predict": [P, fp, I, fp],
+        "fc2d_b200_mlp_set_tensor_form": [P, I],
         "fc2d_b200_mlp_newton_histogram": [P, I, ctypes.POINTER(ctypes.c_longlong)],
         "fc2d_b200_sample_interfaces": [P, I, ctypes.c_ulonglong, dp],
         "fc2d_b200_set_pstar_seed": [P, P],
@@ -403,6 +404,10 @@ class PStarMLP:
         Y = np.zeros(len(X), np.float32)
         self._check("fc2d_b200_mlp_predict", self.lib.fc2d_b200_mlp_predict(self.h, _fp(X), len(X), _fp(Y)))
         return Y
+
+    def set_tensor_form(self, tcgen05: bool) -> None:
+        """Batched evaluation on the tcgen05 tensor cores (default) or in the per-warp mma.sync form."""
+        self._check("fc2d_b200_mlp_set_tensor_form", self.lib.fc2d_b200_mlp_set_tensor_form(self.h, int(tcgen05)))
 
     def newton_histogram(self, use_mlp: bool) -> np.ndarray:
         h = (ctypes.c_longlong * 32)()

@@ -35,6 +35,7 @@ CU_UNITS = {
     "k_metric.cu": ["-fmad=false"],
     "k_output.cu": ["-fmad=false"],
     "k_mlp.cu": [],
+    "k_mlp_tc.cu": [],
     "k_step2_f32w_adv.cu": ["--use_fast_math"],
     "k_step2_f32w_sw.cu": ["--use_fast_math"],
     "k_step2_f32w_euler.cu": ["--use_fast_math"],

@@ -70,6 +70,7 @@ struct StepParams {
 enum { STATUS_NEWTON = 1,       // exact Euler: Newton did not converge from the seed nor from PVRS
        STATUS_DEPTH = 2,        // shallow water: negative depth in a patch
        STATUS_NONFINITE = 4,    // a non-finite value in q
-       STATUS_STAGING = 8 };    // a patch's asynchronous copy into shared memory did not arrive
+       STATUS_STAGING = 8,      // a patch's asynchronous copy into shared memory did not arrive
+       STATUS_TENSOR = 16 };    // a tensor-core MMA of the batched network evaluation did not complete
 
 }  // namespace fcb

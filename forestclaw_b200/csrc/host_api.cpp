@@ -2253,7 +2253,29 @@ struct fc2d_b200_mlp {
     int n = 0, cap = 0;
     int step = 0;
     double gamma = 1.4, tol = 1e-12;
+    int tensor_form = 1;                 // batched evaluation: 1 tcgen05 tiles, 0 per-warp mma.sync
+    unsigned* status = nullptr;          // STATUS_TENSOR of the tcgen05 evaluation (device)
 };
+
+// The network on n states: tcgen05 tiles of 128 states (default) or the per-warp form
+// the solver uses.  The caller synchronises the stream, then checks mlp_status.
+static void mlp_eval(fc2d_b200_mlp* m, const float* X, int n, float* Y)
+{
+    if (m->tensor_form) {
+        cudaMemsetAsync(m->status, 0, sizeof(unsigned), m->st);
+        launch_mlp_predict_tc(X, n, m->blob, Y, m->status, m->st);
+    } else {
+        launch_mlp_predict(X, n, m->blob, Y, m->st);
+    }
+}
+static int mlp_status(fc2d_b200_mlp* m)
+{
+    if (!m->tensor_form) return 0;
+    unsigned st = 0;
+    CK(cudaMemcpy(&st, m->status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (st & STATUS_TENSOR) return fail(FC2D_B200_EDEVICE, "device status: a tensor-core MMA of the network did not complete");
+    return 0;
+}
 
 static unsigned long long host_splitmix(unsigned long long& s)
 {
@@ -2288,6 +2310,9 @@ extern "C" int fc2d_b200_mlp_create(int device, unsigned long long seed, fc2d_b2
     m->device = device;
     CK(cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking));
     CK(mlp_setup());
+    CK(mlp_tc_setup());
+    CK(cudaMalloc(&m->status, sizeof(unsigned)));
+    CK(cudaMemset(m->status, 0, sizeof(unsigned)));
     CK(cudaMalloc(&m->prm, sizeof(float) * MLP_NPARAM));
     CK(cudaMalloc(&m->grad, sizeof(float) * MLP_NPARAM));
     CK(cudaMalloc(&m->m, sizeof(float) * MLP_NPARAM));
@@ -2321,7 +2346,7 @@ extern "C" int fc2d_b200_mlp_destroy(fc2d_b200_mlp_t* m)
     cudaStreamSynchronize(m->st);
     for (void* p : {(void*)m->prm, (void*)m->grad, (void*)m->m, (void*)m->v, m->blob, (void*)m->partial,
                     (void*)m->loss_partial, (void*)m->loss_dev, (void*)m->prim, (void*)m->X, (void*)m->Y,
-                    (void*)m->Yp, (void*)m->idx, (void*)m->iters})
+                    (void*)m->Yp, (void*)m->idx, (void*)m->iters, (void*)m->status})
         if (p) cudaFree(p);
     cudaStreamDestroy(m->st);
     delete m;
@@ -2465,11 +2490,11 @@ extern "C" int fc2d_b200_mlp_predict(fc2d_b200_mlp_t* m, const float* X, int n, 
     CK(cudaMalloc(&Xd, sizeof(float) * MLP_IN * (size_t)n));
     CK(cudaMalloc(&Yd, sizeof(float) * (size_t)n));
     CK(cudaMemcpyAsync(Xd, X, sizeof(float) * MLP_IN * (size_t)n, cudaMemcpyHostToDevice, m->st));
-    launch_mlp_predict(Xd, n, m->blob, Yd, m->st);
+    mlp_eval(m, Xd, n, Yd);
     CK(cudaMemcpyAsync(Y, Yd, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, m->st));
     CK(cudaStreamSynchronize(m->st));
     cudaFree(Xd); cudaFree(Yd);
-    return 0;
+    return mlp_status(m);
 }
 
 extern "C" int fc2d_b200_mlp_newton_histogram(fc2d_b200_mlp_t* m, int use_mlp, long long* hist)
@@ -2477,13 +2502,24 @@ extern "C" int fc2d_b200_mlp_newton_histogram(fc2d_b200_mlp_t* m, int use_mlp, l
     DeviceScope dev_scope_(m ? m->device : -1);
     if (!m || !hist || m->n <= 0) return fail(FC2D_B200_ESTATE, "no data");
     CK(cudaSetDevice(m->device));
-    if (use_mlp) launch_mlp_predict(m->X, m->n, m->blob, m->Yp, m->st);
+    if (use_mlp) mlp_eval(m, m->X, m->n, m->Yp);
     launch_mlp_newton_iters(m->prim, m->X, use_mlp ? m->Yp : nullptr, m->n, m->gamma, m->tol, m->iters, m->st);
     std::vector<int> it(m->n);
     CK(cudaMemcpyAsync(it.data(), m->iters, sizeof(int) * (size_t)m->n, cudaMemcpyDeviceToHost, m->st));
     CK(cudaStreamSynchronize(m->st));
+    if (use_mlp) {
+        const int rc = mlp_status(m);
+        if (rc) return rc;
+    }
     for (int k = 0; k < 32; k++) hist[k] = 0;
     for (int v : it) hist[v < 31 ? v : 31]++;
+    return 0;
+}
+
+extern "C" int fc2d_b200_mlp_set_tensor_form(fc2d_b200_mlp_t* m, int tcgen05)
+{
+    if (!m) return fail(FC2D_B200_EINVAL, "null network");
+    m->tensor_form = tcgen05 != 0;
     return 0;
 }
 

@@ -154,6 +154,10 @@ void launch_mlp_step(const float* X, const float* Y, const int* idx, int nb, voi
                      float* m, float* v, float* partial, float* loss_partial, float* loss, float lr, int step,
                      bool update, cudaStream_t st);
 void launch_mlp_predict(const float* X, int n, const void* blob, float* Y, cudaStream_t st);
+// the same evaluation on the tcgen05 tensor cores, 128 states per CTA (k_mlp_tc.cu); a
+// tile whose MMAs do not complete sets STATUS_TENSOR in *status and writes nothing
+cudaError_t mlp_tc_setup();
+void launch_mlp_predict_tc(const float* X, int n, const void* blob, float* Y, unsigned* status, cudaStream_t st);
 void launch_mlp_newton_iters(const double* prim, const float* X, const float* Yseed, int n, double gam, double tol,
                              int* iters, cudaStream_t st);
 void launch_sample_interfaces(const Dims& d, const double* q, int np, double gam, unsigned long long seed, int n,

@@ -431,6 +431,12 @@ int fc2d_b200_mlp_train(fc2d_b200_mlp_t* m, int epochs, int batch, float lr, uns
 int fc2d_b200_mlp_gradient(fc2d_b200_mlp_t* m, const float* X, const float* Y, int n, float* grad, double* loss);
 /* The deployed forward (approximate tanh, as inside the solver). */
 int fc2d_b200_mlp_predict(fc2d_b200_mlp_t* m, const float* X, int n, float* Y);
+/* Batched evaluation (fc2d_b200_mlp_predict, fc2d_b200_mlp_newton_histogram): tcgen05 = 1
+ * (default) runs tiles of 128 states on the tcgen05 tensor cores (accumulators in tensor
+ * memory), 0 the per-warp mma.sync form the solver's update uses for its 32 interfaces;
+ * the two agree to FP32 rounding.  A tensor-core tile that does not complete returns
+ * FC2D_B200_EDEVICE. */
+int fc2d_b200_mlp_set_tensor_form(fc2d_b200_mlp_t* m, int tcgen05);
 /* Newton-iteration histogram over the training set from the PVRS (0) or network (1) start. */
 int fc2d_b200_mlp_newton_histogram(fc2d_b200_mlp_t* m, int use_mlp, long long* hist32);
 /* Uniform sample of n normal-direction interfaces of the solver's forest (Euler). */

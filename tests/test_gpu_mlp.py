@@ -42,6 +42,28 @@ def test_forward_matches_oracle():
     m.close()
 
 
+@pytest.mark.parametrize("n", [1, 127, 128, 1000, 70001])
+def test_tensor_memory_form_matches_warp_form(n):
+    """The batched evaluation on tcgen05 (128-state tiles, FP32 accumulators in tensor
+    memory; partial last tile) against the per-warp mma.sync form the solver uses and
+    against the NumPy restatement: the same BF16 network, sums in another order."""
+    import forestclaw_b200 as fb
+    m = fb.PStarMLP(seed=3)
+    X, _ = mlp_ref.features(_random_states(np.random.default_rng(n), n))
+    X = X.astype(np.float32)
+    y_tc = m.predict(X)
+    m.set_tensor_form(False)
+    y_w = m.predict(X)
+    m.set_tensor_form(True)
+    yr, _ = mlp_ref.forward(m.params.astype(np.float64), X, bf=True)
+    scale = 1 + np.abs(yr).max()
+    assert np.all(np.isfinite(y_tc))
+    assert np.abs(y_tc - y_w).max() <= 5e-3 * scale, np.abs(y_tc - y_w).max()
+    assert np.abs(y_tc - y_w).mean() <= 2e-4 * scale
+    assert np.abs(y_tc - yr).max() <= 5e-3 * scale
+    m.close()
+
+
 def test_gradient_matches_oracle():
     import forestclaw_b200 as fb
     m = fb.PStarMLP(seed=2)
