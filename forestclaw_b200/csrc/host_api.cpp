@@ -2258,19 +2258,23 @@ struct fc2d_b200_mlp {
 };
 
 // The network on n states: tcgen05 tiles of 128 states (default) or the per-warp form
-// the solver uses.  The caller synchronises the stream, then checks mlp_status.
+// the solver uses.  The caller clears the status word first (mlp_clear) and checks it
+// after synchronising the stream (mlp_status).
 static void mlp_eval(fc2d_b200_mlp* m, const float* X, int n, float* Y)
 {
     if (m->tensor_form) {
-        cudaMemsetAsync(m->status, 0, sizeof(unsigned), m->st);
         launch_mlp_predict_tc(X, n, m->blob, Y, m->status, m->st);
     } else {
         launch_mlp_predict(X, n, m->blob, Y, m->st);
     }
 }
+static int mlp_clear(fc2d_b200_mlp* m)
+{
+    CK(cudaMemsetAsync(m->status, 0, sizeof(unsigned), m->st));
+    return 0;
+}
 static int mlp_status(fc2d_b200_mlp* m)
 {
-    if (!m->tensor_form) return 0;
     unsigned st = 0;
     CK(cudaMemcpy(&st, m->status, sizeof(unsigned), cudaMemcpyDeviceToHost));
     if (st & STATUS_TENSOR) return fail(FC2D_B200_EDEVICE, "device status: a tensor-core MMA of the network did not complete");
@@ -2438,11 +2442,13 @@ extern "C" int fc2d_b200_mlp_train(fc2d_b200_mlp_t* m, int epochs, int batch, fl
             std::swap(perm[i], perm[j]);
         }
         CK(cudaMemcpyAsync(m->idx, perm.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, m->st));
+        rc = mlp_clear(m);
+        if (rc) return rc;
         for (int b = 0; b < nsteps; b++) {
             const int nb = std::min(batch, n - b * batch);
             m->step++;
             launch_mlp_step(m->X, m->Y, m->idx + (size_t)b * batch, nb, m->blob, m->prm, m->grad, m->m, m->v,
-                            m->partial, m->loss_partial, losses + b, lr, m->step, true, m->st);
+                            m->partial, m->loss_partial, losses + b, lr, m->step, true, m->status, m->st);
         }
         CK(cudaGetLastError());
         std::vector<float> l(nsteps);
@@ -2451,6 +2457,8 @@ extern "C" int fc2d_b200_mlp_train(fc2d_b200_mlp_t* m, int epochs, int batch, fl
         double sum = 0.0;
         for (int b = 0; b < nsteps; b++) sum += l[b] * std::min(batch, n - b * batch);
         last = sum / n;
+        rc = mlp_status(m);
+        if (rc) { cudaFree(losses); return rc; }
     }
     cudaFree(losses);
     if (loss_out) *loss_out = last;
@@ -2470,15 +2478,17 @@ extern "C" int fc2d_b200_mlp_gradient(fc2d_b200_mlp_t* m, const float* X, const 
     CK(cudaMalloc(&Yd, sizeof(float) * (size_t)n));
     CK(cudaMemcpyAsync(Xd, X, sizeof(float) * MLP_IN * (size_t)n, cudaMemcpyHostToDevice, m->st));
     CK(cudaMemcpyAsync(Yd, Y, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, m->st));
+    rc = mlp_clear(m);
+    if (rc) return rc;
     launch_mlp_step(Xd, Yd, nullptr, n, m->blob, m->prm, m->grad, m->m, m->v, m->partial, m->loss_partial,
-                    m->loss_dev, 0.0f, 1, false, m->st);
+                    m->loss_dev, 0.0f, 1, false, m->status, m->st);
     float l = 0.0f;
     CK(cudaMemcpyAsync(grad, m->grad, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost, m->st));
     CK(cudaMemcpyAsync(&l, m->loss_dev, sizeof(float), cudaMemcpyDeviceToHost, m->st));
     CK(cudaStreamSynchronize(m->st));
     cudaFree(Xd); cudaFree(Yd);
     if (loss) *loss = l;
-    return 0;
+    return mlp_status(m);
 }
 
 extern "C" int fc2d_b200_mlp_predict(fc2d_b200_mlp_t* m, const float* X, int n, float* Y)
@@ -2490,6 +2500,8 @@ extern "C" int fc2d_b200_mlp_predict(fc2d_b200_mlp_t* m, const float* X, int n, 
     CK(cudaMalloc(&Xd, sizeof(float) * MLP_IN * (size_t)n));
     CK(cudaMalloc(&Yd, sizeof(float) * (size_t)n));
     CK(cudaMemcpyAsync(Xd, X, sizeof(float) * MLP_IN * (size_t)n, cudaMemcpyHostToDevice, m->st));
+    int rc = mlp_clear(m);
+    if (rc) return rc;
     mlp_eval(m, Xd, n, Yd);
     CK(cudaMemcpyAsync(Y, Yd, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, m->st));
     CK(cudaStreamSynchronize(m->st));
@@ -2502,7 +2514,11 @@ extern "C" int fc2d_b200_mlp_newton_histogram(fc2d_b200_mlp_t* m, int use_mlp, l
     DeviceScope dev_scope_(m ? m->device : -1);
     if (!m || !hist || m->n <= 0) return fail(FC2D_B200_ESTATE, "no data");
     CK(cudaSetDevice(m->device));
-    if (use_mlp) mlp_eval(m, m->X, m->n, m->Yp);
+    if (use_mlp) {
+        const int rc = mlp_clear(m);
+        if (rc) return rc;
+        mlp_eval(m, m->X, m->n, m->Yp);
+    }
     launch_mlp_newton_iters(m->prim, m->X, use_mlp ? m->Yp : nullptr, m->n, m->gamma, m->tol, m->iters, m->st);
     std::vector<int> it(m->n);
     CK(cudaMemcpyAsync(it.data(), m->iters, sizeof(int) * (size_t)m->n, cudaMemcpyDeviceToHost, m->st));

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "k_mlp.cuh"
+#include "k_tc.cuh"
 #include "kernels.h"
 #include "riemann.cuh"
 
@@ -62,11 +63,90 @@ __global__ void k_mlp_targets(const double* __restrict__ prim, int n, double gam
     if (iters) iters[k] = it & 0xff;
 }
 
+// The training forward of one tile of FB_ROWS rows (row = threadIdx.x holds x) on the
+// tcgen05 tensor cores: H1 and H2 (accurate tanh, FP32) to sH1 / sH2, the output y of the
+// row returned.  ops: 30 KB of shared memory for the operands (16-byte aligned).
+__device__ float mlp_tc_forward(const MlpView& W, const float x[MLP_IN], int row, char* ops,
+                                float (*sH1)[MLP_H + 1], float (*sH2)[MLP_H + 1], unsigned* status)
+{
+    __shared__ unsigned long long s_bar;
+    __shared__ uint32_t s_tmem;
+    constexpr int NCOL = 128;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    char* a1 = ops;                        // 128 x 16 bf16 (kchunks 2)
+    char* b1 = a1 + 4096;                  // 64 x 16
+    char* a2 = b1 + 2048;                  // 128 x 64 (kchunks 8)
+    char* b2 = a2 + 16384;                 // 64 x 64
+    if (warp == 0) tc_alloc(&s_tmem, NCOL);
+    if (tid == 0) tc_bar_init(&s_bar);
+    for (int k = 0; k < 16; k++)
+        *reinterpret_cast<uint16_t*>(a1 + kmajor_off(row, k, 2)) = bf16_bits(k < MLP_IN ? x[k] : 0.0f);
+    const uint16_t* w1 = reinterpret_cast<const uint16_t*>(W.w1);
+    const uint16_t* w2 = reinterpret_cast<const uint16_t*>(W.w2);
+    for (int e = tid; e < 64 * 16; e += FB_THREADS) *reinterpret_cast<uint16_t*>(b1 + kmajor_off(e >> 4, e & 15, 2)) = w1[e];
+    for (int e = tid; e < 64 * 64; e += FB_THREADS) *reinterpret_cast<uint16_t*>(b2 + kmajor_off(e >> 6, e & 63, 8)) = w2[e];
+    tc_publish();
+    const uint32_t tm = s_tmem, lanes = tm + ((uint32_t)(warp * 32) << 16);
+    if (tid == 0) {
+        tc_mma(tm, smem_desc(a1, 256), smem_desc(b1, 256), tc_idesc(FB_ROWS, 64), 0);
+        tc_commit(&s_bar);
+    }
+    bool ok = __syncthreads_and(tc_wait(&s_bar, 0));
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    float y = 0.0f;
+    if (ok) {
+        for (int c0 = 0; c0 < 64; c0 += 16) {
+            float v[16];
+            tc_ld16(lanes + c0, v);
+            for (int k = 0; k < 16; k++) {
+                const float h = mlp_act<false>(v[k] + W.f[MLP_BLOB_F_B1 + c0 + k]);
+                sH1[row][c0 + k] = h;
+                *reinterpret_cast<uint16_t*>(a2 + kmajor_off(row, c0 + k, 8)) = bf16_bits(h);
+            }
+        }
+        tc_publish();
+        if (tid == 0) {
+            for (int kk = 0; kk < 4; kk++)
+                tc_mma(tm + 64, smem_desc(a2 + kk * 256, 1024), smem_desc(b2 + kk * 256, 1024), tc_idesc(FB_ROWS, 64),
+                       kk > 0);
+            tc_commit(&s_bar);
+        }
+        ok = __syncthreads_and(tc_wait(&s_bar, 1));
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    }
+    if (ok) {
+        for (int c0 = 0; c0 < 64; c0 += 16) {
+            float v[16];
+            tc_ld16(lanes + 64 + c0, v);
+            for (int k = 0; k < 16; k++) {
+                const float h = mlp_act<false>(v[k] + W.f[MLP_BLOB_F_B2 + c0 + k]);
+                sH2[row][c0 + k] = h;
+                y = y + W.f[MLP_BLOB_F_W3 + c0 + k] * h;
+            }
+        }
+        y = y + W.f[MLP_BLOB_F_B3];
+    } else {
+        if (tid == 0 && status) atomicOr(status, (unsigned)STATUS_TENSOR);
+        (void)tc_wait(&s_bar, 0);
+        (void)tc_wait(&s_bar, 1);
+        for (int c = 0; c < MLP_H; c++) { sH1[row][c] = 0.0f; sH2[row][c] = 0.0f; }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) tc_dealloc(tm, NCOL);
+    return y;
+}
+
 // ---- forward + backward of one minibatch ---------------------------------------
+// The forward of the CTA's 128 rows runs on the tcgen05 tensor cores (the tiles of
+// k_mlp_tc.cu, with the training's accurate tanh): the BF16 operands sit in the dZ
+// area of shared memory, which the backward uses only afterwards, and the FP32
+// accumulators in 128 TMEM columns.  A commit that does not arrive sets STATUS_TENSOR.
+// The backward is FP32 on the CUDA cores.
 __global__ void __launch_bounds__(FB_THREADS)
 k_mlp_fwdbwd(const float* __restrict__ X, const float* __restrict__ Y, const int* __restrict__ idx, int nb,
              const void* __restrict__ blob, const float* __restrict__ prm, float* __restrict__ partial,
-             float* __restrict__ loss_partial)
+             float* __restrict__ loss_partial, unsigned* __restrict__ status)
 {
     extern __shared__ float fb_smem[];
     float (*sX)[MLP_IN] = reinterpret_cast<float (*)[MLP_IN]>(fb_smem);
@@ -90,20 +170,7 @@ k_mlp_fwdbwd(const float* __restrict__ X, const float* __restrict__ Y, const int
         x[0] = 1.0f; x[1] = 0.0f; x[2] = 1.0f; x[3] = 1.0f; x[4] = 0.0f; x[5] = 1.0f;
     }
     for (int c = 0; c < MLP_IN; c++) sX[row][c] = valid ? x[c] : 0.0f;
-    MlpFrag h1, h2;
-    mlp_warp_hidden<false>(W, x, h1, h2);
-    const float y = mlp_warp_output(W, h2);
-    // activations to shared memory (C-fragment layout -> rows)
-    {
-        const int g = lane >> 2, tt = lane & 3;
-        for (int mt = 0; mt < 2; mt++)
-            for (int nt = 0; nt < 8; nt++)
-                for (int c = 0; c < 4; c++) {
-                    const int rr = warp * 32 + 16 * mt + g + 8 * (c >> 1), col = 8 * nt + 2 * tt + (c & 1);
-                    sH1[rr][col] = h1.h[mt][nt][c];
-                    sH2[rr][col] = h2.h[mt][nt][c];
-                }
-    }
+    const float y = mlp_tc_forward(W, x, row, reinterpret_cast<char*>(sD), sH1, sH2, status);
     const float e = valid ? (y - t) : 0.0f;
     sdy[row] = 2.0f * e / (float)nb;
     // loss partial (sum of e^2 / nb over the CTA)
@@ -293,10 +360,10 @@ void launch_mlp_targets(const double* prim, int n, double gam, double tol, float
 int mlp_fwdbwd_blocks(int nb) { return nblk(nb, FB_ROWS); }
 void launch_mlp_step(const float* X, const float* Y, const int* idx, int nb, void* blob, float* prm, float* grad,
                      float* m, float* v, float* partial, float* loss_partial, float* loss, float lr, int step,
-                     bool update, cudaStream_t st)
+                     bool update, unsigned* status, cudaStream_t st)
 {
     const int nb_blk = nblk(nb, FB_ROWS);
-    k_mlp_fwdbwd<<<nb_blk, FB_THREADS, FB_SMEM, st>>>(X, Y, idx, nb, blob, prm, partial, loss_partial);
+    k_mlp_fwdbwd<<<nb_blk, FB_THREADS, FB_SMEM, st>>>(X, Y, idx, nb, blob, prm, partial, loss_partial, status);
     k_mlp_reduce<<<nblk(MLP_NPARAM, 256), 256, 0, st>>>(partial, loss_partial, nb_blk, grad, loss);
     if (!update) return;
     const float b1 = 0.9f, b2 = 0.999f;

@@ -21,6 +21,7 @@
 #include <cuda_bf16.h>
 #include "kernels.h"
 #include "k_mlp.cuh"
+#include "k_tc.cuh"
 
 namespace fcb {
 
@@ -28,7 +29,6 @@ namespace {
 
 constexpr int TC_ROWS = 128;                 // states per tile (MMA M)
 constexpr int TC_COLS = 128;                 // TMEM columns: layer 1 at 0, layer 2 at 64
-constexpr int TC_WAIT_LIMIT = 1 << 22;       // mbarrier polls before giving up
 // dynamic shared memory per CTA: the operands need 30 KB; asking for 56 KB keeps at
 // most four CTAs on an SM, so the 4 x 128 TMEM columns they allocate always fit
 constexpr int TC_SMEM = 56 * 1024;
@@ -42,92 +42,6 @@ struct TcSmem {
     unsigned long long bar;                  // MMA completion
     uint32_t tmem;                           // TMEM base written by tcgen05.alloc
 };
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-// byte offset of element (r, k) in a K-major no-swizzle operand with kchunks 8-element
-// chunks of K per row
-__device__ __forceinline__ int kmajor_off(int r, int k, int kchunks)
-{
-    return (r >> 3) * (kchunks * 128) + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2;
-}
-
-// shared memory matrix descriptor: start, leading byte offset 128, stride byte offset
-// sbo, descriptor version 1 (bits 46-47), no swizzle (layout type 0, bits 61-63)
-__device__ __forceinline__ uint64_t smem_desc(const void* base, int sbo)
-{
-    return (uint64_t)((smem_addr(base) & 0x3FFFF) >> 4) | ((uint64_t)(128 >> 4) << 16) |
-           ((uint64_t)((sbo & 0x3FFFF) >> 4) << 32) | (1ull << 46);
-}
-
-// instruction descriptor of kind::f16: D FP32 (bits 4-5 = 1), A and B BF16 (bits 7-9,
-// 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28
-__host__ __device__ constexpr uint32_t tc_idesc(int m, int n)
-{
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
-}
-
-__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, int acc)
-{
-    asm volatile(
-        "{\n\t"
-        ".reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
-        "}\n" ::"r"(d_tmem),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
-}
-
-__device__ __forceinline__ void tc_commit(unsigned long long* bar)
-{
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ bool tc_wait(unsigned long long* bar, unsigned parity)
-{
-    const uint32_t a = smem_addr(bar);
-    for (int it = 0; it < TC_WAIT_LIMIT; it++) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t"
-            ".reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.b32 %0, 1, 0, p;\n\t"
-            "}\n"
-            : "=r"(done)
-            : "r"(a), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
-// 16 FP32 columns of this warp's 32 TMEM lanes (one row per thread)
-__device__ __forceinline__ void tc_ld16(uint32_t taddr, float v[16])
-{
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
-}
-
-__device__ __forceinline__ uint16_t bf16_bits(float x)
-{
-    return __bfloat16_as_ushort(__float2bfloat16_rn(x));
-}
-
-__device__ __forceinline__ float tanh_approx(float z)
-{
-    float r;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(r) : "f"(z));
-    return r;
-}
 
 }  // namespace
 
@@ -164,15 +78,7 @@ k_mlp_predict_tc(const float* __restrict__ X, int n, const void* __restrict__ bl
     for (int e = tid; e < 64 * 64; e += TC_ROWS)
         *reinterpret_cast<uint16_t*>(b2 + kmajor_off(e >> 6, e & 63, 8)) = w2[e];
     for (int e = tid; e < 256; e += TC_ROWS) S.bias[e] = bf[e];
-    // make the generic-proxy writes of shared memory visible to the tensor cores, and
-    // order them (and TMEM use) across the CTA's threads
-    auto publish = [&]() {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    };
-    publish();
+    tc_publish();
     const uint32_t tm = S.tmem;
     const uint32_t lanes = tm + ((uint32_t)(warp * 32) << 16);  // this warp's TMEM lanes
     const int ntiles = (n + TC_ROWS - 1) / TC_ROWS;
@@ -186,7 +92,7 @@ k_mlp_predict_tc(const float* __restrict__ X, int n, const void* __restrict__ bl
             const float x = k >= MLP_IN ? 0.0f : (valid ? X[(size_t)r * MLP_IN + k] : (k == 1 || k == 4 ? 0.0f : 1.0f));
             *reinterpret_cast<uint16_t*>(a1 + kmajor_off(tid, k, 2)) = bf16_bits(x);
         }
-        publish();
+        tc_publish();
         // ---- layer 1: D[0..63] = A1 W1^T (M 128, N 64, K 16) ----
         if (tid == 0) {
             tc_mma(tm, smem_desc(a1, 256), smem_desc(b1, 256), tc_idesc(TC_ROWS, 64), 0);
@@ -203,7 +109,7 @@ k_mlp_predict_tc(const float* __restrict__ X, int n, const void* __restrict__ bl
                 *reinterpret_cast<uint16_t*>(a2 + kmajor_off(tid, c0 + k, 8)) =
                     bf16_bits(tanh_approx(v[k] + S.bias[MLP_BLOB_F_B1 + c0 + k]));
         }
-        publish();
+        tc_publish();
         // ---- layer 2: D[64..127] = A2 W2^T (M 128, N 64, K 64 in four steps of 16) ----
         if (tid == 0) {
             for (int kk = 0; kk < 4; kk++)

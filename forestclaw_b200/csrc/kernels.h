@@ -152,7 +152,7 @@ void launch_mlp_targets(const double* prim, int n, double gam, double tol, float
 int mlp_fwdbwd_blocks(int nb);
 void launch_mlp_step(const float* X, const float* Y, const int* idx, int nb, void* blob, float* prm, float* grad,
                      float* m, float* v, float* partial, float* loss_partial, float* loss, float lr, int step,
-                     bool update, cudaStream_t st);
+                     bool update, unsigned* status, cudaStream_t st);
 void launch_mlp_predict(const float* X, int n, const void* blob, float* Y, cudaStream_t st);
 // the same evaluation on the tcgen05 tensor cores, 128 states per CTA (k_mlp_tc.cu); a
 // tile whose MMAs do not complete sets STATUS_TENSOR in *status and writes nothing
