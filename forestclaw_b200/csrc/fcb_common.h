@@ -27,8 +27,11 @@ enum { PATCH_HAS_FINE_NBR = 1, PATCH_BCC3 = 2 };
 #define MLP_GATE 0.2
 enum { MLP_IN = 6, MLP_H = 64, MLP_NPARAM = 64 * 6 + 64 + 64 * 64 + 64 + 64 + 1 };
 enum { MLP_OFF_W1 = 0, MLP_OFF_B1 = 384, MLP_OFF_W2 = 448, MLP_OFF_B2 = 4544, MLP_OFF_W3 = 4608, MLP_OFF_B3 = 4672 };
+// blob: floats b1 b2 w3 b3 (256 floats), bf16 W1 [64][16] and W2 [64][64] row-major, then
+// W1 and W2 again in the tensor cores' K-major core-matrix order (k_tc.cuh kmajor_off)
 enum { MLP_BLOB_F_B1 = 0, MLP_BLOB_F_B2 = 64, MLP_BLOB_F_W3 = 128, MLP_BLOB_F_B3 = 192,
-       MLP_BLOB_W1_BYTE = 1024, MLP_BLOB_W2_BYTE = 1024 + 64 * 16 * 2, MLP_BLOB_BYTES = 1024 + 64 * 16 * 2 + 64 * 64 * 2 };   // a face or corner neighbour is finer (fclaw2d_patch.c:980-1034)
+       MLP_BLOB_W1_BYTE = 1024, MLP_BLOB_W2_BYTE = 1024 + 64 * 16 * 2, MLP_BLOB_TC_BYTE = 1024 + 64 * 16 * 2 + 64 * 64 * 2,
+       MLP_BLOB_TC_LEN = 64 * 16 * 2 + 64 * 64 * 2, MLP_BLOB_BYTES = MLP_BLOB_TC_BYTE + MLP_BLOB_TC_LEN };
 
 // Parameters of one level update launch (clawpack46 method flags and the
 // per-step scalars the reference passes through common blocks).

@@ -44,6 +44,16 @@ __global__ void k_mlp_blob(const float* __restrict__ prm, void* __restrict__ blo
         w1[k] = __float2bfloat16_rn(c < MLP_IN ? prm[MLP_OFF_W1 + n * MLP_IN + c] : 0.0f);
     }
     for (int k = threadIdx.x; k < 64 * 64; k += blockDim.x) w2[k] = __float2bfloat16_rn(prm[MLP_OFF_W2 + k]);
+    // the tcgen05 operand copies: W1 (kchunks 2) then W2 (kchunks 8)
+    char* tc = reinterpret_cast<char*>(blob) + MLP_BLOB_TC_BYTE;
+    for (int k = threadIdx.x; k < 64 * 16; k += blockDim.x) {
+        const int n = k / 16, c = k % 16;
+        *reinterpret_cast<__nv_bfloat16*>(tc + kmajor_off(n, c, 2)) =
+            __float2bfloat16_rn(c < MLP_IN ? prm[MLP_OFF_W1 + n * MLP_IN + c] : 0.0f);
+    }
+    for (int k = threadIdx.x; k < 64 * 64; k += blockDim.x)
+        *reinterpret_cast<__nv_bfloat16*>(tc + 64 * 16 * 2 + kmajor_off(k / 64, k % 64, 8)) =
+            __float2bfloat16_rn(prm[MLP_OFF_W2 + k]);
 }
 
 // ---- targets: exact star pressure of every sample ------------------------------
@@ -73,18 +83,19 @@ __device__ float mlp_tc_forward(const MlpView& W, const float x[MLP_IN], int row
     __shared__ uint32_t s_tmem;
     constexpr int NCOL = 128;
     const int tid = threadIdx.x, warp = tid >> 5;
-    char* a1 = ops;                        // 128 x 16 bf16 (kchunks 2)
-    char* b1 = a1 + 4096;                  // 64 x 16
-    char* a2 = b1 + 2048;                  // 128 x 64 (kchunks 8)
-    char* b2 = a2 + 16384;                 // 64 x 64
+    char* b1 = ops;                        // 64 x 16 bf16 (kchunks 2)
+    char* b2 = b1 + 2048;                  // 64 x 64 (kchunks 8)
+    char* a1 = b2 + 8192;                  // 128 x 16
+    char* a2 = a1 + 4096;                  // 128 x 64
     if (warp == 0) tc_alloc(&s_tmem, NCOL);
     if (tid == 0) tc_bar_init(&s_bar);
     for (int k = 0; k < 16; k++)
         *reinterpret_cast<uint16_t*>(a1 + kmajor_off(row, k, 2)) = bf16_bits(k < MLP_IN ? x[k] : 0.0f);
-    const uint16_t* w1 = reinterpret_cast<const uint16_t*>(W.w1);
-    const uint16_t* w2 = reinterpret_cast<const uint16_t*>(W.w2);
-    for (int e = tid; e < 64 * 16; e += FB_THREADS) *reinterpret_cast<uint16_t*>(b1 + kmajor_off(e >> 4, e & 15, 2)) = w1[e];
-    for (int e = tid; e < 64 * 64; e += FB_THREADS) *reinterpret_cast<uint16_t*>(b2 + kmajor_off(e >> 6, e & 63, 8)) = w2[e];
+    {   // W1 | W2 in core-matrix order, 16 bytes per load
+        const uint4* src = reinterpret_cast<const uint4*>(reinterpret_cast<const char*>(W.f) + MLP_BLOB_TC_BYTE);
+        uint4* dst = reinterpret_cast<uint4*>(b1);
+        for (int e = tid; e < MLP_BLOB_TC_LEN / 16; e += FB_THREADS) dst[e] = src[e];
+    }
     tc_publish();
     const uint32_t tm = s_tmem, lanes = tm + ((uint32_t)(warp * 32) << 16);
     if (tid == 0) {

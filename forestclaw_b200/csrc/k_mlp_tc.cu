@@ -34,10 +34,10 @@ constexpr int TC_COLS = 128;                 // TMEM columns: layer 1 at 0, laye
 constexpr int TC_SMEM = 56 * 1024;
 
 struct TcSmem {
-    uint16_t a1[TC_ROWS * 16];               // states, bf16          (kchunks 2)
     uint16_t b1[64 * 16];                    // W1 [n][k]             (kchunks 2)
+    uint16_t b2[64 * 64];                    // W2 [n][k]             (kchunks 8), right after W1
+    uint16_t a1[TC_ROWS * 16];               // states, bf16          (kchunks 2)
     uint16_t a2[TC_ROWS * 64];               // layer-1 activations   (kchunks 8)
-    uint16_t b2[64 * 64];                    // W2 [n][k]             (kchunks 8)
     float bias[256];                         // b1, b2, w3, b3
     unsigned long long bar;                  // MMA completion
     uint32_t tmem;                           // TMEM base written by tcgen05.alloc
@@ -67,16 +67,15 @@ k_mlp_predict_tc(const float* __restrict__ X, int n, const void* __restrict__ bl
     }
     // ---- the weights and biases, once ----
     const float* bf = reinterpret_cast<const float*>(blob);
-    const uint16_t* w1 = reinterpret_cast<const uint16_t*>(reinterpret_cast<const char*>(blob) + MLP_BLOB_W1_BYTE);
-    const uint16_t* w2 = reinterpret_cast<const uint16_t*>(reinterpret_cast<const char*>(blob) + MLP_BLOB_W2_BYTE);
     char* a1 = reinterpret_cast<char*>(S.a1);
     char* a2 = reinterpret_cast<char*>(S.a2);
     char* b1 = reinterpret_cast<char*>(S.b1);
     char* b2 = reinterpret_cast<char*>(S.b2);
-    for (int e = tid; e < 64 * 16; e += TC_ROWS)
-        *reinterpret_cast<uint16_t*>(b1 + kmajor_off(e >> 4, e & 15, 2)) = w1[e];
-    for (int e = tid; e < 64 * 64; e += TC_ROWS)
-        *reinterpret_cast<uint16_t*>(b2 + kmajor_off(e >> 6, e & 63, 8)) = w2[e];
+    {   // W1 | W2 in core-matrix order (the blob's tensor-core copy), 16 bytes per load
+        const uint4* src = reinterpret_cast<const uint4*>(reinterpret_cast<const char*>(blob) + MLP_BLOB_TC_BYTE);
+        uint4* dst = reinterpret_cast<uint4*>(b1);
+        for (int e = tid; e < MLP_BLOB_TC_LEN / 16; e += TC_ROWS) dst[e] = src[e];
+    }
     for (int e = tid; e < 256; e += TC_ROWS) S.bias[e] = bf[e];
     tc_publish();
     const uint32_t tm = S.tmem;

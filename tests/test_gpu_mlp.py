@@ -42,7 +42,7 @@ def test_forward_matches_oracle():
     m.close()
 
 
-@pytest.mark.parametrize("n", [1, 127, 128, 1000, 70001])
+@pytest.mark.parametrize("n", [1, 127, 128, 1000, 70001, 1 << 20])
 def test_tensor_memory_form_matches_warp_form(n):
     """The batched evaluation on tcgen05 (128-state tiles, FP32 accumulators in tensor
     memory; partial last tile) against the per-warp mma.sync form the solver uses and
