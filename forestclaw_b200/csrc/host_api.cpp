@@ -1825,7 +1825,7 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     }
     launch_repop(d, s->repop_dev.p, (int)ops.size(), s->q, sp.q, s->qlast, sp.qlast, s->qinterp, sp.qinterp, s->regs,
                  sp.regs, s->sphere ? s->area : nullptr, s->sphere ? sp.area : nullptr, s->st);
-    CK(cudaStreamSynchronize(s->st));
+    CK(cudaGetLastError());       // the repopulation runs while the host builds the tables below
     std::swap(s->q, sp.q); std::swap(s->qlast, sp.qlast); std::swap(s->qinterp, sp.qinterp);
     std::swap(s->aux, sp.aux); std::swap(s->regs, sp.regs); std::swap(s->desc, sp.desc);
     std::swap(s->area, sp.area);
