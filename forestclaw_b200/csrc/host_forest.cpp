@@ -88,6 +88,20 @@ const CSTable& cs_table()
     static const CSTable t;
     return t;
 }
+// Runs tasks 0..n-1 on up to nt threads (the calling one included).
+template <class Fn>
+void run_tasks(int n, int nt, Fn fn)
+{
+    nt = std::max(1, std::min(nt, n));
+    if (nt == 1) { for (int i = 0; i < n; i++) fn(i); return; }
+    std::atomic<int> next{0};
+    auto loop = [&]() { for (int i; (i = next.fetch_add(1)) < n;) fn(i); };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; t++) th.emplace_back(loop);
+    loop();
+    for (auto& x : th) x.join();
+}
+
 }  // namespace
 
 const CSFace& cs_face(int b, int f) { return cs_table().f[b][f]; }
@@ -300,14 +314,18 @@ bool Forest::build(const std::vector<Leaf>& leaves, std::string& err)
 // ---------------------------------------------------------------------------
 // adaptation
 // ---------------------------------------------------------------------------
-std::vector<Leaf> adapt_leaves(const Forest& f, const std::vector<int>& mark, int& changed, std::string& err)
+// The leaves that replace patches list[0..n) of one instance (all patches: list null),
+// 2:1 balanced within the instance (instances never touch one another).
+static std::vector<Leaf> adapt_patches(const Forest& f, const std::vector<int>& mark, const int* list, int n,
+                                       int& changed)
 {
     const int np = f.np();
     std::vector<Leaf> L;
-    L.reserve(np * 2 + 8);
+    L.reserve(n * 2 + 8);
     std::vector<char> done(np, 0);
     changed = 0;
-    for (int i = 0; i < np; i++) {
+    for (int q = 0; q < n; q++) {
+        const int i = list ? list[q] : q;
         if (done[i]) continue;
         const PatchInfo& P = f.p[i];
         if (mark[i] > 0) {
@@ -384,12 +402,32 @@ std::vector<Leaf> adapt_leaves(const Forest& f, const std::vector<int>& mark, in
         L.swap(M);
     }
     if (!changed) {
-        bool same = ((int)L.size() == np);
+        bool same = ((int)L.size() == n);
         for (size_t i = 0; same && i < L.size(); i++)
             if (f.lookup(L[i].inst, L[i].level, L[i].gx, L[i].gy) < 0) same = false;
         if (!same) changed = 1;
     }
+    return L;
+}
+
+std::vector<Leaf> adapt_leaves(const Forest& f, const std::vector<int>& mark, int& changed, std::string& err)
+{
     (void)err;
+    const int ni = f.ninst(), np = f.np();
+    if (ni <= 1) return adapt_patches(f, mark, nullptr, np, changed);
+    // a batch: the instances on threads, their leaves in instance order
+    std::vector<std::vector<int>> list(ni);
+    for (int i = 0; i < np; i++) list[f.p[i].inst].push_back(i);
+    std::vector<std::vector<Leaf>> out(ni);
+    std::vector<int> ch(ni, 0);
+    const int nt = std::max(1, std::min((int)std::thread::hardware_concurrency(), 16));
+    run_tasks(ni, nt, [&](int k) { out[k] = adapt_patches(f, mark, list[k].data(), (int)list[k].size(), ch[k]); });
+    std::vector<Leaf> L;
+    changed = 0;
+    for (int k = 0; k < ni; k++) {
+        L.insert(L.end(), out[k].begin(), out[k].end());
+        changed |= ch[k];
+    }
     return L;
 }
 
@@ -579,20 +617,6 @@ struct TableCtx {
         return {a0, b0, a1 - a0, a2 - a0, b1 - b0, b2 - b0};
     }
 };
-
-// Runs tasks 0..n-1 on up to nt threads (the calling one included).
-template <class Fn>
-void run_tasks(int n, int nt, Fn fn)
-{
-    nt = std::max(1, std::min(nt, n));
-    if (nt == 1) { for (int i = 0; i < n; i++) fn(i); return; }
-    std::atomic<int> next{0};
-    auto loop = [&]() { for (int i; (i = next.fetch_add(1)) < n;) fn(i); };
-    std::vector<std::thread> th;
-    for (int t = 1; t < nt; t++) th.emplace_back(loop);
-    loop();
-    for (auto& x : th) x.join();
-}
 
 }  // namespace
 
