@@ -143,15 +143,21 @@ int Forest::step(int i, int l, int x, int y, int dx, int dy, int& ox, int& oy) c
     return 1;
 }
 
-static uint64_t interleave(uint32_t x, uint32_t y)
+// The bits of v at the even positions of a 64-bit word (binary magic numbers: shift and
+// mask in halving steps).
+static uint64_t spread_bits(uint32_t v)
 {
-    uint64_t r = 0;
-    for (int b = 0; b < 32; b++) {
-        r |= (uint64_t)((x >> b) & 1u) << (2 * b);
-        r |= (uint64_t)((y >> b) & 1u) << (2 * b + 1);
-    }
-    return r;
+    uint64_t x = v;
+    x = (x | (x << 16)) & 0x0000FFFF0000FFFFull;
+    x = (x | (x << 8)) & 0x00FF00FF00FF00FFull;
+    x = (x | (x << 4)) & 0x0F0F0F0F0F0F0F0Full;
+    x = (x | (x << 2)) & 0x3333333333333333ull;
+    x = (x | (x << 1)) & 0x5555555555555555ull;
+    return x;
 }
+
+// Morton (Z-order) key: bit b of x at 2b, bit b of y at 2b + 1.
+static uint64_t interleave(uint32_t x, uint32_t y) { return spread_bits(x) | (spread_bits(y) << 1); }
 
 // p4est brick tree numbering: rank of the block position in Morton order.
 static int brick_block(int mi, int mj, int bx, int by)
@@ -199,28 +205,34 @@ int Forest::lookup(int i, int l, int x, int y) const
 
 bool Forest::build(const std::vector<Leaf>& leaves, std::string& err)
 {
-    std::vector<PatchInfo> q(leaves.size());
-    for (size_t i = 0; i < leaves.size(); i++) {
-        const Leaf& lf = leaves[i];
-        PatchInfo& P = q[i];
-        P = PatchInfo{};
-        P.level = lf.level; P.gx = lf.gx; P.gy = lf.gy; P.inst = lf.inst;
-        if (P.inst < 0 || P.inst >= ninst()) { err = "leaf of an unknown instance"; return false; }
-        geometry(P);
-    }
-    // slot order: level, instance, block, Morton (sorted as indices: the records are large)
-    std::vector<int> ord(q.size());
-    for (size_t i = 0; i < ord.size(); i++) ord[i] = (int)i;
-    std::sort(ord.begin(), ord.end(), [&](int ia, int ib) {
-        const PatchInfo& a = q[ia];
-        const PatchInfo& b = q[ib];
-        if (a.level != b.level) return a.level < b.level;
-        if (a.inst != b.inst) return a.inst < b.inst;
-        if (a.block != b.block) return a.block < b.block;
-        return a.morton < b.morton;
+    const int nl = (int)leaves.size();
+    for (const Leaf& lf : leaves)
+        if (lf.inst < 0 || lf.inst >= ninst()) { err = "leaf of an unknown instance"; return false; }
+    const int nt = std::max(1, std::min((int)std::thread::hardware_concurrency(), 16));
+    constexpr int CH = 1024;                                    // leaves per task
+    const int nch = (nl + CH - 1) / CH;
+    // geometry of every leaf, and its slot key: level, instance, block, Morton
+    struct SlotKey { uint64_t hi, morton; int leaf; };
+    std::vector<PatchInfo>& q = scratch_;
+    q.resize(nl);
+    std::vector<SlotKey> ord(nl);
+    run_tasks(nch, nt, [&](int c) {
+        for (int i = c * CH, e = std::min(nl, i + CH); i < e; i++) {
+            const Leaf& lf = leaves[i];
+            PatchInfo& P = q[i];
+            P = PatchInfo{};
+            P.level = lf.level; P.gx = lf.gx; P.gy = lf.gy; P.inst = lf.inst;
+            geometry(P);
+            ord[i] = {((uint64_t)P.level << 56) | ((uint64_t)P.inst << 28) | (uint64_t)P.block, P.morton, i};
+        }
     });
-    p.resize(q.size());
-    for (size_t i = 0; i < ord.size(); i++) p[i] = q[ord[i]];
+    std::sort(ord.begin(), ord.end(), [](const SlotKey& a, const SlotKey& b) {
+        return a.hi != b.hi ? a.hi < b.hi : a.morton < b.morton;
+    });
+    p.resize(nl);
+    run_tasks(nch, nt, [&](int c) {
+        for (int i = c * CH, e = std::min(nl, i + CH); i < e; i++) p[i] = q[ord[i].leaf];
+    });
     index_.reset(p.size());
     for (int i = 0; i < np(); i++) index_.put(key(p[i].inst, p[i].level, p[i].gx, p[i].gy), i);
     for (int l = 0; l < 34; l++) lev_off[l] = 0;
@@ -293,20 +305,9 @@ bool Forest::build(const std::vector<Leaf>& leaves, std::string& err)
             }
         }
     };
-    const int n = np();
-    int nt = (int)std::thread::hardware_concurrency();
-    nt = std::max(1, std::min(nt, std::min(16, n / 256)));
-    auto chunk = [&](int t) {
-        const int a = (int)((long)n * t / nt), b = (int)((long)n * (t + 1) / nt);
-        for (int ip = a; ip < b; ip++) neighbours(ip);
-    };
-    if (nt == 1) chunk(0);
-    else {
-        std::vector<std::thread> th;
-        for (int t = 1; t < nt; t++) th.emplace_back(chunk, t);
-        chunk(0);
-        for (auto& x : th) x.join();
-    }
+    run_tasks(nch, nt, [&](int c) {
+        for (int ip = c * CH, e = std::min(nl, ip + CH); ip < e; ip++) neighbours(ip);
+    });
     if (unbalanced) { err = "forest is not 2:1 face balanced"; return false; }
     return true;
 }

@@ -124,6 +124,7 @@ public:
 
 private:
     KeyIndex index_;
+    std::vector<PatchInfo> scratch_;   // leaves with their geometry, before the slot order
 };
 
 // Refine marked leaves, coarsen fully marked families, then 2:1 balance
