@@ -621,17 +621,9 @@ struct TableCtx {
 
 }  // namespace
 
-// Every gather index must lie in the q slab: a wrong transform would otherwise send the
-// ghost-fill kernels outside it (copy and average entries are checked as they are made).
-static bool tables_in_bounds(const Tables& T, long nall)
-{
-    auto ok = [&](long k) { return k >= 0 && k < nall; };
-    bool good = true;
-    for (const InterpEnt& e : T.interp) good = good && ok(e.dst) && ok(e.src) && e.sub >= 0 && e.sub < 4;
-    for (const PhysEnt& e : T.phys) good = good && ok(e.dst) && ok(e.src);
-    return good;
-}
-
+// Every gather index must lie in the q slab, or a wrong transform would send the ghost-fill
+// kernels outside it: copy and average ops are checked as they are made, interpolation and
+// physical-BC entries as they are concatenated.
 bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out, TableWork& w, std::string& err)
 {
     TableCtx T(f);
@@ -696,7 +688,7 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out,
     for (int l = 0; l < nlev; l++)
         for (int a = f.lev_off[l]; a < f.lev_off[l + 1]; a += 64) pch.push_back({l, a, std::min(f.lev_off[l + 1], a + 64)});
     w.copy.resize(pch.size()); w.avg.resize(pch.size()); w.phys.resize(pch.size()); w.ti.resize(pch.size());
-    out.sync.assign((size_t)np * SYNC_SLOTS, SyncOp{0, 0, 0, 0, 0, SYNC_NONE, {0, 0}});
+    out.sync.resize((size_t)np * SYNC_SLOTS);           // every slot is written by its patch's task
     auto phys_sync = [&](int c) {
         const int a0 = pch[c].a, a1 = pch[c].b;
         // ---- setphysical: clawpack46_bc2_default with chains resolved per patch ----
@@ -769,6 +761,7 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out,
                     slot[nops++] = {ip, fi, fc, ig, noff, SYNC_F2C, {0, 0}};
                 }
             }
+            for (; nops < SYNC_SLOTS; nops++) slot[nops] = SyncOp{0, 0, 0, 0, 0, SYNC_NONE, {0, 0}};
         }
     };
     auto patches = [&](int c) {
@@ -921,29 +914,47 @@ bool build_tables(const Forest& f, const int mthbc[4], bool inflow, Tables& out,
     });
     if (bad) { err = "a ghost-fill table writes outside its destination patches"; return false; }
 
-    // flat tables in level order (the chunks of a level are consecutive)
-    out.copy.clear(); out.avg.clear(); out.interp.clear(); out.phys.clear(); out.ti.clear();
-    for (int l = 0, c = 0, ci = 0; l < 33; l++) {
-        out.copy_off[l] = (int)out.copy.size();
-        out.avg_off[l] = (int)out.avg.size();
-        out.phys_off[l] = (int)out.phys.size();
-        out.ti_off[l] = (int)out.ti.size();
-        out.interp_off[l] = (int)out.interp.size();
-        for (; c < npch && pch[c].l == l; c++) {
-            out.copy.insert(out.copy.end(), w.copy[c].begin(), w.copy[c].end());
-            out.avg.insert(out.avg.end(), w.avg[c].begin(), w.avg[c].end());
-            out.phys.insert(out.phys.end(), w.phys[c].begin(), w.phys[c].end());
-            out.ti.insert(out.ti.end(), w.ti[c].begin(), w.ti[c].end());
-        }
-        for (; ci < nchunk && chunks[ci].l == l; ci++)
-            out.interp.insert(out.interp.end(), w.interp[ci].begin(), w.interp[ci].end());
+    // flat tables in level order (the chunks of a level are consecutive): each chunk's
+    // place from prefix sums, then the chunks copied there, and their entries checked
+    // against the patches, on the worker threads
+    std::vector<size_t> oc(npch + 1, 0), oa(npch + 1, 0), oph(npch + 1, 0), oti(npch + 1, 0), oi(nchunk + 1, 0);
+    for (int c = 0; c < npch; c++) {
+        oc[c + 1] = oc[c] + w.copy[c].size();
+        oa[c + 1] = oa[c] + w.avg[c].size();
+        oph[c + 1] = oph[c] + w.phys[c].size();
+        oti[c + 1] = oti[c] + w.ti[c].size();
     }
-    out.copy_off[33] = (int)out.copy.size();
-    out.avg_off[33] = (int)out.avg.size();
-    out.phys_off[33] = (int)out.phys.size();
-    out.ti_off[33] = (int)out.ti.size();
-    out.interp_off[33] = (int)out.interp.size();
-    if (!tables_in_bounds(out, (long)np * nq)) {
+    for (int c = 0; c < nchunk; c++) oi[c + 1] = oi[c] + w.interp[c].size();
+    for (int l = 0, c = 0, ci = 0; l < 34; l++) {
+        out.copy_off[l] = (int)oc[c];
+        out.avg_off[l] = (int)oa[c];
+        out.phys_off[l] = (int)oph[c];
+        out.ti_off[l] = (int)oti[c];
+        out.interp_off[l] = (int)oi[ci];
+        while (c < npch && pch[c].l == l) c++;
+        while (ci < nchunk && chunks[ci].l == l) ci++;
+    }
+    // (no clear first: a vector that shrinks or keeps its size is not refilled with zeros)
+    out.copy.resize(oc[npch]); out.avg.resize(oa[npch]); out.phys.resize(oph[npch]); out.ti.resize(oti[npch]);
+    out.interp.resize(oi[nchunk]);
+    const long nall = (long)np * nq;
+    auto in_all = [&](long k) { return k >= 0 && k < nall; };
+    run_tasks(nchunk + npch, nt, [&](int k) {
+        bool good = true;
+        if (k < nchunk) {
+            std::copy(w.interp[k].begin(), w.interp[k].end(), out.interp.begin() + oi[k]);
+            for (const InterpEnt& e : w.interp[k]) good = good && in_all(e.dst) && in_all(e.src) && e.sub >= 0 && e.sub < 4;
+        } else {
+            const int c = k - nchunk;
+            std::copy(w.copy[c].begin(), w.copy[c].end(), out.copy.begin() + oc[c]);
+            std::copy(w.avg[c].begin(), w.avg[c].end(), out.avg.begin() + oa[c]);
+            std::copy(w.phys[c].begin(), w.phys[c].end(), out.phys.begin() + oph[c]);
+            std::copy(w.ti[c].begin(), w.ti[c].end(), out.ti.begin() + oti[c]);
+            for (const PhysEnt& e : w.phys[c]) good = good && in_all(e.dst) && in_all(e.src);
+        }
+        if (!good) bad = 1;
+    });
+    if (bad) {
         err = "a ghost-fill table indexes outside the patches (bad transform)";
         return false;
     }
