@@ -874,32 +874,45 @@ def run_batch(args, wl, rank, world, local_rank):
     nroof = max(2, min(args.steps, 4))
     upd_ms, upd_bytes, upd_launches = _roofline_pass([G["g"] for G in groups], [(0.0, G["dt"]) for G in groups],
                                                      flush, nroof)
-    # ---- end to end: q of every group from pinned host memory and back, every step ----
-    bufs = []
-    for G in groups:
-        g = G["g"]
+    # ---- end to end: q of every group from pinned host memory and back, every step, the
+    # ---- regrids inside (every regrid_interval steps, as in the timed loop) ----
+    def qlen(g):
         o = g.opts
-        nq = g.num_patches * o.meqn * (o.mx + 2 * o.mbc) * (o.my + 2 * o.mbc)
-        hq = torch.empty(nq, dtype=torch.float64, pin_memory=True)
-        g.get_q_ptr(hq.data_ptr())
-        bufs.append(hq)
-    e2e_steps = max(2, min(args.steps, 10))
+        return g.num_patches * o.meqn * (o.mx + 2 * o.mbc) * (o.my + 2 * o.mbc)
+    # pinned buffers with room for twice the current forest (a regrid may grow it)
+    bufs = [torch.empty(2 * qlen(G["g"]), dtype=torch.float64, pin_memory=True) for G in groups]
+    for G, hq in zip(groups, bufs):
+        G["g"].get_q_ptr(hq.data_ptr())
+    interval = wl["regrid_interval"]
+    e2e_steps = max(interval, min(args.steps, 3 * interval))
     torch.cuda.synchronize()
     te0 = time.perf_counter()
-    e2e_cells = 0.0
-    for _ in range(e2e_steps):
+    e2e_cells, nbytes, nbytes_d2h, e2e_regrids = 0.0, 0, 0, 0
+    for k in range(e2e_steps):
         c0 = sum(G["g"].cell_updates for G in groups)
         for G, hq in zip(groups, bufs):
             G["g"].set_q_ptr(hq.data_ptr())
         _batch_step(groups)
         for G, hq in zip(groups, bufs):
             G["g"].get_q_ptr(hq.data_ptr())
+            nbytes += 8 * qlen(G["g"])
         e2e_cells += sum(G["g"].cell_updates for G in groups) - c0
+        if (k + 1) % interval == 0:
+            for j, G in enumerate(groups):
+                G["g"].regrid()
+                # the new forest's data back to the host copy (counted with the step's d2h bytes)
+                if qlen(G["g"]) > bufs[j].numel():      # the forest outgrew the pinned buffer
+                    bufs[j] = torch.empty(2 * qlen(G["g"]), dtype=torch.float64, pin_memory=True)
+                G["g"].get_q_ptr(bufs[j].data_ptr())
+                nbytes_d2h += 8 * qlen(G["g"])
+            e2e_regrids += 1
     e2e_s = ranks.max_over_ranks(time.perf_counter() - te0, "cuda")
     e2e_cells = ranks.sum_over_ranks(e2e_cells, "cuda")
-    nbytes = int(sum(b.numel() for b in bufs) * 8)
-    e2e = {"value": e2e_cells / e2e_s, "unit": "cell-updates/s", "h2d_bytes_per_step": nbytes,
-           "d2h_bytes_per_step": nbytes}
+    e2e = {"value": e2e_cells / e2e_s, "unit": "cell-updates/s", "h2d_bytes_per_step": nbytes // e2e_steps,
+           "d2h_bytes_per_step": (nbytes + nbytes_d2h) // e2e_steps, "steps": e2e_steps, "regrids": e2e_regrids,
+           "protocol": "per coarse step: set_q of every group from pinned host memory, the step, get_q to "
+                       "pinned host memory; the regrid every regrid_interval steps inside the wall-clock "
+                       "region, continuing from the device-timed loop's last state"}
     info = {str(G["mx"]): {"instances": len(G["ids"]), "patches": G["g"].num_patches} for G in groups}
     for G in groups:
         G["g"].close()

@@ -17,6 +17,10 @@
 #include <map>
 #include <thread>
 #include <atomic>
+#include <condition_variable>
+#include <functional>
+#include <memory>
+#include <mutex>
 #include "fcb_sphere.h"
 
 namespace fcb {
@@ -88,18 +92,85 @@ const CSTable& cs_table()
     static const CSTable t;
     return t;
 }
+// Worker threads kept for the life of the process (creating and joining a dozen threads
+// per call cost more than the work of a small forest).  A job is n tasks handed out by a
+// shared counter; the calling thread takes tasks too and returns once all n are done, so
+// a job completes even if no worker wakes (another caller's job in flight, a forked
+// child without the workers).  A worker that wakes after its job is done finds the
+// counter spent and never calls the job's function.
+class TaskPool {
+public:
+    static TaskPool& get()
+    {
+        static TaskPool* pool = new TaskPool();             // never destroyed: its threads stay detached
+        return *pool;
+    }
+    void run(int n, int helpers, const std::function<void(int)>& fn)
+    {
+        auto job = std::make_shared<Job>();
+        job->fn = fn;
+        job->n = n;
+        job->slots = std::min(helpers, nworkers_);
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            cur_ = job;
+            gen_++;
+        }
+        cv_.notify_all();
+        work(*job);
+        std::unique_lock<std::mutex> lk(mu_);
+        done_cv_.wait(lk, [&] { return job->done.load() == n; });
+    }
+
+private:
+    struct Job {
+        std::function<void(int)> fn;
+        int n = 0;
+        std::atomic<int> next{0}, done{0}, slots{0};
+    };
+    TaskPool()
+    {
+        nworkers_ = std::max(0, std::min((int)std::thread::hardware_concurrency(), 16) - 1);
+        for (int t = 0; t < nworkers_; t++) std::thread([this] { loop(); }).detach();
+    }
+    void work(Job& j)
+    {
+        for (int i; (i = j.next.fetch_add(1)) < j.n;) {
+            j.fn(i);
+            if (j.done.fetch_add(1) + 1 == j.n) {
+                std::lock_guard<std::mutex> g(mu_);
+                done_cv_.notify_all();
+            }
+        }
+    }
+    void loop()
+    {
+        unsigned long long seen = 0;
+        for (;;) {
+            std::shared_ptr<Job> job;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return gen_ != seen; });
+                seen = gen_;
+                job = cur_;
+            }
+            if (job->slots.fetch_sub(1) > 0) work(*job);
+        }
+    }
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+    std::shared_ptr<Job> cur_;
+    unsigned long long gen_ = 0;
+    int nworkers_ = 0;
+};
+
 // Runs tasks 0..n-1 on up to nt threads (the calling one included).
 template <class Fn>
 void run_tasks(int n, int nt, Fn fn)
 {
     nt = std::max(1, std::min(nt, n));
     if (nt == 1) { for (int i = 0; i < n; i++) fn(i); return; }
-    std::atomic<int> next{0};
-    auto loop = [&]() { for (int i; (i = next.fetch_add(1)) < n;) fn(i); };
-    std::vector<std::thread> th;
-    for (int t = 1; t < nt; t++) th.emplace_back(loop);
-    loop();
-    for (auto& x : th) x.join();
+    TaskPool::get().run(n, nt - 1, std::function<void(int)>(std::ref(fn)));
 }
 
 }  // namespace
