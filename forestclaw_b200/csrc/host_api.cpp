@@ -106,10 +106,22 @@ struct TableArena {
     char* dev = nullptr;
     char* host = nullptr;
     size_t cap = 0, used = 0;
+    cudaEvent_t copied = nullptr;    // the last upload's copy out of host is done
     ~TableArena()
     {
+        if (copied) cudaEventDestroy(copied);
         if (dev) cudaFree(dev);
         if (host) cudaFreeHost(host);
+    }
+    // before the host buffer is written again: the last upload has left it
+    cudaError_t wait_copied() { return copied ? cudaEventSynchronize(copied) : cudaSuccess; }
+    cudaError_t mark_copied(cudaStream_t st)
+    {
+        if (!copied) {
+            cudaError_t e = cudaEventCreateWithFlags(&copied, cudaEventDisableTiming);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaEventRecord(copied, st);
     }
     cudaError_t reserve(size_t bytes)
     {
@@ -147,6 +159,7 @@ struct fc2d_b200_solver {
     fc2d_b200_options_t o;
     Dims d;
     Forest forest;
+    Forest forest_next;          // a regrid's new forest, swapped with forest (both keep their buffers)
     cudaStream_t st = nullptr;
     double *q = nullptr, *qlast = nullptr, *qinterp = nullptr, *aux = nullptr, *regs = nullptr;
     PatchDesc* desc = nullptr;
@@ -441,6 +454,7 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
     {
         TableArena& A = s->arena;
         auto sz = [](const auto& v) { return TableArena::span(v.size() * sizeof(v[0])); };
+        CK(A.wait_copied());
         CK(A.reserve(sz(hd) + sz(T.copy) + sz(T.avg) + sz(T.interp) + sz(T.phys) + sz(T.ti) + sz(T.sync)));
         A.used = 0;
         const DevView<PatchDesc> dv = A.put(hd);       // staged here, then copied into the slab's descriptors
@@ -452,6 +466,7 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
         s->t_sync = A.put(T.sync);
         if (A.used) CK(cudaMemcpyAsync(A.dev, A.host, A.used, cudaMemcpyHostToDevice, s->st));
         if (dv.n) CK(cudaMemcpyAsync(s->desc, dv.p, dv.n * sizeof(PatchDesc), cudaMemcpyDeviceToDevice, s->st));
+        CK(A.mark_copied(s->st));
     }
     {   // interpolation chains: reads of level l's entries against writes of level l-1's
         std::vector<unsigned char>& written = s->interp_written;
@@ -472,7 +487,8 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
             s->interp_chain[l] = clash ? 0 : 1;
         }
     }
-    CK(cudaStreamSynchronize(s->st));
+    // no wait here: the copies run in stream order ahead of every launch that reads the
+    // tables, and the next upload waits for this one's copy before it refills the buffer
     return 0;
 }
 
@@ -1730,7 +1746,7 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
         int rc = halo_exchange(s, true);
         if (rc) return rc;
     }
-    Forest nf;
+    Forest& nf = s->forest_next;                 // built in place: its buffers stay from the last regrid
     nf.g = f.g;
     nf.inst = f.inst;
     if (!nf.build(L, err)) return fail(FC2D_B200_EFOREST, err);
@@ -1830,7 +1846,7 @@ extern "C" int fc2d_b200_regrid(fc2d_b200_solver_t* s, int* changed_out)
     std::swap(s->aux, sp.aux); std::swap(s->regs, sp.regs); std::swap(s->desc, sp.desc);
     std::swap(s->area, sp.area);
     std::swap(s->cap, sp.cap);
-    s->forest = std::move(nf);
+    std::swap(s->forest, s->forest_next);
     s->forest_gen++;
     invalidate_graph(s);
     const double t_repop = wall_ms();

@@ -280,7 +280,7 @@ bool Forest::build(const std::vector<Leaf>& leaves, std::string& err)
     for (const Leaf& lf : leaves)
         if (lf.inst < 0 || lf.inst >= ninst()) { err = "leaf of an unknown instance"; return false; }
     const int nt = std::max(1, std::min((int)std::thread::hardware_concurrency(), 16));
-    constexpr int CH = 1024;                                    // leaves per task
+    constexpr int CH = 256;                                     // leaves per task
     const int nch = (nl + CH - 1) / CH;
     // geometry of every leaf, and its slot key: level, instance, block, Morton
     struct SlotKey { uint64_t hi, morton; int leaf; };
