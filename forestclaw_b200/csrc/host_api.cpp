@@ -137,17 +137,32 @@ struct TableArena {
         return cudaSuccess;
     }
     static size_t span(size_t bytes) { return (bytes + 255) & ~(size_t)255; }
-    // stage v at the next 256-byte boundary; its device range
+    // place v at the next 256-byte boundary (copied by fill(), so v must live until then);
+    // its device range
     template <class T>
     DevView<T> put(const std::vector<T>& v)
     {
         DevView<T> r;
         r.p = reinterpret_cast<T*>(dev + used);
         r.n = v.size();
-        if (!v.empty()) std::memcpy(host + used, v.data(), v.size() * sizeof(T));
+        if (!v.empty()) pending.push_back({host + used, reinterpret_cast<const char*>(v.data()), v.size() * sizeof(T)});
         used += span(v.size() * sizeof(T));
         return r;
     }
+    // the placed vectors into the host buffer, in pieces on the host worker threads
+    void fill()
+    {
+        constexpr size_t PIECE = 256 << 10;
+        std::vector<Piece> work;
+        for (const Piece& p : pending)
+            for (size_t o = 0; o < p.bytes; o += PIECE) work.push_back({p.dst + o, p.src + o, std::min(PIECE, p.bytes - o)});
+        pending.clear();
+        parallel_for((int)work.size(), [&](int k) { std::memcpy(work[k].dst, work[k].src, work[k].bytes); });
+    }
+
+private:
+    struct Piece { char* dst; const char* src; size_t bytes; };
+    std::vector<Piece> pending;
 };
 
 struct LevelRanges {
@@ -464,6 +479,7 @@ static int upload_desc_and_tables(fc2d_b200_solver* s)
         s->t_phys = A.put(T.phys);
         s->t_ti = A.put(T.ti);
         s->t_sync = A.put(T.sync);
+        A.fill();
         if (A.used) CK(cudaMemcpyAsync(A.dev, A.host, A.used, cudaMemcpyHostToDevice, s->st));
         if (dv.n) CK(cudaMemcpyAsync(s->desc, dv.p, dv.n * sizeof(PatchDesc), cudaMemcpyDeviceToDevice, s->st));
         CK(A.mark_copied(s->st));

@@ -118,6 +118,7 @@ public:
         }
         cv_.notify_all();
         work(*job);
+        for (int k = 0; k < SPIN && job->done.load(std::memory_order_acquire) != n; k++) std::this_thread::yield();
         std::unique_lock<std::mutex> lk(mu_);
         done_cv_.wait(lk, [&] { return job->done.load() == n; });
     }
@@ -148,10 +149,13 @@ private:
         unsigned long long seen = 0;
         for (;;) {
             std::shared_ptr<Job> job;
+            // a regrid posts several jobs in a row: look for the next one for a short while
+            // (bounded) before sleeping on the condition variable
+            for (int k = 0; k < SPIN && gen_.load(std::memory_order_acquire) == seen; k++) std::this_thread::yield();
             {
                 std::unique_lock<std::mutex> lk(mu_);
-                cv_.wait(lk, [&] { return gen_ != seen; });
-                seen = gen_;
+                cv_.wait(lk, [&] { return gen_.load() != seen; });
+                seen = gen_.load();
                 job = cur_;
             }
             if (job->slots.fetch_sub(1) > 0) work(*job);
@@ -160,7 +164,8 @@ private:
     std::mutex mu_;
     std::condition_variable cv_, done_cv_;
     std::shared_ptr<Job> cur_;
-    unsigned long long gen_ = 0;
+    std::atomic<unsigned long long> gen_{0};
+    static constexpr int SPIN = 4000;                  // yields before a worker sleeps
     int nworkers_ = 0;
 };
 
@@ -383,13 +388,15 @@ bool Forest::build(const std::vector<Leaf>& leaves, std::string& err)
     return true;
 }
 
+void parallel_for(int n, const std::function<void(int)>& fn) { run_tasks(n, 16, fn); }
+
 // ---------------------------------------------------------------------------
 // adaptation
 // ---------------------------------------------------------------------------
 // The leaves that replace patches list[0..n) of one instance (all patches: list null),
 // 2:1 balanced within the instance (instances never touch one another).
 static std::vector<Leaf> adapt_patches(const Forest& f, const std::vector<int>& mark, const int* list, int n,
-                                       int& changed)
+                                       int& changed, bool threads)
 {
     const int np = f.np();
     std::vector<Leaf> L;
@@ -432,29 +439,51 @@ static std::vector<Leaf> adapt_patches(const Forest& f, const std::vector<int>& 
         std::vector<int> check(L.size());
         for (int i = 0; i < (int)L.size(); i++) check[i] = i;
         std::vector<int> ref, again;
-        std::vector<char> queued(L.size(), 0);
-        while (!check.empty()) {
-            ref.clear();
-            again.clear();
-            for (int i : check) {
+        int kmin = 99;                                  // no leaf is coarser, now or later
+        for (const Leaf& q : L) kmin = std::min(kmin, q.level);
+        // leaves check[a, b): the too-coarse neighbours found (in discovery order, repeats
+        // kept) and the leaves that found one
+        auto scan = [&](size_t a, size_t b, std::vector<int>& found, std::vector<int>& hit) {
+            for (size_t t = a; t < b; t++) {
+                const int i = check[t];
                 const int l = L[i].level, in = L[i].inst;
+                bool any = false;
                 for (int dy = -1; dy <= 1; dy++)
                     for (int dx = -1; dx <= 1; dx++) {
                         if (!dx && !dy) continue;
                         int x, y;
                         if (f.step(in, l, L[i].gx, L[i].gy, dx, dy, x, y) != 1) continue;
-                        for (int k = l - 2; k >= 0; k--) {
+                        for (int k = l - 2; k >= kmin; k--) {
                             const int j = idx.get(Forest::key(in, k, x >> (l - k), y >> (l - k)));
-                            if (j >= 0) {
-                                if (!dead[j]) { dead[j] = 1; ref.push_back(j); }
-                                if (!queued[i]) { queued[i] = 1; again.push_back(i); }
-                                break;
-                            }
+                            if (j >= 0) { found.push_back(j); any = true; break; }
                         }
                     }
+                if (any) hit.push_back(i);
+            }
+        };
+        constexpr size_t SCAN = 512;                    // leaves per task of a threaded pass
+        std::vector<std::vector<int>> found, hit;
+        while (!check.empty()) {
+            ref.clear();
+            again.clear();
+            // a pass only reads idx, so its leaves are scanned in chunks (on threads for a
+            // large pass) and the chunks' findings merged in check order: the same lists
+            // as one scan in order
+            const size_t nc = (threads && check.size() > 2 * SCAN) ? (check.size() + SCAN - 1) / SCAN : 1;
+            found.resize(std::max(found.size(), nc));
+            hit.resize(std::max(hit.size(), nc));
+            for (size_t c = 0; c < nc; c++) { found[c].clear(); hit[c].clear(); }
+            if (nc == 1) scan(0, check.size(), found[0], hit[0]);
+            else
+                run_tasks((int)nc, 16, [&](int c) {
+                    scan(c * SCAN, std::min(check.size(), (c + 1) * SCAN), found[c], hit[c]);
+                });
+            for (size_t c = 0; c < nc; c++) {
+                for (int j : found[c]) if (!dead[j]) { dead[j] = 1; ref.push_back(j); }
+                again.insert(again.end(), hit[c].begin(), hit[c].end());
             }
             check.clear();
-            for (int i : again) { queued[i] = 0; if (!dead[i]) check.push_back(i); }
+            for (int i : again) if (!dead[i]) check.push_back(i);
             for (int j : ref) {
                 idx.put(Forest::key(L[j].inst, L[j].level, L[j].gx, L[j].gy), -1);
                 const Leaf P = L[j];
@@ -462,7 +491,6 @@ static std::vector<Leaf> adapt_patches(const Forest& f, const std::vector<int>& 
                     const int n = (int)L.size();
                     L.push_back({P.level + 1, 2 * P.gx + (c & 1), 2 * P.gy + (c >> 1), P.inst});
                     dead.push_back(0);
-                    queued.push_back(0);
                     idx.put(Forest::key(L[n].inst, L[n].level, L[n].gx, L[n].gy), n);
                     check.push_back(n);
                 }
@@ -486,14 +514,14 @@ std::vector<Leaf> adapt_leaves(const Forest& f, const std::vector<int>& mark, in
 {
     (void)err;
     const int ni = f.ninst(), np = f.np();
-    if (ni <= 1) return adapt_patches(f, mark, nullptr, np, changed);
+    if (ni <= 1) return adapt_patches(f, mark, nullptr, np, changed, true);
     // a batch: the instances on threads, their leaves in instance order
     std::vector<std::vector<int>> list(ni);
     for (int i = 0; i < np; i++) list[f.p[i].inst].push_back(i);
     std::vector<std::vector<Leaf>> out(ni);
     std::vector<int> ch(ni, 0);
     const int nt = std::max(1, std::min((int)std::thread::hardware_concurrency(), 16));
-    run_tasks(ni, nt, [&](int k) { out[k] = adapt_patches(f, mark, list[k].data(), (int)list[k].size(), ch[k]); });
+    run_tasks(ni, nt, [&](int k) { out[k] = adapt_patches(f, mark, list[k].data(), (int)list[k].size(), ch[k], false); });
     std::vector<Leaf> L;
     changed = 0;
     for (int k = 0; k < ni; k++) {

@@ -10,6 +10,7 @@
 #include <stdint.h>
 #include <string>
 #include <unordered_map>
+#include <functional>
 #include <vector>
 #include "kernels.h"
 
@@ -188,6 +189,9 @@ struct TableWork {
     std::vector<std::vector<int>> iop_first;               // per coarse level: CSR offsets over its fine patches
     std::vector<std::vector<InterpEnt>> interp;            // interpolation entries per task
 };
+
+// fn(0) .. fn(n - 1) on the host worker threads (the caller's among them); returns when all are done.
+void parallel_for(int n, const std::function<void(int)>& fn);
 
 // inflow: mthbc = 0 sides are set to a constant state (PhysEnt.cst = 1, src unused).
 // False (with err) if a table would index outside the patches.
