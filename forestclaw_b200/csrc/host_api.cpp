@@ -82,7 +82,7 @@ struct DevVec {
         if (v.size() > cap) {
             if (p) cudaFree(p);
             p = nullptr;
-            cap = v.size() + v.size() / 4 + 16;
+            cap = v.size() + v.size() / 2 + 16;
             cudaError_t e = cudaMalloc(&p, cap * sizeof(T));
             if (e != cudaSuccess) { cap = 0; return e; }
         }
@@ -101,7 +101,7 @@ struct DevView {
 
 // The ghost-fill and time-sync tables of a forest: one device allocation filled from
 // one pinned host buffer, so a regrid uploads them with one copy.  Both grow by a
-// quarter beyond the largest forest seen and are reused from one regrid to the next.
+// half beyond the largest forest seen and are reused from one regrid to the next.
 struct TableArena {
     char* dev = nullptr;
     char* host = nullptr;
@@ -129,7 +129,7 @@ struct TableArena {
         if (dev) cudaFree(dev);
         if (host) cudaFreeHost(host);
         dev = nullptr; host = nullptr; cap = 0;
-        const size_t c = bytes + bytes / 4 + (64 << 10);
+        const size_t c = bytes + bytes / 2 + (1 << 20);
         cudaError_t e = cudaMalloc(&dev, c);
         if (e == cudaSuccess) e = cudaHostAlloc(&host, c, cudaHostAllocDefault);
         if (e != cudaSuccess) return e;
@@ -328,7 +328,7 @@ static int alloc_slabs(fc2d_b200_solver* s, int np)
 {
     const Dims& d = s->d;
     if (np <= s->cap && s->q) return 0;
-    int cap = np + np / 4 + 16;
+    int cap = np + np / 2 + 16;                   // a growing forest reallocates rarely
     double *q, *ql, *qi = nullptr, *aux = nullptr, *regs, *area = nullptr;
     PatchDesc* desc;
     if (s->sphere) CK(cudaMalloc(&area, (size_t)cap * d.narea() * sizeof(double)));
@@ -374,7 +374,8 @@ static int ensure_spare(fc2d_b200_solver* s, int np)
     if (sp.q && np <= sp.cap) return 0;
     free_spare(s);
     const Dims& d = s->d;
-    const int cap = np + np / 4 + 16;
+    // the spare and the current slabs swap at every regrid: the spare at least as large
+    const int cap = std::max(np + np / 2 + 16, s->cap);
     CK(cudaMalloc(&sp.q, (size_t)cap * d.nq() * sizeof(double)));
     CK(cudaMalloc(&sp.qlast, (size_t)cap * d.nq() * sizeof(double)));
     if (s->o.subcycle) CK(cudaMalloc(&sp.qinterp, (size_t)cap * d.nq() * sizeof(double)));
