@@ -669,7 +669,8 @@ def run_ours(args, wl, rank, world, local_rank):
                        "the workload's regrid (host tree edit, device repopulation, graph recapture) inside "
                        "the wall-clock region; the same coarse steps as the device-timed loop, from the same "
                        "state (a second solver spun up the same way)",
-           "cells_match_timed_loop": bool(e2e_cells == cells_all)}
+           "cells_match_timed_loop": bool(e2e_cells == cells_all),
+           "graphs": g.graph_stats()}
     g.close()
     fp64 = None
     if args.precision != "fp64" and not args.no_fp64_compare:

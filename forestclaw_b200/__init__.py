@@ -207,6 +207,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fc2d_b200_synchronize": [P],
         "fc2d_b200_last_update_stats": [P, dp, dp, ip, ip],
         "fc2d_b200_last_step_timing": [P, dp, dp],
+        "fc2d_b200_graph_stats": [P, ip, ip],
         "fc2d_b200_last_regrid_stats": [P, dp],
         "fc2d_b200_set_timing": [P, I],
         "fc2d_b200_event_record": [P, I],
@@ -725,6 +726,12 @@ class Solver:
                                                          ctypes.byref(ul), ctypes.byref(tl)))
         return {"update_ms": ms.value, "update_bytes": by.value, "update_launches": ul.value,
                 "total_launches": tl.value}
+
+    def graph_stats(self) -> dict:
+        """Advance graphs so far: instantiations and in-place updates (fc2d_b200_graph_stats)."""
+        b, u = ctypes.c_int(), ctypes.c_int()
+        self._check("fc2d_b200_graph_stats", self.lib.fc2d_b200_graph_stats(self.h, ctypes.byref(b), ctypes.byref(u)))
+        return {"builds": b.value, "updates": u.value}
 
     def last_step_timing(self) -> dict:
         """The most recent advance: host schedule time and the device span of its work (ms)."""

@@ -2170,6 +2170,14 @@ extern "C" int fc2d_b200_last_update_stats(const fc2d_b200_solver_t* s, double* 
     return 0;
 }
 
+extern "C" int fc2d_b200_graph_stats(const fc2d_b200_solver_t* s, int* builds, int* updates)
+{
+    if (!s) return fail(FC2D_B200_EINVAL, "null solver");
+    if (builds) *builds = s->graph_builds;
+    if (updates) *updates = s->graph_updates;
+    return 0;
+}
+
 extern "C" int fc2d_b200_last_step_timing(const fc2d_b200_solver_t* s, double* host_ms, double* device_ms)
 {
     if (!s) return fail(FC2D_B200_EINVAL, "null solver");

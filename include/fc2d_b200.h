@@ -388,6 +388,10 @@ int fc2d_b200_last_regrid_stats(const fc2d_b200_solver_t* s, double* ms);
 /* Replay each fclaw2d_advance_all_levels as a CUDA graph captured once per
  * forest (on by default; disabled while update timing is on). */
 int fc2d_b200_set_graphs(fc2d_b200_solver_t* s, int enable);
+/* The advance graphs so far: builds, instantiations of a captured graph (the first
+ * advance, or a capture whose launches differ from the graph's); updates, captures
+ * after a regrid applied to the existing graph in place (cudaGraphExecUpdate). */
+int fc2d_b200_graph_stats(const fc2d_b200_solver_t* s, int* builds, int* updates);
 /* Launch the kernels of an advance (level updates, ghost-fill stages, time
  * sync, time interpolation) with programmatic dependent launch: each grid is
  * scheduled while its predecessor's last CTAs run and waits in-kernel for the
