@@ -354,9 +354,12 @@ int fc2d_b200_mass(fc2d_b200_solver_t* s, double* out);
  * the library until the process exits), so npatches*meqn + meqn must not exceed
  * it (else FC2D_B200_EINVAL, nothing runs).
  * Same result as fc2d_b200_mass, bit for bit.  No part of the scratch has to
- * start at zero.  The first call on a device resolves the scratch address; make
- * it before any stream capture begins on that device.  Calls that overlap in
- * time on one device (several host threads) share the scratch and race. */
+ * start at zero.  fc2d_b200_create loads the module that holds the array and
+ * resolves its device address (cudaGetSymbolAddress, once per device per
+ * process), so this call itself loads and looks up nothing.  The cached address
+ * is invalid after the device's primary context is destroyed (cudaDeviceReset):
+ * create no solver across such a reset.  Calls that overlap in time on one
+ * device (several host threads) share the scratch and race. */
 #define FC2D_B200_MASS_SCRATCH_DOUBLES 131072
 int fc2d_b200_mass_noalloc(fc2d_b200_solver_t* s, double* out);
 /* Newton iterations of the exact Euler solver: out[k] = interfaces solved in k
